@@ -1,0 +1,244 @@
+/*
+ * pa_b200.h -- C ABI of libpa_b200.so, a B200 (sm_100a) implementation of
+ * Plato Analyze's per-cell linear-tetrahedron hot path: SIMP elastostatics
+ * (residual, state/control Jacobians), the "Internal Elastic Energy"
+ * (compliance) criterion, a matrix-free Jacobi-PCG solve of the constrained
+ * system, and the J2 radial return.
+ *
+ * Conventions
+ *  - Every entry point returns pa_status (0 = success).  No C++ exception
+ *    crosses this boundary; pa_last_error() returns the calling thread's
+ *    last message.
+ *  - Array arguments may be device pointers or host pointers (pageable or
+ *    pinned).  Host arrays are staged through library-owned device buffers;
+ *    an entry point that was given a host output returns after the result
+ *    is on the host.  Device-only calls are asynchronous on the problem's
+ *    stream, except those that return a host scalar.
+ *  - Sizes are implied by the mesh: N nodes, C cells, 3N state dofs, B CRS
+ *    blocks (pa_mesh_sizes).  Nodal vectors are interleaved (x,y,z) per
+ *    node, as the reference's ScalarVector of a 3-dof-per-node physics.
+ *  - Handles are not reentrant: one host thread drives one pa_problem at a
+ *    time.  Several problems may share a mesh.
+ *
+ * Each declaration names the reference interface it replaces (paths relative
+ * to the platoanalyze source tree).
+ */
+#ifndef PA_B200_H
+#define PA_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  PA_OK = 0,
+  PA_ERR_INVALID_ARG = 1,  /* bad pointer, size or parameter */
+  PA_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+  PA_ERR_NOT_CONVERGED = 3,/* iteration cap reached before the tolerance */
+  PA_ERR_BREAKDOWN = 4,    /* Krylov breakdown (p.Ap <= 0 or non-finite) */
+  PA_ERR_NONFINITE = 5,    /* NaN/Inf in an input or a reduction */
+  PA_ERR_NO_DEVICE = 6,    /* no CUDA device visible */
+  PA_ERR_UNSUPPORTED = 7   /* valid request this build does not serve */
+} pa_status;
+
+typedef struct pa_mesh pa_mesh;
+typedef struct pa_problem pa_problem;
+
+/* Library version string and the calling thread's last error message. */
+const char* pa_version(void);
+const char* pa_last_error(void);
+
+/* ---------------------------------------------------------------- mesh --- */
+
+/* Linear-tet mesh from connectivity (C x 4, int32) and coordinates (N x 3).
+ * Replaces the Omega_h::Mesh the reference's SpatialModel wraps
+ * (src/SpatialModel.hpp:15-149) and the node-star CRS graph of
+ * CreateBlockMatrix (src/ImplicitFunctors.hpp:735-808).  Builds the
+ * block-CRS graph (columns sorted ascending, diagonal included) and the
+ * shared-memory cell tiles the kernels use. */
+pa_status pa_mesh_create(const int32_t* cells2nodes, int64_t num_cells, const double* coords,
+                         int64_t num_nodes, pa_mesh** out);
+
+/* Structured box [0,lx]x[0,ly]x[0,lz] with nx*ny*nz hexes, each split into
+ * six tets around its (0,0,0)-(1,1,1) diagonal in the order of the
+ * reference's single-hex box (unit_tests/OmegaHUtilitiesTests.cpp:258-287).
+ * Nodes are numbered x fastest.  Stands in for Omega_h::build_box
+ * (unit_tests/PlatoTestHelpers.hpp:240-249) with this build's own numbering. */
+pa_status pa_mesh_create_box(int32_t nx, int32_t ny, int32_t nz, double lx, double ly, double lz,
+                             pa_mesh** out);
+
+pa_status pa_mesh_destroy(pa_mesh* mesh);
+
+/* Sizes: cells C, nodes N, CRS blocks B, cell tiles T. Any output may be NULL. */
+pa_status pa_mesh_sizes(const pa_mesh* mesh, int64_t* num_cells, int64_t* num_nodes,
+                        int64_t* num_blocks, int64_t* num_tiles);
+
+/* Host copies of the connectivity (C x 4) and coordinates (N x 3). */
+pa_status pa_mesh_get(const pa_mesh* mesh, int32_t* cells2nodes, double* coords);
+
+/* Host copy of the block-CRS graph: rowmap (N+1), cols (B). */
+pa_status pa_mesh_graph(const pa_mesh* mesh, int32_t* rowmap, int32_t* cols);
+
+/* Replace the CRS graph by a caller's graph with the same nonzero pattern but
+ * any in-row column order, e.g. the Omega_h star order the reference's
+ * CrsMatrix carries (src/alg/CrsMatrix.hpp:28-30).  gradient_u and
+ * gradient_z then fill entries in that order. */
+pa_status pa_mesh_set_graph(pa_mesh* mesh, const int32_t* rowmap, const int32_t* cols, int64_t num_blocks);
+
+/* Boundary faces (triangles, 3 node ids each) lying on the plane
+ * coord[axis] == value.  Call with faces == NULL to get the count. */
+pa_status pa_mesh_boundary_faces(const pa_mesh* mesh, int32_t axis, double value, int32_t* faces,
+                                 int64_t* num_faces);
+
+/* ------------------------------------------------------------- problem --- */
+
+#define PA_CONTROL_NODAL 0 /* reference layout: N nodal controls, cell density = mean of 4 */
+#define PA_CONTROL_CELL 1  /* one density per cell; gradient_z is per cell */
+
+/* Material and penalty, the "Isotropic Linear Elastic" material
+ * (src/IsotropicLinearElasticMaterial.cpp:86-108) and the SIMP "Penalty
+ * Function" keys Exponent / Minimum Value (src/Simp.hpp:41-50). */
+typedef struct {
+  double youngs_modulus;
+  double poissons_ratio;
+  double simp_exponent;
+  double simp_min;
+  int32_t control_layout;
+} pa_elastic_params;
+
+/* Elliptic mechanics problem on `mesh` (src/elliptic/Problem.hpp:93-114).
+ * `stream` is a cudaStream_t (NULL: the library creates its own). */
+pa_status pa_problem_create(pa_mesh* mesh, const pa_elastic_params* params, void* stream, pa_problem** out);
+pa_status pa_problem_destroy(pa_problem* problem);
+
+/* Uniform traction `flux` on boundary triangles: NaturalBC "Uniform" with
+ * SurfaceLoadIntegral (src/NaturalBC.hpp:41-110, src/SurfaceLoadIntegral.hpp:96-160).
+ * Adds to the problem's load set. */
+pa_status pa_problem_add_traction(pa_problem* problem, const int32_t* faces, int64_t num_faces,
+                                  const double flux[3]);
+pa_status pa_problem_clear_tractions(pa_problem* problem);
+
+/* Essential BCs: dof ids (3*node + component) and values
+ * (Elliptic::Problem::setEssentialBoundaryConditions, src/elliptic/Problem.hpp:636-650). */
+pa_status pa_problem_set_dirichlet(pa_problem* problem, const int32_t* dofs, const double* values, int64_t n);
+
+/* --------------------------------------- Elliptic::VectorFunction --------- */
+
+/* r = K(z) u - F_traction: VectorFunction::value (src/elliptic/VectorFunction.hpp:231-310). */
+pa_status pa_vf_value(pa_problem* problem, const double* u, const double* z, double* r);
+
+/* dR/du into 9*B block-CRS entries [block][i][j] on the mesh graph:
+ * VectorFunction::gradient_u (src/elliptic/VectorFunction.hpp:505-594). */
+pa_status pa_vf_gradient_u(pa_problem* problem, const double* u, const double* z, double* entries);
+
+/* dR/dz, transposed: nodal layout -> 3*B entries of 1x3 blocks (row =
+ * control node, col = state node) on the mesh graph; cell layout -> 12*C
+ * entries (row = cell, its 4 nodes x 3 dofs in local order).
+ * VectorFunction::gradient_z (src/elliptic/VectorFunction.hpp:598-689). */
+pa_status pa_vf_gradient_z(pa_problem* problem, const double* u, const double* z, double* entries);
+
+/* --------------------- PhysicsScalarFunction "Internal Elastic Energy" ---- */
+
+/* f = sum_c 1/2 vol p(rho) eps:C:eps  (src/elliptic/PhysicsScalarFunction.hpp:225,
+ * src/elliptic/InternalElasticEnergy.hpp:100-158).  `value` is a host pointer. */
+pa_status pa_sf_value(pa_problem* problem, const double* u, const double* z, double* value);
+/* df/du, 3N (src/elliptic/PhysicsScalarFunction.hpp:365). */
+pa_status pa_sf_gradient_u(pa_problem* problem, const double* u, const double* z, double* grad);
+/* df/dz, N (nodal) or C (cell) (src/elliptic/PhysicsScalarFunction.hpp:432). */
+pa_status pa_sf_gradient_z(pa_problem* problem, const double* u, const double* z, double* grad);
+
+/* ----------------------------------------------------- matrix-free ------- */
+
+#define PA_FP64 0
+#define PA_FP32 1
+
+/* y = K(z) x without assembling K.  precision PA_FP64 (x, y double) or
+ * PA_FP32 (x, y float).  constrained != 0 applies the symmetric Dirichlet
+ * elimination of applyBlockConstraints (src/ApplyConstraints.hpp:11-79):
+ * constrained rows and columns removed, identity on the diagonal.  No
+ * reference counterpart (the reference always assembles). */
+pa_status pa_apply(pa_problem* problem, const double* z, const void* x, void* y, int32_t precision,
+                   int32_t constrained);
+
+/* Symmetric Dirichlet elimination on an assembled block CRS + rhs with the
+ * problem's BCs times `scale`: applyBlockConstraints<3> (src/ApplyConstraints.hpp:11-79). */
+pa_status pa_apply_block_constraints(pa_problem* problem, double* entries, double* rhs, double scale);
+
+/* ----------------------------------------------------------- solver ------ */
+
+#define PA_SOLVER_PCG_FP64 0  /* matrix-free Jacobi-PCG, FP64 throughout */
+#define PA_SOLVER_PCG_MIXED 1 /* FP32 apply/vectors, FP64 dots, FP64 true-residual updates */
+
+typedef struct {
+  int32_t method;        /* PA_SOLVER_* */
+  double rel_tol;        /* ||b - K x|| / ||b|| target */
+  int32_t max_iters;     /* <= 0: 20 * sqrt(ndof) + 1000 */
+  int32_t check_every;   /* iterations between convergence checks / residual replacement */
+  int32_t use_initial_guess; /* 0: start from x = 0 (as Problem::solution does) */
+} pa_solve_options;
+
+typedef struct {
+  int32_t iterations;     /* CG iterations */
+  int32_t replacements;   /* FP64 true-residual replacements (mixed) */
+  double rel_residual;    /* final FP64 ||b - K x|| / ||b|| of the constrained system */
+  double seconds;         /* device time of the solve */
+  int32_t converged;
+  int64_t kernel_launches; /* kernels this library launched for the solve */
+} pa_solve_stats;
+
+pa_status pa_solve_options_default(pa_solve_options* options);
+
+/* Solve the Dirichlet-constrained system K(z) x = b (b unconstrained; the
+ * problem's BC values are imposed as applyBlockConstraints does) -- the
+ * AbstractSolver::solve boundary (src/alg/PlatoAbstractSolver.hpp:19-27). */
+pa_status pa_solve(pa_problem* problem, const double* z, const double* b, double* x,
+                   const pa_solve_options* options, pa_solve_stats* stats);
+
+/* Elliptic::Problem::solution (src/elliptic/Problem.hpp:259-311): u = 0,
+ * R = value(u, z), solve K du = -R with BCs, u += du. */
+pa_status pa_problem_solution(pa_problem* problem, const double* z, double* u,
+                              const pa_solve_options* options, pa_solve_stats* stats);
+
+/* Elliptic::Problem::criterionGradient for the energy criterion
+ * (src/elliptic/Problem.hpp:413-468).  self_adjoint != 0: -df/dz.  Otherwise
+ * the adjoint route: K lambda = -df/du with zero BCs, g = df/dz + (dR/dz)^T lambda. */
+pa_status pa_problem_criterion_gradient(pa_problem* problem, const double* z, const double* u, double* grad,
+                                        int32_t self_adjoint, const pa_solve_options* options);
+
+/* Diagnostic, no reference counterpart: average device time (ms) of one
+ * fused CG kernel launch (p update + matrix-free K p + p.Kp, the solver's
+ * hot kernel) over `reps` back-to-back launches on the problem's stream,
+ * and its algorithmic bytes per launch:
+ * C*(16 + s) + N*6*3*s, s = 4 (PA_FP32) or 8 (PA_FP64). */
+pa_status pa_time_cg_apply(pa_problem* problem, const double* z, int32_t precision, int32_t reps,
+                           double* ms_per_launch, int64_t* algorithmic_bytes);
+
+/* ---------------------------------------------------------- J2 return ---- */
+
+/* J2 parameters: "Isotropic Linear Elastic" + "J2 Plasticity" keys of
+ * J2PlasticityLocalResidual::initialize (src/J2PlasticityLocalResidual.hpp:130-200). */
+typedef struct {
+  double youngs_modulus;
+  double poissons_ratio;
+  double initial_yield_stress;
+  double hardening_modulus_isotropic;
+  double hardening_modulus_kinematic;
+  double elastic_penalty_exponent;   /* reference default 1.0 */
+  double elastic_min_ersatz;         /* reference default 1e-9 */
+  double plastic_penalty_exponent;   /* reference default 0.5 */
+  double plastic_min_ersatz;         /* reference default 1e-4 */
+} pa_j2_params;
+
+/* Radial return of every cell: J2PlasticityLocalResidual::updateLocalState
+ * (src/J2PlasticityLocalResidual.hpp:421-523).  u: 3N displacements;
+ * z: N nodal densities; prev_local / local: C x 14 local states
+ * [acc. plastic strain, dgamma, plastic strain (6), backstress (6)]. */
+pa_status pa_j2_radial_return(pa_problem* problem, const pa_j2_params* params, const double* u, const double* z,
+                              const double* prev_local, double* local);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PA_B200_H */

@@ -1,0 +1,340 @@
+"""Host-side mirror of Plato Analyze's interfaces for the linear-tet hot path.
+
+Class and method names follow the reference so that its callers and tests
+translate line by line:
+
+* ``Problem``               - Elliptic::Problem (src/elliptic/Problem.hpp:44-715):
+                              solution(z), criterionValue, criterionGradient.
+* ``VectorFunction``        - Elliptic::VectorFunction (src/elliptic/VectorFunction.hpp):
+                              value / gradient_u / gradient_z.
+* ``PhysicsScalarFunction`` - "Internal Elastic Energy"
+                              (src/elliptic/PhysicsScalarFunction.hpp): value / gradient_u / gradient_z.
+
+All arithmetic happens in libpa_b200.so through the C ABI (include/pa_b200.h).
+Arrays may be NumPy arrays (host) or torch CUDA tensors (device); results
+come back in the kind of array the first array argument was.
+"""
+import ctypes as ct
+
+import numpy as np
+
+from . import _abi
+
+_NP = {np.float64: "float64", np.float32: "float32", np.int32: "int32"}
+
+
+def _is_torch(a):
+    return type(a).__module__.startswith("torch")
+
+
+def _ptr(a, dtype, count=None, name="array"):
+    """Raw pointer of a contiguous array of `dtype` (NumPy or torch)."""
+    if a is None:
+        return None
+    if _is_torch(a):
+        import torch
+        want = {np.float64: torch.float64, np.float32: torch.float32, np.int32: torch.int32}[dtype]
+        if a.dtype != want or not a.is_contiguous():
+            raise TypeError(f"{name}: need a contiguous torch tensor of {want}")
+        if count is not None and a.numel() != count:
+            raise ValueError(f"{name}: expected {count} entries, got {a.numel()}")
+        return ct.c_void_p(a.data_ptr())
+    if not isinstance(a, np.ndarray) or a.dtype != dtype or not a.flags.c_contiguous:
+        raise TypeError(f"{name}: need a C-contiguous numpy array of {np.dtype(dtype)}")
+    if count is not None and a.size != count:
+        raise ValueError(f"{name}: expected {count} entries, got {a.size}")
+    return ct.c_void_p(a.ctypes.data)
+
+
+def _empty(like, n, dtype=np.float64):
+    if like is not None and _is_torch(like):
+        import torch
+        t = {np.float64: torch.float64, np.float32: torch.float32}[dtype]
+        return torch.empty(n, dtype=t, device=like.device)
+    return np.empty(n, dtype=dtype)
+
+
+def _as(a, dtype):
+    if a is None or _is_torch(a):
+        return a
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+class Mesh:
+    """Linear-tet mesh: connectivity, coordinates, block-CRS graph, cell tiles."""
+
+    def __init__(self, handle):
+        self._lib = _abi.load()
+        self._h = handle
+        C, N, B, T = (ct.c_int64() for _ in range(4))
+        _abi.check(self._lib.pa_mesh_sizes(self._h, ct.byref(C), ct.byref(N), ct.byref(B), ct.byref(T)))
+        self.num_cells, self.num_nodes, self.num_blocks, self.num_tiles = C.value, N.value, B.value, T.value
+
+    @classmethod
+    def box(cls, nx, ny, nz, lx=1.0, ly=1.0, lz=1.0):
+        lib = _abi.load()
+        h = ct.c_void_p()
+        _abi.check(lib.pa_mesh_create_box(nx, ny, nz, lx, ly, lz, ct.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_arrays(cls, cells, coords):
+        lib = _abi.load()
+        cells = np.ascontiguousarray(cells, dtype=np.int32)
+        coords = np.ascontiguousarray(coords, dtype=np.float64)
+        h = ct.c_void_p()
+        _abi.check(lib.pa_mesh_create(_ptr(cells, np.int32), cells.shape[0], _ptr(coords, np.float64),
+                                      coords.shape[0], ct.byref(h)))
+        return cls(h)
+
+    def arrays(self):
+        cells = np.empty((self.num_cells, 4), np.int32)
+        coords = np.empty((self.num_nodes, 3), np.float64)
+        _abi.check(self._lib.pa_mesh_get(self._h, _ptr(cells, np.int32), _ptr(coords, np.float64)))
+        return cells, coords
+
+    def graph(self):
+        rowmap = np.empty(self.num_nodes + 1, np.int32)
+        cols = np.empty(self.num_blocks, np.int32)
+        _abi.check(self._lib.pa_mesh_graph(self._h, _ptr(rowmap, np.int32), _ptr(cols, np.int32)))
+        return rowmap, cols
+
+    def set_graph(self, rowmap, cols):
+        rowmap = np.ascontiguousarray(rowmap, np.int32)
+        cols = np.ascontiguousarray(cols, np.int32)
+        _abi.check(self._lib.pa_mesh_set_graph(self._h, _ptr(rowmap, np.int32), _ptr(cols, np.int32), cols.size))
+
+    def boundary_faces(self, axis, value):
+        n = ct.c_int64()
+        _abi.check(self._lib.pa_mesh_boundary_faces(self._h, axis, float(value), None, ct.byref(n)))
+        faces = np.empty((n.value, 3), np.int32)
+        _abi.check(self._lib.pa_mesh_boundary_faces(self._h, axis, float(value), _ptr(faces, np.int32), ct.byref(n)))
+        return faces
+
+    def close(self):
+        if self._h:
+            self._lib.pa_mesh_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class SolveOptions:
+    def __init__(self, method="fp64", rel_tol=1e-10, max_iters=0, check_every=64, use_initial_guess=False):
+        self.method, self.rel_tol, self.max_iters = method, rel_tol, max_iters
+        self.check_every, self.use_initial_guess = check_every, use_initial_guess
+
+    def c(self):
+        o = _abi.SolveOptions()
+        _abi.load().pa_solve_options_default(ct.byref(o))
+        o.method = {"fp64": _abi.PA_SOLVER_PCG_FP64, "mixed": _abi.PA_SOLVER_PCG_MIXED}[self.method]
+        o.rel_tol = float(self.rel_tol)
+        o.max_iters = int(self.max_iters)
+        o.check_every = int(self.check_every)
+        o.use_initial_guess = int(bool(self.use_initial_guess))
+        return o
+
+
+class Problem:
+    """Elliptic mechanics problem (Elliptic::Problem<Mechanics<3>>)."""
+
+    def __init__(self, mesh, youngs_modulus=1.0, poissons_ratio=0.3, simp_exponent=3.0, simp_min=1e-9,
+                 control_layout="nodal", stream=None):
+        self._lib = _abi.load()
+        self.mesh = mesh
+        self.control_layout = control_layout
+        p = _abi.ElasticParams(youngs_modulus, poissons_ratio, simp_exponent, simp_min,
+                               _abi.PA_CONTROL_CELL if control_layout == "cell" else _abi.PA_CONTROL_NODAL)
+        h = ct.c_void_p()
+        _abi.check(self._lib.pa_problem_create(mesh._h, ct.byref(p), ct.c_void_p(stream or 0), ct.byref(h)))
+        self._h = h
+        self.ndof = 3 * mesh.num_nodes
+        self.nz = mesh.num_cells if control_layout == "cell" else mesh.num_nodes
+
+    # -- boundary conditions -------------------------------------------------
+    def add_traction(self, faces, flux):
+        faces = np.ascontiguousarray(faces, np.int32)
+        flux = np.ascontiguousarray(flux, np.float64)
+        _abi.check(self._lib.pa_problem_add_traction(self._h, _ptr(faces, np.int32), faces.shape[0],
+                                                     _ptr(flux, np.float64, 3)))
+
+    def clear_tractions(self):
+        _abi.check(self._lib.pa_problem_clear_tractions(self._h))
+
+    def set_dirichlet(self, dofs, values=None):
+        dofs = np.ascontiguousarray(dofs, np.int32)
+        values = np.zeros(dofs.size) if values is None else np.ascontiguousarray(values, np.float64)
+        _abi.check(self._lib.pa_problem_set_dirichlet(self._h, _ptr(dofs, np.int32), _ptr(values, np.float64),
+                                                      dofs.size))
+
+    # -- functions -------------------------------------------------------------
+    def vector_function(self):
+        return VectorFunction(self)
+
+    def scalar_function(self, name="Internal Elastic Energy"):
+        if name != "Internal Elastic Energy":
+            raise NotImplementedError(f"criterion {name!r} is outside this build's scope")
+        return PhysicsScalarFunction(self)
+
+    def apply(self, z, x, y=None, constrained=False):
+        """Matrix-free y = K(z) x in the precision of x (float64 or float32)."""
+        z = _as(z, np.float64)
+        fp32 = (x.dtype == np.float32) if not _is_torch(x) else (str(x.dtype) == "torch.float32")
+        dt = np.float32 if fp32 else np.float64
+        y = _empty(x, self.ndof, dt) if y is None else y
+        _abi.check(self._lib.pa_apply(self._h, _ptr(z, np.float64, self.nz, "z"),
+                                      _ptr(x, dt, self.ndof, "x"), _ptr(y, dt, self.ndof, "y"),
+                                      _abi.PA_FP32 if fp32 else _abi.PA_FP64, int(bool(constrained))))
+        return y
+
+    def apply_block_constraints(self, entries, rhs, scale=1.0):
+        _abi.check(self._lib.pa_apply_block_constraints(self._h, _ptr(entries, np.float64, 9 * self.mesh.num_blocks),
+                                                        _ptr(rhs, np.float64, self.ndof), float(scale)))
+        return entries, rhs
+
+    # -- solves ------------------------------------------------------------------
+    def solve(self, z, b, x=None, options=None, allow_not_converged=False):
+        b = _as(b, np.float64)
+        z = _as(z, np.float64)
+        options = options or SolveOptions()
+        x = _empty(b, self.ndof) if x is None else x
+        st = _abi.SolveStats()
+        o = options.c()
+        s = self._lib.pa_solve(self._h, _ptr(z, np.float64, self.nz, "z"),
+                               _ptr(b, np.float64, self.ndof, "b"), _ptr(x, np.float64, self.ndof, "x"),
+                               ct.byref(o), ct.byref(st))
+        _abi.check(s, allow=(3,) if allow_not_converged else ())
+        return x, _stats(st)
+
+    def solution(self, z, u=None, options=None, allow_not_converged=False):
+        """Elliptic::Problem::solution: one Newton step from u = 0."""
+        z = _as(z, np.float64)
+        options = options or SolveOptions()
+        u = _empty(z, self.ndof) if u is None else u
+        st = _abi.SolveStats()
+        o = options.c()
+        s = self._lib.pa_problem_solution(self._h, _ptr(z, np.float64, self.nz, "z"),
+                                          _ptr(u, np.float64, self.ndof, "u"), ct.byref(o), ct.byref(st))
+        _abi.check(s, allow=(3,) if allow_not_converged else ())
+        return u, _stats(st)
+
+    def criterion_value(self, z, u):
+        return self.scalar_function().value(u, z)
+
+    def criterion_gradient(self, z, u, self_adjoint=True, options=None):
+        u = _as(u, np.float64)
+        z = _as(z, np.float64)
+        options = options or SolveOptions()
+        g = _empty(z, self.nz)
+        o = options.c()
+        _abi.check(self._lib.pa_problem_criterion_gradient(self._h, _ptr(z, np.float64, self.nz, "z"),
+                                                           _ptr(u, np.float64, self.ndof, "u"),
+                                                           _ptr(g, np.float64, self.nz, "grad"),
+                                                           int(bool(self_adjoint)), ct.byref(o)))
+        return g
+
+    def j2_radial_return(self, params, u, z, prev_local, local=None):
+        """J2PlasticityLocalResidual::updateLocalState for every cell (C x 14 states)."""
+        prev_local = _as(prev_local, np.float64)
+        u = _as(u, np.float64)
+        z = _as(z, np.float64)
+        C = self.mesh.num_cells
+        local = _empty(u, 14 * C) if local is None else local
+        jp = _abi.J2Params(*[float(params[k]) for k in (
+            "youngs_modulus", "poissons_ratio", "initial_yield_stress", "hardening_modulus_isotropic",
+            "hardening_modulus_kinematic", "elastic_penalty_exponent", "elastic_min_ersatz",
+            "plastic_penalty_exponent", "plastic_min_ersatz")])
+        _abi.check(self._lib.pa_j2_radial_return(self._h, ct.byref(jp), _ptr(u, np.float64, self.ndof),
+                                                 _ptr(z, np.float64, self.mesh.num_nodes),
+                                                 _ptr(prev_local, np.float64, 14 * C, "prev_local"),
+                                                 _ptr(local, np.float64, 14 * C, "local")))
+        return local
+
+    def close(self):
+        if self._h:
+            self._lib.pa_problem_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _stats(st):
+    return {"iterations": st.iterations, "replacements": st.replacements, "rel_residual": st.rel_residual,
+            "seconds": st.seconds, "converged": bool(st.converged), "kernel_launches": st.kernel_launches}
+
+
+class VectorFunction:
+    """Elliptic::VectorFunction for the elastostatics residual."""
+
+    def __init__(self, problem):
+        self.p = problem
+
+    def value(self, u, z, out=None):
+        u = _as(u, np.float64)
+        z = _as(z, np.float64)
+        out = _empty(u, self.p.ndof) if out is None else out
+        _abi.check(self.p._lib.pa_vf_value(self.p._h, _ptr(u, np.float64, self.p.ndof, "u"),
+                                           _ptr(z, np.float64, self.p.nz, "z"),
+                                           _ptr(out, np.float64, self.p.ndof, "r")))
+        return out
+
+    def gradient_u(self, u, z, out=None):
+        u = _as(u, np.float64)
+        z = _as(z, np.float64)
+        n = 9 * self.p.mesh.num_blocks
+        out = _empty(u, n) if out is None else out
+        _abi.check(self.p._lib.pa_vf_gradient_u(self.p._h, _ptr(u, np.float64, self.p.ndof, "u"),
+                                                _ptr(z, np.float64, self.p.nz, "z"),
+                                                _ptr(out, np.float64, n, "entries")))
+        return out
+
+    def gradient_z(self, u, z, out=None):
+        u = _as(u, np.float64)
+        z = _as(z, np.float64)
+        n = 12 * self.p.mesh.num_cells if self.p.control_layout == "cell" else 3 * self.p.mesh.num_blocks
+        out = _empty(u, n) if out is None else out
+        _abi.check(self.p._lib.pa_vf_gradient_z(self.p._h, _ptr(u, np.float64, self.p.ndof, "u"),
+                                                _ptr(z, np.float64, self.p.nz, "z"),
+                                                _ptr(out, np.float64, n, "entries")))
+        return out
+
+
+class PhysicsScalarFunction:
+    """PhysicsScalarFunction for the "Internal Elastic Energy" criterion."""
+
+    def __init__(self, problem):
+        self.p = problem
+
+    def value(self, u, z):
+        u = _as(u, np.float64)
+        z = _as(z, np.float64)
+        v = ct.c_double()
+        _abi.check(self.p._lib.pa_sf_value(self.p._h, _ptr(u, np.float64, self.p.ndof, "u"),
+                                           _ptr(z, np.float64, self.p.nz, "z"), ct.byref(v)))
+        return v.value
+
+    def gradient_u(self, u, z, out=None):
+        u = _as(u, np.float64)
+        z = _as(z, np.float64)
+        out = _empty(u, self.p.ndof) if out is None else out
+        _abi.check(self.p._lib.pa_sf_gradient_u(self.p._h, _ptr(u, np.float64, self.p.ndof, "u"),
+                                                _ptr(z, np.float64, self.p.nz, "z"),
+                                                _ptr(out, np.float64, self.p.ndof, "grad")))
+        return out
+
+    def gradient_z(self, u, z, out=None):
+        u = _as(u, np.float64)
+        z = _as(z, np.float64)
+        out = _empty(u, self.p.nz) if out is None else out
+        _abi.check(self.p._lib.pa_sf_gradient_z(self.p._h, _ptr(u, np.float64, self.p.ndof, "u"),
+                                                _ptr(z, np.float64, self.p.nz, "z"),
+                                                _ptr(out, np.float64, self.p.nz, "grad")))
+        return out

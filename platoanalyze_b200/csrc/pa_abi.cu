@@ -1,0 +1,628 @@
+// pa_abi.cu -- the extern "C" entry points of libpa_b200.so.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <memory>
+
+#include "pa_problem.cuh"
+#include "pa_cell.cuh"
+
+namespace pa {
+
+pa_status solve_device(Problem& P, const double* z, const double* b, double* x_out, const pa_solve_options& o,
+                       pa_solve_stats* st);
+void launch_dRdz_transpose_times(const Problem& P, const double* u, const double* z, const double* lambda,
+                                 double* g, cudaStream_t s);
+void launch_block_constraints(const Problem& P, double* entries, double* rhs, double scale, cudaStream_t s);
+void launch_scale(double* v, int64_t n, double a, cudaStream_t s);
+double time_cg_apply(Problem& P, const double* z, bool fp32, int reps);
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+int num_sms() {
+  static int cached[64] = {0};
+  int dev = 0;
+  PA_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) dev = 0;
+  if (!cached[dev]) PA_CUDA(cudaDeviceGetAttribute(&cached[dev], cudaDevAttrMultiProcessorCount, dev));
+  return cached[dev];
+}
+
+namespace {
+
+template <typename F>
+pa_status guard(F&& f) {
+  try {
+    f();
+    return PA_OK;
+  } catch (const Error& e) {
+    set_last_error(e.what());
+    return e.status;
+  } catch (const std::bad_alloc&) {
+    set_last_error("host allocation failed");
+    return PA_ERR_CUDA;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return PA_ERR_INVALID_ARG;
+  }
+}
+
+template <typename F>
+pa_status guard_status(F&& f) {
+  try {
+    return f();
+  } catch (const Error& e) {
+    set_last_error(e.what());
+    return e.status;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return PA_ERR_INVALID_ARG;
+  }
+}
+
+void require_device() {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    throw Error(PA_ERR_NO_DEVICE, "no CUDA device is visible to libpa_b200");
+  }
+}
+
+bool is_device_pointer(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// Maps caller arrays to device arrays for one call: device pointers pass
+// through; host arrays are copied into staging buffers (in) and back (out).
+class Stage {
+ public:
+  explicit Stage(Problem& P) : P_(P) {}
+  template <typename T>
+  const T* in(const T* p, int64_t count, const char* name) {
+    PA_CHECK(p != nullptr, std::string("null pointer: ") + name);
+    if (is_device_pointer(p)) return p;
+    T* d = reinterpret_cast<T*>(buffer(count * sizeof(T)));
+    PA_CUDA(cudaMemcpyAsync(d, p, count * sizeof(T), cudaMemcpyHostToDevice, P_.stream));
+    return d;
+  }
+  template <typename T>
+  T* out(T* p, int64_t count, const char* name, bool copy_in = false) {
+    PA_CHECK(p != nullptr, std::string("null pointer: ") + name);
+    if (is_device_pointer(p)) return p;
+    T* d = reinterpret_cast<T*>(buffer(count * sizeof(T)));
+    if (copy_in) PA_CUDA(cudaMemcpyAsync(d, p, count * sizeof(T), cudaMemcpyHostToDevice, P_.stream));
+    outs_.push_back({p, d, size_t(count * sizeof(T))});
+    return d;
+  }
+  void finish() {
+    for (auto& o : outs_) PA_CUDA(cudaMemcpyAsync(o.host, o.dev, o.bytes, cudaMemcpyDeviceToHost, P_.stream));
+    if (!outs_.empty()) PA_CUDA(cudaStreamSynchronize(P_.stream));
+    PA_CUDA(cudaGetLastError());
+  }
+
+ private:
+  struct Out {
+    void* host;
+    void* dev;
+    size_t bytes;
+  };
+  void* buffer(size_t bytes) {
+    auto& pool = P_.staging;
+    if (slot_ >= pool.size()) pool.emplace_back(new DevBuf<char>());
+    DevBuf<char>& b = *pool[slot_++];
+    if (b.n < bytes) b.resize(bytes);
+    return b.get();
+  }
+  Problem& P_;
+  size_t slot_ = 0;
+  std::vector<Out> outs_;
+};
+
+}  // namespace
+
+}  // namespace pa
+
+struct pa_problem {
+  pa::Problem P;
+};
+struct pa_mesh {
+  pa::Mesh m;
+};
+
+using pa::Error;
+using pa::guard;
+using pa::Problem;
+
+namespace {
+
+Problem& prob(pa_problem* h) {
+  if (!h) throw Error(PA_ERR_INVALID_ARG, "null pa_problem");
+  PA_CUDA(cudaSetDevice(h->P.mesh->device));
+  return h->P;
+}
+
+void upload_bcs(Problem& P) {
+  const int64_t N = P.N();
+  std::vector<uint8_t> mask(N, 0);
+  for (int32_t d : P.bc_dofs) mask[d / 3] |= uint8_t(1u << (d % 3));
+  P.d_node_mask.upload(mask.data(), mask.size(), P.stream);
+  if (!P.bc_dofs.empty()) {
+    P.d_bc_dofs.upload(P.bc_dofs.data(), P.bc_dofs.size(), P.stream);
+    P.d_bc_vals.upload(P.bc_vals.data(), P.bc_vals.size(), P.stream);
+  }
+  PA_CUDA(cudaStreamSynchronize(P.stream));
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* pa_version(void) { return "pa_b200 0.1 (sm_100a)"; }
+const char* pa_last_error(void) { return pa::g_last_error.c_str(); }
+
+pa_status pa_mesh_create(const int32_t* cells2nodes, int64_t num_cells, const double* coords, int64_t num_nodes,
+                         pa_mesh** out) {
+  return guard([&] {
+    PA_CHECK(out && cells2nodes && coords, "null argument");
+    PA_CHECK(num_cells > 0 && num_nodes > 0, "empty mesh");
+    pa::require_device();
+    std::unique_ptr<pa_mesh> h(new pa_mesh());
+    h->m.C = num_cells;
+    h->m.N = num_nodes;
+    h->m.cells.assign(cells2nodes, cells2nodes + 4 * num_cells);
+    h->m.coords.assign(coords, coords + 3 * num_nodes);
+    pa::mesh_build(h->m);
+    *out = h.release();
+  });
+}
+
+pa_status pa_mesh_create_box(int32_t nx, int32_t ny, int32_t nz, double lx, double ly, double lz, pa_mesh** out) {
+  return guard([&] {
+    PA_CHECK(out, "null argument");
+    PA_CHECK(nx > 0 && ny > 0 && nz > 0, "box needs positive hex counts");
+    PA_CHECK(lx > 0 && ly > 0 && lz > 0, "box needs positive lengths");
+    pa::require_device();
+    static const int tet[6][4][3] = {
+        {{0, 0, 0}, {1, 1, 0}, {0, 1, 0}, {1, 1, 1}}, {{0, 0, 0}, {0, 1, 0}, {0, 1, 1}, {1, 1, 1}},
+        {{0, 0, 0}, {0, 1, 1}, {0, 0, 1}, {1, 1, 1}}, {{0, 0, 0}, {1, 0, 1}, {1, 1, 1}, {0, 0, 1}},
+        {{1, 0, 0}, {1, 0, 1}, {1, 1, 1}, {0, 0, 0}}, {{1, 0, 0}, {1, 1, 1}, {1, 1, 0}, {0, 0, 0}}};
+    std::unique_ptr<pa_mesh> h(new pa_mesh());
+    pa::Mesh& m = h->m;
+    const int64_t px = nx + 1, py = ny + 1;
+    m.N = px * py * int64_t(nz + 1);
+    m.C = 6LL * nx * ny * nz;
+    m.coords.resize(3 * m.N);
+    m.cells.resize(4 * m.C);
+    for (int64_t k = 0; k <= nz; ++k)
+      for (int64_t j = 0; j <= ny; ++j)
+        for (int64_t i = 0; i <= nx; ++i) {
+          const int64_t v = i + px * (j + py * k);
+          m.coords[3 * v + 0] = lx * double(i) / nx;
+          m.coords[3 * v + 1] = ly * double(j) / ny;
+          m.coords[3 * v + 2] = lz * double(k) / nz;
+        }
+    int64_t c = 0;
+    for (int64_t k = 0; k < nz; ++k)
+      for (int64_t j = 0; j < ny; ++j)
+        for (int64_t i = 0; i < nx; ++i)
+          for (int t = 0; t < 6; ++t, ++c)
+            for (int n = 0; n < 4; ++n) {
+              const int* o = tet[t][n];
+              m.cells[4 * c + n] = int32_t((i + o[0]) + px * ((j + o[1]) + py * (k + o[2])));
+            }
+    pa::mesh_build(m);
+    *out = h.release();
+  });
+}
+
+pa_status pa_mesh_destroy(pa_mesh* mesh) {
+  return guard([&] { delete mesh; });
+}
+
+pa_status pa_mesh_sizes(const pa_mesh* mesh, int64_t* num_cells, int64_t* num_nodes, int64_t* num_blocks,
+                        int64_t* num_tiles) {
+  return guard([&] {
+    PA_CHECK(mesh, "null pa_mesh");
+    if (num_cells) *num_cells = mesh->m.C;
+    if (num_nodes) *num_nodes = mesh->m.N;
+    if (num_blocks) *num_blocks = mesh->m.B;
+    if (num_tiles) *num_tiles = mesh->m.T;
+  });
+}
+
+pa_status pa_mesh_get(const pa_mesh* mesh, int32_t* cells2nodes, double* coords) {
+  return guard([&] {
+    PA_CHECK(mesh, "null pa_mesh");
+    if (cells2nodes) std::memcpy(cells2nodes, mesh->m.cells.data(), sizeof(int32_t) * mesh->m.cells.size());
+    if (coords) std::memcpy(coords, mesh->m.coords.data(), sizeof(double) * mesh->m.coords.size());
+  });
+}
+
+pa_status pa_mesh_graph(const pa_mesh* mesh, int32_t* rowmap, int32_t* cols) {
+  return guard([&] {
+    PA_CHECK(mesh, "null pa_mesh");
+    if (rowmap) std::memcpy(rowmap, mesh->m.rowmap.data(), sizeof(int32_t) * mesh->m.rowmap.size());
+    if (cols) std::memcpy(cols, mesh->m.cols.data(), sizeof(int32_t) * mesh->m.cols.size());
+  });
+}
+
+pa_status pa_mesh_set_graph(pa_mesh* mesh, const int32_t* rowmap, const int32_t* cols, int64_t num_blocks) {
+  return guard([&] {
+    PA_CHECK(mesh && rowmap && cols, "null argument");
+    pa::Mesh& m = mesh->m;
+    PA_CHECK(num_blocks == m.B, "graph has a different number of blocks than the mesh's node-star pattern");
+    PA_CHECK(rowmap[0] == 0 && rowmap[m.N] == num_blocks, "rowmap does not span the blocks");
+    std::vector<int32_t> a, b;
+    for (int64_t v = 0; v < m.N; ++v) {
+      PA_CHECK(rowmap[v + 1] - rowmap[v] == m.rowmap[v + 1] - m.rowmap[v], "row lengths differ from the mesh pattern");
+      a.assign(cols + rowmap[v], cols + rowmap[v + 1]);
+      b.assign(m.cols.begin() + m.rowmap[v], m.cols.begin() + m.rowmap[v + 1]);
+      std::sort(a.begin(), a.end());
+      std::sort(b.begin(), b.end());
+      PA_CHECK(a == b, "row columns differ from the mesh pattern");
+    }
+    m.cols.assign(cols, cols + num_blocks);
+    if (m.d_cell_entry.n) m.build_graph_entries();
+  });
+}
+
+pa_status pa_mesh_boundary_faces(const pa_mesh* mesh, int32_t axis, double value, int32_t* faces,
+                                 int64_t* num_faces) {
+  return guard([&] {
+    PA_CHECK(mesh && num_faces, "null argument");
+    PA_CHECK(axis >= 0 && axis < 3, "axis must be 0, 1 or 2");
+    const pa::Mesh& m = mesh->m;
+    const double tol = 1e-12 * (1.0 + std::fabs(value));
+    int64_t nf = 0;
+    for (int64_t c = 0; c < m.C; ++c)
+      for (int drop = 0; drop < 4; ++drop) {
+        int32_t f[3];
+        int k = 0;
+        bool on = true;
+        for (int n = 0; n < 4; ++n) {
+          if (n == drop) continue;
+          f[k++] = m.cells[4 * c + n];
+          on = on && std::fabs(m.coords[3 * int64_t(m.cells[4 * c + n]) + axis] - value) <= tol;
+        }
+        if (!on) continue;
+        if (faces) std::memcpy(faces + 3 * nf, f, sizeof(f));
+        ++nf;
+      }
+    *num_faces = nf;
+  });
+}
+
+pa_status pa_problem_create(pa_mesh* mesh, const pa_elastic_params* params, void* stream, pa_problem** out) {
+  return guard([&] {
+    PA_CHECK(mesh && params && out, "null argument");
+    PA_CHECK(params->youngs_modulus > 0, "Youngs Modulus must be positive");
+    PA_CHECK(params->poissons_ratio > -1.0 && params->poissons_ratio < 0.5, "Poissons Ratio must lie in (-1, 0.5)");
+    PA_CHECK(params->control_layout == PA_CONTROL_NODAL || params->control_layout == PA_CONTROL_CELL,
+             "unknown control layout");
+    PA_CUDA(cudaSetDevice(mesh->m.device));
+    std::unique_ptr<pa_problem> h(new pa_problem());
+    Problem& P = h->P;
+    P.mesh = &mesh->m;
+    P.ep = pa::ElasticParams{params->youngs_modulus, params->poissons_ratio, params->simp_exponent, params->simp_min,
+                             params->control_layout};
+    if (stream) {
+      P.stream = reinterpret_cast<cudaStream_t>(stream);
+    } else {
+      PA_CUDA(cudaStreamCreateWithFlags(&P.stream, cudaStreamNonBlocking));
+      P.own_stream = true;
+    }
+    upload_bcs(P);
+    *out = h.release();
+  });
+}
+
+pa_status pa_problem_destroy(pa_problem* problem) {
+  return guard([&] {
+    if (!problem) return;
+    Problem& P = problem->P;
+    cudaSetDevice(P.mesh->device);
+    cudaStreamSynchronize(P.stream);
+    if (P.ev0) cudaEventDestroy(P.ev0);
+    if (P.ev1) cudaEventDestroy(P.ev1);
+    cudaStream_t s = P.own_stream ? P.stream : nullptr;
+    delete problem;
+    if (s) cudaStreamDestroy(s);
+  });
+}
+
+pa_status pa_problem_add_traction(pa_problem* problem, const int32_t* faces, int64_t num_faces, const double flux[3]) {
+  return guard([&] {
+    Problem& P = prob(problem);
+    PA_CHECK(flux && (faces || num_faces == 0) && num_faces >= 0, "null argument");
+    for (int64_t i = 0; i < 3 * num_faces; ++i)
+      PA_CHECK(faces[i] >= 0 && faces[i] < P.N(), "face node id out of range");
+    P.faces.insert(P.faces.end(), faces, faces + 3 * num_faces);
+    for (int64_t f = 0; f < num_faces; ++f) P.face_flux.insert(P.face_flux.end(), flux, flux + 3);
+    P.d_faces.upload(P.faces.data(), P.faces.size(), P.stream);
+    P.d_face_flux.upload(P.face_flux.data(), P.face_flux.size(), P.stream);
+    PA_CUDA(cudaStreamSynchronize(P.stream));
+  });
+}
+
+pa_status pa_problem_clear_tractions(pa_problem* problem) {
+  return guard([&] {
+    Problem& P = prob(problem);
+    P.faces.clear();
+    P.face_flux.clear();
+  });
+}
+
+pa_status pa_problem_set_dirichlet(pa_problem* problem, const int32_t* dofs, const double* values, int64_t n) {
+  return guard([&] {
+    Problem& P = prob(problem);
+    PA_CHECK(n >= 0 && (n == 0 || (dofs && values)), "null argument");
+    for (int64_t i = 0; i < n; ++i) {
+      PA_CHECK(dofs[i] >= 0 && dofs[i] < P.ndof(), "Dirichlet dof out of range");
+      PA_CHECK(std::isfinite(values[i]), "non-finite Dirichlet value");
+    }
+    P.bc_dofs.assign(dofs, dofs + n);
+    P.bc_vals.assign(values, values + n);
+    upload_bcs(P);
+  });
+}
+
+pa_status pa_vf_value(pa_problem* problem, const double* u, const double* z, double* r) {
+  return guard([&] {
+    Problem& P = prob(problem);
+    pa::Stage st(P);
+    const double* du = st.in(u, P.ndof(), "u");
+    const double* dz = st.in(z, P.nz(), "z");
+    double* dr = st.out(r, P.ndof(), "r");
+    pa::launch_value(P, du, dz, dr, P.stream);
+    pa::launch_traction(P, dr, -1.0, P.stream);
+    st.finish();
+  });
+}
+
+pa_status pa_vf_gradient_u(pa_problem* problem, const double* u, const double* z, double* entries) {
+  return guard([&] {
+    Problem& P = prob(problem);
+    (void)u;  // K does not depend on u for linear elasticity; kept for the reference's signature
+    if (!P.mesh->d_cell_entry.n) P.mesh->build_graph_entries();
+    pa::Stage st(P);
+    const double* dz = st.in(z, P.nz(), "z");
+    double* de = st.out(entries, 9 * P.mesh->B, "entries");
+    pa::launch_gradient_u(P, dz, de, P.stream);
+    st.finish();
+  });
+}
+
+pa_status pa_vf_gradient_z(pa_problem* problem, const double* u, const double* z, double* entries) {
+  return guard([&] {
+    Problem& P = prob(problem);
+    if (!P.mesh->d_cell_entry.n) P.mesh->build_graph_entries();
+    pa::Stage st(P);
+    const double* du = st.in(u, P.ndof(), "u");
+    const double* dz = st.in(z, P.nz(), "z");
+    const int64_t n = P.ep.layout == PA_CONTROL_CELL ? 12 * P.C() : 3 * P.mesh->B;
+    double* de = st.out(entries, n, "entries");
+    pa::launch_gradient_z(P, du, dz, de, P.stream);
+    st.finish();
+  });
+}
+
+static void energy_call(pa_problem* problem, const double* u, const double* z, double* value, double* gu, double* gz) {
+  Problem& P = prob(problem);
+  pa::Stage st(P);
+  const double* du = st.in(u, P.ndof(), "u");
+  const double* dz = st.in(z, P.nz(), "z");
+  double* dgu = gu ? st.out(gu, P.ndof(), "grad") : nullptr;
+  double* dgz = gz ? st.out(gz, P.nz(), "grad") : nullptr;
+  const int64_t grid = (P.C() + 255) / 256;
+  if (value) {
+    if (P.d_partials.n < size_t(grid)) P.d_partials.resize(grid);
+    if (P.d_scalar.n < 2) P.d_scalar.resize(2);
+  }
+  pa::launch_energy(P, du, dz, P.d_partials.get(), value ? P.d_scalar.get() : nullptr, dgu, dgz, P.stream);
+  if (value) {
+    PA_CUDA(cudaMemcpyAsync(value, P.d_scalar.get(), sizeof(double), cudaMemcpyDeviceToHost, P.stream));
+    PA_CUDA(cudaStreamSynchronize(P.stream));
+  }
+  st.finish();
+}
+
+pa_status pa_sf_value(pa_problem* problem, const double* u, const double* z, double* value) {
+  return guard([&] {
+    PA_CHECK(value, "null value pointer");
+    energy_call(problem, u, z, value, nullptr, nullptr);
+  });
+}
+
+pa_status pa_sf_gradient_u(pa_problem* problem, const double* u, const double* z, double* grad) {
+  return guard([&] {
+    PA_CHECK(grad, "null grad pointer");
+    energy_call(problem, u, z, nullptr, grad, nullptr);
+  });
+}
+
+pa_status pa_sf_gradient_z(pa_problem* problem, const double* u, const double* z, double* grad) {
+  return guard([&] {
+    PA_CHECK(grad, "null grad pointer");
+    energy_call(problem, u, z, nullptr, nullptr, grad);
+  });
+}
+
+pa_status pa_apply(pa_problem* problem, const double* z, const void* x, void* y, int32_t precision,
+                   int32_t constrained) {
+  return guard([&] {
+    Problem& P = prob(problem);
+    PA_CHECK(precision == PA_FP64 || precision == PA_FP32, "precision must be PA_FP64 or PA_FP32");
+    pa::Stage st(P);
+    const double* dz = st.in(z, P.nz(), "z");
+    const int64_t n = P.ndof();
+    P.ws.w64.resize(P.C());
+    if (precision == PA_FP32) P.ws.w32.resize(P.C());
+    pa::launch_cell_weights(P, dz, P.ws.w64.get(), precision == PA_FP32 ? P.ws.w32.get() : nullptr, P.stream);
+    const uint8_t* mask = constrained ? P.d_node_mask.get() : nullptr;
+    if (precision == PA_FP64) {
+      const double* dx = st.in(static_cast<const double*>(x), n, "x");
+      double* dy = st.out(static_cast<double*>(y), n, "y");
+      pa::launch_apply_tiled<double>(P, P.ws.w64.get(), dx, dy, mask, P.stream);
+      if (constrained && !P.bc_dofs.empty()) {
+        // identity rows on constrained dofs
+        std::vector<int32_t>& d = P.bc_dofs;
+        for (size_t i = 0; i < d.size(); ++i)
+          PA_CUDA(cudaMemcpyAsync(dy + d[i], dx + d[i], sizeof(double), cudaMemcpyDeviceToDevice, P.stream));
+      }
+    } else {
+      const float* dx = st.in(static_cast<const float*>(x), n, "x");
+      float* dy = st.out(static_cast<float*>(y), n, "y");
+      pa::launch_apply_tiled<float>(P, P.ws.w32.get(), dx, dy, mask, P.stream);
+      if (constrained && !P.bc_dofs.empty()) {
+        std::vector<int32_t>& d = P.bc_dofs;
+        for (size_t i = 0; i < d.size(); ++i)
+          PA_CUDA(cudaMemcpyAsync(dy + d[i], dx + d[i], sizeof(float), cudaMemcpyDeviceToDevice, P.stream));
+      }
+    }
+    st.finish();
+  });
+}
+
+pa_status pa_apply_block_constraints(pa_problem* problem, double* entries, double* rhs, double scale) {
+  return guard([&] {
+    Problem& P = prob(problem);
+    if (!P.mesh->d_cell_entry.n) P.mesh->build_graph_entries();
+    pa::Stage st(P);
+    double* de = st.out(entries, 9 * P.mesh->B, "entries", true);
+    double* dr = st.out(rhs, P.ndof(), "rhs", true);
+    pa::launch_block_constraints(P, de, dr, scale, P.stream);
+    st.finish();
+  });
+}
+
+pa_status pa_solve_options_default(pa_solve_options* o) {
+  return guard([&] {
+    PA_CHECK(o, "null options");
+    o->method = PA_SOLVER_PCG_FP64;
+    o->rel_tol = 1e-10;
+    o->max_iters = 0;
+    o->check_every = 64;
+    o->use_initial_guess = 0;
+  });
+}
+
+pa_status pa_solve(pa_problem* problem, const double* z, const double* b, double* x, const pa_solve_options* options,
+                   pa_solve_stats* stats) {
+  return pa::guard_status([&] {
+    Problem& P = prob(problem);
+    pa_solve_options o;
+    pa_solve_options_default(&o);
+    if (options) o = *options;
+    pa::Stage st(P);
+    const double* dz = st.in(z, P.nz(), "z");
+    const double* db = st.in(b, P.ndof(), "b");
+    double* dx = st.out(x, P.ndof(), "x", o.use_initial_guess != 0);
+    pa_status s = pa::solve_device(P, dz, db, dx, o, stats);
+    st.finish();
+    return s;
+  });
+}
+
+pa_status pa_problem_solution(pa_problem* problem, const double* z, double* u, const pa_solve_options* options,
+                              pa_solve_stats* stats) {
+  return pa::guard_status([&] {
+    Problem& P = prob(problem);
+    pa_solve_options o;
+    pa_solve_options_default(&o);
+    if (options) o = *options;
+    o.use_initial_guess = 0;
+    pa::Stage st(P);
+    const double* dz = st.in(z, P.nz(), "z");
+    double* du = st.out(u, P.ndof(), "u");
+    // R = value(0, z) = -F; solve K du = -R; u = du
+    P.d_rhs.resize(P.ndof());
+    double* rhs = P.d_rhs.get();
+    PA_CUDA(cudaMemsetAsync(rhs, 0, sizeof(double) * P.ndof(), P.stream));
+    pa::launch_traction(P, rhs, 1.0, P.stream);  // -R(u=0) = F
+    pa_status s = pa::solve_device(P, dz, rhs, du, o, stats);
+    st.finish();
+    return s;
+  });
+}
+
+pa_status pa_problem_criterion_gradient(pa_problem* problem, const double* z, const double* u, double* grad,
+                                        int32_t self_adjoint, const pa_solve_options* options) {
+  return pa::guard_status([&] {
+    Problem& P = prob(problem);
+    pa::Stage st(P);
+    const double* du = st.in(u, P.ndof(), "u");
+    const double* dz = st.in(z, P.nz(), "z");
+    double* dg = st.out(grad, P.nz(), "grad");
+    pa::launch_energy(P, du, dz, nullptr, nullptr, nullptr, dg, P.stream);  // df/dz
+    pa_status s = PA_OK;
+    if (self_adjoint) {
+      // -df/dz (src/elliptic/Problem.hpp:438-441)
+      pa::launch_scale(dg, P.nz(), -1.0, P.stream);
+    } else {
+      // lambda: K lambda = -df/du with homogeneous BCs; g += (dR/dz)^T lambda
+      pa_solve_options o;
+      pa_solve_options_default(&o);
+      if (options) o = *options;
+      o.use_initial_guess = 0;
+      pa::DevBuf<double> dfdu(P.ndof()), lam(P.ndof());
+      pa::launch_energy(P, du, dz, nullptr, nullptr, dfdu.get(), nullptr, P.stream);
+      pa::launch_scale(dfdu.get(), P.ndof(), -1.0, P.stream);
+      std::vector<double> saved = P.bc_vals;
+      std::fill(P.bc_vals.begin(), P.bc_vals.end(), 0.0);
+      upload_bcs(P);
+      s = pa::solve_device(P, dz, dfdu.get(), lam.get(), o, nullptr);
+      P.bc_vals = saved;
+      upload_bcs(P);
+      pa::launch_dRdz_transpose_times(P, du, dz, lam.get(), dg, P.stream);
+    }
+    st.finish();
+    return s;
+  });
+}
+
+pa_status pa_j2_radial_return(pa_problem* problem, const pa_j2_params* params, const double* u, const double* z,
+                              const double* prev_local, double* local) {
+  return guard([&] {
+    Problem& P = prob(problem);
+    PA_CHECK(params, "null J2 parameters");
+    PA_CHECK(params->youngs_modulus > 0 && params->initial_yield_stress > 0, "J2 moduli must be positive");
+    pa::Stage st(P);
+    const double* du = st.in(u, P.ndof(), "u");
+    const double* dz = st.in(z, P.N(), "z");
+    const double* dp = st.in(prev_local, 14 * P.C(), "prev_local");
+    double* dl = st.out(local, 14 * P.C(), "local");
+    pa::launch_j2(P, *params, du, dz, dp, dl, P.stream);
+    st.finish();
+  });
+}
+
+pa_status pa_time_cg_apply(pa_problem* problem, const double* z, int32_t precision, int32_t reps,
+                           double* ms_per_launch, int64_t* algorithmic_bytes) {
+  return guard([&] {
+    Problem& P = prob(problem);
+    PA_CHECK(precision == PA_FP64 || precision == PA_FP32, "precision must be PA_FP64 or PA_FP32");
+    PA_CHECK(reps > 0 && ms_per_launch, "need reps > 0 and an output");
+    pa::Stage st(P);
+    const double* dz = st.in(z, P.nz(), "z");
+    *ms_per_launch = pa::time_cg_apply(P, dz, precision == PA_FP32, reps);
+    if (algorithmic_bytes) {
+      const int64_t sv = precision == PA_FP32 ? 4 : 8;
+      // cells: 4 int32 node ids + penalty weight; nodes: coords, p_old, r, D^-1 in, p_new, K p out
+      *algorithmic_bytes = P.C() * (16 + sv) + P.N() * (3 * sv) * 6;
+    }
+    st.finish();
+  });
+}
+
+}  // extern "C"

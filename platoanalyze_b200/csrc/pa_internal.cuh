@@ -1,0 +1,163 @@
+// pa_internal.cuh -- shared declarations of libpa_b200 (not part of the ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+#include <stdexcept>
+
+#include "../../include/pa_b200.h"
+
+namespace pa {
+
+// ------------------------------------------------------------------ errors --
+struct Error : public std::runtime_error {
+  pa_status status;
+  Error(pa_status s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+void set_last_error(const std::string& msg);
+
+#define PA_CUDA(call)                                                                              \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess)                                                                         \
+      throw ::pa::Error(PA_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_) + " at " + \
+                                         __FILE__ + ":" + std::to_string(__LINE__));               \
+  } while (0)
+
+#define PA_CHECK(cond, msg)                                         \
+  do {                                                              \
+    if (!(cond)) throw ::pa::Error(PA_ERR_INVALID_ARG, (msg));      \
+  } while (0)
+
+// Launch-error check after a kernel launch.
+#define PA_LAUNCHED() PA_CUDA(cudaGetLastError())
+
+// ----------------------------------------------------------- device buffer --
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  explicit DevBuf(size_t count) { resize(count); }
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void resize(size_t count) {
+    if (count == n && p) return;
+    release();
+    if (count) PA_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    n = count;
+  }
+  void upload(const T* h, size_t count, cudaStream_t s = 0) {
+    resize(count);
+    if (count) PA_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+  }
+  T* get() const { return p; }
+};
+
+// ------------------------------------------------------------- tile layout --
+// Cells are grouped into tiles of at most kTileCells cells touching at most
+// kTileNodes distinct nodes.  A tile's nodes are staged in shared memory;
+// each cell stores its 4 tile-local node ids as 4 bytes.  tile_nodes entries
+// carry two flags: kShared (the node also belongs to another tile, so its
+// sum is added atomically) and kOwner (this tile writes per-node outputs of
+// the node, exactly one tile per node).
+constexpr int kTileCells = 256;
+constexpr int kTileNodes = 256;
+constexpr uint32_t kShared = 0x80000000u;
+constexpr uint32_t kOwner = 0x40000000u;
+constexpr uint32_t kNodeMask = 0x3fffffffu;
+
+struct TileView {
+  const int32_t* tile_cell_start;  // T+1, internal cell index
+  const int32_t* tile_node_start;  // T+1
+  const uint32_t* tile_nodes;      // flagged global node ids
+  const uint32_t* cell_local;      // C, 4 x uint8 local ids (internal order)
+  const int32_t* cell_perm;        // C, internal -> user cell id
+  int32_t num_tiles;
+};
+
+struct Mesh {
+  int device = 0;
+  int64_t C = 0, N = 0, B = 0, T = 0;
+  std::vector<int32_t> cells;    // C*4 user order
+  std::vector<double> coords;    // N*3
+  std::vector<int32_t> rowmap;   // N+1
+  std::vector<int32_t> cols;     // B
+  DevBuf<int32_t> d_cells;
+  DevBuf<double> d_coords;
+  DevBuf<float> d_coords32;
+  DevBuf<int32_t> d_rowmap, d_cols;
+  DevBuf<int32_t> d_cell_entry;  // C*16 CRS block index of (a,b) pairs
+  DevBuf<int32_t> d_tile_cell_start, d_tile_node_start, d_cell_perm;
+  DevBuf<uint32_t> d_tile_nodes, d_cell_local;
+  std::vector<int32_t> h_cell_perm;  // internal -> user
+  TileView tiles() const {
+    return TileView{d_tile_cell_start.get(), d_tile_node_start.get(), d_tile_nodes.get(), d_cell_local.get(),
+                    d_cell_perm.get(), int32_t(T)};
+  }
+  void build_graph_entries();
+};
+
+void mesh_build(Mesh& m);  // tiles + graph + device upload
+
+// ----------------------------------------------------------------- material --
+template <typename T>
+struct Iso {
+  T lam, mu;  // Lame parameters; C = lam I(x)I + 2 mu on normal, mu on engineering shear
+};
+
+struct ElasticParams {
+  double E, nu, p, pmin;
+  int layout;
+  Iso<double> iso() const {
+    double c = E / ((1.0 + nu) * (1.0 - 2.0 * nu));
+    return Iso<double>{c * nu, 0.5 * c * (1.0 - 2.0 * nu)};
+  }
+};
+
+// Per-iteration scalars of the PCG kernels, resident in device memory.
+struct PcgScalars {
+  double rz;       // r . z of the current residual
+  double rz_prev;  // previous r . z
+  double pap;      // p . K p
+  double alpha, beta;
+  double rr;       // ||r||^2 (recursive residual)
+  double bb;       // ||b||^2
+  double stop2;    // stop when rr <= stop2
+  int32_t done;    // 1 once converged (kernels become no-ops)
+  int32_t breakdown;
+  int32_t iters;   // iterations completed
+  int32_t pad;
+};
+
+struct Problem;
+
+// ------------------------------------------------------------ kernel APIs --
+// (implemented in pa_elastic.cu)
+void launch_value(const Problem& P, const double* u, const double* z, double* r, cudaStream_t s);
+void launch_traction(const Problem& P, double* r, double scale, cudaStream_t s);
+void launch_gradient_u(const Problem& P, const double* z, double* entries, cudaStream_t s);
+void launch_gradient_z(const Problem& P, const double* u, const double* z, double* entries, cudaStream_t s);
+void launch_energy(const Problem& P, const double* u, const double* z, double* cell_partials /*>=grid*/,
+                   double* value_out /*device scalar or null*/, double* grad_u, double* grad_z, cudaStream_t s);
+void launch_cell_weights(const Problem& P, const double* z, double* w64, float* w32, cudaStream_t s);
+template <typename T>
+void launch_apply_tiled(const Problem& P, const T* w, const T* x, T* y, const uint8_t* node_mask,
+                        cudaStream_t s);
+void launch_diag(const Problem& P, const double* w, double* diag, cudaStream_t s);
+void launch_j2(const Problem& P, const pa_j2_params& jp, const double* u, const double* z, const double* prev,
+               double* cur, cudaStream_t s);
+
+int num_sms();
+
+}  // namespace pa

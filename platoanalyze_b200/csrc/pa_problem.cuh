@@ -1,0 +1,55 @@
+// pa_problem.cuh -- the problem handle behind pa_problem* (not part of the ABI).
+#pragma once
+#include <memory>
+
+#include "pa_internal.cuh"
+
+namespace pa {
+
+// Device workspace of the PCG solvers; sized on first use, reused across solves.
+struct SolverWorkspace {
+  int64_t ndof = 0;
+  // FP64 vectors
+  DevBuf<double> x, b, r, p0, p1, ap, dinv, t, w64;
+  // FP32 vectors (mixed precision)
+  DevBuf<float> r32, p32a, p32b, ap32, dinv32, dx32, w32;
+  DevBuf<float> coords32;
+  DevBuf<double> partials;
+  DevBuf<unsigned int> counters;
+  DevBuf<PcgScalars> sc;
+  DevBuf<double> rr_hist;
+  void ensure(int64_t ndof_, int64_t C, int grid, bool mixed);
+};
+
+struct Problem {
+  Mesh* mesh = nullptr;
+  ElasticParams ep{};
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  // natural BCs
+  std::vector<int32_t> faces;     // 3 per face
+  std::vector<double> face_flux;  // 3 per face
+  DevBuf<int32_t> d_faces;
+  DevBuf<double> d_face_flux;
+  // essential BCs
+  std::vector<int32_t> bc_dofs;
+  std::vector<double> bc_vals;
+  DevBuf<int32_t> d_bc_dofs;
+  DevBuf<double> d_bc_vals;
+  DevBuf<uint8_t> d_node_mask;  // N, bit d = dof d constrained
+  // scratch for reductions / staging
+  DevBuf<double> d_partials;
+  DevBuf<double> d_scalar;
+  DevBuf<unsigned int> d_counter;
+  DevBuf<double> d_rhs;
+  std::vector<std::unique_ptr<DevBuf<char>>> staging;  // host-array staging, reused across calls
+  SolverWorkspace ws;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  int64_t N() const { return mesh->N; }
+  int64_t C() const { return mesh->C; }
+  int64_t ndof() const { return 3 * mesh->N; }
+  int64_t nz() const { return ep.layout == PA_CONTROL_CELL ? mesh->C : mesh->N; }
+};
+
+}  // namespace pa

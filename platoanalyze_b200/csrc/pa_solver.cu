@@ -1,0 +1,537 @@
+// pa_solver.cu -- matrix-free Jacobi-preconditioned CG on the
+// Dirichlet-constrained stiffness system, FP64 or mixed precision.
+//
+// The reference hands the assembled, symmetrically constrained block CRS to
+// AmgX or AztecOO (AbstractSolver::solve, src/alg/PlatoAbstractSolver.hpp:19-27;
+// constraints by applyBlockConstraints, src/ApplyConstraints.hpp:11-79).  This
+// solver solves the same linear system without assembling it:
+//   K_ff x_f = b_f - K_fc x_D,   x_c = x_D,
+// i.e. the constrained rows/columns are masked in the matrix-free apply.
+//
+// One CG iteration is two kernels:
+//   K1 (pa_tiled.cuh, mode 1): p = D^-1 r + beta p_old (formed while staging),
+//      Ap = K p, and p.Ap from per-cell energies; its last CTA sets alpha.
+//   K2 (k_cg_update): x += alpha p, r -= alpha Ap, Ap = 0, r.z and r.r; its
+//      last CTA sets beta and the convergence flag.
+// All scalars stay on the device; chunks of iterations are captured once in a
+// CUDA graph and replayed; the host reads the scalars once per chunk.
+//
+// Mixed precision: K1/K2 run on FP32 vectors and the FP32 operator (dots
+// accumulated in FP64); x is kept in FP64 and the FP32 update dx is folded in
+// once per chunk, where the FP64 true residual b - K x is recomputed with the
+// FP64 operator and replaces the recursive FP32 residual (reliable updates),
+// and convergence is decided on that FP64 residual.
+#include <cmath>
+#include <algorithm>
+
+#include "pa_problem.cuh"
+#include "pa_tiled.cuh"
+
+namespace pa {
+
+namespace {
+
+constexpr int kVecThreads = 256;
+
+int vec_grid(int64_t n) {
+  const int64_t want = (n + kVecThreads - 1) / kVecThreads;
+  const int64_t cap = int64_t(num_sms()) * 8;
+  return int(std::max<int64_t>(1, std::min(want, cap)));
+}
+
+__device__ __forceinline__ void block_sum2(double& a, double& b, double* smem /*64*/) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_down_sync(0xffffffffu, a, o);
+    b += __shfl_down_sync(0xffffffffu, b, o);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) { smem[warp] = a; smem[32 + warp] = b; }
+  __syncthreads();
+  a = b = 0.0;
+  if (warp == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    a = lane < nw ? smem[lane] : 0.0;
+    b = lane < nw ? smem[32 + lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_down_sync(0xffffffffu, a, o);
+      b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+  }
+}
+
+// CG update (K2).  T = vector type; X = type of the iterate / its update.
+template <typename T, typename X>
+__global__ void __launch_bounds__(kVecThreads) k_cg_update(int64_t n, X* __restrict__ x, T* __restrict__ r,
+                                                           const T* __restrict__ p, T* __restrict__ ap,
+                                                           const T* __restrict__ dinv, PcgScalars* __restrict__ sc,
+                                                           double* __restrict__ partials, unsigned int* counter,
+                                                           double* __restrict__ rr_hist) {
+  __shared__ double s_red[64];
+  if (sc->done) return;
+  const double alpha = sc->alpha;
+  const T a = T(alpha);
+  double rz = 0.0, rr = 0.0;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    const T pi = p[i];
+    x[i] += X(alpha) * X(pi);
+    const T ri = r[i] - a * ap[i];
+    r[i] = ri;
+    ap[i] = T(0);
+    const T zi = dinv[i] * ri;
+    rz += double(ri) * double(zi);
+    rr += double(ri) * double(ri);
+  }
+  block_sum2(rz, rr, s_red);
+  if (threadIdx.x == 0) { partials[2 * blockIdx.x] = rz; partials[2 * blockIdx.x + 1] = rr; }
+  if (last_block_arrive(counter)) {
+    double t0 = 0.0, t1 = 0.0;
+    for (int i = threadIdx.x; i < gridDim.x; i += blockDim.x) {
+      t0 += __ldcg(&partials[2 * i]);
+      t1 += __ldcg(&partials[2 * i + 1]);
+    }
+    block_sum2(t0, t1, s_red);
+    if (threadIdx.x == 0) {
+      sc->beta = t0 / sc->rz;
+      sc->rz_prev = sc->rz;
+      sc->rz = t0;
+      sc->rr = t1;
+      const int it = sc->iters + 1;
+      sc->iters = it;
+      if (rr_hist) rr_hist[it] = t1;
+      if (!isfinite(t0) || !isfinite(t1)) { sc->breakdown = 1; sc->done = 1; }
+      if (t1 <= sc->stop2) sc->done = 1;
+      *counter = 0u;
+    }
+  }
+}
+
+// r.z, r.r of a fresh residual (z = D^-1 r); resets beta, sets stop2 = tol2 * bb.
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) k_cg_init(int64_t n, const T* __restrict__ r, const T* __restrict__ dinv,
+                                                         PcgScalars* __restrict__ sc, double* __restrict__ partials,
+                                                         unsigned int* counter, double tol2, int reset) {
+  __shared__ double s_red[64];
+  double rz = 0.0, rr = 0.0;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    const double ri = double(r[i]);
+    rz += ri * double(dinv[i] * r[i]);
+    rr += ri * ri;
+  }
+  block_sum2(rz, rr, s_red);
+  if (threadIdx.x == 0) { partials[2 * blockIdx.x] = rz; partials[2 * blockIdx.x + 1] = rr; }
+  if (last_block_arrive(counter)) {
+    double t0 = 0.0, t1 = 0.0;
+    for (int i = threadIdx.x; i < gridDim.x; i += blockDim.x) {
+      t0 += __ldcg(&partials[2 * i]);
+      t1 += __ldcg(&partials[2 * i + 1]);
+    }
+    block_sum2(t0, t1, s_red);
+    if (threadIdx.x == 0) {
+      sc->rz = t0;
+      sc->rr = t1;
+      if (reset) {
+        sc->beta = 0.0;
+        sc->bb = t1;
+        sc->iters = 0;
+        sc->breakdown = 0;
+        sc->stop2 = tol2 * t1;
+      }
+      sc->done = (t1 <= sc->stop2) ? 1 : 0;
+      *counter = 0u;
+    }
+  }
+}
+
+// out = (a - b) masked to free dofs (mask bit set -> 0), FP64.
+__global__ void k_sub_masked(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
+                             const uint8_t* __restrict__ mask, double* __restrict__ out) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    const bool c = mask && ((mask[i / 3] >> (i % 3)) & 1);
+    out[i] = c ? 0.0 : a[i] - (b ? b[i] : 0.0);
+  }
+}
+
+// D^-1 with constrained (and zero) diagonal entries mapped to 0.
+template <typename T>
+__global__ void k_inv_diag(int64_t n, const double* __restrict__ diag, const uint8_t* __restrict__ mask,
+                           T* __restrict__ dinv) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    const bool c = mask && ((mask[i / 3] >> (i % 3)) & 1);
+    dinv[i] = (c || diag[i] == 0.0) ? T(0) : T(1.0 / diag[i]);
+  }
+}
+
+__global__ void k_to_f32(int64_t n, const double* __restrict__ a, float* __restrict__ out) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    out[i] = float(a[i]);
+}
+
+// x += dx; dx = 0
+__global__ void k_fold(int64_t n, double* __restrict__ x, float* __restrict__ dx) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    x[i] += double(dx[i]);
+    dx[i] = 0.0f;
+  }
+}
+
+// Dirichlet lift vector: xd[dof] = scale * value for each BC, 0 elsewhere.
+__global__ void k_scatter_bc(int64_t nbc, const int32_t* __restrict__ dofs, const double* __restrict__ vals,
+                             double scale, double* __restrict__ xd) {
+  const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i < nbc) xd[dofs[i]] = scale * vals[i];
+}
+
+// x[dof] = scale * value (final solution on constrained dofs).
+__global__ void k_set_bc(int64_t nbc, const int32_t* __restrict__ dofs, const double* __restrict__ vals, double scale,
+                         double* __restrict__ x) {
+  const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i < nbc) x[dofs[i]] = scale * vals[i];
+}
+
+__global__ void k_dot2(int64_t n, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ out) {
+  __shared__ double s_red[64];
+  double s = 0.0, t = 0.0;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    s += a[i] * a[i];
+    t += b[i] * b[i];
+  }
+  block_sum2(s, t, s_red);
+  if (threadIdx.x == 0) { atomicAdd(&out[0], s); atomicAdd(&out[1], t); }
+}
+
+template <typename T>
+int fused_apply_grid() {
+  int per_sm = 0;
+  PA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_apply_tiled<T, 1>, kApplyThreads, 0));
+  return std::max(1, per_sm) * num_sms();
+}
+
+template <typename T>
+ApplyArgs<T> fused_args(Problem& P, const T* coords, const T* w, const T* p_old, T* p_new, T* ap, const T* r,
+                        const T* dinv) {
+  SolverWorkspace& ws = P.ws;
+  ApplyArgs<T> a{};
+  a.tv = P.mesh->tiles();
+  a.coords = coords;
+  a.w = w;
+  a.node_mask = P.d_node_mask.get();
+  Iso<double> i64 = P.ep.iso();
+  a.iso = Iso<T>{T(i64.lam), T(i64.mu)};
+  a.x = p_old;
+  a.y = ap;
+  a.r = r;
+  a.dinv = dinv;
+  a.p_new = p_new;
+  a.sc = ws.sc.get();
+  a.partials = ws.partials.get();
+  a.counter = ws.counters.get();
+  return a;
+}
+
+}  // namespace
+
+void SolverWorkspace::ensure(int64_t n, int64_t C, int grid, bool mixed) {
+  if (ndof != n) {
+    x.resize(n); b.resize(n); r.resize(n); p0.resize(n); p1.resize(n); ap.resize(n); dinv.resize(n); t.resize(n);
+    w64.resize(C);
+    ndof = n;
+    r32.release(); p32a.release(); p32b.release(); ap32.release(); dinv32.release(); dx32.release(); w32.release();
+  }
+  if (mixed && r32.n != size_t(n)) {
+    r32.resize(n); p32a.resize(n); p32b.resize(n); ap32.resize(n); dinv32.resize(n); dx32.resize(n); w32.resize(C);
+  }
+  if (partials.n < size_t(2 * grid + 64)) partials.resize(2 * grid + 64);
+  if (counters.n < 4) {
+    counters.resize(4);
+    PA_CUDA(cudaMemset(counters.get(), 0, 4 * sizeof(unsigned int)));
+  }
+  if (sc.n < 1) sc.resize(1);
+}
+
+// A CUDA graph of `chunk` fused CG iterations (K1, K2 pairs), captured once
+// per solve and replayed; p alternates between two buffers so that the
+// staging pass of K1 never reads a p value another CTA already replaced.
+template <typename T, typename X>
+struct CgGraph {
+  cudaGraphExec_t exec = nullptr;
+  cudaGraph_t graph = nullptr;
+  int chunk = 0;
+  ~CgGraph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+  }
+  void capture(Problem& P, const T* coords, const T* w, T* pa, T* pb, T* ap, T* r, const T* dinv, X* x, int chunk_) {
+    cudaStream_t s = P.stream;
+    SolverWorkspace& ws = P.ws;
+    const int64_t n = P.ndof();
+    const int vg = vec_grid(n);
+    int ag = fused_apply_grid<T>();
+    if (ag > P.mesh->T) ag = int(P.mesh->T);
+    chunk = chunk_ + (chunk_ % 2);
+    ApplyArgs<T> a_even = fused_args<T>(P, coords, w, pa, pb, ap, r, dinv);  // reads pa, writes pb
+    ApplyArgs<T> a_odd = fused_args<T>(P, coords, w, pb, pa, ap, r, dinv);   // reads pb, writes pa
+    PA_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < chunk; ++k) {
+      k_apply_tiled<T, 1><<<ag, kApplyThreads, 0, s>>>(k % 2 == 0 ? a_even : a_odd);
+      const T* pnew = (k % 2 == 0) ? pb : pa;
+      k_cg_update<T, X><<<vg, kVecThreads, 0, s>>>(n, x, r, pnew, ap, dinv, ws.sc.get(), ws.partials.get(),
+                                                   ws.counters.get() + 1, nullptr);
+    }
+    cudaError_t ce = cudaStreamEndCapture(s, &graph);
+    if (ce != cudaSuccess) throw Error(PA_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+    PA_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+  }
+  // One replay; returns the device scalars after it.
+  PcgScalars run(Problem& P) {
+    PcgScalars hs{};
+    PA_CUDA(cudaGraphLaunch(exec, P.stream));
+    PA_CUDA(cudaMemcpyAsync(&hs, P.ws.sc.get(), sizeof(PcgScalars), cudaMemcpyDeviceToHost, P.stream));
+    PA_CUDA(cudaStreamSynchronize(P.stream));
+    return hs;
+  }
+};
+
+static double host_norm2(Problem& P, const double* v) {
+  cudaStream_t s = P.stream;
+  const int64_t n = P.ndof();
+  if (P.d_scalar.n < 2) P.d_scalar.resize(2);
+  PA_CUDA(cudaMemsetAsync(P.d_scalar.get(), 0, 2 * sizeof(double), s));
+  k_dot2<<<vec_grid(n), kVecThreads, 0, s>>>(n, v, v, P.d_scalar.get());
+  PA_LAUNCHED();
+  double h[2];
+  PA_CUDA(cudaMemcpyAsync(h, P.d_scalar.get(), 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  PA_CUDA(cudaStreamSynchronize(s));
+  return h[0];
+}
+
+// (Re)start the recursive residual from r (FP64 or FP32 copy), keeping p and
+// beta unless `reset`.  Writes the stop threshold (recursive hint) and clears
+// the done flag.
+template <typename T>
+static PcgScalars restart_residual(Problem& P, const T* r, const T* dinv, bool reset, double stop2, double bb) {
+  cudaStream_t s = P.stream;
+  SolverWorkspace& ws = P.ws;
+  const int64_t n = P.ndof();
+  k_cg_init<T><<<vec_grid(n), kVecThreads, 0, s>>>(n, r, dinv, ws.sc.get(), ws.partials.get(), ws.counters.get(),
+                                                   0.0, reset ? 1 : 0);
+  PA_LAUNCHED();
+  PcgScalars cur{};
+  PA_CUDA(cudaMemcpyAsync(&cur, ws.sc.get(), sizeof(PcgScalars), cudaMemcpyDeviceToHost, s));
+  PA_CUDA(cudaStreamSynchronize(s));
+  cur.stop2 = stop2;
+  cur.bb = bb;
+  cur.done = 0;
+  if (reset) { cur.iters = 0; cur.beta = 0.0; cur.breakdown = 0; }
+  PA_CUDA(cudaMemcpyAsync(ws.sc.get(), &cur, sizeof(PcgScalars), cudaMemcpyHostToDevice, s));
+  return cur;
+}
+
+// Solve the constrained system for z; b and x_out are device pointers (3N).
+pa_status solve_device(Problem& P, const double* z, const double* b, double* x_out, const pa_solve_options& o,
+                       pa_solve_stats* st) {
+  cudaStream_t s = P.stream;
+  const int64_t n = P.ndof();
+  const bool mixed = o.method == PA_SOLVER_PCG_MIXED;
+  PA_CHECK(o.method == PA_SOLVER_PCG_FP64 || mixed, "unknown solver method");
+  PA_CHECK(o.rel_tol > 0.0, "rel_tol must be positive");
+  const int grid_need = std::max(std::max(fused_apply_grid<double>(), fused_apply_grid<float>()), vec_grid(n));
+  P.ws.ensure(n, P.C(), grid_need, mixed);
+  SolverWorkspace& ws = P.ws;
+  const int max_iters = o.max_iters > 0 ? o.max_iters : int(20.0 * std::sqrt(double(n)) + 1000);
+  const int chunk = o.check_every > 0 ? o.check_every : 64;
+  const double tol2 = o.rel_tol * o.rel_tol;
+  const int vg = vec_grid(n);
+  const uint8_t* mask = P.d_node_mask.get();
+  const int64_t nbc = int64_t(P.bc_dofs.size());
+  int64_t launches = 0;  // kernels of this library launched by the solve (graph nodes included)
+
+  if (!P.ev0) { PA_CUDA(cudaEventCreate(&P.ev0)); PA_CUDA(cudaEventCreate(&P.ev1)); }
+  PA_CUDA(cudaEventRecord(P.ev0, s));
+
+  // SIMP weights in tile order; Jacobi diagonal and its masked inverse.
+  launch_cell_weights(P, z, ws.w64.get(), mixed ? ws.w32.get() : nullptr, s);
+  launch_diag(P, ws.w64.get(), ws.t.get(), s);
+  k_inv_diag<double><<<vg, kVecThreads, 0, s>>>(n, ws.t.get(), mask, ws.dinv.get());
+  PA_LAUNCHED();
+  launches += 3;
+  if (mixed) {
+    k_inv_diag<float><<<vg, kVecThreads, 0, s>>>(n, ws.t.get(), mask, ws.dinv32.get());
+    PA_LAUNCHED();
+    launches += 1;
+  }
+  // b' = mask(b - K x_D), x_D = Dirichlet values (held in p0 for the moment).
+  double* bprime = ws.b.get();
+  if (nbc) {
+    PA_CUDA(cudaMemsetAsync(ws.p0.get(), 0, sizeof(double) * n, s));
+    k_scatter_bc<<<int((nbc + 255) / 256), 256, 0, s>>>(nbc, P.d_bc_dofs.get(), P.d_bc_vals.get(), 1.0, ws.p0.get());
+    PA_LAUNCHED();
+    launch_apply_tiled<double>(P, ws.w64.get(), ws.p0.get(), ws.t.get(), nullptr, s);
+    k_sub_masked<<<vg, kVecThreads, 0, s>>>(n, b, ws.t.get(), mask, bprime);
+    launches += 3;
+  } else {
+    k_sub_masked<<<vg, kVecThreads, 0, s>>>(n, b, nullptr, nullptr, bprime);
+    launches += 1;
+  }
+  PA_LAUNCHED();
+  // initial free-dof iterate
+  if (o.use_initial_guess) {
+    k_sub_masked<<<vg, kVecThreads, 0, s>>>(n, x_out, nullptr, mask, ws.x.get());
+    launches += 1;
+  } else {
+    PA_CUDA(cudaMemsetAsync(ws.x.get(), 0, sizeof(double) * n, s));
+  }
+  PA_LAUNCHED();
+  // FP64 true residual r = b' - K_masked x
+  auto true_residual = [&]() {
+    launch_apply_tiled<double>(P, ws.w64.get(), ws.x.get(), ws.t.get(), mask, s);
+    k_sub_masked<<<vg, kVecThreads, 0, s>>>(n, bprime, ws.t.get(), mask, ws.r.get());
+    PA_LAUNCHED();
+    launches += 3;
+    return host_norm2(P, ws.r.get());
+  };
+  double bb = host_norm2(P, bprime);
+  launches += 1;
+  if (!(bb > 0.0)) bb = 1.0;
+  double rr_true = true_residual();
+
+  // Krylov vectors
+  PA_CUDA(cudaMemsetAsync(ws.p0.get(), 0, sizeof(double) * n, s));
+  PA_CUDA(cudaMemsetAsync(ws.p1.get(), 0, sizeof(double) * n, s));
+  PA_CUDA(cudaMemsetAsync(ws.ap.get(), 0, sizeof(double) * n, s));
+  if (mixed) {
+    PA_CUDA(cudaMemsetAsync(ws.dx32.get(), 0, sizeof(float) * n, s));
+    PA_CUDA(cudaMemsetAsync(ws.p32a.get(), 0, sizeof(float) * n, s));
+    PA_CUDA(cudaMemsetAsync(ws.p32b.get(), 0, sizeof(float) * n, s));
+    PA_CUDA(cudaMemsetAsync(ws.ap32.get(), 0, sizeof(float) * n, s));
+  }
+  CgGraph<double, double> g64;
+  CgGraph<float, float> g32;
+  if (mixed)
+    g32.capture(P, P.mesh->d_coords32.get(), ws.w32.get(), ws.p32a.get(), ws.p32b.get(), ws.ap32.get(), ws.r32.get(),
+                ws.dinv32.get(), ws.dx32.get(), chunk);
+  else
+    g64.capture(P, P.mesh->d_coords.get(), ws.w64.get(), ws.p0.get(), ws.p1.get(), ws.ap.get(), ws.r.get(),
+                ws.dinv.get(), ws.x.get(), chunk);
+
+  // Recursive-residual stop hint, confirmed on the FP64 true residual.
+  const double hint = mixed ? 0.25 : 0.81;
+  int replacements = 0, iters = 0;
+  bool converged = rr_true <= tol2 * bb, breakdown = false, first = true;
+  while (!converged) {
+    PcgScalars hs{};
+    if (mixed) {
+      k_to_f32<<<vg, kVecThreads, 0, s>>>(n, ws.r.get(), ws.r32.get());
+      PA_LAUNCHED();
+      hs = restart_residual<float>(P, ws.r32.get(), ws.dinv32.get(), first, hint * tol2 * bb, bb);
+      hs = g32.run(P);  // one chunk, then fold dx and replace the residual
+      launches += 3 + 2LL * g32.chunk;
+      // newest p in p32b after an odd number of iterations: keep p32a current
+      if ((hs.iters - iters) % 2)
+        PA_CUDA(cudaMemcpyAsync(ws.p32a.get(), ws.p32b.get(), sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
+      k_fold<<<vg, kVecThreads, 0, s>>>(n, ws.x.get(), ws.dx32.get());
+      PA_LAUNCHED();
+    } else {
+      hs = restart_residual<double>(P, ws.r.get(), ws.dinv.get(), first, hint * tol2 * bb, bb);
+      const int start = hs.iters;
+      launches += 1;
+      do {
+        hs = g64.run(P);
+        launches += 2LL * g64.chunk;
+      } while (!hs.done && hs.iters < max_iters);
+      if ((hs.iters - start) % 2)
+        PA_CUDA(cudaMemcpyAsync(ws.p0.get(), ws.p1.get(), sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    }
+    first = false;
+    iters = hs.iters;
+    rr_true = true_residual();
+    ++replacements;
+    converged = rr_true <= tol2 * bb;
+    if (hs.breakdown) { breakdown = !converged; break; }
+    if (iters >= max_iters) break;
+  }
+  const double relres = std::sqrt(rr_true / bb);
+
+  // x_out = x_f + x_D
+  PA_CUDA(cudaMemcpyAsync(x_out, ws.x.get(), sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  if (nbc) {
+    k_set_bc<<<int((nbc + 255) / 256), 256, 0, s>>>(nbc, P.d_bc_dofs.get(), P.d_bc_vals.get(), 1.0, x_out);
+    PA_LAUNCHED();
+    launches += 1;
+  }
+  PA_CUDA(cudaEventRecord(P.ev1, s));
+  PA_CUDA(cudaEventSynchronize(P.ev1));
+  float ms = 0.f;
+  PA_CUDA(cudaEventElapsedTime(&ms, P.ev0, P.ev1));
+  if (st) {
+    st->iterations = iters;
+    st->replacements = replacements;
+    st->rel_residual = relres;
+    st->seconds = ms * 1e-3;
+    st->converged = converged ? 1 : 0;
+    st->kernel_launches = launches;
+  }
+  if (breakdown) return PA_ERR_BREAKDOWN;
+  if (!std::isfinite(relres)) return PA_ERR_NONFINITE;
+  return converged ? PA_OK : PA_ERR_NOT_CONVERGED;
+}
+
+// Average device time of the fused CG kernel K1 over `reps` back-to-back
+// launches (state: r = 1, p_old = 0, beta = 0.5), for the roofline report.
+double time_cg_apply(Problem& P, const double* z, bool fp32, int reps) {
+  cudaStream_t s = P.stream;
+  const int64_t n = P.ndof();
+  const int grid_need = std::max(std::max(fused_apply_grid<double>(), fused_apply_grid<float>()), vec_grid(n));
+  P.ws.ensure(n, P.C(), grid_need, true);
+  SolverWorkspace& ws = P.ws;
+  launch_cell_weights(P, z, ws.w64.get(), ws.w32.get(), s);
+  launch_diag(P, ws.w64.get(), ws.t.get(), s);
+  k_inv_diag<double><<<vec_grid(n), kVecThreads, 0, s>>>(n, ws.t.get(), P.d_node_mask.get(), ws.dinv.get());
+  k_inv_diag<float><<<vec_grid(n), kVecThreads, 0, s>>>(n, ws.t.get(), P.d_node_mask.get(), ws.dinv32.get());
+  PA_LAUNCHED();
+  PcgScalars init{};
+  init.beta = 0.5;
+  init.rz = 1.0;
+  PA_CUDA(cudaMemcpyAsync(ws.sc.get(), &init, sizeof(init), cudaMemcpyHostToDevice, s));
+  int ag = fp32 ? fused_apply_grid<float>() : fused_apply_grid<double>();
+  if (ag > P.mesh->T) ag = int(P.mesh->T);
+  if (!P.ev0) { PA_CUDA(cudaEventCreate(&P.ev0)); PA_CUDA(cudaEventCreate(&P.ev1)); }
+  float ms = 0.f;
+  if (fp32) {
+    std::vector<float> ones(n, 1.0f);
+    PA_CUDA(cudaMemcpyAsync(ws.r32.get(), ones.data(), sizeof(float) * n, cudaMemcpyHostToDevice, s));
+    PA_CUDA(cudaMemsetAsync(ws.p32a.get(), 0, sizeof(float) * n, s));
+    PA_CUDA(cudaMemsetAsync(ws.p32b.get(), 0, sizeof(float) * n, s));
+    PA_CUDA(cudaMemsetAsync(ws.ap32.get(), 0, sizeof(float) * n, s));
+    ApplyArgs<float> a = fused_args<float>(P, P.mesh->d_coords32.get(), ws.w32.get(), ws.p32a.get(), ws.p32b.get(),
+                                           ws.ap32.get(), ws.r32.get(), ws.dinv32.get());
+    ApplyArgs<float> b = fused_args<float>(P, P.mesh->d_coords32.get(), ws.w32.get(), ws.p32b.get(), ws.p32a.get(),
+                                           ws.ap32.get(), ws.r32.get(), ws.dinv32.get());
+    k_apply_tiled<float, 1><<<ag, kApplyThreads, 0, s>>>(a);  // warm
+    PA_CUDA(cudaEventRecord(P.ev0, s));
+    for (int i = 0; i < reps; ++i) k_apply_tiled<float, 1><<<ag, kApplyThreads, 0, s>>>(i % 2 ? a : b);
+    PA_CUDA(cudaEventRecord(P.ev1, s));
+  } else {
+    std::vector<double> ones(n, 1.0);
+    PA_CUDA(cudaMemcpyAsync(ws.r.get(), ones.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    PA_CUDA(cudaMemsetAsync(ws.p0.get(), 0, sizeof(double) * n, s));
+    PA_CUDA(cudaMemsetAsync(ws.p1.get(), 0, sizeof(double) * n, s));
+    PA_CUDA(cudaMemsetAsync(ws.ap.get(), 0, sizeof(double) * n, s));
+    ApplyArgs<double> a = fused_args<double>(P, P.mesh->d_coords.get(), ws.w64.get(), ws.p0.get(), ws.p1.get(),
+                                             ws.ap.get(), ws.r.get(), ws.dinv.get());
+    ApplyArgs<double> b = fused_args<double>(P, P.mesh->d_coords.get(), ws.w64.get(), ws.p1.get(), ws.p0.get(),
+                                             ws.ap.get(), ws.r.get(), ws.dinv.get());
+    k_apply_tiled<double, 1><<<ag, kApplyThreads, 0, s>>>(a);
+    PA_CUDA(cudaEventRecord(P.ev0, s));
+    for (int i = 0; i < reps; ++i) k_apply_tiled<double, 1><<<ag, kApplyThreads, 0, s>>>(i % 2 ? a : b);
+    PA_CUDA(cudaEventRecord(P.ev1, s));
+  }
+  PA_LAUNCHED();
+  PA_CUDA(cudaEventSynchronize(P.ev1));
+  PA_CUDA(cudaEventElapsedTime(&ms, P.ev0, P.ev1));
+  return double(ms) / reps;
+}
+
+}  // namespace pa

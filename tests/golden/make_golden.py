@@ -1,0 +1,172 @@
+"""Generate the golden fixtures in tests/golden/ from the reference's own tests.
+
+Run from the repository root in a container where the platoanalyze source tree
+is mounted (default /root/reference; override with PA_REFERENCE):
+
+    python tests/golden/make_golden.py
+
+The reference cannot be built here (it needs Trilinos, Omega_h and Kokkos), so
+its unit tests are read as text and their gold arrays extracted:
+
+* unit_tests/DerivativeTests.cpp, ElastostaticResidual3D and
+  InternalElasticEnergy3D: 2x2x2 unit box, E=1e6, nu=0.3, SIMP p=1, min 0,
+  z = 1, u_i = 1e-4 (i+1).
+* unit_tests/PlasticityTests.cpp, J2PlasticityUtils_UpdatePlasticStep3D.
+
+The gold values depend on the vertex numbering of Omega_h's build_box, whose
+source is not available.  It is identified here by search rather than
+restated: the tet split is the one the reference's single-hex box test lists
+(unit_tests/OmegaHUtilitiesTests.cpp:258-287, the six tets around the hex
+diagonal, repeated in every hex), and the vertex permutation is the solution
+of a 0/1 integer program (scipy.optimize.milp): a bijection from the 27 grid
+points to vertex ids such that K(perm) u equals the 81 gold residual values.
+The fixture records the permutation found, so tests never need the search.
+
+The gold Jacobian and dR/dz arrays are raw block-CRS entry arrays whose
+in-row column order is Omega_h's node-star order (not sorted).  Only row 0
+is covered by the gold (45 and 24 entries); its column order is recovered by
+matching each gold 3x3 / 1x3 block to exactly one neighbour block.
+"""
+import json
+import os
+import re
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+from oracle import np_ref  # noqa: E402
+
+REF = os.environ.get("PA_REFERENCE", "/root/reference")
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+
+def grab(src, name, start):
+    i = src.index(name, start)
+    j = src.index("{", i)
+    k = src.index("}", j)
+    return [float(x) for x in re.findall(r"[-+]?[0-9]*\.?[0-9]+(?:[eE][-+]?[0-9]+)?", src[j + 1:k])]
+
+
+def identify_numbering(R_gold):
+    """Solve for the vertex permutation of the 2x2x2 box (see module doc)."""
+    from scipy.optimize import Bounds, LinearConstraint, milp
+
+    cells, coords = np_ref.box_mesh(2, 2, 2)  # grid numbering, same tet split
+    prob = np_ref.Problem(cells, coords, E=1e6, nu=0.3, p=1.0, pmin=0.0)
+    K = prob.stiffness_dense(np.ones(27))
+    # u(vertex v) = 1e-4 (3v+1, 3v+2, 3v+3) = 3e-4 v (1,1,1) + rigid shift; K kills the shift.
+    Kh = np.zeros((27, 3, 27))
+    for g in range(27):
+        for h in range(27):
+            Kh[g, :, h] = K[3 * g:3 * g + 3, 3 * h:3 * h + 3].sum(1)
+    R = np.asarray(R_gold).reshape(27, 3)
+    nv = 27 * 27  # x[g*27 + v] = 1 iff grid point g carries vertex id v
+    rows, lo, hi = [], [], []
+    for g in range(27):
+        r = np.zeros(nv); r[g * 27:(g + 1) * 27] = 1; rows.append(r); lo.append(1); hi.append(1)
+    for v in range(27):
+        r = np.zeros(nv); r[v::27] = 1; rows.append(r); lo.append(1); hi.append(1)
+    for g in range(27):
+        for d in range(3):
+            r = np.zeros(nv)
+            for h in range(27):
+                r[h * 27:(h + 1) * 27] += 3e-4 * Kh[g, d, h] * np.arange(27)
+            r[g * 27:(g + 1) * 27] -= R[:, d]
+            rows.append(r / 100.0); lo.append(-1e-6); hi.append(1e-6)
+    res = milp(c=np.zeros(nv), constraints=LinearConstraint(np.array(rows), lo, hi),
+               integrality=np.ones(nv), bounds=Bounds(0, 1))
+    assert res.status == 0, res.message
+    perm = res.x.reshape(27, 27).round().astype(int).argmax(1)  # grid point -> vertex id
+    v_coords = np.zeros((27, 3))
+    v_coords[perm] = coords
+    v_cells = perm[cells]
+    return v_cells.astype(np.int32), v_coords
+
+
+def star_order_row0(blocks_gold, Kfull, cols_sorted, bi, bj):
+    """Column order of row 0 that reproduces the gold block sequence."""
+    order = []
+    for b in blocks_gold:
+        hits = [int(c) for c in cols_sorted
+                if np.allclose(Kfull[0:bi, bj * c:bj * c + bj].ravel(), b, rtol=1e-12, atol=1e-9) and c not in order]
+        assert len(hits) == 1, hits
+        order.append(hits[0])
+    return order
+
+
+def derivative_tests():
+    src = open(os.path.join(REF, "unit_tests/DerivativeTests.cpp")).read()
+    s0 = src.index("DerivativeTests, ElastostaticResidual3D")
+    s1 = src.index("DerivativeTests, InternalElasticEnergy3D")
+    gold = {
+        "residual": grab(src, "residual_gold", s0),
+        "jacobian_entries": grab(src, "gold_jac_entries", s0),
+        "gradient_z_entries": grab(src, "gold_grad_entries", s0),
+        "gradient_x_entries": grab(src, "gold_grad_x_entries", s0),
+        "energy_value": 46.125,
+        "energy_grad_u": grab(src, "grad_u_gold", s1),
+        "energy_grad_z": grab(src, "grad_z_gold", s1),
+        "energy_grad_x": grab(src, "grad_x_gold", s1),
+    }
+    cells, coords = identify_numbering(gold["residual"])
+    prob = np_ref.Problem(cells, coords, E=1e6, nu=0.3, p=1.0, pmin=0.0)
+    z = np.ones(27)
+    u = 1e-4 * np.arange(1, 82, dtype=np.float64)
+    K = prob.stiffness_dense(z)
+    G = prob.gradient_z_dense(u, z)
+    rowmap, cols = np_ref.crs_graph(cells, 27)
+    row0 = [int(c) for c in cols[rowmap[0]:rowmap[1]]]
+    jac_order = star_order_row0(np.asarray(gold["jacobian_entries"]).reshape(-1, 9), K, row0, 3, 3)
+    gz_order = star_order_row0(np.asarray(gold["gradient_z_entries"]).reshape(-1, 3), G, row0, 1, 3)
+    assert gz_order[:len(jac_order)] == jac_order
+    return {
+        "source": "unit_tests/DerivativeTests.cpp:273-700 (ElastostaticResidual3D, InternalElasticEnergy3D)",
+        "mesh": "Omega_h build_box 2x2x2 on the unit cube; numbering identified by tests/golden/make_golden.py",
+        "material": {"youngs_modulus": 1.0e6, "poissons_ratio": 0.3, "simp_exponent": 1.0, "simp_min": 0.0},
+        "state": "u_i = 1e-4 * (i + 1), z = 1",
+        "tolerances": {"residual": 1e-13, "jacobian_entries": 1e-15, "gradient_z_entries": 2e-14,
+                       "gradient_x_entries": 1e-13, "energy_value": 1e-13, "energy_grad_u": 1e-13,
+                       "energy_grad_z": 1e-13},
+        "cells": cells.tolist(),
+        "coords": coords.tolist(),
+        "row0_star_order": gz_order,
+        "gold": gold,
+    }
+
+
+def j2_plastic_step():
+    src = open(os.path.join(REF, "unit_tests/PlasticityTests.cpp")).read()
+    s = src.index("J2PlasticityUtils_UpdatePlasticStep3D")
+    e = src.index("TEUCHOS_UNIT_TEST", s + 10)
+    body = src[s:e]
+    i = body.index("tGold")
+    j = body.index("{{", i)
+    k = body.index("}};", j)
+    rows = re.findall(r"\{([^{}]*)\}", body[j + 1:k + 1])
+    gold = []
+    for r in rows:
+        vals = []
+        for tok in re.findall(r"tHostPrevLocalState\(\d,\d\)|[-+]?[0-9]*\.?[0-9]+", r):
+            m = re.match(r"tHostPrevLocalState\((\d),(\d)\)", tok)
+            vals.append((int(m.group(1)) + 1.0) * (int(m.group(2)) + 1.0) if m else float(tok))
+        gold.append(vals)
+    return {
+        "source": "unit_tests/PlasticityTests.cpp:283-333 (J2PlasticityUtils_UpdatePlasticStep3D)",
+        "setup": "prev[i][j] = (i+1)(j+1); normal[i][j] = (i+1)(j+2)/5; local state starts as prev; H_kin = 3",
+        "tolerance": 1e-4,
+        "gold": gold,
+    }
+
+
+def main():
+    with open(os.path.join(OUT, "derivative_tests_3d.json"), "w") as f:
+        json.dump(derivative_tests(), f, indent=1)
+    with open(os.path.join(OUT, "j2_plastic_step_3d.json"), "w") as f:
+        json.dump(j2_plastic_step(), f, indent=1)
+    print("wrote fixtures to", OUT)
+
+
+if __name__ == "__main__":
+    main()
