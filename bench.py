@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--method", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--rel-tol", type=float, default=1e-8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-kernel", action="store_true",
+                    help="only build the workload and time the fused CG kernel (for ncu captures)")
+    ap.add_argument("--reps", type=int, default=3)
     return ap.parse_args()
 
 
@@ -209,6 +212,29 @@ def traffic_from_profiles(kernel_tag):
         return None
 
 
+def profile_kernel(args):
+    """Build the workload and launch the fused CG kernel 1 + reps times per
+    precision (a short, self-contained command for ncu)."""
+    import ctypes as ct
+    import torch
+    import platoanalyze_b200 as pa  # noqa: F401
+    from platoanalyze_b200 import _abi
+    from platoanalyze_b200.workloads import cantilever, cell_density
+    dims = dims_of(args.dims)
+    torch.cuda.set_device(0)
+    mesh, prob, faces, dofs = cantilever(dims)
+    z = torch.tensor(cell_density(dims, SEED, kind="smoothed", sigma=3.0, lo=0.01, hi=1.0), device="cuda")
+    out = {"dims": dims, "tiles": mesh.num_tiles}
+    for prec, name in ((1, "fp32"), (0, "fp64")):
+        ms, nb = ct.c_double(), ct.c_int64()
+        _abi.check(_abi.load().pa_time_cg_apply(prob._h, ct.c_void_p(z.data_ptr()), prec, args.reps, ct.byref(ms),
+                                                ct.byref(nb)))
+        out[name] = {"ms_per_launch": ms.value, "GB/s": nb.value / (ms.value * 1e-3) / 1e9,
+                     "algorithmic_bytes": nb.value}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -342,6 +368,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile_kernel:
+        return profile_kernel(args)
     return run_ours(args)
 
 

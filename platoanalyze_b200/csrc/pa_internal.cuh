@@ -65,24 +65,27 @@ struct DevBuf {
 };
 
 // ------------------------------------------------------------- tile layout --
-// Cells are grouped into tiles of at most kTileCells cells touching at most
+// Cells are grouped into clusters (six tets of one hex, or a single tet) and
+// clusters into tiles of at most kTileClusters clusters touching at most
 // kTileNodes distinct nodes.  A tile's nodes are staged in shared memory;
-// each cell stores its 4 tile-local node ids as 4 bytes.  tile_nodes entries
-// carry two flags: kShared (the node also belongs to another tile, so its
-// sum is added atomically) and kOwner (this tile writes per-node outputs of
-// the node, exactly one tile per node).
-constexpr int kTileCells = 256;
-constexpr int kTileNodes = 256;
+// each cluster stores up to 8 tile-local node ids as uint16.  tile_nodes
+// entries carry two flags: kShared (the node also belongs to another tile,
+// so its sum is added atomically) and kOwner (this tile writes per-node
+// outputs of the node; exactly one tile per node).
+constexpr int kTileClusters = 256;
+constexpr int kTileNodes = 512;
 constexpr uint32_t kShared = 0x80000000u;
 constexpr uint32_t kOwner = 0x40000000u;
 constexpr uint32_t kNodeMask = 0x3fffffffu;
 
 struct TileView {
-  const int32_t* tile_cell_start;  // T+1, internal cell index
-  const int32_t* tile_node_start;  // T+1
-  const uint32_t* tile_nodes;      // flagged global node ids
-  const uint32_t* cell_local;      // C, 4 x uint8 local ids (internal order)
-  const int32_t* cell_perm;        // C, internal -> user cell id
+  const int32_t* tile_cluster_start;  // T+1
+  const int32_t* tile_hex_count;      // T: the first tile_hex_count clusters of a tile are hexes
+  const int32_t* tile_node_start;     // T+1
+  const uint32_t* tile_nodes;         // flagged global node ids
+  const uint4* cluster_nodes;         // 8 x uint16 tile-local node ids (hex slot order / cell order)
+  const int32_t* cluster_cell_start;  // first internal cell of each cluster
+  const int32_t* cell_perm;           // C, internal -> user cell id
   int32_t num_tiles;
 };
 
@@ -98,12 +101,14 @@ struct Mesh {
   DevBuf<float> d_coords32;
   DevBuf<int32_t> d_rowmap, d_cols;
   DevBuf<int32_t> d_cell_entry;  // C*16 CRS block index of (a,b) pairs
-  DevBuf<int32_t> d_tile_cell_start, d_tile_node_start, d_cell_perm;
-  DevBuf<uint32_t> d_tile_nodes, d_cell_local;
+  int64_t num_clusters = 0, num_hex = 0;
+  DevBuf<int32_t> d_tile_cluster_start, d_tile_hex_count, d_tile_node_start, d_cluster_cell_start, d_cell_perm;
+  DevBuf<uint32_t> d_tile_nodes;
+  DevBuf<uint4> d_cluster_nodes;
   std::vector<int32_t> h_cell_perm;  // internal -> user
   TileView tiles() const {
-    return TileView{d_tile_cell_start.get(), d_tile_node_start.get(), d_tile_nodes.get(), d_cell_local.get(),
-                    d_cell_perm.get(), int32_t(T)};
+    return TileView{d_tile_cluster_start.get(), d_tile_hex_count.get(), d_tile_node_start.get(), d_tile_nodes.get(),
+                    d_cluster_nodes.get(), d_cluster_cell_start.get(), d_cell_perm.get(), int32_t(T)};
   }
   void build_graph_entries();
 };

@@ -20,10 +20,114 @@ inline uint64_t spread3(uint64_t v) {  // 21 bits -> every third bit
   return v;
 }
 
-// Cell order for tiling: Morton (Z-order) of the cell centroids, so that
-// consecutive cells are spatially compact and a tile of 256 tets touches few
-// nodes (about 100 on a structured box).
-std::vector<int32_t> morton_order(const Mesh& m) {
+struct Cluster {
+  int32_t cell0;        // first user cell (hex: the 6 cells in template order below)
+  int32_t hex_cells[6]; // hex only: user cells of template tets T0..T5
+  int32_t nodes[8];     // hex: slot s = a + 2b + 4c; single: its 4 nodes
+  bool hex;
+  uint64_t key;
+};
+
+// Six consecutive cells form a hex cluster when their union has 8 nodes, two
+// of which (the diagonal) belong to all six tets and the other six form a
+// ring in which consecutive tets share one node.  Labeling: diagonal ->
+// slots 0 and 7, ring r0..r5 -> slots 3, 2, 6, 4, 5, 1, so that tet
+// {d0, d1, r_k, r_k+1} is template tet T_k of hex_slot().
+bool match_hex(const Mesh& m, int64_t c0, Cluster& out) {
+  int32_t nodes[24];
+  for (int j = 0; j < 6; ++j)
+    for (int n = 0; n < 4; ++n) nodes[4 * j + n] = m.cells[4 * (c0 + j) + n];
+  int32_t uniq[24];
+  int nu = 0;
+  for (int i = 0; i < 24; ++i) {
+    bool seen = false;
+    for (int k = 0; k < nu && !seen; ++k) seen = uniq[k] == nodes[i];
+    if (!seen) uniq[nu++] = nodes[i];
+  }
+  if (nu != 8) return false;
+  auto has = [&](int j, int32_t v) {
+    for (int n = 0; n < 4; ++n)
+      if (nodes[4 * j + n] == v) return true;
+    return false;
+  };
+  int32_t diag[2];
+  int nd = 0;
+  for (int k = 0; k < 8; ++k) {
+    bool all = true;
+    for (int j = 0; j < 6 && all; ++j) all = has(j, uniq[k]);
+    if (all) {
+      if (nd == 2) return false;
+      diag[nd++] = uniq[k];
+    }
+  }
+  if (nd != 2) return false;
+  // ring nodes of each tet
+  int32_t ring[6][2];
+  for (int j = 0; j < 6; ++j) {
+    int r = 0;
+    for (int n = 0; n < 4; ++n) {
+      const int32_t v = nodes[4 * j + n];
+      if (v == diag[0] || v == diag[1]) continue;
+      if (r == 2) return false;
+      ring[j][r++] = v;
+    }
+    if (r != 2 || ring[j][0] == ring[j][1]) return false;
+  }
+  // walk the cycle: tet order t_0..t_5 with ring nodes (r_k, r_k+1)
+  int order[6];
+  int32_t rn[7];
+  bool used[6] = {false, false, false, false, false, false};
+  order[0] = 0;
+  used[0] = true;
+  rn[0] = ring[0][0];
+  rn[1] = ring[0][1];
+  for (int k = 1; k < 6; ++k) {
+    int next = -1;
+    for (int j = 0; j < 6; ++j)
+      if (!used[j] && (ring[j][0] == rn[k] || ring[j][1] == rn[k])) {
+        if (next >= 0) return false;
+        next = j;
+      }
+    if (next < 0) return false;
+    used[next] = true;
+    order[k] = next;
+    rn[k + 1] = ring[next][0] == rn[k] ? ring[next][1] : ring[next][0];
+  }
+  if (rn[6] != rn[0]) return false;
+  for (int a = 0; a < 6; ++a)
+    for (int b = a + 1; b < 6; ++b)
+      if (rn[a] == rn[b]) return false;
+  static const int ring_slot[6] = {3, 2, 6, 4, 5, 1};
+  out.hex = true;
+  out.cell0 = int32_t(c0);
+  out.nodes[0] = diag[0];
+  out.nodes[7] = diag[1];
+  for (int k = 0; k < 6; ++k) out.nodes[ring_slot[k]] = rn[k];
+  for (int k = 0; k < 6; ++k) out.hex_cells[k] = int32_t(c0 + order[k]);
+  return true;
+}
+
+// Clusters (hex groups of six consecutive cells, else single cells), ordered
+// along the Morton (Z-order) curve of their centroids, packed greedily into
+// tiles of <= kTileClusters clusters and <= kTileNodes nodes.
+void build_tiles(Mesh& m) {
+  std::vector<Cluster> cl;
+  cl.reserve(m.C / 6 + 16);
+  for (int64_t c = 0; c < m.C;) {
+    Cluster h;
+    if (c + 6 <= m.C && match_hex(m, c, h)) {
+      cl.push_back(h);
+      c += 6;
+      continue;
+    }
+    Cluster s{};
+    s.hex = false;
+    s.cell0 = int32_t(c);
+    for (int n = 0; n < 4; ++n) s.nodes[n] = m.cells[4 * c + n];
+    for (int n = 4; n < 8; ++n) s.nodes[n] = -1;
+    cl.push_back(s);
+    ++c;
+  }
   double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
   for (int64_t v = 0; v < m.N; ++v)
     for (int d = 0; d < 3; ++d) {
@@ -32,75 +136,105 @@ std::vector<int32_t> morton_order(const Mesh& m) {
     }
   double scale[3];
   for (int d = 0; d < 3; ++d) scale[d] = (hi[d] > lo[d]) ? double((1 << 21) - 1) / (hi[d] - lo[d]) : 0.0;
-  std::vector<std::pair<uint64_t, int32_t>> keys(m.C);
-  for (int64_t c = 0; c < m.C; ++c) {
+  for (auto& k : cl) {
+    const int nn = k.hex ? 8 : 4;
     double ctr[3] = {0, 0, 0};
-    for (int n = 0; n < 4; ++n)
-      for (int d = 0; d < 3; ++d) ctr[d] += 0.25 * m.coords[3 * int64_t(m.cells[4 * c + n]) + d];
+    for (int n = 0; n < nn; ++n)
+      for (int d = 0; d < 3; ++d) ctr[d] += m.coords[3 * int64_t(k.nodes[n]) + d] / nn;
     uint64_t q[3];
     for (int d = 0; d < 3; ++d) q[d] = uint64_t(std::llround((ctr[d] - lo[d]) * scale[d]));
-    keys[c] = {spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2), int32_t(c)};
+    k.key = spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2);
   }
-  std::sort(keys.begin(), keys.end());
-  std::vector<int32_t> order(m.C);
-  for (int64_t i = 0; i < m.C; ++i) order[i] = keys[i].second;
-  return order;
-}
+  std::stable_sort(cl.begin(), cl.end(), [](const Cluster& a, const Cluster& b) { return a.key < b.key; });
 
-void build_tiles(Mesh& m) {
-  std::vector<int32_t> order = morton_order(m);
-  std::vector<int32_t> tile_cell_start{0}, tile_node_start{0};
-  std::vector<uint32_t> tile_nodes, cell_local(m.C);
+  std::vector<int32_t> tile_cluster_start{0}, tile_hex_count, tile_node_start{0}, cluster_cell_start, perm;
+  std::vector<uint32_t> tile_nodes;
+  std::vector<uint4> cluster_nodes;
+  perm.reserve(m.C);
   std::vector<int32_t> stamp(m.N, -1), local(m.N, 0), node_tiles(m.N, 0), owner(m.N, -1);
   std::vector<int32_t> cur_nodes;
-  cur_nodes.reserve(kTileNodes);
+  std::vector<const Cluster*> cur;
   int32_t tile = 0;
-  int64_t first_cell = 0;
+  int64_t nhex_total = 0;
 
-  auto close_tile = [&](int64_t end_cell) {
-    // Sort the tile's nodes by id (coalesced staging loads) and fix local ids.
+  auto close_tile = [&]() {
     std::vector<int32_t> sorted = cur_nodes;
     std::sort(sorted.begin(), sorted.end());
     for (size_t i = 0; i < sorted.size(); ++i) local[sorted[i]] = int32_t(i);
-    for (int64_t i = first_cell; i < end_cell; ++i) {
-      const int32_t c = order[i];
-      uint32_t packed = 0;
-      for (int n = 0; n < 4; ++n) packed |= uint32_t(local[m.cells[4 * int64_t(c) + n]]) << (8 * n);
-      cell_local[i] = packed;
+    std::stable_partition(cur.begin(), cur.end(), [](const Cluster* k) { return k->hex; });
+    int32_t nh = 0;
+    for (const Cluster* k : cur) {
+      cluster_cell_start.push_back(int32_t(perm.size()));
+      uint16_t ids[8];
+      for (int n = 0; n < 8; ++n) ids[n] = k->nodes[n] >= 0 ? uint16_t(local[k->nodes[n]]) : uint16_t(0xffff);
+      uint4 q;
+      q.x = uint32_t(ids[0]) | (uint32_t(ids[1]) << 16);
+      q.y = uint32_t(ids[2]) | (uint32_t(ids[3]) << 16);
+      q.z = uint32_t(ids[4]) | (uint32_t(ids[5]) << 16);
+      q.w = uint32_t(ids[6]) | (uint32_t(ids[7]) << 16);
+      cluster_nodes.push_back(q);
+      if (k->hex) {
+        ++nh;
+        for (int j = 0; j < 6; ++j) perm.push_back(k->hex_cells[j]);
+      } else {
+        perm.push_back(k->cell0);
+      }
     }
     for (int32_t v : sorted) {
       tile_nodes.push_back(uint32_t(v));
       node_tiles[v] += 1;
       if (owner[v] < 0) owner[v] = tile;
     }
-    tile_cell_start.push_back(int32_t(end_cell));
+    nhex_total += nh;
+    tile_hex_count.push_back(nh);
+    tile_cluster_start.push_back(int32_t(cluster_nodes.size()));
     tile_node_start.push_back(int32_t(tile_nodes.size()));
     cur_nodes.clear();
+    cur.clear();
     ++tile;
-    first_cell = end_cell;
   };
 
-  for (int64_t i = 0; i < m.C; ++i) {
-    const int32_t c = order[i];
+  for (const Cluster& k : cl) {
+    const int nn = k.hex ? 8 : 4;
     int fresh = 0;
-    for (int n = 0; n < 4; ++n) {
-      const int32_t v = m.cells[4 * int64_t(c) + n];
-      bool seen = stamp[v] == tile;
-      for (int k = 0; k < n && !seen; ++k) seen = (m.cells[4 * int64_t(c) + k] == v);
-      fresh += seen ? 0 : 1;
-    }
-    if (i - first_cell >= kTileCells || int(cur_nodes.size()) + fresh > kTileNodes) close_tile(i);
-    for (int n = 0; n < 4; ++n) {
-      const int32_t v = m.cells[4 * int64_t(c) + n];
+    for (int n = 0; n < nn; ++n) fresh += stamp[k.nodes[n]] == tile ? 0 : 1;
+    if (int(cur.size()) >= kTileClusters || int(cur_nodes.size()) + fresh > kTileNodes) close_tile();
+    for (int n = 0; n < nn; ++n) {
+      const int32_t v = k.nodes[n];
       if (stamp[v] != tile) {
         stamp[v] = tile;
         cur_nodes.push_back(v);
       }
     }
+    cur.push_back(&k);
   }
-  if (m.C > first_cell) close_tile(m.C);
+  if (!cur.empty()) close_tile();
+  if (int64_t(perm.size()) != m.C) throw Error(PA_ERR_INVALID_ARG, "cluster build lost cells");
+  // Structural checks the kernel relies on (every shared-memory index in range,
+  // every cell exactly once).
+  {
+    std::vector<uint8_t> seen(m.C, 0);
+    for (int32_t c : perm) {
+      if (c < 0 || c >= m.C || seen[c]) throw Error(PA_ERR_INVALID_ARG, "cell permutation is not a bijection");
+      seen[c] = 1;
+    }
+    for (int32_t t = 0; t < tile; ++t) {
+      const int32_t nn = tile_node_start[t + 1] - tile_node_start[t];
+      const int32_t nk = tile_cluster_start[t + 1] - tile_cluster_start[t];
+      if (nn > kTileNodes || nk > kTileClusters || tile_hex_count[t] > nk)
+        throw Error(PA_ERR_INVALID_ARG, "tile exceeds its shared-memory capacity");
+      for (int32_t k = tile_cluster_start[t]; k < tile_cluster_start[t + 1]; ++k) {
+        const uint4 q = cluster_nodes[k];
+        const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+        const int used = (k - tile_cluster_start[t]) < tile_hex_count[t] ? 8 : 4;
+        for (int n = 0; n < used; ++n) {
+          const uint32_t id = (w[n / 2] >> (16 * (n % 2))) & 0xffffu;
+          if (int32_t(id) >= nn) throw Error(PA_ERR_INVALID_ARG, "cluster node id outside its tile");
+        }
+      }
+    }
+  }
 
-  // Flags: shared (written by atomics) and owner (exactly one tile per node).
   for (int32_t t = 0; t < tile; ++t)
     for (int32_t k = tile_node_start[t]; k < tile_node_start[t + 1]; ++k) {
       const uint32_t v = tile_nodes[k];
@@ -110,12 +244,16 @@ void build_tiles(Mesh& m) {
       tile_nodes[k] = f;
     }
   m.T = tile;
-  m.h_cell_perm = order;
-  m.d_tile_cell_start.upload(tile_cell_start.data(), tile_cell_start.size());
+  m.num_clusters = int64_t(cluster_nodes.size());
+  m.num_hex = nhex_total;
+  m.h_cell_perm = perm;
+  m.d_tile_cluster_start.upload(tile_cluster_start.data(), tile_cluster_start.size());
+  m.d_tile_hex_count.upload(tile_hex_count.data(), tile_hex_count.size());
   m.d_tile_node_start.upload(tile_node_start.data(), tile_node_start.size());
   m.d_tile_nodes.upload(tile_nodes.data(), tile_nodes.size());
-  m.d_cell_local.upload(cell_local.data(), cell_local.size());
-  m.d_cell_perm.upload(order.data(), order.size());
+  m.d_cluster_nodes.upload(cluster_nodes.data(), cluster_nodes.size());
+  m.d_cluster_cell_start.upload(cluster_cell_start.data(), cluster_cell_start.size());
+  m.d_cell_perm.upload(perm.data(), perm.size());
 }
 
 // Node-star graph plus diagonal, sorted columns: the pattern CreateBlockMatrix

@@ -1,30 +1,35 @@
-// pa_tiled.cuh -- tile-staged matrix-free K.x, the hot kernel of the solve.
+// pa_tiled.cuh -- tile-staged, hex-clustered matrix-free K.x: the hot kernel
+// of the solve.
 //
-// Design (B200): a persistent grid of CTAs (a multiple of the SM count) walks
-// the cell tiles.  For each tile the CTA
-//   1. stages the tile's nodes (<= 256) in shared memory: coordinates, input
-//      vector, Dirichlet mask -- one coalesced pass over the tile's sorted
-//      node list, so each node's data is read from HBM/L2 once per tile
-//      instead of once per incident cell (about 24 tets share a node);
-//   2. evaluates one tet per thread entirely in registers (geometry, strain,
-//      stress, SIMP weight, divergence), reading its 4 nodes through 1-byte
-//      local ids (4 bytes of connectivity per cell instead of 16);
-//   3. accumulates the 12 cell results into shared-memory node sums
-//      (shared-memory atomics, no global contention);
-//   4. writes each node sum once: a plain store for nodes only this tile
-//      touches, one global atomic add per dof for nodes shared with other
-//      tiles (~1 atomic per cell instead of the reference's 12,
-//      src/Assembly.hpp:1189-1209).
-// The PCG variant additionally forms p = D^-1 r + beta p_old while staging
-// (the owner tile writes p once) and reduces p.Kp = sum_cells p_e^T K_e p_e
-// from the per-cell energies, so the search-direction update and the first
-// dot product need no extra pass over the vectors.
+// Mesh layout (built once on the host, pa_mesh.cu):
+//  * cells are grouped into clusters: a "hex" cluster is six tets that form
+//    the six-tet split of one hexahedron around a diagonal (the split every
+//    hex-derived tet mesh, e.g. a structured box, has); any other cell is a
+//    "single" cluster.  A hex cluster touches 8 nodes for 6 cells, a single
+//    one 4 nodes for 1 cell.
+//  * clusters are ordered along a Morton curve and packed into tiles of at
+//    most kTileClusters clusters touching at most kTileNodes nodes.
+//
+// Kernel (a persistent grid, a multiple of the SM count, walks the tiles):
+//  1. stage the tile's nodes in shared memory (coordinates, input vector,
+//     Dirichlet mask) in one coalesced pass over the tile's sorted node list;
+//  2. one thread per cluster: read the cluster's nodes from shared memory
+//     into registers once, evaluate its tets (geometry, strain, stress, SIMP
+//     weight, divergence) and accumulate the node sums in registers -- a hex
+//     cluster reads 8 nodes and issues 24 shared-memory atomics for 6 tets,
+//     instead of 24 node reads and 72 atomics cell by cell;
+//  3. write each node sum once: a plain store for nodes only this tile
+//     touches, a global atomic add for nodes shared with other tiles.
+// The PCG variant (MODE 1) forms p = D^-1 r + beta p_old while staging (the
+// owner tile writes p once) and reduces p.Kp = sum_cells p_e^T K_e p_e from
+// the per-tet energies, so the search-direction update and the first dot
+// product need no extra pass over the vectors.
 #pragma once
 #include "pa_cell.cuh"
 
 namespace pa {
 
-constexpr int kApplyThreads = kTileCells;
+constexpr int kApplyThreads = kTileClusters;
 
 template <typename T>
 struct ApplyArgs {
@@ -71,10 +76,29 @@ __device__ __forceinline__ bool last_block_arrive(unsigned int* counter) {
   return s_last;
 }
 
+// Six tets of a hex cluster in slot numbering s = a + 2b + 4c of corner (a,b,c);
+// a constant expression, so that after unrolling every register index is static.
+__host__ __device__ constexpr int hex_slot(int j, int n) {
+  constexpr int t[6][4] = {{0, 3, 2, 7}, {0, 2, 6, 7}, {0, 6, 4, 7}, {0, 5, 7, 4}, {1, 5, 7, 0}, {1, 7, 3, 0}};
+  return t[j][n];
+}
+
+// One tet: contributions r[4][3] for its nodes from xs (coords) and us (input);
+// returns the tet's energy sig:eps (for p.Kp).
+template <typename T>
+__device__ __forceinline__ T tet_apply(const Iso<T>& iso, T w, const T (&xc)[4][3], const T (&u)[12], T (&r)[12]) {
+  T g[4][3], vol, e[6], sig[6];
+  tet_geometry(xc, g, vol);
+  tet_strain(g, u, e);
+  tet_stress(iso, vol * w, e, sig);
+  tet_divergence(g, sig, r);
+  return voigt_dot(sig, e);
+}
+
 template <typename T, int MODE>
-__global__ void __launch_bounds__(kApplyThreads, 2) k_apply_tiled(ApplyArgs<T> a) {
-  __shared__ T s_x[kTileNodes * 3];
+__global__ void __launch_bounds__(kApplyThreads, 1) k_apply_tiled(ApplyArgs<T> a) {
   __shared__ T s_c[kTileNodes * 3];
+  __shared__ T s_x[kTileNodes * 3];
   __shared__ T s_y[kTileNodes * 3];
   __shared__ uint32_t s_node[kTileNodes];
   __shared__ uint8_t s_mask[kTileNodes];
@@ -89,7 +113,9 @@ __global__ void __launch_bounds__(kApplyThreads, 2) k_apply_tiled(ApplyArgs<T> a
 
   for (int tile = blockIdx.x; tile < a.tv.num_tiles; tile += gridDim.x) {
     const int n0 = a.tv.tile_node_start[tile], nn = a.tv.tile_node_start[tile + 1] - n0;
-    const int c0 = a.tv.tile_cell_start[tile], nc = a.tv.tile_cell_start[tile + 1] - c0;
+    const int k0 = a.tv.tile_cluster_start[tile], nk = a.tv.tile_cluster_start[tile + 1] - k0;
+    const int nhex = a.tv.tile_hex_count[tile];
+    // 1. stage nodes
     for (int i = threadIdx.x; i < nn; i += blockDim.x) {
       const uint32_t f = a.tv.tile_nodes[n0 + i];
       const int64_t gid = f & kNodeMask;
@@ -112,32 +138,64 @@ __global__ void __launch_bounds__(kApplyThreads, 2) k_apply_tiled(ApplyArgs<T> a
       }
     }
     __syncthreads();
-    if (threadIdx.x < nc) {
-      const int c = c0 + threadIdx.x;
-      const uint32_t loc = a.tv.cell_local[c];
-      int ln[4];
-      T xc[4][3], u[12];
+    // 2. one cluster per thread
+    const int t = threadIdx.x;
+    if (t < nk) {
+      const int k = k0 + t;
+      const uint4 q = a.tv.cluster_nodes[k];
+      const int c0 = a.tv.cluster_cell_start[k];
+      int ln[8] = {int(q.x & 0xffff), int(q.x >> 16), int(q.y & 0xffff), int(q.y >> 16),
+                   int(q.z & 0xffff), int(q.z >> 16), int(q.w & 0xffff), int(q.w >> 16)};
+      if (t < nhex) {
+        T X[8][3], U[8][3], Y[8][3];
 #pragma unroll
-      for (int n = 0; n < 4; ++n) {
-        ln[n] = (loc >> (8 * n)) & 0xff;
+        for (int s = 0; s < 8; ++s)
 #pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          xc[n][d] = s_c[3 * ln[n] + d];
-          u[3 * n + d] = s_x[3 * ln[n] + d];
+          for (int d = 0; d < 3; ++d) {
+            X[s][d] = s_c[3 * ln[s] + d];
+            U[s][d] = s_x[3 * ln[s] + d];
+            Y[s][d] = T(0);
+          }
+#pragma unroll
+        for (int j = 0; j < 6; ++j) {
+          T xc[4][3], u[12], r[12];
+#pragma unroll
+          for (int n = 0; n < 4; ++n)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+              xc[n][d] = X[hex_slot(j, n)][d];
+              u[3 * n + d] = U[hex_slot(j, n)][d];
+            }
+          const T en = tet_apply(a.iso, a.w[c0 + j], xc, u, r);
+          if (MODE == 1) pap += double(en);
+#pragma unroll
+          for (int n = 0; n < 4; ++n)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) Y[hex_slot(j, n)][d] += r[3 * n + d];
         }
+#pragma unroll
+        for (int s = 0; s < 8; ++s)
+#pragma unroll
+          for (int d = 0; d < 3; ++d) atomicAdd(&s_y[3 * ln[s] + d], Y[s][d]);
+      } else {
+        T xc[4][3], u[12], r[12];
+#pragma unroll
+        for (int n = 0; n < 4; ++n)
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            xc[n][d] = s_c[3 * ln[n] + d];
+            u[3 * n + d] = s_x[3 * ln[n] + d];
+          }
+        const T en = tet_apply(a.iso, a.w[c0], xc, u, r);
+        if (MODE == 1) pap += double(en);
+#pragma unroll
+        for (int n = 0; n < 4; ++n)
+#pragma unroll
+          for (int d = 0; d < 3; ++d) atomicAdd(&s_y[3 * ln[n] + d], r[3 * n + d]);
       }
-      T g[4][3], vol, e[6], sig[6], r[12];
-      tet_geometry(xc, g, vol);
-      tet_strain(g, u, e);
-      tet_stress(a.iso, vol * a.w[c], e, sig);
-      if (MODE == 1) pap += double(voigt_dot(sig, e));
-      tet_divergence(g, sig, r);
-#pragma unroll
-      for (int n = 0; n < 4; ++n)
-#pragma unroll
-        for (int d = 0; d < 3; ++d) atomicAdd(&s_y[3 * ln[n] + d], r[3 * n + d]);
     }
     __syncthreads();
+    // 3. write node sums
     for (int i = threadIdx.x; i < nn; i += blockDim.x) {
       const uint32_t f = s_node[i];
       const int64_t gid = f & kNodeMask;

@@ -17,22 +17,35 @@ def rel_inf(a, b):
     return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
 
 
-def perturbed_box(nx, ny, nz, seed, amp=0.1):
+def perturbed_box(nx, ny, nz, seed, amp=0.1, order="hex"):
+    """Box mesh with jittered interior nodes.  order="hex": the generator's
+    order (six tets of a hex consecutive: hex clusters); "mixed": the hexes in
+    random order with a random vertex order inside each tet (still hex
+    clusters) plus a shuffled tail of single cells; "shuffled": all cells
+    shuffled (single-cell clusters)."""
     from oracle import np_ref
     cells, coords = np_ref.box_mesh(nx, ny, nz, float(nx), float(ny), float(nz))
     rng = np.random.default_rng(seed)
     inner = np.all((coords > 1e-9) & (coords < np.array([nx, ny, nz]) - 1e-9), axis=1)
     coords[inner] += amp * rng.uniform(-1, 1, (inner.sum(), 3))
-    return cells, coords
+    if order == "mixed":
+        hexes = cells.reshape(-1, 6, 4)[rng.permutation(cells.shape[0] // 6)]
+        cells = np.array([rng.permutation(c) for c in hexes.reshape(-1, 4)], dtype=np.int32)
+        tail = cells.shape[0] // 3
+        cells[-tail:] = cells[-tail:][rng.permutation(tail)]
+    elif order == "shuffled":
+        cells = cells[rng.permutation(cells.shape[0])]
+    return np.ascontiguousarray(cells), coords
 
 
-CASES = [((3, 2, 2), 0, "nodal"), ((7, 5, 4), 1, "cell"), ((12, 9, 7), 2, "nodal"), ((1, 1, 1), 3, "cell")]
+CASES = [((3, 2, 2), 0, "nodal", "hex"), ((7, 5, 4), 1, "cell", "mixed"), ((12, 9, 7), 2, "nodal", "hex"),
+         ((1, 1, 1), 3, "cell", "hex"), ((6, 5, 4), 4, "nodal", "shuffled"), ((9, 7, 5), 5, "cell", "mixed")]
 
 
-@pytest.fixture(scope="module", params=CASES, ids=lambda c: f"{c[0][0]}x{c[0][1]}x{c[0][2]}-{c[2]}")
+@pytest.fixture(scope="module", params=CASES, ids=lambda c: f"{c[0][0]}x{c[0][1]}x{c[0][2]}-{c[2]}-{c[3]}")
 def setup(request, pa, oracle_lib):
-    dims, seed, layout = request.param
-    cells, coords = perturbed_box(*dims, seed)
+    dims, seed, layout, order = request.param
+    cells, coords = perturbed_box(*dims, seed, order=order)
     rng = np.random.default_rng(100 + seed)
     E, nu, p, pmin = 3.0, 0.27, 3.0, 1e-6
     lay = 1 if layout == "cell" else 0
