@@ -157,6 +157,9 @@ void upload_bcs(Problem& P) {
   std::vector<uint8_t> mask(N, 0);
   for (int32_t d : P.bc_dofs) mask[d / 3] |= uint8_t(1u << (d % 3));
   P.d_node_mask.upload(mask.data(), mask.size(), P.stream);
+  std::vector<uint32_t> tn = P.mesh->h_tile_nodes;
+  for (uint32_t& f : tn) f |= uint32_t(mask[f & pa::kNodeIdMask]) << pa::kMaskShift;
+  P.d_tile_nodes_bc.upload(tn.data(), tn.size(), P.stream);
   if (!P.bc_dofs.empty()) {
     P.d_bc_dofs.upload(P.bc_dofs.data(), P.bc_dofs.size(), P.stream);
     P.d_bc_vals.upload(P.bc_vals.data(), P.bc_vals.size(), P.stream);
@@ -469,11 +472,10 @@ pa_status pa_apply(pa_problem* problem, const double* z, const void* x, void* y,
     P.ws.w64.resize(P.C());
     if (precision == PA_FP32) P.ws.w32.resize(P.C());
     pa::launch_cell_weights(P, dz, P.ws.w64.get(), precision == PA_FP32 ? P.ws.w32.get() : nullptr, P.stream);
-    const uint8_t* mask = constrained ? P.d_node_mask.get() : nullptr;
     if (precision == PA_FP64) {
       const double* dx = st.in(static_cast<const double*>(x), n, "x");
       double* dy = st.out(static_cast<double*>(y), n, "y");
-      pa::launch_apply_tiled<double>(P, P.ws.w64.get(), dx, dy, mask, P.stream);
+      pa::launch_apply_tiled<double>(P, P.ws.w64.get(), dx, dy, constrained != 0, P.stream);
       if (constrained && !P.bc_dofs.empty()) {
         // identity rows on constrained dofs
         std::vector<int32_t>& d = P.bc_dofs;
@@ -483,7 +485,7 @@ pa_status pa_apply(pa_problem* problem, const double* z, const void* x, void* y,
     } else {
       const float* dx = st.in(static_cast<const float*>(x), n, "x");
       float* dy = st.out(static_cast<float*>(y), n, "y");
-      pa::launch_apply_tiled<float>(P, P.ws.w32.get(), dx, dy, mask, P.stream);
+      pa::launch_apply_tiled<float>(P, P.ws.w32.get(), dx, dy, constrained != 0, P.stream);
       if (constrained && !P.bc_dofs.empty()) {
         std::vector<int32_t>& d = P.bc_dofs;
         for (size_t i = 0; i < d.size(); ++i)

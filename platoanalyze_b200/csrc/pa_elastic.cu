@@ -377,35 +377,25 @@ void launch_scale(double* v, int64_t n, double a, cudaStream_t s) {
   PA_LAUNCHED();
 }
 
-int apply_grid(const void* kernel) {
-  int per_sm = 0;
-  PA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kApplyThreads, 0));
-  if (per_sm < 1) per_sm = 1;
-  return per_sm * num_sms();
-}
-
 template <typename T>
-void launch_apply_tiled(const Problem& P, const T* w, const T* x, T* y, const uint8_t* node_mask, cudaStream_t s) {
+void launch_apply_tiled(const Problem& P, const T* w, const T* x, T* y, bool constrained, cudaStream_t s) {
   ApplyArgs<T> a{};
   a.tv = P.mesh->tiles();
+  a.tile_nodes = constrained ? P.d_tile_nodes_bc.get() : P.mesh->d_tile_nodes.get();
   a.coords = std::is_same<T, double>::value ? reinterpret_cast<const T*>(P.mesh->d_coords.get())
                                             : reinterpret_cast<const T*>(P.mesh->d_coords32.get());
   a.w = w;
-  a.node_mask = node_mask;
   Iso<double> i64 = P.ep.iso();
   a.iso = Iso<T>{T(i64.lam), T(i64.mu)};
   a.x = x;
   a.y = y;
   PA_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * P.ndof(), s));
-  int grid = apply_grid(reinterpret_cast<const void*>(&k_apply_tiled<T, 0>));
-  if (grid > a.tv.num_tiles) grid = a.tv.num_tiles;
-  k_apply_tiled<T, 0><<<grid, kApplyThreads, 0, s>>>(a);
+  const int grid = apply_kernel_setup<T, 0>(a.tv.num_tiles);
+  k_apply_tiled<T, 0><<<grid, kApplyThreads, tile_smem_bytes<T, 0>(), s>>>(a);
   PA_LAUNCHED();
 }
 
-template void launch_apply_tiled<double>(const Problem&, const double*, const double*, double*, const uint8_t*,
-                                         cudaStream_t);
-template void launch_apply_tiled<float>(const Problem&, const float*, const float*, float*, const uint8_t*,
-                                        cudaStream_t);
+template void launch_apply_tiled<double>(const Problem&, const double*, const double*, double*, bool, cudaStream_t);
+template void launch_apply_tiled<float>(const Problem&, const float*, const float*, float*, bool, cudaStream_t);
 
 }  // namespace pa

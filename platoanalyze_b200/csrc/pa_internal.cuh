@@ -69,22 +69,24 @@ struct DevBuf {
 // clusters into tiles of at most kTileClusters clusters touching at most
 // kTileNodes distinct nodes.  A tile's nodes are staged in shared memory;
 // each cluster stores up to 8 tile-local node ids as uint16.  tile_nodes
-// entries carry two flags: kShared (the node also belongs to another tile,
-// so its sum is added atomically) and kOwner (this tile writes per-node
-// outputs of the node; exactly one tile per node).
+// entries are a 27-bit node id plus flags: kShared (the node also belongs to
+// another tile, so its sum is added atomically), kOwner (this tile writes
+// per-node outputs of the node; exactly one tile per node) and three
+// Dirichlet-mask bits (bit d: dof d constrained; set in a problem's copy).
 constexpr int kTileClusters = 256;
 constexpr int kTileNodes = 512;
 constexpr uint32_t kShared = 0x80000000u;
 constexpr uint32_t kOwner = 0x40000000u;
-constexpr uint32_t kNodeMask = 0x3fffffffu;
+constexpr int kMaskShift = 27;
+constexpr uint32_t kNodeIdMask = (1u << kMaskShift) - 1u;
 
 struct TileView {
   const int32_t* tile_cluster_start;  // T+1
+  const int32_t* tile_cell_start;     // T+1, internal cell index
   const int32_t* tile_hex_count;      // T: the first tile_hex_count clusters of a tile are hexes
   const int32_t* tile_node_start;     // T+1
   const uint32_t* tile_nodes;         // flagged global node ids
   const uint4* cluster_nodes;         // 8 x uint16 tile-local node ids (hex slot order / cell order)
-  const int32_t* cluster_cell_start;  // first internal cell of each cluster
   const int32_t* cell_perm;           // C, internal -> user cell id
   int32_t num_tiles;
 };
@@ -102,13 +104,14 @@ struct Mesh {
   DevBuf<int32_t> d_rowmap, d_cols;
   DevBuf<int32_t> d_cell_entry;  // C*16 CRS block index of (a,b) pairs
   int64_t num_clusters = 0, num_hex = 0;
-  DevBuf<int32_t> d_tile_cluster_start, d_tile_hex_count, d_tile_node_start, d_cluster_cell_start, d_cell_perm;
+  DevBuf<int32_t> d_tile_cluster_start, d_tile_cell_start, d_tile_hex_count, d_tile_node_start, d_cell_perm;
   DevBuf<uint32_t> d_tile_nodes;
   DevBuf<uint4> d_cluster_nodes;
   std::vector<int32_t> h_cell_perm;  // internal -> user
+  std::vector<uint32_t> h_tile_nodes; // flagged ids without mask bits
   TileView tiles() const {
-    return TileView{d_tile_cluster_start.get(), d_tile_hex_count.get(), d_tile_node_start.get(), d_tile_nodes.get(),
-                    d_cluster_nodes.get(), d_cluster_cell_start.get(), d_cell_perm.get(), int32_t(T)};
+    return TileView{d_tile_cluster_start.get(), d_tile_cell_start.get(), d_tile_hex_count.get(),
+                    d_tile_node_start.get(), d_tile_nodes.get(), d_cluster_nodes.get(), d_cell_perm.get(), int32_t(T)};
   }
   void build_graph_entries();
 };
@@ -156,9 +159,9 @@ void launch_gradient_z(const Problem& P, const double* u, const double* z, doubl
 void launch_energy(const Problem& P, const double* u, const double* z, double* cell_partials /*>=grid*/,
                    double* value_out /*device scalar or null*/, double* grad_u, double* grad_z, cudaStream_t s);
 void launch_cell_weights(const Problem& P, const double* z, double* w64, float* w32, cudaStream_t s);
+// y = K x with the tile kernel; constrained = mask the problem's Dirichlet dofs.
 template <typename T>
-void launch_apply_tiled(const Problem& P, const T* w, const T* x, T* y, const uint8_t* node_mask,
-                        cudaStream_t s);
+void launch_apply_tiled(const Problem& P, const T* w, const T* x, T* y, bool constrained, cudaStream_t s);
 void launch_diag(const Problem& P, const double* w, double* diag, cudaStream_t s);
 void launch_j2(const Problem& P, const pa_j2_params& jp, const double* u, const double* z, const double* prev,
                double* cur, cudaStream_t s);

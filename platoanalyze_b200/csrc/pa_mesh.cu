@@ -147,7 +147,7 @@ void build_tiles(Mesh& m) {
   }
   std::stable_sort(cl.begin(), cl.end(), [](const Cluster& a, const Cluster& b) { return a.key < b.key; });
 
-  std::vector<int32_t> tile_cluster_start{0}, tile_hex_count, tile_node_start{0}, cluster_cell_start, perm;
+  std::vector<int32_t> tile_cluster_start{0}, tile_cell_start{0}, tile_hex_count, tile_node_start{0}, perm;
   std::vector<uint32_t> tile_nodes;
   std::vector<uint4> cluster_nodes;
   perm.reserve(m.C);
@@ -164,7 +164,6 @@ void build_tiles(Mesh& m) {
     std::stable_partition(cur.begin(), cur.end(), [](const Cluster* k) { return k->hex; });
     int32_t nh = 0;
     for (const Cluster* k : cur) {
-      cluster_cell_start.push_back(int32_t(perm.size()));
       uint16_t ids[8];
       for (int n = 0; n < 8; ++n) ids[n] = k->nodes[n] >= 0 ? uint16_t(local[k->nodes[n]]) : uint16_t(0xffff);
       uint4 q;
@@ -188,6 +187,7 @@ void build_tiles(Mesh& m) {
     nhex_total += nh;
     tile_hex_count.push_back(nh);
     tile_cluster_start.push_back(int32_t(cluster_nodes.size()));
+    tile_cell_start.push_back(int32_t(perm.size()));
     tile_node_start.push_back(int32_t(tile_nodes.size()));
     cur_nodes.clear();
     cur.clear();
@@ -221,7 +221,9 @@ void build_tiles(Mesh& m) {
     for (int32_t t = 0; t < tile; ++t) {
       const int32_t nn = tile_node_start[t + 1] - tile_node_start[t];
       const int32_t nk = tile_cluster_start[t + 1] - tile_cluster_start[t];
-      if (nn > kTileNodes || nk > kTileClusters || tile_hex_count[t] > nk)
+      const int32_t nc = tile_cell_start[t + 1] - tile_cell_start[t];
+      if (nn > kTileNodes || nk > kTileClusters || tile_hex_count[t] > nk || nc > 6 * kTileClusters ||
+          nc != 6 * tile_hex_count[t] + (nk - tile_hex_count[t]))
         throw Error(PA_ERR_INVALID_ARG, "tile exceeds its shared-memory capacity");
       for (int32_t k = tile_cluster_start[t]; k < tile_cluster_start[t + 1]; ++k) {
         const uint4 q = cluster_nodes[k];
@@ -252,7 +254,8 @@ void build_tiles(Mesh& m) {
   m.d_tile_node_start.upload(tile_node_start.data(), tile_node_start.size());
   m.d_tile_nodes.upload(tile_nodes.data(), tile_nodes.size());
   m.d_cluster_nodes.upload(cluster_nodes.data(), cluster_nodes.size());
-  m.d_cluster_cell_start.upload(cluster_cell_start.data(), cluster_cell_start.size());
+  m.d_tile_cell_start.upload(tile_cell_start.data(), tile_cell_start.size());
+  m.h_tile_nodes = tile_nodes;
   m.d_cell_perm.upload(perm.data(), perm.size());
 }
 
@@ -308,7 +311,7 @@ void Mesh::build_graph_entries() {
 
 void mesh_build(Mesh& m) {
   PA_CHECK(m.C > 0 && m.N > 0, "mesh needs at least one cell and one node");
-  PA_CHECK(m.N < int64_t(kNodeMask), "too many nodes for 30-bit node ids");
+  PA_CHECK(m.N <= int64_t(kNodeIdMask), "too many nodes for 27-bit node ids");
   for (int64_t i = 0; i < 4 * m.C; ++i)
     PA_CHECK(m.cells[i] >= 0 && m.cells[i] < m.N, "cells2nodes entry out of range");
   for (int64_t i = 0; i < 3 * m.N; ++i) PA_CHECK(std::isfinite(m.coords[i]), "non-finite coordinate");

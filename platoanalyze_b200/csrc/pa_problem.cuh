@@ -37,6 +37,7 @@ struct Problem {
   DevBuf<int32_t> d_bc_dofs;
   DevBuf<double> d_bc_vals;
   DevBuf<uint8_t> d_node_mask;  // N, bit d = dof d constrained
+  DevBuf<uint32_t> d_tile_nodes_bc;  // the mesh's flagged tile node ids with the mask bits of these BCs
   // scratch for reductions / staging
   DevBuf<double> d_partials;
   DevBuf<double> d_scalar;

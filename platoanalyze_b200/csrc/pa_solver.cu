@@ -203,10 +203,8 @@ __global__ void k_dot2(int64_t n, const double* __restrict__ a, const double* __
 }
 
 template <typename T>
-int fused_apply_grid() {
-  int per_sm = 0;
-  PA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_apply_tiled<T, 1>, kApplyThreads, 0));
-  return std::max(1, per_sm) * num_sms();
+int fused_apply_grid(int num_tiles) {
+  return apply_kernel_setup<T, 1>(num_tiles);
 }
 
 template <typename T>
@@ -217,7 +215,7 @@ ApplyArgs<T> fused_args(Problem& P, const T* coords, const T* w, const T* p_old,
   a.tv = P.mesh->tiles();
   a.coords = coords;
   a.w = w;
-  a.node_mask = P.d_node_mask.get();
+  a.tile_nodes = P.d_tile_nodes_bc.get();
   Iso<double> i64 = P.ep.iso();
   a.iso = Iso<T>{T(i64.lam), T(i64.mu)};
   a.x = p_old;
@@ -268,14 +266,13 @@ struct CgGraph {
     SolverWorkspace& ws = P.ws;
     const int64_t n = P.ndof();
     const int vg = vec_grid(n);
-    int ag = fused_apply_grid<T>();
-    if (ag > P.mesh->T) ag = int(P.mesh->T);
+    const int ag = fused_apply_grid<T>(int(P.mesh->T));
     chunk = chunk_ + (chunk_ % 2);
     ApplyArgs<T> a_even = fused_args<T>(P, coords, w, pa, pb, ap, r, dinv);  // reads pa, writes pb
     ApplyArgs<T> a_odd = fused_args<T>(P, coords, w, pb, pa, ap, r, dinv);   // reads pb, writes pa
     PA_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < chunk; ++k) {
-      k_apply_tiled<T, 1><<<ag, kApplyThreads, 0, s>>>(k % 2 == 0 ? a_even : a_odd);
+      k_apply_tiled<T, 1><<<ag, kApplyThreads, tile_smem_bytes<T, 1>(), s>>>(k % 2 == 0 ? a_even : a_odd);
       const T* pnew = (k % 2 == 0) ? pb : pa;
       k_cg_update<T, X><<<vg, kVecThreads, 0, s>>>(n, x, r, pnew, ap, dinv, ws.sc.get(), ws.partials.get(),
                                                    ws.counters.get() + 1, nullptr);
@@ -337,7 +334,8 @@ pa_status solve_device(Problem& P, const double* z, const double* b, double* x_o
   const bool mixed = o.method == PA_SOLVER_PCG_MIXED;
   PA_CHECK(o.method == PA_SOLVER_PCG_FP64 || mixed, "unknown solver method");
   PA_CHECK(o.rel_tol > 0.0, "rel_tol must be positive");
-  const int grid_need = std::max(std::max(fused_apply_grid<double>(), fused_apply_grid<float>()), vec_grid(n));
+  const int grid_need = std::max(std::max(fused_apply_grid<double>(int(P.mesh->T)),
+                                          fused_apply_grid<float>(int(P.mesh->T))), vec_grid(n));
   P.ws.ensure(n, P.C(), grid_need, mixed);
   SolverWorkspace& ws = P.ws;
   const int max_iters = o.max_iters > 0 ? o.max_iters : int(20.0 * std::sqrt(double(n)) + 1000);
@@ -368,7 +366,7 @@ pa_status solve_device(Problem& P, const double* z, const double* b, double* x_o
     PA_CUDA(cudaMemsetAsync(ws.p0.get(), 0, sizeof(double) * n, s));
     k_scatter_bc<<<int((nbc + 255) / 256), 256, 0, s>>>(nbc, P.d_bc_dofs.get(), P.d_bc_vals.get(), 1.0, ws.p0.get());
     PA_LAUNCHED();
-    launch_apply_tiled<double>(P, ws.w64.get(), ws.p0.get(), ws.t.get(), nullptr, s);
+    launch_apply_tiled<double>(P, ws.w64.get(), ws.p0.get(), ws.t.get(), false, s);
     k_sub_masked<<<vg, kVecThreads, 0, s>>>(n, b, ws.t.get(), mask, bprime);
     launches += 3;
   } else {
@@ -386,7 +384,7 @@ pa_status solve_device(Problem& P, const double* z, const double* b, double* x_o
   PA_LAUNCHED();
   // FP64 true residual r = b' - K_masked x
   auto true_residual = [&]() {
-    launch_apply_tiled<double>(P, ws.w64.get(), ws.x.get(), ws.t.get(), mask, s);
+    launch_apply_tiled<double>(P, ws.w64.get(), ws.x.get(), ws.t.get(), true, s);
     k_sub_masked<<<vg, kVecThreads, 0, s>>>(n, bprime, ws.t.get(), mask, ws.r.get());
     PA_LAUNCHED();
     launches += 3;
@@ -483,7 +481,8 @@ pa_status solve_device(Problem& P, const double* z, const double* b, double* x_o
 double time_cg_apply(Problem& P, const double* z, bool fp32, int reps) {
   cudaStream_t s = P.stream;
   const int64_t n = P.ndof();
-  const int grid_need = std::max(std::max(fused_apply_grid<double>(), fused_apply_grid<float>()), vec_grid(n));
+  const int grid_need = std::max(std::max(fused_apply_grid<double>(int(P.mesh->T)),
+                                          fused_apply_grid<float>(int(P.mesh->T))), vec_grid(n));
   P.ws.ensure(n, P.C(), grid_need, true);
   SolverWorkspace& ws = P.ws;
   launch_cell_weights(P, z, ws.w64.get(), ws.w32.get(), s);
@@ -495,8 +494,7 @@ double time_cg_apply(Problem& P, const double* z, bool fp32, int reps) {
   init.beta = 0.5;
   init.rz = 1.0;
   PA_CUDA(cudaMemcpyAsync(ws.sc.get(), &init, sizeof(init), cudaMemcpyHostToDevice, s));
-  int ag = fp32 ? fused_apply_grid<float>() : fused_apply_grid<double>();
-  if (ag > P.mesh->T) ag = int(P.mesh->T);
+  const int ag = fp32 ? fused_apply_grid<float>(int(P.mesh->T)) : fused_apply_grid<double>(int(P.mesh->T));
   if (!P.ev0) { PA_CUDA(cudaEventCreate(&P.ev0)); PA_CUDA(cudaEventCreate(&P.ev1)); }
   float ms = 0.f;
   if (fp32) {
@@ -509,9 +507,10 @@ double time_cg_apply(Problem& P, const double* z, bool fp32, int reps) {
                                            ws.ap32.get(), ws.r32.get(), ws.dinv32.get());
     ApplyArgs<float> b = fused_args<float>(P, P.mesh->d_coords32.get(), ws.w32.get(), ws.p32b.get(), ws.p32a.get(),
                                            ws.ap32.get(), ws.r32.get(), ws.dinv32.get());
-    k_apply_tiled<float, 1><<<ag, kApplyThreads, 0, s>>>(a);  // warm
+    const size_t sm = tile_smem_bytes<float, 1>();
+    k_apply_tiled<float, 1><<<ag, kApplyThreads, sm, s>>>(a);  // warm
     PA_CUDA(cudaEventRecord(P.ev0, s));
-    for (int i = 0; i < reps; ++i) k_apply_tiled<float, 1><<<ag, kApplyThreads, 0, s>>>(i % 2 ? a : b);
+    for (int i = 0; i < reps; ++i) k_apply_tiled<float, 1><<<ag, kApplyThreads, sm, s>>>(i % 2 ? a : b);
     PA_CUDA(cudaEventRecord(P.ev1, s));
   } else {
     std::vector<double> ones(n, 1.0);
@@ -523,9 +522,10 @@ double time_cg_apply(Problem& P, const double* z, bool fp32, int reps) {
                                              ws.ap.get(), ws.r.get(), ws.dinv.get());
     ApplyArgs<double> b = fused_args<double>(P, P.mesh->d_coords.get(), ws.w64.get(), ws.p1.get(), ws.p0.get(),
                                              ws.ap.get(), ws.r.get(), ws.dinv.get());
-    k_apply_tiled<double, 1><<<ag, kApplyThreads, 0, s>>>(a);
+    const size_t sm = tile_smem_bytes<double, 1>();
+    k_apply_tiled<double, 1><<<ag, kApplyThreads, sm, s>>>(a);
     PA_CUDA(cudaEventRecord(P.ev0, s));
-    for (int i = 0; i < reps; ++i) k_apply_tiled<double, 1><<<ag, kApplyThreads, 0, s>>>(i % 2 ? a : b);
+    for (int i = 0; i < reps; ++i) k_apply_tiled<double, 1><<<ag, kApplyThreads, sm, s>>>(i % 2 ? a : b);
     PA_CUDA(cudaEventRecord(P.ev1, s));
   }
   PA_LAUNCHED();

@@ -1,5 +1,5 @@
-// pa_tiled.cuh -- tile-staged, hex-clustered matrix-free K.x: the hot kernel
-// of the solve.
+// pa_tiled.cuh -- tile-staged, hex-clustered, software-pipelined matrix-free
+// K.x: the hot kernel of the solve.
 //
 // Mesh layout (built once on the host, pa_mesh.cu):
 //  * cells are grouped into clusters: a "hex" cluster is six tets that form
@@ -8,23 +8,29 @@
 //    "single" cluster.  A hex cluster touches 8 nodes for 6 cells, a single
 //    one 4 nodes for 1 cell.
 //  * clusters are ordered along a Morton curve and packed into tiles of at
-//    most kTileClusters clusters touching at most kTileNodes nodes.
+//    most kTileClusters clusters touching at most kTileNodes nodes; a tile's
+//    cells are contiguous in the internal cell order.
 //
-// Kernel (a persistent grid, a multiple of the SM count, walks the tiles):
-//  1. stage the tile's nodes in shared memory (coordinates, input vector,
-//     Dirichlet mask) in one coalesced pass over the tile's sorted node list;
-//  2. one thread per cluster: read the cluster's nodes from shared memory
-//     into registers once, evaluate its tets (geometry, strain, stress, SIMP
-//     weight, divergence) and accumulate the node sums in registers -- a hex
-//     cluster reads 8 nodes and issues 24 shared-memory atomics for 6 tets,
-//     instead of 24 node reads and 72 atomics cell by cell;
-//  3. write each node sum once: a plain store for nodes only this tile
+// Kernel: a persistent grid (a multiple of the SM count) walks the tiles.  For
+// each tile the CTA
+//  1. has the tile's data already in shared memory: node coordinates and
+//     input vectors (gathered through the tile's sorted node list), cluster
+//     records and penalty weights -- all brought in by cp.async while the
+//     previous tile was computing (two buffers), so the gathers' latency is
+//     hidden behind arithmetic;
+//  2. forms the input vector (PCG mode: p = D^-1 r + beta p_old, masked; the
+//     owner tile writes p once);
+//  3. one thread per cluster: reads the cluster's nodes from shared memory into
+//     registers once, evaluates its tets (geometry, strain, stress, SIMP
+//     weight, divergence), accumulates node sums in registers and adds them to
+//     the tile's shared sums -- 24 shared atomics per 6 tets;
+//  4. writes each node sum once: a plain store for nodes only this tile
 //     touches, a global atomic add for nodes shared with other tiles.
-// The PCG variant (MODE 1) forms p = D^-1 r + beta p_old while staging (the
-// owner tile writes p once) and reduces p.Kp = sum_cells p_e^T K_e p_e from
-// the per-tet energies, so the search-direction update and the first dot
-// product need no extra pass over the vectors.
+// PCG mode also reduces p.Kp = sum_cells p_e^T K_e p_e from the per-tet
+// energies; the last CTA to finish turns it into alpha.
 #pragma once
+#include <algorithm>
+
 #include "pa_cell.cuh"
 
 namespace pa {
@@ -34,12 +40,12 @@ constexpr int kApplyThreads = kTileClusters;
 template <typename T>
 struct ApplyArgs {
   TileView tv;
-  const T* coords;          // N*3
-  const T* w;               // C, SIMP weight per cell, internal order
-  const uint8_t* node_mask; // N (bit d: dof d constrained) or null
+  const uint32_t* tile_nodes;  // flagged node ids (mask bits set for the problem's BCs, or none)
+  const T* coords;             // N*3
+  const T* w;                  // C, SIMP weight per cell, internal order
   Iso<T> iso;
-  const T* x;               // plain: input vector; pcg: p_old
-  T* y;                     // output, zero on entry
+  const T* x;                  // plain: input vector; pcg: p_old
+  T* y;                        // output, zero on entry
   // PCG fusion (mode 1)
   const T* r;
   const T* dinv;
@@ -83,8 +89,8 @@ __host__ __device__ constexpr int hex_slot(int j, int n) {
   return t[j][n];
 }
 
-// One tet: contributions r[4][3] for its nodes from xs (coords) and us (input);
-// returns the tet's energy sig:eps (for p.Kp).
+// One tet: node contributions r from coordinates xc and input u; returns the
+// tet's energy sig:eps (for p.Kp).
 template <typename T>
 __device__ __forceinline__ T tet_apply(const Iso<T>& iso, T w, const T (&xc)[4][3], const T (&u)[12], T (&r)[12]) {
   T g[4][3], vol, e[6], sig[6];
@@ -95,14 +101,84 @@ __device__ __forceinline__ T tet_apply(const Iso<T>& iso, T w, const T (&xc)[4][
   return voigt_dot(sig, e);
 }
 
+// ---------------------------------------------------------------- cp.async --
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  if (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Shared-memory layout of one CTA (dynamic shared memory).
+template <typename T, int MODE>
+struct TileSmem {
+  static constexpr int kRaw = MODE == 1 ? 12 : 6;  // per node: coords(3) + x(3) | r(3) dinv(3) p_old(3)
+  T raw[2][kRaw][kTileNodes];                      // gathered node data, two buffers
+  T x[3][kTileNodes];                              // input vector of the current tile
+  T y[3][kTileNodes];                              // node sums of the current tile
+  T w[2][6 * kTileClusters];                       // penalty weights of the tile's cells
+  uint4 rec[2][kTileClusters];                     // cluster node ids
+  uint32_t ids[2][kTileNodes];                     // flagged node ids
+  int32_t meta[2][8];                              // n0, nn, k0, nk, nhex, cell0, ncell
+  double red[32];
+};
+
+template <typename T, int MODE>
+constexpr size_t tile_smem_bytes() {
+  return sizeof(TileSmem<T, MODE>);
+}
+
+// Issue the loads of tile `tile`'s header and node ids (buffer b).
+template <typename T, int MODE>
+__device__ __forceinline__ void prefetch_ids(const ApplyArgs<T>& a, TileSmem<T, MODE>& S, int tile, int b) {
+  const int n0 = a.tv.tile_node_start[tile], nn = a.tv.tile_node_start[tile + 1] - n0;
+  const int k0 = a.tv.tile_cluster_start[tile], nk = a.tv.tile_cluster_start[tile + 1] - k0;
+  if (threadIdx.x == 0) {
+    const int c0 = a.tv.tile_cell_start[tile];
+    S.meta[b][0] = n0;
+    S.meta[b][1] = nn;
+    S.meta[b][2] = k0;
+    S.meta[b][3] = nk;
+    S.meta[b][4] = a.tv.tile_hex_count[tile];
+    S.meta[b][5] = c0;
+    S.meta[b][6] = a.tv.tile_cell_start[tile + 1] - c0;
+  }
+  for (int i = threadIdx.x; i < nn; i += blockDim.x) cp_async<4>(&S.ids[b][i], &a.tile_nodes[n0 + i]);
+  for (int i = threadIdx.x; i < nk; i += blockDim.x) cp_async<16>(&S.rec[b][i], &a.tv.cluster_nodes[k0 + i]);
+  cp_async_commit();
+}
+
+// Issue the gathers of the node data and weights of the tile whose ids sit in buffer b.
+template <typename T, int MODE>
+__device__ __forceinline__ void prefetch_data(const ApplyArgs<T>& a, TileSmem<T, MODE>& S, int b) {
+  const int nn = S.meta[b][1];
+  for (int i = threadIdx.x; i < nn; i += blockDim.x) {
+    const int64_t base = 3 * int64_t(S.ids[b][i] & kNodeIdMask);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      cp_async<sizeof(T)>(&S.raw[b][d][i], &a.coords[base + d]);
+      if (MODE == 0) {
+        cp_async<sizeof(T)>(&S.raw[b][3 + d][i], &a.x[base + d]);
+      } else {
+        cp_async<sizeof(T)>(&S.raw[b][3 + d][i], &a.r[base + d]);
+        cp_async<sizeof(T)>(&S.raw[b][6 + d][i], &a.dinv[base + d]);
+        cp_async<sizeof(T)>(&S.raw[b][9 + d][i], &a.x[base + d]);
+      }
+    }
+  }
+  const int c0 = S.meta[b][5], nc = S.meta[b][6];
+  for (int i = threadIdx.x; i < nc; i += blockDim.x) cp_async<sizeof(T)>(&S.w[b][i], &a.w[c0 + i]);
+  cp_async_commit();
+}
+
 template <typename T, int MODE>
 __global__ void __launch_bounds__(kApplyThreads, 1) k_apply_tiled(ApplyArgs<T> a) {
-  __shared__ T s_c[kTileNodes * 3];
-  __shared__ T s_x[kTileNodes * 3];
-  __shared__ T s_y[kTileNodes * 3];
-  __shared__ uint32_t s_node[kTileNodes];
-  __shared__ uint8_t s_mask[kTileNodes];
-  __shared__ double s_red[32];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  TileSmem<T, MODE>& S = *reinterpret_cast<TileSmem<T, MODE>*>(smem_raw);
 
   T beta = T(0);
   if (MODE == 1) {
@@ -110,50 +186,61 @@ __global__ void __launch_bounds__(kApplyThreads, 1) k_apply_tiled(ApplyArgs<T> a
     beta = T(a.sc->beta);
   }
   double pap = 0.0;
+  const int stride = gridDim.x;
+  int tile = blockIdx.x;
 
-  for (int tile = blockIdx.x; tile < a.tv.num_tiles; tile += gridDim.x) {
-    const int n0 = a.tv.tile_node_start[tile], nn = a.tv.tile_node_start[tile + 1] - n0;
-    const int k0 = a.tv.tile_cluster_start[tile], nk = a.tv.tile_cluster_start[tile + 1] - k0;
-    const int nhex = a.tv.tile_hex_count[tile];
-    // 1. stage nodes
+  // prologue: ids + data of the first tile, ids of the second
+  if (tile < a.tv.num_tiles) {
+    prefetch_ids(a, S, tile, 0);
+    cp_async_wait_all();
+    __syncthreads();
+    prefetch_data(a, S, 0);
+    if (tile + stride < a.tv.num_tiles) prefetch_ids(a, S, tile + stride, 1);
+  }
+
+  for (int k = 0; tile < a.tv.num_tiles; ++k, tile += stride) {
+    const int b = k & 1;
+    cp_async_wait_all();  // data of this tile, ids of the next
+    __syncthreads();
+    const bool has_next = tile + stride < a.tv.num_tiles;
+    if (has_next) prefetch_data(a, S, b ^ 1);
+
+    // 2. input vector of this tile; zero its sums
+    const int nn = S.meta[b][1];
     for (int i = threadIdx.x; i < nn; i += blockDim.x) {
-      const uint32_t f = a.tv.tile_nodes[n0 + i];
-      const int64_t gid = f & kNodeMask;
-      const uint8_t mk = a.node_mask ? a.node_mask[gid] : uint8_t(0);
-      s_node[i] = f;
-      s_mask[i] = mk;
+      const uint32_t f = S.ids[b][i];
+      const uint32_t mk = (f >> kMaskShift) & 7u;
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        const int64_t dof = 3 * gid + d;
-        s_c[3 * i + d] = a.coords[dof];
-        s_y[3 * i + d] = T(0);
         T v;
         if (MODE == 0) {
-          v = (mk >> d) & 1 ? T(0) : a.x[dof];
+          v = (mk >> d) & 1 ? T(0) : S.raw[b][3 + d][i];
         } else {
-          v = (mk >> d) & 1 ? T(0) : a.dinv[dof] * a.r[dof] + beta * a.x[dof];
-          if (f & kOwner) a.p_new[dof] = v;
+          v = (mk >> d) & 1 ? T(0) : S.raw[b][6 + d][i] * S.raw[b][3 + d][i] + beta * S.raw[b][9 + d][i];
+          if (f & kOwner) a.p_new[3 * int64_t(f & kNodeIdMask) + d] = v;
         }
-        s_x[3 * i + d] = v;
+        S.x[d][i] = v;
+        S.y[d][i] = T(0);
       }
     }
     __syncthreads();
-    // 2. one cluster per thread
+
+    // 3. one cluster per thread
     const int t = threadIdx.x;
+    const int nk = S.meta[b][3], nhex = S.meta[b][4];
     if (t < nk) {
-      const int k = k0 + t;
-      const uint4 q = a.tv.cluster_nodes[k];
-      const int c0 = a.tv.cluster_cell_start[k];
-      int ln[8] = {int(q.x & 0xffff), int(q.x >> 16), int(q.y & 0xffff), int(q.y >> 16),
-                   int(q.z & 0xffff), int(q.z >> 16), int(q.w & 0xffff), int(q.w >> 16)};
+      const uint4 q = S.rec[b][t];
+      const int ln[8] = {int(q.x & 0xffff), int(q.x >> 16), int(q.y & 0xffff), int(q.y >> 16),
+                         int(q.z & 0xffff), int(q.z >> 16), int(q.w & 0xffff), int(q.w >> 16)};
       if (t < nhex) {
+        const T* wv = &S.w[b][6 * t];
         T X[8][3], U[8][3], Y[8][3];
 #pragma unroll
         for (int s = 0; s < 8; ++s)
 #pragma unroll
           for (int d = 0; d < 3; ++d) {
-            X[s][d] = s_c[3 * ln[s] + d];
-            U[s][d] = s_x[3 * ln[s] + d];
+            X[s][d] = S.raw[b][d][ln[s]];
+            U[s][d] = S.x[d][ln[s]];
             Y[s][d] = T(0);
           }
 #pragma unroll
@@ -166,7 +253,7 @@ __global__ void __launch_bounds__(kApplyThreads, 1) k_apply_tiled(ApplyArgs<T> a
               xc[n][d] = X[hex_slot(j, n)][d];
               u[3 * n + d] = U[hex_slot(j, n)][d];
             }
-          const T en = tet_apply(a.iso, a.w[c0 + j], xc, u, r);
+          const T en = tet_apply(a.iso, wv[j], xc, u, r);
           if (MODE == 1) pap += double(en);
 #pragma unroll
           for (int n = 0; n < 4; ++n)
@@ -176,34 +263,36 @@ __global__ void __launch_bounds__(kApplyThreads, 1) k_apply_tiled(ApplyArgs<T> a
 #pragma unroll
         for (int s = 0; s < 8; ++s)
 #pragma unroll
-          for (int d = 0; d < 3; ++d) atomicAdd(&s_y[3 * ln[s] + d], Y[s][d]);
+          for (int d = 0; d < 3; ++d) atomicAdd(&S.y[d][ln[s]], Y[s][d]);
       } else {
+        // single tets follow the hexes: cell index = 6 * nhex + (t - nhex)
         T xc[4][3], u[12], r[12];
 #pragma unroll
         for (int n = 0; n < 4; ++n)
 #pragma unroll
           for (int d = 0; d < 3; ++d) {
-            xc[n][d] = s_c[3 * ln[n] + d];
-            u[3 * n + d] = s_x[3 * ln[n] + d];
+            xc[n][d] = S.raw[b][d][ln[n]];
+            u[3 * n + d] = S.x[d][ln[n]];
           }
-        const T en = tet_apply(a.iso, a.w[c0], xc, u, r);
+        const T en = tet_apply(a.iso, S.w[b][6 * nhex + (t - nhex)], xc, u, r);
         if (MODE == 1) pap += double(en);
 #pragma unroll
         for (int n = 0; n < 4; ++n)
 #pragma unroll
-          for (int d = 0; d < 3; ++d) atomicAdd(&s_y[3 * ln[n] + d], r[3 * n + d]);
+          for (int d = 0; d < 3; ++d) atomicAdd(&S.y[d][ln[n]], r[3 * n + d]);
       }
     }
     __syncthreads();
-    // 3. write node sums
+
+    // 4. write node sums
     for (int i = threadIdx.x; i < nn; i += blockDim.x) {
-      const uint32_t f = s_node[i];
-      const int64_t gid = f & kNodeMask;
-      const uint8_t mk = s_mask[i];
+      const uint32_t f = S.ids[b][i];
+      const int64_t gid = f & kNodeIdMask;
+      const uint32_t mk = (f >> kMaskShift) & 7u;
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         if ((mk >> d) & 1) continue;
-        const T v = s_y[3 * i + d];
+        const T v = S.y[d][i];
         if (f & kShared)
           atomicAdd(&a.y[3 * gid + d], v);
         else
@@ -211,15 +300,18 @@ __global__ void __launch_bounds__(kApplyThreads, 1) k_apply_tiled(ApplyArgs<T> a
       }
     }
     __syncthreads();
+    // ids of the tile after next into this buffer
+    if (tile + 2 * stride < a.tv.num_tiles) prefetch_ids(a, S, tile + 2 * stride, b);
   }
+  cp_async_wait_all();
 
   if (MODE == 1) {
-    const double bsum = block_sum(pap, s_red);
+    const double bsum = block_sum(pap, S.red);
     if (threadIdx.x == 0) a.partials[blockIdx.x] = bsum;
     if (last_block_arrive(a.counter)) {
       double v = 0.0;
       for (int i = threadIdx.x; i < gridDim.x; i += blockDim.x) v += __ldcg(&a.partials[i]);
-      v = block_sum(v, s_red);
+      v = block_sum(v, S.red);
       if (threadIdx.x == 0) {
         PcgScalars* sc = a.sc;
         sc->pap = v;
@@ -234,6 +326,19 @@ __global__ void __launch_bounds__(kApplyThreads, 1) k_apply_tiled(ApplyArgs<T> a
       }
     }
   }
+}
+
+// Configure dynamic shared memory once per kernel instance; returns the
+// persistent grid size (resident CTAs per SM x SMs, capped by the tile count).
+template <typename T, int MODE>
+int apply_kernel_setup(int num_tiles) {
+  const size_t smem = tile_smem_bytes<T, MODE>();
+  PA_CUDA(cudaFuncSetAttribute(k_apply_tiled<T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  int blocks = 0;
+  PA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_apply_tiled<T, MODE>, kApplyThreads, smem));
+  int grid = std::max(1, blocks) * num_sms();
+  if (grid > num_tiles) grid = num_tiles;
+  return std::max(grid, 1);
 }
 
 }  // namespace pa
