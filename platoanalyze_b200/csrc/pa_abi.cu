@@ -472,25 +472,29 @@ pa_status pa_apply(pa_problem* problem, const double* z, const void* x, void* y,
     P.ws.w64.resize(P.C());
     if (precision == PA_FP32) P.ws.w32.resize(P.C());
     pa::launch_cell_weights(P, dz, P.ws.w64.get(), precision == PA_FP32 ? P.ws.w32.get() : nullptr, P.stream);
+    const int64_t nbc = constrained ? int64_t(P.bc_dofs.size()) : 0;
     if (precision == PA_FP64) {
       const double* dx = st.in(static_cast<const double*>(x), n, "x");
       double* dy = st.out(static_cast<double*>(y), n, "y");
-      pa::launch_apply_tiled<double>(P, P.ws.w64.get(), dx, dy, constrained != 0, P.stream);
-      if (constrained && !P.bc_dofs.empty()) {
-        // identity rows on constrained dofs
-        std::vector<int32_t>& d = P.bc_dofs;
-        for (size_t i = 0; i < d.size(); ++i)
-          PA_CUDA(cudaMemcpyAsync(dy + d[i], dx + d[i], sizeof(double), cudaMemcpyDeviceToDevice, P.stream));
-      }
+      pa::DevBuf<double>& xs = P.ws.x;
+      pa::DevBuf<double>& ys = P.ws.t;
+      if (xs.n < size_t(n)) xs.resize(n);
+      if (ys.n < size_t(n)) ys.resize(n);
+      pa::launch_aos_to_soa<double, double>(dx, xs.get(), P.N(), P.stream);
+      pa::launch_apply_tiled<double>(P, P.ws.w64.get(), xs.get(), ys.get(), constrained != 0, P.stream);
+      pa::launch_soa_to_aos<double, double>(ys.get(), dy, P.N(), P.stream);
+      pa::launch_copy_dofs<double>(P.d_bc_dofs.get(), nbc, dx, dy, P.stream);  // identity rows
     } else {
       const float* dx = st.in(static_cast<const float*>(x), n, "x");
       float* dy = st.out(static_cast<float*>(y), n, "y");
-      pa::launch_apply_tiled<float>(P, P.ws.w32.get(), dx, dy, constrained != 0, P.stream);
-      if (constrained && !P.bc_dofs.empty()) {
-        std::vector<int32_t>& d = P.bc_dofs;
-        for (size_t i = 0; i < d.size(); ++i)
-          PA_CUDA(cudaMemcpyAsync(dy + d[i], dx + d[i], sizeof(float), cudaMemcpyDeviceToDevice, P.stream));
-      }
+      pa::DevBuf<float>& xs = P.ws.r32;
+      pa::DevBuf<float>& ys = P.ws.ap32;
+      if (xs.n < size_t(n)) xs.resize(n);
+      if (ys.n < size_t(n)) ys.resize(n);
+      pa::launch_aos_to_soa<float, float>(dx, xs.get(), P.N(), P.stream);
+      pa::launch_apply_tiled<float>(P, P.ws.w32.get(), xs.get(), ys.get(), constrained != 0, P.stream);
+      pa::launch_soa_to_aos<float, float>(ys.get(), dy, P.N(), P.stream);
+      pa::launch_copy_dofs<float>(P.d_bc_dofs.get(), nbc, dx, dy, P.stream);
     }
     st.finish();
   });

@@ -382,8 +382,9 @@ void launch_apply_tiled(const Problem& P, const T* w, const T* x, T* y, bool con
   ApplyArgs<T> a{};
   a.tv = P.mesh->tiles();
   a.tile_nodes = constrained ? P.d_tile_nodes_bc.get() : P.mesh->d_tile_nodes.get();
-  a.coords = std::is_same<T, double>::value ? reinterpret_cast<const T*>(P.mesh->d_coords.get())
-                                            : reinterpret_cast<const T*>(P.mesh->d_coords32.get());
+  a.N = P.N();
+  a.coords = std::is_same<T, double>::value ? reinterpret_cast<const T*>(P.mesh->d_coords_soa.get())
+                                            : reinterpret_cast<const T*>(P.mesh->d_coords32_soa.get());
   a.w = w;
   Iso<double> i64 = P.ep.iso();
   a.iso = Iso<T>{T(i64.lam), T(i64.mu)};
@@ -394,6 +395,49 @@ void launch_apply_tiled(const Problem& P, const T* w, const T* x, T* y, bool con
   k_apply_tiled<T, 0><<<grid, kApplyThreads, tile_smem_bytes<T, 0>(), s>>>(a);
   PA_LAUNCHED();
 }
+
+template <typename S, typename T>
+__global__ void k_aos_to_soa(const S* __restrict__ aos, T* __restrict__ soa, int64_t N) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < 3 * N; i += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t v = i / 3, d = i - 3 * v;
+    soa[d * N + v] = T(aos[i]);
+  }
+}
+template <typename T, typename S>
+__global__ void k_soa_to_aos(const T* __restrict__ soa, S* __restrict__ aos, int64_t N) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < 3 * N; i += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t v = i / 3, d = i - 3 * v;
+    aos[i] = S(soa[d * N + v]);
+  }
+}
+template <typename T>
+__global__ void k_copy_dofs(const int32_t* __restrict__ dofs, int64_t n, const T* __restrict__ src, T* __restrict__ dst) {
+  const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i < n) dst[dofs[i]] = src[dofs[i]];
+}
+
+template <typename S, typename T>
+void launch_aos_to_soa(const S* aos, T* soa, int64_t N, cudaStream_t s) {
+  k_aos_to_soa<S, T><<<grid_for(std::min<int64_t>(3 * N, 148LL * 8 * kThreads)), kThreads, 0, s>>>(aos, soa, N);
+  PA_LAUNCHED();
+}
+template <typename T, typename S>
+void launch_soa_to_aos(const T* soa, S* aos, int64_t N, cudaStream_t s) {
+  k_soa_to_aos<T, S><<<grid_for(std::min<int64_t>(3 * N, 148LL * 8 * kThreads)), kThreads, 0, s>>>(soa, aos, N);
+  PA_LAUNCHED();
+}
+template <typename T>
+void launch_copy_dofs(const int32_t* dofs, int64_t n, const T* src, T* dst, cudaStream_t s) {
+  if (!n) return;
+  k_copy_dofs<T><<<grid_for(n), kThreads, 0, s>>>(dofs, n, src, dst);
+  PA_LAUNCHED();
+}
+template void launch_aos_to_soa<double, double>(const double*, double*, int64_t, cudaStream_t);
+template void launch_aos_to_soa<float, float>(const float*, float*, int64_t, cudaStream_t);
+template void launch_soa_to_aos<double, double>(const double*, double*, int64_t, cudaStream_t);
+template void launch_soa_to_aos<float, float>(const float*, float*, int64_t, cudaStream_t);
+template void launch_copy_dofs<double>(const int32_t*, int64_t, const double*, double*, cudaStream_t);
+template void launch_copy_dofs<float>(const int32_t*, int64_t, const float*, float*, cudaStream_t);
 
 template void launch_apply_tiled<double>(const Problem&, const double*, const double*, double*, bool, cudaStream_t);
 template void launch_apply_tiled<float>(const Problem&, const float*, const float*, float*, bool, cudaStream_t);

@@ -99,8 +99,9 @@ struct Mesh {
   std::vector<int32_t> rowmap;   // N+1
   std::vector<int32_t> cols;     // B
   DevBuf<int32_t> d_cells;
-  DevBuf<double> d_coords;
-  DevBuf<float> d_coords32;
+  DevBuf<double> d_coords;           // N*3 interleaved (cell kernels)
+  DevBuf<double> d_coords_soa;       // 3N component-major (tile kernel, FP64)
+  DevBuf<float> d_coords32_soa;      // 3N component-major (tile kernel, FP32)
   DevBuf<int32_t> d_rowmap, d_cols;
   DevBuf<int32_t> d_cell_entry;  // C*16 CRS block index of (a,b) pairs
   int64_t num_clusters = 0, num_hex = 0;
@@ -159,9 +160,17 @@ void launch_gradient_z(const Problem& P, const double* u, const double* z, doubl
 void launch_energy(const Problem& P, const double* u, const double* z, double* cell_partials /*>=grid*/,
                    double* value_out /*device scalar or null*/, double* grad_u, double* grad_z, cudaStream_t s);
 void launch_cell_weights(const Problem& P, const double* z, double* w64, float* w32, cudaStream_t s);
-// y = K x with the tile kernel; constrained = mask the problem's Dirichlet dofs.
+// y = K x with the tile kernel on component-major (SoA) vectors;
+// constrained = mask the problem's Dirichlet dofs.
 template <typename T>
 void launch_apply_tiled(const Problem& P, const T* w, const T* x, T* y, bool constrained, cudaStream_t s);
+// interleaved (AoS, the ABI's layout) <-> component-major (SoA) copies
+template <typename S, typename T>
+void launch_aos_to_soa(const S* aos, T* soa, int64_t N, cudaStream_t s);
+template <typename T, typename S>
+void launch_soa_to_aos(const T* soa, S* aos, int64_t N, cudaStream_t s);
+template <typename T>
+void launch_copy_dofs(const int32_t* dofs, int64_t n, const T* src, T* dst, cudaStream_t s);
 void launch_diag(const Problem& P, const double* w, double* diag, cudaStream_t s);
 void launch_j2(const Problem& P, const pa_j2_params& jp, const double* u, const double* z, const double* prev,
                double* cur, cudaStream_t s);

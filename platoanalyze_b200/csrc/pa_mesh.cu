@@ -320,8 +320,15 @@ void mesh_build(Mesh& m) {
   build_tiles(m);
   m.d_cells.upload(m.cells.data(), m.cells.size());
   m.d_coords.upload(m.coords.data(), m.coords.size());
-  std::vector<float> c32(m.coords.begin(), m.coords.end());
-  m.d_coords32.upload(c32.data(), c32.size());
+  std::vector<double> soa(3 * m.N);
+  std::vector<float> soa32(3 * m.N);
+  for (int64_t v = 0; v < m.N; ++v)
+    for (int d = 0; d < 3; ++d) {
+      soa[d * m.N + v] = m.coords[3 * v + d];
+      soa32[d * m.N + v] = float(m.coords[3 * v + d]);
+    }
+  m.d_coords_soa.upload(soa.data(), soa.size());
+  m.d_coords32_soa.upload(soa32.data(), soa32.size());
   PA_CUDA(cudaDeviceSynchronize());
 }
 

@@ -145,22 +145,39 @@ __global__ void __launch_bounds__(kVecThreads) k_cg_init(int64_t n, const T* __r
   }
 }
 
-// out = (a - b) masked to free dofs (mask bit set -> 0), FP64.
-__global__ void k_sub_masked(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
-                             const uint8_t* __restrict__ mask, double* __restrict__ out) {
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-    const bool c = mask && ((mask[i / 3] >> (i % 3)) & 1);
-    out[i] = c ? 0.0 : a[i] - (b ? b[i] : 0.0);
+// Vectors inside the solver are component-major (SoA, v[d * N + node]); the
+// ABI's vectors are interleaved (AoS, v[3 * node + d]).  mask[node] bit d
+// marks a constrained dof.
+
+// out_soa = mask ? 0 : a_aos - t_soa   (t may be null)
+__global__ void k_aos_minus_soa(int64_t N, const double* __restrict__ a, const double* __restrict__ t,
+                                const uint8_t* __restrict__ mask, double* __restrict__ out) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < 3 * N; i += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t d = i / N, v = i - d * N;
+    const bool c = mask && ((mask[v] >> d) & 1);
+    out[i] = c ? 0.0 : a[3 * v + d] - (t ? t[i] : 0.0);
   }
 }
 
-// D^-1 with constrained (and zero) diagonal entries mapped to 0.
+// out = mask ? 0 : a - b   (all SoA)
+__global__ void k_sub_masked(int64_t N, const double* __restrict__ a, const double* __restrict__ b,
+                             const uint8_t* __restrict__ mask, double* __restrict__ out) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < 3 * N; i += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t d = i / N, v = i - d * N;
+    const bool c = mask && ((mask[v] >> d) & 1);
+    out[i] = c ? 0.0 : a[i] - b[i];
+  }
+}
+
+// D^-1 (SoA) from the interleaved diagonal; constrained and zero entries -> 0.
 template <typename T>
-__global__ void k_inv_diag(int64_t n, const double* __restrict__ diag, const uint8_t* __restrict__ mask,
+__global__ void k_inv_diag(int64_t N, const double* __restrict__ diag_aos, const uint8_t* __restrict__ mask,
                            T* __restrict__ dinv) {
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-    const bool c = mask && ((mask[i / 3] >> (i % 3)) & 1);
-    dinv[i] = (c || diag[i] == 0.0) ? T(0) : T(1.0 / diag[i]);
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < 3 * N; i += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t d = i / N, v = i - d * N;
+    const bool c = mask && ((mask[v] >> d) & 1);
+    const double g = diag_aos[3 * v + d];
+    dinv[i] = (c || g == 0.0) ? T(0) : T(1.0 / g);
   }
 }
 
@@ -177,11 +194,11 @@ __global__ void k_fold(int64_t n, double* __restrict__ x, float* __restrict__ dx
   }
 }
 
-// Dirichlet lift vector: xd[dof] = scale * value for each BC, 0 elsewhere.
+// Dirichlet lift vector (SoA): xd[d * N + node] = scale * value for each BC dof.
 __global__ void k_scatter_bc(int64_t nbc, const int32_t* __restrict__ dofs, const double* __restrict__ vals,
-                             double scale, double* __restrict__ xd) {
+                             double scale, int64_t N, double* __restrict__ xd) {
   const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  if (i < nbc) xd[dofs[i]] = scale * vals[i];
+  if (i < nbc) xd[(dofs[i] % 3) * N + dofs[i] / 3] = scale * vals[i];
 }
 
 // x[dof] = scale * value (final solution on constrained dofs).
@@ -213,6 +230,7 @@ ApplyArgs<T> fused_args(Problem& P, const T* coords, const T* w, const T* p_old,
   SolverWorkspace& ws = P.ws;
   ApplyArgs<T> a{};
   a.tv = P.mesh->tiles();
+  a.N = P.N();
   a.coords = coords;
   a.w = w;
   a.tile_nodes = P.d_tile_nodes_bc.get();
@@ -350,13 +368,14 @@ pa_status solve_device(Problem& P, const double* z, const double* b, double* x_o
   PA_CUDA(cudaEventRecord(P.ev0, s));
 
   // SIMP weights in tile order; Jacobi diagonal and its masked inverse.
+  const int64_t N = P.N();
   launch_cell_weights(P, z, ws.w64.get(), mixed ? ws.w32.get() : nullptr, s);
   launch_diag(P, ws.w64.get(), ws.t.get(), s);
-  k_inv_diag<double><<<vg, kVecThreads, 0, s>>>(n, ws.t.get(), mask, ws.dinv.get());
+  k_inv_diag<double><<<vg, kVecThreads, 0, s>>>(N, ws.t.get(), mask, ws.dinv.get());
   PA_LAUNCHED();
   launches += 3;
   if (mixed) {
-    k_inv_diag<float><<<vg, kVecThreads, 0, s>>>(n, ws.t.get(), mask, ws.dinv32.get());
+    k_inv_diag<float><<<vg, kVecThreads, 0, s>>>(N, ws.t.get(), mask, ws.dinv32.get());
     PA_LAUNCHED();
     launches += 1;
   }
@@ -364,19 +383,20 @@ pa_status solve_device(Problem& P, const double* z, const double* b, double* x_o
   double* bprime = ws.b.get();
   if (nbc) {
     PA_CUDA(cudaMemsetAsync(ws.p0.get(), 0, sizeof(double) * n, s));
-    k_scatter_bc<<<int((nbc + 255) / 256), 256, 0, s>>>(nbc, P.d_bc_dofs.get(), P.d_bc_vals.get(), 1.0, ws.p0.get());
+    k_scatter_bc<<<int((nbc + 255) / 256), 256, 0, s>>>(nbc, P.d_bc_dofs.get(), P.d_bc_vals.get(), 1.0, N,
+                                                        ws.p0.get());
     PA_LAUNCHED();
     launch_apply_tiled<double>(P, ws.w64.get(), ws.p0.get(), ws.t.get(), false, s);
-    k_sub_masked<<<vg, kVecThreads, 0, s>>>(n, b, ws.t.get(), mask, bprime);
+    k_aos_minus_soa<<<vg, kVecThreads, 0, s>>>(N, b, ws.t.get(), mask, bprime);
     launches += 3;
   } else {
-    k_sub_masked<<<vg, kVecThreads, 0, s>>>(n, b, nullptr, nullptr, bprime);
+    k_aos_minus_soa<<<vg, kVecThreads, 0, s>>>(N, b, nullptr, nullptr, bprime);
     launches += 1;
   }
   PA_LAUNCHED();
   // initial free-dof iterate
   if (o.use_initial_guess) {
-    k_sub_masked<<<vg, kVecThreads, 0, s>>>(n, x_out, nullptr, mask, ws.x.get());
+    k_aos_minus_soa<<<vg, kVecThreads, 0, s>>>(N, x_out, nullptr, mask, ws.x.get());
     launches += 1;
   } else {
     PA_CUDA(cudaMemsetAsync(ws.x.get(), 0, sizeof(double) * n, s));
@@ -385,7 +405,7 @@ pa_status solve_device(Problem& P, const double* z, const double* b, double* x_o
   // FP64 true residual r = b' - K_masked x
   auto true_residual = [&]() {
     launch_apply_tiled<double>(P, ws.w64.get(), ws.x.get(), ws.t.get(), true, s);
-    k_sub_masked<<<vg, kVecThreads, 0, s>>>(n, bprime, ws.t.get(), mask, ws.r.get());
+    k_sub_masked<<<vg, kVecThreads, 0, s>>>(N, bprime, ws.t.get(), mask, ws.r.get());
     PA_LAUNCHED();
     launches += 3;
     return host_norm2(P, ws.r.get());
@@ -408,10 +428,10 @@ pa_status solve_device(Problem& P, const double* z, const double* b, double* x_o
   CgGraph<double, double> g64;
   CgGraph<float, float> g32;
   if (mixed)
-    g32.capture(P, P.mesh->d_coords32.get(), ws.w32.get(), ws.p32a.get(), ws.p32b.get(), ws.ap32.get(), ws.r32.get(),
+    g32.capture(P, P.mesh->d_coords32_soa.get(), ws.w32.get(), ws.p32a.get(), ws.p32b.get(), ws.ap32.get(), ws.r32.get(),
                 ws.dinv32.get(), ws.dx32.get(), chunk);
   else
-    g64.capture(P, P.mesh->d_coords.get(), ws.w64.get(), ws.p0.get(), ws.p1.get(), ws.ap.get(), ws.r.get(),
+    g64.capture(P, P.mesh->d_coords_soa.get(), ws.w64.get(), ws.p0.get(), ws.p1.get(), ws.ap.get(), ws.r.get(),
                 ws.dinv.get(), ws.x.get(), chunk);
 
   // Recursive-residual stop hint, confirmed on the FP64 true residual.
@@ -452,8 +472,9 @@ pa_status solve_device(Problem& P, const double* z, const double* b, double* x_o
   }
   const double relres = std::sqrt(rr_true / bb);
 
-  // x_out = x_f + x_D
-  PA_CUDA(cudaMemcpyAsync(x_out, ws.x.get(), sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  // x_out = x_f + x_D (back to the interleaved layout)
+  launch_soa_to_aos<double, double>(ws.x.get(), x_out, N, s);
+  launches += 1;
   if (nbc) {
     k_set_bc<<<int((nbc + 255) / 256), 256, 0, s>>>(nbc, P.d_bc_dofs.get(), P.d_bc_vals.get(), 1.0, x_out);
     PA_LAUNCHED();
@@ -487,8 +508,8 @@ double time_cg_apply(Problem& P, const double* z, bool fp32, int reps) {
   SolverWorkspace& ws = P.ws;
   launch_cell_weights(P, z, ws.w64.get(), ws.w32.get(), s);
   launch_diag(P, ws.w64.get(), ws.t.get(), s);
-  k_inv_diag<double><<<vec_grid(n), kVecThreads, 0, s>>>(n, ws.t.get(), P.d_node_mask.get(), ws.dinv.get());
-  k_inv_diag<float><<<vec_grid(n), kVecThreads, 0, s>>>(n, ws.t.get(), P.d_node_mask.get(), ws.dinv32.get());
+  k_inv_diag<double><<<vec_grid(n), kVecThreads, 0, s>>>(P.N(), ws.t.get(), P.d_node_mask.get(), ws.dinv.get());
+  k_inv_diag<float><<<vec_grid(n), kVecThreads, 0, s>>>(P.N(), ws.t.get(), P.d_node_mask.get(), ws.dinv32.get());
   PA_LAUNCHED();
   PcgScalars init{};
   init.beta = 0.5;
@@ -503,9 +524,9 @@ double time_cg_apply(Problem& P, const double* z, bool fp32, int reps) {
     PA_CUDA(cudaMemsetAsync(ws.p32a.get(), 0, sizeof(float) * n, s));
     PA_CUDA(cudaMemsetAsync(ws.p32b.get(), 0, sizeof(float) * n, s));
     PA_CUDA(cudaMemsetAsync(ws.ap32.get(), 0, sizeof(float) * n, s));
-    ApplyArgs<float> a = fused_args<float>(P, P.mesh->d_coords32.get(), ws.w32.get(), ws.p32a.get(), ws.p32b.get(),
+    ApplyArgs<float> a = fused_args<float>(P, P.mesh->d_coords32_soa.get(), ws.w32.get(), ws.p32a.get(), ws.p32b.get(),
                                            ws.ap32.get(), ws.r32.get(), ws.dinv32.get());
-    ApplyArgs<float> b = fused_args<float>(P, P.mesh->d_coords32.get(), ws.w32.get(), ws.p32b.get(), ws.p32a.get(),
+    ApplyArgs<float> b = fused_args<float>(P, P.mesh->d_coords32_soa.get(), ws.w32.get(), ws.p32b.get(), ws.p32a.get(),
                                            ws.ap32.get(), ws.r32.get(), ws.dinv32.get());
     const size_t sm = tile_smem_bytes<float, 1>();
     k_apply_tiled<float, 1><<<ag, kApplyThreads, sm, s>>>(a);  // warm
@@ -518,9 +539,9 @@ double time_cg_apply(Problem& P, const double* z, bool fp32, int reps) {
     PA_CUDA(cudaMemsetAsync(ws.p0.get(), 0, sizeof(double) * n, s));
     PA_CUDA(cudaMemsetAsync(ws.p1.get(), 0, sizeof(double) * n, s));
     PA_CUDA(cudaMemsetAsync(ws.ap.get(), 0, sizeof(double) * n, s));
-    ApplyArgs<double> a = fused_args<double>(P, P.mesh->d_coords.get(), ws.w64.get(), ws.p0.get(), ws.p1.get(),
+    ApplyArgs<double> a = fused_args<double>(P, P.mesh->d_coords_soa.get(), ws.w64.get(), ws.p0.get(), ws.p1.get(),
                                              ws.ap.get(), ws.r.get(), ws.dinv.get());
-    ApplyArgs<double> b = fused_args<double>(P, P.mesh->d_coords.get(), ws.w64.get(), ws.p1.get(), ws.p0.get(),
+    ApplyArgs<double> b = fused_args<double>(P, P.mesh->d_coords_soa.get(), ws.w64.get(), ws.p1.get(), ws.p0.get(),
                                              ws.ap.get(), ws.r.get(), ws.dinv.get());
     const size_t sm = tile_smem_bytes<double, 1>();
     k_apply_tiled<double, 1><<<ag, kApplyThreads, sm, s>>>(a);

@@ -37,11 +37,13 @@ namespace pa {
 
 constexpr int kApplyThreads = kTileClusters;
 
+// Vectors are stored component-major (SoA): v[d * N + node].
 template <typename T>
 struct ApplyArgs {
   TileView tv;
   const uint32_t* tile_nodes;  // flagged node ids (mask bits set for the problem's BCs, or none)
-  const T* coords;             // N*3
+  int64_t N;                   // nodes (SoA stride)
+  const T* coords;             // 3N, SoA
   const T* w;                  // C, SIMP weight per cell, internal order
   Iso<T> iso;
   const T* x;                  // plain: input vector; pcg: p_old
@@ -113,17 +115,30 @@ __device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// Packed node records in shared memory: coordinates + first input
+// component in one 16-byte (FP32) / two 16-byte (FP64) loads, the other two
+// input components in one 8- / 16-byte load.
+template <typename T>
+struct alignas(16) Node4 {
+  T x, y, z, u0;
+};
+template <typename T>
+struct alignas(2 * sizeof(T)) Node2 {
+  T u1, u2;
+};
+
 // Shared-memory layout of one CTA (dynamic shared memory).
 template <typename T, int MODE>
 struct TileSmem {
-  static constexpr int kRaw = MODE == 1 ? 12 : 6;  // per node: coords(3) + x(3) | r(3) dinv(3) p_old(3)
-  T raw[2][kRaw][kTileNodes];                      // gathered node data, two buffers
-  T x[3][kTileNodes];                              // input vector of the current tile
-  T y[3][kTileNodes];                              // node sums of the current tile
-  T w[2][6 * kTileClusters];                       // penalty weights of the tile's cells
-  uint4 rec[2][kTileClusters];                     // cluster node ids
-  uint32_t ids[2][kTileNodes];                     // flagged node ids
-  int32_t meta[2][8];                              // n0, nn, k0, nk, nhex, cell0, ncell
+  static constexpr int kRawBufs = MODE == 1 ? 2 : 1;
+  Node4<T> xc[2][kTileNodes];             // coordinates + input (component 0), two buffers
+  Node2<T> uu[2][kTileNodes];             // input components 1, 2
+  T raw[kRawBufs][9][kTileNodes];         // PCG: r, D^-1, p_old gathered for the tile
+  T y[3][kTileNodes];                     // node sums of the current tile
+  T w[2][6 * kTileClusters];              // penalty weights of the tile's cells
+  uint4 rec[2][kTileClusters];            // cluster node ids
+  uint32_t ids[2][kTileNodes];            // flagged node ids
+  int32_t meta[2][8];                     // n0, nn, k0, nk, nhex, cell0, ncell
   double red[32];
 };
 
@@ -132,7 +147,7 @@ constexpr size_t tile_smem_bytes() {
   return sizeof(TileSmem<T, MODE>);
 }
 
-// Issue the loads of tile `tile`'s header and node ids (buffer b).
+// Issue the loads of tile `tile`'s header, node ids and cluster records (buffer b).
 template <typename T, int MODE>
 __device__ __forceinline__ void prefetch_ids(const ApplyArgs<T>& a, TileSmem<T, MODE>& S, int tile, int b) {
   const int n0 = a.tv.tile_node_start[tile], nn = a.tv.tile_node_start[tile + 1] - n0;
@@ -156,17 +171,22 @@ __device__ __forceinline__ void prefetch_ids(const ApplyArgs<T>& a, TileSmem<T, 
 template <typename T, int MODE>
 __device__ __forceinline__ void prefetch_data(const ApplyArgs<T>& a, TileSmem<T, MODE>& S, int b) {
   const int nn = S.meta[b][1];
+  const int64_t N = a.N;
   for (int i = threadIdx.x; i < nn; i += blockDim.x) {
-    const int64_t base = 3 * int64_t(S.ids[b][i] & kNodeIdMask);
+    const int64_t g = int64_t(S.ids[b][i] & kNodeIdMask);
+    cp_async<sizeof(T)>(&S.xc[b][i].x, &a.coords[g]);
+    cp_async<sizeof(T)>(&S.xc[b][i].y, &a.coords[N + g]);
+    cp_async<sizeof(T)>(&S.xc[b][i].z, &a.coords[2 * N + g]);
+    if constexpr (MODE == 0) {
+      cp_async<sizeof(T)>(&S.xc[b][i].u0, &a.x[g]);
+      cp_async<sizeof(T)>(&S.uu[b][i].u1, &a.x[N + g]);
+      cp_async<sizeof(T)>(&S.uu[b][i].u2, &a.x[2 * N + g]);
+    } else {
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      cp_async<sizeof(T)>(&S.raw[b][d][i], &a.coords[base + d]);
-      if (MODE == 0) {
-        cp_async<sizeof(T)>(&S.raw[b][3 + d][i], &a.x[base + d]);
-      } else {
-        cp_async<sizeof(T)>(&S.raw[b][3 + d][i], &a.r[base + d]);
-        cp_async<sizeof(T)>(&S.raw[b][6 + d][i], &a.dinv[base + d]);
-        cp_async<sizeof(T)>(&S.raw[b][9 + d][i], &a.x[base + d]);
+      for (int d = 0; d < 3; ++d) {
+        cp_async<sizeof(T)>(&S.raw[b][d][i], &a.r[d * N + g]);
+        cp_async<sizeof(T)>(&S.raw[b][3 + d][i], &a.dinv[d * N + g]);
+        cp_async<sizeof(T)>(&S.raw[b][6 + d][i], &a.x[d * N + g]);
       }
     }
   }
@@ -210,18 +230,28 @@ __global__ void __launch_bounds__(kApplyThreads, 1) k_apply_tiled(ApplyArgs<T> a
     for (int i = threadIdx.x; i < nn; i += blockDim.x) {
       const uint32_t f = S.ids[b][i];
       const uint32_t mk = (f >> kMaskShift) & 7u;
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        T v;
-        if (MODE == 0) {
-          v = (mk >> d) & 1 ? T(0) : S.raw[b][3 + d][i];
-        } else {
-          v = (mk >> d) & 1 ? T(0) : S.raw[b][6 + d][i] * S.raw[b][3 + d][i] + beta * S.raw[b][9 + d][i];
-          if (f & kOwner) a.p_new[3 * int64_t(f & kNodeIdMask) + d] = v;
+      if constexpr (MODE == 0) {
+        if (mk) {
+          if (mk & 1u) S.xc[b][i].u0 = T(0);
+          if (mk & 2u) S.uu[b][i].u1 = T(0);
+          if (mk & 4u) S.uu[b][i].u2 = T(0);
         }
-        S.x[d][i] = v;
-        S.y[d][i] = T(0);
+      } else {
+        T v[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+          v[d] = (mk >> d) & 1 ? T(0) : S.raw[b][3 + d][i] * S.raw[b][d][i] + beta * S.raw[b][6 + d][i];
+        S.xc[b][i].u0 = v[0];
+        S.uu[b][i].u1 = v[1];
+        S.uu[b][i].u2 = v[2];
+        if (f & kOwner) {
+          const int64_t g = int64_t(f & kNodeIdMask);
+#pragma unroll
+          for (int d = 0; d < 3; ++d) a.p_new[d * a.N + g] = v[d];
+        }
       }
+#pragma unroll
+      for (int d = 0; d < 3; ++d) S.y[d][i] = T(0);
     }
     __syncthreads();
 
@@ -236,13 +266,18 @@ __global__ void __launch_bounds__(kApplyThreads, 1) k_apply_tiled(ApplyArgs<T> a
         const T* wv = &S.w[b][6 * t];
         T X[8][3], U[8][3], Y[8][3];
 #pragma unroll
-        for (int s = 0; s < 8; ++s)
+        for (int s = 0; s < 8; ++s) {
+          const Node4<T> q4 = S.xc[b][ln[s]];
+          const Node2<T> q2 = S.uu[b][ln[s]];
+          X[s][0] = q4.x;
+          X[s][1] = q4.y;
+          X[s][2] = q4.z;
+          U[s][0] = q4.u0;
+          U[s][1] = q2.u1;
+          U[s][2] = q2.u2;
 #pragma unroll
-          for (int d = 0; d < 3; ++d) {
-            X[s][d] = S.raw[b][d][ln[s]];
-            U[s][d] = S.x[d][ln[s]];
-            Y[s][d] = T(0);
-          }
+          for (int d = 0; d < 3; ++d) Y[s][d] = T(0);
+        }
 #pragma unroll
         for (int j = 0; j < 6; ++j) {
           T xc[4][3], u[12], r[12];
@@ -268,12 +303,16 @@ __global__ void __launch_bounds__(kApplyThreads, 1) k_apply_tiled(ApplyArgs<T> a
         // single tets follow the hexes: cell index = 6 * nhex + (t - nhex)
         T xc[4][3], u[12], r[12];
 #pragma unroll
-        for (int n = 0; n < 4; ++n)
-#pragma unroll
-          for (int d = 0; d < 3; ++d) {
-            xc[n][d] = S.raw[b][d][ln[n]];
-            u[3 * n + d] = S.x[d][ln[n]];
-          }
+        for (int n = 0; n < 4; ++n) {
+          const Node4<T> q4 = S.xc[b][ln[n]];
+          const Node2<T> q2 = S.uu[b][ln[n]];
+          xc[n][0] = q4.x;
+          xc[n][1] = q4.y;
+          xc[n][2] = q4.z;
+          u[3 * n + 0] = q4.u0;
+          u[3 * n + 1] = q2.u1;
+          u[3 * n + 2] = q2.u2;
+        }
         const T en = tet_apply(a.iso, S.w[b][6 * nhex + (t - nhex)], xc, u, r);
         if (MODE == 1) pap += double(en);
 #pragma unroll
@@ -294,9 +333,9 @@ __global__ void __launch_bounds__(kApplyThreads, 1) k_apply_tiled(ApplyArgs<T> a
         if ((mk >> d) & 1) continue;
         const T v = S.y[d][i];
         if (f & kShared)
-          atomicAdd(&a.y[3 * gid + d], v);
+          atomicAdd(&a.y[d * a.N + gid], v);
         else
-          a.y[3 * gid + d] = v;
+          a.y[d * a.N + gid] = v;
       }
     }
     __syncthreads();
