@@ -62,28 +62,64 @@ __device__ __forceinline__ void block_sum2(double& a, double& b, double* smem /*
   }
 }
 
-// CG update (K2).  T = vector type; X = type of the iterate / its update.
-template <typename T, typename X>
-__global__ void __launch_bounds__(kVecThreads) k_cg_update(int64_t n, X* __restrict__ x, T* __restrict__ r,
+// 16-byte vector of T (float4 / double2) for the streaming kernels.
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<float> {
+  using type = float4;
+  static constexpr int n = 4;
+};
+template <>
+struct Vec16<double> {
+  using type = double2;
+  static constexpr int n = 2;
+};
+
+template <typename T>
+__device__ __forceinline__ void cg_update_one(T& x, T& r, T p, T& ap, T dinv, T a, double& rz, double& rr) {
+  x += a * p;
+  const T ri = r - a * ap;
+  r = ri;
+  ap = T(0);
+  rz += double(ri) * double(dinv * ri);
+  rr += double(ri) * double(ri);
+}
+
+// CG update (K2): x += alpha p, r -= alpha Ap, Ap = 0, r.z and r.r; the last
+// CTA sets beta, the iteration count and the convergence flag.  All vectors
+// are T (the iterate is an FP32 correction in mixed precision) and 16-byte
+// aligned; the body streams them as 16-byte vectors.
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) k_cg_update(int64_t n, T* __restrict__ x, T* __restrict__ r,
                                                            const T* __restrict__ p, T* __restrict__ ap,
                                                            const T* __restrict__ dinv, PcgScalars* __restrict__ sc,
                                                            double* __restrict__ partials, unsigned int* counter,
                                                            double* __restrict__ rr_hist) {
+  using V = typename Vec16<T>::type;
+  constexpr int W = Vec16<T>::n;
   __shared__ double s_red[64];
   if (sc->done) return;
-  const double alpha = sc->alpha;
-  const T a = T(alpha);
+  const T a = T(sc->alpha);
   double rz = 0.0, rr = 0.0;
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-    const T pi = p[i];
-    x[i] += X(alpha) * X(pi);
-    const T ri = r[i] - a * ap[i];
-    r[i] = ri;
-    ap[i] = T(0);
-    const T zi = dinv[i] * ri;
-    rz += double(ri) * double(zi);
-    rr += double(ri) * double(ri);
+  const int64_t nv = n / W;
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nv; i += stride) {
+    V xv = reinterpret_cast<V*>(x)[i], rv = reinterpret_cast<V*>(r)[i], av = reinterpret_cast<V*>(ap)[i];
+    const V pv = reinterpret_cast<const V*>(p)[i], dv = reinterpret_cast<const V*>(dinv)[i];
+    T* xs = reinterpret_cast<T*>(&xv);
+    T* rs = reinterpret_cast<T*>(&rv);
+    T* as = reinterpret_cast<T*>(&av);
+    const T* ps = reinterpret_cast<const T*>(&pv);
+    const T* ds = reinterpret_cast<const T*>(&dv);
+#pragma unroll
+    for (int k = 0; k < W; ++k) cg_update_one(xs[k], rs[k], ps[k], as[k], ds[k], a, rz, rr);
+    reinterpret_cast<V*>(x)[i] = xv;
+    reinterpret_cast<V*>(r)[i] = rv;
+    reinterpret_cast<V*>(ap)[i] = av;
   }
+  for (int64_t i = nv * W + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += stride)
+    cg_update_one(x[i], r[i], p[i], ap[i], dinv[i], a, rz, rr);
   block_sum2(rz, rr, s_red);
   if (threadIdx.x == 0) { partials[2 * blockIdx.x] = rz; partials[2 * blockIdx.x + 1] = rr; }
   if (last_block_arrive(counter)) {
@@ -292,7 +328,7 @@ struct CgGraph {
     for (int k = 0; k < chunk; ++k) {
       k_apply_tiled<T, 1><<<ag, kApplyThreads, tile_smem_bytes<T, 1>(), s>>>(k % 2 == 0 ? a_even : a_odd);
       const T* pnew = (k % 2 == 0) ? pb : pa;
-      k_cg_update<T, X><<<vg, kVecThreads, 0, s>>>(n, x, r, pnew, ap, dinv, ws.sc.get(), ws.partials.get(),
+      k_cg_update<T><<<vg, kVecThreads, 0, s>>>(n, x, r, pnew, ap, dinv, ws.sc.get(), ws.partials.get(),
                                                    ws.counters.get() + 1, nullptr);
     }
     cudaError_t ce = cudaStreamEndCapture(s, &graph);

@@ -103,6 +103,65 @@ __device__ __forceinline__ T tet_apply(const Iso<T>& iso, T w, const T (&xc)[4][
   return voigt_dot(sig, e);
 }
 
+// One tet in "relative" form, vertices (v0, va, vb, v3) with edge vectors
+// e0 = x_v0 - x_v3, ea, eb and input differences du = u - u_v3.  With
+// h0 = ea x eb, h1 = eb x e0, h2 = e0 x ea (the rows of det * J^-1, since J has
+// columns e0, ea, eb) and det = e0 . h0, the reference's per-cell chain
+// (ComputeGradientWorkset, Strain, LinearStress, ApplyWeighting,
+// StressDivergence) becomes
+//   eps_u = sum_n h_n (x) du_n        (= det * strain; Voigt, engineering shears)
+//   sig'  = s C eps_u,  s = w / (6 |det|)
+//   r_n   = h_n . sig'  for n = 0..2,  r_v3 = -(r_0 + r_1 + r_2)
+// i.e. vol * w * B^T C B u with vol = |det| / 6, one reciprocal per tet and no
+// per-entry scaling of the gradients.  Returns eps_u : sig' = p_e^T K_e p_e.
+// h1 and h2 are passed in because a hex cluster shares them between tets.
+template <typename T>
+__device__ __forceinline__ T tet_rel(const Iso<T>& iso, T w, const T (&e0)[3], const T (&ea)[3], const T (&eb)[3],
+                                     const T (&h1)[3], const T (&h2)[3], const T (&d0)[3], const T (&da)[3],
+                                     const T (&db)[3], T (&r0)[3], T (&ra)[3], T (&rb)[3]) {
+  T h0[3];
+  h0[0] = ea[1] * eb[2] - ea[2] * eb[1];
+  h0[1] = ea[2] * eb[0] - ea[0] * eb[2];
+  h0[2] = ea[0] * eb[1] - ea[1] * eb[0];
+  const T det = e0[0] * h0[0] + e0[1] * h0[1] + e0[2] * h0[2];
+  const T sc = w / (T(6) * fabs(det));
+  // eps_u = sum_n h_n (x) du_n
+  const T exx = h0[0] * d0[0] + h1[0] * da[0] + h2[0] * db[0];
+  const T eyy = h0[1] * d0[1] + h1[1] * da[1] + h2[1] * db[1];
+  const T ezz = h0[2] * d0[2] + h1[2] * da[2] + h2[2] * db[2];
+  const T gyz = h0[1] * d0[2] + h0[2] * d0[1] + h1[1] * da[2] + h1[2] * da[1] + h2[1] * db[2] + h2[2] * db[1];
+  const T gxz = h0[0] * d0[2] + h0[2] * d0[0] + h1[0] * da[2] + h1[2] * da[0] + h2[0] * db[2] + h2[2] * db[0];
+  const T gxy = h0[0] * d0[1] + h0[1] * d0[0] + h1[0] * da[1] + h1[1] * da[0] + h2[0] * db[1] + h2[1] * db[0];
+  const T lam = iso.lam * sc, mu = iso.mu * sc, two_mu = mu + mu;
+  const T ltr = lam * (exx + eyy + ezz);
+  const T sxx = ltr + two_mu * exx, syy = ltr + two_mu * eyy, szz = ltr + two_mu * ezz;
+  const T syz = mu * gyz, sxz = mu * gxz, sxy = mu * gxy;
+  r0[0] = h0[0] * sxx + h0[1] * sxy + h0[2] * sxz;
+  r0[1] = h0[0] * sxy + h0[1] * syy + h0[2] * syz;
+  r0[2] = h0[0] * sxz + h0[1] * syz + h0[2] * szz;
+  ra[0] = h1[0] * sxx + h1[1] * sxy + h1[2] * sxz;
+  ra[1] = h1[0] * sxy + h1[1] * syy + h1[2] * syz;
+  ra[2] = h1[0] * sxz + h1[1] * syz + h1[2] * szz;
+  rb[0] = h2[0] * sxx + h2[1] * sxy + h2[2] * sxz;
+  rb[1] = h2[0] * sxy + h2[1] * syy + h2[2] * syz;
+  rb[2] = h2[0] * sxz + h2[1] * syz + h2[2] * szz;
+  return sxx * exx + syy * eyy + szz * ezz + syz * gyz + sxz * gxz + sxy * gxy;
+}
+
+template <typename T>
+__device__ __forceinline__ void cross3(const T (&a)[3], const T (&b)[3], T (&c)[3]) {
+  c[0] = a[1] * b[2] - a[2] * b[1];
+  c[1] = a[2] * b[0] - a[0] * b[2];
+  c[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+// Ring of a hex cluster: tet k has vertices (slot 0, ring(k), ring(k+1), slot 7),
+// the same vertex sets as hex_slot(k, .).
+__host__ __device__ constexpr int hex_ring(int k) {
+  constexpr int r[7] = {3, 2, 6, 4, 5, 1, 3};
+  return r[k];
+}
+
 // ---------------------------------------------------------------- cp.async --
 template <int BYTES>
 __device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
@@ -264,61 +323,83 @@ __global__ void __launch_bounds__(kApplyThreads, 1) k_apply_tiled(ApplyArgs<T> a
                          int(q.z & 0xffff), int(q.z >> 16), int(q.w & 0xffff), int(q.w >> 16)};
       if (t < nhex) {
         const T* wv = &S.w[b][6 * t];
-        T X[8][3], U[8][3], Y[8][3];
+        // edge vectors and input differences relative to slot 7 (the diagonal end)
+        T E[7][3], D[7][3], Y[7][3];
+        {
+          const Node4<T> q7 = S.xc[b][ln[7]];
+          const Node2<T> p7 = S.uu[b][ln[7]];
 #pragma unroll
-        for (int s = 0; s < 8; ++s) {
-          const Node4<T> q4 = S.xc[b][ln[s]];
-          const Node2<T> q2 = S.uu[b][ln[s]];
-          X[s][0] = q4.x;
-          X[s][1] = q4.y;
-          X[s][2] = q4.z;
-          U[s][0] = q4.u0;
-          U[s][1] = q2.u1;
-          U[s][2] = q2.u2;
+          for (int s = 0; s < 7; ++s) {
+            const Node4<T> q4 = S.xc[b][ln[s]];
+            const Node2<T> q2 = S.uu[b][ln[s]];
+            E[s][0] = q4.x - q7.x;
+            E[s][1] = q4.y - q7.y;
+            E[s][2] = q4.z - q7.z;
+            D[s][0] = q4.u0 - q7.u0;
+            D[s][1] = q2.u1 - p7.u1;
+            D[s][2] = q2.u2 - p7.u2;
 #pragma unroll
-          for (int d = 0; d < 3; ++d) Y[s][d] = T(0);
+            for (int d = 0; d < 3; ++d) Y[s][d] = T(0);
+          }
         }
+        // C[s] = E[0] x E[s] for the ring slots, shared by the two tets at s
+        T Cx[7][3];
 #pragma unroll
-        for (int j = 0; j < 6; ++j) {
-          T xc[4][3], u[12], r[12];
+        for (int k = 0; k < 6; ++k) cross3(E[0], E[hex_ring(k)], Cx[hex_ring(k)]);
 #pragma unroll
-          for (int n = 0; n < 4; ++n)
+        for (int k = 0; k < 6; ++k) {
+          const int sa = hex_ring(k), sb = hex_ring(k + 1);
+          T h1[3], r0[3], ra[3], rb[3];
 #pragma unroll
-            for (int d = 0; d < 3; ++d) {
-              xc[n][d] = X[hex_slot(j, n)][d];
-              u[3 * n + d] = U[hex_slot(j, n)][d];
-            }
-          const T en = tet_apply(a.iso, wv[j], xc, u, r);
+          for (int d = 0; d < 3; ++d) h1[d] = -Cx[sb][d];
+          const T en = tet_rel(a.iso, wv[k], E[0], E[sa], E[sb], h1, Cx[sa], D[0], D[sa], D[sb], r0, ra, rb);
           if (MODE == 1) pap += double(en);
 #pragma unroll
-          for (int n = 0; n < 4; ++n)
-#pragma unroll
-            for (int d = 0; d < 3; ++d) Y[hex_slot(j, n)][d] += r[3 * n + d];
+          for (int d = 0; d < 3; ++d) {
+            Y[0][d] += r0[d];
+            Y[sa][d] += ra[d];
+            Y[sb][d] += rb[d];
+          }
         }
+        // slot 7 closes each tet's partition of unity: Y7 = -(Y0 + ... + Y6)
+        T Y7[3] = {T(0), T(0), T(0)};
 #pragma unroll
-        for (int s = 0; s < 8; ++s)
+        for (int s = 0; s < 7; ++s)
+#pragma unroll
+          for (int d = 0; d < 3; ++d) Y7[d] -= Y[s][d];
+#pragma unroll
+        for (int s = 0; s < 7; ++s)
 #pragma unroll
           for (int d = 0; d < 3; ++d) atomicAdd(&S.y[d][ln[s]], Y[s][d]);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) atomicAdd(&S.y[d][ln[7]], Y7[d]);
       } else {
         // single tets follow the hexes: cell index = 6 * nhex + (t - nhex)
-        T xc[4][3], u[12], r[12];
+        T e[3][3], du[3][3], h1[3], h2[3], r[3][3];
+        const Node4<T> q3 = S.xc[b][ln[3]];
+        const Node2<T> p3 = S.uu[b][ln[3]];
 #pragma unroll
-        for (int n = 0; n < 4; ++n) {
+        for (int n = 0; n < 3; ++n) {
           const Node4<T> q4 = S.xc[b][ln[n]];
           const Node2<T> q2 = S.uu[b][ln[n]];
-          xc[n][0] = q4.x;
-          xc[n][1] = q4.y;
-          xc[n][2] = q4.z;
-          u[3 * n + 0] = q4.u0;
-          u[3 * n + 1] = q2.u1;
-          u[3 * n + 2] = q2.u2;
+          e[n][0] = q4.x - q3.x;
+          e[n][1] = q4.y - q3.y;
+          e[n][2] = q4.z - q3.z;
+          du[n][0] = q4.u0 - q3.u0;
+          du[n][1] = q2.u1 - p3.u1;
+          du[n][2] = q2.u2 - p3.u2;
         }
-        const T en = tet_apply(a.iso, S.w[b][6 * nhex + (t - nhex)], xc, u, r);
+        cross3(e[2], e[0], h1);
+        cross3(e[0], e[1], h2);
+        const T en = tet_rel(a.iso, S.w[b][6 * nhex + (t - nhex)], e[0], e[1], e[2], h1, h2, du[0], du[1], du[2],
+                             r[0], r[1], r[2]);
         if (MODE == 1) pap += double(en);
 #pragma unroll
-        for (int n = 0; n < 4; ++n)
+        for (int n = 0; n < 3; ++n)
 #pragma unroll
-          for (int d = 0; d < 3; ++d) atomicAdd(&S.y[d][ln[n]], r[3 * n + d]);
+          for (int d = 0; d < 3; ++d) atomicAdd(&S.y[d][ln[n]], r[n][d]);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) atomicAdd(&S.y[d][ln[3]], -(r[0][d] + r[1][d] + r[2][d]));
       }
     }
     __syncthreads();
