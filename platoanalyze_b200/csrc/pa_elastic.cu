@@ -391,8 +391,8 @@ void launch_apply_tiled(const Problem& P, const T* w, const T* x, T* y, bool con
   a.x = x;
   a.y = y;
   PA_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * P.ndof(), s));
-  const int grid = apply_kernel_setup<T, 0>(a.tv.num_tiles);
-  k_apply_tiled<T, 0><<<grid, kApplyThreads, tile_smem_bytes<T, 0>(), s>>>(a);
+  const int grid = apply_kernel_setup<T, 0>(*P.mesh);
+  launch_apply_kernel<T, 0>(*P.mesh, grid, s, a);
   PA_LAUNCHED();
 }
 

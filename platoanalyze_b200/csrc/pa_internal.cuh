@@ -66,15 +66,14 @@ struct DevBuf {
 
 // ------------------------------------------------------------- tile layout --
 // Cells are grouped into clusters (six tets of one hex, or a single tet) and
-// clusters into tiles of at most kTileClusters clusters touching at most
-// kTileNodes distinct nodes.  A tile's nodes are staged in shared memory;
+// clusters into tiles of at most tile_clusters clusters (64, 128 or 256)
+// touching at most 2 * tile_clusters distinct nodes.  A tile's nodes are staged in shared memory;
 // each cluster stores up to 8 tile-local node ids as uint16.  tile_nodes
 // entries are a 27-bit node id plus flags: kShared (the node also belongs to
 // another tile, so its sum is added atomically), kOwner (this tile writes
 // per-node outputs of the node; exactly one tile per node) and three
 // Dirichlet-mask bits (bit d: dof d constrained; set in a problem's copy).
-constexpr int kTileClusters = 256;
-constexpr int kTileNodes = 512;
+constexpr int kMaxTileClusters = 256;  // tile sizes: 64, 128 or 256 clusters (= threads per CTA)
 constexpr uint32_t kShared = 0x80000000u;
 constexpr uint32_t kOwner = 0x40000000u;
 constexpr int kMaskShift = 27;
@@ -105,6 +104,7 @@ struct Mesh {
   DevBuf<int32_t> d_rowmap, d_cols;
   DevBuf<int32_t> d_cell_entry;  // C*16 CRS block index of (a,b) pairs
   int64_t num_clusters = 0, num_hex = 0;
+  int tile_clusters = 256;  // clusters per tile (threads per CTA); a tile touches <= 2x as many nodes
   DevBuf<int32_t> d_tile_cluster_start, d_tile_cell_start, d_tile_hex_count, d_tile_node_start, d_cell_perm;
   DevBuf<uint32_t> d_tile_nodes;
   DevBuf<uint4> d_cluster_nodes;

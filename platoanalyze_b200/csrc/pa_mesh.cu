@@ -2,6 +2,7 @@
 // map, and the shared-memory cell tiles of the matrix-free kernel.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <numeric>
 
 #include "pa_problem.cuh"
@@ -109,7 +110,7 @@ bool match_hex(const Mesh& m, int64_t c0, Cluster& out) {
 
 // Clusters (hex groups of six consecutive cells, else single cells), ordered
 // along the Morton (Z-order) curve of their centroids, packed greedily into
-// tiles of <= kTileClusters clusters and <= kTileNodes nodes.
+// tiles of <= tile_clusters clusters and <= 2 tile_clusters nodes.
 void build_tiles(Mesh& m) {
   std::vector<Cluster> cl;
   cl.reserve(m.C / 6 + 16);
@@ -147,6 +148,7 @@ void build_tiles(Mesh& m) {
   }
   std::stable_sort(cl.begin(), cl.end(), [](const Cluster& a, const Cluster& b) { return a.key < b.key; });
 
+  const int tile_k = m.tile_clusters, tile_n = 2 * m.tile_clusters;
   std::vector<int32_t> tile_cluster_start{0}, tile_cell_start{0}, tile_hex_count, tile_node_start{0}, perm;
   std::vector<uint32_t> tile_nodes;
   std::vector<uint4> cluster_nodes;
@@ -198,7 +200,7 @@ void build_tiles(Mesh& m) {
     const int nn = k.hex ? 8 : 4;
     int fresh = 0;
     for (int n = 0; n < nn; ++n) fresh += stamp[k.nodes[n]] == tile ? 0 : 1;
-    if (int(cur.size()) >= kTileClusters || int(cur_nodes.size()) + fresh > kTileNodes) close_tile();
+    if (int(cur.size()) >= tile_k || int(cur_nodes.size()) + fresh > tile_n) close_tile();
     for (int n = 0; n < nn; ++n) {
       const int32_t v = k.nodes[n];
       if (stamp[v] != tile) {
@@ -222,7 +224,7 @@ void build_tiles(Mesh& m) {
       const int32_t nn = tile_node_start[t + 1] - tile_node_start[t];
       const int32_t nk = tile_cluster_start[t + 1] - tile_cluster_start[t];
       const int32_t nc = tile_cell_start[t + 1] - tile_cell_start[t];
-      if (nn > kTileNodes || nk > kTileClusters || tile_hex_count[t] > nk || nc > 6 * kTileClusters ||
+      if (nn > tile_n || nk > tile_k || tile_hex_count[t] > nk || nc > 6 * tile_k ||
           nc != 6 * tile_hex_count[t] + (nk - tile_hex_count[t]))
         throw Error(PA_ERR_INVALID_ARG, "tile exceeds its shared-memory capacity");
       for (int32_t k = tile_cluster_start[t]; k < tile_cluster_start[t + 1]; ++k) {
@@ -316,6 +318,9 @@ void mesh_build(Mesh& m) {
     PA_CHECK(m.cells[i] >= 0 && m.cells[i] < m.N, "cells2nodes entry out of range");
   for (int64_t i = 0; i < 3 * m.N; ++i) PA_CHECK(std::isfinite(m.coords[i]), "non-finite coordinate");
   PA_CUDA(cudaGetDevice(&m.device));
+  if (const char* e = std::getenv("PA_TILE_CLUSTERS")) m.tile_clusters = std::atoi(e);
+  PA_CHECK(m.tile_clusters == 64 || m.tile_clusters == 128 || m.tile_clusters == 256,
+           "tile size (clusters per tile) must be 64, 128 or 256");
   build_graph(m);
   build_tiles(m);
   m.d_cells.upload(m.cells.data(), m.cells.size());

@@ -256,8 +256,8 @@ __global__ void k_dot2(int64_t n, const double* __restrict__ a, const double* __
 }
 
 template <typename T>
-int fused_apply_grid(int num_tiles) {
-  return apply_kernel_setup<T, 1>(num_tiles);
+int fused_apply_grid(const Mesh& m) {
+  return apply_kernel_setup<T, 1>(m);
 }
 
 template <typename T>
@@ -320,13 +320,13 @@ struct CgGraph {
     SolverWorkspace& ws = P.ws;
     const int64_t n = P.ndof();
     const int vg = vec_grid(n);
-    const int ag = fused_apply_grid<T>(int(P.mesh->T));
+    const int ag = fused_apply_grid<T>(*P.mesh);
     chunk = chunk_ + (chunk_ % 2);
     ApplyArgs<T> a_even = fused_args<T>(P, coords, w, pa, pb, ap, r, dinv);  // reads pa, writes pb
     ApplyArgs<T> a_odd = fused_args<T>(P, coords, w, pb, pa, ap, r, dinv);   // reads pb, writes pa
     PA_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < chunk; ++k) {
-      k_apply_tiled<T, 1><<<ag, kApplyThreads, tile_smem_bytes<T, 1>(), s>>>(k % 2 == 0 ? a_even : a_odd);
+      launch_apply_kernel<T, 1>(*P.mesh, ag, s, k % 2 == 0 ? a_even : a_odd);
       const T* pnew = (k % 2 == 0) ? pb : pa;
       k_cg_update<T><<<vg, kVecThreads, 0, s>>>(n, x, r, pnew, ap, dinv, ws.sc.get(), ws.partials.get(),
                                                    ws.counters.get() + 1, nullptr);
@@ -388,8 +388,8 @@ pa_status solve_device(Problem& P, const double* z, const double* b, double* x_o
   const bool mixed = o.method == PA_SOLVER_PCG_MIXED;
   PA_CHECK(o.method == PA_SOLVER_PCG_FP64 || mixed, "unknown solver method");
   PA_CHECK(o.rel_tol > 0.0, "rel_tol must be positive");
-  const int grid_need = std::max(std::max(fused_apply_grid<double>(int(P.mesh->T)),
-                                          fused_apply_grid<float>(int(P.mesh->T))), vec_grid(n));
+  const int grid_need = std::max(std::max(fused_apply_grid<double>(*P.mesh), fused_apply_grid<float>(*P.mesh)),
+                                vec_grid(n));
   P.ws.ensure(n, P.C(), grid_need, mixed);
   SolverWorkspace& ws = P.ws;
   const int max_iters = o.max_iters > 0 ? o.max_iters : int(20.0 * std::sqrt(double(n)) + 1000);
@@ -538,8 +538,8 @@ pa_status solve_device(Problem& P, const double* z, const double* b, double* x_o
 double time_cg_apply(Problem& P, const double* z, bool fp32, int reps) {
   cudaStream_t s = P.stream;
   const int64_t n = P.ndof();
-  const int grid_need = std::max(std::max(fused_apply_grid<double>(int(P.mesh->T)),
-                                          fused_apply_grid<float>(int(P.mesh->T))), vec_grid(n));
+  const int grid_need = std::max(std::max(fused_apply_grid<double>(*P.mesh), fused_apply_grid<float>(*P.mesh)),
+                                vec_grid(n));
   P.ws.ensure(n, P.C(), grid_need, true);
   SolverWorkspace& ws = P.ws;
   launch_cell_weights(P, z, ws.w64.get(), ws.w32.get(), s);
@@ -551,7 +551,7 @@ double time_cg_apply(Problem& P, const double* z, bool fp32, int reps) {
   init.beta = 0.5;
   init.rz = 1.0;
   PA_CUDA(cudaMemcpyAsync(ws.sc.get(), &init, sizeof(init), cudaMemcpyHostToDevice, s));
-  const int ag = fp32 ? fused_apply_grid<float>(int(P.mesh->T)) : fused_apply_grid<double>(int(P.mesh->T));
+  const int ag = fp32 ? fused_apply_grid<float>(*P.mesh) : fused_apply_grid<double>(*P.mesh);
   if (!P.ev0) { PA_CUDA(cudaEventCreate(&P.ev0)); PA_CUDA(cudaEventCreate(&P.ev1)); }
   float ms = 0.f;
   if (fp32) {
@@ -564,10 +564,9 @@ double time_cg_apply(Problem& P, const double* z, bool fp32, int reps) {
                                            ws.ap32.get(), ws.r32.get(), ws.dinv32.get());
     ApplyArgs<float> b = fused_args<float>(P, P.mesh->d_coords32_soa.get(), ws.w32.get(), ws.p32b.get(), ws.p32a.get(),
                                            ws.ap32.get(), ws.r32.get(), ws.dinv32.get());
-    const size_t sm = tile_smem_bytes<float, 1>();
-    k_apply_tiled<float, 1><<<ag, kApplyThreads, sm, s>>>(a);  // warm
+    launch_apply_kernel<float, 1>(*P.mesh, ag, s, a);  // warm
     PA_CUDA(cudaEventRecord(P.ev0, s));
-    for (int i = 0; i < reps; ++i) k_apply_tiled<float, 1><<<ag, kApplyThreads, sm, s>>>(i % 2 ? a : b);
+    for (int i = 0; i < reps; ++i) launch_apply_kernel<float, 1>(*P.mesh, ag, s, i % 2 ? a : b);
     PA_CUDA(cudaEventRecord(P.ev1, s));
   } else {
     std::vector<double> ones(n, 1.0);
@@ -579,10 +578,9 @@ double time_cg_apply(Problem& P, const double* z, bool fp32, int reps) {
                                              ws.ap.get(), ws.r.get(), ws.dinv.get());
     ApplyArgs<double> b = fused_args<double>(P, P.mesh->d_coords_soa.get(), ws.w64.get(), ws.p1.get(), ws.p0.get(),
                                              ws.ap.get(), ws.r.get(), ws.dinv.get());
-    const size_t sm = tile_smem_bytes<double, 1>();
-    k_apply_tiled<double, 1><<<ag, kApplyThreads, sm, s>>>(a);
+    launch_apply_kernel<double, 1>(*P.mesh, ag, s, a);
     PA_CUDA(cudaEventRecord(P.ev0, s));
-    for (int i = 0; i < reps; ++i) k_apply_tiled<double, 1><<<ag, kApplyThreads, sm, s>>>(i % 2 ? a : b);
+    for (int i = 0; i < reps; ++i) launch_apply_kernel<double, 1>(*P.mesh, ag, s, i % 2 ? a : b);
     PA_CUDA(cudaEventRecord(P.ev1, s));
   }
   PA_LAUNCHED();

@@ -8,7 +8,7 @@
 //    "single" cluster.  A hex cluster touches 8 nodes for 6 cells, a single
 //    one 4 nodes for 1 cell.
 //  * clusters are ordered along a Morton curve and packed into tiles of at
-//    most kTileClusters clusters touching at most kTileNodes nodes; a tile's
+//    at most TILE clusters (64, 128 or 256) touching at most 2 TILE nodes; a tile's
 //    cells are contiguous in the internal cell order.
 //
 // Kernel: a persistent grid (a multiple of the SM count) walks the tiles.  For
@@ -34,8 +34,6 @@
 #include "pa_cell.cuh"
 
 namespace pa {
-
-constexpr int kApplyThreads = kTileClusters;
 
 // Vectors are stored component-major (SoA): v[d * N + node].
 template <typename T>
@@ -186,29 +184,31 @@ struct alignas(2 * sizeof(T)) Node2 {
   T u1, u2;
 };
 
-// Shared-memory layout of one CTA (dynamic shared memory).
-template <typename T, int MODE>
+// Shared-memory layout of one CTA (dynamic shared memory); TILE clusters
+// (threads) and up to 2 * TILE nodes per tile.
+template <typename T, int MODE, int TILE>
 struct TileSmem {
+  static constexpr int kTileNodes = 2 * TILE;
   static constexpr int kRawBufs = MODE == 1 ? 2 : 1;
   Node4<T> xc[2][kTileNodes];             // coordinates + input (component 0), two buffers
   Node2<T> uu[2][kTileNodes];             // input components 1, 2
   T raw[kRawBufs][9][kTileNodes];         // PCG: r, D^-1, p_old gathered for the tile
   T y[3][kTileNodes];                     // node sums of the current tile
-  T w[2][6 * kTileClusters];              // penalty weights of the tile's cells
-  uint4 rec[2][kTileClusters];            // cluster node ids
+  T w[2][6 * TILE];                       // penalty weights of the tile's cells
+  uint4 rec[2][TILE];                     // cluster node ids
   uint32_t ids[2][kTileNodes];            // flagged node ids
   int32_t meta[2][8];                     // n0, nn, k0, nk, nhex, cell0, ncell
   double red[32];
 };
 
-template <typename T, int MODE>
+template <typename T, int MODE, int TILE>
 constexpr size_t tile_smem_bytes() {
-  return sizeof(TileSmem<T, MODE>);
+  return sizeof(TileSmem<T, MODE, TILE>);
 }
 
 // Issue the loads of tile `tile`'s header, node ids and cluster records (buffer b).
-template <typename T, int MODE>
-__device__ __forceinline__ void prefetch_ids(const ApplyArgs<T>& a, TileSmem<T, MODE>& S, int tile, int b) {
+template <typename T, int MODE, int TILE>
+__device__ __forceinline__ void prefetch_ids(const ApplyArgs<T>& a, TileSmem<T, MODE, TILE>& S, int tile, int b) {
   const int n0 = a.tv.tile_node_start[tile], nn = a.tv.tile_node_start[tile + 1] - n0;
   const int k0 = a.tv.tile_cluster_start[tile], nk = a.tv.tile_cluster_start[tile + 1] - k0;
   if (threadIdx.x == 0) {
@@ -227,8 +227,8 @@ __device__ __forceinline__ void prefetch_ids(const ApplyArgs<T>& a, TileSmem<T, 
 }
 
 // Issue the gathers of the node data and weights of the tile whose ids sit in buffer b.
-template <typename T, int MODE>
-__device__ __forceinline__ void prefetch_data(const ApplyArgs<T>& a, TileSmem<T, MODE>& S, int b) {
+template <typename T, int MODE, int TILE>
+__device__ __forceinline__ void prefetch_data(const ApplyArgs<T>& a, TileSmem<T, MODE, TILE>& S, int b) {
   const int nn = S.meta[b][1];
   const int64_t N = a.N;
   for (int i = threadIdx.x; i < nn; i += blockDim.x) {
@@ -254,10 +254,10 @@ __device__ __forceinline__ void prefetch_data(const ApplyArgs<T>& a, TileSmem<T,
   cp_async_commit();
 }
 
-template <typename T, int MODE>
-__global__ void __launch_bounds__(kApplyThreads, 1) k_apply_tiled(ApplyArgs<T> a) {
+template <typename T, int MODE, int TILE>
+__global__ void __launch_bounds__(TILE, 1) k_apply_tiled(ApplyArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  TileSmem<T, MODE>& S = *reinterpret_cast<TileSmem<T, MODE>*>(smem_raw);
+  TileSmem<T, MODE, TILE>& S = *reinterpret_cast<TileSmem<T, MODE, TILE>*>(smem_raw);
 
   T beta = T(0);
   if (MODE == 1) {
@@ -448,17 +448,35 @@ __global__ void __launch_bounds__(kApplyThreads, 1) k_apply_tiled(ApplyArgs<T> a
   }
 }
 
-// Configure dynamic shared memory once per kernel instance; returns the
-// persistent grid size (resident CTAs per SM x SMs, capped by the tile count).
-template <typename T, int MODE>
-int apply_kernel_setup(int num_tiles) {
-  const size_t smem = tile_smem_bytes<T, MODE>();
-  PA_CUDA(cudaFuncSetAttribute(k_apply_tiled<T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+// Configure dynamic shared memory of one instance; returns the persistent
+// grid size (resident CTAs per SM x SMs, capped by the tile count).
+template <typename T, int MODE, int TILE>
+int apply_grid_for(int num_tiles) {
+  const size_t smem = tile_smem_bytes<T, MODE, TILE>();
+  PA_CUDA(cudaFuncSetAttribute(k_apply_tiled<T, MODE, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   int blocks = 0;
-  PA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_apply_tiled<T, MODE>, kApplyThreads, smem));
-  int grid = std::max(1, blocks) * num_sms();
-  if (grid > num_tiles) grid = num_tiles;
+  PA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_apply_tiled<T, MODE, TILE>, TILE, smem));
+  const int grid = std::min(std::max(1, blocks) * num_sms(), num_tiles);
   return std::max(grid, 1);
+}
+
+template <typename T, int MODE>
+int apply_kernel_setup(const Mesh& m) {
+  switch (m.tile_clusters) {
+    case 64: return apply_grid_for<T, MODE, 64>(int(m.T));
+    case 128: return apply_grid_for<T, MODE, 128>(int(m.T));
+    default: return apply_grid_for<T, MODE, 256>(int(m.T));
+  }
+}
+
+// Launch (also inside stream capture) the instance matching the mesh's tile size.
+template <typename T, int MODE>
+void launch_apply_kernel(const Mesh& m, int grid, cudaStream_t s, const ApplyArgs<T>& a) {
+  switch (m.tile_clusters) {
+    case 64: k_apply_tiled<T, MODE, 64><<<grid, 64, tile_smem_bytes<T, MODE, 64>(), s>>>(a); break;
+    case 128: k_apply_tiled<T, MODE, 128><<<grid, 128, tile_smem_bytes<T, MODE, 128>(), s>>>(a); break;
+    default: k_apply_tiled<T, MODE, 256><<<grid, 256, tile_smem_bytes<T, MODE, 256>(), s>>>(a); break;
+  }
 }
 
 }  // namespace pa
