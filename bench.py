@@ -201,6 +201,22 @@ def run_reference(args):
     return 0
 
 
+# ------------------------------------------------------- multi-rank helpers --
+def max_over_ranks(value, world, device="cuda"):
+    """Max of a per-rank float over all ranks (one all-reduce; identity at N=1)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world, cells_per_rank, steps, max_ms):
+    """Units all ranks processed divided by the slowest rank's time."""
+    return world * cells_per_rank * steps / (max_ms * 1e-3)
+
+
 # ----------------------------------------------------------------- GPU side --
 def traffic_from_profiles(kernel_tag):
     """DRAM bytes per launch recorded by the ncu summary in profiles/, if any."""
@@ -289,11 +305,8 @@ def run_ours(args):
     clk = clocks.stop()
     if world > 1:
         dist.barrier()
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = float(t.item())
-    value = world * C * args.steps / (max_ms * 1e-3)
+    max_ms = max_over_ranks(total_ms, world)
+    value = whole_job_rate(world, C, args.steps, max_ms)
 
     # end to end through the C ABI with host (pinned) buffers: z in, u out
     z_pin = torch.tensor(z_host, dtype=torch.float64).pin_memory()
@@ -306,10 +319,7 @@ def run_ours(args):
         t0 = time.perf_counter()
         _, st = prob.solution(z_pin, u_pin, options=opts)
         e2e_ms += 1e3 * (time.perf_counter() - t0)
-    te = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * C * args.steps / (float(te.item()) * 1e-3)
+    e2e_value = whole_job_rate(world, C, args.steps, max_over_ranks(e2e_ms, world))
     rel_u = float(np.abs(u_pin.numpy() - u.cpu().numpy()).max() / max(np.abs(u.cpu().numpy()).max(), 1e-300))
 
     # plain FP64 Jacobi-PCG on the same system (the comparison the metric names)

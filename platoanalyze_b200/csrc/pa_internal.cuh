@@ -8,7 +8,7 @@
 #include <vector>
 #include <stdexcept>
 
-#include "../../include/pa_b200.h"
+#include "pa_b200.h"  // include/ is on the compiler include path
 
 namespace pa {
 
@@ -104,7 +104,7 @@ struct Mesh {
   DevBuf<int32_t> d_rowmap, d_cols;
   DevBuf<int32_t> d_cell_entry;  // C*16 CRS block index of (a,b) pairs
   int64_t num_clusters = 0, num_hex = 0;
-  int tile_clusters = 256;  // clusters per tile (threads per CTA); a tile touches <= 2x as many nodes
+  int tile_clusters = 128;  // clusters per tile (threads per CTA); a tile touches <= 2x as many nodes
   DevBuf<int32_t> d_tile_cluster_start, d_tile_cell_start, d_tile_hex_count, d_tile_node_start, d_cell_perm;
   DevBuf<uint32_t> d_tile_nodes;
   DevBuf<uint4> d_cluster_nodes;
