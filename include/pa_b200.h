@@ -149,6 +149,23 @@ pa_status pa_sf_gradient_u(pa_problem* problem, const double* u, const double* z
 /* df/dz, N (nodal) or C (cell) (src/elliptic/PhysicsScalarFunction.hpp:432). */
 pa_status pa_sf_gradient_z(pa_problem* problem, const double* u, const double* z, double* grad);
 
+/* Allocation-free compliance value.  No counterpart in the reference: it is
+ * for callers that cannot allocate device memory while they run (a host
+ * framework that owns all device memory through its own pool, a timed loop
+ * where cudaMalloc's implicit device synchronisation is not acceptable, code
+ * that cannot create library handles).  Same value as pa_sf_value, from raw
+ * DEVICE arrays (cells2nodes 16-byte aligned, int32 C x 4; coords N x 3; u 3N;
+ * z N or C per params->control_layout) into the DEVICE scalar `value`, on
+ * `stream` (a cudaStream_t, NULL = default stream), asynchronously.  The
+ * library allocates nothing: block partial sums live in a fixed 256 KB
+ * __device__ array, which limits a call to 8,388,608 cells (larger meshes are
+ * rejected with PA_ERR_INVALID_ARG).  The first call on a device looks up that
+ * array's address (do it before any stream capture); calls whose kernels
+ * overlap on the GPU race on the shared array, so serialise them on one stream. */
+pa_status pa_sf_value_noalloc(const int32_t* cells2nodes, int64_t num_cells, const double* coords,
+                              int64_t num_nodes, const double* u, const double* z,
+                              const pa_elastic_params* params, double* value, void* stream);
+
 /* ----------------------------------------------------- matrix-free ------- */
 
 #define PA_FP64 0

@@ -13,6 +13,7 @@ P = ct.c_void_p
 I32, I64, F64 = ct.c_int32, ct.c_int64, ct.c_double
 
 PA_OK = 0
+PA_ERR_INVALID_ARG = 1
 STATUS_NAMES = {0: "PA_OK", 1: "PA_ERR_INVALID_ARG", 2: "PA_ERR_CUDA", 3: "PA_ERR_NOT_CONVERGED",
                 4: "PA_ERR_BREAKDOWN", 5: "PA_ERR_NONFINITE", 6: "PA_ERR_NO_DEVICE", 7: "PA_ERR_UNSUPPORTED"}
 PA_CONTROL_NODAL, PA_CONTROL_CELL = 0, 1
@@ -65,6 +66,7 @@ SIGNATURES = [
     ("pa_sf_value", I32, [P, P, P, P]),
     ("pa_sf_gradient_u", I32, [P, P, P, P]),
     ("pa_sf_gradient_z", I32, [P, P, P, P]),
+    ("pa_sf_value_noalloc", I32, [P, I64, P, I64, P, P, ct.POINTER(ElasticParams), P, P]),
     ("pa_apply", I32, [P, P, P, P, I32, I32]),
     ("pa_apply_block_constraints", I32, [P, P, P, F64]),
     ("pa_solve_options_default", I32, [ct.POINTER(SolveOptions)]),
