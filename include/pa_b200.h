@@ -139,6 +139,13 @@ pa_status pa_vf_gradient_u(pa_problem* problem, const double* u, const double* z
  * VectorFunction::gradient_z (src/elliptic/VectorFunction.hpp:598-689). */
 pa_status pa_vf_gradient_z(pa_problem* problem, const double* u, const double* z, double* entries);
 
+/* dR/dx (shape sensitivity), transposed into 9*B block-CRS entries on the mesh
+ * graph: block (row = node of the coordinate, col = node of the residual dof),
+ * entry [coordinate component][residual component]; includes the surface
+ * load's dependence on the face areas.  VectorFunction::gradient_x
+ * (src/elliptic/VectorFunction.hpp:317-408). */
+pa_status pa_vf_gradient_x(pa_problem* problem, const double* u, const double* z, double* entries);
+
 /* --------------------- PhysicsScalarFunction "Internal Elastic Energy" ---- */
 
 /* f = sum_c 1/2 vol p(rho) eps:C:eps  (src/elliptic/PhysicsScalarFunction.hpp:225,
@@ -148,6 +155,8 @@ pa_status pa_sf_value(pa_problem* problem, const double* u, const double* z, dou
 pa_status pa_sf_gradient_u(pa_problem* problem, const double* u, const double* z, double* grad);
 /* df/dz, N (nodal) or C (cell) (src/elliptic/PhysicsScalarFunction.hpp:432). */
 pa_status pa_sf_gradient_z(pa_problem* problem, const double* u, const double* z, double* grad);
+/* df/dx, 3N (PhysicsScalarFunction::gradient_x, src/elliptic/PhysicsScalarFunction.hpp:293-360). */
+pa_status pa_sf_gradient_x(pa_problem* problem, const double* u, const double* z, double* grad);
 
 /* Allocation-free compliance value.  No counterpart in the reference: it is
  * for callers that cannot allocate device memory while they run (a host

@@ -36,6 +36,8 @@ def lib():
         L.pao_apply.argtypes = [I64, I64, P, P, P, P, ct.c_int, F64, F64, F64, F64, P]
         L.pao_j2_update.argtypes = [I64, P, P, P, P] + [F64] * 8 + [P, P]
         L.pao_j2_plastic_step.argtypes = [I64, P, P, F64, P]
+        L.pao_gradient_x.argtypes = [I64, I64, P, P, P, P, ct.c_int, F64, F64, F64, F64, I64, P, P, P, P, P]
+        L.pao_energy_grad_x.argtypes = [I64, I64, P, P, P, P, ct.c_int, F64, F64, F64, F64, P]
         L.pao_num_threads.restype = ct.c_int
         L.pao_set_threads.argtypes = [ct.c_int]
         _lib = L
@@ -121,6 +123,25 @@ class Oracle:
         lib().pao_gradient_z(self.C, self.N, _p(self.cells), _p(self.coords), _p(u), _p(z), self.layout, *self.mat,
                              _p(rowmap), _p(cols), _p(vals))
         return vals
+
+    def gradient_x(self, u, z, faces=None, flux=(0.0, 0.0, 0.0), graph=None):
+        rowmap, cols = graph if graph is not None else self.graph()
+        rowmap, cols = _c(rowmap, np.int32), _c(cols, np.int32)
+        u, z = _c(u, np.float64), _c(z, np.float64)
+        nf = 0 if faces is None else len(faces)
+        fa = _c(faces, np.int32) if nf else None
+        fl = _c(flux, np.float64)
+        vals = np.empty(9 * len(cols))
+        lib().pao_gradient_x(self.C, self.N, _p(self.cells), _p(self.coords), _p(u), _p(z), self.layout, *self.mat,
+                             nf, _p(fa), _p(fl), _p(rowmap), _p(cols), _p(vals))
+        return vals
+
+    def energy_grad_x(self, u, z):
+        u, z = _c(u, np.float64), _c(z, np.float64)
+        gx = np.empty(3 * self.N)
+        lib().pao_energy_grad_x(self.C, self.N, _p(self.cells), _p(self.coords), _p(u), _p(z), self.layout,
+                                *self.mat, _p(gx))
+        return gx
 
     def energy(self, u, z, grads=True):
         u, z = _c(u, np.float64), _c(z, np.float64)

@@ -51,6 +51,21 @@ template <int N> inline Dual<N> dpow(const Dual<N>& a, double p) {
   return r;
 }
 inline double dpow(double a, double p) { return std::pow(a, p); }
+template <int N> inline Dual<N> operator/(const Dual<N>& a, const Dual<N>& b) {
+  Dual<N> r; r.v = a.v / b.v;
+  for (int i = 0; i < N; ++i) r.d[i] = (a.d[i] * b.v - a.v * b.d[i]) / (b.v * b.v);
+  return r;
+}
+template <int N> inline Dual<N> operator/(double a, const Dual<N>& b) { return Dual<N>(a) / b; }
+template <int N> inline Dual<N> operator-(const Dual<N>& a) { Dual<N> r; r.v = -a.v; for (int i = 0; i < N; ++i) r.d[i] = -a.d[i]; return r; }
+template <int N> inline Dual<N> dabs(const Dual<N>& a) { return a.v < 0 ? -a : a; }
+inline double dabs(double a) { return std::fabs(a); }
+template <int N> inline Dual<N> dsqrt(const Dual<N>& a) {
+  Dual<N> r; r.v = std::sqrt(a.v);
+  for (int i = 0; i < N; ++i) r.d[i] = a.d[i] / (2.0 * r.v);
+  return r;
+}
+inline double dsqrt(double a) { return std::sqrt(a); }
 inline double val(double x) { return x; }
 template <int N> inline double val(const Dual<N>& x) { return x.v; }
 
@@ -90,9 +105,23 @@ void cell_gradients(const double X[4][3], double g[4][3], double& vol) {
   vol = std::fabs(det) / 6.0;
 }
 
-// Strain<3> (src/Strain.hpp:56-94): Voigt {xx,yy,zz,yz,xz,xy}, engineering shears.
+// Same as cell_gradients for a differentiable configuration type (gradient_x).
 template <typename T>
-void strain(const double g[4][3], const T u[12], T e[6]) {
+void cell_gradients_t(const T X[4][3], T g[4][3], T& vol) {
+  T j11 = X[0][0] - X[3][0], j12 = X[1][0] - X[3][0], j13 = X[2][0] - X[3][0];
+  T j21 = X[0][1] - X[3][1], j22 = X[1][1] - X[3][1], j23 = X[2][1] - X[3][1];
+  T j31 = X[0][2] - X[3][2], j32 = X[1][2] - X[3][2], j33 = X[2][2] - X[3][2];
+  T det = j11 * j22 * j33 + j12 * j23 * j31 + j13 * j21 * j32 - j11 * j23 * j32 - j12 * j21 * j33 - j13 * j22 * j31;
+  g[0][0] = (j22 * j33 - j23 * j32) / det; g[0][1] = (j13 * j32 - j12 * j33) / det; g[0][2] = (j12 * j23 - j13 * j22) / det;
+  g[1][0] = (j23 * j31 - j21 * j33) / det; g[1][1] = (j11 * j33 - j13 * j31) / det; g[1][2] = (j13 * j21 - j11 * j23) / det;
+  g[2][0] = (j21 * j32 - j22 * j31) / det; g[2][1] = (j12 * j31 - j11 * j32) / det; g[2][2] = (j11 * j22 - j12 * j21) / det;
+  for (int d = 0; d < 3; ++d) g[3][d] = -(g[0][d] + g[1][d] + g[2][d]);
+  vol = dabs(det) / 6.0;
+}
+
+// Strain<3> (src/Strain.hpp:56-94): Voigt {xx,yy,zz,yz,xz,xy}, engineering shears.
+template <typename T, typename G>
+void strain(const G g[4][3], const T u[12], T e[6]) {
   for (int i = 0; i < 6; ++i) e[i] = T(0.0);
   for (int n = 0; n < 4; ++n) {
     e[0] += u[3 * n + 0] * g[n][0];
@@ -120,8 +149,8 @@ T simp(const Elastic& m, const T& rho) {
 }
 
 // StressDivergence<3> (src/StressDivergence.hpp:70-90).
-template <typename T>
-void divergence(const double g[4][3], double vol, const T s[6], T r[12]) {
+template <typename T, typename G, typename V>
+void divergence(const G g[4][3], V vol, const T s[6], T r[12]) {
   static const int voigt[3][3] = {{0, 5, 4}, {5, 1, 3}, {4, 3, 2}};
   for (int i = 0; i < 3; ++i)
     for (int n = 0; n < 4; ++n)
@@ -543,6 +572,87 @@ void pao_j2_plastic_step(int64_t C, const double* prev, const double* normal, do
     for (int i = 3; i < 6; ++i) cv[2 + i] = pv[2 + i] + 2.0 * m1 * n[i];
     double m2 = cv[1] * s23 * h_kin;
     for (int i = 0; i < 6; ++i) cv[8 + i] = pv[8 + i] + m2 * n[i];
+  }
+}
+
+// VectorFunction::gradient_x (src/elliptic/VectorFunction.hpp:317-408): the
+// configuration evaluation type (12 coordinate partials per cell) and the
+// transposed block assembly -- block (row = node of coordinate dof k,
+// col = node of residual dof i), entry [k % 3][i % 3] -- plus the uniform
+// surface load's dependence on the face area (scale -1).
+void pao_gradient_x(int64_t C, int64_t N, const int32_t* cells, const double* coords, const double* u,
+                    const double* z, int layout, double E, double nu, double p, double pmin,
+                    int64_t nfaces, const int32_t* faces, const double* flux,
+                    const int32_t* rowmap, const int32_t* cols, double* vals) {
+  Elastic m = make_elastic(E, nu, p, pmin);
+  std::memset(vals, 0, sizeof(double) * 9 * rowmap[N]);
+#pragma omp parallel for schedule(static)
+  for (int64_t c = 0; c < C; ++c) {
+    Dual<12> X[4][3], g[4][3], vol, ue[12], re[12];
+    double zc[4];
+    for (int n = 0; n < 4; ++n)
+      for (int d = 0; d < 3; ++d) {
+        X[n][d] = Dual<12>(coords[3 * int64_t(cells[4 * c + n]) + d]);
+        X[n][d].d[3 * n + d] = 1.0;
+      }
+    cell_gradients_t(X, g, vol);
+    for (int i = 0; i < 12; ++i) ue[i] = Dual<12>(u[3 * cells[4 * c + i / 3] + i % 3]);
+    load_zc(z, cells, c, layout, zc);
+    Dual<12> e[6], s[6], sw[6];
+    strain(g, ue, e);
+    stress(m, e, s);
+    double w = simp(m, cell_rho(zc, layout));
+    for (int i = 0; i < 6; ++i) sw[i] = s[i] * w;
+    for (int i = 0; i < 12; ++i) re[i] = Dual<12>(0.0);
+    divergence(g, vol, sw, re);
+    for (int a = 0; a < 4; ++a)       // config node (row)
+      for (int b = 0; b < 4; ++b) {   // state node (column)
+        int64_t k = find_entry(rowmap, cols, cells[4 * c + a], cells[4 * c + b]);
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) atomic_add(&vals[9 * k + 3 * i + j], re[3 * b + j].d[3 * a + i]);
+      }
+  }
+  for (int64_t f = 0; f < nfaces; ++f) {
+    const int32_t* v = faces + 3 * f;
+    Dual<9> a[3], b[3], cr[3], xs[3][3];
+    for (int n = 0; n < 3; ++n)
+      for (int d = 0; d < 3; ++d) { xs[n][d] = Dual<9>(coords[3 * v[n] + d]); xs[n][d].d[3 * n + d] = 1.0; }
+    for (int d = 0; d < 3; ++d) { a[d] = xs[0][d] - xs[2][d]; b[d] = xs[1][d] - xs[2][d]; }
+    cr[0] = a[1] * b[2] - a[2] * b[1]; cr[1] = a[2] * b[0] - a[0] * b[2]; cr[2] = a[0] * b[1] - a[1] * b[0];
+    Dual<9> w = (-1.0 / 6.0) * dsqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+    for (int an = 0; an < 3; ++an)
+      for (int bn = 0; bn < 3; ++bn) {
+        int64_t k = find_entry(rowmap, cols, v[an], v[bn]);
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) vals[9 * k + 3 * i + j] += w.d[3 * an + i] * flux[j];
+      }
+  }
+}
+
+// PhysicsScalarFunction::gradient_x for the internal energy: df/dx (3N).
+void pao_energy_grad_x(int64_t C, int64_t N, const int32_t* cells, const double* coords, const double* u,
+                       const double* z, int layout, double E, double nu, double p, double pmin, double* gx) {
+  Elastic m = make_elastic(E, nu, p, pmin);
+  std::memset(gx, 0, sizeof(double) * 3 * N);
+#pragma omp parallel for schedule(static)
+  for (int64_t c = 0; c < C; ++c) {
+    Dual<12> X[4][3], g[4][3], vol, ue[12];
+    double zc[4];
+    for (int n = 0; n < 4; ++n)
+      for (int d = 0; d < 3; ++d) {
+        X[n][d] = Dual<12>(coords[3 * int64_t(cells[4 * c + n]) + d]);
+        X[n][d].d[3 * n + d] = 1.0;
+      }
+    cell_gradients_t(X, g, vol);
+    for (int i = 0; i < 12; ++i) ue[i] = Dual<12>(u[3 * cells[4 * c + i / 3] + i % 3]);
+    load_zc(z, cells, c, layout, zc);
+    Dual<12> e[6], s[6], acc(0.0);
+    strain(g, ue, e);
+    stress(m, e, s);
+    double w = simp(m, cell_rho(zc, layout));
+    for (int i = 0; i < 6; ++i) acc += (s[i] * w) * e[i];
+    Dual<12> f = 0.5 * acc * vol;
+    for (int k = 0; k < 12; ++k) atomic_add(&gx[3 * int64_t(cells[4 * c + k / 3]) + k % 3], f.d[k]);
   }
 }
 

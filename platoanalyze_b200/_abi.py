@@ -63,9 +63,11 @@ SIGNATURES = [
     ("pa_vf_value", I32, [P, P, P, P]),
     ("pa_vf_gradient_u", I32, [P, P, P, P]),
     ("pa_vf_gradient_z", I32, [P, P, P, P]),
+    ("pa_vf_gradient_x", I32, [P, P, P, P]),
     ("pa_sf_value", I32, [P, P, P, P]),
     ("pa_sf_gradient_u", I32, [P, P, P, P]),
     ("pa_sf_gradient_z", I32, [P, P, P, P]),
+    ("pa_sf_gradient_x", I32, [P, P, P, P]),
     ("pa_sf_value_noalloc", I32, [P, I64, P, I64, P, P, ct.POINTER(ElasticParams), P, P]),
     ("pa_apply", I32, [P, P, P, P, I32, I32]),
     ("pa_apply_block_constraints", I32, [P, P, P, F64]),

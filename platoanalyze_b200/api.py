@@ -307,6 +307,18 @@ class VectorFunction:
         return out
 
 
+    def gradient_x(self, u, z, out=None):
+        """dR/dx transposed into block-CRS entries (VectorFunction::gradient_x)."""
+        u = _as(u, np.float64)
+        z = _as(z, np.float64)
+        n = 9 * self.p.mesh.num_blocks
+        out = _empty(u, n) if out is None else out
+        _abi.check(self.p._lib.pa_vf_gradient_x(self.p._h, _ptr(u, np.float64, self.p.ndof, "u"),
+                                                _ptr(z, np.float64, self.p.nz, "z"),
+                                                _ptr(out, np.float64, n, "entries")))
+        return out
+
+
 class PhysicsScalarFunction:
     """PhysicsScalarFunction for the "Internal Elastic Energy" criterion."""
 
@@ -337,4 +349,13 @@ class PhysicsScalarFunction:
         _abi.check(self.p._lib.pa_sf_gradient_z(self.p._h, _ptr(u, np.float64, self.p.ndof, "u"),
                                                 _ptr(z, np.float64, self.p.nz, "z"),
                                                 _ptr(out, np.float64, self.p.nz, "grad")))
+        return out
+
+    def gradient_x(self, u, z, out=None):
+        u = _as(u, np.float64)
+        z = _as(z, np.float64)
+        out = _empty(u, self.p.ndof) if out is None else out
+        _abi.check(self.p._lib.pa_sf_gradient_x(self.p._h, _ptr(u, np.float64, self.p.ndof, "u"),
+                                                _ptr(z, np.float64, self.p.nz, "z"),
+                                                _ptr(out, np.float64, self.p.ndof, "grad")))
         return out

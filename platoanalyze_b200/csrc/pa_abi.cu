@@ -16,6 +16,8 @@ void launch_dRdz_transpose_times(const Problem& P, const double* u, const double
                                  double* g, cudaStream_t s);
 void launch_block_constraints(const Problem& P, double* entries, double* rhs, double scale, cudaStream_t s);
 void launch_scale(double* v, int64_t n, double a, cudaStream_t s);
+void launch_gradient_x(const Problem& P, const double* u, const double* z, double* entries, cudaStream_t s);
+void launch_energy_grad_x(const Problem& P, const double* u, const double* z, double* gx, cudaStream_t s);
 double time_cg_apply(Problem& P, const double* z, bool fp32, int reps);
 
 namespace {
@@ -416,6 +418,31 @@ pa_status pa_vf_gradient_z(pa_problem* problem, const double* u, const double* z
     const int64_t n = P.ep.layout == PA_CONTROL_CELL ? 12 * P.C() : 3 * P.mesh->B;
     double* de = st.out(entries, n, "entries");
     pa::launch_gradient_z(P, du, dz, de, P.stream);
+    st.finish();
+  });
+}
+
+pa_status pa_vf_gradient_x(pa_problem* problem, const double* u, const double* z, double* entries) {
+  return guard([&] {
+    Problem& P = prob(problem);
+    if (!P.mesh->d_cell_entry.n) P.mesh->build_graph_entries();
+    pa::Stage st(P);
+    const double* du = st.in(u, P.ndof(), "u");
+    const double* dz = st.in(z, P.nz(), "z");
+    double* de = st.out(entries, 9 * P.mesh->B, "entries");
+    pa::launch_gradient_x(P, du, dz, de, P.stream);
+    st.finish();
+  });
+}
+
+pa_status pa_sf_gradient_x(pa_problem* problem, const double* u, const double* z, double* grad) {
+  return guard([&] {
+    Problem& P = prob(problem);
+    pa::Stage st(P);
+    const double* du = st.in(u, P.ndof(), "u");
+    const double* dz = st.in(z, P.nz(), "z");
+    double* dg = st.out(grad, P.ndof(), "grad");
+    pa::launch_energy_grad_x(P, du, dz, dg, P.stream);
     st.finish();
   });
 }

@@ -301,6 +301,125 @@ __global__ void k_scale(double* __restrict__ v, int64_t n, double a) {
     v[i] *= a;
 }
 
+// ------------------------------------------------------------ gradient_x --
+// Configuration derivatives by forward-mode directional differentiation: each
+// of the 12 coordinate dofs of a cell is seeded in turn on a one-partial dual
+// number D1, so the per-cell chain of pa_cell.cuh is reused unchanged.
+struct D1 {
+  double v, d;
+  __device__ D1() : v(0.0), d(0.0) {}
+  __device__ D1(double x) : v(x), d(0.0) {}
+  __device__ D1(double x, double dx) : v(x), d(dx) {}
+};
+__device__ __forceinline__ D1 operator+(D1 a, D1 b) { return D1(a.v + b.v, a.d + b.d); }
+__device__ __forceinline__ D1 operator-(D1 a, D1 b) { return D1(a.v - b.v, a.d - b.d); }
+__device__ __forceinline__ D1 operator-(D1 a) { return D1(-a.v, -a.d); }
+__device__ __forceinline__ D1 operator*(D1 a, D1 b) { return D1(a.v * b.v, a.d * b.v + a.v * b.d); }
+__device__ __forceinline__ D1 operator/(D1 a, D1 b) { return D1(a.v / b.v, (a.d * b.v - a.v * b.d) / (b.v * b.v)); }
+__device__ __forceinline__ D1& operator+=(D1& a, D1 b) { a = a + b; return a; }
+__device__ __forceinline__ D1 fabs(D1 a) { return a.v < 0.0 ? -a : a; }
+__device__ __forceinline__ D1 sqrt(D1 a) {
+  const double r = ::sqrt(a.v);
+  return D1(r, a.d / (2.0 * r));
+}
+
+// dR/dx transposed into the block CRS: block (row = node of coordinate dof k,
+// col = node of residual dof i), entry [k % 3][i % 3]
+// (VectorFunction::gradient_x, src/elliptic/VectorFunction.hpp:317-408).
+__global__ void k_gradient_x(CellIn m, Mat64 mat, const double* __restrict__ u, const double* __restrict__ z,
+                             const int32_t* __restrict__ cell_entry, double* __restrict__ vals) {
+  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (c >= m.C) return;
+  int v[4];
+  double x0[4][3], ue0[12];
+  load_cell(m, c, v, x0);
+  load_u(u, v, ue0);
+  const double w = simp(cell_density(z, mat.layout, c, v), mat.p, mat.pmin);
+  const Iso<D1> iso{D1(mat.iso.lam), D1(mat.iso.mu)};
+  for (int k = 0; k < 12; ++k) {
+    D1 x[4][3], g[4][3], vol, ue[12], e[6], sig[6], re[12];
+#pragma unroll
+    for (int n = 0; n < 4; ++n)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) x[n][d] = D1(x0[n][d], (3 * n + d == k) ? 1.0 : 0.0);
+#pragma unroll
+    for (int i = 0; i < 12; ++i) ue[i] = D1(ue0[i]);
+    tet_geometry(x, g, vol);
+    tet_strain(g, ue, e);
+    tet_stress(iso, vol * D1(w), e, sig);
+    tet_divergence(g, sig, re);
+    const int a = k / 3, ka = k % 3;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      double* dst = vals + 9 * int64_t(cell_entry[16 * c + 4 * a + b]) + 3 * ka;
+#pragma unroll
+      for (int j = 0; j < 3; ++j) atomicAdd(&dst[j], re[3 * b + j].d);
+    }
+  }
+}
+
+__device__ __forceinline__ int64_t find_block(const int32_t* __restrict__ rowmap, const int32_t* __restrict__ cols,
+                                              int32_t row, int32_t col) {
+  for (int32_t k = rowmap[row]; k < rowmap[row + 1]; ++k)
+    if (cols[k] == col) return k;
+  return -1;
+}
+
+// Surface load's dependence on the face area, scale -1 (SurfaceLoadIntegral,
+// src/SurfaceLoadIntegral.hpp:96-160): weight = -(1/6)|(x0-x2) x (x1-x2)|.
+__global__ void k_traction_x(const int32_t* __restrict__ faces, const double* __restrict__ flux, int64_t nf,
+                             const double* __restrict__ coords, const int32_t* __restrict__ rowmap,
+                             const int32_t* __restrict__ cols, double* __restrict__ vals) {
+  const int64_t f = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (f >= nf) return;
+  const int32_t vs[3] = {faces[3 * f], faces[3 * f + 1], faces[3 * f + 2]};
+  for (int k = 0; k < 9; ++k) {
+    D1 xs[3][3];
+    for (int n = 0; n < 3; ++n)
+      for (int d = 0; d < 3; ++d) xs[n][d] = D1(coords[3 * int64_t(vs[n]) + d], (3 * n + d == k) ? 1.0 : 0.0);
+    D1 a[3], b[3];
+    for (int d = 0; d < 3; ++d) {
+      a[d] = xs[0][d] - xs[2][d];
+      b[d] = xs[1][d] - xs[2][d];
+    }
+    const D1 cx = a[1] * b[2] - a[2] * b[1], cy = a[2] * b[0] - a[0] * b[2], cz = a[0] * b[1] - a[1] * b[0];
+    const D1 wgt = D1(-1.0 / 6.0) * sqrt(cx * cx + cy * cy + cz * cz);
+    const int an = k / 3, ka = k % 3;
+    for (int bn = 0; bn < 3; ++bn) {
+      const int64_t e = find_block(rowmap, cols, vs[an], vs[bn]);
+      if (e < 0) continue;
+      for (int j = 0; j < 3; ++j) atomicAdd(&vals[9 * e + 3 * ka + j], wgt.d * flux[3 * f + j]);
+    }
+  }
+}
+
+// df/dx of the internal energy (PhysicsScalarFunction::gradient_x).
+__global__ void k_energy_grad_x(CellIn m, Mat64 mat, const double* __restrict__ u, const double* __restrict__ z,
+                                double* __restrict__ gx) {
+  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (c >= m.C) return;
+  int v[4];
+  double x0[4][3], ue0[12];
+  load_cell(m, c, v, x0);
+  load_u(u, v, ue0);
+  const double w = simp(cell_density(z, mat.layout, c, v), mat.p, mat.pmin);
+  const Iso<D1> iso{D1(mat.iso.lam), D1(mat.iso.mu)};
+  for (int k = 0; k < 12; ++k) {
+    D1 x[4][3], g[4][3], vol, ue[12], e[6], sig[6];
+#pragma unroll
+    for (int n = 0; n < 4; ++n)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) x[n][d] = D1(x0[n][d], (3 * n + d == k) ? 1.0 : 0.0);
+#pragma unroll
+    for (int i = 0; i < 12; ++i) ue[i] = D1(ue0[i]);
+    tet_geometry(x, g, vol);
+    tet_strain(g, ue, e);
+    tet_stress(iso, vol * D1(w), e, sig);
+    const D1 f = D1(0.5) * voigt_dot(sig, e);
+    atomicAdd(&gx[3 * int64_t(v[k / 3]) + k % 3], f.d);
+  }
+}
+
 CellIn cell_in(const Problem& P) { return CellIn{P.mesh->d_cells.get(), P.mesh->d_coords.get(), P.mesh->C}; }
 Mat64 mat64(const Problem& P) { return Mat64{P.ep.iso(), P.ep.p, P.ep.pmin, P.ep.layout}; }
 
@@ -369,6 +488,24 @@ void launch_block_constraints(const Problem& P, double* entries, double* rhs, do
                                                 P.mesh->d_rowmap.get(), P.mesh->d_cols.get(), entries, rhs);
   PA_LAUNCHED();
   k_bc_second<<<grid_for(nbc), kThreads, 0, s>>>(nbc, P.d_bc_dofs.get(), P.d_bc_vals.get(), scale, rhs);
+  PA_LAUNCHED();
+}
+
+void launch_gradient_x(const Problem& P, const double* u, const double* z, double* entries, cudaStream_t s) {
+  PA_CUDA(cudaMemsetAsync(entries, 0, sizeof(double) * 9 * P.mesh->B, s));
+  k_gradient_x<<<grid_for(P.C(), 128), 128, 0, s>>>(cell_in(P), mat64(P), u, z, P.mesh->d_cell_entry.get(), entries);
+  PA_LAUNCHED();
+  const int64_t nf = int64_t(P.faces.size() / 3);
+  if (nf) {
+    k_traction_x<<<grid_for(nf), kThreads, 0, s>>>(P.d_faces.get(), P.d_face_flux.get(), nf, P.mesh->d_coords.get(),
+                                                   P.mesh->d_rowmap.get(), P.mesh->d_cols.get(), entries);
+    PA_LAUNCHED();
+  }
+}
+
+void launch_energy_grad_x(const Problem& P, const double* u, const double* z, double* gx, cudaStream_t s) {
+  PA_CUDA(cudaMemsetAsync(gx, 0, sizeof(double) * P.ndof(), s));
+  k_energy_grad_x<<<grid_for(P.C(), 128), 128, 0, s>>>(cell_in(P), mat64(P), u, z, gx);
   PA_LAUNCHED();
 }
 

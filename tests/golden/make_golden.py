@@ -22,6 +22,10 @@ of a 0/1 integer program (scipy.optimize.milp): a bijection from the 27 grid
 points to vertex ids such that K(perm) u equals the 81 gold residual values.
 The fixture records the permutation found, so tests never need the search.
 
+The residual, Jacobian and energy gold are also invariant under the point
+reflection x -> 1 - x, which the configuration gradient is not; the
+orientation is taken from the sign of the first gold gradient_x entry.
+
 The gold Jacobian and dR/dz arrays are raw block-CRS entry arrays whose
 in-row column order is Omega_h's node-star order (not sorted).  Only row 0
 is covered by the gold (45 and 24 entries); its column order is recovered by
@@ -85,6 +89,27 @@ def identify_numbering(R_gold):
     return v_cells.astype(np.int32), v_coords
 
 
+def choose_orientation(cells, coords, gold_dRdx00):
+    """The residual, Jacobian and energy gold are invariant under the point
+    reflection x -> 1 - x of the box (gradients flip sign, B^T C B does not),
+    so the integer program cannot tell the two numberings apart; the
+    configuration gradient can.  Keep the orientation whose dR_0x/dx_0x (the
+    first gold gradient_x entry; node 0 is its own row-0 column) has the gold's
+    sign, checked by a central difference."""
+    u = 1e-4 * np.arange(1, 3 * coords.shape[0] + 1, dtype=np.float64)
+    z = np.ones(coords.shape[0])
+    h = 1e-6
+    cp, cm = coords.copy(), coords.copy()
+    cp[0, 0] += h
+    cm[0, 0] -= h
+    rp = np_ref.Problem(cells, cp, E=1e6, nu=0.3, p=1.0, pmin=0.0).value(u, z)
+    rm = np_ref.Problem(cells, cm, E=1e6, nu=0.3, p=1.0, pmin=0.0).value(u, z)
+    fd = (rp[0] - rm[0]) / (2 * h)
+    if np.sign(fd) != np.sign(gold_dRdx00):
+        coords = 1.0 - coords
+    return cells, coords
+
+
 def star_order_row0(blocks_gold, Kfull, cols_sorted, bi, bj):
     """Column order of row 0 that reproduces the gold block sequence."""
     order = []
@@ -111,6 +136,7 @@ def derivative_tests():
         "energy_grad_x": grab(src, "grad_x_gold", s1),
     }
     cells, coords = identify_numbering(gold["residual"])
+    cells, coords = choose_orientation(cells, coords, gold["gradient_x_entries"][0])
     prob = np_ref.Problem(cells, coords, E=1e6, nu=0.3, p=1.0, pmin=0.0)
     z = np.ones(27)
     u = 1e-4 * np.arange(1, 82, dtype=np.float64)

@@ -53,3 +53,20 @@ def test_self_adjoint_criterion_gradient_is_minus_partial(golden):
     d, mesh, prob, u, z = golden
     g = prob.criterion_gradient(z, u, self_adjoint=True)
     floating_equality(-g, d["gold"]["energy_grad_z"], 1e-13)
+
+
+def test_elastostatic_gradient_x_3d_reference_column_order(golden):
+    d, mesh, prob, u, z = golden
+    rowmap, cols = mesh.graph()
+    mesh.set_graph(*star_graph(rowmap, cols, d["row0_star_order"]))
+    try:
+        gold = d["gold"]["gradient_x_entries"]
+        floating_equality(prob.vector_function().gradient_x(u, z)[:len(gold)], gold,
+                          d["tolerances"]["gradient_x_entries"])
+    finally:
+        mesh.set_graph(rowmap, cols)
+
+
+def test_internal_elastic_energy_3d_gradient_x(golden):
+    d, mesh, prob, u, z = golden
+    floating_equality(prob.scalar_function().gradient_x(u, z), d["gold"]["energy_grad_x"], 1e-13)

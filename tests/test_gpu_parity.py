@@ -81,6 +81,15 @@ def test_gradient_z(setup):
     assert rel_inf(G, ref) < RTOL64
 
 
+def test_gradient_x(setup):
+    s = setup
+    G = s["prob"].vector_function().gradient_x(s["u"], s["z"])
+    ref = s["O"].gradient_x(s["u"], s["z"], s["faces"], s["flux"], s["mesh"].graph())
+    assert rel_inf(G, ref) < RTOL64
+    gx = s["prob"].scalar_function().gradient_x(s["u"], s["z"])
+    assert rel_inf(gx, s["O"].energy_grad_x(s["u"], s["z"])) < RTOL64
+
+
 def test_energy(setup):
     s = setup
     sf = s["prob"].scalar_function()

@@ -112,3 +112,32 @@ def test_oracle_gradients_match_finite_differences(oracle_lib):
     du = rng.standard_normal(3 * O.N)
     fd = (O.energy(u + h * du, z, grads=False) - O.energy(u - h * du, z, grads=False)) / (2 * h)
     assert abs(fd - gu @ du) <= 1e-7 * abs(fd)
+
+
+def test_elastostatic_residual_3d_gradient_x(case):
+    d, O, u, z = case
+    graph = star_graph(*O.graph(), d["row0_star_order"])
+    vals = O.gradient_x(u, z, graph=graph)
+    gold = d["gold"]["gradient_x_entries"]
+    floating_equality(vals[:len(gold)], gold, d["tolerances"]["gradient_x_entries"])
+
+
+def test_internal_elastic_energy_3d_gradient_x(case):
+    d, O, u, z = case
+    floating_equality(O.energy_grad_x(u, z), d["gold"]["energy_grad_x"], 1e-13)
+
+
+def test_oracle_gradient_x_matches_finite_differences(oracle_lib):
+    from oracle import np_ref
+    rng = np.random.default_rng(11)
+    cells, coords = np_ref.box_mesh(2, 1, 1, 2.0, 1.0, 1.0)
+    coords = coords + 0.05 * rng.standard_normal(coords.shape)
+    O = oracle_lib.Oracle(cells, coords, E=1.0, nu=0.3, p=3.0, pmin=1e-9)
+    u = rng.standard_normal(3 * O.N)
+    z = rng.uniform(0.3, 1.0, O.N)
+    gx = O.energy_grad_x(u, z)
+    dx = rng.standard_normal(coords.shape)
+    h = 1e-6
+    fp = oracle_lib.Oracle(cells, coords + h * dx, E=1.0, nu=0.3, p=3.0, pmin=1e-9).energy(u, z, grads=False)
+    fm = oracle_lib.Oracle(cells, coords - h * dx, E=1.0, nu=0.3, p=3.0, pmin=1e-9).energy(u, z, grads=False)
+    assert abs((fp - fm) / (2 * h) - gx @ dx.ravel()) <= 1e-6 * abs(gx @ dx.ravel())
