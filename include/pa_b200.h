@@ -264,6 +264,40 @@ typedef struct {
 pa_status pa_j2_radial_return(pa_problem* problem, const pa_j2_params* params, const double* u, const double* z,
                               const double* prev_local, double* local);
 
+/* J2 local residual: J2PlasticityLocalResidual::evaluate
+ * (src/J2PlasticityLocalResidual.hpp:291-409), 14 equations per cell at local
+ * states `local` (current) and `prev_local`; u: 3N, z: N nodal; residual: C x 14. */
+pa_status pa_j2_local_residual(pa_problem* problem, const pa_j2_params* params, const double* u, const double* z,
+                               const double* local, const double* prev_local, double* residual);
+
+typedef struct {
+  int32_t steps;       /* pseudo-time load steps; Dirichlet values ramp as (k+1)/steps */
+  int32_t max_newton;  /* Newton iterations per step */
+  double newton_tol;   /* ||R_free|| <= newton_tol * (||R_free|| at the step's first iteration) */
+} pa_j2_solve_options;
+
+typedef struct {
+  int32_t steps;
+  int32_t newton_iterations;  /* tangent solves over all steps */
+  int64_t cg_iterations;      /* PCG iterations over all tangent solves */
+  double seconds;             /* device time */
+  double final_rel_residual;  /* relative Newton residual of the last step */
+  int32_t converged;
+} pa_j2_stats;
+
+/* Elasto-plastic solve, displacement-form small-strain J2 with linear
+ * isotropic/kinematic hardening: load steps over the problem's Dirichlet
+ * values (the final values), Newton with per-cell radial return (FP64) and the
+ * consistent tangent applied matrix-free inside the problem's PCG
+ * (`linear`: FP64 or mixed).  Replaces PlasticityProblem::solution's forward
+ * solve (src/PlasticityProblem.hpp:352, :791-846) with
+ * NewtonRaphsonSolver::solve (src/NewtonRaphsonSolver.hpp:570-640); the
+ * reference's global residual is the stabilized u-p form, this one the
+ * displacement form.  Outputs u (3N) and the final local states (C x 14). */
+pa_status pa_j2_solve(pa_problem* problem, const pa_j2_params* params, const double* z,
+                      const pa_j2_solve_options* options, const pa_solve_options* linear, double* u, double* local,
+                      pa_j2_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -43,6 +43,15 @@ class J2Params(ct.Structure):
                 ("plastic_penalty_exponent", F64), ("plastic_min_ersatz", F64)]
 
 
+class J2SolveOptions(ct.Structure):
+    _fields_ = [("steps", I32), ("max_newton", I32), ("newton_tol", F64)]
+
+
+class J2Stats(ct.Structure):
+    _fields_ = [("steps", I32), ("newton_iterations", I32), ("cg_iterations", I64), ("seconds", F64),
+                ("final_rel_residual", F64), ("converged", I32)]
+
+
 # (name, restype, argtypes) for every symbol of include/pa_b200.h
 SIGNATURES = [
     ("pa_version", ct.c_char_p, []),
@@ -77,6 +86,9 @@ SIGNATURES = [
     ("pa_problem_criterion_gradient", I32, [P, P, P, P, I32, ct.POINTER(SolveOptions)]),
     ("pa_time_cg_apply", I32, [P, P, I32, I32, P, P]),
     ("pa_j2_radial_return", I32, [P, ct.POINTER(J2Params), P, P, P, P]),
+    ("pa_j2_local_residual", I32, [P, ct.POINTER(J2Params), P, P, P, P, P]),
+    ("pa_j2_solve", I32, [P, ct.POINTER(J2Params), P, ct.POINTER(J2SolveOptions), ct.POINTER(SolveOptions), P, P,
+                          ct.POINTER(J2Stats)]),
 ]
 
 _lib = None

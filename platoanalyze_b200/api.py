@@ -244,15 +244,53 @@ class Problem:
         z = _as(z, np.float64)
         C = self.mesh.num_cells
         local = _empty(u, 14 * C) if local is None else local
-        jp = _abi.J2Params(*[float(params[k]) for k in (
-            "youngs_modulus", "poissons_ratio", "initial_yield_stress", "hardening_modulus_isotropic",
-            "hardening_modulus_kinematic", "elastic_penalty_exponent", "elastic_min_ersatz",
-            "plastic_penalty_exponent", "plastic_min_ersatz")])
+        jp = self._j2_params(params)
         _abi.check(self._lib.pa_j2_radial_return(self._h, ct.byref(jp), _ptr(u, np.float64, self.ndof),
                                                  _ptr(z, np.float64, self.mesh.num_nodes),
                                                  _ptr(prev_local, np.float64, 14 * C, "prev_local"),
                                                  _ptr(local, np.float64, 14 * C, "local")))
         return local
+
+    @staticmethod
+    def _j2_params(params):
+        return _abi.J2Params(*[float(params[k]) for k in (
+            "youngs_modulus", "poissons_ratio", "initial_yield_stress", "hardening_modulus_isotropic",
+            "hardening_modulus_kinematic", "elastic_penalty_exponent", "elastic_min_ersatz",
+            "plastic_penalty_exponent", "plastic_min_ersatz")])
+
+    def j2_local_residual(self, params, u, z, local, prev_local, out=None):
+        """J2PlasticityLocalResidual::evaluate for every cell (C x 14)."""
+        C = self.mesh.num_cells
+        u, z = _as(u, np.float64), _as(z, np.float64)
+        local, prev_local = _as(local, np.float64), _as(prev_local, np.float64)
+        out = _empty(u, 14 * C) if out is None else out
+        jp = self._j2_params(params)
+        _abi.check(self._lib.pa_j2_local_residual(self._h, ct.byref(jp), _ptr(u, np.float64, self.ndof, "u"),
+                                                  _ptr(z, np.float64, self.mesh.num_nodes, "z"),
+                                                  _ptr(local, np.float64, 14 * C, "local"),
+                                                  _ptr(prev_local, np.float64, 14 * C, "prev_local"),
+                                                  _ptr(out, np.float64, 14 * C, "residual")))
+        return out
+
+    def j2_solve(self, params, z, steps=20, max_newton=25, newton_tol=1e-8, options=None, u=None, local=None,
+                 allow_not_converged=False):
+        """Load-stepped Newton solve of the J2 problem (pa_j2_solve); the
+        problem's Dirichlet values are the final prescribed displacements."""
+        C = self.mesh.num_cells
+        z = _as(z, np.float64)
+        u = _empty(z, self.ndof) if u is None else u
+        local = _empty(z, 14 * C) if local is None else local
+        jp = self._j2_params(params)
+        jo = _abi.J2SolveOptions(int(steps), int(max_newton), float(newton_tol))
+        lo = (options or SolveOptions("mixed", rel_tol=1e-8)).c()
+        js = _abi.J2Stats()
+        status = self._lib.pa_j2_solve(self._h, ct.byref(jp), _ptr(z, np.float64, self.mesh.num_nodes, "z"),
+                                       ct.byref(jo), ct.byref(lo), _ptr(u, np.float64, self.ndof, "u"),
+                                       _ptr(local, np.float64, 14 * C, "local"), ct.byref(js))
+        _abi.check(status, allow=(3,) if allow_not_converged else ())
+        return u, local, {"steps": js.steps, "newton_iterations": js.newton_iterations,
+                          "cg_iterations": js.cg_iterations, "seconds": js.seconds,
+                          "final_rel_residual": js.final_rel_residual, "converged": bool(js.converged)}
 
     def close(self):
         if self._h:

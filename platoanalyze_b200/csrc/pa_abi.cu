@@ -19,6 +19,10 @@ void launch_scale(double* v, int64_t n, double a, cudaStream_t s);
 void launch_gradient_x(const Problem& P, const double* u, const double* z, double* entries, cudaStream_t s);
 void launch_energy_grad_x(const Problem& P, const double* u, const double* z, double* gx, cudaStream_t s);
 double time_cg_apply(Problem& P, const double* z, bool fp32, int reps);
+void launch_j2_local_residual(const Problem& P, const pa_j2_params& jp, const double* u, const double* z,
+                              const double* loc, const double* prev, double* H, cudaStream_t s);
+pa_status j2_solve(Problem& P, const pa_j2_params& jp, const double* z, const pa_j2_solve_options& jo,
+                   const pa_solve_options& lo, double* u, double* local, pa_j2_stats* js);
 
 namespace {
 thread_local std::string g_last_error;
@@ -655,6 +659,43 @@ pa_status pa_time_cg_apply(pa_problem* problem, const double* z, int32_t precisi
       *algorithmic_bytes = P.C() * (16 + sv) + P.N() * (3 * sv) * 6;
     }
     st.finish();
+  });
+}
+
+pa_status pa_j2_local_residual(pa_problem* problem, const pa_j2_params* params, const double* u, const double* z,
+                               const double* local, const double* prev_local, double* residual) {
+  return guard([&] {
+    Problem& P = prob(problem);
+    PA_CHECK(params, "null J2 parameters");
+    pa::Stage st(P);
+    const double* du = st.in(u, P.ndof(), "u");
+    const double* dz = st.in(z, P.N(), "z");
+    const double* dl = st.in(local, 14 * P.C(), "local");
+    const double* dp = st.in(prev_local, 14 * P.C(), "prev_local");
+    double* dh = st.out(residual, 14 * P.C(), "residual");
+    pa::launch_j2_local_residual(P, *params, du, dz, dl, dp, dh, P.stream);
+    st.finish();
+  });
+}
+
+pa_status pa_j2_solve(pa_problem* problem, const pa_j2_params* params, const double* z,
+                      const pa_j2_solve_options* options, const pa_solve_options* linear, double* u, double* local,
+                      pa_j2_stats* stats) {
+  return pa::guard_status([&] {
+    Problem& P = prob(problem);
+    PA_CHECK(params && options, "null J2 parameters or options");
+    PA_CHECK(params->youngs_modulus > 0 && params->initial_yield_stress > 0, "J2 moduli must be positive");
+    pa_solve_options lo;
+    pa_solve_options_default(&lo);
+    if (linear) lo = *linear;
+    lo.use_initial_guess = 0;
+    pa::Stage st(P);
+    const double* dz = st.in(z, P.N(), "z");
+    double* du = st.out(u, P.ndof(), "u");
+    double* dl = st.out(local, 14 * P.C(), "local");
+    pa_status s = pa::j2_solve(P, *params, dz, *options, lo, du, dl, stats);
+    st.finish();
+    return s;
   });
 }
 

@@ -515,8 +515,10 @@ void launch_scale(double* v, int64_t n, double a, cudaStream_t s) {
 }
 
 template <typename T>
-void launch_apply_tiled(const Problem& P, const T* w, const T* x, T* y, bool constrained, cudaStream_t s) {
+void launch_apply_tiled(const Problem& P, const T* w, const T* x, T* y, bool constrained, cudaStream_t s,
+                        const T* plas) {
   ApplyArgs<T> a{};
+  a.plas = plas;
   a.tv = P.mesh->tiles();
   a.tile_nodes = constrained ? P.d_tile_nodes_bc.get() : P.mesh->d_tile_nodes.get();
   a.N = P.N();
@@ -576,7 +578,9 @@ template void launch_soa_to_aos<float, float>(const float*, float*, int64_t, cud
 template void launch_copy_dofs<double>(const int32_t*, int64_t, const double*, double*, cudaStream_t);
 template void launch_copy_dofs<float>(const int32_t*, int64_t, const float*, float*, cudaStream_t);
 
-template void launch_apply_tiled<double>(const Problem&, const double*, const double*, double*, bool, cudaStream_t);
-template void launch_apply_tiled<float>(const Problem&, const float*, const float*, float*, bool, cudaStream_t);
+template void launch_apply_tiled<double>(const Problem&, const double*, const double*, double*, bool, cudaStream_t,
+                                         const double*);
+template void launch_apply_tiled<float>(const Problem&, const float*, const float*, float*, bool, cudaStream_t,
+                                        const float*);
 
 }  // namespace pa

@@ -106,6 +106,7 @@ struct Mesh {
   int64_t num_clusters = 0, num_hex = 0;
   int tile_clusters = 128;  // clusters per tile (threads per CTA); a tile touches <= 2x as many nodes
   DevBuf<int32_t> d_tile_cluster_start, d_tile_cell_start, d_tile_hex_count, d_tile_node_start, d_cell_perm;
+  DevBuf<int32_t> d_cell_iperm;  // user -> internal cell id
   DevBuf<uint32_t> d_tile_nodes;
   DevBuf<uint4> d_cluster_nodes;
   std::vector<int32_t> h_cell_perm;  // internal -> user
@@ -163,7 +164,8 @@ void launch_cell_weights(const Problem& P, const double* z, double* w64, float* 
 // y = K x with the tile kernel on component-major (SoA) vectors;
 // constrained = mask the problem's Dirichlet dofs.
 template <typename T>
-void launch_apply_tiled(const Problem& P, const T* w, const T* x, T* y, bool constrained, cudaStream_t s);
+void launch_apply_tiled(const Problem& P, const T* w, const T* x, T* y, bool constrained, cudaStream_t s,
+                        const T* plas = nullptr);
 // interleaved (AoS, the ABI's layout) <-> component-major (SoA) copies
 template <typename S, typename T>
 void launch_aos_to_soa(const S* aos, T* soa, int64_t N, cudaStream_t s);

@@ -9,6 +9,9 @@
 // the 14-double local states are staged through shared memory so that both
 // the load of the previous state and the store of the new one are coalesced.
 #include "pa_problem.cuh"
+#include <algorithm>
+#include <cmath>
+
 #include "pa_cell.cuh"
 
 namespace pa {
@@ -91,22 +94,364 @@ __global__ void __launch_bounds__(kJ2Threads) k_j2(const int32_t* __restrict__ c
   for (int i = threadIdx.x; i < nloc * kLocal; i += kJ2Threads) cur[c0 * kLocal + i] = s_state[i];
 }
 
+struct J2Full {
+  J2Dev p;
+  double kappa;  // bulk modulus E / (3 (1 - 2 nu))
+  double lam;    // Lame lambda (for the tile kernel's iso parameters)
+};
+
+// One cell's return mapping from `st` (previous local state, updated in
+// place) at total strain e; outputs the new stress (Voigt, tensor shears),
+// the tangent record {n(6), theta1, theta2} and the elastic penalty.
+__device__ __forceinline__ void j2_cell(const J2Full& q, double rho, const double e[6], double st[14],
+                                        double sig[6], double rec[8], double& pe) {
+  pe = simp(rho, q.p.pe, q.p.pe_min);
+  const double mu_p = pe * q.p.mu;
+  const double ppen = simp(rho, q.p.pp, q.p.pp_min);
+  const double hi = ppen * q.p.hiso, hk = ppen * q.p.hkin;
+  const double eqps_prev = st[0];
+  double ee[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) ee[i] = e[i] - st[2 + i];
+  double tr3 = (ee[0] + ee[1] + ee[2]) / 3.0;
+  double n[6] = {2.0 * mu_p * (ee[0] - tr3), 2.0 * mu_p * (ee[1] - tr3), 2.0 * mu_p * (ee[2] - tr3),
+                 mu_p * ee[3], mu_p * ee[4], mu_p * ee[5]};
+#pragma unroll
+  for (int i = 0; i < 6; ++i) n[i] -= st[8 + i];
+  const double norm = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2] + 2.0 * (n[3] * n[3] + n[4] * n[4] + n[5] * n[5]));
+  const double sy = ppen * q.p.sy0 + hi * eqps_prev;
+  const double s32 = 1.2247448713915890491, s23 = 0.81649658092772603273;
+  const double ftr = s32 * norm - sy;
+  st[1] = 0.0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) rec[i] = 0.0;
+  if (ftr > 1.0e-10) {
+    const double dg = ftr / (3.0 * mu_p + hi + hk);
+    st[1] = dg;
+    st[0] = eqps_prev + dg;
+    const double inv = 1.0 / norm;
+    const double m1 = dg * s32 * inv, m2 = dg * s23 * hk * inv;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) st[2 + i] += m1 * n[i];
+#pragma unroll
+    for (int i = 3; i < 6; ++i) st[2 + i] += 2.0 * m1 * n[i];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      st[8 + i] += m2 * n[i];
+      rec[i] = n[i] * inv;
+    }
+    rec[6] = 2.449489742783178098 * mu_p * dg * inv;  // theta1 = sqrt(6) mu_p dgamma / |eta_trial|
+    rec[7] = 3.0 * mu_p / (3.0 * mu_p + hi + hk);      // theta2
+  }
+  // stress at the returned state: kappa_p tr(e) 1 + 2 mu_p dev(e - eps_p)
+#pragma unroll
+  for (int i = 0; i < 6; ++i) ee[i] = e[i] - st[2 + i];
+  tr3 = (ee[0] + ee[1] + ee[2]) / 3.0;
+  const double ptr = pe * q.kappa * (e[0] + e[1] + e[2]);
+  sig[0] = ptr + 2.0 * mu_p * (ee[0] - tr3);
+  sig[1] = ptr + 2.0 * mu_p * (ee[1] - tr3);
+  sig[2] = ptr + 2.0 * mu_p * (ee[2] - tr3);
+  sig[3] = mu_p * ee[3];
+  sig[4] = mu_p * ee[4];
+  sig[5] = mu_p * ee[5];
+}
+
+// Newton residual of the displacement form: R += vol B^T sigma(u) after the
+// return mapping from `prev`; writes the new local states, the per-cell tangent
+// records and elastic penalties in tile order (FP64 and FP32).
+__global__ void __launch_bounds__(kJ2Threads) k_j2_newton(const int32_t* __restrict__ cells,
+                                                          const double* __restrict__ coords, int64_t C, J2Full q,
+                                                          const double* __restrict__ u, const double* __restrict__ z,
+                                                          const double* __restrict__ prev, double* __restrict__ cur,
+                                                          const int32_t* __restrict__ iperm, double* __restrict__ rec64,
+                                                          float* __restrict__ rec32, double* __restrict__ w64,
+                                                          float* __restrict__ w32, double* __restrict__ R) {
+  __shared__ double s_state[kJ2Threads * kLocal];
+  const int64_t c0 = int64_t(blockIdx.x) * kJ2Threads;
+  const int nloc = int((C - c0) < int64_t(kJ2Threads) ? (C - c0) : int64_t(kJ2Threads));
+  for (int i = threadIdx.x; i < nloc * kLocal; i += kJ2Threads) s_state[i] = prev[c0 * kLocal + i];
+  __syncthreads();
+  if (threadIdx.x < nloc) {
+    const int64_t c = c0 + threadIdx.x;
+    const int4 qv = reinterpret_cast<const int4*>(cells)[c];
+    const int v[4] = {qv.x, qv.y, qv.z, qv.w};
+    double x[4][3], ue[12], g[4][3], vol, e[6], sig[6], rec[8], pe, re[12];
+#pragma unroll
+    for (int n = 0; n < 4; ++n)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        x[n][d] = __ldg(&coords[3 * int64_t(v[n]) + d]);
+        ue[3 * n + d] = __ldg(&u[3 * int64_t(v[n]) + d]);
+      }
+    tet_geometry(x, g, vol);
+    tet_strain(g, ue, e);
+    const double rho = 0.25 * (__ldg(&z[v[0]]) + __ldg(&z[v[1]]) + __ldg(&z[v[2]]) + __ldg(&z[v[3]]));
+    j2_cell(q, rho, e, s_state + threadIdx.x * kLocal, sig, rec, pe);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) sig[i] *= vol;
+    tet_divergence(g, sig, re);
+#pragma unroll
+    for (int n = 0; n < 4; ++n)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) atomicAdd(&R[3 * int64_t(v[n]) + d], re[3 * n + d]);
+    const int64_t ic = iperm[c];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      rec64[8 * ic + i] = rec[i];
+      rec32[8 * ic + i] = float(rec[i]);
+    }
+    w64[ic] = pe;
+    w32[ic] = float(pe);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nloc * kLocal; i += kJ2Threads) cur[c0 * kLocal + i] = s_state[i];
+}
+
+// Jacobi diagonal of the consistent tangent: for node a and direction i,
+// vol * eps_ai^T C_ep eps_ai with eps_ai = B_a e_i.
+__global__ void k_j2_diag(const int32_t* __restrict__ cells, const double* __restrict__ coords, int64_t C, J2Full q,
+                          const int32_t* __restrict__ iperm, const double* __restrict__ rec64,
+                          const double* __restrict__ w64, double* __restrict__ diag) {
+  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (c >= C) return;
+  const int4 qv = reinterpret_cast<const int4*>(cells)[c];
+  const int v[4] = {qv.x, qv.y, qv.z, qv.w};
+  double x[4][3], g[4][3], vol;
+#pragma unroll
+  for (int n = 0; n < 4; ++n)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) x[n][d] = __ldg(&coords[3 * int64_t(v[n]) + d]);
+  tet_geometry(x, g, vol);
+  const int64_t ic = iperm[c];
+  const double* r = rec64 + 8 * ic;
+  const double pe = w64[ic];
+  const double mu = q.p.mu, k = q.kappa, t1 = r[6], t2 = r[7];
+  for (int n = 0; n < 4; ++n)
+    for (int i = 0; i < 3; ++i) {
+      double e[6] = {0, 0, 0, 0, 0, 0};
+      e[i] = g[n][i];
+      if (i == 0) { e[4] = g[n][2]; e[5] = g[n][1]; }
+      if (i == 1) { e[3] = g[n][2]; e[5] = g[n][0]; }
+      if (i == 2) { e[3] = g[n][1]; e[4] = g[n][0]; }
+      const double tr = e[0] + e[1] + e[2], m = tr / 3.0;
+      const double ne = r[0] * e[0] + r[1] * e[1] + r[2] * e[2] + r[3] * e[3] + r[4] * e[4] + r[5] * e[5];
+      const double ma = mu * (1.0 - t1), b = 2.0 * mu * (t2 - t1);
+      double val = k * tr * tr;
+      for (int j = 0; j < 3; ++j) val += (2.0 * ma * (e[j] - m) - b * ne * r[j]) * e[j];
+      for (int j = 3; j < 6; ++j) val += (ma * e[j] - b * ne * r[j]) * e[j];
+      atomicAdd(&diag[3 * int64_t(v[n]) + i], pe * vol * val);
+    }
+}
+
+// J2PlasticityLocalResidual::evaluate (src/J2PlasticityLocalResidual.hpp:291-409):
+// the 14 local residual equations of each cell at the given states.
+__global__ void k_j2_local_residual(const int32_t* __restrict__ cells, const double* __restrict__ coords, int64_t C,
+                                    J2Dev p, const double* __restrict__ u, const double* __restrict__ z,
+                                    const double* __restrict__ loc, const double* __restrict__ prev,
+                                    double* __restrict__ H) {
+  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (c >= C) return;
+  const int4 qv = reinterpret_cast<const int4*>(cells)[c];
+  const int v[4] = {qv.x, qv.y, qv.z, qv.w};
+  double x[4][3], ue[12], g[4][3], vol, e[6];
+#pragma unroll
+  for (int n = 0; n < 4; ++n)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      x[n][d] = coords[3 * int64_t(v[n]) + d];
+      ue[3 * n + d] = u[3 * int64_t(v[n]) + d];
+    }
+  tet_geometry(x, g, vol);
+  tet_strain(g, ue, e);
+  const double* L = loc + 14 * c;
+  const double* Pv = prev + 14 * c;
+  double* h = H + 14 * c;
+  const double rho = 0.25 * (z[v[0]] + z[v[1]] + z[v[2]] + z[v[3]]);
+  const double mu_p = simp(rho, p.pe, p.pe_min) * p.mu;
+  const double ppen = simp(rho, p.pp, p.pp_min);
+  const double hi = ppen * p.hiso, hk = ppen * p.hkin;
+  double ee[6];
+  for (int i = 0; i < 6; ++i) ee[i] = e[i] - L[2 + i];
+  const double tr3 = (ee[0] + ee[1] + ee[2]) / 3.0;
+  double n[6] = {2.0 * mu_p * (ee[0] - tr3), 2.0 * mu_p * (ee[1] - tr3), 2.0 * mu_p * (ee[2] - tr3),
+                 mu_p * ee[3], mu_p * ee[4], mu_p * ee[5]};
+  for (int i = 0; i < 6; ++i) n[i] -= L[8 + i];
+  const double norm = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2] + 2.0 * (n[3] * n[3] + n[4] * n[4] + n[5] * n[5]));
+  const double s32 = 1.2247448713915890491, s23 = 0.81649658092772603273;
+  h[0] = L[0] - Pv[0];
+  h[1] = L[1];
+  for (int i = 2; i < 14; ++i) h[i] = L[i] - Pv[i];
+  if (L[1] > 0.0) {
+    const double inv = 1.0 / norm;
+    h[0] = L[0] - Pv[0] - L[1];
+    h[1] = s32 * norm - (ppen * p.sy0 + hi * L[0]);
+    for (int i = 0; i < 3; ++i) h[2 + i] = L[2 + i] - Pv[2 + i] - s32 * L[1] * n[i] * inv;
+    for (int i = 3; i < 6; ++i) h[2 + i] = L[2 + i] - Pv[2 + i] - 2.0 * s32 * L[1] * n[i] * inv;
+    for (int i = 0; i < 6; ++i) h[8 + i] = L[8 + i] - Pv[8 + i] - s23 * L[1] * hk * n[i] * inv;
+  }
+}
+
+__global__ void k_set_dofs(int64_t n, const int32_t* __restrict__ dofs, const double* __restrict__ vals, double scale,
+                           double* __restrict__ u) {
+  const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i < n) u[dofs[i]] = scale * vals[i];
+}
+
+__global__ void k_axpy_neg_masked(int64_t n, const uint8_t* __restrict__ mask, const double* __restrict__ R,
+                                  double* __restrict__ b, double* __restrict__ sumsq) {
+  double acc = 0.0;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    const bool c = mask && ((mask[i / 3] >> (i % 3)) & 1);
+    const double v = c ? 0.0 : -R[i];
+    b[i] = v;
+    acc += v * v;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(sumsq, acc);
+}
+
+__global__ void k_add(int64_t n, const double* __restrict__ d, double* __restrict__ u) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    u[i] += d[i];
+}
+
+J2Dev j2dev(const pa_j2_params& jp) {
+  return J2Dev{jp.youngs_modulus / (2.0 * (1.0 + jp.poissons_ratio)),
+               jp.initial_yield_stress,
+               jp.hardening_modulus_isotropic,
+               jp.hardening_modulus_kinematic,
+               jp.elastic_penalty_exponent,
+               jp.elastic_min_ersatz,
+               jp.plastic_penalty_exponent,
+               jp.plastic_min_ersatz};
+}
+
 }  // namespace
 
 void launch_j2(const Problem& P, const pa_j2_params& jp, const double* u, const double* z, const double* prev,
                double* cur, cudaStream_t s) {
-  J2Dev p{jp.youngs_modulus / (2.0 * (1.0 + jp.poissons_ratio)),
-          jp.initial_yield_stress,
-          jp.hardening_modulus_isotropic,
-          jp.hardening_modulus_kinematic,
-          jp.elastic_penalty_exponent,
-          jp.elastic_min_ersatz,
-          jp.plastic_penalty_exponent,
-          jp.plastic_min_ersatz};
+  const J2Dev p = j2dev(jp);
   const int64_t C = P.C();
   const int grid = int((C + kJ2Threads - 1) / kJ2Threads);
   k_j2<<<grid, kJ2Threads, 0, s>>>(P.mesh->d_cells.get(), P.mesh->d_coords.get(), C, p, u, z, prev, cur);
   PA_LAUNCHED();
+}
+
+void launch_j2_local_residual(const Problem& P, const pa_j2_params& jp, const double* u, const double* z,
+                              const double* loc, const double* prev, double* H, cudaStream_t s) {
+  const int64_t C = P.C();
+  k_j2_local_residual<<<int((C + 127) / 128), 128, 0, s>>>(P.mesh->d_cells.get(), P.mesh->d_coords.get(), C, j2dev(jp),
+                                                           u, z, loc, prev, H);
+  PA_LAUNCHED();
+}
+
+pa_status solve_operator(Problem& P, const SolveOperator& op, const double* b, double* x_out,
+                         const pa_solve_options& o, pa_solve_stats* st, bool record_start);
+
+// Displacement-form small-strain J2 problem by pseudo-time load stepping and
+// Newton's method.  The reference's driver is NewtonRaphsonSolver::solve
+// (src/NewtonRaphsonSolver.hpp:570-640) over PlasticityProblem's load steps
+// (src/PlasticityProblem.hpp:791-846): Dirichlet values ramp linearly, each
+// Newton iteration performs the radial return from the last converged local
+// state, assembles the residual and solves with the consistent tangent.
+// Here the tangent is applied matrix-free (tile kernel, J2 records) inside the
+// problem's PCG (FP32 apply + FP64 true residual in mixed mode).
+pa_status j2_solve(Problem& P, const pa_j2_params& jp, const double* z, const pa_j2_solve_options& jo,
+                   const pa_solve_options& lo, double* u, double* local, pa_j2_stats* js) {
+  cudaStream_t s = P.stream;
+  const int64_t C = P.C(), n = P.ndof();
+  const J2Full q{j2dev(jp), jp.youngs_modulus / (3.0 * (1.0 - 2.0 * jp.poissons_ratio)),
+                 jp.youngs_modulus * jp.poissons_ratio / ((1.0 + jp.poissons_ratio) * (1.0 - 2.0 * jp.poissons_ratio))};
+  PA_CHECK(jo.steps > 0 && jo.max_newton > 0 && jo.newton_tol > 0, "J2 solve options out of range");
+  // tile kernel material: lambda, mu of the elastic law; penalties per cell
+  ElasticParams saved = P.ep;
+  P.ep.E = jp.youngs_modulus;
+  P.ep.nu = jp.poissons_ratio;
+  DevBuf<double> prev(14 * C), rec64(8 * C), w64(C), R(n), b(n), du(n), diag(n), sumsq(1);
+  DevBuf<float> rec32(8 * C), w32(C);
+  PA_CUDA(cudaMemsetAsync(u, 0, sizeof(double) * n, s));
+  PA_CUDA(cudaMemsetAsync(prev.get(), 0, sizeof(double) * 14 * C, s));
+  if (!P.ev0) { PA_CUDA(cudaEventCreate(&P.ev0)); PA_CUDA(cudaEventCreate(&P.ev1)); }
+  cudaEvent_t t0, t1;
+  PA_CUDA(cudaEventCreate(&t0));
+  PA_CUDA(cudaEventCreate(&t1));
+  PA_CUDA(cudaEventRecord(t0, s));
+  const int64_t nbc = int64_t(P.bc_dofs.size());
+  const int grid = int((C + kJ2Threads - 1) / kJ2Threads);
+  int newton_total = 0;
+  int64_t cg_total = 0;
+  bool all_converged = true;
+  double last_rel = 0.0;
+  pa_status status = PA_OK;
+  for (int step = 0; step < jo.steps && status == PA_OK; ++step) {
+    if (nbc)
+      k_set_dofs<<<int((nbc + 255) / 256), 256, 0, s>>>(nbc, P.d_bc_dofs.get(), P.d_bc_vals.get(),
+                                                        double(step + 1) / jo.steps, u);
+    double r0 = -1.0;
+    bool converged = false;
+    for (int it = 0; it < jo.max_newton; ++it) {
+      PA_CUDA(cudaMemsetAsync(R.get(), 0, sizeof(double) * n, s));
+      k_j2_newton<<<grid, kJ2Threads, 0, s>>>(P.mesh->d_cells.get(), P.mesh->d_coords.get(), C, q, u, z, prev.get(),
+                                             local, P.mesh->d_cell_iperm.get(), rec64.get(), rec32.get(), w64.get(),
+                                             w32.get(), R.get());
+      PA_LAUNCHED();
+      PA_CUDA(cudaMemsetAsync(sumsq.get(), 0, sizeof(double), s));
+      k_axpy_neg_masked<<<int(std::min<int64_t>((n + 255) / 256, 148 * 8)), 256, 0, s>>>(
+          n, P.d_node_mask.get(), R.get(), b.get(), sumsq.get());
+      PA_LAUNCHED();
+      double h = 0.0;
+      PA_CUDA(cudaMemcpyAsync(&h, sumsq.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
+      PA_CUDA(cudaStreamSynchronize(s));
+      const double rn = std::sqrt(h);
+      if (!std::isfinite(rn)) { status = PA_ERR_NONFINITE; break; }
+      if (r0 < 0.0) r0 = rn;
+      last_rel = r0 > 0.0 ? rn / r0 : 0.0;
+      if (rn <= jo.newton_tol * r0 || rn == 0.0) { converged = true; break; }
+      ++newton_total;
+      // K_T du = -R with homogeneous Dirichlet conditions
+      PA_CUDA(cudaMemsetAsync(diag.get(), 0, sizeof(double) * n, s));
+      k_j2_diag<<<int((C + 127) / 128), 128, 0, s>>>(P.mesh->d_cells.get(), P.mesh->d_coords.get(), C, q,
+                                                    P.mesh->d_cell_iperm.get(), rec64.get(), w64.get(), diag.get());
+      PA_LAUNCHED();
+      SolveOperator op;
+      op.w64 = w64.get();
+      op.w32 = w32.get();
+      op.plas64 = rec64.get();
+      op.plas32 = rec32.get();
+      op.diag_aos = diag.get();
+      op.homogeneous_bc = true;
+      pa_solve_stats st{};
+      const pa_status ls = solve_operator(P, op, b.get(), du.get(), lo, &st, true);
+      cg_total += st.iterations;
+      if (ls != PA_OK && ls != PA_ERR_NOT_CONVERGED) { status = ls; break; }
+      k_add<<<int(std::min<int64_t>((n + 255) / 256, 148 * 8)), 256, 0, s>>>(n, du.get(), u);
+      PA_LAUNCHED();
+    }
+    if (status != PA_OK) break;
+    if (!converged) {
+      // final return mapping at the last iterate so `local` matches u
+      all_converged = false;
+    }
+    PA_CUDA(cudaMemcpyAsync(prev.get(), local, sizeof(double) * 14 * C, cudaMemcpyDeviceToDevice, s));
+  }
+  PA_CUDA(cudaEventRecord(t1, s));
+  PA_CUDA(cudaEventSynchronize(t1));
+  float ms = 0.f;
+  PA_CUDA(cudaEventElapsedTime(&ms, t0, t1));
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  P.ep = saved;
+  if (js) {
+    js->steps = jo.steps;
+    js->newton_iterations = newton_total;
+    js->cg_iterations = cg_total;
+    js->seconds = ms * 1e-3;
+    js->final_rel_residual = last_rel;
+    js->converged = all_converged ? 1 : 0;
+  }
+  if (status != PA_OK) return status;
+  return all_converged ? PA_OK : PA_ERR_NOT_CONVERGED;
 }
 
 }  // namespace pa

@@ -259,6 +259,9 @@ void build_tiles(Mesh& m) {
   m.d_tile_cell_start.upload(tile_cell_start.data(), tile_cell_start.size());
   m.h_tile_nodes = tile_nodes;
   m.d_cell_perm.upload(perm.data(), perm.size());
+  std::vector<int32_t> iperm(m.C);
+  for (int64_t i = 0; i < m.C; ++i) iperm[perm[i]] = int32_t(i);
+  m.d_cell_iperm.upload(iperm.data(), iperm.size());
 }
 
 // Node-star graph plus diagonal, sorted columns: the pattern CreateBlockMatrix

@@ -10,7 +10,7 @@ namespace pa {
 struct SolverWorkspace {
   int64_t ndof = 0;
   // FP64 vectors
-  DevBuf<double> x, b, r, p0, p1, ap, dinv, t, w64;
+  DevBuf<double> x, b, r, p0, p1, ap, dinv, t, w64, diag;
   // FP32 vectors (mixed precision)
   DevBuf<float> r32, p32a, p32b, ap32, dinv32, dx32, w32;
   DevBuf<float> coords32;
@@ -19,6 +19,17 @@ struct SolverWorkspace {
   DevBuf<PcgScalars> sc;
   DevBuf<double> rr_hist;
   void ensure(int64_t ndof_, int64_t C, int grid, bool mixed);
+};
+
+// The operator a solve uses: SIMP weights per cell (tile order), optional J2
+// tangent records (8 per cell, tile order) and the interleaved Jacobi diagonal.
+struct SolveOperator {
+  const double* w64 = nullptr;
+  const float* w32 = nullptr;
+  const double* plas64 = nullptr;
+  const float* plas32 = nullptr;
+  const double* diag_aos = nullptr;
+  bool homogeneous_bc = false;  // impose zero (not the problem's) Dirichlet values
 };
 
 struct Problem {

@@ -262,13 +262,14 @@ int fused_apply_grid(const Mesh& m) {
 
 template <typename T>
 ApplyArgs<T> fused_args(Problem& P, const T* coords, const T* w, const T* p_old, T* p_new, T* ap, const T* r,
-                        const T* dinv) {
+                        const T* dinv, const T* plas = nullptr) {
   SolverWorkspace& ws = P.ws;
   ApplyArgs<T> a{};
   a.tv = P.mesh->tiles();
   a.N = P.N();
   a.coords = coords;
   a.w = w;
+  a.plas = plas;
   a.tile_nodes = P.d_tile_nodes_bc.get();
   Iso<double> i64 = P.ep.iso();
   a.iso = Iso<T>{T(i64.lam), T(i64.mu)};
@@ -288,6 +289,7 @@ ApplyArgs<T> fused_args(Problem& P, const T* coords, const T* w, const T* p_old,
 void SolverWorkspace::ensure(int64_t n, int64_t C, int grid, bool mixed) {
   if (ndof != n) {
     x.resize(n); b.resize(n); r.resize(n); p0.resize(n); p1.resize(n); ap.resize(n); dinv.resize(n); t.resize(n);
+    diag.resize(n);
     w64.resize(C);
     ndof = n;
     r32.release(); p32a.release(); p32b.release(); ap32.release(); dinv32.release(); dx32.release(); w32.release();
@@ -315,15 +317,16 @@ struct CgGraph {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
   }
-  void capture(Problem& P, const T* coords, const T* w, T* pa, T* pb, T* ap, T* r, const T* dinv, X* x, int chunk_) {
+  void capture(Problem& P, const T* coords, const T* w, T* pa, T* pb, T* ap, T* r, const T* dinv, X* x, int chunk_,
+               const T* plas = nullptr) {
     cudaStream_t s = P.stream;
     SolverWorkspace& ws = P.ws;
     const int64_t n = P.ndof();
     const int vg = vec_grid(n);
     const int ag = fused_apply_grid<T>(*P.mesh);
     chunk = chunk_ + (chunk_ % 2);
-    ApplyArgs<T> a_even = fused_args<T>(P, coords, w, pa, pb, ap, r, dinv);  // reads pa, writes pb
-    ApplyArgs<T> a_odd = fused_args<T>(P, coords, w, pb, pa, ap, r, dinv);   // reads pb, writes pa
+    ApplyArgs<T> a_even = fused_args<T>(P, coords, w, pa, pb, ap, r, dinv, plas);  // reads pa, writes pb
+    ApplyArgs<T> a_odd = fused_args<T>(P, coords, w, pb, pa, ap, r, dinv, plas);   // reads pb, writes pa
     PA_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < chunk; ++k) {
       launch_apply_kernel<T, 1>(*P.mesh, ag, s, k % 2 == 0 ? a_even : a_odd);
@@ -380,9 +383,11 @@ static PcgScalars restart_residual(Problem& P, const T* r, const T* dinv, bool r
   return cur;
 }
 
-// Solve the constrained system for z; b and x_out are device pointers (3N).
-pa_status solve_device(Problem& P, const double* z, const double* b, double* x_out, const pa_solve_options& o,
-                       pa_solve_stats* st) {
+// Solve the constrained system K x = b for the given operator (weights,
+// optional J2 tangent records, Jacobi diagonal); b and x_out are device
+// pointers in the interleaved layout (3N).
+pa_status solve_operator(Problem& P, const SolveOperator& op, const double* b, double* x_out,
+                         const pa_solve_options& o, pa_solve_stats* st, bool record_start) {
   cudaStream_t s = P.stream;
   const int64_t n = P.ndof();
   const bool mixed = o.method == PA_SOLVER_PCG_MIXED;
@@ -397,21 +402,20 @@ pa_status solve_device(Problem& P, const double* z, const double* b, double* x_o
   const double tol2 = o.rel_tol * o.rel_tol;
   const int vg = vec_grid(n);
   const uint8_t* mask = P.d_node_mask.get();
-  const int64_t nbc = int64_t(P.bc_dofs.size());
+  const int64_t nbc = op.homogeneous_bc ? 0 : int64_t(P.bc_dofs.size());
   int64_t launches = 0;  // kernels of this library launched by the solve (graph nodes included)
 
   if (!P.ev0) { PA_CUDA(cudaEventCreate(&P.ev0)); PA_CUDA(cudaEventCreate(&P.ev1)); }
-  PA_CUDA(cudaEventRecord(P.ev0, s));
+  if (record_start) PA_CUDA(cudaEventRecord(P.ev0, s));
 
-  // SIMP weights in tile order; Jacobi diagonal and its masked inverse.
+  // masked inverse of the Jacobi diagonal
   const int64_t N = P.N();
-  launch_cell_weights(P, z, ws.w64.get(), mixed ? ws.w32.get() : nullptr, s);
-  launch_diag(P, ws.w64.get(), ws.t.get(), s);
-  k_inv_diag<double><<<vg, kVecThreads, 0, s>>>(N, ws.t.get(), mask, ws.dinv.get());
+  k_inv_diag<double><<<vg, kVecThreads, 0, s>>>(N, op.diag_aos, mask, ws.dinv.get());
   PA_LAUNCHED();
-  launches += 3;
+  launches += 1;
   if (mixed) {
-    k_inv_diag<float><<<vg, kVecThreads, 0, s>>>(N, ws.t.get(), mask, ws.dinv32.get());
+    PA_CHECK(op.w32 != nullptr, "mixed precision needs FP32 weights");
+    k_inv_diag<float><<<vg, kVecThreads, 0, s>>>(N, op.diag_aos, mask, ws.dinv32.get());
     PA_LAUNCHED();
     launches += 1;
   }
@@ -422,7 +426,7 @@ pa_status solve_device(Problem& P, const double* z, const double* b, double* x_o
     k_scatter_bc<<<int((nbc + 255) / 256), 256, 0, s>>>(nbc, P.d_bc_dofs.get(), P.d_bc_vals.get(), 1.0, N,
                                                         ws.p0.get());
     PA_LAUNCHED();
-    launch_apply_tiled<double>(P, ws.w64.get(), ws.p0.get(), ws.t.get(), false, s);
+    launch_apply_tiled<double>(P, op.w64, ws.p0.get(), ws.t.get(), false, s, op.plas64);
     k_aos_minus_soa<<<vg, kVecThreads, 0, s>>>(N, b, ws.t.get(), mask, bprime);
     launches += 3;
   } else {
@@ -440,7 +444,7 @@ pa_status solve_device(Problem& P, const double* z, const double* b, double* x_o
   PA_LAUNCHED();
   // FP64 true residual r = b' - K_masked x
   auto true_residual = [&]() {
-    launch_apply_tiled<double>(P, ws.w64.get(), ws.x.get(), ws.t.get(), true, s);
+    launch_apply_tiled<double>(P, op.w64, ws.x.get(), ws.t.get(), true, s, op.plas64);
     k_sub_masked<<<vg, kVecThreads, 0, s>>>(N, bprime, ws.t.get(), mask, ws.r.get());
     PA_LAUNCHED();
     launches += 3;
@@ -464,11 +468,11 @@ pa_status solve_device(Problem& P, const double* z, const double* b, double* x_o
   CgGraph<double, double> g64;
   CgGraph<float, float> g32;
   if (mixed)
-    g32.capture(P, P.mesh->d_coords32_soa.get(), ws.w32.get(), ws.p32a.get(), ws.p32b.get(), ws.ap32.get(), ws.r32.get(),
-                ws.dinv32.get(), ws.dx32.get(), chunk);
+    g32.capture(P, P.mesh->d_coords32_soa.get(), op.w32, ws.p32a.get(), ws.p32b.get(), ws.ap32.get(), ws.r32.get(),
+                ws.dinv32.get(), ws.dx32.get(), chunk, op.plas32);
   else
-    g64.capture(P, P.mesh->d_coords_soa.get(), ws.w64.get(), ws.p0.get(), ws.p1.get(), ws.ap.get(), ws.r.get(),
-                ws.dinv.get(), ws.x.get(), chunk);
+    g64.capture(P, P.mesh->d_coords_soa.get(), op.w64, ws.p0.get(), ws.p1.get(), ws.ap.get(), ws.r.get(),
+                ws.dinv.get(), ws.x.get(), chunk, op.plas64);
 
   // Recursive-residual stop hint, confirmed on the FP64 true residual.
   const double hint = mixed ? 0.25 : 0.81;
@@ -508,7 +512,7 @@ pa_status solve_device(Problem& P, const double* z, const double* b, double* x_o
   }
   const double relres = std::sqrt(rr_true / bb);
 
-  // x_out = x_f + x_D (back to the interleaved layout)
+  // x_out = x_f + x_D (back to the interleaved layout); constrained dofs are 0 in x_f
   launch_soa_to_aos<double, double>(ws.x.get(), x_out, N, s);
   launches += 1;
   if (nbc) {
@@ -531,6 +535,29 @@ pa_status solve_device(Problem& P, const double* z, const double* b, double* x_o
   if (breakdown) return PA_ERR_BREAKDOWN;
   if (!std::isfinite(relres)) return PA_ERR_NONFINITE;
   return converged ? PA_OK : PA_ERR_NOT_CONVERGED;
+}
+
+// Elastic solve for density z: SIMP weights and Jacobi diagonal from z, then
+// solve_operator.
+pa_status solve_device(Problem& P, const double* z, const double* b, double* x_out, const pa_solve_options& o,
+                       pa_solve_stats* st) {
+  const bool mixed = o.method == PA_SOLVER_PCG_MIXED;
+  const int64_t n = P.ndof();
+  const int grid_need = std::max(std::max(fused_apply_grid<double>(*P.mesh), fused_apply_grid<float>(*P.mesh)),
+                                vec_grid(n));
+  P.ws.ensure(n, P.C(), grid_need, mixed);
+  SolverWorkspace& ws = P.ws;
+  if (!P.ev0) { PA_CUDA(cudaEventCreate(&P.ev0)); PA_CUDA(cudaEventCreate(&P.ev1)); }
+  PA_CUDA(cudaEventRecord(P.ev0, P.stream));  // the solve time includes weights and diagonal
+  launch_cell_weights(P, z, ws.w64.get(), mixed ? ws.w32.get() : nullptr, P.stream);
+  launch_diag(P, ws.w64.get(), ws.diag.get(), P.stream);
+  SolveOperator op;
+  op.w64 = ws.w64.get();
+  op.w32 = mixed ? ws.w32.get() : nullptr;
+  op.diag_aos = ws.diag.get();
+  pa_status status = solve_operator(P, op, b, x_out, o, st, false);
+  if (st) st->kernel_launches += 2;
+  return status;
 }
 
 // Average device time of the fused CG kernel K1 over `reps` back-to-back

@@ -43,6 +43,7 @@ struct ApplyArgs {
   int64_t N;                   // nodes (SoA stride)
   const T* coords;             // 3N, SoA
   const T* w;                  // C, SIMP weight per cell, internal order
+  const T* plas;               // null (elastic) or 8 per cell, internal order: J2 tangent record
   Iso<T> iso;
   const T* x;                  // plain: input vector; pcg: p_old
   T* y;                        // output, zero on entry
@@ -113,10 +114,17 @@ __device__ __forceinline__ T tet_apply(const Iso<T>& iso, T w, const T (&xc)[4][
 // i.e. vol * w * B^T C B u with vol = |det| / 6, one reciprocal per tet and no
 // per-entry scaling of the gradients.  Returns eps_u : sig' = p_e^T K_e p_e.
 // h1 and h2 are passed in because a hex cluster shares them between tets.
+// With `pl` non-null the stress is the J2 consistent tangent instead of the
+// elastic one: pl = {n (6, tensor Voigt), theta1, theta2} of the cell's last
+// return mapping and
+//   sigma = w [kappa tr(eps) 1 + 2 mu (1 - theta1) dev(eps) - 2 mu (theta2 - theta1) (n : eps) n],
+// theta1 = sqrt(6) mu_p dgamma / |eta_trial|, theta2 = 3 mu_p / (3 mu_p + H_iso,p + H_kin,p)
+// (zero for an elastic cell).
 template <typename T>
 __device__ __forceinline__ T tet_rel(const Iso<T>& iso, T w, const T (&e0)[3], const T (&ea)[3], const T (&eb)[3],
                                      const T (&h1)[3], const T (&h2)[3], const T (&d0)[3], const T (&da)[3],
-                                     const T (&db)[3], T (&r0)[3], T (&ra)[3], T (&rb)[3]) {
+                                     const T (&db)[3], T (&r0)[3], T (&ra)[3], T (&rb)[3],
+                                     const T* __restrict__ pl = nullptr) {
   T h0[3];
   h0[0] = ea[1] * eb[2] - ea[2] * eb[1];
   h0[1] = ea[2] * eb[0] - ea[0] * eb[2];
@@ -130,10 +138,30 @@ __device__ __forceinline__ T tet_rel(const Iso<T>& iso, T w, const T (&e0)[3], c
   const T gyz = h0[1] * d0[2] + h0[2] * d0[1] + h1[1] * da[2] + h1[2] * da[1] + h2[1] * db[2] + h2[2] * db[1];
   const T gxz = h0[0] * d0[2] + h0[2] * d0[0] + h1[0] * da[2] + h1[2] * da[0] + h2[0] * db[2] + h2[2] * db[0];
   const T gxy = h0[0] * d0[1] + h0[1] * d0[0] + h1[0] * da[1] + h1[1] * da[0] + h2[0] * db[1] + h2[1] * db[0];
-  const T lam = iso.lam * sc, mu = iso.mu * sc, two_mu = mu + mu;
-  const T ltr = lam * (exx + eyy + ezz);
-  const T sxx = ltr + two_mu * exx, syy = ltr + two_mu * eyy, szz = ltr + two_mu * ezz;
-  const T syz = mu * gyz, sxz = mu * gxz, sxy = mu * gxy;
+  T sxx, syy, szz, syz, sxz, sxy;
+  if (pl == nullptr) {
+    const T lam = iso.lam * sc, mu = iso.mu * sc, two_mu = mu + mu;
+    const T ltr = lam * (exx + eyy + ezz);
+    sxx = ltr + two_mu * exx;
+    syy = ltr + two_mu * eyy;
+    szz = ltr + two_mu * ezz;
+    syz = mu * gyz;
+    sxz = mu * gxz;
+    sxy = mu * gxy;
+  } else {
+    const T n0 = pl[0], n1 = pl[1], n2 = pl[2], n3 = pl[3], n4 = pl[4], n5 = pl[5], t1 = pl[6], t2 = pl[7];
+    const T tr = exx + eyy + ezz, m = tr * (T(1) / T(3));
+    const T k = (iso.lam + iso.mu * (T(2) / T(3))) * sc;
+    const T ma = iso.mu * (T(1) - t1) * sc, two_ma = ma + ma;
+    const T bne = T(2) * iso.mu * (t2 - t1) * sc * (n0 * exx + n1 * eyy + n2 * ezz + n3 * gyz + n4 * gxz + n5 * gxy);
+    const T ktr = k * tr;
+    sxx = ktr + two_ma * (exx - m) - bne * n0;
+    syy = ktr + two_ma * (eyy - m) - bne * n1;
+    szz = ktr + two_ma * (ezz - m) - bne * n2;
+    syz = ma * gyz - bne * n3;
+    sxz = ma * gxz - bne * n4;
+    sxy = ma * gxy - bne * n5;
+  }
   r0[0] = h0[0] * sxx + h0[1] * sxy + h0[2] * sxz;
   r0[1] = h0[0] * sxy + h0[1] * syy + h0[2] * syz;
   r0[2] = h0[0] * sxz + h0[1] * syz + h0[2] * szz;
@@ -352,7 +380,8 @@ __global__ void __launch_bounds__(TILE, 1) k_apply_tiled(ApplyArgs<T> a) {
           T h1[3], r0[3], ra[3], rb[3];
 #pragma unroll
           for (int d = 0; d < 3; ++d) h1[d] = -Cx[sb][d];
-          const T en = tet_rel(a.iso, wv[k], E[0], E[sa], E[sb], h1, Cx[sa], D[0], D[sa], D[sb], r0, ra, rb);
+          const T* pl = a.plas ? a.plas + 8 * (int64_t(S.meta[b][5]) + 6 * t + k) : nullptr;
+          const T en = tet_rel(a.iso, wv[k], E[0], E[sa], E[sb], h1, Cx[sa], D[0], D[sa], D[sb], r0, ra, rb, pl);
           if (MODE == 1) pap += double(en);
 #pragma unroll
           for (int d = 0; d < 3; ++d) {
@@ -391,8 +420,9 @@ __global__ void __launch_bounds__(TILE, 1) k_apply_tiled(ApplyArgs<T> a) {
         }
         cross3(e[2], e[0], h1);
         cross3(e[0], e[1], h2);
-        const T en = tet_rel(a.iso, S.w[b][6 * nhex + (t - nhex)], e[0], e[1], e[2], h1, h2, du[0], du[1], du[2],
-                             r[0], r[1], r[2]);
+        const int cl = 6 * nhex + (t - nhex);
+        const T* pl = a.plas ? a.plas + 8 * (int64_t(S.meta[b][5]) + cl) : nullptr;
+        const T en = tet_rel(a.iso, S.w[b][cl], e[0], e[1], e[2], h1, h2, du[0], du[1], du[2], r[0], r[1], r[2], pl);
         if (MODE == 1) pap += double(en);
 #pragma unroll
         for (int n = 0; n < 3; ++n)

@@ -141,3 +141,46 @@ def test_oracle_gradient_x_matches_finite_differences(oracle_lib):
     fp = oracle_lib.Oracle(cells, coords + h * dx, E=1.0, nu=0.3, p=3.0, pmin=1e-9).energy(u, z, grads=False)
     fm = oracle_lib.Oracle(cells, coords - h * dx, E=1.0, nu=0.3, p=3.0, pmin=1e-9).energy(u, z, grads=False)
     assert abs((fp - fm) / (2 * h) - gx @ dx.ravel()) <= 1e-6 * abs(gx @ dx.ravel())
+
+
+def j2_evaluate_3d_case():
+    """J2Plasticity_Evaluate3D (unit_tests/PlasticityTests.cpp:1749-1864): a
+    1x1x1 box, u = 0.1 (y+z, x+z, x+y) (the test's boundary helper adds its
+    values), control 0.9, the parameters of its tGenericParamList_Two."""
+    from oracle import np_ref, np_j2
+    cells, X = np_ref.box_mesh(1, 1, 1)
+    u = 0.1 * np.stack([X[:, 1] + X[:, 2], X[:, 0] + X[:, 2], X[:, 0] + X[:, 1]], axis=1).ravel()
+    prm = np_j2.J2Params(520.0, 0.3, 3.0, 20.0, 15.0, pe=3.0, pe_min=1e-9, pp=2.5, pp_min=1e-9)
+    cur = np.array([0.3, 0.5, -0.1, 0.0, 0.1, 0.2, 0.2, 0.2, 12.0, -4.0, -8.0, 1.0, 1.0, 1.0])
+    prev = np.array([0.2, 0.75, 0.0, -0.2, 0.2, 0.2, 0.2, 0.2, 2.0, 40.0, -42.0, 2.0, 2.0, 2.0])
+    gold = [-0.400000, 26.941399, -0.480125, 0.111393, 0.368732, 0.0443036, 0.0443036, 0.0443036, 7.078994,
+            -44.680887, 37.601894, -0.829778, -0.829778, -0.829778]
+    return cells, X, u, prm, cur, prev, gold
+
+
+def test_j2_local_residual_evaluate_3d():
+    from oracle import np_ref, np_j2
+    cells, X, u, prm, cur, prev, gold = j2_evaluate_3d_case()
+    for c in cells:
+        g, _ = np_ref.cell_gradients(X[c])
+        eps = np_ref.bmatrix(g) @ u.reshape(-1, 3)[c].ravel()
+        H = np_j2.local_residual(prm, 0.9, eps, cur, prev)
+        floating_equality(H, gold, 1e-5)
+
+
+def test_j2_radial_return_satisfies_local_residual():
+    """After the return mapping the local residual vanishes (plastic and elastic cells)."""
+    from oracle import np_j2
+    rng = np.random.default_rng(5)
+    prm = np_j2.J2Params(200e3, 0.3, 250.0, 1000.0, 300.0, pe=3.0, pp=2.5)
+    for k in range(20):
+        eps = 3e-3 * rng.standard_normal(6)
+        prev = np.zeros(14)
+        prev[0] = abs(1e-3 * rng.standard_normal())
+        prev[2:14] = 1e-3 * rng.standard_normal(12)
+        prev[8:14] *= 1e4
+        prev[2:5] -= prev[2:5].mean()    # plastic strain and backstress are deviatoric
+        prev[8:11] -= prev[8:11].mean()
+        cur, _ = np_j2.radial_return(prm, 0.9, eps, prev)
+        H = np_j2.local_residual(prm, 0.9, eps, cur, prev)
+        assert np.abs(H).max() <= 1e-8 * max(1.0, np.abs(cur).max() * 1e3)
