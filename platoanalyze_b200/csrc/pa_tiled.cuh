@@ -282,8 +282,10 @@ __device__ __forceinline__ void prefetch_data(const ApplyArgs<T>& a, TileSmem<T,
   cp_async_commit();
 }
 
+// FP32 instances ask for 640 resident threads per SM (<= 96 registers, 20
+// warps); FP64 instances are register-bound at one or two CTAs.
 template <typename T, int MODE, int TILE>
-__global__ void __launch_bounds__(TILE, 1) k_apply_tiled(ApplyArgs<T> a) {
+__global__ void __launch_bounds__(TILE, (sizeof(T) == 4 ? 640 / TILE : 1)) k_apply_tiled(ApplyArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TileSmem<T, MODE, TILE>& S = *reinterpret_cast<TileSmem<T, MODE, TILE>*>(smem_raw);
 
