@@ -49,6 +49,12 @@ def parse():
     ap.add_argument("--profile-kernel", action="store_true",
                     help="only build the workload and time the fused CG kernel (for ncu captures)")
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--newton-tol", type=float, default=1e-8, help="J2: relative Newton tolerance per load step")
+    ap.add_argument("--workload", default="cantilever", choices=["cantilever", "j2", "learned"],
+                    help="cantilever: the SIMP solve (default); j2: the elasto-plastic bar; learned: the "
+                         "learned-preconditioner solve on 64^3 after SIMP-pair training")
+    ap.add_argument("--simp-iterations", type=int, default=30)
+    ap.add_argument("--train-steps", type=int, default=400)
     return ap.parse_args()
 
 
@@ -374,12 +380,243 @@ def run_ours(args):
     return 0
 
 
+J2_DIMS = (80, 40, 40)
+J2_PARAMS = dict(youngs_modulus=200e3, poissons_ratio=0.3, initial_yield_stress=250.0,
+                 hardening_modulus_isotropic=1000.0, hardening_modulus_kinematic=0.0, elastic_penalty_exponent=3.0,
+                 elastic_min_ersatz=1e-9, plastic_penalty_exponent=2.5, plastic_min_ersatz=1e-9)
+
+
+def j2_bar(pa, dims, strain=0.02, stream=None):
+    """80x40x40 hex x 6 tet bar, x = 0 clamped, u_x = strain * L prescribed on
+    x = L (the final value; pa_j2_solve ramps it over the load steps)."""
+    nx, ny, nz = dims
+    mesh = pa.Mesh.box(nx, ny, nz, float(nx), float(ny), float(nz))
+    prob = pa.Problem(mesh, J2_PARAMS["youngs_modulus"], J2_PARAMS["poissons_ratio"], stream=stream)
+    px, py = nx + 1, ny + 1
+    jj, kk = np.meshgrid(np.arange(py), np.arange(nz + 1), indexing="ij")
+    x0 = (px * (jj + py * kk)).ravel()
+    x1 = x0 + nx
+    dofs = np.concatenate([3 * x0, 3 * x0 + 1, 3 * x0 + 2, 3 * x1])
+    vals = np.concatenate([np.zeros(3 * x0.size), np.full(x1.size, strain * nx)])
+    order = np.argsort(dofs)
+    prob.set_dirichlet(dofs[order].astype(np.int32), vals[order])
+    return mesh, prob
+
+
+def j2_return_bytes(C, N):
+    """Algorithmic bytes of one radial return over the mesh: connectivity
+    (16 B), 14 + 14 local-state doubles and the cell's density per cell;
+    coordinates and displacements (3 + 3 doubles) per node."""
+    return C * (16 + 14 * 8 * 2 + 8) + N * (3 * 8 + 3 * 8)
+
+
+def cpu_j2_return_rate(dims, threads, reps=5):
+    """Oracle (C++/OpenMP FP64) radial return over the full mesh at a
+    plastic state: cells/s, median of `reps` after one warm-up."""
+    from oracle import cpu
+    cpu.set_threads(threads)
+    nx, ny, nz = dims
+    cells, coords = cpu.box_mesh(nx, ny, nz, float(nx), float(ny), float(nz))
+    O = cpu.Oracle(cells, coords, E=J2_PARAMS["youngs_modulus"], nu=0.3, p=1.0, pmin=0.0)
+    u = np.zeros(3 * O.N)
+    u[0::3] = 0.02 * coords[:, 0]  # 2% axial strain: every cell past yield
+    z = np.ones(O.N)
+    prev = np.zeros(14 * O.C)
+    mu = J2_PARAMS["youngs_modulus"] / (2 * (1 + J2_PARAMS["poissons_ratio"]))
+    ts = []
+    for k in range(reps + 1):
+        t0 = time.perf_counter()
+        O.j2_update(u, z, prev, mu, 250.0, 1000.0, 0.0)
+        if k:
+            ts.append(time.perf_counter() - t0)
+    t = float(np.median(ts))
+    return O.C / t, t
+
+
+def run_j2(args):
+    """cfg5: small-strain J2 bar, 20 load steps to 2% axial strain; one step
+    of the benchmark = one whole load-stepped Newton solve (FP64 return
+    mapping and residual, mixed-precision tangent solves)."""
+    import torch
+    import platoanalyze_b200 as pa
+
+    dims = J2_DIMS if args.dims == "160x80x80" else dims_of(args.dims)
+    C, N = counts(dims)
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    mesh, prob = j2_bar(pa, dims, stream=stream.cuda_stream)
+    z = torch.ones(N, dtype=torch.float64, device="cuda")
+    u = torch.empty(3 * N, dtype=torch.float64, device="cuda")
+    local = torch.empty(14 * C, dtype=torch.float64, device="cuda")
+    lin = pa.SolveOptions(args.method, rel_tol=args.rel_tol)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device="cuda")
+
+    def solve_once():
+        _, _, st = prob.j2_solve(J2_PARAMS, z, steps=20, max_newton=25, newton_tol=args.newton_tol, options=lin,
+                                 u=u, local=local, allow_not_converged=True)
+        return st
+
+    for _ in range(args.warmup):
+        solve_once()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    total_ms, stats = 0.0, []
+    for _ in range(args.steps):
+        flush.fill_(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        stats.append(solve_once())
+        e1.record(stream)
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1)
+    clk = clocks.stop()
+    loc = local.view(-1, 14)
+    plastic_frac = float((loc[:, 0] > 0).double().mean().item())
+
+    # the radial return alone (FP64), from the converged state: roofline
+    prev = torch.zeros_like(local)
+    out = torch.empty_like(local)
+    for _ in range(3):
+        prob.j2_radial_return(J2_PARAMS, u, z, prev, out)
+    reps, ms = 20, 0.0
+    for _ in range(reps):
+        flush.fill_(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        prob.j2_radial_return(J2_PARAMS, u, z, prev, out)
+        e1.record(stream)
+        e1.synchronize()
+        ms += e0.elapsed_time(e1)
+    ms /= reps
+    nbytes = j2_return_bytes(C, N)
+    peak, peak_kind = peaks()
+    achieved = nbytes / (ms * 1e-3) / 1e9
+
+    # end to end with host buffers: z in, u and the local states out
+    z_pin = torch.ones(N, dtype=torch.float64).pin_memory()
+    u_pin = torch.empty(3 * N, dtype=torch.float64).pin_memory()
+    l_pin = torch.empty(14 * C, dtype=torch.float64).pin_memory()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    prob.j2_solve(J2_PARAMS, z_pin, steps=20, max_newton=25, newton_tol=args.newton_tol, options=lin, u=u_pin,
+                  local=l_pin, allow_not_converged=True)
+    e2e_ms = 1e3 * (time.perf_counter() - t0)
+
+    value = C * args.steps / (total_ms * 1e-3)
+    line = {
+        "metric": "J2 load-stepped solve cells/s, 1 B200", "value": value, "unit": "cells/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 return map + residual / " + ("f32 apply, f64 dots+refinement" if args.method == "mixed"
+                                                   else "f64 tangent solves"),
+        "data": "synthetic (uniform density 1)",
+        "config": {"workload": f"J2 bar {dims[0]}x{dims[1]}x{dims[2]} hex x 6 tets, 20 load steps to 2% axial strain, "
+                               "E=200e3 nu=0.3 sigma_y=250 H_iso=1000", "cells": C, "nodes": N,
+                   "linear": args.method, "linear_rel_tol": args.rel_tol, "l2": "256 MB buffer written between steps"},
+        "newton_iterations": [s["newton_iterations"] for s in stats], "cg_iterations": [s["cg_iterations"] for s in stats],
+        "newton_tol": args.newton_tol, "converged": all(s["converged"] for s in stats),
+        "worst_step_rel_residual": max(s["final_rel_residual"] for s in stats),
+        "linear_unconverged": [s["linear_unconverged"] for s in stats], "plastic_cell_fraction": plastic_frac,
+        "clocks": clk,
+        "e2e": {"value": C / (e2e_ms * 1e-3), "unit": "cells/s", "h2d_bytes_per_step": 8 * N,
+                "d2h_bytes_per_step": 8 * (3 * N + 14 * C)},
+        "roofline": {"bound": "hbm", "kernel": "k_j2 (radial return, FP64)", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_launch": nbytes, "ms_per_launch": ms},
+    }
+    if not args.no_cpu_baseline:
+        threads = host_cores()
+        rate, t = cpu_j2_return_rate(dims, threads)
+        line["cpu_baseline"] = {"value": rate, "unit": "cells/s (radial return)", "cores": threads, "kind": "port",
+                                "sample": f"oracle radial return over the full {C}-cell mesh at 2% strain, "
+                                          f"{t * 1e3:.1f} ms; the GPU return takes {ms:.3f} ms"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_learned(args):
+    """cfg4: 64x64x64 hexes x 6 tets cantilever; (residual, error) pairs from
+    SIMP/OC design iterations (volume fraction 0.4, move 0.2) with plain
+    solves, the network trained on the GPU, then the design after the last
+    iteration (not seen in training) solved to relres 1e-8 by the learned
+    flexible CG (mixed), the plain FP64 Jacobi-PCG and the mixed Jacobi-PCG."""
+    import torch
+    import platoanalyze_b200 as pa
+    from platoanalyze_b200.workloads import cantilever, simp_training_pairs
+
+    dims = (64, 64, 64) if args.dims == "160x80x80" else dims_of(args.dims)
+    C, N = counts(dims)
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    mesh, prob, faces, dofs = cantilever(dims, stream=stream.cuda_stream)
+    t0 = time.perf_counter()
+    dens, sd, res, en, final, hist = simp_training_pairs(prob, dims, iterations=args.simp_iterations)
+    torch.cuda.synchronize()
+    t_pairs = time.perf_counter() - t0
+    pc = pa.LearnedPreconditioner.for_box(*dims, seed=0)
+    tr = pc.train(prob, dens, sd, res, en, steps=args.train_steps, batch=4, learning_rate=1e-3, seed=1)
+    prob.set_preconditioner(pc)
+    z = torch.tensor(final, device="cuda")
+    u = torch.empty(3 * N, dtype=torch.float64, device="cuda")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device="cuda")
+    opts = {"learned": pa.SolveOptions("learned", rel_tol=args.rel_tol),
+            "mixed": pa.SolveOptions("mixed", rel_tol=args.rel_tol),
+            "fp64": pa.SolveOptions("fp64", rel_tol=args.rel_tol)}
+
+    def timed(name, steps, warmup):
+        for _ in range(warmup):
+            prob.solution(z, u, options=opts[name])
+        ms, st = [], None
+        for _ in range(steps):
+            flush.fill_(1)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            _, st = prob.solution(z, u, options=opts[name])
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return float(np.median(ms)), st, prob.scalar_function().value(u, z)
+
+    clocks = ClockSampler(0)
+    clocks.start()
+    ms_l, st_l, f_l = timed("learned", args.steps, args.warmup)
+    clk = clocks.stop()
+    ms_m, st_m, f_m = timed("mixed", max(1, args.steps // 2), 1)
+    ms_d, st_d, f_d = timed("fp64", max(1, args.steps // 2), 1)
+    line = {
+        "metric": METRIC, "value": C / (ms_l * 1e-3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_l, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16 network (f32 accumulate) / f32 apply / f64 dots+refinement",
+        "data": "synthetic (SIMP/OC designs from a uniform 0.4 start)",
+        "config": {"workload": f"learned-PC SIMP cantilever {dims[0]}x{dims[1]}x{dims[2]} hex x 6 tets, "
+                               f"Problem::solution to relres {args.rel_tol:g}", "cells": C, "nodes": N,
+                   "simp_iterations": args.simp_iterations, "pairs": int(len(sd)), "train_steps": args.train_steps,
+                   "network_params": pc.num_params, "l2": "256 MB buffer written between timed steps"},
+        "learned": {"solve_s": ms_l * 1e-3, **st_l, "compliance_rel_err_vs_fp64": abs(f_l - f_d) / abs(f_d)},
+        "jacobi_mixed": {"solve_s": ms_m * 1e-3, **st_m, "compliance_rel_err_vs_fp64": abs(f_m - f_d) / abs(f_d)},
+        "jacobi_fp64": {"solve_s": ms_d * 1e-3, **st_d},
+        "speedup_learned_vs_fp64": ms_d / ms_l, "speedup_mixed_vs_fp64": ms_d / ms_m,
+        "training": tr, "pair_generation_s": t_pairs,
+        "simp_history": [{k: h[k] for k in ("iteration", "compliance", "cg_iterations")} for h in hist],
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.profile_kernel:
         return profile_kernel(args)
+    if args.workload == "j2":
+        return run_j2(args)
+    if args.workload == "learned":
+        return run_learned(args)
     return run_ours(args)
 
 

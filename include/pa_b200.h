@@ -45,6 +45,7 @@ typedef enum {
 
 typedef struct pa_mesh pa_mesh;
 typedef struct pa_problem pa_problem;
+typedef struct pa_pc pa_pc;
 
 /* Library version string and the calling thread's last error message. */
 const char* pa_version(void);
@@ -196,6 +197,10 @@ pa_status pa_apply_block_constraints(pa_problem* problem, double* entries, doubl
 
 #define PA_SOLVER_PCG_FP64 0  /* matrix-free Jacobi-PCG, FP64 throughout */
 #define PA_SOLVER_PCG_MIXED 1 /* FP32 apply/vectors, FP64 dots, FP64 true-residual updates */
+#define PA_SOLVER_FCG_LEARNED 2 /* flexible CG preconditioned by the problem's learned network
+                                   (pa_problem_set_preconditioner), precision as PA_SOLVER_PCG_MIXED;
+                                   continues as PA_SOLVER_PCG_MIXED when the residual stalls or the
+                                   network's direction is not a descent direction */
 
 typedef struct {
   int32_t method;        /* PA_SOLVER_* */
@@ -212,6 +217,7 @@ typedef struct {
   double seconds;         /* device time of the solve */
   int32_t converged;
   int64_t kernel_launches; /* kernels this library launched for the solve */
+  int32_t fallback_iterations; /* PA_SOLVER_FCG_LEARNED: iterations run by the Jacobi fallback */
 } pa_solve_stats;
 
 pa_status pa_solve_options_default(pa_solve_options* options);
@@ -281,8 +287,9 @@ typedef struct {
   int32_t newton_iterations;  /* tangent solves over all steps */
   int64_t cg_iterations;      /* PCG iterations over all tangent solves */
   double seconds;             /* device time */
-  double final_rel_residual;  /* relative Newton residual of the last step */
+  double final_rel_residual;  /* largest over the steps of the relative Newton residual at the step's end */
   int32_t converged;
+  int32_t linear_unconverged; /* tangent solves that stopped at their iteration cap */
 } pa_j2_stats;
 
 /* Elasto-plastic solve, displacement-form small-strain J2 with linear
@@ -297,6 +304,62 @@ typedef struct {
 pa_status pa_j2_solve(pa_problem* problem, const pa_j2_params* params, const double* z,
                       const pa_j2_solve_options* options, const pa_solve_options* linear, double* u, double* local,
                       pa_j2_stats* stats);
+
+/* ------------------------------------------------ learned preconditioner --- */
+/* No counterpart in the reference (its solvers are AmgX / AztecOO / Belos).
+ * A small convolutional network on the nodal grid of a structured box mesh
+ * (pa_mesh_create_box numbering: node i + gx (j + gy k)) maps the residual of
+ * the constrained system to a correction:
+ *   M r = D^-1 r + s D^-1/2 f(D^-1/2 r / s, stiffness, Dirichlet),  s = RMS(D^-1/2 r),
+ * with D the Jacobi diagonal and f four 3x3x3 convolutions (5 -> 32 -> 32 ->
+ * 32 -> 3 channels, ReLU between them), BF16 weights and activations, FP32
+ * accumulation on the tensor cores.  Input features per node: the three
+ * scaled residual components, 1 + log10(mean diagonal / max diagonal) / 9
+ * clipped to [0, 1], and the constrained fraction of the node's dofs.  A new
+ * network has zero weights in its last layer, so M starts as Jacobi. */
+
+typedef struct {
+  int32_t steps;        /* optimizer steps (Adam) */
+  int32_t batch;        /* samples per step */
+  double learning_rate; /* Adam step size; cosine-decayed to 5% over the steps */
+  uint64_t seed;        /* sample order */
+} pa_pc_train_options;
+
+typedef struct {
+  double initial_loss;  /* mean loss of the first step */
+  double final_loss;    /* mean loss of the last min(10, steps) steps */
+  double seconds;       /* device time of the training */
+  int32_t steps;
+  int64_t kernel_launches;
+} pa_pc_train_stats;
+
+/* Network for a grid of gx x gy x gz nodes; hidden-layer weights He-normal
+ * from `seed`, last layer zero. */
+pa_status pa_pc_create(int32_t gx, int32_t gy, int32_t gz, uint64_t seed, pa_pc** pc);
+pa_status pa_pc_destroy(pa_pc* pc);
+/* Parameters as one FP32 vector: per layer the weights [out][in][kz][ky][kx]
+ * then the biases [out]. */
+pa_status pa_pc_num_params(const pa_pc* pc, int64_t* count);
+pa_status pa_pc_get_params(pa_pc* pc, float* params);
+pa_status pa_pc_set_params(pa_pc* pc, const float* params);
+/* The network alone on given input features (G x 5 FP32 per node; G = gx gy gz),
+ * output G x 3 FP32 (the correction f before scaling). */
+pa_status pa_pc_forward(pa_pc* pc, const float* features, float* out);
+/* Gradient of sum(grad_out . f(features)) with respect to the parameters. */
+pa_status pa_pc_backward(pa_pc* pc, const float* features, const float* grad_out, float* grad_params);
+/* out = M r for the problem at density z (interleaved 3N vectors). */
+pa_status pa_pc_apply(pa_problem* problem, pa_pc* pc, const double* z, const double* r, double* out);
+/* Train on residual/error pairs: sample s has residual r_s (3N, interleaved,
+ * zero on constrained dofs) of the problem at density densities[sample_density[s]]
+ * (each num_densities x nz), and e_s . r_s = energies[s] where K e_s = r_s.
+ * Loss per sample: ||e_s - M r_s||_K^2 / ||e_s||_K^2, evaluated with the
+ * matrix-free operator; gradients by the library's own backward kernels. */
+pa_status pa_pc_train(pa_problem* problem, pa_pc* pc, int32_t num_densities, const double* densities,
+                      int32_t num_samples, const int32_t* sample_density, const double* residuals,
+                      const double* energies, const pa_pc_train_options* options, pa_pc_train_stats* stats);
+/* Attach (or detach with NULL) the network PA_SOLVER_FCG_LEARNED uses; the
+ * mesh must be the network's grid.  The problem does not own the network. */
+pa_status pa_problem_set_preconditioner(pa_problem* problem, pa_pc* pc);
 
 #ifdef __cplusplus
 }

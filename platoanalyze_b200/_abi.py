@@ -18,7 +18,7 @@ STATUS_NAMES = {0: "PA_OK", 1: "PA_ERR_INVALID_ARG", 2: "PA_ERR_CUDA", 3: "PA_ER
                 4: "PA_ERR_BREAKDOWN", 5: "PA_ERR_NONFINITE", 6: "PA_ERR_NO_DEVICE", 7: "PA_ERR_UNSUPPORTED"}
 PA_CONTROL_NODAL, PA_CONTROL_CELL = 0, 1
 PA_FP64, PA_FP32 = 0, 1
-PA_SOLVER_PCG_FP64, PA_SOLVER_PCG_MIXED = 0, 1
+PA_SOLVER_PCG_FP64, PA_SOLVER_PCG_MIXED, PA_SOLVER_FCG_LEARNED = 0, 1, 2
 
 
 class ElasticParams(ct.Structure):
@@ -33,7 +33,7 @@ class SolveOptions(ct.Structure):
 
 class SolveStats(ct.Structure):
     _fields_ = [("iterations", I32), ("replacements", I32), ("rel_residual", F64), ("seconds", F64),
-                ("converged", I32), ("kernel_launches", I64)]
+                ("converged", I32), ("kernel_launches", I64), ("fallback_iterations", I32)]
 
 
 class J2Params(ct.Structure):
@@ -49,7 +49,16 @@ class J2SolveOptions(ct.Structure):
 
 class J2Stats(ct.Structure):
     _fields_ = [("steps", I32), ("newton_iterations", I32), ("cg_iterations", I64), ("seconds", F64),
-                ("final_rel_residual", F64), ("converged", I32)]
+                ("final_rel_residual", F64), ("converged", I32), ("linear_unconverged", I32)]
+
+
+class PcTrainOptions(ct.Structure):
+    _fields_ = [("steps", I32), ("batch", I32), ("learning_rate", F64), ("seed", ct.c_uint64)]
+
+
+class PcTrainStats(ct.Structure):
+    _fields_ = [("initial_loss", F64), ("final_loss", F64), ("seconds", F64), ("steps", I32),
+                ("kernel_launches", I64)]
 
 
 # (name, restype, argtypes) for every symbol of include/pa_b200.h
@@ -89,6 +98,16 @@ SIGNATURES = [
     ("pa_j2_local_residual", I32, [P, ct.POINTER(J2Params), P, P, P, P, P]),
     ("pa_j2_solve", I32, [P, ct.POINTER(J2Params), P, ct.POINTER(J2SolveOptions), ct.POINTER(SolveOptions), P, P,
                           ct.POINTER(J2Stats)]),
+    ("pa_pc_create", I32, [I32, I32, I32, ct.c_uint64, P]),
+    ("pa_pc_destroy", I32, [P]),
+    ("pa_pc_num_params", I32, [P, P]),
+    ("pa_pc_get_params", I32, [P, P]),
+    ("pa_pc_set_params", I32, [P, P]),
+    ("pa_pc_forward", I32, [P, P, P]),
+    ("pa_pc_backward", I32, [P, P, P, P]),
+    ("pa_pc_apply", I32, [P, P, P, P, P]),
+    ("pa_pc_train", I32, [P, P, I32, P, I32, P, P, P, ct.POINTER(PcTrainOptions), ct.POINTER(PcTrainStats)]),
+    ("pa_problem_set_preconditioner", I32, [P, P]),
 ]
 
 _lib = None

@@ -131,7 +131,8 @@ class SolveOptions:
     def c(self):
         o = _abi.SolveOptions()
         _abi.load().pa_solve_options_default(ct.byref(o))
-        o.method = {"fp64": _abi.PA_SOLVER_PCG_FP64, "mixed": _abi.PA_SOLVER_PCG_MIXED}[self.method]
+        o.method = {"fp64": _abi.PA_SOLVER_PCG_FP64, "mixed": _abi.PA_SOLVER_PCG_MIXED,
+                    "learned": _abi.PA_SOLVER_FCG_LEARNED}[self.method]
         o.rel_tol = float(self.rel_tol)
         o.max_iters = int(self.max_iters)
         o.check_every = int(self.check_every)
@@ -225,6 +226,11 @@ class Problem:
     def criterion_value(self, z, u):
         return self.scalar_function().value(u, z)
 
+    def set_preconditioner(self, pc):
+        """Network SolveOptions("learned") uses (None detaches); the mesh must be its grid."""
+        _abi.check(self._lib.pa_problem_set_preconditioner(self._h, pc._h if pc is not None else None))
+        self._pc = pc
+
     def criterion_gradient(self, z, u, self_adjoint=True, options=None):
         u = _as(u, np.float64)
         z = _as(z, np.float64)
@@ -290,7 +296,8 @@ class Problem:
         _abi.check(status, allow=(3,) if allow_not_converged else ())
         return u, local, {"steps": js.steps, "newton_iterations": js.newton_iterations,
                           "cg_iterations": js.cg_iterations, "seconds": js.seconds,
-                          "final_rel_residual": js.final_rel_residual, "converged": bool(js.converged)}
+                          "final_rel_residual": js.final_rel_residual, "converged": bool(js.converged),
+                          "linear_unconverged": js.linear_unconverged}
 
     def close(self):
         if self._h:
@@ -306,7 +313,8 @@ class Problem:
 
 def _stats(st):
     return {"iterations": st.iterations, "replacements": st.replacements, "rel_residual": st.rel_residual,
-            "seconds": st.seconds, "converged": bool(st.converged), "kernel_launches": st.kernel_launches}
+            "seconds": st.seconds, "converged": bool(st.converged), "kernel_launches": st.kernel_launches,
+            "fallback_iterations": st.fallback_iterations}
 
 
 class VectorFunction:
@@ -397,3 +405,88 @@ class PhysicsScalarFunction:
                                                 _ptr(z, np.float64, self.p.nz, "z"),
                                                 _ptr(out, np.float64, self.p.ndof, "grad")))
         return out
+
+
+class LearnedPreconditioner:
+    """Convolutional preconditioner on the nodal grid of a structured box
+    (pa_pc_*): M r = D^-1 r + s D^-1/2 f(D^-1/2 r / s, stiffness, Dirichlet).
+    No counterpart in the reference; used by SolveOptions("learned")."""
+
+    def __init__(self, grid, seed=0):
+        self._lib = _abi.load()
+        self.grid = tuple(int(g) for g in grid)
+        h = ct.c_void_p()
+        _abi.check(self._lib.pa_pc_create(*self.grid, ct.c_uint64(seed), ct.byref(h)))
+        self._h = h
+        n = ct.c_int64()
+        _abi.check(self._lib.pa_pc_num_params(self._h, ct.byref(n)))
+        self.num_params = n.value
+        self.num_points = self.grid[0] * self.grid[1] * self.grid[2]
+
+    @classmethod
+    def for_box(cls, nx, ny, nz, seed=0):
+        return cls((nx + 1, ny + 1, nz + 1), seed)
+
+    def get_params(self):
+        out = np.empty(self.num_params, np.float32)
+        _abi.check(self._lib.pa_pc_get_params(self._h, _ptr(out, np.float32, self.num_params)))
+        return out
+
+    def set_params(self, params):
+        params = np.ascontiguousarray(params, np.float32)
+        _abi.check(self._lib.pa_pc_set_params(self._h, _ptr(params, np.float32, self.num_params, "params")))
+
+    def forward(self, features):
+        f = _as(features, np.float32)
+        out = _empty(f, 3 * self.num_points, np.float32)
+        _abi.check(self._lib.pa_pc_forward(self._h, _ptr(f, np.float32, 5 * self.num_points, "features"),
+                                           _ptr(out, np.float32, 3 * self.num_points, "out")))
+        return out
+
+    def backward(self, features, grad_out):
+        f = _as(features, np.float32)
+        g = _as(grad_out, np.float32)
+        out = _empty(f, self.num_params, np.float32)
+        _abi.check(self._lib.pa_pc_backward(self._h, _ptr(f, np.float32, 5 * self.num_points, "features"),
+                                            _ptr(g, np.float32, 3 * self.num_points, "grad_out"),
+                                            _ptr(out, np.float32, self.num_params, "grad_params")))
+        return out
+
+    def apply(self, problem, z, r, out=None):
+        z, r = _as(z, np.float64), _as(r, np.float64)
+        out = _empty(r, problem.ndof) if out is None else out
+        _abi.check(self._lib.pa_pc_apply(problem._h, self._h, _ptr(z, np.float64, problem.nz, "z"),
+                                         _ptr(r, np.float64, problem.ndof, "r"),
+                                         _ptr(out, np.float64, problem.ndof, "out")))
+        return out
+
+    def train(self, problem, densities, sample_density, residuals, energies, steps=200, batch=4,
+              learning_rate=1e-3, seed=0):
+        """Train on (residual, error) pairs: residuals[s] = K(densities[sample_density[s]]) e_s
+        (zero on constrained dofs), energies[s] = e_s . residuals[s]."""
+        densities = _as(densities, np.float64)
+        residuals = _as(residuals, np.float64)
+        sd = np.ascontiguousarray(sample_density, np.int32)
+        en = np.ascontiguousarray(energies, np.float64)
+        nd = (densities.numel() if _is_torch(densities) else densities.size) // problem.nz
+        ns = sd.size
+        o = _abi.PcTrainOptions(int(steps), int(batch), float(learning_rate), int(seed))
+        st = _abi.PcTrainStats()
+        _abi.check(self._lib.pa_pc_train(problem._h, self._h, nd, _ptr(densities, np.float64, nd * problem.nz,
+                                                                          "densities"),
+                                         ns, _ptr(sd, np.int32, ns), _ptr(residuals, np.float64, ns * problem.ndof,
+                                                                          "residuals"),
+                                         _ptr(en, np.float64, ns), ct.byref(o), ct.byref(st)))
+        return {"initial_loss": st.initial_loss, "final_loss": st.final_loss, "seconds": st.seconds,
+                "steps": st.steps, "kernel_launches": st.kernel_launches}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.pa_pc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -7,6 +7,7 @@
 
 #include "pa_problem.cuh"
 #include "pa_cell.cuh"
+#include "pa_learned.cuh"
 
 namespace pa {
 
@@ -144,6 +145,10 @@ struct pa_problem {
 };
 struct pa_mesh {
   pa::Mesh m;
+};
+struct pa_pc {
+  pa::LearnedPC* pc = nullptr;
+  ~pa_pc() { pa::pc_delete(pc); }
 };
 
 using pa::Error;
@@ -696,6 +701,181 @@ pa_status pa_j2_solve(pa_problem* problem, const pa_j2_params* params, const dou
     pa_status s = pa::j2_solve(P, *params, dz, *options, lo, du, dl, stats);
     st.finish();
     return s;
+  });
+}
+
+}  // extern "C"
+
+/* ------------------------------------------------ learned preconditioner --- */
+
+namespace {
+
+pa::LearnedPC& pcref(pa_pc* h) {
+  if (!h || !h->pc) throw Error(PA_ERR_INVALID_ARG, "null pa_pc");
+  PA_CUDA(cudaSetDevice(pa::pc_device(*h->pc)));
+  return *h->pc;
+}
+
+// Device view of a caller array for a network-only call (host arrays copied in).
+template <typename T>
+const T* pc_in(const T* p, int64_t count, pa::DevBuf<char>& tmp, cudaStream_t s, const char* name) {
+  PA_CHECK(p != nullptr, std::string("null pointer: ") + name);
+  if (pa::is_device_pointer(p)) return p;
+  tmp.resize(size_t(count) * sizeof(T));
+  PA_CUDA(cudaMemcpyAsync(tmp.get(), p, size_t(count) * sizeof(T), cudaMemcpyHostToDevice, s));
+  return reinterpret_cast<const T*>(tmp.get());
+}
+
+// Device output for a network-only call; copied back to a host array by pc_out_finish.
+template <typename T>
+T* pc_out(T* p, int64_t count, pa::DevBuf<char>& tmp, const char* name) {
+  PA_CHECK(p != nullptr, std::string("null pointer: ") + name);
+  if (pa::is_device_pointer(p)) return p;
+  tmp.resize(size_t(count) * sizeof(T));
+  return reinterpret_cast<T*>(tmp.get());
+}
+template <typename T>
+void pc_out_finish(T* p, const T* d, int64_t count, cudaStream_t s) {
+  if (static_cast<const void*>(p) != static_cast<const void*>(d))
+    PA_CUDA(cudaMemcpyAsync(p, d, size_t(count) * sizeof(T), cudaMemcpyDeviceToHost, s));
+  PA_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace
+
+extern "C" {
+
+pa_status pa_pc_create(int32_t gx, int32_t gy, int32_t gz, uint64_t seed, pa_pc** out) {
+  return guard([&] {
+    PA_CHECK(out, "null argument");
+    pa::require_device();
+    std::unique_ptr<pa_pc> h(new pa_pc());
+    h->pc = pa::pc_new(gx, gy, gz, seed);
+    *out = h.release();
+  });
+}
+
+pa_status pa_pc_destroy(pa_pc* pc) {
+  return guard([&] {
+    if (pc && pc->pc) PA_CUDA(cudaSetDevice(pa::pc_device(*pc->pc)));
+    delete pc;
+  });
+}
+
+pa_status pa_pc_num_params(const pa_pc* pc, int64_t* count) {
+  return guard([&] {
+    PA_CHECK(pc && count, "null argument");
+    *count = pa::pc_num_params();
+  });
+}
+
+pa_status pa_pc_get_params(pa_pc* pc, float* params) {
+  return guard([&] {
+    pa::LearnedPC& L = pcref(pc);
+    cudaStream_t s = pa::pc_stream(L);
+    pa::DevBuf<char> t;
+    const int64_t n = pa::pc_num_params();
+    float* d = pc_out(params, n, t, "params");
+    pa::pc_get_params(L, d, s);
+    pc_out_finish(params, d, n, s);
+  });
+}
+
+pa_status pa_pc_set_params(pa_pc* pc, const float* params) {
+  return guard([&] {
+    pa::LearnedPC& L = pcref(pc);
+    cudaStream_t s = pa::pc_stream(L);
+    pa::DevBuf<char> t;
+    pa::pc_set_params(L, pc_in(params, pa::pc_num_params(), t, s, "params"), s);
+    PA_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+pa_status pa_pc_forward(pa_pc* pc, const float* features, float* out) {
+  return guard([&] {
+    pa::LearnedPC& L = pcref(pc);
+    cudaStream_t s = pa::pc_stream(L);
+    const int64_t G = pa::pc_grid_points(L);
+    pa::DevBuf<char> ti, to;
+    const float* df = pc_in(features, 5 * G, ti, s, "features");
+    float* dout = pc_out(out, 3 * G, to, "out");
+    pa::pc_forward_features(L, df, dout, s);
+    pc_out_finish(out, dout, 3 * G, s);
+  });
+}
+
+pa_status pa_pc_backward(pa_pc* pc, const float* features, const float* grad_out, float* grad_params) {
+  return guard([&] {
+    pa::LearnedPC& L = pcref(pc);
+    cudaStream_t s = pa::pc_stream(L);
+    const int64_t G = pa::pc_grid_points(L), np = pa::pc_num_params();
+    pa::DevBuf<char> tf, tg, to;
+    const float* df = pc_in(features, 5 * G, tf, s, "features");
+    const float* dg = pc_in(grad_out, 3 * G, tg, s, "grad_out");
+    float* dp = pc_out(grad_params, np, to, "grad_params");
+    pa::pc_backward_features(L, df, dg, dp, s);
+    pc_out_finish(grad_params, dp, np, s);
+  });
+}
+
+pa_status pa_pc_apply(pa_problem* problem, pa_pc* pc, const double* z, const double* r, double* out) {
+  return guard([&] {
+    Problem& P = prob(problem);
+    pa::LearnedPC& L = pcref(pc);
+    pa::pc_check_grid(L, *P.mesh);
+    pa::Stage st(P);
+    const double* dz = st.in(z, P.nz(), "z");
+    const double* dr = st.in(r, P.ndof(), "r");
+    double* dout = st.out(out, P.ndof(), "out");
+    pa::pc_apply(L, P, dz, dr, dout);
+    st.finish();
+  });
+}
+
+pa_status pa_pc_train(pa_problem* problem, pa_pc* pc, int32_t num_densities, const double* densities,
+                      int32_t num_samples, const int32_t* sample_density, const double* residuals,
+                      const double* energies, const pa_pc_train_options* options, pa_pc_train_stats* stats) {
+  return guard([&] {
+    Problem& P = prob(problem);
+    pa::LearnedPC& L = pcref(pc);
+    PA_CHECK(options != nullptr, "null options");
+    PA_CHECK(num_densities > 0 && num_samples > 0, "empty training set");
+    PA_CHECK(sample_density && energies, "null argument");
+    pa::pc_check_grid(L, *P.mesh);
+    pa::Stage st(P);
+    pa::PcTrainSet set;
+    set.num_densities = num_densities;
+    set.num_samples = num_samples;
+    set.densities = st.in(densities, int64_t(num_densities) * P.nz(), "densities");
+    set.residuals = st.in(residuals, int64_t(num_samples) * P.ndof(), "residuals");
+    set.sample_density.resize(num_samples);
+    set.sample_energy.resize(num_samples);
+    if (pa::is_device_pointer(sample_density))
+      PA_CUDA(cudaMemcpy(set.sample_density.data(), sample_density, sizeof(int32_t) * num_samples,
+                         cudaMemcpyDeviceToHost));
+    else
+      std::copy(sample_density, sample_density + num_samples, set.sample_density.begin());
+    if (pa::is_device_pointer(energies))
+      PA_CUDA(cudaMemcpy(set.sample_energy.data(), energies, sizeof(double) * num_samples, cudaMemcpyDeviceToHost));
+    else
+      std::copy(energies, energies + num_samples, set.sample_energy.begin());
+    pa::pc_train(L, P, set, *options, stats);
+    st.finish();
+  });
+}
+
+pa_status pa_problem_set_preconditioner(pa_problem* problem, pa_pc* pc) {
+  return guard([&] {
+    Problem& P = prob(problem);
+    PA_CHECK(P.ep.layout == PA_CONTROL_CELL || P.ep.layout == PA_CONTROL_NODAL, "bad problem");
+    if (!pc) {
+      P.pc = nullptr;
+      return;
+    }
+    pa::LearnedPC& L = pcref(pc);
+    PA_CHECK(pa::pc_device(L) == P.mesh->device, "network and problem live on different devices");
+    pa::pc_check_grid(L, *P.mesh);
+    P.pc = &L;
   });
 }
 

@@ -575,6 +575,8 @@ template void launch_aos_to_soa<double, double>(const double*, double*, int64_t,
 template void launch_aos_to_soa<float, float>(const float*, float*, int64_t, cudaStream_t);
 template void launch_soa_to_aos<double, double>(const double*, double*, int64_t, cudaStream_t);
 template void launch_soa_to_aos<float, float>(const float*, float*, int64_t, cudaStream_t);
+template void launch_aos_to_soa<double, float>(const double*, float*, int64_t, cudaStream_t);
+template void launch_soa_to_aos<float, double>(const float*, double*, int64_t, cudaStream_t);
 template void launch_copy_dofs<double>(const int32_t*, int64_t, const double*, double*, cudaStream_t);
 template void launch_copy_dofs<float>(const int32_t*, int64_t, const float*, float*, cudaStream_t);
 

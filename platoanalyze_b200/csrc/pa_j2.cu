@@ -382,57 +382,77 @@ pa_status j2_solve(Problem& P, const pa_j2_params& jp, const double* z, const pa
   int newton_total = 0;
   int64_t cg_total = 0;
   bool all_converged = true;
-  double last_rel = 0.0;
+  double last_rel = 0.0, worst_rel = 0.0;
+  int linear_unconverged = 0;
   pa_status status = PA_OK;
+  // residual (and tangent records) at u; b = -R on the free dofs; returns ||R_free||
+  auto residual = [&]() {
+    PA_CUDA(cudaMemsetAsync(R.get(), 0, sizeof(double) * n, s));
+    k_j2_newton<<<grid, kJ2Threads, 0, s>>>(P.mesh->d_cells.get(), P.mesh->d_coords.get(), C, q, u, z, prev.get(),
+                                           local, P.mesh->d_cell_iperm.get(), rec64.get(), rec32.get(), w64.get(),
+                                           w32.get(), R.get());
+    PA_LAUNCHED();
+    PA_CUDA(cudaMemsetAsync(sumsq.get(), 0, sizeof(double), s));
+    k_axpy_neg_masked<<<int(std::min<int64_t>((n + 255) / 256, 148 * 8)), 256, 0, s>>>(
+        n, P.d_node_mask.get(), R.get(), b.get(), sumsq.get());
+    PA_LAUNCHED();
+    double h = 0.0;
+    PA_CUDA(cudaMemcpyAsync(&h, sumsq.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
+    PA_CUDA(cudaStreamSynchronize(s));
+    return std::sqrt(h);
+  };
+  // K_T du = -R with the tangent of the last residual evaluation; Dirichlet
+  // values of du: bc_scale x the problem's (0: homogeneous)
+  auto tangent_solve = [&](double bc_scale) {
+    PA_CUDA(cudaMemsetAsync(diag.get(), 0, sizeof(double) * n, s));
+    k_j2_diag<<<int((C + 127) / 128), 128, 0, s>>>(P.mesh->d_cells.get(), P.mesh->d_coords.get(), C, q,
+                                                  P.mesh->d_cell_iperm.get(), rec64.get(), w64.get(), diag.get());
+    PA_LAUNCHED();
+    SolveOperator op;
+    op.w64 = w64.get();
+    op.w32 = w32.get();
+    op.plas64 = rec64.get();
+    op.plas32 = rec32.get();
+    op.diag_aos = diag.get();
+    op.homogeneous_bc = bc_scale == 0.0;
+    op.bc_scale = bc_scale;
+    pa_solve_stats st{};
+    const pa_status ls = solve_operator(P, op, b.get(), du.get(), lo, &st, true);
+    cg_total += st.iterations;
+    ++newton_total;
+    if (ls == PA_ERR_NOT_CONVERGED) ++linear_unconverged;
+    if (ls != PA_OK && ls != PA_ERR_NOT_CONVERGED) return ls;
+    k_add<<<int(std::min<int64_t>((n + 255) / 256, 148 * 8)), 256, 0, s>>>(n, du.get(), u);
+    PA_LAUNCHED();
+    return PA_OK;
+  };
   for (int step = 0; step < jo.steps && status == PA_OK; ++step) {
+    const double s_old = double(step) / jo.steps, s_new = double(step + 1) / jo.steps;
+    // reference norm of the step: the residual with the new boundary values
+    // on the last converged field
     if (nbc)
-      k_set_dofs<<<int((nbc + 255) / 256), 256, 0, s>>>(nbc, P.d_bc_dofs.get(), P.d_bc_vals.get(),
-                                                        double(step + 1) / jo.steps, u);
-    double r0 = -1.0;
+      k_set_dofs<<<int((nbc + 255) / 256), 256, 0, s>>>(nbc, P.d_bc_dofs.get(), P.d_bc_vals.get(), s_new, u);
+    const double r0 = residual();
+    if (!std::isfinite(r0)) { status = PA_ERR_NONFINITE; break; }
+    if (nbc)
+      k_set_dofs<<<int((nbc + 255) / 256), 256, 0, s>>>(nbc, P.d_bc_dofs.get(), P.d_bc_vals.get(), s_old, u);
+    // predictor (NewtonRaphsonSolver's first iteration, src/NewtonRaphsonSolver.hpp:127-131):
+    // residual and tangent at the converged state, the Dirichlet increment imposed in the solve
+    residual();
+    status = tangent_solve(s_new - s_old);
+    if (status != PA_OK) break;
     bool converged = false;
     for (int it = 0; it < jo.max_newton; ++it) {
-      PA_CUDA(cudaMemsetAsync(R.get(), 0, sizeof(double) * n, s));
-      k_j2_newton<<<grid, kJ2Threads, 0, s>>>(P.mesh->d_cells.get(), P.mesh->d_coords.get(), C, q, u, z, prev.get(),
-                                             local, P.mesh->d_cell_iperm.get(), rec64.get(), rec32.get(), w64.get(),
-                                             w32.get(), R.get());
-      PA_LAUNCHED();
-      PA_CUDA(cudaMemsetAsync(sumsq.get(), 0, sizeof(double), s));
-      k_axpy_neg_masked<<<int(std::min<int64_t>((n + 255) / 256, 148 * 8)), 256, 0, s>>>(
-          n, P.d_node_mask.get(), R.get(), b.get(), sumsq.get());
-      PA_LAUNCHED();
-      double h = 0.0;
-      PA_CUDA(cudaMemcpyAsync(&h, sumsq.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
-      PA_CUDA(cudaStreamSynchronize(s));
-      const double rn = std::sqrt(h);
+      const double rn = residual();
       if (!std::isfinite(rn)) { status = PA_ERR_NONFINITE; break; }
-      if (r0 < 0.0) r0 = rn;
       last_rel = r0 > 0.0 ? rn / r0 : 0.0;
       if (rn <= jo.newton_tol * r0 || rn == 0.0) { converged = true; break; }
-      ++newton_total;
-      // K_T du = -R with homogeneous Dirichlet conditions
-      PA_CUDA(cudaMemsetAsync(diag.get(), 0, sizeof(double) * n, s));
-      k_j2_diag<<<int((C + 127) / 128), 128, 0, s>>>(P.mesh->d_cells.get(), P.mesh->d_coords.get(), C, q,
-                                                    P.mesh->d_cell_iperm.get(), rec64.get(), w64.get(), diag.get());
-      PA_LAUNCHED();
-      SolveOperator op;
-      op.w64 = w64.get();
-      op.w32 = w32.get();
-      op.plas64 = rec64.get();
-      op.plas32 = rec32.get();
-      op.diag_aos = diag.get();
-      op.homogeneous_bc = true;
-      pa_solve_stats st{};
-      const pa_status ls = solve_operator(P, op, b.get(), du.get(), lo, &st, true);
-      cg_total += st.iterations;
-      if (ls != PA_OK && ls != PA_ERR_NOT_CONVERGED) { status = ls; break; }
-      k_add<<<int(std::min<int64_t>((n + 255) / 256, 148 * 8)), 256, 0, s>>>(n, du.get(), u);
-      PA_LAUNCHED();
+      status = tangent_solve(0.0);
+      if (status != PA_OK) break;
     }
     if (status != PA_OK) break;
-    if (!converged) {
-      // final return mapping at the last iterate so `local` matches u
-      all_converged = false;
-    }
+    if (!converged) all_converged = false;
+    worst_rel = std::max(worst_rel, last_rel);
     PA_CUDA(cudaMemcpyAsync(prev.get(), local, sizeof(double) * 14 * C, cudaMemcpyDeviceToDevice, s));
   }
   PA_CUDA(cudaEventRecord(t1, s));
@@ -447,7 +467,8 @@ pa_status j2_solve(Problem& P, const pa_j2_params& jp, const double* z, const pa
     js->newton_iterations = newton_total;
     js->cg_iterations = cg_total;
     js->seconds = ms * 1e-3;
-    js->final_rel_residual = last_rel;
+    js->final_rel_residual = worst_rel;
+    js->linear_unconverged = linear_unconverged;
     js->converged = all_converged ? 1 : 0;
   }
   if (status != PA_OK) return status;

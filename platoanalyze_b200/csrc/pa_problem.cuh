@@ -14,6 +14,8 @@ struct SolverWorkspace {
   // FP32 vectors (mixed precision)
   DevBuf<float> r32, p32a, p32b, ap32, dinv32, dx32, w32;
   DevBuf<float> coords32;
+  DevBuf<float> ones32, z32;   // flexible CG: all-ones "diagonal", preconditioned residual
+  DevBuf<double> fcg_state;    // flexible CG scalars
   DevBuf<double> partials;
   DevBuf<unsigned int> counters;
   DevBuf<PcgScalars> sc;
@@ -30,10 +32,14 @@ struct SolveOperator {
   const float* plas32 = nullptr;
   const double* diag_aos = nullptr;
   bool homogeneous_bc = false;  // impose zero (not the problem's) Dirichlet values
+  double bc_scale = 1.0;        // otherwise impose bc_scale times the problem's values
 };
+
+struct LearnedPC;
 
 struct Problem {
   Mesh* mesh = nullptr;
+  LearnedPC* pc = nullptr;  // network of PA_SOLVER_FCG_LEARNED (not owned)
   ElasticParams ep{};
   cudaStream_t stream = nullptr;
   bool own_stream = false;

@@ -22,8 +22,10 @@
 // FP64 operator and replaces the recursive FP32 residual (reliable updates),
 // and convergence is decided on that FP64 residual.
 #include <cmath>
+#include <cstddef>
 #include <algorithm>
 
+#include "pa_learned.cuh"
 #include "pa_problem.cuh"
 #include "pa_tiled.cuh"
 
@@ -255,6 +257,160 @@ __global__ void k_dot2(int64_t n, const double* __restrict__ a, const double* __
   if (threadIdx.x == 0) { atomicAdd(&out[0], s); atomicAdd(&out[1], t); }
 }
 
+// ---------------------------------------------------------- flexible CG --
+// Flexible CG (one-term truncation) with the learned preconditioner M:
+//   z = M r,  beta = -(z . q_old) / (p_old . q_old),  p = z + beta p_old,
+//   q = K p,  alpha = (z . r) / (p . q),  x += alpha p,  r -= alpha q.
+// p, q and p.q come from the fused apply kernel in its PCG mode, given z in
+// place of r and an all-ones vector in place of D^-1.
+struct FcgState {
+  double rdr;      // r . D^-1 r of the current residual (the network's input scale)
+  double pq_prev;  // p . K p of the previous direction
+  int32_t first;   // 1: the next direction is z itself
+  int32_t pad;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) k_fcg_z(int64_t N, const T* __restrict__ r, const T* __restrict__ dinv,
+                                                       const float* __restrict__ dsq, const float* __restrict__ out,
+                                                       T* __restrict__ q, T* __restrict__ z, FcgState* __restrict__ fs,
+                                                       double inv_nfree, PcgScalars* __restrict__ sc,
+                                                       double* __restrict__ partials, unsigned int* counter) {
+  __shared__ double s_red[64];
+  if (sc->done) return;
+  const double s2 = fs->rdr * inv_nfree;
+  const T sig = T(s2 > 0.0 ? sqrt(s2) : 0.0);
+  double zq = 0.0, zr = 0.0;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < 3 * N; i += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t d = i / N, v = i - d * N;
+    const T zi = dinv[i] * r[i] + sig * T(dsq[i]) * T(out[4 * v + d]);
+    zq += double(zi) * double(q[i]);
+    zr += double(zi) * double(r[i]);
+    q[i] = T(0);
+    z[i] = zi;
+  }
+  block_sum2(zq, zr, s_red);
+  if (threadIdx.x == 0) { partials[2 * blockIdx.x] = zq; partials[2 * blockIdx.x + 1] = zr; }
+  if (last_block_arrive(counter)) {
+    double t0 = 0.0, t1 = 0.0;
+    for (int i = threadIdx.x; i < gridDim.x; i += blockDim.x) {
+      t0 += __ldcg(&partials[2 * i]);
+      t1 += __ldcg(&partials[2 * i + 1]);
+    }
+    block_sum2(t0, t1, s_red);
+    if (threadIdx.x == 0) {
+      if (!(t1 > 0.0) || !isfinite(t0) || !isfinite(t1)) {
+        sc->breakdown = 2;  // not a descent direction: the host falls back to Jacobi
+        sc->done = 1;
+      } else {
+        sc->beta = fs->first ? 0.0 : -t0 / fs->pq_prev;
+        sc->rz = t1;
+        fs->first = 0;
+      }
+      *counter = 0u;
+    }
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void fcg_update_one(T& x, T& r, T p, T q, T dinv, T a, double& rdr, double& rr) {
+  x += a * p;
+  const T ri = r - a * q;
+  r = ri;
+  rdr += double(ri) * double(dinv * ri);
+  rr += double(ri) * double(ri);
+}
+
+// x += alpha p, r -= alpha q (q kept for the next beta), r.D^-1 r and r.r; the
+// last CTA keeps p.q, counts the iteration and sets the convergence flag.
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) k_fcg_update(int64_t n, T* __restrict__ x, T* __restrict__ r,
+                                                            const T* __restrict__ p, const T* __restrict__ q,
+                                                            const T* __restrict__ dinv, PcgScalars* __restrict__ sc,
+                                                            FcgState* __restrict__ fs, double* __restrict__ partials,
+                                                            unsigned int* counter) {
+  using V = typename Vec16<T>::type;
+  constexpr int W = Vec16<T>::n;
+  __shared__ double s_red[64];
+  if (sc->done) return;
+  const T a = T(sc->alpha);
+  double rdr = 0.0, rr = 0.0;
+  const int64_t nv = n / W;
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nv; i += stride) {
+    V xv = reinterpret_cast<V*>(x)[i], rv = reinterpret_cast<V*>(r)[i];
+    const V pv = reinterpret_cast<const V*>(p)[i], qv = reinterpret_cast<const V*>(q)[i];
+    const V dv = reinterpret_cast<const V*>(dinv)[i];
+    T* xs = reinterpret_cast<T*>(&xv);
+    T* rs = reinterpret_cast<T*>(&rv);
+    const T* ps = reinterpret_cast<const T*>(&pv);
+    const T* qs = reinterpret_cast<const T*>(&qv);
+    const T* ds = reinterpret_cast<const T*>(&dv);
+#pragma unroll
+    for (int k = 0; k < W; ++k) fcg_update_one(xs[k], rs[k], ps[k], qs[k], ds[k], a, rdr, rr);
+    reinterpret_cast<V*>(x)[i] = xv;
+    reinterpret_cast<V*>(r)[i] = rv;
+  }
+  for (int64_t i = nv * W + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += stride)
+    fcg_update_one(x[i], r[i], p[i], q[i], dinv[i], a, rdr, rr);
+  block_sum2(rdr, rr, s_red);
+  if (threadIdx.x == 0) { partials[2 * blockIdx.x] = rdr; partials[2 * blockIdx.x + 1] = rr; }
+  if (last_block_arrive(counter)) {
+    double t0 = 0.0, t1 = 0.0;
+    for (int i = threadIdx.x; i < gridDim.x; i += blockDim.x) {
+      t0 += __ldcg(&partials[2 * i]);
+      t1 += __ldcg(&partials[2 * i + 1]);
+    }
+    block_sum2(t0, t1, s_red);
+    if (threadIdx.x == 0) {
+      fs->rdr = t0;
+      fs->pq_prev = sc->pap;
+      sc->rr = t1;
+      sc->iters = sc->iters + 1;
+      if (!isfinite(t0) || !isfinite(t1)) { sc->breakdown = 1; sc->done = 1; }
+      if (t1 <= sc->stop2) sc->done = 1;
+      *counter = 0u;
+    }
+  }
+}
+
+// r.D^-1 r and r.r of a fresh residual; `reset` restarts the direction recurrence.
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) k_fcg_init(int64_t n, const T* __restrict__ r, const T* __restrict__ dinv,
+                                                          FcgState* __restrict__ fs, PcgScalars* __restrict__ sc,
+                                                          double* __restrict__ partials, unsigned int* counter,
+                                                          int reset) {
+  __shared__ double s_red[64];
+  double rdr = 0.0, rr = 0.0;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    const double ri = double(r[i]);
+    rdr += ri * double(dinv[i]) * ri;
+    rr += ri * ri;
+  }
+  block_sum2(rdr, rr, s_red);
+  if (threadIdx.x == 0) { partials[2 * blockIdx.x] = rdr; partials[2 * blockIdx.x + 1] = rr; }
+  if (last_block_arrive(counter)) {
+    double t0 = 0.0, t1 = 0.0;
+    for (int i = threadIdx.x; i < gridDim.x; i += blockDim.x) {
+      t0 += __ldcg(&partials[2 * i]);
+      t1 += __ldcg(&partials[2 * i + 1]);
+    }
+    block_sum2(t0, t1, s_red);
+    if (threadIdx.x == 0) {
+      fs->rdr = t0;
+      if (reset) fs->first = 1;
+      sc->rr = t1;
+      sc->done = (t1 <= sc->stop2) ? 1 : 0;
+      *counter = 0u;
+    }
+  }
+}
+
+__global__ void k_fill_f32(int64_t n, float v, float* __restrict__ out) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    out[i] = v;
+}
+
 template <typename T>
 int fused_apply_grid(const Mesh& m) {
   return apply_kernel_setup<T, 1>(m);
@@ -423,7 +579,7 @@ pa_status solve_operator(Problem& P, const SolveOperator& op, const double* b, d
   double* bprime = ws.b.get();
   if (nbc) {
     PA_CUDA(cudaMemsetAsync(ws.p0.get(), 0, sizeof(double) * n, s));
-    k_scatter_bc<<<int((nbc + 255) / 256), 256, 0, s>>>(nbc, P.d_bc_dofs.get(), P.d_bc_vals.get(), 1.0, N,
+    k_scatter_bc<<<int((nbc + 255) / 256), 256, 0, s>>>(nbc, P.d_bc_dofs.get(), P.d_bc_vals.get(), op.bc_scale, N,
                                                         ws.p0.get());
     PA_LAUNCHED();
     launch_apply_tiled<double>(P, op.w64, ws.p0.get(), ws.t.get(), false, s, op.plas64);
@@ -516,7 +672,8 @@ pa_status solve_operator(Problem& P, const SolveOperator& op, const double* b, d
   launch_soa_to_aos<double, double>(ws.x.get(), x_out, N, s);
   launches += 1;
   if (nbc) {
-    k_set_bc<<<int((nbc + 255) / 256), 256, 0, s>>>(nbc, P.d_bc_dofs.get(), P.d_bc_vals.get(), 1.0, x_out);
+    k_set_bc<<<int((nbc + 255) / 256), 256, 0, s>>>(nbc, P.d_bc_dofs.get(), P.d_bc_vals.get(), op.bc_scale,
+                                                    x_out);
     PA_LAUNCHED();
     launches += 1;
   }
@@ -531,16 +688,243 @@ pa_status solve_operator(Problem& P, const SolveOperator& op, const double* b, d
     st->seconds = ms * 1e-3;
     st->converged = converged ? 1 : 0;
     st->kernel_launches = launches;
+    st->fallback_iterations = 0;
   }
   if (breakdown) return PA_ERR_BREAKDOWN;
   if (!std::isfinite(relres)) return PA_ERR_NONFINITE;
   return converged ? PA_OK : PA_ERR_NOT_CONVERGED;
 }
 
+// Flexible CG with the learned preconditioner, mixed precision as in
+// solve_operator (FP32 vectors and apply, FP64 dots, FP64 x and true-residual
+// replacement once per chunk).  One iteration = the network (pack + four
+// convolutions), z/beta, the fused apply (p, K p, p.Kp, alpha), the update.
+// The solve continues as mixed Jacobi-PCG from the current iterate when the
+// network's direction is not a descent direction or the true residual has not
+// decreased over two chunks.
+pa_status solve_fcg(Problem& P, const SolveOperator& op, LearnedPC& pc, const double* b, double* x_out,
+                    const pa_solve_options& o, pa_solve_stats* st) {
+  cudaStream_t s = P.stream;
+  const int64_t n = P.ndof(), N = P.N();
+  PA_CHECK(o.rel_tol > 0.0, "rel_tol must be positive");
+  PA_CHECK(op.w32 != nullptr && op.plas32 == nullptr, "the learned preconditioner serves the elastic operator");
+  const int grid_need = std::max(std::max(fused_apply_grid<double>(*P.mesh), fused_apply_grid<float>(*P.mesh)),
+                                vec_grid(n));
+  P.ws.ensure(n, P.C(), grid_need, true);
+  SolverWorkspace& ws = P.ws;
+  if (ws.ones32.n != size_t(n)) { ws.ones32.resize(n); ws.z32.resize(n); }
+  if (ws.fcg_state.n < 4) ws.fcg_state.resize(4);
+  FcgState* fs = reinterpret_cast<FcgState*>(ws.fcg_state.get());
+  const int max_iters = o.max_iters > 0 ? o.max_iters : int(20.0 * std::sqrt(double(n)) + 1000);
+  int chunk = o.check_every > 0 ? o.check_every : 64;
+  chunk += chunk % 2;
+  const double tol2 = o.rel_tol * o.rel_tol;
+  const int vg = vec_grid(n);
+  const uint8_t* mask = P.d_node_mask.get();
+  const int64_t nbc = op.homogeneous_bc ? 0 : int64_t(P.bc_dofs.size());
+  const double inv_nfree = 1.0 / double(free_dofs(P));
+  int64_t launches = 0;
+
+  if (!P.ev0) { PA_CUDA(cudaEventCreate(&P.ev0)); PA_CUDA(cudaEventCreate(&P.ev1)); }
+  cudaEvent_t t0;
+  PA_CUDA(cudaEventCreate(&t0));
+  PA_CUDA(cudaEventRecord(t0, s));
+
+  // operator pieces: D^-1 (FP32, SoA), D^-1/2 and node features; ones for the fused apply
+  pc_prepare_operator(pc, P, op.diag_aos, ws.dinv32.get(), s);
+  k_fill_f32<<<vg, kVecThreads, 0, s>>>(n, 1.0f, ws.ones32.get());
+  PA_LAUNCHED();
+  launches += 3;
+  // b' = mask(b - K x_D)
+  double* bprime = ws.b.get();
+  if (nbc) {
+    PA_CUDA(cudaMemsetAsync(ws.p0.get(), 0, sizeof(double) * n, s));
+    k_scatter_bc<<<int((nbc + 255) / 256), 256, 0, s>>>(nbc, P.d_bc_dofs.get(), P.d_bc_vals.get(), op.bc_scale, N,
+                                                        ws.p0.get());
+    PA_LAUNCHED();
+    launch_apply_tiled<double>(P, op.w64, ws.p0.get(), ws.t.get(), false, s);
+    k_aos_minus_soa<<<vg, kVecThreads, 0, s>>>(N, b, ws.t.get(), mask, bprime);
+    launches += 3;
+  } else {
+    k_aos_minus_soa<<<vg, kVecThreads, 0, s>>>(N, b, nullptr, nullptr, bprime);
+    launches += 1;
+  }
+  PA_LAUNCHED();
+  if (o.use_initial_guess) {
+    k_aos_minus_soa<<<vg, kVecThreads, 0, s>>>(N, x_out, nullptr, mask, ws.x.get());
+    launches += 1;
+  } else {
+    PA_CUDA(cudaMemsetAsync(ws.x.get(), 0, sizeof(double) * n, s));
+  }
+  PA_LAUNCHED();
+  auto true_residual = [&]() {
+    launch_apply_tiled<double>(P, op.w64, ws.x.get(), ws.t.get(), true, s);
+    k_sub_masked<<<vg, kVecThreads, 0, s>>>(N, bprime, ws.t.get(), mask, ws.r.get());
+    PA_LAUNCHED();
+    launches += 3;
+    return host_norm2(P, ws.r.get());
+  };
+  double bb = host_norm2(P, bprime);
+  launches += 1;
+  if (!(bb > 0.0)) bb = 1.0;
+  double rr_true = true_residual();
+
+  PA_CUDA(cudaMemsetAsync(ws.dx32.get(), 0, sizeof(float) * n, s));
+  PA_CUDA(cudaMemsetAsync(ws.p32a.get(), 0, sizeof(float) * n, s));
+  PA_CUDA(cudaMemsetAsync(ws.p32b.get(), 0, sizeof(float) * n, s));
+  PA_CUDA(cudaMemsetAsync(ws.ap32.get(), 0, sizeof(float) * n, s));
+
+  // one chunk of iterations, captured once
+  const int32_t* done = reinterpret_cast<const int32_t*>(reinterpret_cast<const char*>(ws.sc.get()) +
+                                                         offsetof(PcgScalars, done));
+  const int ag = fused_apply_grid<float>(*P.mesh);
+  const float* coords32 = P.mesh->d_coords32_soa.get();
+  ApplyArgs<float> a_even = fused_args<float>(P, coords32, op.w32, ws.p32a.get(), ws.p32b.get(), ws.ap32.get(),
+                                              ws.z32.get(), ws.ones32.get());
+  ApplyArgs<float> a_odd = fused_args<float>(P, coords32, op.w32, ws.p32b.get(), ws.p32a.get(), ws.ap32.get(),
+                                             ws.z32.get(), ws.ones32.get());
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  PA_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  for (int k = 0; k < chunk; ++k) {
+    pc_launch_network<float>(pc, ws.r32.get(), &fs->rdr, inv_nfree, done, s);
+    k_fcg_z<float><<<vg, kVecThreads, 0, s>>>(N, ws.r32.get(), ws.dinv32.get(), pc_dsq(pc), pc_output(pc),
+                                              ws.ap32.get(), ws.z32.get(), fs, inv_nfree, ws.sc.get(),
+                                              ws.partials.get(), ws.counters.get() + 2);
+    launch_apply_kernel<float, 1>(*P.mesh, ag, s, k % 2 == 0 ? a_even : a_odd);
+    const float* pnew = (k % 2 == 0) ? ws.p32b.get() : ws.p32a.get();
+    k_fcg_update<float><<<vg, kVecThreads, 0, s>>>(n, ws.dx32.get(), ws.r32.get(), pnew, ws.ap32.get(),
+                                                   ws.dinv32.get(), ws.sc.get(), fs, ws.partials.get(),
+                                                   ws.counters.get() + 3);
+  }
+  {
+    cudaError_t ce = cudaStreamEndCapture(s, &graph);
+    if (ce != cudaSuccess) throw Error(PA_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+  }
+  PA_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+  struct GraphGuard {
+    cudaGraph_t g;
+    cudaGraphExec_t e;
+    ~GraphGuard() {
+      if (e) cudaGraphExecDestroy(e);
+      if (g) cudaGraphDestroy(g);
+    }
+  } guard_graph{graph, exec};
+  const int per_iter = kPcNetworkLaunches + 3;
+
+  const double hint = 0.25;
+  int replacements = 0, iters = 0;
+  bool converged = rr_true <= tol2 * bb, fallback = false, first = true;
+  std::vector<double> hist;
+  while (!converged) {
+    k_to_f32<<<vg, kVecThreads, 0, s>>>(n, ws.r.get(), ws.r32.get());
+    PA_LAUNCHED();
+    PcgScalars cur{};
+    cur.stop2 = hint * tol2 * bb;
+    cur.bb = bb;
+    cur.iters = iters;
+    PA_CUDA(cudaMemcpyAsync(ws.sc.get(), &cur, sizeof(cur), cudaMemcpyHostToDevice, s));
+    k_fcg_init<float><<<vg, kVecThreads, 0, s>>>(n, ws.r32.get(), ws.dinv32.get(), fs, ws.sc.get(), ws.partials.get(),
+                                                 ws.counters.get() + 2, first ? 1 : 0);
+    PA_LAUNCHED();
+    PA_CUDA(cudaGraphLaunch(exec, s));
+    PcgScalars hs{};
+    PA_CUDA(cudaMemcpyAsync(&hs, ws.sc.get(), sizeof(hs), cudaMemcpyDeviceToHost, s));
+    PA_CUDA(cudaStreamSynchronize(s));
+    launches += 3 + int64_t(per_iter) * chunk;
+    if ((hs.iters - iters) % 2)
+      PA_CUDA(cudaMemcpyAsync(ws.p32a.get(), ws.p32b.get(), sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
+    k_fold<<<vg, kVecThreads, 0, s>>>(n, ws.x.get(), ws.dx32.get());
+    PA_LAUNCHED();
+    first = false;
+    iters = hs.iters;
+    rr_true = true_residual();
+    ++replacements;
+    converged = rr_true <= tol2 * bb;
+    hist.push_back(rr_true);
+    if (converged || iters >= max_iters) break;
+    const bool stalled = hist.size() >= 3 && !(rr_true < hist[hist.size() - 3]);
+    if (hs.breakdown || stalled || !std::isfinite(rr_true)) {
+      fallback = true;
+      break;
+    }
+  }
+  pc_check_error(pc, s);
+
+  launch_soa_to_aos<double, double>(ws.x.get(), x_out, N, s);
+  launches += 1;
+  if (nbc) {
+    k_set_bc<<<int((nbc + 255) / 256), 256, 0, s>>>(nbc, P.d_bc_dofs.get(), P.d_bc_vals.get(), op.bc_scale,
+                                                    x_out);
+    PA_LAUNCHED();
+    launches += 1;
+  }
+  pa_status status = PA_OK;
+  int fb_iters = 0;
+  if (fallback && iters < max_iters) {
+    pa_solve_options fo = o;
+    fo.method = PA_SOLVER_PCG_MIXED;
+    fo.use_initial_guess = 1;
+    fo.max_iters = max_iters - iters;
+    pa_solve_stats fst{};
+    status = solve_operator(P, op, b, x_out, fo, &fst, false);
+    fb_iters = fst.iterations;
+    replacements += fst.replacements;
+    launches += fst.kernel_launches;
+    converged = fst.converged != 0;
+    rr_true = fst.rel_residual * fst.rel_residual * bb;
+  } else {
+    const double relres = std::sqrt(rr_true / bb);
+    status = converged ? PA_OK : (std::isfinite(relres) ? PA_ERR_NOT_CONVERGED : PA_ERR_NONFINITE);
+  }
+  PA_CUDA(cudaEventRecord(P.ev1, s));
+  PA_CUDA(cudaEventSynchronize(P.ev1));
+  float ms = 0.f;
+  PA_CUDA(cudaEventElapsedTime(&ms, t0, P.ev1));
+  cudaEventDestroy(t0);
+  if (st) {
+    st->iterations = iters + fb_iters;
+    st->fallback_iterations = fb_iters;
+    st->replacements = replacements;
+    st->rel_residual = std::sqrt(rr_true / bb);
+    st->seconds = ms * 1e-3;
+    st->converged = converged ? 1 : 0;
+    st->kernel_launches = launches;
+  }
+  return status;
+}
+
 // Elastic solve for density z: SIMP weights and Jacobi diagonal from z, then
-// solve_operator.
+// solve_operator (or the flexible CG with the problem's learned network).
 pa_status solve_device(Problem& P, const double* z, const double* b, double* x_out, const pa_solve_options& o,
                        pa_solve_stats* st) {
+  if (o.method == PA_SOLVER_FCG_LEARNED) {
+    PA_CHECK(P.pc != nullptr, "PA_SOLVER_FCG_LEARNED needs a network (pa_problem_set_preconditioner)");
+    const int64_t n = P.ndof();
+    const int grid_need = std::max(std::max(fused_apply_grid<double>(*P.mesh), fused_apply_grid<float>(*P.mesh)),
+                                  vec_grid(n));
+    P.ws.ensure(n, P.C(), grid_need, true);
+    SolverWorkspace& ws = P.ws;
+    if (!P.ev0) { PA_CUDA(cudaEventCreate(&P.ev0)); PA_CUDA(cudaEventCreate(&P.ev1)); }
+    cudaEvent_t t0;
+    PA_CUDA(cudaEventCreate(&t0));
+    PA_CUDA(cudaEventRecord(t0, P.stream));
+    launch_cell_weights(P, z, ws.w64.get(), ws.w32.get(), P.stream);
+    launch_diag(P, ws.w64.get(), ws.diag.get(), P.stream);
+    SolveOperator op;
+    op.w64 = ws.w64.get();
+    op.w32 = ws.w32.get();
+    op.diag_aos = ws.diag.get();
+    pa_status status = solve_fcg(P, op, *P.pc, b, x_out, o, st);
+    float ms = 0.f;
+    PA_CUDA(cudaEventElapsedTime(&ms, t0, P.ev1));
+    cudaEventDestroy(t0);
+    if (st) {
+      st->kernel_launches += 2;
+      st->seconds = ms * 1e-3;  // weights and diagonal included
+    }
+    return status;
+  }
   const bool mixed = o.method == PA_SOLVER_PCG_MIXED;
   const int64_t n = P.ndof();
   const int grid_need = std::max(std::max(fused_apply_grid<double>(*P.mesh), fused_apply_grid<float>(*P.mesh)),

@@ -58,3 +58,86 @@ def cantilever(dims, youngs_modulus=1.0, poissons_ratio=0.3, simp_exponent=3.0, 
     dofs = np.sort(np.concatenate([3 * nodes, 3 * nodes + 1, 3 * nodes + 2])).astype(np.int32)
     prob.set_dirichlet(dofs)
     return mesh, prob, faces, dofs
+
+
+# ------------------------------------------------------------------------------
+# SIMP design iterations and (residual, error) pairs for the learned
+# preconditioner.  The optimality-criteria update belongs to the optimizer that
+# drives Plato Analyze (Plato Engine, not part of the reference); it is written
+# here from the published method (Bendsoe & Sigmund: OC with bisection on the
+# volume multiplier, move limit, damping 1/2, sensitivity filter of radius
+# 1.5 hexes) only to produce the densities the pairs come from.
+
+def sensitivity_filter(rho, dc, dims, radius=1.5):
+    """Mesh-independency filter on the hex grid: dc_i = sum_j H_ij rho_j dc_j /
+    (max(rho_i, 1e-3) sum_j H_ij), H_ij = max(0, radius - dist(i, j))."""
+    from scipy.ndimage import correlate
+    nx, ny, nz = dims
+    r = int(np.floor(radius))
+    ax = np.arange(-r, r + 1)
+    dz, dy, dx = np.meshgrid(ax, ax, ax, indexing="ij")
+    H = np.maximum(0.0, radius - np.sqrt(dx ** 2 + dy ** 2 + dz ** 2))
+    g = lambda a: a.reshape(nz, ny, nx)
+    num = correlate(g(rho * dc), H, mode="constant")
+    den = correlate(np.ones((nz, ny, nx)), H, mode="constant")
+    return (num / (np.maximum(g(rho), 1e-3) * den)).ravel()
+
+
+def oc_update(rho, dc, volfrac, move=0.2, eta=0.5, rho_min=1e-3):
+    """Optimality-criteria update with bisection on the volume multiplier."""
+    lo, hi = 1e-12, 1e12
+    dc = np.minimum(dc, -1e-300)
+    new = rho
+    while (hi - lo) / (hi + lo) > 1e-7:
+        lam = np.sqrt(lo * hi)
+        new = rho * (-dc / lam) ** eta
+        new = np.clip(new, np.maximum(rho - move, rho_min), np.minimum(rho + move, 1.0))
+        if new.mean() > volfrac:
+            lo = lam
+        else:
+            hi = lam
+    return new
+
+
+def simp_training_pairs(prob, dims, iterations=30, snapshots=(64, 256, 1024), volfrac=0.4, move=0.2,
+                        check_every=64, device="cuda", log=None):
+    """Run `iterations` SIMP/OC design iterations on the cantilever; at each,
+    the plain (Jacobi-PCG) solve to 1e-10 gives u*, and the iterates x_k of
+    plain solves stopped after k in `snapshots` iterations give the pairs
+    e = u* - x_k, r = K e (constrained operator), E = e . r.
+
+    Returns (densities [n_it x C], sample_density, residuals [n_s x 3N],
+    energies, final_density, history) with the big arrays as torch tensors on
+    `device`; final_density is the OC update after the last iteration (a
+    design the pairs did not see)."""
+    import torch
+    from .api import SolveOptions
+    nx, ny, nz = dims
+    H = nx * ny * nz
+    rho = np.full(H, volfrac)
+    dens, sd, res, en, hist = [], [], [], [], []
+    plain = SolveOptions("mixed", rel_tol=1e-10, check_every=check_every)
+    for it in range(iterations):
+        zc = torch.tensor(np.repeat(rho, 6), device=device)
+        u, st = prob.solution(zc, options=plain)
+        c = prob.scalar_function().value(u, zc)
+        g = prob.criterion_gradient(zc, u)  # compliance sensitivity at equilibrium (<= 0), per cell
+        dc = g.view(-1, 6).sum(1).cpu().numpy()
+        dens.append(zc)
+        for k in snapshots:
+            xk, _ = prob.solution(zc, options=SolveOptions("mixed", rel_tol=1e-14, max_iters=k,
+                                                           check_every=check_every), allow_not_converged=True)
+            e = u - xk
+            r = prob.apply(zc, e, constrained=True)
+            E = float(torch.dot(e, r).item())
+            if E > 0.0:
+                res.append(r)
+                en.append(E)
+                sd.append(it)
+        hist.append({"iteration": it, "compliance": c, "cg_iterations": st["iterations"],
+                     "volume": float(rho.mean())})
+        if log:
+            log(hist[-1])
+        dc = sensitivity_filter(rho, dc, dims)
+        rho = oc_update(rho, dc, volfrac, move)
+    return (torch.stack(dens), np.array(sd, np.int32), torch.stack(res), np.array(en), np.repeat(rho, 6), hist)

@@ -1,0 +1,141 @@
+"""Learned preconditioner on the GPU through the C ABI: the tensor-core network
+and the library's backward kernels against the NumPy oracle
+(oracle/np_net.py), the preconditioner M r against the oracle, training on
+SIMP (residual, error) pairs, and the flexible-CG solve it serves."""
+import numpy as np
+import pytest
+
+from oracle import np_net, np_ref
+
+pytestmark = pytest.mark.gpu
+
+
+def _params(seed, last=0.3):
+    rng = np.random.default_rng(seed)
+    p = np.zeros(np_net.num_params(), np.float32)
+    o = 0
+    for ci, co in zip(np_net.CIN, np_net.COUT):
+        n = co * ci * 27
+        p[o:o + n] = rng.normal(0.0, np.sqrt(2.0 / (27 * ci)), n) * (last if co == 3 else 1.0)
+        o += n
+        p[o:o + co] = rng.normal(0.0, 0.05, co)
+        o += co
+    return p
+
+
+def _features(grid, seed):
+    rng = np.random.default_rng(seed)
+    G = grid[0] * grid[1] * grid[2]
+    f = np.empty((G, 5), np.float32)
+    f[:, :3] = rng.normal(size=(G, 3))
+    f[:, 3] = rng.uniform(0.0, 1.0, G)
+    f[:, 4] = rng.integers(0, 4, G) / 3.0
+    return f
+
+
+# grids with partial 8 x 16 tiles in x and y, and a single z layer
+@pytest.mark.parametrize("grid", [(11, 19, 3), (8, 16, 1), (17, 9, 5)])
+def test_network_forward_matches_oracle(pa, grid):
+    pc = pa.LearnedPreconditioner(grid, seed=1)
+    assert pc.num_params == np_net.num_params()
+    p = _params(2)
+    pc.set_params(p)
+    assert np.array_equal(pc.get_params(), p)
+    f = _features(grid, 3)
+    got = pc.forward(f).reshape(-1, 3)
+    ref, _ = np_net.forward(p, f, grid)
+    scale = np.abs(ref).max()
+    err = np.abs(got - ref)
+    # BF16 activations: an accumulation-order difference can flip one BF16 rounding
+    assert err.max() <= 2e-2 * scale, err.max() / scale
+    assert err.mean() <= 2e-3 * scale, err.mean() / scale
+
+
+def test_network_backward_matches_oracle(pa):
+    grid = (11, 19, 3)
+    pc = pa.LearnedPreconditioner(grid, seed=1)
+    p = _params(4)
+    pc.set_params(p)
+    f = _features(grid, 5)
+    gout = np.random.default_rng(6).normal(size=(np.prod(grid), 3)).astype(np.float32)
+    got = pc.backward(f, gout)
+    ref = np_net.backward(p, f, grid, gout)
+    o = 0
+    for l, (ci, co) in enumerate(zip(np_net.CIN, np_net.COUT)):
+        n = co * ci * 27 + co
+        a, b = got[o:o + n], ref[o:o + n]
+        assert np.linalg.norm(a - b) <= 1e-2 * np.linalg.norm(b), (l, np.linalg.norm(a - b) / np.linalg.norm(b))
+        o += n
+
+
+def _box(pa, nx, ny, nz, seed):
+    from platoanalyze_b200.workloads import cantilever, cell_density
+    mesh, prob, faces, dofs = cantilever((nx, ny, nz))
+    z = cell_density((nx, ny, nz), seed, kind="smoothed", sigma=1.5, lo=0.01, hi=1.0)
+    cells, coords = np_ref.box_mesh(nx, ny, nz, float(nx), float(ny), float(nz))
+    K = np_ref.Problem(cells, coords, E=1.0, nu=0.3, p=3.0, pmin=1e-9, layout=1).stiffness_dense(z)
+    N = coords.shape[0]
+    mask = np.zeros(N, np.uint8)
+    mask[np.where(coords[:, 0] < 1e-9)[0]] = 7
+    return mesh, prob, z, K, mask
+
+
+def test_new_network_is_jacobi(pa):
+    nx, ny, nz = 6, 3, 3
+    mesh, prob, z, K, mask = _box(pa, nx, ny, nz, 11)
+    pc = pa.LearnedPreconditioner.for_box(nx, ny, nz, seed=3)
+    free = np.repeat(mask == 0, 3)
+    r = np.random.default_rng(1).normal(size=3 * mesh.num_nodes) * free
+    got = pc.apply(prob, z, r)
+    dinv, _, _ = np_net.node_features(np.diag(K), mask)
+    want = dinv.ravel() * r
+    assert np.abs(got - want).max() <= 1e-6 * np.abs(want).max()
+
+
+def test_preconditioner_matches_oracle(pa):
+    nx, ny, nz = 10, 4, 3
+    mesh, prob, z, K, mask = _box(pa, nx, ny, nz, 12)
+    pc = pa.LearnedPreconditioner.for_box(nx, ny, nz)
+    p = _params(7)
+    pc.set_params(p)
+    free = np.repeat(mask == 0, 3)
+    r = np.random.default_rng(2).normal(size=3 * mesh.num_nodes) * free
+    got = pc.apply(prob, z, r)
+    want = np_net.apply(p, (nx + 1, ny + 1, nz + 1), np.diag(K), mask, r)
+    assert np.abs(got - want).max() <= 2e-2 * np.abs(want).max()
+
+
+def test_grid_mismatch_is_rejected(pa):
+    from platoanalyze_b200._abi import PaError
+    mesh, prob, z, K, mask = _box(pa, 6, 3, 3, 1)
+    pc = pa.LearnedPreconditioner((7, 4, 5))
+    with pytest.raises(PaError):
+        prob.set_preconditioner(pc)
+    with pytest.raises(PaError):
+        prob.solution(z, options=pa.SolveOptions("learned", rel_tol=1e-8))  # no network attached
+
+
+def test_training_and_flexible_cg(pa):
+    """SIMP pairs -> training lowers the energy-norm loss; the flexible-CG
+    solve with the trained network reaches 1e-8 and matches the FP64 solve's
+    compliance within 1e-6."""
+    import torch
+    from platoanalyze_b200.workloads import cantilever, simp_training_pairs
+    dims = (24, 12, 12)
+    mesh, prob, faces, dofs = cantilever(dims)
+    dens, sd, res, en, final, hist = simp_training_pairs(prob, dims, iterations=4, snapshots=(16, 64, 256),
+                                                         check_every=16)
+    assert len(sd) >= 8
+    assert hist[-1]["compliance"] < hist[0]["compliance"]  # the design improves
+    pc = pa.LearnedPreconditioner.for_box(*dims, seed=0)
+    st = pc.train(prob, dens, sd, res, en, steps=60, batch=2, learning_rate=2e-3, seed=1)
+    assert np.isfinite(st["final_loss"]) and st["final_loss"] < st["initial_loss"], st
+    prob.set_preconditioner(pc)
+    z = torch.tensor(final, device="cuda")
+    u64, s64 = prob.solution(z, options=pa.SolveOptions("fp64", rel_tol=1e-8))
+    ul, sl = prob.solution(z, options=pa.SolveOptions("learned", rel_tol=1e-8, check_every=32))
+    assert sl["converged"] and sl["rel_residual"] <= 1e-8, sl
+    f64 = prob.scalar_function().value(u64, z)
+    fl = prob.scalar_function().value(ul, z)
+    assert abs(fl - f64) <= 1e-6 * abs(f64)
+    print(f"\nlearned: {sl}\nfp64: {s64}\ntraining: {st}")
