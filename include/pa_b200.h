@@ -290,6 +290,7 @@ typedef struct {
   double final_rel_residual;  /* largest over the steps of the relative Newton residual at the step's end */
   int32_t converged;
   int32_t linear_unconverged; /* tangent solves that stopped at their iteration cap */
+  int32_t line_search_halvings; /* step halvings of the Newton line search */
 } pa_j2_stats;
 
 /* Elasto-plastic solve, displacement-form small-strain J2 with linear
@@ -300,7 +301,12 @@ typedef struct {
  * solve (src/PlasticityProblem.hpp:352, :791-846) with
  * NewtonRaphsonSolver::solve (src/NewtonRaphsonSolver.hpp:570-640); the
  * reference's global residual is the stabilized u-p form, this one the
- * displacement form.  Outputs u (3N) and the final local states (C x 14). */
+ * displacement form.  Each step starts as the reference's does
+ * (src/NewtonRaphsonSolver.hpp:127-131): tangent at the converged state with
+ * the Dirichlet increment imposed in the solve; the Newton iterations that
+ * follow use a backtracking line search on the residual norm.  A step ends
+ * when ||R_free|| <= newton_tol x ||R_free|| of the new boundary values on the
+ * previous field.  Outputs u (3N) and the final local states (C x 14). */
 pa_status pa_j2_solve(pa_problem* problem, const pa_j2_params* params, const double* z,
                       const pa_j2_solve_options* options, const pa_solve_options* linear, double* u, double* local,
                       pa_j2_stats* stats);

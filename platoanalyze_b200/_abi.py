@@ -49,7 +49,8 @@ class J2SolveOptions(ct.Structure):
 
 class J2Stats(ct.Structure):
     _fields_ = [("steps", I32), ("newton_iterations", I32), ("cg_iterations", I64), ("seconds", F64),
-                ("final_rel_residual", F64), ("converged", I32), ("linear_unconverged", I32)]
+                ("final_rel_residual", F64), ("converged", I32), ("linear_unconverged", I32),
+                ("line_search_halvings", I32)]
 
 
 class PcTrainOptions(ct.Structure):

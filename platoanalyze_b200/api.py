@@ -297,7 +297,8 @@ class Problem:
         return u, local, {"steps": js.steps, "newton_iterations": js.newton_iterations,
                           "cg_iterations": js.cg_iterations, "seconds": js.seconds,
                           "final_rel_residual": js.final_rel_residual, "converged": bool(js.converged),
-                          "linear_unconverged": js.linear_unconverged}
+                          "linear_unconverged": js.linear_unconverged,
+                          "line_search_halvings": js.line_search_halvings}
 
     def close(self):
         if self._h:

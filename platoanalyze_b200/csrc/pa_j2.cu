@@ -311,9 +311,9 @@ __global__ void k_axpy_neg_masked(int64_t n, const uint8_t* __restrict__ mask, c
   if ((threadIdx.x & 31) == 0) atomicAdd(sumsq, acc);
 }
 
-__global__ void k_add(int64_t n, const double* __restrict__ d, double* __restrict__ u) {
+__global__ void k_add(int64_t n, const double* __restrict__ d, double* __restrict__ u, double a) {
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
-    u[i] += d[i];
+    u[i] += a * d[i];
 }
 
 J2Dev j2dev(const pa_j2_params& jp) {
@@ -383,7 +383,7 @@ pa_status j2_solve(Problem& P, const pa_j2_params& jp, const double* z, const pa
   int64_t cg_total = 0;
   bool all_converged = true;
   double last_rel = 0.0, worst_rel = 0.0;
-  int linear_unconverged = 0;
+  int linear_unconverged = 0, line_search_halvings = 0;
   pa_status status = PA_OK;
   // residual (and tangent records) at u; b = -R on the free dofs; returns ||R_free||
   auto residual = [&]() {
@@ -422,9 +422,11 @@ pa_status j2_solve(Problem& P, const pa_j2_params& jp, const double* z, const pa
     ++newton_total;
     if (ls == PA_ERR_NOT_CONVERGED) ++linear_unconverged;
     if (ls != PA_OK && ls != PA_ERR_NOT_CONVERGED) return ls;
-    k_add<<<int(std::min<int64_t>((n + 255) / 256, 148 * 8)), 256, 0, s>>>(n, du.get(), u);
-    PA_LAUNCHED();
     return PA_OK;
+  };
+  auto add_du = [&](double a) {
+    k_add<<<int(std::min<int64_t>((n + 255) / 256, 148 * 8)), 256, 0, s>>>(n, du.get(), u, a);
+    PA_LAUNCHED();
   };
   for (int step = 0; step < jo.steps && status == PA_OK; ++step) {
     const double s_old = double(step) / jo.steps, s_new = double(step + 1) / jo.steps;
@@ -441,15 +443,32 @@ pa_status j2_solve(Problem& P, const pa_j2_params& jp, const double* z, const pa
     residual();
     status = tangent_solve(s_new - s_old);
     if (status != PA_OK) break;
+    add_du(1.0);
+    // Newton with a backtracking line search on ||R_free||: when thousands of
+    // cells cross the yield surface in one step, full steps can overshoot
+    // and cycle; halving until the residual norm decreases (at most
+    // kMaxHalvings times, then the last trial is taken) restores descent.
+    constexpr int kMaxHalvings = 5;
     bool converged = false;
+    double rn = residual();
     for (int it = 0; it < jo.max_newton; ++it) {
-      const double rn = residual();
       if (!std::isfinite(rn)) { status = PA_ERR_NONFINITE; break; }
       last_rel = r0 > 0.0 ? rn / r0 : 0.0;
       if (rn <= jo.newton_tol * r0 || rn == 0.0) { converged = true; break; }
       status = tangent_solve(0.0);
       if (status != PA_OK) break;
+      double a = 1.0;
+      add_du(a);
+      double rt = residual();
+      for (int h = 0; h < kMaxHalvings && !(rt <= (1.0 - 1e-4 * a) * rn); ++h) {
+        a *= 0.5;
+        add_du(-a);  // u_base + a du
+        rt = residual();
+        ++line_search_halvings;
+      }
+      rn = rt;
     }
+    if (status == PA_OK && !converged && std::isfinite(rn)) last_rel = r0 > 0.0 ? rn / r0 : 0.0;
     if (status != PA_OK) break;
     if (!converged) all_converged = false;
     worst_rel = std::max(worst_rel, last_rel);
@@ -469,6 +488,7 @@ pa_status j2_solve(Problem& P, const pa_j2_params& jp, const double* z, const pa
     js->seconds = ms * 1e-3;
     js->final_rel_residual = worst_rel;
     js->linear_unconverged = linear_unconverged;
+    js->line_search_halvings = line_search_halvings;
     js->converged = all_converged ? 1 : 0;
   }
   if (status != PA_OK) return status;
