@@ -70,6 +70,8 @@ pa_status pa_mesh_create(const int32_t* cells2nodes, int64_t num_cells, const do
 pa_status pa_mesh_create_box(int32_t nx, int32_t ny, int32_t nz, double lx, double ly, double lz,
                              pa_mesh** out);
 
+/* Handles may be destroyed in any order: a mesh (or a network, pa_pc_destroy)
+ * still used by problems is released when the last of them is destroyed. */
 pa_status pa_mesh_destroy(pa_mesh* mesh);
 
 /* Sizes: cells C, nodes N, CRS blocks B, cell tiles T. Any output may be NULL. */
@@ -310,6 +312,27 @@ typedef struct {
 pa_status pa_j2_solve(pa_problem* problem, const pa_j2_params* params, const double* z,
                       const pa_j2_solve_options* options, const pa_solve_options* linear, double* u, double* local,
                       pa_j2_stats* stats);
+
+/* ------------------------------------------------------ batched solves --- */
+/* No counterpart in the reference (one Problem solves one mesh).  A parted
+ * mesh is the disjoint union of independent sub-meshes: part p owns the nodes
+ * [node_offsets[p], node_offsets[p+1]) and every cell whose nodes lie there
+ * (a cell spanning two parts is rejected).  On a parted mesh,
+ * PA_SOLVER_PCG_MIXED runs one independent Jacobi-PCG per part (its own
+ * alpha, beta, stopping test and iteration count) with all parts advanced by
+ * the same kernels, so each part's result is that of solving it alone.
+ * Call pa_mesh_set_parts before creating problems on the mesh; at most 4096
+ * parts. */
+pa_status pa_mesh_set_parts(pa_mesh* mesh, int32_t num_parts, const int64_t* node_offsets);
+/* Per-part iteration counts and final relative residuals of the last batched
+ * solve (num_parts entries each; either output may be NULL). */
+pa_status pa_problem_part_stats(pa_problem* problem, int32_t* iterations, double* rel_residuals);
+/* Tile-size autotuner: times the fused FP32 CG kernel at density z for tiles
+ * of 64, 128 and 256 clusters, keeps the fastest (rebuilding the mesh's tiles)
+ * and returns it; ms_per_apply (3 entries, may be NULL) gets the timings.  The
+ * problem must be the only one on its mesh. */
+pa_status pa_problem_autotune_tiles(pa_problem* problem, const double* z, int32_t* tile_clusters,
+                                    double* ms_per_apply);
 
 /* ------------------------------------------------ learned preconditioner --- */
 /* No counterpart in the reference (its solvers are AmgX / AztecOO / Belos).

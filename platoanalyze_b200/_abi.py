@@ -109,6 +109,9 @@ SIGNATURES = [
     ("pa_pc_apply", I32, [P, P, P, P, P]),
     ("pa_pc_train", I32, [P, P, I32, P, I32, P, P, P, ct.POINTER(PcTrainOptions), ct.POINTER(PcTrainStats)]),
     ("pa_problem_set_preconditioner", I32, [P, P]),
+    ("pa_mesh_set_parts", I32, [P, I32, P]),
+    ("pa_problem_part_stats", I32, [P, P, P]),
+    ("pa_problem_autotune_tiles", I32, [P, P, P, P]),
 ]
 
 _lib = None

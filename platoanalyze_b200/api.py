@@ -46,6 +46,12 @@ def _ptr(a, dtype, count=None, name="array"):
     return ct.c_void_p(a.ctypes.data)
 
 
+def _ptr_i64(a):
+    if not isinstance(a, np.ndarray) or a.dtype != np.int64 or not a.flags.c_contiguous:
+        raise TypeError("need a C-contiguous numpy array of int64")
+    return ct.c_void_p(a.ctypes.data)
+
+
 def _empty(like, n, dtype=np.float64):
     if like is not None and _is_torch(like):
         import torch
@@ -66,6 +72,7 @@ class Mesh:
     def __init__(self, handle):
         self._lib = _abi.load()
         self._h = handle
+        self.num_parts = 1
         C, N, B, T = (ct.c_int64() for _ in range(4))
         _abi.check(self._lib.pa_mesh_sizes(self._h, ct.byref(C), ct.byref(N), ct.byref(B), ct.byref(T)))
         self.num_cells, self.num_nodes, self.num_blocks, self.num_tiles = C.value, N.value, B.value, T.value
@@ -103,6 +110,16 @@ class Mesh:
         rowmap = np.ascontiguousarray(rowmap, np.int32)
         cols = np.ascontiguousarray(cols, np.int32)
         _abi.check(self._lib.pa_mesh_set_graph(self._h, _ptr(rowmap, np.int32), _ptr(cols, np.int32), cols.size))
+
+    def set_parts(self, node_offsets):
+        """Declare the mesh a disjoint union of independent parts (node ranges);
+        batched mixed solves then run one CG per part.  Before any Problem."""
+        off = np.ascontiguousarray(node_offsets, np.int64)
+        _abi.check(self._lib.pa_mesh_set_parts(self._h, off.size - 1, _ptr_i64(off)))
+        self.num_parts = off.size - 1
+        C, N, B, T = (ct.c_int64() for _ in range(4))
+        _abi.check(self._lib.pa_mesh_sizes(self._h, ct.byref(C), ct.byref(N), ct.byref(B), ct.byref(T)))
+        self.num_tiles = T.value
 
     def boundary_faces(self, axis, value):
         n = ct.c_int64()
@@ -225,6 +242,26 @@ class Problem:
 
     def criterion_value(self, z, u):
         return self.scalar_function().value(u, z)
+
+    def part_stats(self):
+        """Per-part iterations and relative residuals of the last batched solve."""
+        P = self.mesh.num_parts
+        it = np.empty(P, np.int32)
+        rr = np.empty(P, np.float64)
+        _abi.check(self._lib.pa_problem_part_stats(self._h, _ptr(it, np.int32), _ptr(rr, np.float64)))
+        return it, rr
+
+    def autotune_tiles(self, z):
+        """Pick the fastest tile size (64/128/256 clusters) for the fused CG kernel at density z."""
+        z = _as(z, np.float64)
+        k = ct.c_int32()
+        ms = np.zeros(3)
+        _abi.check(self._lib.pa_problem_autotune_tiles(self._h, _ptr(z, np.float64, self.nz, "z"), ct.byref(k),
+                                                       _ptr(ms, np.float64, 3)))
+        C, N, B, T = (ct.c_int64() for _ in range(4))
+        _abi.check(self._lib.pa_mesh_sizes(self.mesh._h, ct.byref(C), ct.byref(N), ct.byref(B), ct.byref(T)))
+        self.mesh.num_tiles = T.value
+        return k.value, dict(zip((64, 128, 256), ms.tolist()))
 
     def set_preconditioner(self, pc):
         """Network SolveOptions("learned") uses (None detaches); the mesh must be its grid."""

@@ -140,14 +140,20 @@ class Stage {
 
 }  // namespace pa
 
-struct pa_problem {
-  pa::Problem P;
-};
 struct pa_mesh {
   pa::Mesh m;
+  bool destroy_requested = false;  // pa_mesh_destroy while problems still use the mesh
+};
+struct pa_pc;
+struct pa_problem {
+  pa::Problem P;
+  pa_mesh* mesh = nullptr;  // the problem keeps its mesh alive until it is destroyed
+  pa_pc* pc = nullptr;      // and its attached network
 };
 struct pa_pc {
   pa::LearnedPC* pc = nullptr;
+  int32_t attached = 0;            // problems using this network
+  bool destroy_requested = false;  // released by the last of them
   ~pa_pc() { pa::pc_delete(pc); }
 };
 
@@ -240,8 +246,17 @@ pa_status pa_mesh_create_box(int32_t nx, int32_t ny, int32_t nz, double lx, doub
   });
 }
 
+// A mesh destroyed while problems still use it is released by the last of
+// them (handles may be destroyed in any order).
 pa_status pa_mesh_destroy(pa_mesh* mesh) {
-  return guard([&] { delete mesh; });
+  return guard([&] {
+    if (!mesh) return;
+    if (mesh->m.live_problems > 0) {
+      mesh->destroy_requested = true;
+      return;
+    }
+    delete mesh;
+  });
 }
 
 pa_status pa_mesh_sizes(const pa_mesh* mesh, int64_t* num_cells, int64_t* num_nodes, int64_t* num_blocks,
@@ -327,7 +342,9 @@ pa_status pa_problem_create(pa_mesh* mesh, const pa_elastic_params* params, void
     PA_CUDA(cudaSetDevice(mesh->m.device));
     std::unique_ptr<pa_problem> h(new pa_problem());
     Problem& P = h->P;
+    PA_CHECK(!mesh->destroy_requested, "mesh already destroyed");
     P.mesh = &mesh->m;
+    h->mesh = mesh;
     P.ep = pa::ElasticParams{params->youngs_modulus, params->poissons_ratio, params->simp_exponent, params->simp_min,
                              params->control_layout};
     if (stream) {
@@ -337,6 +354,7 @@ pa_status pa_problem_create(pa_mesh* mesh, const pa_elastic_params* params, void
       P.own_stream = true;
     }
     upload_bcs(P);
+    mesh->m.live_problems += 1;
     *out = h.release();
   });
 }
@@ -345,13 +363,18 @@ pa_status pa_problem_destroy(pa_problem* problem) {
   return guard([&] {
     if (!problem) return;
     Problem& P = problem->P;
-    cudaSetDevice(P.mesh->device);
+    pa_mesh* mh = problem->mesh;
+    PA_CUDA(cudaSetDevice(P.mesh->device));
     cudaStreamSynchronize(P.stream);
     if (P.ev0) cudaEventDestroy(P.ev0);
     if (P.ev1) cudaEventDestroy(P.ev1);
     cudaStream_t s = P.own_stream ? P.stream : nullptr;
+    pa_pc* pc = problem->pc;
     delete problem;
     if (s) cudaStreamDestroy(s);
+    mh->m.live_problems -= 1;
+    if (mh->m.live_problems == 0 && mh->destroy_requested) delete mh;
+    if (pc && --pc->attached == 0 && pc->destroy_requested) delete pc;
   });
 }
 
@@ -757,7 +780,12 @@ pa_status pa_pc_create(int32_t gx, int32_t gy, int32_t gz, uint64_t seed, pa_pc*
 
 pa_status pa_pc_destroy(pa_pc* pc) {
   return guard([&] {
-    if (pc && pc->pc) PA_CUDA(cudaSetDevice(pa::pc_device(*pc->pc)));
+    if (!pc) return;
+    if (pc->attached > 0) {
+      pc->destroy_requested = true;  // released when the last problem using it detaches
+      return;
+    }
+    if (pc->pc) PA_CUDA(cudaSetDevice(pa::pc_device(*pc->pc)));
     delete pc;
   });
 }
@@ -868,14 +896,91 @@ pa_status pa_problem_set_preconditioner(pa_problem* problem, pa_pc* pc) {
   return guard([&] {
     Problem& P = prob(problem);
     PA_CHECK(P.ep.layout == PA_CONTROL_CELL || P.ep.layout == PA_CONTROL_NODAL, "bad problem");
-    if (!pc) {
+    auto detach = [&]() {
+      pa_pc* old = problem->pc;
+      problem->pc = nullptr;
       P.pc = nullptr;
+      if (old && --old->attached == 0 && old->destroy_requested) delete old;
+    };
+    if (!pc) {
+      detach();
       return;
     }
+    PA_CHECK(!pc->destroy_requested, "network already destroyed");
     pa::LearnedPC& L = pcref(pc);
     PA_CHECK(pa::pc_device(L) == P.mesh->device, "network and problem live on different devices");
     pa::pc_check_grid(L, *P.mesh);
+    if (problem->pc == pc) return;
+    detach();
+    problem->pc = pc;
+    pc->attached += 1;
     P.pc = &L;
+  });
+}
+
+/* ------------------------------------------------------ batched solves --- */
+
+pa_status pa_mesh_set_parts(pa_mesh* mesh, int32_t num_parts, const int64_t* node_offsets) {
+  return guard([&] {
+    PA_CHECK(mesh && node_offsets, "null argument");
+    pa::Mesh& m = mesh->m;
+    PA_CHECK(m.live_problems == 0, "set the parts before creating problems on the mesh");
+    PA_CHECK(num_parts >= 1 && num_parts <= pa::kMaxParts, "num_parts out of range");
+    PA_CHECK(node_offsets[0] == 0 && node_offsets[num_parts] == m.N, "part node offsets must run from 0 to N");
+    for (int32_t p = 0; p < num_parts; ++p) PA_CHECK(node_offsets[p + 1] > node_offsets[p], "empty or unsorted part");
+    PA_CUDA(cudaSetDevice(m.device));
+    std::vector<int64_t> saved = m.part_node_offsets;
+    const int32_t saved_n = m.num_parts;
+    m.num_parts = num_parts;
+    m.part_node_offsets.assign(node_offsets, node_offsets + num_parts + 1);
+    try {
+      pa::mesh_rebuild_tiles(m);
+    } catch (...) {
+      m.num_parts = saved_n;
+      m.part_node_offsets = saved;
+      pa::mesh_rebuild_tiles(m);
+      throw;
+    }
+  });
+}
+
+pa_status pa_problem_part_stats(pa_problem* problem, int32_t* iterations, double* rel_residuals) {
+  return guard([&] {
+    Problem& P = prob(problem);
+    PA_CHECK(!P.part_iterations.empty(), "no batched solve has run on this problem");
+    if (iterations) std::copy(P.part_iterations.begin(), P.part_iterations.end(), iterations);
+    if (rel_residuals) std::copy(P.part_rel_residual.begin(), P.part_rel_residual.end(), rel_residuals);
+  });
+}
+
+pa_status pa_problem_autotune_tiles(pa_problem* problem, const double* z, int32_t* tile_clusters,
+                                    double* ms_per_apply) {
+  return guard([&] {
+    Problem& P = prob(problem);
+    pa::Mesh& m = *P.mesh;
+    PA_CHECK(m.live_problems == 1, "autotuning rebuilds the mesh's tiles: the problem must be its mesh's only one");
+    pa::Stage st(P);
+    const double* dz = st.in(z, P.nz(), "z");
+    const int sizes[3] = {64, 128, 256};
+    double best = 1e300;
+    int best_k = m.tile_clusters;
+    for (int i = 0; i < 3; ++i) {
+      m.tile_clusters = sizes[i];
+      pa::mesh_rebuild_tiles(m);
+      upload_bcs(P);
+      pa::time_cg_apply(P, dz, true, 3);  // warm
+      const double ms = pa::time_cg_apply(P, dz, true, 10);
+      if (ms_per_apply) ms_per_apply[i] = ms;
+      if (ms < best) {
+        best = ms;
+        best_k = sizes[i];
+      }
+    }
+    m.tile_clusters = best_k;
+    pa::mesh_rebuild_tiles(m);
+    upload_bcs(P);
+    if (tile_clusters) *tile_clusters = best_k;
+    st.finish();
   });
 }
 

@@ -111,6 +111,15 @@ struct Mesh {
   DevBuf<uint4> d_cluster_nodes;
   std::vector<int32_t> h_cell_perm;  // internal -> user
   std::vector<uint32_t> h_tile_nodes; // flagged ids without mask bits
+  // Parts: independent sub-meshes solved side by side (batched solves).  Part
+  // p owns nodes [part_node_offsets[p], part_node_offsets[p+1]); no cell spans
+  // two parts and no tile holds cells of two parts.
+  int32_t num_parts = 1;
+  int32_t live_problems = 0;               // problems created on this mesh and not destroyed
+  std::vector<int64_t> part_node_offsets;  // P+1 (empty: one part)
+  std::vector<int32_t> h_tile_part;        // T
+  DevBuf<uint16_t> d_node_part;            // N (parts > 1)
+  DevBuf<int32_t> d_tile_part;             // T (parts > 1)
   TileView tiles() const {
     return TileView{d_tile_cluster_start.get(), d_tile_cell_start.get(), d_tile_hex_count.get(),
                     d_tile_node_start.get(), d_tile_nodes.get(), d_cluster_nodes.get(), d_cell_perm.get(), int32_t(T)};
@@ -119,6 +128,7 @@ struct Mesh {
 };
 
 void mesh_build(Mesh& m);  // tiles + graph + device upload
+void mesh_rebuild_tiles(Mesh& m);  // tiles only (after a change of parts or tile size)
 
 // ----------------------------------------------------------------- material --
 template <typename T>
@@ -149,6 +159,13 @@ struct PcgScalars {
   int32_t iters;   // iterations completed
   int32_t pad;
 };
+
+// Per-part scalars of the batched PCG (one independent CG per part).
+struct PartScalars {
+  double rz, pap, alpha, beta, rr, stop2;
+  int32_t done, breakdown, iters, pad;
+};
+constexpr int kMaxParts = 4096;
 
 struct Problem;
 

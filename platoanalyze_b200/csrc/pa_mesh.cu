@@ -26,6 +26,7 @@ struct Cluster {
   int32_t hex_cells[6]; // hex only: user cells of template tets T0..T5
   int32_t nodes[8];     // hex: slot s = a + 2b + 4c; single: its 4 nodes
   bool hex;
+  int32_t part;
   uint64_t key;
 };
 
@@ -129,6 +130,19 @@ void build_tiles(Mesh& m) {
     cl.push_back(s);
     ++c;
   }
+  // part of every cluster (all its nodes must lie in one part)
+  std::vector<uint16_t> npart;
+  if (m.num_parts > 1) {
+    npart.resize(m.N);
+    for (int32_t p = 0; p < m.num_parts; ++p)
+      for (int64_t v = m.part_node_offsets[p]; v < m.part_node_offsets[p + 1]; ++v) npart[v] = uint16_t(p);
+  }
+  for (auto& k : cl) {
+    k.part = npart.empty() ? 0 : npart[k.nodes[0]];
+    const int nn = k.hex ? 8 : 4;
+    for (int n = 1; n < nn; ++n)
+      if (!npart.empty() && npart[k.nodes[n]] != k.part) throw Error(PA_ERR_INVALID_ARG, "a cell spans two parts");
+  }
   double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
   for (int64_t v = 0; v < m.N; ++v)
     for (int d = 0; d < 3; ++d) {
@@ -146,10 +160,13 @@ void build_tiles(Mesh& m) {
     for (int d = 0; d < 3; ++d) q[d] = uint64_t(std::llround((ctr[d] - lo[d]) * scale[d]));
     k.key = spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2);
   }
-  std::stable_sort(cl.begin(), cl.end(), [](const Cluster& a, const Cluster& b) { return a.key < b.key; });
+  std::stable_sort(cl.begin(), cl.end(),
+                   [](const Cluster& a, const Cluster& b) { return a.part != b.part ? a.part < b.part : a.key < b.key; });
 
   const int tile_k = m.tile_clusters, tile_n = 2 * m.tile_clusters;
-  std::vector<int32_t> tile_cluster_start{0}, tile_cell_start{0}, tile_hex_count, tile_node_start{0}, perm;
+  std::vector<int32_t> tile_cluster_start{0}, tile_cell_start{0}, tile_hex_count, tile_node_start{0}, perm,
+      tile_part;
+  int32_t cur_part = 0;
   std::vector<uint32_t> tile_nodes;
   std::vector<uint4> cluster_nodes;
   perm.reserve(m.C);
@@ -187,6 +204,7 @@ void build_tiles(Mesh& m) {
       if (owner[v] < 0) owner[v] = tile;
     }
     nhex_total += nh;
+    tile_part.push_back(cur_part);
     tile_hex_count.push_back(nh);
     tile_cluster_start.push_back(int32_t(cluster_nodes.size()));
     tile_cell_start.push_back(int32_t(perm.size()));
@@ -200,7 +218,9 @@ void build_tiles(Mesh& m) {
     const int nn = k.hex ? 8 : 4;
     int fresh = 0;
     for (int n = 0; n < nn; ++n) fresh += stamp[k.nodes[n]] == tile ? 0 : 1;
-    if (int(cur.size()) >= tile_k || int(cur_nodes.size()) + fresh > tile_n) close_tile();
+    if (int(cur.size()) >= tile_k || int(cur_nodes.size()) + fresh > tile_n || (!cur.empty() && k.part != cur_part))
+      close_tile();
+    cur_part = k.part;
     for (int n = 0; n < nn; ++n) {
       const int32_t v = k.nodes[n];
       if (stamp[v] != tile) {
@@ -262,6 +282,14 @@ void build_tiles(Mesh& m) {
   std::vector<int32_t> iperm(m.C);
   for (int64_t i = 0; i < m.C; ++i) iperm[perm[i]] = int32_t(i);
   m.d_cell_iperm.upload(iperm.data(), iperm.size());
+  m.h_tile_part = tile_part;
+  if (m.num_parts > 1) {
+    m.d_tile_part.upload(tile_part.data(), tile_part.size());
+    m.d_node_part.upload(npart.data(), npart.size());
+  } else {
+    m.d_tile_part.release();
+    m.d_node_part.release();
+  }
 }
 
 // Node-star graph plus diagonal, sorted columns: the pattern CreateBlockMatrix
@@ -312,6 +340,13 @@ void Mesh::build_graph_entries() {
   d_cell_entry.upload(ent.data(), ent.size());
   d_rowmap.upload(rowmap.data(), rowmap.size());
   d_cols.upload(cols.data(), cols.size());
+}
+
+void mesh_rebuild_tiles(Mesh& m) {
+  PA_CHECK(m.tile_clusters == 64 || m.tile_clusters == 128 || m.tile_clusters == 256,
+           "tile size (clusters per tile) must be 64, 128 or 256");
+  build_tiles(m);
+  PA_CUDA(cudaDeviceSynchronize());
 }
 
 void mesh_build(Mesh& m) {

@@ -63,11 +63,17 @@ struct Problem {
   std::vector<std::unique_ptr<DevBuf<char>>> staging;  // host-array staging, reused across calls
   SolverWorkspace ws;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // per-part results of the last batched solve (parted meshes)
+  std::vector<int32_t> part_iterations;
+  std::vector<double> part_rel_residual;
 
   int64_t N() const { return mesh->N; }
   int64_t C() const { return mesh->C; }
   int64_t ndof() const { return 3 * mesh->N; }
   int64_t nz() const { return ep.layout == PA_CONTROL_CELL ? mesh->C : mesh->N; }
 };
+
+pa_status solve_batched(Problem& P, const SolveOperator& op, const double* b, double* x_out,
+                        const pa_solve_options& o, pa_solve_stats* st);
 
 }  // namespace pa

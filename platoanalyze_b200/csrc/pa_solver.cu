@@ -932,6 +932,27 @@ pa_status solve_device(Problem& P, const double* z, const double* b, double* x_o
   P.ws.ensure(n, P.C(), grid_need, mixed);
   SolverWorkspace& ws = P.ws;
   if (!P.ev0) { PA_CUDA(cudaEventCreate(&P.ev0)); PA_CUDA(cudaEventCreate(&P.ev1)); }
+  if (mixed && P.mesh->num_parts > 1) {
+    // parted mesh: one independent CG per part
+    cudaEvent_t t0;
+    PA_CUDA(cudaEventCreate(&t0));
+    PA_CUDA(cudaEventRecord(t0, P.stream));
+    launch_cell_weights(P, z, ws.w64.get(), ws.w32.get(), P.stream);
+    launch_diag(P, ws.w64.get(), ws.diag.get(), P.stream);
+    SolveOperator op;
+    op.w64 = ws.w64.get();
+    op.w32 = ws.w32.get();
+    op.diag_aos = ws.diag.get();
+    pa_status status = solve_batched(P, op, b, x_out, o, st);
+    float ms = 0.f;
+    PA_CUDA(cudaEventElapsedTime(&ms, t0, P.ev1));
+    cudaEventDestroy(t0);
+    if (st) {
+      st->kernel_launches += 2;
+      st->seconds = ms * 1e-3;
+    }
+    return status;
+  }
   PA_CUDA(cudaEventRecord(P.ev0, P.stream));  // the solve time includes weights and diagonal
   launch_cell_weights(P, z, ws.w64.get(), mixed ? ws.w32.get() : nullptr, P.stream);
   launch_diag(P, ws.w64.get(), ws.diag.get(), P.stream);

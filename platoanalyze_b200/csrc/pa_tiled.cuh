@@ -54,6 +54,11 @@ struct ApplyArgs {
   PcgScalars* sc;
   double* partials;
   unsigned int* counter;
+  // batched PCG (mode 2): one CG per mesh part
+  const int32_t* tile_part;  // T
+  PartScalars* psc;          // P
+  double* pacc;              // P, zero between launches
+  int32_t num_parts;
 };
 
 __device__ __forceinline__ double block_sum(double v, double* smem /*>= 32*/) {
@@ -217,7 +222,7 @@ struct alignas(2 * sizeof(T)) Node2 {
 template <typename T, int MODE, int TILE>
 struct TileSmem {
   static constexpr int kTileNodes = 2 * TILE;
-  static constexpr int kRawBufs = MODE == 1 ? 2 : 1;
+  static constexpr int kRawBufs = MODE >= 1 ? 2 : 1;
   Node4<T> xc[2][kTileNodes];             // coordinates + input (component 0), two buffers
   Node2<T> uu[2][kTileNodes];             // input components 1, 2
   T raw[kRawBufs][9][kTileNodes];         // PCG: r, D^-1, p_old gathered for the tile
@@ -290,7 +295,7 @@ __global__ void __launch_bounds__(TILE, (sizeof(T) == 4 ? 640 / TILE : 1)) k_app
   TileSmem<T, MODE, TILE>& S = *reinterpret_cast<TileSmem<T, MODE, TILE>*>(smem_raw);
 
   T beta = T(0);
-  if (MODE == 1) {
+  if (MODE >= 1) {
     if (a.sc->done) return;
     beta = T(a.sc->beta);
   }
@@ -313,6 +318,29 @@ __global__ void __launch_bounds__(TILE, (sizeof(T) == 4 ? 640 / TILE : 1)) k_app
     __syncthreads();
     const bool has_next = tile + stride < a.tv.num_tiles;
     if (has_next) prefetch_data(a, S, b ^ 1);
+    // batched mode: this tile's part, its beta, and whether it has converged
+    int part = 0;
+    bool skip = false;
+    if constexpr (MODE == 2) {
+      part = a.tile_part[tile];
+      skip = a.psc[part].done != 0;
+      beta = T(a.psc[part].beta);
+      pap = 0.0;
+      if (skip) {
+        // a stopped part keeps its direction: p_new = p_old on its owned nodes,
+        // so both p buffers stay current if the part resumes
+        const int nn = S.meta[b][1];
+        for (int i = threadIdx.x; i < nn; i += blockDim.x) {
+          const uint32_t f = S.ids[b][i];
+          const int64_t g = int64_t(f & kNodeIdMask);
+          if ((f & kOwner) && g < a.N) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) a.p_new[d * a.N + g] = S.raw[b][6 + d][i];
+          }
+        }
+      }
+    }
+    if (!skip) {
 
     // 2. input vector of this tile; zero its sums
     const int nn = S.meta[b][1];
@@ -384,7 +412,7 @@ __global__ void __launch_bounds__(TILE, (sizeof(T) == 4 ? 640 / TILE : 1)) k_app
           for (int d = 0; d < 3; ++d) h1[d] = -Cx[sb][d];
           const T* pl = a.plas ? a.plas + 8 * (int64_t(S.meta[b][5]) + 6 * t + k) : nullptr;
           const T en = tet_rel(a.iso, wv[k], E[0], E[sa], E[sb], h1, Cx[sa], D[0], D[sa], D[sb], r0, ra, rb, pl);
-          if (MODE == 1) pap += double(en);
+          if (MODE >= 1) pap += double(en);
 #pragma unroll
           for (int d = 0; d < 3; ++d) {
             Y[0][d] += r0[d];
@@ -425,7 +453,7 @@ __global__ void __launch_bounds__(TILE, (sizeof(T) == 4 ? 640 / TILE : 1)) k_app
         const int cl = 6 * nhex + (t - nhex);
         const T* pl = a.plas ? a.plas + 8 * (int64_t(S.meta[b][5]) + cl) : nullptr;
         const T en = tet_rel(a.iso, S.w[b][cl], e[0], e[1], e[2], h1, h2, du[0], du[1], du[2], r[0], r[1], r[2], pl);
-        if (MODE == 1) pap += double(en);
+        if (MODE >= 1) pap += double(en);
 #pragma unroll
         for (int n = 0; n < 3; ++n)
 #pragma unroll
@@ -452,12 +480,42 @@ __global__ void __launch_bounds__(TILE, (sizeof(T) == 4 ? 640 / TILE : 1)) k_app
       }
     }
     __syncthreads();
+    if constexpr (MODE == 2) {
+      // p.Kp of this tile into its part
+      const double v = block_sum(pap, S.red);
+      if (threadIdx.x == 0) atomicAdd(&a.pacc[part], v);
+    }
+    }  // !skip
+    // a skipped tile read buffer b above; every thread must be done with it
+    // before the next line refills it (the non-skipped path synchronised after
+    // its write-back)
+    if (skip) __syncthreads();
     // ids of the tile after next into this buffer
     if (tile + 2 * stride < a.tv.num_tiles) prefetch_ids(a, S, tile + 2 * stride, b);
   }
   cp_async_wait_all();
 
-  if (MODE == 1) {
+  if constexpr (MODE == 2) {
+    if (last_block_arrive(a.counter)) {
+      for (int p = threadIdx.x; p < a.num_parts; p += blockDim.x) {
+        PartScalars& ps = a.psc[p];
+        const double v = __ldcg(&a.pacc[p]);
+        a.pacc[p] = 0.0;
+        if (ps.done) continue;
+        ps.pap = v;
+        if (!(v > 0.0) || !isfinite(v)) {
+          ps.breakdown = 1;
+          ps.done = 1;
+          ps.alpha = 0.0;
+        } else {
+          ps.alpha = ps.rz / v;
+        }
+      }
+      if (threadIdx.x == 0) *a.counter = 0u;
+    }
+  }
+
+  if constexpr (MODE == 1) {
     const double bsum = block_sum(pap, S.red);
     if (threadIdx.x == 0) a.partials[blockIdx.x] = bsum;
     if (last_block_arrive(a.counter)) {

@@ -141,3 +141,77 @@ def simp_training_pairs(prob, dims, iterations=30, snapshots=(64, 256, 1024), vo
         dc = sensitivity_filter(rho, dc, dims)
         rho = oc_update(rho, dc, volfrac, move)
     return (torch.stack(dens), np.array(sd, np.int32), torch.stack(res), np.array(en), np.repeat(rho, 6), hist)
+
+
+# ------------------------------------------------------------------------------
+# Batched boxes: many independent cantilevers solved side by side on one
+# parted mesh (one CG per box).
+
+def _box(nx, ny, nz):
+    px, py = nx + 1, ny + 1
+    k, j, i = np.meshgrid(np.arange(nz + 1), np.arange(ny + 1), np.arange(nx + 1), indexing="ij")
+    coords = np.stack([i.ravel(), j.ravel(), k.ravel()], axis=1).astype(np.float64)
+    hk, hj, hi = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    hi, hj, hk = hi.ravel(), hj.ravel(), hk.ravel()
+    cells = np.empty((hi.size, 6, 4), dtype=np.int32)
+    for t, tet in enumerate(HEX_TETS):
+        for n, (a, b, c) in enumerate(tet):
+            cells[:, t, n] = (hi + a) + px * ((hj + b) + py * (hk + c))
+    # x = nx faces: tets 4 and 5 of the hexes with i = nx - 1
+    last = hi == nx - 1
+    node = lambda a, b, c: (hi[last] + a) + px * ((hj[last] + b) + py * (hk[last] + c))
+    faces = np.concatenate([np.stack([node(1, 0, 0), node(1, 0, 1), node(1, 1, 1)], 1),
+                            np.stack([node(1, 0, 0), node(1, 1, 1), node(1, 1, 0)], 1)]).astype(np.int32)
+    jj, kk = np.meshgrid(np.arange(py), np.arange(nz + 1), indexing="ij")
+    clamp = (px * (jj + py * kk)).ravel()
+    return cells.reshape(-1, 4), coords, faces, clamp
+
+
+# Six tets of a unit hex (vertex offsets), the split of pa_mesh_create_box.
+HEX_TETS = (
+    ((0, 0, 0), (1, 1, 0), (0, 1, 0), (1, 1, 1)),
+    ((0, 0, 0), (0, 1, 0), (0, 1, 1), (1, 1, 1)),
+    ((0, 0, 0), (0, 1, 1), (0, 0, 1), (1, 1, 1)),
+    ((0, 0, 0), (1, 0, 1), (1, 1, 1), (0, 0, 1)),
+    ((1, 0, 0), (1, 0, 1), (1, 1, 1), (0, 0, 0)),
+    ((1, 0, 0), (1, 1, 1), (1, 1, 0), (0, 0, 0)),
+)
+
+
+def batch_specs(count=64, seed=1234, lo=16, hi=48):
+    """Box sizes U{lo..hi}^3 and unit traction directions (uniform on the
+    sphere) from one seed; box i's density uses seed + i."""
+    rng = np.random.default_rng(seed)
+    dims = rng.integers(lo, hi + 1, size=(count, 3))
+    d = rng.normal(size=(count, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    return [tuple(int(v) for v in row) for row in dims], d
+
+
+def batched_boxes(specs, directions, seed=1234, stream=None, sigma=3.0):
+    """One parted mesh + Problem holding every box (each clamped at its x = 0
+    face, unit total traction along its direction on its x = max face) and
+    the per-cell densities (smoothed field, seed + i).  Boxes are laid out
+    along x with a gap, parts = boxes."""
+    cells_l, coords_l, z_l, faces_l, clamp_l, offs = [], [], [], [], [], [0]
+    x0, nn = 0.0, 0
+    for i, (nx, ny, nz) in enumerate(specs):
+        c, X, f, cl = _box(nx, ny, nz)
+        X[:, 0] += x0
+        cells_l.append(c + nn)
+        coords_l.append(X)
+        faces_l.append(f + nn)
+        clamp_l.append(cl + nn)
+        z_l.append(cell_density((nx, ny, nz), seed + i, kind="smoothed", sigma=sigma, lo=0.01, hi=1.0))
+        nn += X.shape[0]
+        offs.append(nn)
+        x0 += nx + 4.0
+    mesh = Mesh.from_arrays(np.concatenate(cells_l), np.concatenate(coords_l))
+    mesh.set_parts(np.array(offs, np.int64))
+    prob = Problem(mesh, 1.0, 0.3, 3.0, 1e-9, control_layout="cell", stream=stream)
+    for (nx, ny, nz), f, d in zip(specs, faces_l, directions):
+        prob.add_traction(f, np.asarray(d, np.float64) / (ny * nz))
+    clamp = np.concatenate(clamp_l)
+    dofs = np.sort(np.concatenate([3 * clamp, 3 * clamp + 1, 3 * clamp + 2])).astype(np.int32)
+    prob.set_dirichlet(dofs)
+    return mesh, prob, np.concatenate(z_l), np.array(offs, np.int64)

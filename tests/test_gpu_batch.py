@@ -1,0 +1,84 @@
+"""Batched solves on a parted mesh (one independent CG per part) through the C
+ABI: every part's displacement equals the solve of that box alone, parts stop
+independently, a cell spanning two parts is rejected, and the tile-size
+autotuner keeps the solution."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SPECS = [(6, 3, 3), (8, 4, 3), (5, 5, 5), (10, 3, 4), (4, 4, 4), (7, 2, 3)]
+
+
+def _alone(pa, dims, direction, z, check_every=16):
+    from platoanalyze_b200.workloads import _box
+    nx, ny, nz = dims
+    cells, coords, faces, clamp = _box(nx, ny, nz)
+    mesh = pa.Mesh.from_arrays(cells, coords)
+    prob = pa.Problem(mesh, 1.0, 0.3, 3.0, 1e-9, control_layout="cell")
+    prob.add_traction(faces, np.asarray(direction) / (ny * nz))
+    dofs = np.sort(np.concatenate([3 * clamp, 3 * clamp + 1, 3 * clamp + 2])).astype(np.int32)
+    prob.set_dirichlet(dofs)
+    u, st = prob.solution(z, options=pa.SolveOptions("fp64", rel_tol=1e-12))
+    _, stm = prob.solution(z, options=pa.SolveOptions("mixed", rel_tol=1e-8, check_every=check_every))
+    return u, stm["iterations"]
+
+
+def test_batched_parts_match_separate_solves(pa):
+    from platoanalyze_b200.workloads import batch_specs, batched_boxes
+    _, dirs = batch_specs(len(SPECS), seed=5)
+    mesh, prob, z, offs = batched_boxes(SPECS, dirs, seed=11, sigma=1.5)
+    assert mesh.num_parts == len(SPECS)
+    u, st = prob.solution(z, options=pa.SolveOptions("mixed", rel_tol=1e-8, check_every=16))
+    assert st["converged"], st
+    its, rel = prob.part_stats()
+    assert (rel <= 1e-8).all(), rel
+    assert its.min() < its.max()  # parts stop independently
+    c0 = 0
+    for p, (dims, d) in enumerate(zip(SPECS, dirs)):
+        C = 6 * dims[0] * dims[1] * dims[2]
+        ua, it_alone = _alone(pa, dims, d, z[c0:c0 + C])
+        ub = u[3 * offs[p]:3 * offs[p + 1]]
+        assert np.abs(ub - ua).max() <= 1e-6 * np.abs(ua).max(), p
+        # the same algorithm per part: iteration counts of the batched and the single solve agree
+        assert abs(int(its[p]) - it_alone) <= 0.1 * it_alone + 16, (p, its[p], it_alone)
+        c0 += C
+
+
+def test_part_boundary_inside_a_box_is_rejected(pa):
+    from platoanalyze_b200._abi import PaError
+    from platoanalyze_b200.workloads import _box
+    cells, coords, _, _ = _box(4, 3, 3)
+    mesh = pa.Mesh.from_arrays(cells, coords)
+    with pytest.raises(PaError):
+        mesh.set_parts(np.array([0, 10, coords.shape[0]], np.int64))
+
+
+def test_autotune_keeps_the_solution(pa):
+    from platoanalyze_b200.workloads import batch_specs, batched_boxes
+    _, dirs = batch_specs(3, seed=2)
+    mesh, prob, z, offs = batched_boxes(SPECS[:3], dirs, seed=3, sigma=1.5)
+    opts = pa.SolveOptions("mixed", rel_tol=1e-8, check_every=16)
+    u0, _ = prob.solution(z, options=opts)
+    k, ms = prob.autotune_tiles(z)
+    assert k in (64, 128, 256) and all(v > 0 for v in ms.values())
+    u1, st = prob.solution(z, options=opts)
+    assert st["converged"]
+    assert np.abs(u1 - u0).max() <= 1e-6 * np.abs(u0).max()
+
+
+def test_handles_destroyed_in_any_order(pa):
+    """A mesh (and a network) destroyed before the problems that use them
+    stays alive until the last problem goes."""
+    from platoanalyze_b200.workloads import cantilever
+    mesh, prob, faces, dofs = cantilever((6, 3, 3))
+    pc = pa.LearnedPreconditioner.for_box(6, 3, 3)
+    prob.set_preconditioner(pc)
+    z = np.full(mesh.num_cells, 0.5)
+    mesh.close()
+    pc.close()
+    u, st = prob.solution(z, options=pa.SolveOptions("learned", rel_tol=1e-8))
+    assert st["converged"]
+    u2, _ = prob.solution(z, options=pa.SolveOptions("fp64", rel_tol=1e-10))
+    assert np.abs(u - u2).max() <= 1e-6 * np.abs(u2).max()
+    prob.close()
