@@ -235,9 +235,72 @@ def traffic_from_profiles(kernel_tag):
         return None
 
 
+def profile_network(args):
+    """The learned preconditioner's four tensor-core convolutions on the nodal
+    grid of the 64^3 box (65^3 nodes), seeded weights and features: 1 + reps
+    forwards, device time per forward and TFLOP/s (a short command for ncu)."""
+    import torch
+    import platoanalyze_b200 as pa
+    dims = (64, 64, 64) if args.dims == "160x80x80" else dims_of(args.dims)
+    torch.cuda.set_device(0)
+    pc = pa.LearnedPreconditioner.for_box(*dims, seed=0)
+    rng = np.random.default_rng(0)
+    p = pc.get_params()
+    p += rng.normal(0.0, 0.02, p.size).astype(np.float32)
+    pc.set_params(p)
+    G = pc.num_points
+    f = torch.tensor(rng.normal(size=(G, 5)).astype(np.float32), device="cuda")
+    pc.forward(f)
+    ms, flops = pc.time_forward(args.reps)
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            peak, kind = float(json.load(fh)["bf16_tflops"]), "measured"
+    except Exception:
+        peak, kind = 1590.0, "fallback"
+    tf = flops / (ms * 1e-3) / 1e12
+    print(json.dumps({"dims": dims, "grid_nodes": G, "ms_per_forward": ms, "flops": flops, "TFLOP/s": tf,
+                      "peak_bf16_tflops": peak, "peak_kind": kind, "frac": tf / peak}), flush=True)
+    return 0
+
+
+def profile_j2(args):
+    """The FP64 radial return over the 80x40x40 bar at 2% axial strain from a
+    zero local state: 1 + reps launches, device time and GB/s."""
+    import torch
+    import platoanalyze_b200 as pa
+    dims = J2_DIMS if args.dims == "160x80x80" else dims_of(args.dims)
+    C, N = counts(dims)
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    mesh, prob = j2_bar(pa, dims, stream=stream.cuda_stream)
+    cells, coords = mesh.arrays()
+    u = torch.zeros(3 * N, dtype=torch.float64, device="cuda")
+    u[0::3] = 0.02 * torch.tensor(coords[:, 0], device="cuda")
+    z = torch.ones(N, dtype=torch.float64, device="cuda")
+    prev = torch.zeros(14 * C, dtype=torch.float64, device="cuda")
+    out = torch.empty_like(prev)
+    prob.j2_radial_return(J2_PARAMS, u, z, prev, out)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.reps):
+        prob.j2_radial_return(J2_PARAMS, u, z, prev, out)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / args.reps
+    nb = j2_return_bytes(C, N)
+    print(json.dumps({"dims": dims, "ms_per_launch": ms, "algorithmic_bytes": nb, "GB/s": nb / (ms * 1e-3) / 1e9}),
+          flush=True)
+    return 0
+
+
 def profile_kernel(args):
     """Build the workload and launch the fused CG kernel 1 + reps times per
     precision (a short, self-contained command for ncu)."""
+    if args.workload == "learned":
+        return profile_network(args)
+    if args.workload == "j2":
+        return profile_j2(args)
     import ctypes as ct
     import torch
     import platoanalyze_b200 as pa  # noqa: F401

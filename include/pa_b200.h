@@ -376,6 +376,10 @@ pa_status pa_pc_set_params(pa_pc* pc, const float* params);
 pa_status pa_pc_forward(pa_pc* pc, const float* features, float* out);
 /* Gradient of sum(grad_out . f(features)) with respect to the parameters. */
 pa_status pa_pc_backward(pa_pc* pc, const float* features, const float* grad_out, float* grad_params);
+/* Diagnostics: average device time of the network's four convolutions over
+ * `reps` back-to-back launches on the last input, and their algorithmic FLOPs
+ * (2 x 27 x in x out per node and layer, real channel counts). */
+pa_status pa_pc_time_forward(pa_pc* pc, int32_t reps, double* ms_per_forward, int64_t* flops);
 /* out = M r for the problem at density z (interleaved 3N vectors). */
 pa_status pa_pc_apply(pa_problem* problem, pa_pc* pc, const double* z, const double* r, double* out);
 /* Train on residual/error pairs: sample s has residual r_s (3N, interleaved,

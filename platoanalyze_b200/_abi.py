@@ -106,6 +106,7 @@ SIGNATURES = [
     ("pa_pc_set_params", I32, [P, P]),
     ("pa_pc_forward", I32, [P, P, P]),
     ("pa_pc_backward", I32, [P, P, P, P]),
+    ("pa_pc_time_forward", I32, [P, I32, P, P]),
     ("pa_pc_apply", I32, [P, P, P, P, P]),
     ("pa_pc_train", I32, [P, P, I32, P, I32, P, P, P, ct.POINTER(PcTrainOptions), ct.POINTER(PcTrainStats)]),
     ("pa_problem_set_preconditioner", I32, [P, P]),

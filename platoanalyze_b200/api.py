@@ -490,6 +490,12 @@ class LearnedPreconditioner:
                                             _ptr(out, np.float32, self.num_params, "grad_params")))
         return out
 
+    def time_forward(self, reps=20):
+        """(ms per forward of the four convolutions, algorithmic FLOPs) on the last input."""
+        ms, fl = ct.c_double(), ct.c_int64()
+        _abi.check(self._lib.pa_pc_time_forward(self._h, int(reps), ct.byref(ms), ct.byref(fl)))
+        return ms.value, fl.value
+
     def apply(self, problem, z, r, out=None):
         z, r = _as(z, np.float64), _as(r, np.float64)
         out = _empty(r, problem.ndof) if out is None else out

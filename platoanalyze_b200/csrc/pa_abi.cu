@@ -846,6 +846,15 @@ pa_status pa_pc_backward(pa_pc* pc, const float* features, const float* grad_out
   });
 }
 
+pa_status pa_pc_time_forward(pa_pc* pc, int32_t reps, double* ms_per_forward, int64_t* flops) {
+  return guard([&] {
+    pa::LearnedPC& L = pcref(pc);
+    PA_CHECK(reps > 0 && ms_per_forward, "bad arguments");
+    *ms_per_forward = pa::pc_time_forward(L, reps);
+    if (flops) *flops = pa::pc_forward_flops(L);
+  });
+}
+
 pa_status pa_pc_apply(pa_problem* problem, pa_pc* pc, const double* z, const double* r, double* out) {
   return guard([&] {
     Problem& P = prob(problem);

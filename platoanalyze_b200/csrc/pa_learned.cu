@@ -114,9 +114,11 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_tc(ConvArgs a) {
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int tx = tile % ntx, ty = (tile / ntx) % nty, tz = tile / (ntx * nty);
     const int x0 = tx * kTX, y0 = ty * kTY, z0 = tz;
-    // halo: node (x0 + hx - 1, y0 + hy - 1, z0 + hz - 1), zero outside the grid
+    // halo: node (x0 + hx - 1, y0 + hy - 1, z0 + hz - 1), zero outside the grid;
+    // the channel group runs fastest so that consecutive threads read one
+    // node's contiguous channels
     for (int i = tid; i < (CIN / 8) * kHalo; i += kConvThreads) {
-      const int cg = i / kHalo, hv = i - cg * kHalo;
+      const int cg = i % (CIN / 8), hv = i / (CIN / 8);
       const int hx = hv % kHX, hy = (hv / kHX) % kHY, hz = hv / (kHX * kHY);
       const int x = x0 + hx - 1, y = y0 + hy - 1, z = z0 + hz - 1;
       __nv_bfloat16* dst = &S.halo[(cg * kHalo + hv) * 8];
@@ -147,7 +149,8 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_tc(ConvArgs a) {
       }
       tc::commit(&S.mbar);
     }
-    const bool got = tc::mbar_wait(&S.mbar, phase);
+    // the issuing thread waits for the accumulator; the others wait at the barrier
+    const bool got = tid == 0 ? tc::mbar_wait(&S.mbar, phase) : true;
     phase ^= 1u;
     if (__syncthreads_or(got ? 0 : 1)) {
       ok = false;
@@ -212,13 +215,13 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_tc(ConvArgs a) {
 
 template <int CIN, int COUT, bool RELU>
 void launch_conv_instance(const ConvArgs& a, cudaStream_t s) {
-  static int grid_per_sm = 0;  // one device model per process: B200
+  // CTAs per SM from the shared-memory footprint (228 KB per SM, 1 KB reserved
+  // per CTA), at most 4 (4 x 32 of the 512 tensor-memory columns)
+  static int grid_per_sm = 0;
   const size_t smem = sizeof(ConvSmem<CIN, COUT>);
   if (!grid_per_sm) {
     PA_CUDA(cudaFuncSetAttribute(k_conv3_tc<CIN, COUT, RELU>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    int b = 0;
-    PA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_conv3_tc<CIN, COUT, RELU>, kConvThreads, smem));
-    grid_per_sm = std::max(1, b);
+    grid_per_sm = std::max(1, std::min(4, int((228 * 1024) / (smem + 1024))));
   }
   const int ntiles = ((a.gx + kTX - 1) / kTX) * ((a.gy + kTY - 1) / kTY) * a.gz;
   const int grid = std::max(1, std::min(ntiles, grid_per_sm * num_sms()));
@@ -663,6 +666,30 @@ void pc_forward_features(LearnedPC& pc, const float* d_feat, float* d_out, cudaS
   k_take3<<<grid_for(pc.G), 256, 0, s>>>(pc.G, pc.out.get(), d_out);
   PA_LAUNCHED();
   check_err(pc, s);
+}
+
+double pc_time_forward(LearnedPC& pc, int reps) {
+  cudaStream_t s = pc.stream;
+  cudaEvent_t e0, e1;
+  PA_CUDA(cudaEventCreate(&e0));
+  PA_CUDA(cudaEventCreate(&e1));
+  run_layers(pc, nullptr, s);  // warm
+  PA_CUDA(cudaEventRecord(e0, s));
+  for (int i = 0; i < reps; ++i) run_layers(pc, nullptr, s);
+  PA_CUDA(cudaEventRecord(e1, s));
+  PA_CUDA(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  PA_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  check_err(pc, s);
+  return double(ms) / reps;
+}
+
+int64_t pc_forward_flops(const LearnedPC& pc) {
+  int64_t f = 0;
+  for (int l = 0; l < kPcLayers; ++l) f += 2LL * 27 * kCin[l] * kCout[l];
+  return f * pc.G;
 }
 
 void pc_backward_features(LearnedPC& pc, const float* d_feat, const float* d_gout, float* d_gparams, cudaStream_t s) {

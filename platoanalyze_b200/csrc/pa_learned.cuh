@@ -23,6 +23,10 @@ void pc_set_params(LearnedPC& pc, const float* d_params, cudaStream_t s);
 void pc_get_params(const LearnedPC& pc, float* d_params, cudaStream_t s);
 // Network on caller features (G x 5 FP32, rounded to BF16 at the input) -> G x 3 FP32.
 void pc_forward_features(LearnedPC& pc, const float* d_feat, float* d_out, cudaStream_t s);
+// Average device time of the four convolutions (ms) on the current layer-1
+// input, and their algorithmic FLOPs (real channel counts).
+double pc_time_forward(LearnedPC& pc, int reps);
+int64_t pc_forward_flops(const LearnedPC& pc);
 // d(sum gout . out)/d(params) for the same features (forward included).
 void pc_backward_features(LearnedPC& pc, const float* d_feat, const float* d_gout, float* d_gparams, cudaStream_t s);
 // out = M r for density z (interleaved vectors, device).

@@ -268,43 +268,93 @@ struct FcgState {
   double pq_prev;  // p . K p of the previous direction
   int32_t first;   // 1: the next direction is z itself
   int32_t pad;
+  double gamma;    // weight of the network's correction in z
 };
 
+// Weight of the network's correction c = s D^-1/2 f: z = D^-1 r + gamma c with
+// gamma = 1, reduced to 0.5 (r.D^-1 r) / (-c.r) when c.r < -0.5 r.D^-1 r, so
+// that z.r >= 0.5 r.D^-1 r > 0 (z is always a descent direction).
 template <typename T>
-__global__ void __launch_bounds__(kVecThreads) k_fcg_z(int64_t N, const T* __restrict__ r, const T* __restrict__ dinv,
-                                                       const float* __restrict__ dsq, const float* __restrict__ out,
-                                                       T* __restrict__ q, T* __restrict__ z, FcgState* __restrict__ fs,
-                                                       double inv_nfree, PcgScalars* __restrict__ sc,
-                                                       double* __restrict__ partials, unsigned int* counter) {
+__global__ void __launch_bounds__(kVecThreads) k_fcg_gamma(int64_t N, const T* __restrict__ r,
+                                                           const float* __restrict__ dsq,
+                                                           const float* __restrict__ out, FcgState* __restrict__ fs,
+                                                           double inv_nfree, PcgScalars* __restrict__ sc,
+                                                           double* __restrict__ partials, unsigned int* counter) {
   __shared__ double s_red[64];
   if (sc->done) return;
   const double s2 = fs->rdr * inv_nfree;
-  const T sig = T(s2 > 0.0 ? sqrt(s2) : 0.0);
-  double zq = 0.0, zr = 0.0;
+  const double sig = s2 > 0.0 ? sqrt(s2) : 0.0;
+  double cr = 0.0, unused = 0.0;
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < 3 * N; i += int64_t(gridDim.x) * blockDim.x) {
     const int64_t d = i / N, v = i - d * N;
-    const T zi = dinv[i] * r[i] + sig * T(dsq[i]) * T(out[4 * v + d]);
+    cr += double(dsq[i]) * double(out[4 * v + d]) * double(r[i]);
+  }
+  block_sum2(cr, unused, s_red);
+  if (threadIdx.x == 0) partials[2 * blockIdx.x] = cr;
+  if (last_block_arrive(counter)) {
+    double t0 = 0.0, t1 = 0.0;
+    for (int i = threadIdx.x; i < gridDim.x; i += blockDim.x) t0 += __ldcg(&partials[2 * i]);
+    block_sum2(t0, t1, s_red);
+    if (threadIdx.x == 0) {
+      const double c = sig * t0, a = fs->rdr;
+      fs->gamma = (c < -0.5 * a) ? -0.5 * a / c : 1.0;
+      *counter = 0u;
+    }
+  }
+}
+
+// z = D^-1 r + gamma s D^-1/2 f; z.q_old, z.r and p_old.r; q = 0 for the next
+// apply.  Last CTA: beta = -z.q_old / p_old.q_old (flexible CG) and rz =
+// p.r = z.r + beta p_old.r, the numerator of the exact line search
+// alpha = p.r / p.Kp that the fused apply forms.
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) k_fcg_z(int64_t N, const T* __restrict__ r, const T* __restrict__ dinv,
+                                                       const float* __restrict__ dsq, const float* __restrict__ out,
+                                                       const T* __restrict__ p_old, T* __restrict__ q,
+                                                       T* __restrict__ z, FcgState* __restrict__ fs, double inv_nfree,
+                                                       PcgScalars* __restrict__ sc, double* __restrict__ partials,
+                                                       unsigned int* counter) {
+  __shared__ double s_red[64];
+  if (sc->done) return;
+  const double s2 = fs->rdr * inv_nfree;
+  const T sig = T((s2 > 0.0 ? sqrt(s2) : 0.0) * fs->gamma);
+  double zq = 0.0, zr = 0.0, pr = 0.0;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < 3 * N; i += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t d = i / N, v = i - d * N;
+    const T ri = r[i];
+    const T zi = dinv[i] * ri + sig * T(dsq[i]) * T(out[4 * v + d]);
     zq += double(zi) * double(q[i]);
-    zr += double(zi) * double(r[i]);
+    zr += double(zi) * double(ri);
+    pr += double(p_old[i]) * double(ri);
     q[i] = T(0);
     z[i] = zi;
   }
   block_sum2(zq, zr, s_red);
-  if (threadIdx.x == 0) { partials[2 * blockIdx.x] = zq; partials[2 * blockIdx.x + 1] = zr; }
+  double unused = 0.0;
+  block_sum2(pr, unused, s_red);
+  if (threadIdx.x == 0) {
+    partials[3 * blockIdx.x] = zq;
+    partials[3 * blockIdx.x + 1] = zr;
+    partials[3 * blockIdx.x + 2] = pr;
+  }
   if (last_block_arrive(counter)) {
-    double t0 = 0.0, t1 = 0.0;
+    double t0 = 0.0, t1 = 0.0, t2 = 0.0, u2 = 0.0;
     for (int i = threadIdx.x; i < gridDim.x; i += blockDim.x) {
-      t0 += __ldcg(&partials[2 * i]);
-      t1 += __ldcg(&partials[2 * i + 1]);
+      t0 += __ldcg(&partials[3 * i]);
+      t1 += __ldcg(&partials[3 * i + 1]);
+      t2 += __ldcg(&partials[3 * i + 2]);
     }
     block_sum2(t0, t1, s_red);
+    block_sum2(t2, u2, s_red);
     if (threadIdx.x == 0) {
-      if (!(t1 > 0.0) || !isfinite(t0) || !isfinite(t1)) {
+      const double beta = fs->first ? 0.0 : -t0 / fs->pq_prev;
+      const double pr_new = t1 + beta * t2;
+      if (!(t1 > 0.0) || !(pr_new > 0.0) || !isfinite(t0) || !isfinite(pr_new)) {
         sc->breakdown = 2;  // not a descent direction: the host falls back to Jacobi
         sc->done = 1;
       } else {
-        sc->beta = fs->first ? 0.0 : -t0 / fs->pq_prev;
-        sc->rz = t1;
+        sc->beta = beta;
+        sc->rz = pr_new;
         fs->first = 0;
       }
       *counter = 0u;
@@ -453,7 +503,7 @@ void SolverWorkspace::ensure(int64_t n, int64_t C, int grid, bool mixed) {
   if (mixed && r32.n != size_t(n)) {
     r32.resize(n); p32a.resize(n); p32b.resize(n); ap32.resize(n); dinv32.resize(n); dx32.resize(n); w32.resize(C);
   }
-  if (partials.n < size_t(2 * grid + 64)) partials.resize(2 * grid + 64);
+  if (partials.n < size_t(3 * grid + 64)) partials.resize(3 * grid + 64);  // up to 3 per block
   if (counters.n < 4) {
     counters.resize(4);
     PA_CUDA(cudaMemset(counters.get(), 0, 4 * sizeof(unsigned int)));
@@ -698,7 +748,8 @@ pa_status solve_operator(Problem& P, const SolveOperator& op, const double* b, d
 // Flexible CG with the learned preconditioner, mixed precision as in
 // solve_operator (FP32 vectors and apply, FP64 dots, FP64 x and true-residual
 // replacement once per chunk).  One iteration = the network (pack + four
-// convolutions), z/beta, the fused apply (p, K p, p.Kp, alpha), the update.
+// convolutions), the correction weight, z/beta, the fused apply (p, K p, p.Kp,
+// alpha), the update.
 // The solve continues as mixed Jacobi-PCG from the current iterate when the
 // network's direction is not a descent direction or the true residual has not
 // decreased over two chunks.
@@ -713,7 +764,8 @@ pa_status solve_fcg(Problem& P, const SolveOperator& op, LearnedPC& pc, const do
   P.ws.ensure(n, P.C(), grid_need, true);
   SolverWorkspace& ws = P.ws;
   if (ws.ones32.n != size_t(n)) { ws.ones32.resize(n); ws.z32.resize(n); }
-  if (ws.fcg_state.n < 4) ws.fcg_state.resize(4);
+  static_assert(sizeof(FcgState) <= 8 * sizeof(double), "FcgState fits its buffer");
+  if (ws.fcg_state.n < 8) ws.fcg_state.resize(8);
   FcgState* fs = reinterpret_cast<FcgState*>(ws.fcg_state.get());
   const int max_iters = o.max_iters > 0 ? o.max_iters : int(20.0 * std::sqrt(double(n)) + 1000);
   int chunk = o.check_every > 0 ? o.check_every : 64;
@@ -788,7 +840,10 @@ pa_status solve_fcg(Problem& P, const SolveOperator& op, LearnedPC& pc, const do
   PA_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   for (int k = 0; k < chunk; ++k) {
     pc_launch_network<float>(pc, ws.r32.get(), &fs->rdr, inv_nfree, done, s);
-    k_fcg_z<float><<<vg, kVecThreads, 0, s>>>(N, ws.r32.get(), ws.dinv32.get(), pc_dsq(pc), pc_output(pc),
+    k_fcg_gamma<float><<<vg, kVecThreads, 0, s>>>(N, ws.r32.get(), pc_dsq(pc), pc_output(pc), fs, inv_nfree,
+                                                  ws.sc.get(), ws.partials.get(), ws.counters.get() + 2);
+    const float* pold = (k % 2 == 0) ? ws.p32a.get() : ws.p32b.get();
+    k_fcg_z<float><<<vg, kVecThreads, 0, s>>>(N, ws.r32.get(), ws.dinv32.get(), pc_dsq(pc), pc_output(pc), pold,
                                               ws.ap32.get(), ws.z32.get(), fs, inv_nfree, ws.sc.get(),
                                               ws.partials.get(), ws.counters.get() + 2);
     launch_apply_kernel<float, 1>(*P.mesh, ag, s, k % 2 == 0 ? a_even : a_odd);
@@ -810,7 +865,7 @@ pa_status solve_fcg(Problem& P, const SolveOperator& op, LearnedPC& pc, const do
       if (g) cudaGraphDestroy(g);
     }
   } guard_graph{graph, exec};
-  const int per_iter = kPcNetworkLaunches + 3;
+  const int per_iter = kPcNetworkLaunches + 4;
 
   const double hint = 0.25;
   int replacements = 0, iters = 0;
@@ -843,7 +898,13 @@ pa_status solve_fcg(Problem& P, const SolveOperator& op, LearnedPC& pc, const do
     converged = rr_true <= tol2 * bb;
     hist.push_back(rr_true);
     if (converged || iters >= max_iters) break;
-    const bool stalled = hist.size() >= 3 && !(rr_true < hist[hist.size() - 3]);
+    // stalled: no chunk of the last four improved on the best residual before them
+    bool stalled = false;
+    if (hist.size() >= 5) {
+      const double before = *std::min_element(hist.begin(), hist.end() - 4);
+      const double recent = *std::min_element(hist.end() - 4, hist.end());
+      stalled = !(recent < 0.99 * before);
+    }
     if (hs.breakdown || stalled || !std::isfinite(rr_true)) {
       fallback = true;
       break;

@@ -99,7 +99,7 @@ def oc_update(rho, dc, volfrac, move=0.2, eta=0.5, rho_min=1e-3):
     return new
 
 
-def simp_training_pairs(prob, dims, iterations=30, snapshots=(64, 256, 1024), volfrac=0.4, move=0.2,
+def simp_training_pairs(prob, dims, iterations=30, snapshots=(8, 32, 128, 512), volfrac=0.4, move=0.2,
                         check_every=64, device="cuda", log=None):
     """Run `iterations` SIMP/OC design iterations on the cantilever; at each,
     the plain (Jacobi-PCG) solve to 1e-10 gives u*, and the iterates x_k of

@@ -139,3 +139,19 @@ def test_training_and_flexible_cg(pa):
     fl = prob.scalar_function().value(ul, z)
     assert abs(fl - f64) <= 1e-6 * abs(f64)
     print(f"\nlearned: {sl}\nfp64: {s64}\ntraining: {st}")
+
+
+def test_untrained_network_flexible_cg_is_jacobi_pcg(pa):
+    """A new network is exactly Jacobi, so the flexible CG must track the
+    mixed Jacobi-PCG: same solution, about the same iterations, no fallback."""
+    from platoanalyze_b200.workloads import cantilever, cell_density
+    dims = (24, 12, 12)
+    mesh, prob, faces, dofs = cantilever(dims)
+    z = cell_density(dims, 3, kind="smoothed", sigma=2.0, lo=0.01, hi=1.0)
+    pc = pa.LearnedPreconditioner.for_box(*dims, seed=0)
+    prob.set_preconditioner(pc)
+    uj, sj = prob.solution(z, options=pa.SolveOptions("mixed", rel_tol=1e-8, check_every=32))
+    ul, sl = prob.solution(z, options=pa.SolveOptions("learned", rel_tol=1e-8, check_every=32))
+    assert sl["converged"] and sl["fallback_iterations"] == 0, sl
+    assert abs(sl["iterations"] - sj["iterations"]) <= 0.1 * sj["iterations"] + 32, (sl, sj)
+    assert np.abs(ul - uj).max() <= 1e-6 * np.abs(uj).max()
