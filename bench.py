@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--dims", default="160x80x80")
     ap.add_argument("--method", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--rel-tol", type=float, default=1e-8)
+    ap.add_argument("--check-every", type=int, default=64,
+                    help="iterations between FP64 residual replacements (one captured graph chunk)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-kernel", action="store_true",
                     help="only build the workload and time the fused CG kernel (for ncu captures)")
@@ -344,7 +346,7 @@ def run_ours(args):
     z_host = cell_density(dims, SEED + rank, kind="smoothed", sigma=3.0, lo=0.01, hi=1.0)
     z = torch.tensor(z_host, device="cuda")
     u = torch.empty(ndof, dtype=torch.float64, device="cuda")
-    opts = pa.SolveOptions(args.method, rel_tol=args.rel_tol)
+    opts = pa.SolveOptions(args.method, rel_tol=args.rel_tol, check_every=args.check_every)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device="cuda")  # 256 MB > 126 MB L2
 
     def solve_once():
