@@ -18,13 +18,14 @@
 // matrices); tap t = dx + 3 dy + 9 dz for offset (dx-1, dy-1, dz-1).
 //
 // Forward kernel (k_conv3_tc): persistent CTAs of 128 threads; a tile is
-// 8 x 16 x 1 output nodes = the M = 128 rows of one tcgen05.mma.  The CTA
-// keeps all 27 taps of the weights in shared memory, stages the tile's
-// 10 x 18 x 3 input halo channel-group-major ([Cin/8][540 nodes][8]) so that
+// 8 x 16 x 2 output nodes = two layers of the M = 128 rows of a tcgen05.mma.
+// The CTA keeps all 27 taps of the weights in shared memory, stages the tile's
+// 10 x 18 x 4 input halo channel-group-major ([Cin/8][720 nodes][8]) so that
 // every tap's A operand is the same halo viewed at a shifted start address
-// (rows 16 B apart, row groups 160 B apart), and one thread issues
-// 27 * Cin/16 MMAs of 128 x Cout x 16 into a 32-column TMEM accumulator.  The
-// epilogue (tcgen05.ld, bias, ReLU, BF16) writes 64 contiguous bytes per node.
+// (rows 16 B apart, row groups 160 B apart, layers 2880 B apart), and one
+// thread issues 2 x 27 x Cin/16 MMAs of 128 x Cout x 16 into two TMEM
+// accumulators that share each B operand.  The epilogue (tcgen05.ld, bias,
+// ReLU, BF16) writes 64 contiguous bytes per node.
 #include <algorithm>
 #include <cmath>
 #include <random>
@@ -53,11 +54,11 @@ int64_t w_offset(int l) {
 }
 int64_t b_offset(int l) { return w_offset(l) + int64_t(kCout[l]) * kCin[l] * 27; }
 
-constexpr int kTX = 8, kTY = 16;
-constexpr int kHX = kTX + 2, kHY = kTY + 2, kHZ = 3;
-constexpr int kHalo = kHX * kHY * kHZ;  // 540
+constexpr int kTX = 8, kTY = 16, kTZ = 2;
+constexpr int kHX = kTX + 2, kHY = kTY + 2, kHZ = kTZ + 2;
+constexpr int kHalo = kHX * kHY * kHZ;  // 720
 constexpr int kConvThreads = 128;
-constexpr int kTmemCols = 32;
+constexpr int kTmemCols = 64;  // two 128 x Cout accumulators (Cout <= 32)
 
 __device__ __forceinline__ void cp16(void* smem, const void* gmem) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(tc::smem_u32(smem)), "l"(gmem) : "memory");
@@ -91,8 +92,8 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_tc(ConvArgs a) {
   ConvSmem<CIN, COUT>& S = *reinterpret_cast<ConvSmem<CIN, COUT>*>(smem_raw);
   if (a.done && *a.done) return;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int ntx = (a.gx + kTX - 1) / kTX, nty = (a.gy + kTY - 1) / kTY;
-  const int ntiles = ntx * nty * a.gz;
+  const int ntx = (a.gx + kTX - 1) / kTX, nty = (a.gy + kTY - 1) / kTY, ntz = (a.gz + kTZ - 1) / kTZ;
+  const int ntiles = ntx * nty * ntz;
 
   constexpr int kWChunks = 27 * CIN * COUT / 8;
   for (int i = tid; i < kWChunks; i += kConvThreads) cp16(&S.w[8 * i], a.w + 8 * i);
@@ -113,7 +114,7 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_tc(ConvArgs a) {
 
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int tx = tile % ntx, ty = (tile / ntx) % nty, tz = tile / (ntx * nty);
-    const int x0 = tx * kTX, y0 = ty * kTY, z0 = tz;
+    const int x0 = tx * kTX, y0 = ty * kTY, z0 = tz * kTZ;
     // halo: node (x0 + hx - 1, y0 + hy - 1, z0 + hz - 1), zero outside the grid;
     // the channel group runs fastest so that consecutive threads read one
     // node's contiguous channels
@@ -142,9 +143,12 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_tc(ConvArgs a) {
         const uint32_t aoff = uint32_t(((dz * kHY + dy) * kHX + dx) * 16);
 #pragma unroll
         for (int j = 0; j < CIN / 16; ++j) {
-          const uint64_t ad = tc::smem_desc(hb + uint32_t(2 * j * kHalo * 16) + aoff, kHalo * 16, kHX * 16);
+          const uint32_t a0 = hb + uint32_t(2 * j * kHalo * 16) + aoff;
           const uint64_t bd = tc::smem_desc(wb + uint32_t((t * (CIN / 8) + 2 * j) * COUT * 16), COUT * 16, 128);
-          tc::mma_bf16(tmem, ad, bd, idesc, (t | j) != 0 ? 1u : 0u);
+          const uint32_t acc = (t | j) != 0 ? 1u : 0u;
+          // output layer z0 into columns [0, COUT), layer z0 + 1 into [COUT, 2 COUT)
+          tc::mma_bf16(tmem, tc::smem_desc(a0, kHalo * 16, kHX * 16), bd, idesc, acc);
+          tc::mma_bf16(tmem + COUT, tc::smem_desc(a0 + kHY * kHX * 16, kHalo * 16, kHX * 16), bd, idesc, acc);
         }
       }
       tc::commit(&S.mbar);
@@ -157,44 +161,48 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_tc(ConvArgs a) {
       break;
     }
     tc::fence_after_sync();
-    // epilogue: row m = 32 warp + lane of the accumulator is node (x0 + m % 8, y0 + m / 8, z0)
-    const uint32_t taddr = tmem + (uint32_t(warp * 32) << 16);
-    float vals[COUT];
-    if constexpr (COUT == 32) {
-      uint32_t r[32];
-      tc::tmem_ld32(taddr, r);
-      tc::tmem_wait_ld();
-#pragma unroll
-      for (int c = 0; c < 32; ++c) vals[c] = __uint_as_float(r[c]);
-    } else {
-      uint32_t r[16];
-      tc::tmem_ld16(taddr, r);
-      tc::tmem_wait_ld();
-#pragma unroll
-      for (int c = 0; c < 16; ++c) vals[c] = __uint_as_float(r[c]);
-    }
+    // epilogue: row m = 32 warp + lane of accumulator h is node (x0 + m % 8, y0 + m / 8, z0 + h)
     const int m = warp * 32 + lane;
     const int x = x0 + (m & 7), y = y0 + (m >> 3);
-    if (x < a.gx && y < a.gy) {
-      const int64_t v = x + int64_t(a.gx) * (y + int64_t(a.gy) * z0);
 #pragma unroll
-      for (int c = 0; c < COUT; ++c) {
-        vals[c] += S.bias[c];
-        if (RELU) vals[c] = fmaxf(vals[c], 0.0f);
+    for (int h = 0; h < kTZ; ++h) {
+      const uint32_t taddr = tmem + (uint32_t(warp * 32) << 16) + uint32_t(h * COUT);
+      float vals[COUT];
+      if constexpr (COUT == 32) {
+        uint32_t r[32];
+        tc::tmem_ld32(taddr, r);
+        tc::tmem_wait_ld();
+#pragma unroll
+        for (int c = 0; c < 32; ++c) vals[c] = __uint_as_float(r[c]);
+      } else {
+        uint32_t r[16];
+        tc::tmem_ld16(taddr, r);
+        tc::tmem_wait_ld();
+#pragma unroll
+        for (int c = 0; c < 16; ++c) vals[c] = __uint_as_float(r[c]);
       }
-      if (a.out_bf) {
-        uint32_t pk[COUT / 2];
+      const int z = z0 + h;
+      if (x < a.gx && y < a.gy && z < a.gz) {
+        const int64_t v = x + int64_t(a.gx) * (y + int64_t(a.gy) * z);
 #pragma unroll
-        for (int c = 0; c < COUT / 2; ++c) {
-          __nv_bfloat162 h = __floats2bfloat162_rn(vals[2 * c], vals[2 * c + 1]);
-          pk[c] = *reinterpret_cast<uint32_t*>(&h);
+        for (int c = 0; c < COUT; ++c) {
+          vals[c] += S.bias[c];
+          if (RELU) vals[c] = fmaxf(vals[c], 0.0f);
         }
-        uint4* dst = reinterpret_cast<uint4*>(a.out_bf + v * COUT);
+        if (a.out_bf) {
+          uint32_t pk[COUT / 2];
 #pragma unroll
-        for (int q = 0; q < COUT / 8; ++q) dst[q] = make_uint4(pk[4 * q], pk[4 * q + 1], pk[4 * q + 2], pk[4 * q + 3]);
+          for (int c = 0; c < COUT / 2; ++c) {
+            __nv_bfloat162 hh = __floats2bfloat162_rn(vals[2 * c], vals[2 * c + 1]);
+            pk[c] = *reinterpret_cast<uint32_t*>(&hh);
+          }
+          uint4* dst = reinterpret_cast<uint4*>(a.out_bf + v * COUT);
+#pragma unroll
+          for (int q = 0; q < COUT / 8; ++q) dst[q] = make_uint4(pk[4 * q], pk[4 * q + 1], pk[4 * q + 2], pk[4 * q + 3]);
+        }
+        if (a.out_f32)
+          reinterpret_cast<float4*>(a.out_f32)[v] = make_float4(vals[0], vals[1], vals[2], vals[3]);
       }
-      if (a.out_f32)
-        reinterpret_cast<float4*>(a.out_f32)[v] = make_float4(vals[0], vals[1], vals[2], vals[3]);
     }
     tc::fence_before_sync();
   }
@@ -216,14 +224,14 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_tc(ConvArgs a) {
 template <int CIN, int COUT, bool RELU>
 void launch_conv_instance(const ConvArgs& a, cudaStream_t s) {
   // CTAs per SM from the shared-memory footprint (228 KB per SM, 1 KB reserved
-  // per CTA), at most 4 (4 x 32 of the 512 tensor-memory columns)
+  // per CTA), at most 4 (4 x 64 of the 512 tensor-memory columns)
   static int grid_per_sm = 0;
   const size_t smem = sizeof(ConvSmem<CIN, COUT>);
   if (!grid_per_sm) {
     PA_CUDA(cudaFuncSetAttribute(k_conv3_tc<CIN, COUT, RELU>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     grid_per_sm = std::max(1, std::min(4, int((228 * 1024) / (smem + 1024))));
   }
-  const int ntiles = ((a.gx + kTX - 1) / kTX) * ((a.gy + kTY - 1) / kTY) * a.gz;
+  const int ntiles = ((a.gx + kTX - 1) / kTX) * ((a.gy + kTY - 1) / kTY) * ((a.gz + kTZ - 1) / kTZ);
   const int grid = std::max(1, std::min(ntiles, grid_per_sm * num_sms()));
   k_conv3_tc<CIN, COUT, RELU><<<grid, kConvThreads, smem, s>>>(a);
   PA_LAUNCHED();
