@@ -62,7 +62,11 @@ pa_status guard(F&& f) {
 template <typename F>
 pa_status guard_status(F&& f) {
   try {
-    return f();
+    const pa_status st = f();
+    if (st == PA_ERR_NOT_CONVERGED) set_last_error("the iteration cap was reached before the tolerance");
+    else if (st == PA_ERR_BREAKDOWN) set_last_error("Krylov breakdown (p.Kp <= 0 or non-finite)");
+    else if (st == PA_ERR_NONFINITE) set_last_error("non-finite value in a reduction");
+    return st;
   } catch (const Error& e) {
     set_last_error(e.what());
     return e.status;

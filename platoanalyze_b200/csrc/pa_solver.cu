@@ -751,8 +751,8 @@ pa_status solve_operator(Problem& P, const SolveOperator& op, const double* b, d
 // convolutions), the correction weight, z/beta, the fused apply (p, K p, p.Kp,
 // alpha), the update.
 // The solve continues as mixed Jacobi-PCG from the current iterate when the
-// network's direction is not a descent direction or the true residual has not
-// decreased over two chunks.
+// network's direction is not a descent direction, the FP64 residual has not
+// improved for 512 iterations, or half of the iteration budget is spent.
 pa_status solve_fcg(Problem& P, const SolveOperator& op, LearnedPC& pc, const double* b, double* x_out,
                     const pa_solve_options& o, pa_solve_stats* st) {
   cudaStream_t s = P.stream;
@@ -897,12 +897,18 @@ pa_status solve_fcg(Problem& P, const SolveOperator& op, LearnedPC& pc, const do
     ++replacements;
     converged = rr_true <= tol2 * bb;
     hist.push_back(rr_true);
-    if (converged || iters >= max_iters) break;
-    // stalled: no chunk of the last four improved on the best residual before them
+    if (converged) break;
+    if (iters >= max_iters / 2) {  // too slow: hand the rest of the solve to Jacobi-PCG
+      fallback = true;
+      break;
+    }
+    // stalled: no chunk of the last `window` (>= 512 iterations) improved on
+    // the best residual before them (CG residuals are not monotone)
     bool stalled = false;
-    if (hist.size() >= 5) {
-      const double before = *std::min_element(hist.begin(), hist.end() - 4);
-      const double recent = *std::min_element(hist.end() - 4, hist.end());
+    const size_t window = size_t(std::max(4, (512 + chunk - 1) / chunk));
+    if (hist.size() > window) {
+      const double before = *std::min_element(hist.begin(), hist.end() - window);
+      const double recent = *std::min_element(hist.end() - window, hist.end());
       stalled = !(recent < 0.99 * before);
     }
     if (hs.breakdown || stalled || !std::isfinite(rr_true)) {
@@ -922,11 +928,11 @@ pa_status solve_fcg(Problem& P, const SolveOperator& op, LearnedPC& pc, const do
   }
   pa_status status = PA_OK;
   int fb_iters = 0;
-  if (fallback && iters < max_iters) {
+  if (fallback) {
     pa_solve_options fo = o;
     fo.method = PA_SOLVER_PCG_MIXED;
     fo.use_initial_guess = 1;
-    fo.max_iters = max_iters - iters;
+    fo.max_iters = max_iters;  // the fallback is a solve of its own
     pa_solve_stats fst{};
     status = solve_operator(P, op, b, x_out, fo, &fst, false);
     fb_iters = fst.iterations;
