@@ -313,6 +313,25 @@ pa_status pa_j2_solve(pa_problem* problem, const pa_j2_params* params, const dou
                       const pa_j2_solve_options* options, const pa_solve_options* linear, double* u, double* local,
                       pa_j2_stats* stats);
 
+/* Stabilized u-p plasticity residual, InfinitesimalStrainPlasticityResidual::
+ * evaluate (src/InfinitesimalStrainPlasticityResidual.hpp:398-516): state is
+ * 4 dofs per node (u_x, u_y, u_z, p; 4N), local the C x 14 local states, z the
+ * N nodal controls, ppg the projected pressure gradient, per node (3N,
+ * ppg_per_cell = 0) or per cell node (C x 12, ppg_per_cell = 1, the
+ * reference's workset).  residual: per cell (C x 16, node-major, assembled =
+ * 0, the reference's result workset) or assembled (4N, assembled = 1). */
+typedef struct {
+  double youngs_modulus;
+  double poissons_ratio;
+  double penalty_exponent;  /* SIMP on the elastic moduli */
+  double penalty_min;
+  double pressure_scaling;  /* "Pressure Scaling", default 1 */
+} pa_up_params;
+
+pa_status pa_up_residual(pa_problem* problem, const pa_up_params* params, const double* state, const double* local,
+                         const double* ppg, int32_t ppg_per_cell, const double* z, double* residual,
+                         int32_t assembled);
+
 /* ------------------------------------------------------ batched solves --- */
 /* No counterpart in the reference (one Problem solves one mesh).  A parted
  * mesh is the disjoint union of independent sub-meshes: part p owns the nodes

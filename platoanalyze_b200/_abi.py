@@ -53,6 +53,11 @@ class J2Stats(ct.Structure):
                 ("line_search_halvings", I32)]
 
 
+class UpParams(ct.Structure):
+    _fields_ = [("youngs_modulus", F64), ("poissons_ratio", F64), ("penalty_exponent", F64), ("penalty_min", F64),
+                ("pressure_scaling", F64)]
+
+
 class PcTrainOptions(ct.Structure):
     _fields_ = [("steps", I32), ("batch", I32), ("learning_rate", F64), ("seed", ct.c_uint64)]
 
@@ -110,6 +115,7 @@ SIGNATURES = [
     ("pa_pc_apply", I32, [P, P, P, P, P]),
     ("pa_pc_train", I32, [P, P, I32, P, I32, P, P, P, ct.POINTER(PcTrainOptions), ct.POINTER(PcTrainStats)]),
     ("pa_problem_set_preconditioner", I32, [P, P]),
+    ("pa_up_residual", I32, [P, ct.POINTER(UpParams), P, P, P, I32, P, P, I32]),
     ("pa_mesh_set_parts", I32, [P, I32, P]),
     ("pa_problem_part_stats", I32, [P, P, P]),
     ("pa_problem_autotune_tiles", I32, [P, P, P, P]),

@@ -294,6 +294,23 @@ class Problem:
                                                  _ptr(local, np.float64, 14 * C, "local")))
         return local
 
+    def up_residual(self, params, state, local, ppg, z, per_cell_ppg=False, assembled=True, out=None):
+        """Stabilized u-p plasticity residual (InfinitesimalStrainPlasticityResidual::evaluate):
+        per cell (C x 16) or assembled (4N)."""
+        C, N = self.mesh.num_cells, self.mesh.num_nodes
+        state, local, ppg, z = (_as(a, np.float64) for a in (state, local, ppg, z))
+        n_out = 4 * N if assembled else 16 * C
+        out = _empty(state, n_out) if out is None else out
+        up = _abi.UpParams(*[float(params.get(k, d)) for k, d in (
+            ("youngs_modulus", None), ("poissons_ratio", None), ("penalty_exponent", 3.0), ("penalty_min", 1e-9),
+            ("pressure_scaling", 1.0))])
+        _abi.check(self._lib.pa_up_residual(self._h, ct.byref(up), _ptr(state, np.float64, 4 * N, "state"),
+                                            _ptr(local, np.float64, 14 * C, "local"),
+                                            _ptr(ppg, np.float64, 12 * C if per_cell_ppg else 3 * N, "ppg"),
+                                            int(bool(per_cell_ppg)), _ptr(z, np.float64, N, "z"),
+                                            _ptr(out, np.float64, n_out, "residual"), int(bool(assembled))))
+        return out
+
     @staticmethod
     def _j2_params(params):
         return _abi.J2Params(*[float(params[k]) for k in (

@@ -710,6 +710,25 @@ pa_status pa_j2_local_residual(pa_problem* problem, const pa_j2_params* params, 
   });
 }
 
+pa_status pa_up_residual(pa_problem* problem, const pa_up_params* params, const double* state, const double* local,
+                         const double* ppg, int32_t ppg_per_cell, const double* z, double* residual,
+                         int32_t assembled) {
+  return guard([&] {
+    Problem& P = prob(problem);
+    PA_CHECK(params, "null u-p parameters");
+    PA_CHECK(params->youngs_modulus > 0 && params->poissons_ratio > -1.0 && params->poissons_ratio < 0.5,
+             "u-p moduli out of range");
+    pa::Stage st(P);
+    const double* ds = st.in(state, 4 * P.N(), "state");
+    const double* dl = st.in(local, 14 * P.C(), "local");
+    const double* dp = st.in(ppg, ppg_per_cell ? 12 * P.C() : 3 * P.N(), "projected pressure gradient");
+    const double* dz = st.in(z, P.N(), "z");
+    double* dr = st.out(residual, assembled ? 4 * P.N() : 16 * P.C(), "residual");
+    pa::launch_up_residual(P, *params, ds, dl, dp, ppg_per_cell ? 1 : 0, dz, dr, assembled ? 1 : 0, P.stream);
+    st.finish();
+  });
+}
+
 pa_status pa_j2_solve(pa_problem* problem, const pa_j2_params* params, const double* z,
                       const pa_j2_solve_options* options, const pa_solve_options* linear, double* u, double* local,
                       pa_j2_stats* stats) {

@@ -193,6 +193,9 @@ void launch_copy_dofs(const int32_t* dofs, int64_t n, const T* src, T* dst, cuda
 void launch_diag(const Problem& P, const double* w, double* diag, cudaStream_t s);
 void launch_j2(const Problem& P, const pa_j2_params& jp, const double* u, const double* z, const double* prev,
                double* cur, cudaStream_t s);
+void launch_up_residual(const Problem& P, const pa_up_params& up, const double* state, const double* local,
+                        const double* ppg, int ppg_per_cell, const double* z, double* out, int assemble,
+                        cudaStream_t s);
 
 int num_sms();
 

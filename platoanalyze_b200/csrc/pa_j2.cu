@@ -338,6 +338,97 @@ void launch_j2(const Problem& P, const pa_j2_params& jp, const double* u, const 
   PA_LAUNCHED();
 }
 
+// Stabilized u-p plasticity residual, InfinitesimalStrainPlasticityResidual::
+// evaluate (src/InfinitesimalStrainPlasticityResidual.hpp:398-516): 4 dofs per
+// node (u_x, u_y, u_z, p); elastic strain e = eps(u) - eps_p (local state
+// 2..7); deviatoric stress s = 2 mu_p dev(e) (shears mu_p gamma); displacement
+// rows V (s + ps p_c 1) grad N; pressure rows -V stab . grad N + V N theta with
+// theta = ps (tr eps - ps p_c / kappa_p), stab = pen ps tau (ps grad p - Pi),
+// tau = V^(2/3) / (2 mu) (src/ComputeStabilization.hpp:93-108); p_c and Pi
+// (projected pressure gradient) interpolated with the one-point basis (1/4).
+// Pi is per node (ppg_per_cell = 0: 3N) or per cell node (1: C x 12).  Output
+// per cell (C x 16, node-major) or assembled (4N, atomics).
+struct UpDev {
+  double mu, kappa, pe, pe_min, ps;
+};
+
+__global__ void k_up_residual(const int32_t* __restrict__ cells, const double* __restrict__ coords, int64_t C,
+                              UpDev q, const double* __restrict__ state, const double* __restrict__ local,
+                              const double* __restrict__ ppg, int ppg_per_cell, const double* __restrict__ z,
+                              double* __restrict__ out, int assemble) {
+  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (c >= C) return;
+  const int4 qv = reinterpret_cast<const int4*>(cells)[c];
+  const int v[4] = {qv.x, qv.y, qv.z, qv.w};
+  double x[4][3], ue[12], p[4], pi[3] = {0.0, 0.0, 0.0}, g[4][3], vol, eps[6];
+  double rho = 0.0;
+#pragma unroll
+  for (int n = 0; n < 4; ++n) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      x[n][d] = coords[3 * int64_t(v[n]) + d];
+      ue[3 * n + d] = state[4 * int64_t(v[n]) + d];
+      pi[d] += 0.25 * (ppg_per_cell ? ppg[12 * c + 3 * n + d] : ppg[3 * int64_t(v[n]) + d]);
+    }
+    p[n] = state[4 * int64_t(v[n]) + 3];
+    rho += 0.25 * z[v[n]];
+  }
+  tet_geometry(x, g, vol);
+  tet_strain(g, ue, eps);
+  const double* L = local + 14 * c;
+  double e[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) e[i] = eps[i] - L[2 + i];
+  const double pen = simp(rho, q.pe, q.pe_min);
+  const double mu_p = pen * q.mu, kappa_p = pen * q.kappa;
+  const double tr3 = (e[0] + e[1] + e[2]) * (1.0 / 3.0);
+  const double sv[6] = {2.0 * mu_p * (e[0] - tr3), 2.0 * mu_p * (e[1] - tr3), 2.0 * mu_p * (e[2] - tr3),
+                        mu_p * e[3], mu_p * e[4], mu_p * e[5]};
+  double gp[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+  for (int n = 0; n < 4; ++n)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) gp[d] += p[n] * g[n][d];
+  const double pc = q.ps * 0.25 * (p[0] + p[1] + p[2] + p[3]);
+  const double theta = q.ps * (eps[0] + eps[1] + eps[2] - pc / kappa_p);
+  const double cv = cbrt(vol);
+  const double tau = cv * cv / (2.0 * q.mu);
+  double stab[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) stab[d] = pen * q.ps * tau * (q.ps * gp[d] - pi[d]);
+  // stress rows: V (s + pc 1) grad N
+  const double S[3][3] = {{sv[0] + pc, sv[5], sv[4]}, {sv[5], sv[1] + pc, sv[3]}, {sv[4], sv[3], sv[2] + pc}};
+  double r[16];
+#pragma unroll
+  for (int n = 0; n < 4; ++n) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) r[4 * n + i] = vol * (S[i][0] * g[n][0] + S[i][1] * g[n][1] + S[i][2] * g[n][2]);
+    r[4 * n + 3] = -vol * (stab[0] * g[n][0] + stab[1] * g[n][1] + stab[2] * g[n][2]) + vol * 0.25 * theta;
+  }
+  if (assemble) {
+#pragma unroll
+    for (int n = 0; n < 4; ++n)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) atomicAdd(&out[4 * int64_t(v[n]) + k], r[4 * n + k]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < 16; ++k) out[16 * c + k] = r[k];
+  }
+}
+
+void launch_up_residual(const Problem& P, const pa_up_params& up, const double* state, const double* local,
+                        const double* ppg, int ppg_per_cell, const double* z, double* out, int assemble,
+                        cudaStream_t s) {
+  const int64_t C = P.C();
+  const double mu = up.youngs_modulus / (2.0 * (1.0 + up.poissons_ratio));
+  const double kappa = up.youngs_modulus / (3.0 * (1.0 - 2.0 * up.poissons_ratio));
+  const UpDev q{mu, kappa, up.penalty_exponent, up.penalty_min, up.pressure_scaling};
+  if (assemble) PA_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * 4 * P.N(), s));
+  k_up_residual<<<int((C + 127) / 128), 128, 0, s>>>(P.mesh->d_cells.get(), P.mesh->d_coords.get(), C, q, state,
+                                                     local, ppg, ppg_per_cell, z, out, assemble);
+  PA_LAUNCHED();
+}
+
 void launch_j2_local_residual(const Problem& P, const pa_j2_params& jp, const double* u, const double* z,
                               const double* loc, const double* prev, double* H, cudaStream_t s) {
   const int64_t C = P.C();

@@ -12,6 +12,8 @@ its unit tests are read as text and their gold arrays extracted:
   InternalElasticEnergy3D: 2x2x2 unit box, E=1e6, nu=0.3, SIMP p=1, min 0,
   z = 1, u_i = 1e-4 (i+1).
 * unit_tests/PlasticityTests.cpp, J2PlasticityUtils_UpdatePlasticStep3D.
+* unit_tests/ElastoPlasticityTests.cpp, ElastoPlasticity_Residual3D_Elastic
+  (stabilized u-p residual on the single-hex box).
 
 The gold values depend on the vertex numbering of Omega_h's build_box, whose
 source is not available.  It is identified here by search rather than
@@ -186,11 +188,69 @@ def j2_plastic_step():
     }
 
 
+def up_residual_3d():
+    """ElastoPlasticity_Residual3D_Elastic (unit_tests/ElastoPlasticityTests.cpp:1967-2100):
+    stabilized u-p residual on the single-hex box (6 tets), E = 1e11, nu = 0.35,
+    SIMP 3 / 1e-9, controls 1, zero local states, nodal state
+    (1e-7, 2e-7, 3e-7, 4e-7) x vertex id, projected pressure gradient
+    4e-7 (n+1)(d+1)(c+1) at node n of cell c.  The per-cell vertex coordinates
+    are the reference's own (unit_tests/OmegaHUtilitiesTests.cpp:258-287, the
+    six-tet split); the vertex ids of the eight corners are identified by
+    exhaustive search over the 8! numberings against the gold residual."""
+    import itertools
+    from oracle import np_up
+    src = open(os.path.join(REF, "unit_tests/ElastoPlasticityTests.cpp")).read()
+    s = src.index("ElastoPlasticity_Residual3D_Elastic")
+    i = src.index("tGold", s)
+    j = src.index("{", i)
+    k = src.index("};", j)
+    rows = re.findall(r"\{([^{}]*)\}", src[j + 1:k + 1])
+    gold = [[float(t) for t in re.findall(r"[-+]?[0-9]*\.?[0-9]+(?:[eE][-+]?[0-9]+)?", r)] for r in rows]
+    gold = np.array(gold)
+    assert gold.shape == (6, 16), gold.shape
+    corners = [(a, b, c) for c in (0, 1) for b in (0, 1) for a in (0, 1)]
+    tets = np_ref.HEX_TETS
+    coords_c = np.array(corners, dtype=np.float64)
+    cells_c = np.array([[corners.index(v) for v in t] for t in tets])
+    ppg = np.array([[[4e-7 * (n + 1) * (d + 1) * (c + 1) for d in range(3)] for n in range(4)] for c in range(6)])
+    local = np.zeros((6, 14))
+    hits = []
+    for perm in itertools.permutations(range(8)):
+        perm = np.array(perm)  # corner -> vertex id
+        ids = perm.astype(np.float64)
+        state = np.zeros((8, 4))
+        for d in range(4):
+            state[:, d] = (d + 1) * 1e-7 * ids
+        R = np_up.up_residual_cells(cells_c, coords_c, state.ravel(), local, ppg, np.ones(8), 1e11, 0.35)
+        if np.all(np.abs(R - gold) <= 1e-4 * np.maximum(np.abs(gold), 1e-30) + 1e-12):
+            hits.append(perm)
+    assert len(hits) >= 1, "no numbering reproduces the gold"
+    perm = hits[0]
+    v_coords = np.zeros((8, 3))
+    v_coords[perm] = coords_c
+    v_cells = perm[cells_c]
+    return {
+        "source": "unit_tests/ElastoPlasticityTests.cpp:1967-2100 (ElastoPlasticity_Residual3D_Elastic)",
+        "mesh": "Omega_h build_box 1x1x1, six tets; vertex ids identified by tests/golden/make_golden.py",
+        "numberings_matching": len(hits),
+        "material": {"youngs_modulus": 1e11, "poissons_ratio": 0.35, "simp_exponent": 3.0, "simp_min": 1e-9,
+                     "pressure_scaling": 1.0},
+        "state": "vertex v: (1e-7 v, 2e-7 v, 3e-7 v, 4e-7 v); controls 1; local states 0",
+        "projected_pressure_gradient": ppg.reshape(6, 12).tolist(),
+        "tolerance": 1e-4,
+        "cells": v_cells.tolist(),
+        "coords": v_coords.tolist(),
+        "gold": gold.tolist(),
+    }
+
+
 def main():
     with open(os.path.join(OUT, "derivative_tests_3d.json"), "w") as f:
         json.dump(derivative_tests(), f, indent=1)
     with open(os.path.join(OUT, "j2_plastic_step_3d.json"), "w") as f:
         json.dump(j2_plastic_step(), f, indent=1)
+    with open(os.path.join(OUT, "up_residual_3d.json"), "w") as f:
+        json.dump(up_residual_3d(), f, indent=1)
     print("wrote fixtures to", OUT)
 
 
