@@ -1,6 +1,6 @@
 """The benchmark's N > 1 host logic on CPU ranks (gloo, world size 2):
-the max-over-ranks timing and the whole-job rate, and the reference arm's
-rank != 0 early exit."""
+the max-over-ranks timing and the whole-job rate, the batched workload's
+dealing of boxes to ranks, and the reference arm's rank != 0 early exit."""
 import os
 import socket
 
@@ -27,7 +27,11 @@ def _rank_main(rank, world, port, out):
     try:
         mx = bench.max_over_ranks(10.0 * (rank + 1), world, device="cpu")
         rate = bench.whole_job_rate(world, 1000, 2, mx)
-        out.put((rank, mx, rate))
+        # batched workload: the boxes dealt to the ranks cover every box once
+        mine = bench.dealt_boxes(64, world, rank)
+        every = [None] * world
+        dist.all_gather_object(every, mine)
+        out.put((rank, mx, rate, sorted(b for lst in every for b in lst)))
         dist.barrier()
     finally:
         dist.destroy_process_group()
@@ -45,9 +49,10 @@ def test_max_over_ranks_gloo():
         p.join(timeout=120)
         assert p.exitcode == 0
     res = sorted(q.get(timeout=10) for _ in range(world))
-    for rank, mx, rate in res:
+    for rank, mx, rate, boxes in res:
         assert mx == 20.0
         assert rate == pytest.approx(2 * 1000 * 2 / 0.020)
+        assert boxes == list(range(64))
 
 
 def test_reference_arm_nonzero_rank_exits_without_work(monkeypatch):
