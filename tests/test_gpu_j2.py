@@ -60,3 +60,39 @@ def test_j2_newton_matches_oracle(pa, method, hkin):
     assert np.abs(loc - loc_ref).max() <= 1e-6 * max(np.abs(loc_ref).max(), 1e-12) + 1e-12
     # Newton with the consistent tangent converges in a handful of iterations per step
     assert st["newton_iterations"] <= 8 * steps
+
+
+def test_j2_newton_on_a_shuffled_mesh(pa):
+    """Cells and their vertex order shuffled (every tet a single cluster in the
+    tile kernel, tangent records reached through the single-cell path): the
+    same load-stepped solution as the structured numbering."""
+    from oracle import np_ref
+    rng = np.random.default_rng(8)
+    cells, coords = np_ref.box_mesh(6, 2, 2, 6.0, 2.0, 2.0)
+    perm = rng.permutation(cells.shape[0])
+    shuffled = cells[perm].copy()
+    for c in range(shuffled.shape[0]):  # any vertex order is valid: the volume uses |det|
+        shuffled[c] = shuffled[c][rng.permutation(4)]
+    results = []
+    for cl in (cells, shuffled):
+        mesh = pa.Mesh.from_arrays(cl, coords)
+        prob = pa.Problem(mesh, 200e3, 0.3)
+        x0 = np.where(coords[:, 0] < 1e-9)[0]
+        x1 = np.where(coords[:, 0] > 6.0 - 1e-9)[0]
+        dofs = np.concatenate([3 * x0, 3 * x0 + 1, 3 * x0 + 2, 3 * x1])
+        vals = np.concatenate([np.zeros(3 * x0.size), np.full(x1.size, 0.02 * 6.0)])
+        order = np.argsort(dofs)
+        prob.set_dirichlet(dofs[order].astype(np.int32), vals[order])
+        params = dict(youngs_modulus=200e3, poissons_ratio=0.3, initial_yield_stress=250.0,
+                      hardening_modulus_isotropic=1000.0, hardening_modulus_kinematic=0.0,
+                      elastic_penalty_exponent=3.0, elastic_min_ersatz=1e-9, plastic_penalty_exponent=2.5,
+                      plastic_min_ersatz=1e-9)
+        u, local, st = prob.j2_solve(params, np.ones(coords.shape[0]), steps=5, max_newton=30, newton_tol=1e-10,
+                                     options=pa.SolveOptions("fp64", rel_tol=1e-12))
+        assert st["converged"], st
+        results.append((u, np.asarray(local).reshape(-1, 14), mesh.num_tiles))
+    (u0, l0, _), (u1, l1, _) = results
+    assert np.abs(u1 - u0).max() <= 1e-8 * np.abs(u0).max()
+    # local states follow the user's cell order
+    assert np.abs(l1 - l0[perm]).max() <= 1e-6 * max(np.abs(l0).max(), 1e-12) + 1e-12
+    assert (l0[:, 0] > 0).any()
