@@ -336,6 +336,7 @@ pa_status solve_batched(Problem& P, const SolveOperator& op, const double* b, do
     a.tv = m.tiles();
     a.N = N;
     a.coords = m.d_coords32_soa.get();
+    a.coords4 = m.d_coords32_aos4.get();
     a.w = op.w32;
     a.tile_nodes = P.d_tile_nodes_bc.get();
     Iso<double> i64 = P.ep.iso();

@@ -101,6 +101,7 @@ struct Mesh {
   DevBuf<double> d_coords;           // N*3 interleaved (cell kernels)
   DevBuf<double> d_coords_soa;       // 3N component-major (tile kernel, FP64)
   DevBuf<float> d_coords32_soa;      // 3N component-major (tile kernel, FP32)
+  DevBuf<float4> d_coords32_aos4;    // N x (x, y, z, 0): one 16-byte gather per node (FP32 PCG modes)
   DevBuf<int32_t> d_rowmap, d_cols;
   DevBuf<int32_t> d_cell_entry;  // C*16 CRS block index of (a,b) pairs
   int64_t num_clusters = 0, num_hex = 0;

@@ -372,6 +372,10 @@ void mesh_build(Mesh& m) {
     }
   m.d_coords_soa.upload(soa.data(), soa.size());
   m.d_coords32_soa.upload(soa32.data(), soa32.size());
+  std::vector<float4> aos4(m.N);
+  for (int64_t v = 0; v < m.N; ++v)
+    aos4[v] = make_float4(float(m.coords[3 * v]), float(m.coords[3 * v + 1]), float(m.coords[3 * v + 2]), 0.0f);
+  m.d_coords32_aos4.upload(aos4.data(), aos4.size());
   PA_CUDA(cudaDeviceSynchronize());
 }
 

@@ -474,6 +474,7 @@ ApplyArgs<T> fused_args(Problem& P, const T* coords, const T* w, const T* p_old,
   a.tv = P.mesh->tiles();
   a.N = P.N();
   a.coords = coords;
+  if constexpr (std::is_same<T, float>::value) a.coords4 = P.mesh->d_coords32_aos4.get();
   a.w = w;
   a.plas = plas;
   a.tile_nodes = P.d_tile_nodes_bc.get();

@@ -42,6 +42,7 @@ struct ApplyArgs {
   const uint32_t* tile_nodes;  // flagged node ids (mask bits set for the problem's BCs, or none)
   int64_t N;                   // nodes (SoA stride)
   const T* coords;             // 3N, SoA
+  const float4* coords4;       // FP32 PCG modes: N x (x, y, z, 0), one 16-byte gather per node (or null)
   const T* w;                  // C, SIMP weight per cell, internal order
   const T* plas;               // null (elastic) or 8 per cell, internal order: J2 tangent record
   Iso<T> iso;
@@ -266,9 +267,20 @@ __device__ __forceinline__ void prefetch_data(const ApplyArgs<T>& a, TileSmem<T,
   const int64_t N = a.N;
   for (int i = threadIdx.x; i < nn; i += blockDim.x) {
     const int64_t g = int64_t(S.ids[b][i] & kNodeIdMask);
-    cp_async<sizeof(T)>(&S.xc[b][i].x, &a.coords[g]);
-    cp_async<sizeof(T)>(&S.xc[b][i].y, &a.coords[N + g]);
-    cp_async<sizeof(T)>(&S.xc[b][i].z, &a.coords[2 * N + g]);
+    bool packed = false;
+    if constexpr (sizeof(T) == 4 && MODE >= 1) {
+      // (x, y, z, 0) in one copy; the fourth slot is the input component 0,
+      // which the PCG modes write after this copy has landed
+      if (a.coords4) {
+        cp_async<16>(&S.xc[b][i], &a.coords4[g]);
+        packed = true;
+      }
+    }
+    if (!packed) {
+      cp_async<sizeof(T)>(&S.xc[b][i].x, &a.coords[g]);
+      cp_async<sizeof(T)>(&S.xc[b][i].y, &a.coords[N + g]);
+      cp_async<sizeof(T)>(&S.xc[b][i].z, &a.coords[2 * N + g]);
+    }
     if constexpr (MODE == 0) {
       cp_async<sizeof(T)>(&S.xc[b][i].u0, &a.x[g]);
       cp_async<sizeof(T)>(&S.uu[b][i].u1, &a.x[N + g]);
