@@ -291,6 +291,7 @@ pa_status solve_batched(Problem& P, const SolveOperator& op, const double* b, do
   k_b_inv_diag<double><<<vg, kBT, 0, s>>>(N, op.diag_aos, mask, ws.dinv.get());
   k_b_inv_diag<float><<<vg, kBT, 0, s>>>(N, op.diag_aos, mask, ws.dinv32.get());
   PA_LAUNCHED();
+  launch_pack4(N, ws.dinv32.get(), ws.dinv4.get(), s);
   launches += 2;
   double* bprime = ws.b.get();
   if (nbc) {
@@ -345,6 +346,7 @@ pa_status solve_batched(Problem& P, const SolveOperator& op, const double* b, do
     a.y = ws.ap32.get();
     a.r = ws.r32.get();
     a.dinv = ws.dinv32.get();
+    a.dinv4 = ws.dinv4.get();
     a.p_new = p_new;
     a.sc = ws.sc.get();
     a.partials = ws.partials.get();

@@ -198,6 +198,9 @@ void launch_up_residual(const Problem& P, const pa_up_params& up, const double* 
                         const double* ppg, int ppg_per_cell, const double* z, double* out, int assemble,
                         cudaStream_t s);
 
+// out[v] = (soa[v], soa[N + v], soa[2N + v], 0)
+void launch_pack4(int64_t N, const float* soa, float4* out, cudaStream_t s);
+
 int num_sms();
 
 }  // namespace pa

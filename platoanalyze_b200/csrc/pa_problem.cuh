@@ -15,6 +15,7 @@ struct SolverWorkspace {
   DevBuf<float> r32, p32a, p32b, ap32, dinv32, dx32, w32;
   DevBuf<float> coords32;
   DevBuf<float> ones32, z32;   // flexible CG: all-ones "diagonal", preconditioned residual
+  DevBuf<float4> dinv4, ones4; // D^-1 (and the all-ones diagonal) as N x (x, y, z, 0) for the FP32 tile kernel
   DevBuf<double> fcg_state;    // flexible CG scalars
   DevBuf<double> partials;
   DevBuf<unsigned int> counters;

@@ -468,13 +468,14 @@ int fused_apply_grid(const Mesh& m) {
 
 template <typename T>
 ApplyArgs<T> fused_args(Problem& P, const T* coords, const T* w, const T* p_old, T* p_new, T* ap, const T* r,
-                        const T* dinv, const T* plas = nullptr) {
+                        const T* dinv, const T* plas = nullptr, const float4* dinv4 = nullptr) {
   SolverWorkspace& ws = P.ws;
   ApplyArgs<T> a{};
   a.tv = P.mesh->tiles();
   a.N = P.N();
   a.coords = coords;
   if constexpr (std::is_same<T, float>::value) a.coords4 = P.mesh->d_coords32_aos4.get();
+  a.dinv4 = dinv4;
   a.w = w;
   a.plas = plas;
   a.tile_nodes = P.d_tile_nodes_bc.get();
@@ -493,6 +494,18 @@ ApplyArgs<T> fused_args(Problem& P, const T* coords, const T* w, const T* p_old,
 
 }  // namespace
 
+namespace {
+__global__ void k_pack4(int64_t N, const float* __restrict__ soa, float4* __restrict__ out) {
+  for (int64_t v = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; v < N; v += int64_t(gridDim.x) * blockDim.x)
+    out[v] = make_float4(soa[v], soa[N + v], soa[2 * N + v], 0.0f);
+}
+}  // namespace
+
+void launch_pack4(int64_t N, const float* soa, float4* out, cudaStream_t s) {
+  k_pack4<<<vec_grid(N), kVecThreads, 0, s>>>(N, soa, out);
+  PA_LAUNCHED();
+}
+
 void SolverWorkspace::ensure(int64_t n, int64_t C, int grid, bool mixed) {
   if (ndof != n) {
     x.resize(n); b.resize(n); r.resize(n); p0.resize(n); p1.resize(n); ap.resize(n); dinv.resize(n); t.resize(n);
@@ -503,6 +516,7 @@ void SolverWorkspace::ensure(int64_t n, int64_t C, int grid, bool mixed) {
   }
   if (mixed && r32.n != size_t(n)) {
     r32.resize(n); p32a.resize(n); p32b.resize(n); ap32.resize(n); dinv32.resize(n); dx32.resize(n); w32.resize(C);
+    dinv4.resize(n / 3); ones4.resize(n / 3);
   }
   if (partials.n < size_t(3 * grid + 64)) partials.resize(3 * grid + 64);  // up to 3 per block
   if (counters.n < 4) {
@@ -525,15 +539,15 @@ struct CgGraph {
     if (graph) cudaGraphDestroy(graph);
   }
   void capture(Problem& P, const T* coords, const T* w, T* pa, T* pb, T* ap, T* r, const T* dinv, X* x, int chunk_,
-               const T* plas = nullptr) {
+               const T* plas = nullptr, const float4* dinv4 = nullptr) {
     cudaStream_t s = P.stream;
     SolverWorkspace& ws = P.ws;
     const int64_t n = P.ndof();
     const int vg = vec_grid(n);
     const int ag = fused_apply_grid<T>(*P.mesh);
     chunk = chunk_ + (chunk_ % 2);
-    ApplyArgs<T> a_even = fused_args<T>(P, coords, w, pa, pb, ap, r, dinv, plas);  // reads pa, writes pb
-    ApplyArgs<T> a_odd = fused_args<T>(P, coords, w, pb, pa, ap, r, dinv, plas);   // reads pb, writes pa
+    ApplyArgs<T> a_even = fused_args<T>(P, coords, w, pa, pb, ap, r, dinv, plas, dinv4);  // reads pa, writes pb
+    ApplyArgs<T> a_odd = fused_args<T>(P, coords, w, pb, pa, ap, r, dinv, plas, dinv4);   // reads pb, writes pa
     PA_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < chunk; ++k) {
       launch_apply_kernel<T, 1>(*P.mesh, ag, s, k % 2 == 0 ? a_even : a_odd);
@@ -624,7 +638,8 @@ pa_status solve_operator(Problem& P, const SolveOperator& op, const double* b, d
     PA_CHECK(op.w32 != nullptr, "mixed precision needs FP32 weights");
     k_inv_diag<float><<<vg, kVecThreads, 0, s>>>(N, op.diag_aos, mask, ws.dinv32.get());
     PA_LAUNCHED();
-    launches += 1;
+    launch_pack4(N, ws.dinv32.get(), ws.dinv4.get(), s);
+    launches += 2;
   }
   // b' = mask(b - K x_D), x_D = Dirichlet values (held in p0 for the moment).
   double* bprime = ws.b.get();
@@ -676,7 +691,7 @@ pa_status solve_operator(Problem& P, const SolveOperator& op, const double* b, d
   CgGraph<float, float> g32;
   if (mixed)
     g32.capture(P, P.mesh->d_coords32_soa.get(), op.w32, ws.p32a.get(), ws.p32b.get(), ws.ap32.get(), ws.r32.get(),
-                ws.dinv32.get(), ws.dx32.get(), chunk, op.plas32);
+                ws.dinv32.get(), ws.dx32.get(), chunk, op.plas32, ws.dinv4.get());
   else
     g64.capture(P, P.mesh->d_coords_soa.get(), op.w64, ws.p0.get(), ws.p1.get(), ws.ap.get(), ws.r.get(),
                 ws.dinv.get(), ws.x.get(), chunk, op.plas64);
@@ -787,6 +802,7 @@ pa_status solve_fcg(Problem& P, const SolveOperator& op, LearnedPC& pc, const do
   pc_prepare_operator(pc, P, op.diag_aos, ws.dinv32.get(), s);
   k_fill_f32<<<vg, kVecThreads, 0, s>>>(n, 1.0f, ws.ones32.get());
   PA_LAUNCHED();
+  launch_pack4(N, ws.ones32.get(), ws.ones4.get(), s);
   launches += 3;
   // b' = mask(b - K x_D)
   double* bprime = ws.b.get();
@@ -833,9 +849,9 @@ pa_status solve_fcg(Problem& P, const SolveOperator& op, LearnedPC& pc, const do
   const int ag = fused_apply_grid<float>(*P.mesh);
   const float* coords32 = P.mesh->d_coords32_soa.get();
   ApplyArgs<float> a_even = fused_args<float>(P, coords32, op.w32, ws.p32a.get(), ws.p32b.get(), ws.ap32.get(),
-                                              ws.z32.get(), ws.ones32.get());
+                                              ws.z32.get(), ws.ones32.get(), nullptr, ws.ones4.get());
   ApplyArgs<float> a_odd = fused_args<float>(P, coords32, op.w32, ws.p32b.get(), ws.p32a.get(), ws.ap32.get(),
-                                             ws.z32.get(), ws.ones32.get());
+                                             ws.z32.get(), ws.ones32.get(), nullptr, ws.ones4.get());
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   PA_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -1046,6 +1062,7 @@ double time_cg_apply(Problem& P, const double* z, bool fp32, int reps) {
   launch_diag(P, ws.w64.get(), ws.t.get(), s);
   k_inv_diag<double><<<vec_grid(n), kVecThreads, 0, s>>>(P.N(), ws.t.get(), P.d_node_mask.get(), ws.dinv.get());
   k_inv_diag<float><<<vec_grid(n), kVecThreads, 0, s>>>(P.N(), ws.t.get(), P.d_node_mask.get(), ws.dinv32.get());
+  launch_pack4(P.N(), ws.dinv32.get(), ws.dinv4.get(), s);
   PA_LAUNCHED();
   PcgScalars init{};
   init.beta = 0.5;
@@ -1061,9 +1078,9 @@ double time_cg_apply(Problem& P, const double* z, bool fp32, int reps) {
     PA_CUDA(cudaMemsetAsync(ws.p32b.get(), 0, sizeof(float) * n, s));
     PA_CUDA(cudaMemsetAsync(ws.ap32.get(), 0, sizeof(float) * n, s));
     ApplyArgs<float> a = fused_args<float>(P, P.mesh->d_coords32_soa.get(), ws.w32.get(), ws.p32a.get(), ws.p32b.get(),
-                                           ws.ap32.get(), ws.r32.get(), ws.dinv32.get());
+                                           ws.ap32.get(), ws.r32.get(), ws.dinv32.get(), nullptr, ws.dinv4.get());
     ApplyArgs<float> b = fused_args<float>(P, P.mesh->d_coords32_soa.get(), ws.w32.get(), ws.p32b.get(), ws.p32a.get(),
-                                           ws.ap32.get(), ws.r32.get(), ws.dinv32.get());
+                                           ws.ap32.get(), ws.r32.get(), ws.dinv32.get(), nullptr, ws.dinv4.get());
     launch_apply_kernel<float, 1>(*P.mesh, ag, s, a);  // warm
     PA_CUDA(cudaEventRecord(P.ev0, s));
     for (int i = 0; i < reps; ++i) launch_apply_kernel<float, 1>(*P.mesh, ag, s, i % 2 ? a : b);

@@ -43,6 +43,7 @@ struct ApplyArgs {
   int64_t N;                   // nodes (SoA stride)
   const T* coords;             // 3N, SoA
   const float4* coords4;       // FP32 PCG modes: N x (x, y, z, 0), one 16-byte gather per node (or null)
+  const float4* dinv4;         // FP32 PCG modes: D^-1 as N x (x, y, z, 0) (required there)
   const T* w;                  // C, SIMP weight per cell, internal order
   const T* plas;               // null (elastic) or 8 per cell, internal order: J2 tangent record
   Iso<T> iso;
@@ -226,7 +227,13 @@ struct TileSmem {
   static constexpr int kRawBufs = MODE >= 1 ? 2 : 1;
   Node4<T> xc[2][kTileNodes];             // coordinates + input (component 0), two buffers
   Node2<T> uu[2][kTileNodes];             // input components 1, 2
-  T raw[kRawBufs][9][kTileNodes];         // PCG: r, D^-1, p_old gathered for the tile
+  // PCG modes: r, D^-1, p_old gathered for the tile.  FP32 keeps D^-1 as one
+  // 16-byte record per node (dv) and only r and p_old in raw.
+  static constexpr bool kPackedD = sizeof(T) == 4 && MODE >= 1;
+  static constexpr int kRawRows = kPackedD ? 6 : 9;
+  static constexpr int kRowD = 3, kRowP = kPackedD ? 3 : 6;
+  T raw[kRawBufs][kRawRows][kTileNodes];
+  float4 dv[kPackedD ? 2 : 1][kPackedD ? kTileNodes : 1];
   T y[3][kTileNodes];                     // node sums of the current tile
   T w[2][6 * TILE];                       // penalty weights of the tile's cells
   uint4 rec[2][TILE];                     // cluster node ids
@@ -289,9 +296,11 @@ __device__ __forceinline__ void prefetch_data(const ApplyArgs<T>& a, TileSmem<T,
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         cp_async<sizeof(T)>(&S.raw[b][d][i], &a.r[d * N + g]);
-        cp_async<sizeof(T)>(&S.raw[b][3 + d][i], &a.dinv[d * N + g]);
-        cp_async<sizeof(T)>(&S.raw[b][6 + d][i], &a.x[d * N + g]);
+        if constexpr (!TileSmem<T, MODE, TILE>::kPackedD)
+          cp_async<sizeof(T)>(&S.raw[b][TileSmem<T, MODE, TILE>::kRowD + d][i], &a.dinv[d * N + g]);
+        cp_async<sizeof(T)>(&S.raw[b][TileSmem<T, MODE, TILE>::kRowP + d][i], &a.x[d * N + g]);
       }
+      if constexpr (TileSmem<T, MODE, TILE>::kPackedD) cp_async<16>(&S.dv[b][i], &a.dinv4[g]);
     }
   }
   const int c0 = S.meta[b][5], nc = S.meta[b][6];
@@ -347,7 +356,7 @@ __global__ void __launch_bounds__(TILE, (sizeof(T) == 4 ? 640 / TILE : 1)) k_app
           const int64_t g = int64_t(f & kNodeIdMask);
           if ((f & kOwner) && g < a.N) {
 #pragma unroll
-            for (int d = 0; d < 3; ++d) a.p_new[d * a.N + g] = S.raw[b][6 + d][i];
+            for (int d = 0; d < 3; ++d) a.p_new[d * a.N + g] = S.raw[b][TileSmem<T, MODE, TILE>::kRowP + d][i];
           }
         }
       }
@@ -366,10 +375,20 @@ __global__ void __launch_bounds__(TILE, (sizeof(T) == 4 ? 640 / TILE : 1)) k_app
           if (mk & 4u) S.uu[b][i].u2 = T(0);
         }
       } else {
-        T v[3];
+        T v[3], dinv[3];
+        if constexpr (TileSmem<T, MODE, TILE>::kPackedD) {
+          const float4 q = S.dv[b][i];
+          dinv[0] = q.x;
+          dinv[1] = q.y;
+          dinv[2] = q.z;
+        } else {
+#pragma unroll
+          for (int d = 0; d < 3; ++d) dinv[d] = S.raw[b][TileSmem<T, MODE, TILE>::kRowD + d][i];
+        }
 #pragma unroll
         for (int d = 0; d < 3; ++d)
-          v[d] = (mk >> d) & 1 ? T(0) : S.raw[b][3 + d][i] * S.raw[b][d][i] + beta * S.raw[b][6 + d][i];
+          v[d] = (mk >> d) & 1 ? T(0)
+                               : dinv[d] * S.raw[b][d][i] + beta * S.raw[b][TileSmem<T, MODE, TILE>::kRowP + d][i];
         S.xc[b][i].u0 = v[0];
         S.uu[b][i].u1 = v[1];
         S.uu[b][i].u2 = v[2];
@@ -574,6 +593,8 @@ int apply_kernel_setup(const Mesh& m) {
 // Launch (also inside stream capture) the instance matching the mesh's tile size.
 template <typename T, int MODE>
 void launch_apply_kernel(const Mesh& m, int grid, cudaStream_t s, const ApplyArgs<T>& a) {
+  if (sizeof(T) == 4 && MODE >= 1 && a.dinv4 == nullptr)
+    throw Error(PA_ERR_INVALID_ARG, "FP32 fused apply without the packed D^-1");
   switch (m.tile_clusters) {
     case 64: k_apply_tiled<T, MODE, 64><<<grid, 64, tile_smem_bytes<T, MODE, 64>(), s>>>(a); break;
     case 128: k_apply_tiled<T, MODE, 128><<<grid, 128, tile_smem_bytes<T, MODE, 128>(), s>>>(a); break;
