@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--profile-kernel", action="store_true",
                     help="only build the workload and time the fused CG kernel (for ncu captures)")
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--per-tet-geometry", action="store_true",
+                    help="FP32 kernels recompute the tet geometry instead of using the box's hex geometry table")
     ap.add_argument("--newton-tol", type=float, default=1e-8, help="J2: relative Newton tolerance per load step")
     ap.add_argument("--boxes", type=int, default=64, help="batched: number of boxes")
     ap.add_argument("--workload", default="cantilever", choices=["cantilever", "j2", "learned", "batched"],
@@ -310,9 +312,9 @@ def profile_kernel(args):
     from platoanalyze_b200.workloads import cantilever, cell_density
     dims = dims_of(args.dims)
     torch.cuda.set_device(0)
-    mesh, prob, faces, dofs = cantilever(dims)
+    mesh, prob, faces, dofs = cantilever(dims, uniform_geometry=not args.per_tet_geometry)
     z = torch.tensor(cell_density(dims, SEED, kind="smoothed", sigma=3.0, lo=0.01, hi=1.0), device="cuda")
-    out = {"dims": dims, "tiles": mesh.num_tiles}
+    out = {"dims": dims, "tiles": mesh.num_tiles, "uniform_geometry": mesh.uniform_geometry}
     for prec, name in ((1, "fp32"), (0, "fp64")):
         ms, nb = ct.c_double(), ct.c_int64()
         _abi.check(_abi.load().pa_time_cg_apply(prob._h, ct.c_void_p(z.data_ptr()), prec, args.reps, ct.byref(ms),
@@ -342,7 +344,7 @@ def run_ours(args):
     ndof = 3 * N
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    mesh, prob, faces, dofs = cantilever(dims, stream=stream.cuda_stream)
+    mesh, prob, faces, dofs = cantilever(dims, stream=stream.cuda_stream, uniform_geometry=not args.per_tet_geometry)
     z_host = cell_density(dims, SEED + rank, kind="smoothed", sigma=3.0, lo=0.01, hi=1.0)
     z = torch.tensor(z_host, device="cuda")
     tile, tile_ms = prob.autotune_tiles(z)  # tile size of the fused kernel, before any timing
@@ -428,6 +430,7 @@ def run_ours(args):
                                f"Problem::solution to relres {args.rel_tol:g}",
                    "cells": C, "nodes": N, "dofs": ndof, "method": args.method, "parallelism": f"replicas x{world}",
                    "tile_clusters": tile, "autotune_ms_per_apply": tile_ms,
+                   "geometry": "hex geometry table (uniform hexes)" if mesh.uniform_geometry else "per tet",
                    "l2": "256 MB buffer written between timed steps"},
         "solve_s": max_ms / args.steps * 1e-3, "iterations": iters, "fp64_solve_s": st64["seconds"],
         "fp64_iterations": st64["iterations"], "compliance_rel_err_vs_fp64": abs(f_mixed - f_fp64) / abs(f_fp64),

@@ -90,6 +90,18 @@ pa_status pa_mesh_graph(const pa_mesh* mesh, int32_t* rowmap, int32_t* cols);
  * gradient_z then fill entries in that order. */
 pa_status pa_mesh_set_graph(pa_mesh* mesh, const int32_t* rowmap, const int32_t* cols, int64_t num_blocks);
 
+/* Uniform hex geometry.  When every cell belongs to a six-tet hex and all
+ * hexes are translates of one another (a structured voxel grid, any hex
+ * shape), the FP32 matrix-free kernels take each template tet's shape
+ * gradients and volume from a per-mesh table computed once in FP64 instead of
+ * recomputing them per tet from gathered coordinates (no reference
+ * counterpart: the reference recomputes them per cell,
+ * src/ImplicitFunctors.hpp:165-217).  enable = 1 (the default) uses the table
+ * when the mesh qualifies, 0 forces the per-tet geometry, -1 only queries;
+ * *active (may be NULL) receives 1 when the table is in use.  Changing it is
+ * allowed only before problems are created on the mesh. */
+pa_status pa_mesh_uniform_geometry(pa_mesh* mesh, int32_t enable, int32_t* active);
+
 /* Boundary faces (triangles, 3 node ids each) lying on the plane
  * coord[axis] == value.  Call with faces == NULL to get the count. */
 pa_status pa_mesh_boundary_faces(const pa_mesh* mesh, int32_t axis, double value, int32_t* faces,

@@ -121,6 +121,21 @@ class Mesh:
         _abi.check(self._lib.pa_mesh_sizes(self._h, ct.byref(C), ct.byref(N), ct.byref(B), ct.byref(T)))
         self.num_tiles = T.value
 
+    @property
+    def uniform_geometry(self):
+        """True when the FP32 kernels use the per-mesh hex geometry table
+        (every hex a translate of the first)."""
+        a = ct.c_int32()
+        _abi.check(self._lib.pa_mesh_uniform_geometry(self._h, -1, ct.byref(a)))
+        return bool(a.value)
+
+    def set_uniform_geometry(self, enable):
+        """Allow (True, the default) or forbid the hex geometry table; before
+        any Problem on the mesh.  Returns whether the table is in use."""
+        a = ct.c_int32()
+        _abi.check(self._lib.pa_mesh_uniform_geometry(self._h, 1 if enable else 0, ct.byref(a)))
+        return bool(a.value)
+
     def boundary_faces(self, axis, value):
         n = ct.c_int64()
         _abi.check(self._lib.pa_mesh_boundary_faces(self._h, axis, float(value), None, ct.byref(n)))

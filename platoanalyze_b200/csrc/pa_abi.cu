@@ -976,6 +976,20 @@ pa_status pa_mesh_set_parts(pa_mesh* mesh, int32_t num_parts, const int64_t* nod
   });
 }
 
+pa_status pa_mesh_uniform_geometry(pa_mesh* mesh, int32_t enable, int32_t* active) {
+  return guard([&] {
+    PA_CHECK(mesh, "null pa_mesh");
+    pa::Mesh& m = mesh->m;
+    if (enable >= 0 && bool(enable) != m.allow_uniform_geometry) {
+      PA_CHECK(m.live_problems == 0, "change the geometry mode before creating problems on the mesh");
+      PA_CUDA(cudaSetDevice(m.device));
+      m.allow_uniform_geometry = enable != 0;
+      pa::mesh_rebuild_tiles(m);
+    }
+    if (active) *active = m.uniform_hex ? 1 : 0;
+  });
+}
+
 pa_status pa_problem_part_stats(pa_problem* problem, int32_t* iterations, double* rel_residuals) {
   return guard([&] {
     Problem& P = prob(problem);

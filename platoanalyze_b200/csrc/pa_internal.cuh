@@ -90,6 +90,17 @@ struct TileView {
   int32_t num_tiles;
 };
 
+// Geometry shared by every hex cluster of a mesh whose hexes are translates
+// of one another (a structured voxel grid): per template tet k the rows of
+// det * J^-1 (h[k][0..2] for the tet's vertices 0, a, b in the tile kernel's
+// relative form) and s[k] = 1 / (6 |det|).  The tile kernel reads it from its
+// parameter block instead of recomputing the geometry per tet.
+template <typename T>
+struct HexGeo {
+  T h[6][9];
+  T s[6];
+};
+
 struct Mesh {
   int device = 0;
   int64_t C = 0, N = 0, B = 0, T = 0;
@@ -105,6 +116,13 @@ struct Mesh {
   DevBuf<int32_t> d_rowmap, d_cols;
   DevBuf<int32_t> d_cell_entry;  // C*16 CRS block index of (a,b) pairs
   int64_t num_clusters = 0, num_hex = 0;
+  // every cluster a hex and every hex a translate of the first (edge vectors
+  // equal to 1e-9 of the hex size): the FP32 tile kernel then takes the
+  // geometry from geo32 and gathers no coordinates
+  bool uniform_hex = false;
+  bool allow_uniform_geometry = true;  // false: always the per-tet geometry
+  HexGeo<double> geo64{};
+  HexGeo<float> geo32{};
   int tile_clusters = 128;  // clusters per tile (threads per CTA); a tile touches <= 2x as many nodes
   DevBuf<int32_t> d_tile_cluster_start, d_tile_cell_start, d_tile_hex_count, d_tile_node_start, d_cell_perm;
   DevBuf<int32_t> d_cell_iperm;  // user -> internal cell id

@@ -109,6 +109,60 @@ bool match_hex(const Mesh& m, int64_t c0, Cluster& out) {
   return true;
 }
 
+// Uniform hex geometry: every cluster is a hex and each hex's edge vectors
+// E_s = x_slot(s) - x_slot(7) (s = 0..6) equal the first hex's to 1e-9 of its
+// largest edge (FP64 rounding of generated coordinates stays far below that).
+// Then the per-tet rows of det * J^-1 and 1 / (6 |det|) are the same for all
+// hexes; they are computed once here in FP64, in the tile kernel's relative
+// form (template tet k = slots 0, ring(k), ring(k+1), 7).
+void detect_uniform_hex(Mesh& m, const std::vector<Cluster>& cl) {
+  m.uniform_hex = false;
+  if (cl.empty()) return;
+  for (const Cluster& k : cl)
+    if (!k.hex) return;
+  auto edges = [&](const Cluster& k, double (&E)[7][3]) {
+    const int32_t v7 = k.nodes[7];
+    for (int s = 0; s < 7; ++s)
+      for (int d = 0; d < 3; ++d) E[s][d] = m.coords[3 * int64_t(k.nodes[s]) + d] - m.coords[3 * int64_t(v7) + d];
+  };
+  double E0[7][3];
+  edges(cl[0], E0);
+  double size = 0.0;
+  for (int s = 0; s < 7; ++s)
+    for (int d = 0; d < 3; ++d) size = std::max(size, std::fabs(E0[s][d]));
+  if (!(size > 0.0)) return;
+  const double tol = 1e-9 * size;
+  for (const Cluster& k : cl) {
+    double E[7][3];
+    edges(k, E);
+    for (int s = 0; s < 7; ++s)
+      for (int d = 0; d < 3; ++d)
+        if (std::fabs(E[s][d] - E0[s][d]) > tol) return;
+  }
+  static const int ring[7] = {3, 2, 6, 4, 5, 1, 3};
+  auto cross = [](const double* a, const double* b, double* c) {
+    c[0] = a[1] * b[2] - a[2] * b[1];
+    c[1] = a[2] * b[0] - a[0] * b[2];
+    c[2] = a[0] * b[1] - a[1] * b[0];
+  };
+  HexGeo<double> g{};
+  for (int k = 0; k < 6; ++k) {
+    const double *e0 = E0[0], *ea = E0[ring[k]], *eb = E0[ring[k + 1]];
+    cross(ea, eb, &g.h[k][0]);  // h0 = ea x eb
+    cross(eb, e0, &g.h[k][3]);  // h1 = eb x e0
+    cross(e0, ea, &g.h[k][6]);  // h2 = e0 x ea
+    const double det = e0[0] * g.h[k][0] + e0[1] * g.h[k][1] + e0[2] * g.h[k][2];
+    if (!(std::fabs(det) > 1e-12 * size * size * size)) return;  // degenerate tet: keep the general path
+    g.s[k] = 1.0 / (6.0 * std::fabs(det));
+  }
+  m.geo64 = g;
+  for (int k = 0; k < 6; ++k) {
+    for (int i = 0; i < 9; ++i) m.geo32.h[k][i] = float(g.h[k][i]);
+    m.geo32.s[k] = float(g.s[k]);
+  }
+  m.uniform_hex = true;
+}
+
 // Clusters (hex groups of six consecutive cells, else single cells), ordered
 // along the Morton (Z-order) curve of their centroids, packed greedily into
 // tiles of <= tile_clusters clusters and <= 2 tile_clusters nodes.
@@ -130,6 +184,8 @@ void build_tiles(Mesh& m) {
     cl.push_back(s);
     ++c;
   }
+  detect_uniform_hex(m, cl);
+  if (!m.allow_uniform_geometry) m.uniform_hex = false;
   // part of every cluster (all its nodes must lie in one part)
   std::vector<uint16_t> npart;
   if (m.num_parts > 1) {

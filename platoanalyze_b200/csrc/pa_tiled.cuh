@@ -47,6 +47,7 @@ struct ApplyArgs {
   const T* w;                  // C, SIMP weight per cell, internal order
   const T* plas;               // null (elastic) or 8 per cell, internal order: J2 tangent record
   Iso<T> iso;
+  HexGeo<T> geo;               // uniform hex geometry (filled by the launcher when the mesh has it)
   const T* x;                  // plain: input vector; pcg: p_old
   T* y;                        // output, zero on entry
   // PCG fusion (mode 1)
@@ -127,17 +128,13 @@ __device__ __forceinline__ T tet_apply(const Iso<T>& iso, T w, const T (&xc)[4][
 //   sigma = w [kappa tr(eps) 1 + 2 mu (1 - theta1) dev(eps) - 2 mu (theta2 - theta1) (n : eps) n],
 // theta1 = sqrt(6) mu_p dgamma / |eta_trial|, theta2 = 3 mu_p / (3 mu_p + H_iso,p + H_kin,p)
 // (zero for an elastic cell).
+//
+// tet_core is the part after the geometry: rows h0, h1, h2 and the scale
+// sc = w / (6 |det|) given.
 template <typename T>
-__device__ __forceinline__ T tet_rel(const Iso<T>& iso, T w, const T (&e0)[3], const T (&ea)[3], const T (&eb)[3],
-                                     const T (&h1)[3], const T (&h2)[3], const T (&d0)[3], const T (&da)[3],
-                                     const T (&db)[3], T (&r0)[3], T (&ra)[3], T (&rb)[3],
-                                     const T* __restrict__ pl = nullptr) {
-  T h0[3];
-  h0[0] = ea[1] * eb[2] - ea[2] * eb[1];
-  h0[1] = ea[2] * eb[0] - ea[0] * eb[2];
-  h0[2] = ea[0] * eb[1] - ea[1] * eb[0];
-  const T det = e0[0] * h0[0] + e0[1] * h0[1] + e0[2] * h0[2];
-  const T sc = w / (T(6) * fabs(det));
+__device__ __forceinline__ T tet_core(const Iso<T>& iso, T sc, const T (&h0)[3], const T (&h1)[3], const T (&h2)[3],
+                                      const T (&d0)[3], const T (&da)[3], const T (&db)[3], T (&r0)[3], T (&ra)[3],
+                                      T (&rb)[3], const T* __restrict__ pl) {
   // eps_u = sum_n h_n (x) du_n
   const T exx = h0[0] * d0[0] + h1[0] * da[0] + h2[0] * db[0];
   const T eyy = h0[1] * d0[1] + h1[1] * da[1] + h2[1] * db[1];
@@ -182,6 +179,20 @@ __device__ __forceinline__ T tet_rel(const Iso<T>& iso, T w, const T (&e0)[3], c
 }
 
 template <typename T>
+__device__ __forceinline__ T tet_rel(const Iso<T>& iso, T w, const T (&e0)[3], const T (&ea)[3], const T (&eb)[3],
+                                     const T (&h1)[3], const T (&h2)[3], const T (&d0)[3], const T (&da)[3],
+                                     const T (&db)[3], T (&r0)[3], T (&ra)[3], T (&rb)[3],
+                                     const T* __restrict__ pl = nullptr) {
+  T h0[3];
+  h0[0] = ea[1] * eb[2] - ea[2] * eb[1];
+  h0[1] = ea[2] * eb[0] - ea[0] * eb[2];
+  h0[2] = ea[0] * eb[1] - ea[1] * eb[0];
+  const T det = e0[0] * h0[0] + e0[1] * h0[1] + e0[2] * h0[2];
+  const T sc = w / (T(6) * fabs(det));
+  return tet_core(iso, sc, h0, h1, h2, d0, da, db, r0, ra, rb, pl);
+}
+
+template <typename T>
 __device__ __forceinline__ void cross3(const T (&a)[3], const T (&b)[3], T (&c)[3]) {
   c[0] = a[1] * b[2] - a[2] * b[1];
   c[1] = a[2] * b[0] - a[0] * b[2];
@@ -220,13 +231,14 @@ struct alignas(2 * sizeof(T)) Node2 {
 };
 
 // Shared-memory layout of one CTA (dynamic shared memory); TILE clusters
-// (threads) and up to 2 * TILE nodes per tile.
-template <typename T, int MODE, int TILE>
+// (threads) and up to 2 * TILE nodes per tile.  GEO (uniform hex geometry):
+// xc holds the input vector (u0, u1, u2, 0) and uu is not used.
+template <typename T, int MODE, int TILE, bool GEO = false>
 struct TileSmem {
   static constexpr int kTileNodes = 2 * TILE;
   static constexpr int kRawBufs = MODE >= 1 ? 2 : 1;
   Node4<T> xc[2][kTileNodes];             // coordinates + input (component 0), two buffers
-  Node2<T> uu[2][kTileNodes];             // input components 1, 2
+  Node2<T> uu[2][GEO ? 1 : kTileNodes];   // input components 1, 2
   // PCG modes: r, D^-1, p_old gathered for the tile.  FP32 keeps D^-1 as one
   // 16-byte record per node (dv) and only r and p_old in raw.
   static constexpr bool kPackedD = sizeof(T) == 4 && MODE >= 1;
@@ -242,14 +254,15 @@ struct TileSmem {
   double red[32];
 };
 
-template <typename T, int MODE, int TILE>
+template <typename T, int MODE, int TILE, bool GEO>
 constexpr size_t tile_smem_bytes() {
-  return sizeof(TileSmem<T, MODE, TILE>);
+  return sizeof(TileSmem<T, MODE, TILE, GEO>);
 }
 
 // Issue the loads of tile `tile`'s header, node ids and cluster records (buffer b).
-template <typename T, int MODE, int TILE>
-__device__ __forceinline__ void prefetch_ids(const ApplyArgs<T>& a, TileSmem<T, MODE, TILE>& S, int tile, int b) {
+template <typename T, int MODE, int TILE, bool GEO>
+__device__ __forceinline__ void prefetch_ids(const ApplyArgs<T>& a, TileSmem<T, MODE, TILE, GEO>& S, int tile,
+                                             int b) {
   const int n0 = a.tv.tile_node_start[tile], nn = a.tv.tile_node_start[tile + 1] - n0;
   const int k0 = a.tv.tile_cluster_start[tile], nk = a.tv.tile_cluster_start[tile + 1] - k0;
   if (threadIdx.x == 0) {
@@ -268,13 +281,15 @@ __device__ __forceinline__ void prefetch_ids(const ApplyArgs<T>& a, TileSmem<T, 
 }
 
 // Issue the gathers of the node data and weights of the tile whose ids sit in buffer b.
-template <typename T, int MODE, int TILE>
-__device__ __forceinline__ void prefetch_data(const ApplyArgs<T>& a, TileSmem<T, MODE, TILE>& S, int b) {
+// GEO (uniform hex geometry): no coordinates; the node record holds the
+// input vector (u0, u1, u2, 0).
+template <typename T, int MODE, int TILE, bool GEO>
+__device__ __forceinline__ void prefetch_data(const ApplyArgs<T>& a, TileSmem<T, MODE, TILE, GEO>& S, int b) {
   const int nn = S.meta[b][1];
   const int64_t N = a.N;
   for (int i = threadIdx.x; i < nn; i += blockDim.x) {
     const int64_t g = int64_t(S.ids[b][i] & kNodeIdMask);
-    bool packed = false;
+    bool packed = GEO;
     if constexpr (sizeof(T) == 4 && MODE >= 1) {
       // (x, y, z, 0) in one copy; the fourth slot is the input component 0,
       // which the PCG modes write after this copy has landed
@@ -288,7 +303,11 @@ __device__ __forceinline__ void prefetch_data(const ApplyArgs<T>& a, TileSmem<T,
       cp_async<sizeof(T)>(&S.xc[b][i].y, &a.coords[N + g]);
       cp_async<sizeof(T)>(&S.xc[b][i].z, &a.coords[2 * N + g]);
     }
-    if constexpr (MODE == 0) {
+    if constexpr (MODE == 0 && GEO) {
+      cp_async<sizeof(T)>(&S.xc[b][i].x, &a.x[g]);
+      cp_async<sizeof(T)>(&S.xc[b][i].y, &a.x[N + g]);
+      cp_async<sizeof(T)>(&S.xc[b][i].z, &a.x[2 * N + g]);
+    } else if constexpr (MODE == 0) {
       cp_async<sizeof(T)>(&S.xc[b][i].u0, &a.x[g]);
       cp_async<sizeof(T)>(&S.uu[b][i].u1, &a.x[N + g]);
       cp_async<sizeof(T)>(&S.uu[b][i].u2, &a.x[2 * N + g]);
@@ -310,10 +329,10 @@ __device__ __forceinline__ void prefetch_data(const ApplyArgs<T>& a, TileSmem<T,
 
 // FP32 instances ask for 640 resident threads per SM (<= 96 registers, 20
 // warps); FP64 instances are register-bound at one or two CTAs.
-template <typename T, int MODE, int TILE>
+template <typename T, int MODE, int TILE, bool GEO>
 __global__ void __launch_bounds__(TILE, (sizeof(T) == 4 ? 640 / TILE : 1)) k_apply_tiled(ApplyArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  TileSmem<T, MODE, TILE>& S = *reinterpret_cast<TileSmem<T, MODE, TILE>*>(smem_raw);
+  TileSmem<T, MODE, TILE, GEO>& S = *reinterpret_cast<TileSmem<T, MODE, TILE, GEO>*>(smem_raw);
 
   T beta = T(0);
   if (MODE >= 1) {
@@ -329,7 +348,7 @@ __global__ void __launch_bounds__(TILE, (sizeof(T) == 4 ? 640 / TILE : 1)) k_app
     prefetch_ids(a, S, tile, 0);
     cp_async_wait_all();
     __syncthreads();
-    prefetch_data(a, S, 0);
+    prefetch_data<T, MODE, TILE, GEO>(a, S, 0);
     if (tile + stride < a.tv.num_tiles) prefetch_ids(a, S, tile + stride, 1);
   }
 
@@ -338,7 +357,7 @@ __global__ void __launch_bounds__(TILE, (sizeof(T) == 4 ? 640 / TILE : 1)) k_app
     cp_async_wait_all();  // data of this tile, ids of the next
     __syncthreads();
     const bool has_next = tile + stride < a.tv.num_tiles;
-    if (has_next) prefetch_data(a, S, b ^ 1);
+    if (has_next) prefetch_data<T, MODE, TILE, GEO>(a, S, b ^ 1);
     // batched mode: this tile's part, its beta, and whether it has converged
     int part = 0;
     bool skip = false;
@@ -368,7 +387,13 @@ __global__ void __launch_bounds__(TILE, (sizeof(T) == 4 ? 640 / TILE : 1)) k_app
     for (int i = threadIdx.x; i < nn; i += blockDim.x) {
       const uint32_t f = S.ids[b][i];
       const uint32_t mk = (f >> kMaskShift) & 7u;
-      if constexpr (MODE == 0) {
+      if constexpr (MODE == 0 && GEO) {
+        if (mk) {
+          if (mk & 1u) S.xc[b][i].x = T(0);
+          if (mk & 2u) S.xc[b][i].y = T(0);
+          if (mk & 4u) S.xc[b][i].z = T(0);
+        }
+      } else if constexpr (MODE == 0) {
         if (mk) {
           if (mk & 1u) S.xc[b][i].u0 = T(0);
           if (mk & 2u) S.uu[b][i].u1 = T(0);
@@ -389,9 +414,13 @@ __global__ void __launch_bounds__(TILE, (sizeof(T) == 4 ? 640 / TILE : 1)) k_app
         for (int d = 0; d < 3; ++d)
           v[d] = (mk >> d) & 1 ? T(0)
                                : dinv[d] * S.raw[b][d][i] + beta * S.raw[b][TileSmem<T, MODE, TILE>::kRowP + d][i];
-        S.xc[b][i].u0 = v[0];
-        S.uu[b][i].u1 = v[1];
-        S.uu[b][i].u2 = v[2];
+        if constexpr (GEO) {
+          S.xc[b][i] = Node4<T>{v[0], v[1], v[2], T(0)};
+        } else {
+          S.xc[b][i].u0 = v[0];
+          S.uu[b][i].u1 = v[1];
+          S.uu[b][i].u2 = v[2];
+        }
         if (f & kOwner) {
           const int64_t g = int64_t(f & kNodeIdMask);
 #pragma unroll
@@ -412,8 +441,39 @@ __global__ void __launch_bounds__(TILE, (sizeof(T) == 4 ? 640 / TILE : 1)) k_app
                          int(q.z & 0xffff), int(q.z >> 16), int(q.w & 0xffff), int(q.w >> 16)};
       if (t < nhex) {
         const T* wv = &S.w[b][6 * t];
+        T D[7][3], Y[7][3];
+        if constexpr (GEO) {
+          // input differences relative to slot 7; geometry from the table
+          const Node4<T> q7 = S.xc[b][ln[7]];
+#pragma unroll
+          for (int s = 0; s < 7; ++s) {
+            const Node4<T> q4 = S.xc[b][ln[s]];
+            D[s][0] = q4.x - q7.x;
+            D[s][1] = q4.y - q7.y;
+            D[s][2] = q4.z - q7.z;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) Y[s][d] = T(0);
+          }
+#pragma unroll
+          for (int k = 0; k < 6; ++k) {
+            const int sa = hex_ring(k), sb = hex_ring(k + 1);
+            const T h0[3] = {a.geo.h[k][0], a.geo.h[k][1], a.geo.h[k][2]};
+            const T h1[3] = {a.geo.h[k][3], a.geo.h[k][4], a.geo.h[k][5]};
+            const T h2[3] = {a.geo.h[k][6], a.geo.h[k][7], a.geo.h[k][8]};
+            T r0[3], ra[3], rb[3];
+            const T* pl = a.plas ? a.plas + 8 * (int64_t(S.meta[b][5]) + 6 * t + k) : nullptr;
+            const T en = tet_core(a.iso, wv[k] * a.geo.s[k], h0, h1, h2, D[0], D[sa], D[sb], r0, ra, rb, pl);
+            if (MODE >= 1) pap += double(en);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+              Y[0][d] += r0[d];
+              Y[sa][d] += ra[d];
+              Y[sb][d] += rb[d];
+            }
+          }
+        } else {
         // edge vectors and input differences relative to slot 7 (the diagonal end)
-        T E[7][3], D[7][3], Y[7][3];
+        T E[7][3];
         {
           const Node4<T> q7 = S.xc[b][ln[7]];
           const Node2<T> p7 = S.uu[b][ln[7]];
@@ -451,6 +511,7 @@ __global__ void __launch_bounds__(TILE, (sizeof(T) == 4 ? 640 / TILE : 1)) k_app
             Y[sb][d] += rb[d];
           }
         }
+        }  // !GEO
         // slot 7 closes each tet's partition of unity: Y7 = -(Y0 + ... + Y6)
         T Y7[3] = {T(0), T(0), T(0)};
 #pragma unroll
@@ -463,8 +524,9 @@ __global__ void __launch_bounds__(TILE, (sizeof(T) == 4 ? 640 / TILE : 1)) k_app
           for (int d = 0; d < 3; ++d) atomicAdd(&S.y[d][ln[s]], Y[s][d]);
 #pragma unroll
         for (int d = 0; d < 3; ++d) atomicAdd(&S.y[d][ln[7]], Y7[d]);
-      } else {
+      } else if constexpr (!GEO) {
         // single tets follow the hexes: cell index = 6 * nhex + (t - nhex)
+        // (a mesh with uniform hex geometry has none)
         T e[3][3], du[3][3], h1[3], h2[3], r[3][3];
         const Node4<T> q3 = S.xc[b][ln[3]];
         const Node2<T> p3 = S.uu[b][ln[3]];
@@ -571,35 +633,67 @@ __global__ void __launch_bounds__(TILE, (sizeof(T) == 4 ? 640 / TILE : 1)) k_app
 
 // Configure dynamic shared memory of one instance; returns the persistent
 // grid size (resident CTAs per SM x SMs, capped by the tile count).
-template <typename T, int MODE, int TILE>
+template <typename T, int MODE, int TILE, bool GEO>
 int apply_grid_for(int num_tiles) {
-  const size_t smem = tile_smem_bytes<T, MODE, TILE>();
-  PA_CUDA(cudaFuncSetAttribute(k_apply_tiled<T, MODE, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  const size_t smem = tile_smem_bytes<T, MODE, TILE, GEO>();
+  PA_CUDA(cudaFuncSetAttribute(k_apply_tiled<T, MODE, TILE, GEO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               int(smem)));
   int blocks = 0;
-  PA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_apply_tiled<T, MODE, TILE>, TILE, smem));
+  PA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_apply_tiled<T, MODE, TILE, GEO>, TILE, smem));
   const int grid = std::min(std::max(1, blocks) * num_sms(), num_tiles);
   return std::max(grid, 1);
 }
 
-template <typename T, int MODE>
-int apply_kernel_setup(const Mesh& m) {
+// The FP32 instances take the uniform-geometry form when the mesh has it; FP64
+// always recomputes the geometry per tet (its parity is against the oracle's
+// per-cell arithmetic).
+template <typename T>
+bool use_uniform_geometry(const Mesh& m) {
+  return sizeof(T) == 4 && m.uniform_hex;
+}
+
+template <typename T, int MODE, bool GEO>
+int apply_kernel_setup_geo(const Mesh& m) {
   switch (m.tile_clusters) {
-    case 64: return apply_grid_for<T, MODE, 64>(int(m.T));
-    case 128: return apply_grid_for<T, MODE, 128>(int(m.T));
-    default: return apply_grid_for<T, MODE, 256>(int(m.T));
+    case 64: return apply_grid_for<T, MODE, 64, GEO>(int(m.T));
+    case 128: return apply_grid_for<T, MODE, 128, GEO>(int(m.T));
+    default: return apply_grid_for<T, MODE, 256, GEO>(int(m.T));
   }
 }
 
-// Launch (also inside stream capture) the instance matching the mesh's tile size.
+template <typename T, int MODE>
+int apply_kernel_setup(const Mesh& m) {
+  if constexpr (sizeof(T) == 4) {
+    if (use_uniform_geometry<T>(m)) return apply_kernel_setup_geo<T, MODE, true>(m);
+  }
+  return apply_kernel_setup_geo<T, MODE, false>(m);
+}
+
+template <typename T, int MODE, bool GEO>
+void launch_apply_geo(const Mesh& m, int grid, cudaStream_t s, const ApplyArgs<T>& a) {
+  switch (m.tile_clusters) {
+    case 64: k_apply_tiled<T, MODE, 64, GEO><<<grid, 64, tile_smem_bytes<T, MODE, 64, GEO>(), s>>>(a); break;
+    case 128: k_apply_tiled<T, MODE, 128, GEO><<<grid, 128, tile_smem_bytes<T, MODE, 128, GEO>(), s>>>(a); break;
+    default: k_apply_tiled<T, MODE, 256, GEO><<<grid, 256, tile_smem_bytes<T, MODE, 256, GEO>(), s>>>(a); break;
+  }
+}
+
+// Launch (also inside stream capture) the instance matching the mesh's tile
+// size and geometry; the grid must come from apply_kernel_setup<T, MODE> of
+// the same mesh state.
 template <typename T, int MODE>
 void launch_apply_kernel(const Mesh& m, int grid, cudaStream_t s, const ApplyArgs<T>& a) {
   if (sizeof(T) == 4 && MODE >= 1 && a.dinv4 == nullptr)
     throw Error(PA_ERR_INVALID_ARG, "FP32 fused apply without the packed D^-1");
-  switch (m.tile_clusters) {
-    case 64: k_apply_tiled<T, MODE, 64><<<grid, 64, tile_smem_bytes<T, MODE, 64>(), s>>>(a); break;
-    case 128: k_apply_tiled<T, MODE, 128><<<grid, 128, tile_smem_bytes<T, MODE, 128>(), s>>>(a); break;
-    default: k_apply_tiled<T, MODE, 256><<<grid, 256, tile_smem_bytes<T, MODE, 256>(), s>>>(a); break;
+  if constexpr (sizeof(T) == 4) {
+    if (use_uniform_geometry<T>(m)) {
+      ApplyArgs<T> g = a;
+      g.geo = m.geo32;
+      launch_apply_geo<T, MODE, true>(m, grid, s, g);
+      return;
+    }
   }
+  launch_apply_geo<T, MODE, false>(m, grid, s, a);
 }
 
 }  // namespace pa

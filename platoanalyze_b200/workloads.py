@@ -43,10 +43,15 @@ def cell_density(dims, seed, **kw):
     return np.repeat(hex_density(dims, seed, **kw), 6)
 
 
-def cantilever(dims, youngs_modulus=1.0, poissons_ratio=0.3, simp_exponent=3.0, simp_min=1e-9, stream=None):
-    """Mesh + Problem (per-cell controls) with the clamp and the end traction."""
+def cantilever(dims, youngs_modulus=1.0, poissons_ratio=0.3, simp_exponent=3.0, simp_min=1e-9, stream=None,
+               uniform_geometry=True):
+    """Mesh + Problem (per-cell controls) with the clamp and the end traction.
+    uniform_geometry=False makes the FP32 kernels recompute the geometry per
+    tet instead of reading the box's hex geometry table."""
     nx, ny, nz = dims
     mesh = Mesh.box(nx, ny, nz, float(nx), float(ny), float(nz))
+    if not uniform_geometry:
+        mesh.set_uniform_geometry(False)
     prob = Problem(mesh, youngs_modulus, poissons_ratio, simp_exponent, simp_min, control_layout="cell",
                    stream=stream)
     faces = mesh.boundary_faces(0, float(nx))
