@@ -237,7 +237,10 @@ template <typename T, int MODE, int TILE, bool GEO = false>
 struct TileSmem {
   static constexpr int kTileNodes = 2 * TILE;
   static constexpr int kRawBufs = MODE >= 1 ? 2 : 1;
-  Node4<T> xc[2][kTileNodes];             // coordinates + input (component 0), two buffers
+  // node records: gathered by cp.async (two buffers), except in the GEO PCG
+  // modes, where the formation step writes them (one buffer)
+  static constexpr int kXcBufs = (GEO && MODE >= 1) ? 1 : 2;
+  Node4<T> xc[kXcBufs][kTileNodes];       // coordinates + input (component 0)
   Node2<T> uu[2][GEO ? 1 : kTileNodes];   // input components 1, 2
   // PCG modes: r, D^-1, p_old gathered for the tile.  FP32 keeps D^-1 as one
   // 16-byte record per node (dv) and only r and p_old in raw.
@@ -246,37 +249,65 @@ struct TileSmem {
   static constexpr int kRowD = 3, kRowP = kPackedD ? 3 : 6;
   T raw[kRawBufs][kRawRows][kTileNodes];
   float4 dv[kPackedD ? 2 : 1][kPackedD ? kTileNodes : 1];
-  T y[3][kTileNodes];                     // node sums of the current tile
+  // node sums of the current tile: the PCG modes keep them in the r rows of
+  // the tile's gather buffer (raw[b][0..2], dead once the input is formed)
+  T y[MODE >= 1 ? 1 : 3][MODE >= 1 ? 1 : kTileNodes];
   T w[2][6 * TILE];                       // penalty weights of the tile's cells
+  // tile headers and node ids: three buffers, fetched two tiles ahead (the
+  // data gathers of tile k+1 read the ids of tile k+1 while tile k still uses
+  // its own); cluster records travel with the data (two buffers)
   uint4 rec[2][TILE];                     // cluster node ids
-  uint32_t ids[2][kTileNodes];            // flagged node ids
-  int32_t meta[2][8];                     // n0, nn, k0, nk, nhex, cell0, ncell
+  uint32_t ids[3][kTileNodes];            // flagged node ids
+  int32_t meta[3][8];                     // n0, nn, k0, nk, nhex, cell0, ncell
   double red[32];
 };
+
+// Row d of the current tile's node sums (data buffer b).
+template <typename T, int MODE, int TILE, bool GEO>
+__device__ __forceinline__ T* node_sums(TileSmem<T, MODE, TILE, GEO>& S, int b, int d) {
+  if constexpr (MODE >= 1)
+    return S.raw[b][d];
+  else
+    return S.y[d];
+}
 
 template <typename T, int MODE, int TILE, bool GEO>
 constexpr size_t tile_smem_bytes() {
   return sizeof(TileSmem<T, MODE, TILE, GEO>);
 }
 
-// Issue the loads of tile `tile`'s header, node ids and cluster records (buffer b).
+// Header of one tile (node, cluster and cell ranges), loaded into registers
+// one tile before its ids are fetched so that the loads' latency is hidden.
+struct TileHead {
+  int n0, nn, k0, nk, nhex, c0, nc;
+};
+
+__device__ __forceinline__ TileHead load_head(const TileView& tv, int tile) {
+  TileHead h;
+  h.n0 = __ldg(&tv.tile_node_start[tile]);
+  h.nn = __ldg(&tv.tile_node_start[tile + 1]) - h.n0;
+  h.k0 = __ldg(&tv.tile_cluster_start[tile]);
+  h.nk = __ldg(&tv.tile_cluster_start[tile + 1]) - h.k0;
+  h.nhex = __ldg(&tv.tile_hex_count[tile]);
+  h.c0 = __ldg(&tv.tile_cell_start[tile]);
+  h.nc = __ldg(&tv.tile_cell_start[tile + 1]) - h.c0;
+  return h;
+}
+
+// Issue the loads of one tile's node ids and cluster records into id buffer ib.
 template <typename T, int MODE, int TILE, bool GEO>
-__device__ __forceinline__ void prefetch_ids(const ApplyArgs<T>& a, TileSmem<T, MODE, TILE, GEO>& S, int tile,
-                                             int b) {
-  const int n0 = a.tv.tile_node_start[tile], nn = a.tv.tile_node_start[tile + 1] - n0;
-  const int k0 = a.tv.tile_cluster_start[tile], nk = a.tv.tile_cluster_start[tile + 1] - k0;
+__device__ __forceinline__ void prefetch_ids(const ApplyArgs<T>& a, TileSmem<T, MODE, TILE, GEO>& S,
+                                             const TileHead& h, int ib) {
   if (threadIdx.x == 0) {
-    const int c0 = a.tv.tile_cell_start[tile];
-    S.meta[b][0] = n0;
-    S.meta[b][1] = nn;
-    S.meta[b][2] = k0;
-    S.meta[b][3] = nk;
-    S.meta[b][4] = a.tv.tile_hex_count[tile];
-    S.meta[b][5] = c0;
-    S.meta[b][6] = a.tv.tile_cell_start[tile + 1] - c0;
+    S.meta[ib][0] = h.n0;
+    S.meta[ib][1] = h.nn;
+    S.meta[ib][2] = h.k0;
+    S.meta[ib][3] = h.nk;
+    S.meta[ib][4] = h.nhex;
+    S.meta[ib][5] = h.c0;
+    S.meta[ib][6] = h.nc;
   }
-  for (int i = threadIdx.x; i < nn; i += blockDim.x) cp_async<4>(&S.ids[b][i], &a.tile_nodes[n0 + i]);
-  for (int i = threadIdx.x; i < nk; i += blockDim.x) cp_async<16>(&S.rec[b][i], &a.tv.cluster_nodes[k0 + i]);
+  for (int i = threadIdx.x; i < h.nn; i += blockDim.x) cp_async<4>(&S.ids[ib][i], &a.tile_nodes[h.n0 + i]);
   cp_async_commit();
 }
 
@@ -284,24 +315,27 @@ __device__ __forceinline__ void prefetch_ids(const ApplyArgs<T>& a, TileSmem<T, 
 // GEO (uniform hex geometry): no coordinates; the node record holds the
 // input vector (u0, u1, u2, 0).
 template <typename T, int MODE, int TILE, bool GEO>
-__device__ __forceinline__ void prefetch_data(const ApplyArgs<T>& a, TileSmem<T, MODE, TILE, GEO>& S, int b) {
-  const int nn = S.meta[b][1];
+__device__ __forceinline__ void prefetch_data(const ApplyArgs<T>& a, TileSmem<T, MODE, TILE, GEO>& S, int ib,
+                                              int b) {
+  const int nn = S.meta[ib][1];
   const int64_t N = a.N;
   for (int i = threadIdx.x; i < nn; i += blockDim.x) {
-    const int64_t g = int64_t(S.ids[b][i] & kNodeIdMask);
-    bool packed = GEO;
-    if constexpr (sizeof(T) == 4 && MODE >= 1) {
-      // (x, y, z, 0) in one copy; the fourth slot is the input component 0,
-      // which the PCG modes write after this copy has landed
-      if (a.coords4) {
-        cp_async<16>(&S.xc[b][i], &a.coords4[g]);
-        packed = true;
+    const int64_t g = int64_t(S.ids[ib][i] & kNodeIdMask);
+    if constexpr (!GEO) {
+      bool packed = false;
+      if constexpr (sizeof(T) == 4 && MODE >= 1) {
+        // (x, y, z, 0) in one copy; the fourth slot is the input component 0,
+        // which the PCG modes write after this copy has landed
+        if (a.coords4) {
+          cp_async<16>(&S.xc[b][i], &a.coords4[g]);
+          packed = true;
+        }
       }
-    }
-    if (!packed) {
-      cp_async<sizeof(T)>(&S.xc[b][i].x, &a.coords[g]);
-      cp_async<sizeof(T)>(&S.xc[b][i].y, &a.coords[N + g]);
-      cp_async<sizeof(T)>(&S.xc[b][i].z, &a.coords[2 * N + g]);
+      if (!packed) {
+        cp_async<sizeof(T)>(&S.xc[b][i].x, &a.coords[g]);
+        cp_async<sizeof(T)>(&S.xc[b][i].y, &a.coords[N + g]);
+        cp_async<sizeof(T)>(&S.xc[b][i].z, &a.coords[2 * N + g]);
+      }
     }
     if constexpr (MODE == 0 && GEO) {
       cp_async<sizeof(T)>(&S.xc[b][i].x, &a.x[g]);
@@ -322,15 +356,24 @@ __device__ __forceinline__ void prefetch_data(const ApplyArgs<T>& a, TileSmem<T,
       if constexpr (TileSmem<T, MODE, TILE>::kPackedD) cp_async<16>(&S.dv[b][i], &a.dinv4[g]);
     }
   }
-  const int c0 = S.meta[b][5], nc = S.meta[b][6];
+  const int c0 = S.meta[ib][5], nc = S.meta[ib][6];
   for (int i = threadIdx.x; i < nc; i += blockDim.x) cp_async<sizeof(T)>(&S.w[b][i], &a.w[c0 + i]);
+  const int k0 = S.meta[ib][2], nk = S.meta[ib][3];
+  for (int i = threadIdx.x; i < nk; i += blockDim.x) cp_async<16>(&S.rec[b][i], &a.tv.cluster_nodes[k0 + i]);
   cp_async_commit();
 }
 
 // FP32 instances ask for 640 resident threads per SM (<= 96 registers, 20
-// warps); FP64 instances are register-bound at one or two CTAs.
+// warps), the GEO PCG instances of 256-cluster tiles for three CTAs (768
+// threads, <= 85 registers; their shared memory fits three); FP64 instances
+// are register-bound at one or two CTAs.
 template <typename T, int MODE, int TILE, bool GEO>
-__global__ void __launch_bounds__(TILE, (sizeof(T) == 4 ? 640 / TILE : 1)) k_apply_tiled(ApplyArgs<T> a) {
+constexpr int apply_min_blocks() {
+  return sizeof(T) != 4 ? 1 : (GEO && MODE >= 1 && TILE == 256) ? 3 : 640 / TILE;
+}
+
+template <typename T, int MODE, int TILE, bool GEO>
+__global__ void __launch_bounds__(TILE, (apply_min_blocks<T, MODE, TILE, GEO>())) k_apply_tiled(ApplyArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TileSmem<T, MODE, TILE, GEO>& S = *reinterpret_cast<TileSmem<T, MODE, TILE, GEO>*>(smem_raw);
 
@@ -343,21 +386,35 @@ __global__ void __launch_bounds__(TILE, (sizeof(T) == 4 ? 640 / TILE : 1)) k_app
   const int stride = gridDim.x;
   int tile = blockIdx.x;
 
-  // prologue: ids + data of the first tile, ids of the second
-  if (tile < a.tv.num_tiles) {
-    prefetch_ids(a, S, tile, 0);
+  // Pipeline (tile k of this CTA at the top of iteration k): data of tile k
+  // and ids of tile k+1 have landed; the iteration issues the data gathers of
+  // tile k+1 and the id loads of tile k+2, and loads the header of tile k+3
+  // into registers, then computes tile k.  Id buffers rotate over three
+  // slots, data buffers over two.
+  const int T_ = a.tv.num_tiles;
+  TileHead head_next{};  // header of tile k+2 at the top of iteration k
+  if (tile < T_) {
+    prefetch_ids(a, S, load_head(a.tv, tile), 0);
     cp_async_wait_all();
     __syncthreads();
-    prefetch_data<T, MODE, TILE, GEO>(a, S, 0);
-    if (tile + stride < a.tv.num_tiles) prefetch_ids(a, S, tile + stride, 1);
+    prefetch_data<T, MODE, TILE, GEO>(a, S, 0, 0);
+    if (tile + stride < T_) prefetch_ids(a, S, load_head(a.tv, tile + stride), 1);
+    if (tile + 2 * stride < T_) head_next = load_head(a.tv, tile + 2 * stride);
   }
 
-  for (int k = 0; tile < a.tv.num_tiles; ++k, tile += stride) {
+  int ib = 0;  // id buffer of tile k (k mod 3)
+  for (int k = 0; tile < T_; ++k, tile += stride, ib = ib == 2 ? 0 : ib + 1) {
     const int b = k & 1;
+    const int xb = TileSmem<T, MODE, TILE, GEO>::kXcBufs == 1 ? 0 : b;  // node-record buffer
+    const int ib1 = ib == 2 ? 0 : ib + 1, ib2 = ib1 == 2 ? 0 : ib1 + 1;
     cp_async_wait_all();  // data of this tile, ids of the next
     __syncthreads();
-    const bool has_next = tile + stride < a.tv.num_tiles;
-    if (has_next) prefetch_data<T, MODE, TILE, GEO>(a, S, b ^ 1);
+    if (tile + stride < T_) prefetch_data<T, MODE, TILE, GEO>(a, S, ib1, b ^ 1);
+    if (tile + 2 * stride < T_) {
+      // slot ib2 held the ids of tile k-1, finished before the barrier above
+      prefetch_ids(a, S, head_next, ib2);
+      if (tile + 3 * stride < T_) head_next = load_head(a.tv, tile + 3 * stride);
+    }
     // batched mode: this tile's part, its beta, and whether it has converged
     int part = 0;
     bool skip = false;
@@ -369,9 +426,9 @@ __global__ void __launch_bounds__(TILE, (sizeof(T) == 4 ? 640 / TILE : 1)) k_app
       if (skip) {
         // a stopped part keeps its direction: p_new = p_old on its owned nodes,
         // so both p buffers stay current if the part resumes
-        const int nn = S.meta[b][1];
+        const int nn = S.meta[ib][1];
         for (int i = threadIdx.x; i < nn; i += blockDim.x) {
-          const uint32_t f = S.ids[b][i];
+          const uint32_t f = S.ids[ib][i];
           const int64_t g = int64_t(f & kNodeIdMask);
           if ((f & kOwner) && g < a.N) {
 #pragma unroll
@@ -383,19 +440,19 @@ __global__ void __launch_bounds__(TILE, (sizeof(T) == 4 ? 640 / TILE : 1)) k_app
     if (!skip) {
 
     // 2. input vector of this tile; zero its sums
-    const int nn = S.meta[b][1];
+    const int nn = S.meta[ib][1];
     for (int i = threadIdx.x; i < nn; i += blockDim.x) {
-      const uint32_t f = S.ids[b][i];
+      const uint32_t f = S.ids[ib][i];
       const uint32_t mk = (f >> kMaskShift) & 7u;
       if constexpr (MODE == 0 && GEO) {
         if (mk) {
-          if (mk & 1u) S.xc[b][i].x = T(0);
-          if (mk & 2u) S.xc[b][i].y = T(0);
-          if (mk & 4u) S.xc[b][i].z = T(0);
+          if (mk & 1u) S.xc[xb][i].x = T(0);
+          if (mk & 2u) S.xc[xb][i].y = T(0);
+          if (mk & 4u) S.xc[xb][i].z = T(0);
         }
       } else if constexpr (MODE == 0) {
         if (mk) {
-          if (mk & 1u) S.xc[b][i].u0 = T(0);
+          if (mk & 1u) S.xc[xb][i].u0 = T(0);
           if (mk & 2u) S.uu[b][i].u1 = T(0);
           if (mk & 4u) S.uu[b][i].u2 = T(0);
         }
@@ -415,9 +472,9 @@ __global__ void __launch_bounds__(TILE, (sizeof(T) == 4 ? 640 / TILE : 1)) k_app
           v[d] = (mk >> d) & 1 ? T(0)
                                : dinv[d] * S.raw[b][d][i] + beta * S.raw[b][TileSmem<T, MODE, TILE>::kRowP + d][i];
         if constexpr (GEO) {
-          S.xc[b][i] = Node4<T>{v[0], v[1], v[2], T(0)};
+          S.xc[xb][i] = Node4<T>{v[0], v[1], v[2], T(0)};
         } else {
-          S.xc[b][i].u0 = v[0];
+          S.xc[xb][i].u0 = v[0];
           S.uu[b][i].u1 = v[1];
           S.uu[b][i].u2 = v[2];
         }
@@ -428,13 +485,13 @@ __global__ void __launch_bounds__(TILE, (sizeof(T) == 4 ? 640 / TILE : 1)) k_app
         }
       }
 #pragma unroll
-      for (int d = 0; d < 3; ++d) S.y[d][i] = T(0);
+      for (int d = 0; d < 3; ++d) node_sums(S, b, d)[i] = T(0);  // after this node's r was read
     }
     __syncthreads();
 
     // 3. one cluster per thread
     const int t = threadIdx.x;
-    const int nk = S.meta[b][3], nhex = S.meta[b][4];
+    const int nk = S.meta[ib][3], nhex = S.meta[ib][4];
     if (t < nk) {
       const uint4 q = S.rec[b][t];
       const int ln[8] = {int(q.x & 0xffff), int(q.x >> 16), int(q.y & 0xffff), int(q.y >> 16),
@@ -444,10 +501,10 @@ __global__ void __launch_bounds__(TILE, (sizeof(T) == 4 ? 640 / TILE : 1)) k_app
         T D[7][3], Y[7][3];
         if constexpr (GEO) {
           // input differences relative to slot 7; geometry from the table
-          const Node4<T> q7 = S.xc[b][ln[7]];
+          const Node4<T> q7 = S.xc[xb][ln[7]];
 #pragma unroll
           for (int s = 0; s < 7; ++s) {
-            const Node4<T> q4 = S.xc[b][ln[s]];
+            const Node4<T> q4 = S.xc[xb][ln[s]];
             D[s][0] = q4.x - q7.x;
             D[s][1] = q4.y - q7.y;
             D[s][2] = q4.z - q7.z;
@@ -461,7 +518,7 @@ __global__ void __launch_bounds__(TILE, (sizeof(T) == 4 ? 640 / TILE : 1)) k_app
             const T h1[3] = {a.geo.h[k][3], a.geo.h[k][4], a.geo.h[k][5]};
             const T h2[3] = {a.geo.h[k][6], a.geo.h[k][7], a.geo.h[k][8]};
             T r0[3], ra[3], rb[3];
-            const T* pl = a.plas ? a.plas + 8 * (int64_t(S.meta[b][5]) + 6 * t + k) : nullptr;
+            const T* pl = a.plas ? a.plas + 8 * (int64_t(S.meta[ib][5]) + 6 * t + k) : nullptr;
             const T en = tet_core(a.iso, wv[k] * a.geo.s[k], h0, h1, h2, D[0], D[sa], D[sb], r0, ra, rb, pl);
             if (MODE >= 1) pap += double(en);
 #pragma unroll
@@ -475,11 +532,11 @@ __global__ void __launch_bounds__(TILE, (sizeof(T) == 4 ? 640 / TILE : 1)) k_app
         // edge vectors and input differences relative to slot 7 (the diagonal end)
         T E[7][3];
         {
-          const Node4<T> q7 = S.xc[b][ln[7]];
+          const Node4<T> q7 = S.xc[xb][ln[7]];
           const Node2<T> p7 = S.uu[b][ln[7]];
 #pragma unroll
           for (int s = 0; s < 7; ++s) {
-            const Node4<T> q4 = S.xc[b][ln[s]];
+            const Node4<T> q4 = S.xc[xb][ln[s]];
             const Node2<T> q2 = S.uu[b][ln[s]];
             E[s][0] = q4.x - q7.x;
             E[s][1] = q4.y - q7.y;
@@ -501,7 +558,7 @@ __global__ void __launch_bounds__(TILE, (sizeof(T) == 4 ? 640 / TILE : 1)) k_app
           T h1[3], r0[3], ra[3], rb[3];
 #pragma unroll
           for (int d = 0; d < 3; ++d) h1[d] = -Cx[sb][d];
-          const T* pl = a.plas ? a.plas + 8 * (int64_t(S.meta[b][5]) + 6 * t + k) : nullptr;
+          const T* pl = a.plas ? a.plas + 8 * (int64_t(S.meta[ib][5]) + 6 * t + k) : nullptr;
           const T en = tet_rel(a.iso, wv[k], E[0], E[sa], E[sb], h1, Cx[sa], D[0], D[sa], D[sb], r0, ra, rb, pl);
           if (MODE >= 1) pap += double(en);
 #pragma unroll
@@ -521,18 +578,18 @@ __global__ void __launch_bounds__(TILE, (sizeof(T) == 4 ? 640 / TILE : 1)) k_app
 #pragma unroll
         for (int s = 0; s < 7; ++s)
 #pragma unroll
-          for (int d = 0; d < 3; ++d) atomicAdd(&S.y[d][ln[s]], Y[s][d]);
+          for (int d = 0; d < 3; ++d) atomicAdd(&node_sums(S, b, d)[ln[s]], Y[s][d]);
 #pragma unroll
-        for (int d = 0; d < 3; ++d) atomicAdd(&S.y[d][ln[7]], Y7[d]);
+        for (int d = 0; d < 3; ++d) atomicAdd(&node_sums(S, b, d)[ln[7]], Y7[d]);
       } else if constexpr (!GEO) {
         // single tets follow the hexes: cell index = 6 * nhex + (t - nhex)
         // (a mesh with uniform hex geometry has none)
         T e[3][3], du[3][3], h1[3], h2[3], r[3][3];
-        const Node4<T> q3 = S.xc[b][ln[3]];
+        const Node4<T> q3 = S.xc[xb][ln[3]];
         const Node2<T> p3 = S.uu[b][ln[3]];
 #pragma unroll
         for (int n = 0; n < 3; ++n) {
-          const Node4<T> q4 = S.xc[b][ln[n]];
+          const Node4<T> q4 = S.xc[xb][ln[n]];
           const Node2<T> q2 = S.uu[b][ln[n]];
           e[n][0] = q4.x - q3.x;
           e[n][1] = q4.y - q3.y;
@@ -544,28 +601,28 @@ __global__ void __launch_bounds__(TILE, (sizeof(T) == 4 ? 640 / TILE : 1)) k_app
         cross3(e[2], e[0], h1);
         cross3(e[0], e[1], h2);
         const int cl = 6 * nhex + (t - nhex);
-        const T* pl = a.plas ? a.plas + 8 * (int64_t(S.meta[b][5]) + cl) : nullptr;
+        const T* pl = a.plas ? a.plas + 8 * (int64_t(S.meta[ib][5]) + cl) : nullptr;
         const T en = tet_rel(a.iso, S.w[b][cl], e[0], e[1], e[2], h1, h2, du[0], du[1], du[2], r[0], r[1], r[2], pl);
         if (MODE >= 1) pap += double(en);
 #pragma unroll
         for (int n = 0; n < 3; ++n)
 #pragma unroll
-          for (int d = 0; d < 3; ++d) atomicAdd(&S.y[d][ln[n]], r[n][d]);
+          for (int d = 0; d < 3; ++d) atomicAdd(&node_sums(S, b, d)[ln[n]], r[n][d]);
 #pragma unroll
-        for (int d = 0; d < 3; ++d) atomicAdd(&S.y[d][ln[3]], -(r[0][d] + r[1][d] + r[2][d]));
+        for (int d = 0; d < 3; ++d) atomicAdd(&node_sums(S, b, d)[ln[3]], -(r[0][d] + r[1][d] + r[2][d]));
       }
     }
     __syncthreads();
 
     // 4. write node sums
     for (int i = threadIdx.x; i < nn; i += blockDim.x) {
-      const uint32_t f = S.ids[b][i];
+      const uint32_t f = S.ids[ib][i];
       const int64_t gid = f & kNodeIdMask;
       const uint32_t mk = (f >> kMaskShift) & 7u;
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         if ((mk >> d) & 1) continue;
-        const T v = S.y[d][i];
+        const T v = node_sums(S, b, d)[i];
         if (f & kShared)
           atomicAdd(&a.y[d * a.N + gid], v);
         else
@@ -579,12 +636,10 @@ __global__ void __launch_bounds__(TILE, (sizeof(T) == 4 ? 640 / TILE : 1)) k_app
       if (threadIdx.x == 0) atomicAdd(&a.pacc[part], v);
     }
     }  // !skip
-    // a skipped tile read buffer b above; every thread must be done with it
-    // before the next line refills it (the non-skipped path synchronised after
-    // its write-back)
+    // a skipped tile read buffers ib and b above; every thread must be done
+    // with them before the next iteration refills them (the non-skipped path
+    // synchronised after its write-back)
     if (skip) __syncthreads();
-    // ids of the tile after next into this buffer
-    if (tile + 2 * stride < a.tv.num_tiles) prefetch_ids(a, S, tile + 2 * stride, b);
   }
   cp_async_wait_all();
 
