@@ -315,6 +315,27 @@ void build_tiles(Mesh& m) {
     }
   }
 
+  // The table kernel accumulates node sums slot by slot without atomics: it
+  // needs, in every tile, the nodes of any one slot to be distinct across the
+  // tile's hexes (true for translates, unless hexes are duplicated).
+  if (m.uniform_hex) {
+    std::vector<int32_t> mark(tile_n, -1);
+    for (int32_t t = 0; t < tile && m.uniform_hex; ++t)
+      for (int s = 0; s < 8 && m.uniform_hex; ++s) {
+        const int32_t stamp = 8 * t + s;
+        for (int32_t k = tile_cluster_start[t]; k < tile_cluster_start[t + 1]; ++k) {
+          const uint4 q = cluster_nodes[k];
+          const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+          const uint32_t id = (w[s / 2] >> (16 * (s % 2))) & 0xffffu;
+          if (mark[id] == stamp) {
+            m.uniform_hex = false;
+            break;
+          }
+          mark[id] = stamp;
+        }
+      }
+  }
+
   for (int32_t t = 0; t < tile; ++t)
     for (int32_t k = tile_node_start[t]; k < tile_node_start[t + 1]; ++k) {
       const uint32_t v = tile_nodes[k];

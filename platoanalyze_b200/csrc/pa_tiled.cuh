@@ -492,13 +492,22 @@ __global__ void __launch_bounds__(TILE, (apply_min_blocks<T, MODE, TILE, GEO>())
     // 3. one cluster per thread
     const int t = threadIdx.x;
     const int nk = S.meta[ib][3], nhex = S.meta[ib][4];
-    if (t < nk) {
+    T Y[7][3], Y7[3];  // node contributions of this thread's hex (slot order)
+    int ln[8];
+    const bool act = t < nk;
+    if (act) {
       const uint4 q = S.rec[b][t];
-      const int ln[8] = {int(q.x & 0xffff), int(q.x >> 16), int(q.y & 0xffff), int(q.y >> 16),
-                         int(q.z & 0xffff), int(q.z >> 16), int(q.w & 0xffff), int(q.w >> 16)};
+      ln[0] = int(q.x & 0xffff);
+      ln[1] = int(q.x >> 16);
+      ln[2] = int(q.y & 0xffff);
+      ln[3] = int(q.y >> 16);
+      ln[4] = int(q.z & 0xffff);
+      ln[5] = int(q.z >> 16);
+      ln[6] = int(q.w & 0xffff);
+      ln[7] = int(q.w >> 16);
       if (t < nhex) {
         const T* wv = &S.w[b][6 * t];
-        T D[7][3], Y[7][3];
+        T D[7][3];
         if constexpr (GEO) {
           // input differences relative to slot 7; geometry from the table
           const Node4<T> q7 = S.xc[xb][ln[7]];
@@ -570,17 +579,20 @@ __global__ void __launch_bounds__(TILE, (apply_min_blocks<T, MODE, TILE, GEO>())
         }
         }  // !GEO
         // slot 7 closes each tet's partition of unity: Y7 = -(Y0 + ... + Y6)
-        T Y7[3] = {T(0), T(0), T(0)};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) Y7[d] = T(0);
 #pragma unroll
         for (int s = 0; s < 7; ++s)
 #pragma unroll
           for (int d = 0; d < 3; ++d) Y7[d] -= Y[s][d];
+        if constexpr (!GEO) {
 #pragma unroll
-        for (int s = 0; s < 7; ++s)
+          for (int s = 0; s < 7; ++s)
 #pragma unroll
-          for (int d = 0; d < 3; ++d) atomicAdd(&node_sums(S, b, d)[ln[s]], Y[s][d]);
+            for (int d = 0; d < 3; ++d) atomicAdd(&node_sums(S, b, d)[ln[s]], Y[s][d]);
 #pragma unroll
-        for (int d = 0; d < 3; ++d) atomicAdd(&node_sums(S, b, d)[ln[7]], Y7[d]);
+          for (int d = 0; d < 3; ++d) atomicAdd(&node_sums(S, b, d)[ln[7]], Y7[d]);
+        }
       } else if constexpr (!GEO) {
         // single tets follow the hexes: cell index = 6 * nhex + (t - nhex)
         // (a mesh with uniform hex geometry has none)
@@ -612,7 +624,26 @@ __global__ void __launch_bounds__(TILE, (apply_min_blocks<T, MODE, TILE, GEO>())
         for (int d = 0; d < 3; ++d) atomicAdd(&node_sums(S, b, d)[ln[3]], -(r[0][d] + r[1][d] + r[2][d]));
       }
     }
-    __syncthreads();
+    if constexpr (GEO) {
+      // Conflict-free accumulation: two hexes of a tile never share a node in
+      // the same slot (the host checks this per tile before it enables the
+      // table), so slot by slot the read-add-writes of all threads hit
+      // distinct nodes; a barrier separates the slots.  This replaces 24
+      // shared float atomics (compare-and-swap loops) per hex.
+#pragma unroll
+      for (int s = 0; s < 8; ++s) {
+        if (act) {
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            T* y = node_sums(S, b, d);
+            y[ln[s]] += s < 7 ? Y[s][d] : Y7[d];
+          }
+        }
+        __syncthreads();
+      }
+    } else {
+      __syncthreads();
+    }
 
     // 4. write node sums
     for (int i = threadIdx.x; i < nn; i += blockDim.x) {

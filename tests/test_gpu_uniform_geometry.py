@@ -46,6 +46,18 @@ def test_non_uniform_meshes_use_the_per_tet_geometry(pa):
     # single-tet clusters (shuffled cells) never qualify
     rng = np.random.default_rng(0)
     assert not pa.Mesh.from_arrays(cells[rng.permutation(cells.shape[0])], coords).uniform_geometry
+    # a duplicated hex has its twin's node in every slot of the same tile: the
+    # table kernel's slot-by-slot (atomic-free) sums would collide, so the mesh
+    # keeps the per-tet path, which still matches the oracle
+    dup = np.concatenate([cells, cells[:6]])
+    mdup = pa.Mesh.from_arrays(dup, coords)
+    assert not mdup.uniform_geometry
+    from oracle import cpu
+    O = cpu.Oracle(dup, coords, E=1.0, nu=0.3, p=3.0, pmin=1e-9, layout=1)
+    z = rng.uniform(0.1, 1.0, dup.shape[0])
+    u = rng.standard_normal(3 * coords.shape[0])
+    y = pa.Problem(mdup, 1.0, 0.3, 3.0, 1e-9, control_layout="cell").apply(z, u.astype(np.float32))
+    assert rel_inf(y, O.apply(u, z)) < 1e-5
     # the box generator qualifies; switching back on re-detects it
     m = pa.Mesh.box(5, 4, 3, 2.5, 2.0, 1.5)
     assert m.uniform_geometry
