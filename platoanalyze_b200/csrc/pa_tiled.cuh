@@ -206,6 +206,15 @@ __host__ __device__ constexpr int hex_ring(int k) {
   return r[k];
 }
 
+// Fire-and-forget global reduction (no returned value, so nothing waits on
+// it); the address is converted to the global window explicitly.
+__device__ __forceinline__ void red_add_global(float* p, float v) {
+  asm volatile("red.global.add.f32 [%0], %1;\n" ::"l"(__cvta_generic_to_global(p)), "f"(v) : "memory");
+}
+__device__ __forceinline__ void red_add_global(double* p, double v) {
+  asm volatile("red.global.add.f64 [%0], %1;\n" ::"l"(__cvta_generic_to_global(p)), "d"(v) : "memory");
+}
+
 // ---------------------------------------------------------------- cp.async --
 template <int BYTES>
 __device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
@@ -655,7 +664,7 @@ __global__ void __launch_bounds__(TILE, (apply_min_blocks<T, MODE, TILE, GEO>())
         if ((mk >> d) & 1) continue;
         const T v = node_sums(S, b, d)[i];
         if (f & kShared)
-          atomicAdd(&a.y[d * a.N + gid], v);
+          red_add_global(&a.y[d * a.N + gid], v);
         else
           a.y[d * a.N + gid] = v;
       }
