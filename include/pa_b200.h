@@ -92,11 +92,12 @@ pa_status pa_mesh_set_graph(pa_mesh* mesh, const int32_t* rowmap, const int32_t*
 
 /* Uniform hex geometry.  When every cell belongs to a six-tet hex and all
  * hexes are translates of one another (a structured voxel grid, any hex
- * shape), the FP32 matrix-free kernels take each template tet's shape
- * gradients and volume from a per-mesh table computed once in FP64 instead of
- * recomputing them per tet from gathered coordinates (no reference
- * counterpart: the reference recomputes them per cell,
- * src/ImplicitFunctors.hpp:165-217).  enable = 1 (the default) uses the table
+ * shape; edge vectors equal to 1e-9 of the hex size), the FP32 matrix-free
+ * kernels take each template tet's shape gradients and volume from a per-mesh
+ * table computed once in FP64 instead of recomputing them per tet from
+ * gathered coordinates; the FP64 kernels do so when the hexes agree to
+ * rounding level (1e-12 of the hex size).  No reference counterpart: the
+ * reference recomputes them per cell (src/ImplicitFunctors.hpp:165-217).  enable = 1 (the default) uses the table
  * when the mesh qualifies, 0 forces the per-tet geometry, -1 only queries;
  * *active (may be NULL) receives 1 when the table is in use.  Changing it is
  * allowed only before problems are created on the mesh. */

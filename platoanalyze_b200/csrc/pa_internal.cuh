@@ -118,8 +118,11 @@ struct Mesh {
   int64_t num_clusters = 0, num_hex = 0;
   // every cluster a hex and every hex a translate of the first (edge vectors
   // equal to 1e-9 of the hex size): the FP32 tile kernel then takes the
-  // geometry from geo32 and gathers no coordinates
+  // geometry from geo32 and gathers no coordinates; the FP64 kernel does the
+  // same from geo64 when the largest deviation (hex_geo_dev, relative to the
+  // hex size) is at rounding level, <= 1e-12
   bool uniform_hex = false;
+  double hex_geo_dev = 0.0;
   bool allow_uniform_geometry = true;  // false: always the per-tet geometry
   HexGeo<double> geo64{};
   HexGeo<float> geo32{};

@@ -132,13 +132,18 @@ void detect_uniform_hex(Mesh& m, const std::vector<Cluster>& cl) {
     for (int d = 0; d < 3; ++d) size = std::max(size, std::fabs(E0[s][d]));
   if (!(size > 0.0)) return;
   const double tol = 1e-9 * size;
+  double dev = 0.0;
   for (const Cluster& k : cl) {
     double E[7][3];
     edges(k, E);
     for (int s = 0; s < 7; ++s)
-      for (int d = 0; d < 3; ++d)
-        if (std::fabs(E[s][d] - E0[s][d]) > tol) return;
+      for (int d = 0; d < 3; ++d) {
+        const double e = std::fabs(E[s][d] - E0[s][d]);
+        if (e > tol) return;
+        dev = std::max(dev, e);
+      }
   }
+  m.hex_geo_dev = dev / size;
   static const int ring[7] = {3, 2, 6, 4, 5, 1, 3};
   auto cross = [](const double* a, const double* b, double* c) {
     c[0] = a[1] * b[2] - a[2] * b[1];

@@ -739,12 +739,13 @@ int apply_grid_for(int num_tiles) {
   return std::max(grid, 1);
 }
 
-// The FP32 instances take the uniform-geometry form when the mesh has it; FP64
-// always recomputes the geometry per tet (its parity is against the oracle's
-// per-cell arithmetic).
+// The FP32 instances take the uniform-geometry form when the mesh has it; the
+// FP64 ones only when every hex matches the table to rounding level (their
+// parity with the oracle's per-cell FP64 arithmetic is 1e-10).
+constexpr double kGeoDevFp64 = 1e-12;
 template <typename T>
 bool use_uniform_geometry(const Mesh& m) {
-  return sizeof(T) == 4 && m.uniform_hex;
+  return m.uniform_hex && (sizeof(T) == 4 || m.hex_geo_dev <= kGeoDevFp64);
 }
 
 template <typename T, int MODE, bool GEO>
@@ -758,9 +759,7 @@ int apply_kernel_setup_geo(const Mesh& m) {
 
 template <typename T, int MODE>
 int apply_kernel_setup(const Mesh& m) {
-  if constexpr (sizeof(T) == 4) {
-    if (use_uniform_geometry<T>(m)) return apply_kernel_setup_geo<T, MODE, true>(m);
-  }
+  if (use_uniform_geometry<T>(m)) return apply_kernel_setup_geo<T, MODE, true>(m);
   return apply_kernel_setup_geo<T, MODE, false>(m);
 }
 
@@ -780,13 +779,14 @@ template <typename T, int MODE>
 void launch_apply_kernel(const Mesh& m, int grid, cudaStream_t s, const ApplyArgs<T>& a) {
   if (sizeof(T) == 4 && MODE >= 1 && a.dinv4 == nullptr)
     throw Error(PA_ERR_INVALID_ARG, "FP32 fused apply without the packed D^-1");
-  if constexpr (sizeof(T) == 4) {
-    if (use_uniform_geometry<T>(m)) {
-      ApplyArgs<T> g = a;
+  if (use_uniform_geometry<T>(m)) {
+    ApplyArgs<T> g = a;
+    if constexpr (sizeof(T) == 4)
       g.geo = m.geo32;
-      launch_apply_geo<T, MODE, true>(m, grid, s, g);
-      return;
-    }
+    else
+      g.geo = m.geo64;
+    launch_apply_geo<T, MODE, true>(m, grid, s, g);
+    return;
   }
   launch_apply_geo<T, MODE, false>(m, grid, s, a);
 }

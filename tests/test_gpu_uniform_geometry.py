@@ -176,3 +176,43 @@ def test_batched_solve_with_the_geometry_table(pa):
         assert rel_inf(up, u1) <= 1e-5, p
         c0 += c.shape[0]
         shift += nx + 2.0
+
+
+@pytest.mark.parametrize("spacing", SPACINGS)
+def test_fp64_apply_and_solve_with_the_geometry_table(pa, oracle_lib, spacing):
+    """FP64 takes the table only when every hex matches it to rounding level;
+    then it keeps the 1e-10 parity of the per-tet FP64 arithmetic."""
+    dims = (9, 7, 5)
+    cells, coords, table, per_tet = _meshes(pa, dims, spacing)
+    O = oracle_lib.Oracle(cells, coords, E=3.0, nu=0.27, p=3.0, pmin=1e-6, layout=1)
+    rng = np.random.default_rng(9)
+    z = rng.uniform(0.05, 1.0, O.C)
+    u = rng.standard_normal(3 * O.N)
+    ref = O.apply(u, z)
+    for mesh in (table, per_tet):
+        y = pa.Problem(mesh, 3.0, 0.27, 3.0, 1e-6, control_layout="cell").apply(z, u)
+        assert rel_inf(y, ref) < 1e-10
+    sols = []
+    for mesh in (table, per_tet):
+        prob, zc = _cantilever(pa, mesh, dims, spacing, 5)
+        x, st = prob.solution(zc, options=pa.SolveOptions("fp64", rel_tol=1e-11))
+        assert st["converged"], st
+        sols.append(x)
+    assert rel_inf(sols[0], sols[1]) < 1e-8
+
+
+def test_fp64_keeps_the_per_tet_geometry_off_rounding_level(pa, oracle_lib):
+    """Hexes that differ by up to 9.6e-10 of their size: FP32 still uses the table (its
+    own rounding is far larger), FP64 does not, and stays within 1e-10."""
+    cells, coords = np_ref.box_mesh(6, 5, 4, 6.0, 5.0, 4.0)
+    rng = np.random.default_rng(3)
+    jit = coords + 2.4e-10 * rng.uniform(-1.0, 1.0, coords.shape)  # edge vectors differ by <= 9.6e-10
+    mesh = pa.Mesh.from_arrays(cells, jit)
+    assert mesh.uniform_geometry
+    O = oracle_lib.Oracle(cells, jit, E=1.0, nu=0.3, p=3.0, pmin=1e-9, layout=1)
+    z = rng.uniform(0.05, 1.0, O.C)
+    u = rng.standard_normal(3 * O.N)
+    ref = O.apply(u, z)
+    prob = pa.Problem(mesh, 1.0, 0.3, 3.0, 1e-9, control_layout="cell")
+    assert rel_inf(prob.apply(z, u), ref) < 1e-10
+    assert rel_inf(prob.apply(z, u.astype(np.float32)), ref) < 1e-5
