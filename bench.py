@@ -414,7 +414,9 @@ def run_ours(args):
     peak, peak_kind = peaks()
     achieved = nbytes.value / (ms_launch.value * 1e-3) / 1e9
     tag = f"k_apply_tiled_{'fp32' if precision else 'fp64'}_{dims[0]}x{dims[1]}x{dims[2]}"
-    traffic = traffic_from_profiles(tag)
+    traffic = traffic_from_profiles(f"{tag}_tile{tile}")
+    if traffic is None:
+        traffic = traffic_from_profiles(tag)
 
     if world > 1:
         dist.barrier()
