@@ -54,6 +54,9 @@ def parse():
     ap.add_argument("--per-tet-geometry", action="store_true",
                     help="FP32 kernels recompute the tet geometry instead of using the box's hex geometry table")
     ap.add_argument("--newton-tol", type=float, default=1e-8, help="J2: relative Newton tolerance per load step")
+    ap.add_argument("--max-newton", type=int, default=25, help="J2: Newton iterations per load step")
+    ap.add_argument("--forcing", default="adaptive", choices=["adaptive", "fixed"],
+                    help="J2: tangent-solve tolerances (Eisenstat-Walker, or --rel-tol for every solve)")
     ap.add_argument("--boxes", type=int, default=64, help="batched: number of boxes")
     ap.add_argument("--workload", default="cantilever", choices=["cantilever", "j2", "learned", "batched"],
                     help="cantilever: the SIMP solve (default); j2: the elasto-plastic bar; learned: the "
@@ -526,8 +529,9 @@ def run_j2(args):
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device="cuda")
 
     def solve_once():
-        _, _, st = prob.j2_solve(J2_PARAMS, z, steps=20, max_newton=25, newton_tol=args.newton_tol, options=lin,
-                                 u=u, local=local, allow_not_converged=True)
+        _, _, st = prob.j2_solve(J2_PARAMS, z, steps=20, max_newton=args.max_newton, newton_tol=args.newton_tol,
+                                 options=lin, u=u, local=local, allow_not_converged=True,
+                                 adaptive_forcing=args.forcing == "adaptive")
         return st
 
     for _ in range(args.warmup):
@@ -573,7 +577,8 @@ def run_j2(args):
     l_pin = torch.empty(14 * C, dtype=torch.float64).pin_memory()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    prob.j2_solve(J2_PARAMS, z_pin, steps=20, max_newton=25, newton_tol=args.newton_tol, options=lin, u=u_pin,
+    prob.j2_solve(J2_PARAMS, z_pin, steps=20, max_newton=args.max_newton, newton_tol=args.newton_tol, options=lin,
+                  adaptive_forcing=args.forcing == "adaptive", u=u_pin,
                   local=l_pin, allow_not_converged=True)
     e2e_ms = 1e3 * (time.perf_counter() - t0)
 
@@ -587,7 +592,10 @@ def run_j2(args):
         "data": "synthetic (uniform density 1)",
         "config": {"workload": f"J2 bar {dims[0]}x{dims[1]}x{dims[2]} hex x 6 tets, 20 load steps to 2% axial strain, "
                                "E=200e3 nu=0.3 sigma_y=250 H_iso=1000", "cells": C, "nodes": N,
-                   "linear": args.method, "linear_rel_tol": args.rel_tol, "l2": "256 MB buffer written between steps"},
+                   "linear": args.method, "linear_rel_tol": args.rel_tol,
+                   "tangent_tolerance": "Eisenstat-Walker (floor linear_rel_tol)" if args.forcing == "adaptive"
+                   else "linear_rel_tol for every tangent solve",
+                   "l2": "256 MB buffer written between steps"},
         "newton_iterations": [s["newton_iterations"] for s in stats], "cg_iterations": [s["cg_iterations"] for s in stats],
         "newton_tol": args.newton_tol, "converged": all(s["converged"] for s in stats),
         "worst_step_rel_residual": max(s["final_rel_residual"] for s in stats),

@@ -295,6 +295,10 @@ typedef struct {
   int32_t steps;       /* pseudo-time load steps; Dirichlet values ramp as (k+1)/steps */
   int32_t max_newton;  /* Newton iterations per step */
   double newton_tol;   /* ||R_free|| <= newton_tol * (||R_free|| at the step's first iteration) */
+  int32_t adaptive_forcing; /* 0: every tangent solve to linear->rel_tol; 1: inexact Newton, tolerance
+                               eta_k = 0.9 (||R_k|| / ||R_k-1||)^2 (Eisenstat-Walker choice 2,
+                               safeguarded, at most 0.1, at least linear->rel_tol and half the
+                               remaining Newton reduction).  The Newton stopping test is unchanged. */
 } pa_j2_solve_options;
 
 typedef struct {

@@ -44,7 +44,7 @@ class J2Params(ct.Structure):
 
 
 class J2SolveOptions(ct.Structure):
-    _fields_ = [("steps", I32), ("max_newton", I32), ("newton_tol", F64)]
+    _fields_ = [("steps", I32), ("max_newton", I32), ("newton_tol", F64), ("adaptive_forcing", I32)]
 
 
 class J2Stats(ct.Structure):

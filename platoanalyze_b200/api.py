@@ -348,15 +348,17 @@ class Problem:
         return out
 
     def j2_solve(self, params, z, steps=20, max_newton=25, newton_tol=1e-8, options=None, u=None, local=None,
-                 allow_not_converged=False):
+                 allow_not_converged=False, adaptive_forcing=False):
         """Load-stepped Newton solve of the J2 problem (pa_j2_solve); the
-        problem's Dirichlet values are the final prescribed displacements."""
+        problem's Dirichlet values are the final prescribed displacements.
+        adaptive_forcing: inexact Newton (Eisenstat-Walker tolerances for the
+        tangent solves, options.rel_tol as their floor)."""
         C = self.mesh.num_cells
         z = _as(z, np.float64)
         u = _empty(z, self.ndof) if u is None else u
         local = _empty(z, 14 * C) if local is None else local
         jp = self._j2_params(params)
-        jo = _abi.J2SolveOptions(int(steps), int(max_newton), float(newton_tol))
+        jo = _abi.J2SolveOptions(int(steps), int(max_newton), float(newton_tol), 1 if adaptive_forcing else 0)
         lo = (options or SolveOptions("mixed", rel_tol=1e-8)).c()
         js = _abi.J2Stats()
         status = self._lib.pa_j2_solve(self._h, ct.byref(jp), _ptr(z, np.float64, self.mesh.num_nodes, "z"),

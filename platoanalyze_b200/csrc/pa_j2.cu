@@ -494,7 +494,7 @@ pa_status j2_solve(Problem& P, const pa_j2_params& jp, const double* z, const pa
   };
   // K_T du = -R with the tangent of the last residual evaluation; Dirichlet
   // values of du: bc_scale x the problem's (0: homogeneous)
-  auto tangent_solve = [&](double bc_scale) {
+  auto tangent_solve = [&](double bc_scale, double eta) {
     PA_CUDA(cudaMemsetAsync(diag.get(), 0, sizeof(double) * n, s));
     k_j2_diag<<<int((C + 127) / 128), 128, 0, s>>>(P.mesh->d_cells.get(), P.mesh->d_coords.get(), C, q,
                                                   P.mesh->d_cell_iperm.get(), rec64.get(), w64.get(), diag.get());
@@ -508,7 +508,9 @@ pa_status j2_solve(Problem& P, const pa_j2_params& jp, const double* z, const pa
     op.homogeneous_bc = bc_scale == 0.0;
     op.bc_scale = bc_scale;
     pa_solve_stats st{};
-    const pa_status ls = solve_operator(P, op, b.get(), du.get(), lo, &st, true);
+    pa_solve_options lo_k = lo;
+    lo_k.rel_tol = std::max(lo.rel_tol, eta);
+    const pa_status ls = solve_operator(P, op, b.get(), du.get(), lo_k, &st, true);
     cg_total += st.iterations;
     ++newton_total;
     if (ls == PA_ERR_NOT_CONVERGED) ++linear_unconverged;
@@ -532,7 +534,13 @@ pa_status j2_solve(Problem& P, const pa_j2_params& jp, const double* z, const pa
     // predictor (NewtonRaphsonSolver's first iteration, src/NewtonRaphsonSolver.hpp:127-131):
     // residual and tangent at the converged state, the Dirichlet increment imposed in the solve
     residual();
-    status = tangent_solve(s_new - s_old);
+    // inexact Newton (Eisenstat-Walker, choice 2): tangent-solve tolerances
+    // follow the observed reduction of ||R||, so that the early iterations of
+    // a step do not oversolve; 0 keeps the caller's linear tolerance
+    const bool ew = jo.adaptive_forcing != 0;
+    constexpr double kEtaMax = 0.1, kGamma = 0.9;
+    double eta = ew ? kEtaMax : 0.0;
+    status = tangent_solve(s_new - s_old, eta);
     if (status != PA_OK) break;
     add_du(1.0);
     // Newton with a backtracking line search on ||R_free||: when thousands of
@@ -541,12 +549,21 @@ pa_status j2_solve(Problem& P, const pa_j2_params& jp, const double* z, const pa
     // kMaxHalvings times, then the last trial is taken) restores descent.
     constexpr int kMaxHalvings = 5;
     bool converged = false;
-    double rn = residual();
+    double rn = residual(), rn_prev = r0;
     for (int it = 0; it < jo.max_newton; ++it) {
       if (!std::isfinite(rn)) { status = PA_ERR_NONFINITE; break; }
       last_rel = r0 > 0.0 ? rn / r0 : 0.0;
       if (rn <= jo.newton_tol * r0 || rn == 0.0) { converged = true; break; }
-      status = tangent_solve(0.0);
+      if (ew) {
+        const double ratio = rn_prev > 0.0 ? rn / rn_prev : 1.0;
+        double e = kGamma * ratio * ratio;
+        const double guard = kGamma * eta * eta;  // do not tighten abruptly
+        if (guard > 0.1) e = std::max(e, guard);
+        e = std::min(e, kEtaMax);
+        e = std::max(e, 0.5 * jo.newton_tol * r0 / rn);  // no finer than the remaining reduction
+        eta = e;
+      }
+      status = tangent_solve(0.0, eta);
       if (status != PA_OK) break;
       double a = 1.0;
       add_du(a);
@@ -557,6 +574,7 @@ pa_status j2_solve(Problem& P, const pa_j2_params& jp, const double* z, const pa
         rt = residual();
         ++line_search_halvings;
       }
+      rn_prev = rn;
       rn = rt;
     }
     if (status == PA_OK && !converged && std::isfinite(rn)) last_rel = r0 > 0.0 ? rn / r0 : 0.0;
