@@ -48,3 +48,17 @@ def test_no_device_is_reported_not_crashed():
     status = lib.pa_mesh_create_box(2, 2, 2, 1.0, 1.0, 1.0, ctypes.byref(h))
     assert status != _abi.PA_OK
     assert lib.pa_last_error()
+
+
+def test_cpp_headers_compile_against_the_library(tmp_path):
+    """The C++ views of the ABI (include/pa_b200.hpp, include/pa_b200_app.hpp)
+    compile and link against libpa_b200.so without a GPU (running them needs
+    one: tests/test_gpu_cpp_api.py)."""
+    import subprocess
+    libdir = os.path.join(ROOT, "platoanalyze_b200")
+    for src in ("derivative_tests.cpp", "mpmd_app_tests.cpp"):
+        exe = tmp_path / src.replace(".cpp", "")
+        subprocess.check_call(["g++", "-O2", "-std=c++17", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                               os.path.join(ROOT, "tests", "cpp", src), "-o", str(exe), "-L", libdir, "-lpa_b200",
+                               "-Wl,-rpath," + libdir])
+        assert exe.exists()
