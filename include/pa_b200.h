@@ -103,6 +103,16 @@ pa_status pa_mesh_set_graph(pa_mesh* mesh, const int32_t* rowmap, const int32_t*
  * allowed only before problems are created on the mesh. */
 pa_status pa_mesh_uniform_geometry(pa_mesh* mesh, int32_t enable, int32_t* active);
 
+/* Visualisation output: the mesh, the displacement u (3N, interleaved; may be
+ * NULL) and the control (N nodal or C per-cell values by control_layout; may
+ * be NULL) as a VTK XML unstructured grid (.vtu, base64 binary arrays,
+ * tetrahedra) with the reference's field names "Displacements" and "Control"
+ * -- Plato::write / Plato::output through Omega_h's VTK writer
+ * (src/AnalyzeOutput.hpp:469-482).  u and control may be host or device
+ * arrays. */
+pa_status pa_write_vtu(const pa_mesh* mesh, const char* path, const double* u, const double* control,
+                       int32_t control_layout);
+
 /* Boundary faces (triangles, 3 node ids each) lying on the plane
  * coord[axis] == value.  Call with faces == NULL to get the count. */
 pa_status pa_mesh_boundary_faces(const pa_mesh* mesh, int32_t axis, double value, int32_t* faces,

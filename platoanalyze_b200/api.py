@@ -15,6 +15,7 @@ Arrays may be NumPy arrays (host) or torch CUDA tensors (device); results
 come back in the kind of array the first array argument was.
 """
 import ctypes as ct
+import os
 
 import numpy as np
 
@@ -120,6 +121,18 @@ class Mesh:
         C, N, B, T = (ct.c_int64() for _ in range(4))
         _abi.check(self._lib.pa_mesh_sizes(self._h, ct.byref(C), ct.byref(N), ct.byref(B), ct.byref(T)))
         self.num_tiles = T.value
+
+    def write_vtu(self, path, u=None, control=None, control_layout="nodal"):
+        """Write the mesh with the displacement (3N) and the control (N nodal
+        or C per-cell values) as a .vtu file (pa_write_vtu)."""
+        lay = 1 if control_layout == "cell" else 0
+        nz = self.num_cells if lay else self.num_nodes
+        u = None if u is None else _as(u, np.float64)
+        control = None if control is None else _as(control, np.float64)
+        _abi.check(self._lib.pa_write_vtu(self._h, os.fsencode(str(path)),
+                                          None if u is None else _ptr(u, np.float64, 3 * self.num_nodes, "u"),
+                                          None if control is None else _ptr(control, np.float64, nz, "control"),
+                                          lay))
 
     @property
     def uniform_geometry(self):

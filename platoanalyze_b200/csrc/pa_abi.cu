@@ -310,6 +310,15 @@ pa_status pa_mesh_set_graph(pa_mesh* mesh, const int32_t* rowmap, const int32_t*
   });
 }
 
+pa_status pa_write_vtu(const pa_mesh* mesh, const char* path, const double* u, const double* control,
+                       int32_t control_layout) {
+  return guard([&] {
+    PA_CHECK(mesh && path, "null argument");
+    PA_CHECK(control_layout == PA_CONTROL_NODAL || control_layout == PA_CONTROL_CELL, "unknown control layout");
+    pa::write_vtu(mesh->m, path, u, control, control_layout);
+  });
+}
+
 pa_status pa_mesh_boundary_faces(const pa_mesh* mesh, int32_t axis, double value, int32_t* faces,
                                  int64_t* num_faces) {
   return guard([&] {

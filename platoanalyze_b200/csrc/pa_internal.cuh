@@ -150,6 +150,8 @@ struct Mesh {
 };
 
 void mesh_build(Mesh& m);  // tiles + graph + device upload
+// .vtu output of the mesh, u (3N or null) and the control (N or C values, or null)
+void write_vtu(const Mesh& m, const std::string& path, const double* u, const double* control, int control_layout);
 void mesh_rebuild_tiles(Mesh& m);  // tiles only (after a change of parts or tile size)
 
 // ----------------------------------------------------------------- material --
