@@ -216,3 +216,28 @@ def test_fp64_keeps_the_per_tet_geometry_off_rounding_level(pa, oracle_lib):
     prob = pa.Problem(mesh, 1.0, 0.3, 3.0, 1e-9, control_layout="cell")
     assert rel_inf(prob.apply(z, u), ref) < 1e-10
     assert rel_inf(prob.apply(z, u.astype(np.float32)), ref) < 1e-5
+
+
+@pytest.mark.parametrize("tile", [64, 128, 256])
+def test_every_tile_size_with_the_geometry_table(pa, oracle_lib, monkeypatch, tile):
+    """Each tile size is its own kernel instance (shared-memory layout, launch
+    bounds): FP32 and FP64 applies against the oracle, mixed and FP64 solves
+    against each other."""
+    monkeypatch.setenv("PA_TILE_CLUSTERS", str(tile))
+    dims = (12, 6, 5)
+    cells, coords = np_ref.box_mesh(*dims, 12.0, 6.0, 5.0)
+    mesh = pa.Mesh.from_arrays(cells, coords)
+    assert mesh.uniform_geometry
+    O = oracle_lib.Oracle(cells, coords, E=1.0, nu=0.3, p=3.0, pmin=1e-9, layout=1)
+    rng = np.random.default_rng(tile)
+    z = rng.uniform(0.05, 1.0, O.C)
+    u = rng.standard_normal(3 * O.N)
+    ref = O.apply(u, z)
+    prob = pa.Problem(mesh, 1.0, 0.3, 3.0, 1e-9, control_layout="cell")
+    assert rel_inf(prob.apply(z, u), ref) < 1e-10
+    assert rel_inf(prob.apply(z, u.astype(np.float32)), ref) < 1e-5
+    prob, zc = _cantilever(pa, mesh, dims, (1.0, 1.0, 1.0), 7)
+    x64, s64 = prob.solution(zc, options=pa.SolveOptions("fp64", rel_tol=1e-11))
+    xm, sm = prob.solution(zc, options=pa.SolveOptions("mixed", rel_tol=1e-9))
+    assert s64["converged"] and sm["converged"], (s64, sm)
+    assert rel_inf(xm, x64) <= 1e-6
