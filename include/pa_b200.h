@@ -135,7 +135,11 @@ typedef struct {
 } pa_elastic_params;
 
 /* Elliptic mechanics problem on `mesh` (src/elliptic/Problem.hpp:93-114).
- * `stream` is a cudaStream_t (NULL: the library creates its own). */
+ * `stream` is a cudaStream_t.  NULL: the library creates its own blocking
+ * stream, which the legacy default stream orders against in both directions
+ * (device arrays written there before a call are read after them; results
+ * are visible there after the call).  With any other stream the caller
+ * orders its own work against it. */
 pa_status pa_problem_create(pa_mesh* mesh, const pa_elastic_params* params, void* stream, pa_problem** out);
 pa_status pa_problem_destroy(pa_problem* problem);
 

@@ -363,7 +363,10 @@ pa_status pa_problem_create(pa_mesh* mesh, const pa_elastic_params* params, void
     if (stream) {
       P.stream = reinterpret_cast<cudaStream_t>(stream);
     } else {
-      PA_CUDA(cudaStreamCreateWithFlags(&P.stream, cudaStreamNonBlocking));
+      // a blocking stream: ordered against the legacy default stream, so that
+      // a caller working there (e.g. torch's default stream) sees the
+      // library's results, and the library sees the caller's inputs
+      PA_CUDA(cudaStreamCreateWithFlags(&P.stream, cudaStreamDefault));
       P.own_stream = true;
     }
     upload_bcs(P);

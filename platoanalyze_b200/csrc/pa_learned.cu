@@ -611,7 +611,7 @@ LearnedPC* pc_new(int gx, int gy, int gz, uint64_t seed) {
   pc->gy = gy;
   pc->gz = gz;
   pc->G = int64_t(gx) * gy * gz;
-  PA_CUDA(cudaStreamCreateWithFlags(&pc->stream, cudaStreamNonBlocking));
+  PA_CUDA(cudaStreamCreateWithFlags(&pc->stream, cudaStreamDefault));  // ordered against the legacy default stream
   const int64_t np = pc_num_params();
   std::vector<float> h(np, 0.0f);
   std::mt19937_64 rng(seed);

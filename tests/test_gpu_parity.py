@@ -276,3 +276,27 @@ def test_j2_radial_return(pa, oracle_lib, setup):
     if C > 6:
         assert (~plastic).any()
     assert np.abs(got - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max())
+
+
+def test_library_stream_is_ordered_with_torchs_default_stream(pa, oracle_lib):
+    """A problem created without a stream works on a blocking stream: device
+    inputs that torch writes on its default stream just before a call are read
+    after they land, and the results are complete when torch reads them."""
+    import torch
+    cells, coords = perturbed_box(8, 5, 4, 11)
+    O = oracle_lib.Oracle(cells, coords, E=1.0, nu=0.3, p=3.0, pmin=1e-9, layout=1)
+    mesh = pa.Mesh.from_arrays(cells, coords)
+    prob = pa.Problem(mesh, 1.0, 0.3, 3.0, 1e-9, control_layout="cell")
+    rng = np.random.default_rng(5)
+    z = rng.uniform(0.1, 1.0, O.C)
+    u = rng.standard_normal(3 * O.N)
+    ref = O.apply(u, z)
+    zt = torch.tensor(z, device="cuda")
+    for _ in range(3):
+        ut = torch.zeros(3 * O.N, dtype=torch.float64, device="cuda")
+        big = torch.randn(4096, 4096, device="cuda")
+        for _ in range(8):
+            big = (big @ big) * 1e-4  # keeps the default stream busy
+        ut.copy_(torch.tensor(u), non_blocking=False)
+        y = prob.apply(zt, ut)
+        assert rel_inf(y.cpu().numpy(), ref) < RTOL64
