@@ -13,19 +13,23 @@
 //
 // Kernel: a persistent grid (a multiple of the SM count) walks the tiles.  For
 // each tile the CTA
-//  1. has the tile's data already in shared memory: node coordinates and
-//     input vectors (gathered through the tile's sorted node list), cluster
-//     records and penalty weights -- all brought in by cp.async while the
-//     previous tile was computing (two buffers), so the gathers' latency is
-//     hidden behind arithmetic;
+//  1. has the tile's data already in shared memory: input vectors (gathered
+//     through the tile's sorted node list), node coordinates (unless the mesh
+//     has the uniform hex geometry table, below), cluster records and penalty
+//     weights -- brought in by cp.async while the previous tile was computing
+//     (two data buffers; tile headers and node-id lists run further ahead), so
+//     the gathers' latency is hidden behind arithmetic;
 //  2. forms the input vector (PCG mode: p = D^-1 r + beta p_old, masked; the
 //     owner tile writes p once);
 //  3. one thread per cluster: reads the cluster's nodes from shared memory into
 //     registers once, evaluates its tets (geometry, strain, stress, SIMP
-//     weight, divergence), accumulates node sums in registers and adds them to
-//     the tile's shared sums -- 24 shared atomics per 6 tets;
+//     weight, divergence) and accumulates 8 node sums in registers.  With the
+//     geometry table (GEO: every hex a translate of the first) the per-tet
+//     geometry comes from the kernel's parameter block, and the node sums go
+//     to shared memory slot by slot without atomics (a slot's nodes are
+//     distinct across a tile's hexes); otherwise 24 shared atomics per hex;
 //  4. writes each node sum once: a plain store for nodes only this tile
-//     touches, a global atomic add for nodes shared with other tiles.
+//     touches, a `red.global.add` for nodes shared with other tiles.
 // PCG mode also reduces p.Kp = sum_cells p_e^T K_e p_e from the per-tet
 // energies; the last CTA to finish turns it into alpha.
 #pragma once
