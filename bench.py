@@ -39,11 +39,13 @@ FALLBACK_HBM_GBS = 6650.0
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--dims", default="160x80x80")
-    ap.add_argument("--method", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--method", default="mg", choices=["mg", "mixed", "fp64"],
+                    help="mg: CG with a geometric multigrid V-cycle (FP32 smoothing); mixed: Jacobi-PCG, FP32 apply; "
+                         "fp64: Jacobi-PCG in FP64")
     ap.add_argument("--rel-tol", type=float, default=1e-8)
     ap.add_argument("--check-every", type=int, default=64,
                     help="iterations between FP64 residual replacements (one captured graph chunk)")
@@ -324,6 +326,12 @@ def profile_kernel(args):
                                                 ct.byref(nb)))
         out[name] = {"ms_per_launch": ms.value, "GB/s": nb.value / (ms.value * 1e-3) / 1e9,
                      "algorithmic_bytes": nb.value}
+    # the plain FP32 apply (multigrid smoothing) after the fused ones
+    ms, nb = ct.c_double(), ct.c_int64()
+    _abi.check(_abi.load().pa_time_apply(prob._h, ct.c_void_p(z.data_ptr()), 1, args.reps, ct.byref(ms),
+                                         ct.byref(nb)))
+    out["fp32_plain"] = {"ms_per_launch": ms.value, "GB/s": nb.value / (ms.value * 1e-3) / 1e9,
+                         "algorithmic_bytes": nb.value}
     print(json.dumps(out), flush=True)
     return 0
 
@@ -400,23 +408,37 @@ def run_ours(args):
     e2e_value = whole_job_rate(world, C, args.steps, max_over_ranks(e2e_ms, world))
     rel_u = float(np.abs(u_pin.numpy() - u.cpu().numpy()).max() / max(np.abs(u.cpu().numpy()).max(), 1e-300))
 
-    # plain FP64 Jacobi-PCG on the same system (the comparison the metric names)
+    # plain FP64 Jacobi-PCG on the same system (the comparison the metric names),
+    # and the mixed Jacobi-PCG when it is not the timed method
     fp64 = pa.SolveOptions("fp64", rel_tol=args.rel_tol)
     u64 = torch.empty_like(u)
     _, st64 = prob.solution(z, u64, options=fp64)
     f_mixed = prob.scalar_function().value(u, z)
     f_fp64 = prob.scalar_function().value(u64, z)
+    st_jacobi = None
+    if args.method == "mg":
+        _, st_jacobi = prob.solution(z, u64, options=pa.SolveOptions("mixed", rel_tol=args.rel_tol,
+                                                                     check_every=args.check_every))
 
-    # roofline of the dominant kernel (fused CG apply) timed live on this stream
-    precision = 1 if args.method == "mixed" else 0
+    # roofline of the dominant kernel timed live on this stream: the plain
+    # FP32 apply of the multigrid smoother, or the fused CG apply of Jacobi-PCG
     import ctypes as ct
     from platoanalyze_b200 import _abi
     ms_launch, nbytes = ct.c_double(), ct.c_int64()
-    _abi.check(_abi.load().pa_time_cg_apply(prob._h, ct.c_void_p(z.data_ptr()), precision, 50, ct.byref(ms_launch),
-                                            ct.byref(nbytes)))
+    if args.method == "mg":
+        precision = 1
+        kernel = "k_apply_tiled (plain FP32 apply: multigrid smoothing and residuals)"
+        _abi.check(_abi.load().pa_time_apply(prob._h, ct.c_void_p(z.data_ptr()), precision, 50, ct.byref(ms_launch),
+                                             ct.byref(nbytes)))
+        tag = f"k_apply_tiled_plain_fp32_{dims[0]}x{dims[1]}x{dims[2]}"
+    else:
+        precision = 1 if args.method == "mixed" else 0
+        kernel = "k_apply_tiled (fused CG: p update + K p + p.Kp)"
+        _abi.check(_abi.load().pa_time_cg_apply(prob._h, ct.c_void_p(z.data_ptr()), precision, 50,
+                                                ct.byref(ms_launch), ct.byref(nbytes)))
+        tag = f"k_apply_tiled_{'fp32' if precision else 'fp64'}_{dims[0]}x{dims[1]}x{dims[2]}"
     peak, peak_kind = peaks()
     achieved = nbytes.value / (ms_launch.value * 1e-3) / 1e9
-    tag = f"k_apply_tiled_{'fp32' if precision else 'fp64'}_{dims[0]}x{dims[1]}x{dims[2]}"
     traffic = traffic_from_profiles(f"{tag}_tile{tile}")
     if traffic is None:
         traffic = traffic_from_profiles(tag)
@@ -429,21 +451,27 @@ def run_ours(args):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32 apply / f64 dots+refinement" if args.method == "mixed" else "f64",
+        "dtype": {"mixed": "f32 apply / f64 dots+refinement", "fp64": "f64",
+                  "mg": "f64 CG + apply / f32 multigrid smoothing"}[args.method],
         "data": "synthetic (seeded smoothed density field)",
         "config": {"workload": f"SIMP cantilever {dims[0]}x{dims[1]}x{dims[2]} hex x 6 tets, "
                                f"Problem::solution to relres {args.rel_tol:g}",
                    "cells": C, "nodes": N, "dofs": ndof, "method": args.method, "parallelism": f"replicas x{world}",
+                   "preconditioner": ("geometric multigrid V-cycle: box hierarchy to the coarsest even level, "
+                                      "Chebyshev(2) smoothing in D^-1 K, Chebyshev(40) coarsest, trilinear transfers")
+                   if args.method == "mg" else "Jacobi",
                    "tile_clusters": tile, "autotune_ms_per_apply": tile_ms,
                    "geometry": "hex geometry table (uniform hexes)" if mesh.uniform_geometry else "per tet",
                    "l2": "256 MB buffer written between timed steps"},
         "solve_s": max_ms / args.steps * 1e-3, "iterations": iters, "fp64_solve_s": st64["seconds"],
         "fp64_iterations": st64["iterations"], "compliance_rel_err_vs_fp64": abs(f_mixed - f_fp64) / abs(f_fp64),
+        "jacobi_mixed_solve_s": st_jacobi["seconds"] if st_jacobi else None,
+        "jacobi_mixed_iterations": st_jacobi["iterations"] if st_jacobi else None,
         "gpu_launches": launches,
         "clocks": clk,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * C, "d2h_bytes_per_step": 8 * ndof,
                 "max_rel_diff_u_vs_device_run": rel_u},
-        "roofline": {"bound": "hbm", "kernel": "k_apply_tiled (fused CG: p update + K p + p.Kp)",
+        "roofline": {"bound": "hbm", "kernel": kernel,
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind, "traffic": traffic, "algorithmic_bytes_per_launch": nbytes.value,
                      "ms_per_launch": ms_launch.value},

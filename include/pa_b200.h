@@ -226,6 +226,8 @@ pa_status pa_apply_block_constraints(pa_problem* problem, double* entries, doubl
 
 #define PA_SOLVER_PCG_FP64 0  /* matrix-free Jacobi-PCG, FP64 throughout */
 #define PA_SOLVER_PCG_MIXED 1 /* FP32 apply/vectors, FP64 dots, FP64 true-residual updates */
+#define PA_SOLVER_PCG_MG 3    /* FP64 CG preconditioned by a geometric multigrid V-cycle (FP32 Chebyshev
+                                 smoothing); box meshes from pa_mesh_create_box with even hex counts */
 #define PA_SOLVER_FCG_LEARNED 2 /* flexible CG preconditioned by the problem's learned network
                                    (pa_problem_set_preconditioner), precision as PA_SOLVER_PCG_MIXED;
                                    continues as PA_SOLVER_PCG_MIXED when the residual stalls or the
@@ -275,6 +277,12 @@ pa_status pa_problem_criterion_gradient(pa_problem* problem, const double* z, co
  * C*(16 + s) + N*6*3*s, s = 4 (PA_FP32) or 8 (PA_FP64). */
 pa_status pa_time_cg_apply(pa_problem* problem, const double* z, int32_t precision, int32_t reps,
                            double* ms_per_launch, int64_t* algorithmic_bytes);
+
+/* Diagnostic, no reference counterpart: the same for the plain constrained
+ * apply y = K x (the multigrid smoother's kernel, VectorFunction::value's
+ * stiffness part), algorithmic bytes C*(16 + s) + N*3*3*s. */
+pa_status pa_time_apply(pa_problem* problem, const double* z, int32_t precision, int32_t reps,
+                        double* ms_per_launch, int64_t* algorithmic_bytes);
 
 /* ---------------------------------------------------------- J2 return ---- */
 

@@ -18,7 +18,7 @@ STATUS_NAMES = {0: "PA_OK", 1: "PA_ERR_INVALID_ARG", 2: "PA_ERR_CUDA", 3: "PA_ER
                 4: "PA_ERR_BREAKDOWN", 5: "PA_ERR_NONFINITE", 6: "PA_ERR_NO_DEVICE", 7: "PA_ERR_UNSUPPORTED"}
 PA_CONTROL_NODAL, PA_CONTROL_CELL = 0, 1
 PA_FP64, PA_FP32 = 0, 1
-PA_SOLVER_PCG_FP64, PA_SOLVER_PCG_MIXED, PA_SOLVER_FCG_LEARNED = 0, 1, 2
+PA_SOLVER_PCG_FP64, PA_SOLVER_PCG_MIXED, PA_SOLVER_FCG_LEARNED, PA_SOLVER_PCG_MG = 0, 1, 2, 3
 
 
 class ElasticParams(ct.Structure):
@@ -100,6 +100,7 @@ SIGNATURES = [
     ("pa_problem_solution", I32, [P, P, P, ct.POINTER(SolveOptions), ct.POINTER(SolveStats)]),
     ("pa_problem_criterion_gradient", I32, [P, P, P, P, I32, ct.POINTER(SolveOptions)]),
     ("pa_time_cg_apply", I32, [P, P, I32, I32, P, P]),
+    ("pa_time_apply", I32, [P, P, I32, I32, P, P]),
     ("pa_j2_radial_return", I32, [P, ct.POINTER(J2Params), P, P, P, P]),
     ("pa_j2_local_residual", I32, [P, ct.POINTER(J2Params), P, P, P, P, P]),
     ("pa_j2_solve", I32, [P, ct.POINTER(J2Params), P, ct.POINTER(J2SolveOptions), ct.POINTER(SolveOptions), P, P,

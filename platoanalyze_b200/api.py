@@ -177,7 +177,7 @@ class SolveOptions:
         o = _abi.SolveOptions()
         _abi.load().pa_solve_options_default(ct.byref(o))
         o.method = {"fp64": _abi.PA_SOLVER_PCG_FP64, "mixed": _abi.PA_SOLVER_PCG_MIXED,
-                    "learned": _abi.PA_SOLVER_FCG_LEARNED}[self.method]
+                    "learned": _abi.PA_SOLVER_FCG_LEARNED, "mg": _abi.PA_SOLVER_PCG_MG}[self.method]
         o.rel_tol = float(self.rel_tol)
         o.max_iters = int(self.max_iters)
         o.check_every = int(self.check_every)

@@ -20,6 +20,7 @@ void launch_scale(double* v, int64_t n, double a, cudaStream_t s);
 void launch_gradient_x(const Problem& P, const double* u, const double* z, double* entries, cudaStream_t s);
 void launch_energy_grad_x(const Problem& P, const double* u, const double* z, double* gx, cudaStream_t s);
 double time_cg_apply(Problem& P, const double* z, bool fp32, int reps);
+double time_apply(Problem& P, const double* z, bool fp32, int reps);
 void launch_j2_local_residual(const Problem& P, const pa_j2_params& jp, const double* u, const double* z,
                               const double* loc, const double* prev, double* H, cudaStream_t s);
 pa_status j2_solve(Problem& P, const pa_j2_params& jp, const double* z, const pa_j2_solve_options& jo,
@@ -217,35 +218,8 @@ pa_status pa_mesh_create_box(int32_t nx, int32_t ny, int32_t nz, double lx, doub
     PA_CHECK(nx > 0 && ny > 0 && nz > 0, "box needs positive hex counts");
     PA_CHECK(lx > 0 && ly > 0 && lz > 0, "box needs positive lengths");
     pa::require_device();
-    static const int tet[6][4][3] = {
-        {{0, 0, 0}, {1, 1, 0}, {0, 1, 0}, {1, 1, 1}}, {{0, 0, 0}, {0, 1, 0}, {0, 1, 1}, {1, 1, 1}},
-        {{0, 0, 0}, {0, 1, 1}, {0, 0, 1}, {1, 1, 1}}, {{0, 0, 0}, {1, 0, 1}, {1, 1, 1}, {0, 0, 1}},
-        {{1, 0, 0}, {1, 0, 1}, {1, 1, 1}, {0, 0, 0}}, {{1, 0, 0}, {1, 1, 1}, {1, 1, 0}, {0, 0, 0}}};
     std::unique_ptr<pa_mesh> h(new pa_mesh());
-    pa::Mesh& m = h->m;
-    const int64_t px = nx + 1, py = ny + 1;
-    m.N = px * py * int64_t(nz + 1);
-    m.C = 6LL * nx * ny * nz;
-    m.coords.resize(3 * m.N);
-    m.cells.resize(4 * m.C);
-    for (int64_t k = 0; k <= nz; ++k)
-      for (int64_t j = 0; j <= ny; ++j)
-        for (int64_t i = 0; i <= nx; ++i) {
-          const int64_t v = i + px * (j + py * k);
-          m.coords[3 * v + 0] = lx * double(i) / nx;
-          m.coords[3 * v + 1] = ly * double(j) / ny;
-          m.coords[3 * v + 2] = lz * double(k) / nz;
-        }
-    int64_t c = 0;
-    for (int64_t k = 0; k < nz; ++k)
-      for (int64_t j = 0; j < ny; ++j)
-        for (int64_t i = 0; i < nx; ++i)
-          for (int t = 0; t < 6; ++t, ++c)
-            for (int n = 0; n < 4; ++n) {
-              const int* o = tet[t][n];
-              m.cells[4 * c + n] = int32_t((i + o[0]) + px * ((j + o[1]) + py * (k + o[2])));
-            }
-    pa::mesh_build(m);
+    pa::mesh_make_box(h->m, nx, ny, nz, lx, ly, lz);
     *out = h.release();
   });
 }
@@ -386,6 +360,7 @@ pa_status pa_problem_destroy(pa_problem* problem) {
     if (P.ev1) cudaEventDestroy(P.ev1);
     cudaStream_t s = P.own_stream ? P.stream : nullptr;
     pa_pc* pc = problem->pc;
+    pa::mg_release(P);
     delete problem;
     if (s) cudaStreamDestroy(s);
     mh->m.live_problems -= 1;
@@ -684,6 +659,24 @@ pa_status pa_j2_radial_return(pa_problem* problem, const pa_j2_params* params, c
     const double* dp = st.in(prev_local, 14 * P.C(), "prev_local");
     double* dl = st.out(local, 14 * P.C(), "local");
     pa::launch_j2(P, *params, du, dz, dp, dl, P.stream);
+    st.finish();
+  });
+}
+
+pa_status pa_time_apply(pa_problem* problem, const double* z, int32_t precision, int32_t reps,
+                        double* ms_per_launch, int64_t* algorithmic_bytes) {
+  return guard([&] {
+    Problem& P = prob(problem);
+    PA_CHECK(precision == PA_FP64 || precision == PA_FP32, "precision must be PA_FP64 or PA_FP32");
+    PA_CHECK(reps > 0 && ms_per_launch, "need reps > 0 and an output");
+    pa::Stage st(P);
+    const double* dz = st.in(z, P.nz(), "z");
+    *ms_per_launch = pa::time_apply(P, dz, precision == PA_FP32, reps);
+    if (algorithmic_bytes) {
+      const int64_t sv = precision == PA_FP32 ? 4 : 8;
+      // cells: 4 int32 node ids + penalty weight; nodes: coords, x in, y out
+      *algorithmic_bytes = P.C() * (16 + sv) + P.N() * (3 * sv) * 3;
+    }
     st.finish();
   });
 }

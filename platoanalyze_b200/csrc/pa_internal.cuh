@@ -127,6 +127,9 @@ struct Mesh {
   HexGeo<double> geo64{};
   HexGeo<float> geo32{};
   int tile_clusters = 128;  // clusters per tile (threads per CTA); a tile touches <= 2x as many nodes
+  // structured box (mesh_make_box): hex counts and lengths; 0 for other meshes
+  int box_n[3] = {0, 0, 0};
+  double box_l[3] = {0.0, 0.0, 0.0};
   DevBuf<int32_t> d_tile_cluster_start, d_tile_cell_start, d_tile_hex_count, d_tile_node_start, d_cell_perm;
   DevBuf<int32_t> d_cell_iperm;  // user -> internal cell id
   DevBuf<uint32_t> d_tile_nodes;
@@ -150,6 +153,9 @@ struct Mesh {
 };
 
 void mesh_build(Mesh& m);  // tiles + graph + device upload
+// Structured box [0,lx]x[0,ly]x[0,lz] of nx*ny*nz hexes x 6 tets (nodes and
+// hexes numbered x fastest), then mesh_build.
+void mesh_make_box(Mesh& m, int nx, int ny, int nz, double lx, double ly, double lz);
 // .vtu output of the mesh, u (3N or null) and the control (N or C values, or null)
 void write_vtu(const Mesh& m, const std::string& path, const double* u, const double* control, int control_layout);
 void mesh_rebuild_tiles(Mesh& m);  // tiles only (after a change of parts or tile size)

@@ -431,6 +431,42 @@ void mesh_rebuild_tiles(Mesh& m) {
   PA_CUDA(cudaDeviceSynchronize());
 }
 
+void mesh_make_box(Mesh& m, int nx, int ny, int nz, double lx, double ly, double lz) {
+  static const int tet[6][4][3] = {
+      {{0, 0, 0}, {1, 1, 0}, {0, 1, 0}, {1, 1, 1}}, {{0, 0, 0}, {0, 1, 0}, {0, 1, 1}, {1, 1, 1}},
+      {{0, 0, 0}, {0, 1, 1}, {0, 0, 1}, {1, 1, 1}}, {{0, 0, 0}, {1, 0, 1}, {1, 1, 1}, {0, 0, 1}},
+      {{1, 0, 0}, {1, 0, 1}, {1, 1, 1}, {0, 0, 0}}, {{1, 0, 0}, {1, 1, 1}, {1, 1, 0}, {0, 0, 0}}};
+  const int64_t px = nx + 1, py = ny + 1;
+  m.N = px * py * int64_t(nz + 1);
+  m.C = 6LL * nx * ny * nz;
+  m.coords.resize(3 * m.N);
+  m.cells.resize(4 * m.C);
+  for (int64_t k = 0; k <= nz; ++k)
+    for (int64_t j = 0; j <= ny; ++j)
+      for (int64_t i = 0; i <= nx; ++i) {
+        const int64_t v = i + px * (j + py * k);
+        m.coords[3 * v + 0] = lx * double(i) / nx;
+        m.coords[3 * v + 1] = ly * double(j) / ny;
+        m.coords[3 * v + 2] = lz * double(k) / nz;
+      }
+  int64_t c = 0;
+  for (int64_t k = 0; k < nz; ++k)
+    for (int64_t j = 0; j < ny; ++j)
+      for (int64_t i = 0; i < nx; ++i)
+        for (int t = 0; t < 6; ++t, ++c)
+          for (int n = 0; n < 4; ++n) {
+            const int* o = tet[t][n];
+            m.cells[4 * c + n] = int32_t((i + o[0]) + px * ((j + o[1]) + py * (k + o[2])));
+          }
+  m.box_n[0] = nx;
+  m.box_n[1] = ny;
+  m.box_n[2] = nz;
+  m.box_l[0] = lx;
+  m.box_l[1] = ly;
+  m.box_l[2] = lz;
+  mesh_build(m);
+}
+
 void mesh_build(Mesh& m) {
   PA_CHECK(m.C > 0 && m.N > 0, "mesh needs at least one cell and one node");
   PA_CHECK(m.N <= int64_t(kNodeIdMask), "too many nodes for 27-bit node ids");

@@ -37,10 +37,12 @@ struct SolveOperator {
 };
 
 struct LearnedPC;
+struct MgHierarchy;
 
 struct Problem {
   Mesh* mesh = nullptr;
   LearnedPC* pc = nullptr;  // network of PA_SOLVER_FCG_LEARNED (not owned)
+  MgHierarchy* mg = nullptr;  // coarse levels of PA_SOLVER_PCG_MG (owned; mg_release)
   ElasticParams ep{};
   cudaStream_t stream = nullptr;
   bool own_stream = false;
@@ -76,5 +78,9 @@ struct Problem {
 
 pa_status solve_batched(Problem& P, const SolveOperator& op, const double* b, double* x_out,
                         const pa_solve_options& o, pa_solve_stats* st);
+// multigrid-preconditioned CG on box meshes (pa_mg.cu)
+pa_status solve_mg(Problem& P, const SolveOperator& op, const double* b, double* x_out, const pa_solve_options& o,
+                   pa_solve_stats* st);
+void mg_release(Problem& P);
 
 }  // namespace pa

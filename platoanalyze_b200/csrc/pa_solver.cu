@@ -1010,12 +1010,34 @@ pa_status solve_device(Problem& P, const double* z, const double* b, double* x_o
     return status;
   }
   const bool mixed = o.method == PA_SOLVER_PCG_MIXED;
+  const bool mg = o.method == PA_SOLVER_PCG_MG;
   const int64_t n = P.ndof();
   const int grid_need = std::max(std::max(fused_apply_grid<double>(*P.mesh), fused_apply_grid<float>(*P.mesh)),
                                 vec_grid(n));
-  P.ws.ensure(n, P.C(), grid_need, mixed);
+  P.ws.ensure(n, P.C(), grid_need, mixed || mg);
   SolverWorkspace& ws = P.ws;
   if (!P.ev0) { PA_CUDA(cudaEventCreate(&P.ev0)); PA_CUDA(cudaEventCreate(&P.ev1)); }
+  if (mg) {
+    PA_CHECK(P.mesh->num_parts == 1, "PA_SOLVER_PCG_MG solves one box (not a parted mesh)");
+    cudaEvent_t t0;
+    PA_CUDA(cudaEventCreate(&t0));
+    PA_CUDA(cudaEventRecord(t0, P.stream));
+    launch_cell_weights(P, z, ws.w64.get(), ws.w32.get(), P.stream);
+    launch_diag(P, ws.w64.get(), ws.diag.get(), P.stream);
+    SolveOperator op;
+    op.w64 = ws.w64.get();
+    op.w32 = ws.w32.get();
+    op.diag_aos = ws.diag.get();
+    pa_status status = solve_mg(P, op, b, x_out, o, st);
+    float ms = 0.f;
+    PA_CUDA(cudaEventElapsedTime(&ms, t0, P.ev1));
+    cudaEventDestroy(t0);
+    if (st) {
+      st->kernel_launches += 2;
+      st->seconds = ms * 1e-3;  // weights, diagonal and the hierarchy's set-up included
+    }
+    return status;
+  }
   if (mixed && P.mesh->num_parts > 1) {
     // parted mesh: one independent CG per part
     cudaEvent_t t0;
@@ -1100,6 +1122,51 @@ double time_cg_apply(Problem& P, const double* z, bool fp32, int reps) {
     for (int i = 0; i < reps; ++i) launch_apply_kernel<double, 1>(*P.mesh, ag, s, i % 2 ? a : b);
     PA_CUDA(cudaEventRecord(P.ev1, s));
   }
+  PA_LAUNCHED();
+  PA_CUDA(cudaEventSynchronize(P.ev1));
+  PA_CUDA(cudaEventElapsedTime(&ms, P.ev0, P.ev1));
+  return double(ms) / reps;
+}
+
+// Average device time (ms) of the plain constrained apply y = K x (the tile
+// kernel in its plain mode, as the multigrid smoother launches it) over
+// `reps` back-to-back launches; y accumulates across launches (values are
+// not used, only the time).
+double time_apply(Problem& P, const double* z, bool fp32, int reps) {
+  cudaStream_t s = P.stream;
+  const int64_t n = P.ndof();
+  const int grid_need = std::max(std::max(fused_apply_grid<double>(*P.mesh), fused_apply_grid<float>(*P.mesh)),
+                                vec_grid(n));
+  P.ws.ensure(n, P.C(), grid_need, true);
+  SolverWorkspace& ws = P.ws;
+  launch_cell_weights(P, z, ws.w64.get(), ws.w32.get(), s);
+  if (!P.ev0) { PA_CUDA(cudaEventCreate(&P.ev0)); PA_CUDA(cudaEventCreate(&P.ev1)); }
+  float ms = 0.f;
+  auto run = [&](auto* x, auto* y, const auto* w, const auto* coords) {
+    using T = std::remove_const_t<std::remove_pointer_t<decltype(x)>>;
+    std::vector<T> ones(n, T(1));
+    PA_CUDA(cudaMemcpyAsync(x, ones.data(), sizeof(T) * n, cudaMemcpyHostToDevice, s));
+    PA_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * n, s));
+    ApplyArgs<T> a{};
+    a.tv = P.mesh->tiles();
+    a.tile_nodes = P.d_tile_nodes_bc.get();
+    a.N = P.N();
+    a.coords = coords;
+    a.w = w;
+    const Iso<double> i64 = P.ep.iso();
+    a.iso = Iso<T>{T(i64.lam), T(i64.mu)};
+    a.x = x;
+    a.y = y;
+    const int grid = apply_kernel_setup<T, 0>(*P.mesh);
+    launch_apply_kernel<T, 0>(*P.mesh, grid, s, a);  // warm
+    PA_CUDA(cudaEventRecord(P.ev0, s));
+    for (int i = 0; i < reps; ++i) launch_apply_kernel<T, 0>(*P.mesh, grid, s, a);
+    PA_CUDA(cudaEventRecord(P.ev1, s));
+  };
+  if (fp32)
+    run(ws.r32.get(), ws.ap32.get(), static_cast<const float*>(ws.w32.get()), static_cast<const float*>(P.mesh->d_coords32_soa.get()));
+  else
+    run(ws.r.get(), ws.ap.get(), static_cast<const double*>(ws.w64.get()), static_cast<const double*>(P.mesh->d_coords_soa.get()));
   PA_LAUNCHED();
   PA_CUDA(cudaEventSynchronize(P.ev1));
   PA_CUDA(cudaEventElapsedTime(&ms, P.ev0, P.ev1));
