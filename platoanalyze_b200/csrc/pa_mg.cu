@@ -178,10 +178,15 @@ __global__ void k_mg_scale_norm(int64_t n, const float* __restrict__ x, const fl
 __global__ void k_mg_norm2(int64_t n, const float* __restrict__ x, double* __restrict__ acc);
 
 
-__global__ void k_mg_scale(int64_t n, float* __restrict__ x, float s) {
+// x *= 1 / sqrt(*norm2) (a zero or non-finite norm leaves x unchanged)
+__global__ void k_mg_scale_dev(int64_t n, float* __restrict__ x, const double* __restrict__ norm2) {
+  const double q = *norm2;
+  if (!(q > 0.0) || !isfinite(q)) return;
+  const float sc = float(1.0 / sqrt(q));
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
-    x[i] *= s;
+    x[i] *= sc;
 }
+
 
 // deterministic zero-mean start vector in [-1, 1], masked
 __global__ void k_mg_seed(int64_t N, const uint8_t* __restrict__ mask, float* __restrict__ x) {
@@ -224,14 +229,6 @@ __global__ void k_mg_dot(int64_t n, const double* __restrict__ a, const double* 
     s += a[i] * b[i];
   block_add(s, acc);
 }
-// x += a p; r -= a q
-__global__ void k_mg_xr(int64_t n, double a, const double* __restrict__ p, const double* __restrict__ q,
-                        double* __restrict__ x, double* __restrict__ r) {
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-    x[i] += a * p[i];
-    r[i] -= a * q[i];
-  }
-}
 // y = dinv * x (power iteration), plus ||y||^2 into acc
 __global__ void k_mg_scale_norm(int64_t n, const float* __restrict__ x, const float* __restrict__ dinv,
                                 float* __restrict__ y, double* __restrict__ acc) {
@@ -251,11 +248,37 @@ __global__ void k_mg_norm2(int64_t n, const float* __restrict__ x, double* __res
   block_add(s, acc);
 }
 
-// p = z + beta p
-__global__ void k_mg_p(int64_t n, double beta, const double* __restrict__ z, double* __restrict__ p) {
+// sc = {rz, pq, rr, rz_new, alpha, beta, breakdown}
+__global__ void k_mg_alpha(double* sc) {
+  const double pq = sc[1];
+  if (!(pq > 0.0) || !isfinite(pq)) {
+    sc[4] = 0.0;
+    sc[6] = 1.0;
+  } else {
+    sc[4] = sc[0] / pq;
+  }
+}
+__global__ void k_mg_beta(double* sc) {
+  sc[5] = sc[3] / sc[0];
+  sc[0] = sc[3];
+}
+// x += alpha p; r -= alpha q (alpha on the device)
+__global__ void k_mg_xr_dev(int64_t n, const double* __restrict__ sc, const double* __restrict__ p,
+                            const double* __restrict__ q, double* __restrict__ x, double* __restrict__ r) {
+  const double a = sc[4];
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    x[i] += a * p[i];
+    r[i] -= a * q[i];
+  }
+}
+// p = z + beta p (beta on the device)
+__global__ void k_mg_p_dev(int64_t n, const double* __restrict__ sc, const double* __restrict__ z,
+                           double* __restrict__ p) {
+  const double beta = sc[5];
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
     p[i] = z[i] + beta * p[i];
 }
+
 // out = mask ? 0 : a - b   (SoA; b may be null)
 __global__ void k_mg_res64(int64_t N, const double* __restrict__ a, const double* __restrict__ b,
                            const uint8_t* __restrict__ mask, double* __restrict__ out) {
@@ -429,43 +452,43 @@ void mg_setup(Problem& P, const double* w64, const float* w32, const double* dia
     PA_LAUNCHED();
     g_launches += 1;
   }
-  // lmax of D^-1 K per level: power iteration
-  DevBuf<double> acc(1);
-  for (size_t l = 0; l < H.L.size(); ++l) {
+  // lmax of D^-1 K per level: power iteration, all on the device (each
+  // step's squared norm lands in norms[level][step]; the scaling kernel reads
+  // it there), one host read for every level at the end
+  constexpr int kPower = 20;
+  const size_t NL = H.L.size();
+  DevBuf<double> norms(NL * (kPower + 1));
+  PA_CUDA(cudaMemsetAsync(norms.get(), 0, sizeof(double) * NL * (kPower + 1), s));
+  for (size_t l = 0; l < NL; ++l) {
     MgLevel& L = *H.L[l];
     const float* lw32 = l == 0 ? w32 : L.w32.get();
     const int64_t n3 = 3 * L.N;
+    double* nl = norms.get() + l * (kPower + 1);
     k_mg_seed<<<grid_of(n3), kT, 0, s>>>(L.N, L.P->d_node_mask.get(), L.x.get());
+    k_mg_norm2<<<grid_of(n3), kT, 0, s>>>(n3, L.x.get(), nl);
+    k_mg_scale_dev<<<grid_of(n3), kT, 0, s>>>(n3, L.x.get(), nl);  // unit start vector
     PA_LAUNCHED();
-    {  // unit start vector
-      PA_CUDA(cudaMemsetAsync(acc.get(), 0, sizeof(double), s));
-      k_mg_norm2<<<grid_of(n3), kT, 0, s>>>(n3, L.x.get(), acc.get());
-      PA_LAUNCHED();
-      double h0 = 0.0;
-      PA_CUDA(cudaMemcpyAsync(&h0, acc.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
-      PA_CUDA(cudaStreamSynchronize(s));
-      PA_CHECK(h0 > 0.0, "multigrid level without free dofs");
-      k_mg_scale<<<grid_of(n3), kT, 0, s>>>(n3, L.x.get(), float(1.0 / std::sqrt(h0)));
-      PA_LAUNCHED();
-    }
     g_launches += 3;
-    double lam = 0.0;
-    for (int it = 0; it < 20; ++it) {
+    for (int it = 1; it <= kPower; ++it) {
       launch_apply_tiled<float>(*L.P, lw32, L.x.get(), L.ad.get(), true, s);
-      PA_CUDA(cudaMemsetAsync(acc.get(), 0, sizeof(double), s));
-      k_mg_scale_norm<<<grid_of(n3), kT, 0, s>>>(n3, L.ad.get(), L.dinv.get(), L.x.get(), acc.get());
-      PA_LAUNCHED();
-      double h = 0.0;
-      PA_CUDA(cudaMemcpyAsync(&h, acc.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
-      PA_CUDA(cudaStreamSynchronize(s));
-      const double nrm = std::sqrt(h);
-      if (!(nrm > 0.0) || !std::isfinite(nrm)) break;
-      lam = std::max(lam, nrm);  // ||D^-1 K x|| with ||x|| = 1 approaches lmax from below
-      k_mg_scale<<<grid_of(n3), kT, 0, s>>>(n3, L.x.get(), float(1.0 / nrm));
+      k_mg_scale_norm<<<grid_of(n3), kT, 0, s>>>(n3, L.ad.get(), L.dinv.get(), L.x.get(), nl + it);
+      k_mg_scale_dev<<<grid_of(n3), kT, 0, s>>>(n3, L.x.get(), nl + it);
       PA_LAUNCHED();
       g_launches += 3;
     }
-    L.lmax = float(lam);
+  }
+  std::vector<double> h(NL * (kPower + 1));
+  PA_CUDA(cudaMemcpyAsync(h.data(), norms.get(), sizeof(double) * h.size(), cudaMemcpyDeviceToHost, s));
+  PA_CUDA(cudaStreamSynchronize(s));
+  for (size_t l = 0; l < NL; ++l) {
+    PA_CHECK(h[l * (kPower + 1)] > 0.0, "multigrid level without free dofs");
+    double lam = 0.0;  // ||D^-1 K x|| with ||x|| = 1 approaches lmax from below
+    for (int it = 1; it <= kPower; ++it) {
+      const double v = h[l * (kPower + 1) + it];
+      if (std::isfinite(v)) lam = std::max(lam, std::sqrt(v));
+    }
+    PA_CHECK(lam > 0.0, "multigrid: no spectral estimate (zero operator?)");
+    H.L[l]->lmax = float(lam);
   }
 }
 
@@ -619,31 +642,55 @@ pa_status solve_mg(Problem& P, const SolveOperator& op, const double* b, double*
     PA_CUDA(cudaGraphLaunch(gexec, s));
     g_launches += per_precondition;
   };
+  // Outer CG with its scalars on the device: sc = {rz, pq, rr, rz_new, alpha,
+  // beta, breakdown}; alpha and beta come from one-thread kernels, and the
+  // host reads (rr, breakdown) once per iteration for the stopping test.
+  DevBuf<double> scal(8);
+  double* dsc = scal.get();
+  auto dot_into = [&](const double* a, const double* b2, int slot) {
+    PA_CUDA(cudaMemsetAsync(dsc + slot, 0, sizeof(double), s));
+    k_mg_dot<<<vg, kT, 0, s>>>(n, a, b2, dsc + slot);
+    PA_LAUNCHED();
+    g_launches += 1;
+  };
+  auto read_rr = [&](double& rr, bool& bd) {
+    double h[2];
+    PA_CUDA(cudaMemcpyAsync(h, dsc + 2, sizeof(double), cudaMemcpyDeviceToHost, s));
+    PA_CUDA(cudaMemcpyAsync(h + 1, dsc + 6, sizeof(double), cudaMemcpyDeviceToHost, s));
+    PA_CUDA(cudaStreamSynchronize(s));
+    rr = h[0];
+    bd = h[1] != 0.0;
+  };
   int iters = 0, restarts = 0;
   double rr_true = bb;
   bool converged = false, breakdown = false;
   while (!converged && iters < max_iters && !breakdown) {
+    PA_CUDA(cudaMemsetAsync(dsc + 6, 0, sizeof(double), s));
     precondition();
     PA_CUDA(cudaMemcpyAsync(p, z, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-    double rz = host_dot(s, acc, n, r, z);
-    double rr = host_dot(s, acc, n, r, r);
+    dot_into(r, z, 0);  // rz
+    dot_into(r, r, 2);  // rr
+    double rr = 0.0;
+    bool bd = false;
+    read_rr(rr, bd);
     while (rr > tol2 && iters < max_iters) {
       launch_apply_tiled<double>(P, op.w64, p, q, true, s);
-      const double pq = host_dot(s, acc, n, p, q);
-      if (!(pq > 0.0) || !std::isfinite(pq)) { breakdown = true; break; }
-      const double alpha = rz / pq;
-      k_mg_xr<<<vg, kT, 0, s>>>(n, alpha, p, q, x, r);
+      dot_into(p, q, 1);  // pq
+      k_mg_alpha<<<1, 1, 0, s>>>(dsc);
+      k_mg_xr_dev<<<vg, kT, 0, s>>>(n, dsc, p, q, x, r);
       PA_LAUNCHED();
-      g_launches += 2;
+      g_launches += 3;
       ++iters;
-      rr = host_dot(s, acc, n, r, r);
+      dot_into(r, r, 2);  // rr
+      read_rr(rr, bd);
+      if (bd) { breakdown = true; break; }
       if (rr <= tol2) break;
       precondition();
-      const double rz_new = host_dot(s, acc, n, r, z);
-      k_mg_p<<<vg, kT, 0, s>>>(n, rz_new / rz, z, p);
+      dot_into(r, z, 3);  // rz_new
+      k_mg_beta<<<1, 1, 0, s>>>(dsc);
+      k_mg_p_dev<<<vg, kT, 0, s>>>(n, dsc, z, p);
       PA_LAUNCHED();
-      g_launches += 1;
-      rz = rz_new;
+      g_launches += 2;
     }
     // confirm on the true residual r = b' - K x
     launch_apply_tiled<double>(P, op.w64, x, q, true, s);
