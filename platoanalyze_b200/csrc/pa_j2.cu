@@ -510,7 +510,8 @@ pa_status j2_solve(Problem& P, const pa_j2_params& jp, const double* z, const pa
     pa_solve_stats st{};
     pa_solve_options lo_k = lo;
     lo_k.rel_tol = std::max(lo.rel_tol, eta);
-    const pa_status ls = solve_operator(P, op, b.get(), du.get(), lo_k, &st, true);
+    const pa_status ls = lo.method == PA_SOLVER_PCG_MG ? solve_mg(P, op, b.get(), du.get(), lo_k, &st)
+                                                       : solve_operator(P, op, b.get(), du.get(), lo_k, &st, true);
     cg_total += st.iterations;
     ++newton_total;
     if (ls == PA_ERR_NOT_CONVERGED) ++linear_unconverged;

@@ -17,7 +17,10 @@
 //  * coarsest level: Chebyshev of degree 40 on [lmax/1000, 1.1 lmax] (linear,
 //    no factorisation).
 // The outer CG runs in FP64 with the FP64 apply; it stops on the recursive
-// residual and confirms on the true residual b' - K x.
+// residual and confirms on the true residual b' - K x.  For a J2 tangent
+// solve the fine level (smoothing and outer CG) applies the consistent
+// tangent and the coarse levels the elastic operator of the averaged weights
+// (still a symmetric positive definite V-cycle).
 #include <cmath>
 #include <memory>
 #include <vector>
@@ -313,7 +316,10 @@ struct MgLevel {
   std::unique_ptr<Problem> own_prob;
   DevBuf<double> w64, diag;
   DevBuf<float> w32, dinv, x, b, r, d, ad;
+  const float* plas = nullptr;  // level 0 of a J2 tangent solve: the FP32 tangent records
   float lmax = 0.f;
+  DevBuf<float> ev;  // the power iteration's last vector: the next elastic solve starts from it
+  bool ev_valid = false;  // ev (and lmax) come from an elastic operator
 };
 
 struct MgHierarchy {
@@ -372,7 +378,7 @@ void coarse_bcs(const MgLevel& f, MgLevel& c, const std::vector<uint8_t>& fmask,
 
 // Build (first use) or refresh the hierarchy for the problem's box mesh,
 // weights w64 / w32 (tile order) and Dirichlet set.
-void mg_setup(Problem& P, const double* w64, const float* w32, const double* diag_aos) {
+void mg_setup(Problem& P, const double* w64, const float* w32, const double* diag_aos, const float* plas32) {
   const Mesh& m = *P.mesh;
   PA_CHECK(m.box_n[0] > 0, "PA_SOLVER_PCG_MG needs a structured box mesh (pa_mesh_create_box)");
   PA_CHECK(m.box_n[0] % 2 == 0 && m.box_n[1] % 2 == 0 && m.box_n[2] % 2 == 0,
@@ -426,6 +432,7 @@ void mg_setup(Problem& P, const double* w64, const float* w32, const double* dia
     P.mg = H.release();
   }
   MgHierarchy& H = *P.mg;
+  H.L[0]->plas = plas32;  // the coarse levels carry the elastic operator
   // Dirichlet sets by injection
   std::vector<uint8_t> fmask(size_t(P.N()), 0);
   for (int32_t dof : P.bc_dofs) fmask[size_t(dof / 3)] |= uint8_t(1u << (dof % 3));
@@ -454,8 +461,13 @@ void mg_setup(Problem& P, const double* w64, const float* w32, const double* dia
   }
   // lmax of D^-1 K per level: power iteration, all on the device (each
   // step's squared norm lands in norms[level][step]; the scaling kernel reads
-  // it there), one host read for every level at the end
-  constexpr int kPower = 20;
+  // it there), one host read for every level at the end.  An elastic solve
+  // after an elastic solve on the same hierarchy (new SIMP weights) starts
+  // from the previous vector, takes 5 steps and keeps at least 0.95 of the
+  // previous estimate; every other solve starts from a seed and takes 20 (a
+  // J2 tangent changes too much between Newton iterations for a warm start:
+  // measured, the 80x40x40 bar then stopped converging).
+  constexpr int kPower = 20, kPowerWarm = 5;
   const size_t NL = H.L.size();
   DevBuf<double> norms(NL * (kPower + 1));
   PA_CUDA(cudaMemsetAsync(norms.get(), 0, sizeof(double) * NL * (kPower + 1), s));
@@ -464,18 +476,28 @@ void mg_setup(Problem& P, const double* w64, const float* w32, const double* dia
     const float* lw32 = l == 0 ? w32 : L.w32.get();
     const int64_t n3 = 3 * L.N;
     double* nl = norms.get() + l * (kPower + 1);
-    k_mg_seed<<<grid_of(n3), kT, 0, s>>>(L.N, L.P->d_node_mask.get(), L.x.get());
+    if (L.ev.n != size_t(n3)) {
+      L.ev.resize(n3);
+      L.ev_valid = false;
+    }
+    const bool warm = L.ev_valid && plas32 == nullptr;
+    if (warm)
+      PA_CUDA(cudaMemcpyAsync(L.x.get(), L.ev.get(), sizeof(float) * n3, cudaMemcpyDeviceToDevice, s));
+    else
+      k_mg_seed<<<grid_of(n3), kT, 0, s>>>(L.N, L.P->d_node_mask.get(), L.x.get());
     k_mg_norm2<<<grid_of(n3), kT, 0, s>>>(n3, L.x.get(), nl);
     k_mg_scale_dev<<<grid_of(n3), kT, 0, s>>>(n3, L.x.get(), nl);  // unit start vector
     PA_LAUNCHED();
     g_launches += 3;
-    for (int it = 1; it <= kPower; ++it) {
-      launch_apply_tiled<float>(*L.P, lw32, L.x.get(), L.ad.get(), true, s);
+    const int steps = warm ? kPowerWarm : kPower;
+    for (int it = 1; it <= steps; ++it) {
+      launch_apply_tiled<float>(*L.P, lw32, L.x.get(), L.ad.get(), true, s, L.plas);
       k_mg_scale_norm<<<grid_of(n3), kT, 0, s>>>(n3, L.ad.get(), L.dinv.get(), L.x.get(), nl + it);
       k_mg_scale_dev<<<grid_of(n3), kT, 0, s>>>(n3, L.x.get(), nl + it);
       PA_LAUNCHED();
       g_launches += 3;
     }
+    PA_CUDA(cudaMemcpyAsync(L.ev.get(), L.x.get(), sizeof(float) * n3, cudaMemcpyDeviceToDevice, s));
   }
   std::vector<double> h(NL * (kPower + 1));
   PA_CUDA(cudaMemcpyAsync(h.data(), norms.get(), sizeof(double) * h.size(), cudaMemcpyDeviceToHost, s));
@@ -488,7 +510,10 @@ void mg_setup(Problem& P, const double* w64, const float* w32, const double* dia
       if (std::isfinite(v)) lam = std::max(lam, std::sqrt(v));
     }
     PA_CHECK(lam > 0.0, "multigrid: no spectral estimate (zero operator?)");
-    H.L[l]->lmax = float(lam);
+    MgLevel& L = *H.L[l];
+    if (L.ev_valid && plas32 == nullptr) lam = std::max(lam, 0.95 * double(L.lmax));
+    L.lmax = float(lam);
+    L.ev_valid = plas32 == nullptr;
   }
 }
 
@@ -519,14 +544,14 @@ void cheb(MgLevel& L, const float* w32, const float* b, float* x, bool zero_x, c
     PA_CUDA(cudaMemsetAsync(x, 0, sizeof(float) * n3, s));
     k_cheb_start<<<grid_of(n3), kT, 0, s>>>(n3, b, nullptr, L.dinv.get(), c.inv_theta, L.r.get(), L.d.get());
   } else {
-    launch_apply_tiled<float>(*L.P, w32, x, L.ad.get(), true, s);
+    launch_apply_tiled<float>(*L.P, w32, x, L.ad.get(), true, s, L.plas);
     k_cheb_start<<<grid_of(n3), kT, 0, s>>>(n3, b, L.ad.get(), L.dinv.get(), c.inv_theta, L.r.get(), L.d.get());
   }
   PA_LAUNCHED();
   g_launches += zero_x ? 1 : 2;
   for (int k = 1; k < deg; ++k) {
     g_launches += 2;
-    launch_apply_tiled<float>(*L.P, w32, L.d.get(), L.ad.get(), true, s);
+    launch_apply_tiled<float>(*L.P, w32, L.d.get(), L.ad.get(), true, s, L.plas);
     k_cheb_step<<<grid_of(n3), kT, 0, s>>>(n3, x, L.r.get(), L.d.get(), L.ad.get(), L.dinv.get(), c.c1[k - 1],
                                            c.c2[k - 1]);
     PA_LAUNCHED();
@@ -551,7 +576,7 @@ void vcycle(MgHierarchy& H, size_t l, const float* w32_fine, cudaStream_t s) {
   cheb(L, w32, L.b.get(), L.x.get(), true, c, kSmoothDeg, s);
   // residual -> coarse right-hand side
   const int64_t n3 = 3 * L.N;
-  launch_apply_tiled<float>(*L.P, w32, L.x.get(), L.ad.get(), true, s);
+  launch_apply_tiled<float>(*L.P, w32, L.x.get(), L.ad.get(), true, s, L.plas);
   k_mg_sub<<<grid_of(n3), kT, 0, s>>>(n3, L.b.get(), L.ad.get(), L.r.get());
   PA_LAUNCHED();
   MgLevel& Cl = *H.L[l + 1];
@@ -575,12 +600,14 @@ pa_status solve_mg(Problem& P, const SolveOperator& op, const double* b, double*
                    pa_solve_stats* st) {
   cudaStream_t s = P.stream;
   PA_CHECK(o.rel_tol > 0.0, "rel_tol must be positive");
-  PA_CHECK(op.w32 != nullptr && op.plas64 == nullptr, "multigrid solves the elastic operator with FP32 weights");
+  PA_CHECK(op.w32 != nullptr, "multigrid needs the FP32 weights");
+  PA_CHECK((op.plas64 == nullptr) == (op.plas32 == nullptr), "J2 tangent records in both precisions");
   const int64_t N = P.N(), n = P.ndof();
   SolverWorkspace& ws = P.ws;
   if (!P.ev0) { PA_CUDA(cudaEventCreate(&P.ev0)); PA_CUDA(cudaEventCreate(&P.ev1)); }
   g_launches = 0;
-  mg_setup(P, op.w64, op.w32, op.diag_aos);
+  P.ws.ensure(n, P.C(), 1, true);
+  mg_setup(P, op.w64, op.w32, op.diag_aos, op.plas32);
   MgHierarchy& H = *P.mg;
   MgLevel& F = *H.L[0];
   const uint8_t* mask = P.d_node_mask.get();
@@ -601,7 +628,7 @@ pa_status solve_mg(Problem& P, const SolveOperator& op, const double* b, double*
     k_mg_scatter_bc<<<int((nbc + 255) / 256), 256, 0, s>>>(nbc, P.d_bc_dofs.get(), P.d_bc_vals.get(), op.bc_scale, N,
                                                            z);
     PA_LAUNCHED();
-    launch_apply_tiled<double>(P, op.w64, z, q, false, s);
+    launch_apply_tiled<double>(P, op.w64, z, q, false, s, op.plas64);
     k_mg_res64<<<vg, kT, 0, s>>>(N, t, q, mask, bp);
   } else {
     k_mg_res64<<<vg, kT, 0, s>>>(N, t, nullptr, mask, bp);
@@ -674,7 +701,7 @@ pa_status solve_mg(Problem& P, const SolveOperator& op, const double* b, double*
     bool bd = false;
     read_rr(rr, bd);
     while (rr > tol2 && iters < max_iters) {
-      launch_apply_tiled<double>(P, op.w64, p, q, true, s);
+      launch_apply_tiled<double>(P, op.w64, p, q, true, s, op.plas64);
       dot_into(p, q, 1);  // pq
       k_mg_alpha<<<1, 1, 0, s>>>(dsc);
       k_mg_xr_dev<<<vg, kT, 0, s>>>(n, dsc, p, q, x, r);
@@ -693,7 +720,7 @@ pa_status solve_mg(Problem& P, const SolveOperator& op, const double* b, double*
       g_launches += 2;
     }
     // confirm on the true residual r = b' - K x
-    launch_apply_tiled<double>(P, op.w64, x, q, true, s);
+    launch_apply_tiled<double>(P, op.w64, x, q, true, s, op.plas64);
     k_mg_res64<<<vg, kT, 0, s>>>(N, bp, q, mask, r);
     PA_LAUNCHED();
     g_launches += 2;
