@@ -673,7 +673,8 @@ def run_learned(args):
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device="cuda")
     opts = {"learned": pa.SolveOptions("learned", rel_tol=args.rel_tol),
             "mixed": pa.SolveOptions("mixed", rel_tol=args.rel_tol),
-            "fp64": pa.SolveOptions("fp64", rel_tol=args.rel_tol)}
+            "fp64": pa.SolveOptions("fp64", rel_tol=args.rel_tol),
+            "mg": pa.SolveOptions("mg", rel_tol=args.rel_tol)}
 
     def timed(name, steps, warmup):
         for _ in range(warmup):
@@ -695,6 +696,7 @@ def run_learned(args):
     clk = clocks.stop()
     ms_m, st_m, f_m = timed("mixed", max(1, args.steps // 2), 1)
     ms_d, st_d, f_d = timed("fp64", max(1, args.steps // 2), 1)
+    ms_g, st_g, f_g = timed("mg", max(1, args.steps // 2), 1)
     line = {
         "metric": METRIC, "value": C / (ms_l * 1e-3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_l, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -707,7 +709,9 @@ def run_learned(args):
         "learned": {"solve_s": ms_l * 1e-3, **st_l, "compliance_rel_err_vs_fp64": abs(f_l - f_d) / abs(f_d)},
         "jacobi_mixed": {"solve_s": ms_m * 1e-3, **st_m, "compliance_rel_err_vs_fp64": abs(f_m - f_d) / abs(f_d)},
         "jacobi_fp64": {"solve_s": ms_d * 1e-3, **st_d},
+        "multigrid": {"solve_s": ms_g * 1e-3, **st_g, "compliance_rel_err_vs_fp64": abs(f_g - f_d) / abs(f_d)},
         "speedup_learned_vs_fp64": ms_d / ms_l, "speedup_mixed_vs_fp64": ms_d / ms_m,
+        "speedup_multigrid_vs_fp64": ms_d / ms_g,
         "training": tr, "pair_generation_s": t_pairs,
         "simp_history": [{k: h[k] for k in ("iteration", "compliance", "cg_iterations")} for h in hist],
         "clocks": clk,
