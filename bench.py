@@ -5,8 +5,9 @@ Workload (default): 160x80x80 unit hexes x 6 tets (6,144,000 tets, 1,056,321
 nodes, 3,168,963 dofs), E=1, nu=0.3, SIMP p=3 / min 1e-9, per-cell density a
 Gaussian-smoothed (sigma = 3 cells) random field clipped to [0.01, 1], x=0
 face clamped, unit total traction -z on x=160; one step = one full
-Problem::solution (mixed precision Jacobi-PCG: FP32 matrix-free apply and
-vectors, FP64 dots, FP64 true-residual replacement) to relative residual 1e-8.
+Problem::solution to relative residual 1e-8 (default --method mg: FP64 CG
+preconditioned by a geometric multigrid V-cycle with FP32 Chebyshev smoothing
+and a dense coarsest-level inverse; --method mixed / fp64: Jacobi-PCG).
 
 Metric: cells/s = tets solved per second (C / solve time), whole job.
 
@@ -59,6 +60,8 @@ def parse():
     ap.add_argument("--max-newton", type=int, default=25, help="J2: Newton iterations per load step")
     ap.add_argument("--forcing", default="adaptive", choices=["adaptive", "fixed"],
                     help="J2: tangent-solve tolerances (Eisenstat-Walker, or --rel-tol for every solve)")
+    ap.add_argument("--mg-coarse", default="auto", choices=["auto", "chebyshev"],
+                    help="multigrid coarsest level: dense inverse when small enough, or Chebyshev iteration")
     ap.add_argument("--boxes", type=int, default=64, help="batched: number of boxes")
     ap.add_argument("--workload", default="cantilever", choices=["cantilever", "j2", "learned", "batched"],
                     help="cantilever: the SIMP solve (default); j2: the elasto-plastic bar; learned: the "
@@ -360,7 +363,7 @@ def run_ours(args):
     z = torch.tensor(z_host, device="cuda")
     tile, tile_ms = prob.autotune_tiles(z)  # tile size of the fused kernel, before any timing
     u = torch.empty(ndof, dtype=torch.float64, device="cuda")
-    opts = pa.SolveOptions(args.method, rel_tol=args.rel_tol, check_every=args.check_every)
+    opts = pa.SolveOptions(args.method, rel_tol=args.rel_tol, check_every=args.check_every, mg_coarse=args.mg_coarse)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device="cuda")  # 256 MB > 126 MB L2
 
     def solve_once():
@@ -456,7 +459,7 @@ def run_ours(args):
         "data": "synthetic (seeded smoothed density field)",
         "config": {"workload": f"SIMP cantilever {dims[0]}x{dims[1]}x{dims[2]} hex x 6 tets, "
                                f"Problem::solution to relres {args.rel_tol:g}",
-                   "cells": C, "nodes": N, "dofs": ndof, "method": args.method, "parallelism": f"replicas x{world}",
+                   "cells": C, "nodes": N, "dofs": ndof, "method": args.method, "mg_coarse": args.mg_coarse, "parallelism": f"replicas x{world}",
                    "preconditioner": ("geometric multigrid V-cycle: box hierarchy to the coarsest even level, "
                                       "Chebyshev(2) smoothing in D^-1 K, Chebyshev(40) coarsest, trilinear transfers")
                    if args.method == "mg" else "Jacobi",
@@ -553,7 +556,7 @@ def run_j2(args):
     z = torch.ones(N, dtype=torch.float64, device="cuda")
     u = torch.empty(3 * N, dtype=torch.float64, device="cuda")
     local = torch.empty(14 * C, dtype=torch.float64, device="cuda")
-    lin = pa.SolveOptions(args.method, rel_tol=args.rel_tol)
+    lin = pa.SolveOptions(args.method, rel_tol=args.rel_tol, mg_coarse=args.mg_coarse)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device="cuda")
 
     def solve_once():
@@ -620,7 +623,7 @@ def run_j2(args):
         "data": "synthetic (uniform density 1)",
         "config": {"workload": f"J2 bar {dims[0]}x{dims[1]}x{dims[2]} hex x 6 tets, 20 load steps to 2% axial strain, "
                                "E=200e3 nu=0.3 sigma_y=250 H_iso=1000", "cells": C, "nodes": N,
-                   "linear": args.method, "linear_rel_tol": args.rel_tol,
+                   "linear": args.method, "mg_coarse": args.mg_coarse, "linear_rel_tol": args.rel_tol,
                    "tangent_tolerance": "Eisenstat-Walker (floor linear_rel_tol)" if args.forcing == "adaptive"
                    else "linear_rel_tol for every tangent solve",
                    "l2": "256 MB buffer written between steps"},
@@ -674,7 +677,7 @@ def run_learned(args):
     opts = {"learned": pa.SolveOptions("learned", rel_tol=args.rel_tol),
             "mixed": pa.SolveOptions("mixed", rel_tol=args.rel_tol),
             "fp64": pa.SolveOptions("fp64", rel_tol=args.rel_tol),
-            "mg": pa.SolveOptions("mg", rel_tol=args.rel_tol)}
+            "mg": pa.SolveOptions("mg", rel_tol=args.rel_tol, mg_coarse=args.mg_coarse)}
 
     def timed(name, steps, warmup):
         for _ in range(warmup):

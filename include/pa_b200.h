@@ -239,7 +239,16 @@ typedef struct {
   int32_t max_iters;     /* <= 0: 20 * sqrt(ndof) + 1000 */
   int32_t check_every;   /* iterations between convergence checks / residual replacement */
   int32_t use_initial_guess; /* 0: start from x = 0 (as Problem::solution does) */
+  int32_t mg_coarse_solver;  /* PA_SOLVER_PCG_MG: PA_MG_COARSE_* (0, the default, is AUTO) */
 } pa_solve_options;
+
+/* Coarsest multigrid level: AUTO solves it with a dense FP64 inverse (built by
+ * Gauss-Jordan elimination for each solve's weights) when the operator is
+ * elastic and the level has at most 2048 dofs and is nonsingular, else (J2
+ * tangent solves included) by Chebyshev iteration; CHEBYSHEV always iterates
+ * (degree 40 on [lmax/1000, 1.1 lmax] of D^-1 K). */
+#define PA_MG_COARSE_AUTO 0
+#define PA_MG_COARSE_CHEBYSHEV 1
 
 typedef struct {
   int32_t iterations;     /* CG iterations */

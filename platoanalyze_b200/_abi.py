@@ -19,6 +19,7 @@ STATUS_NAMES = {0: "PA_OK", 1: "PA_ERR_INVALID_ARG", 2: "PA_ERR_CUDA", 3: "PA_ER
 PA_CONTROL_NODAL, PA_CONTROL_CELL = 0, 1
 PA_FP64, PA_FP32 = 0, 1
 PA_SOLVER_PCG_FP64, PA_SOLVER_PCG_MIXED, PA_SOLVER_FCG_LEARNED, PA_SOLVER_PCG_MG = 0, 1, 2, 3
+PA_MG_COARSE_AUTO, PA_MG_COARSE_CHEBYSHEV = 0, 1
 
 
 class ElasticParams(ct.Structure):
@@ -28,7 +29,7 @@ class ElasticParams(ct.Structure):
 
 class SolveOptions(ct.Structure):
     _fields_ = [("method", I32), ("rel_tol", F64), ("max_iters", I32), ("check_every", I32),
-                ("use_initial_guess", I32)]
+                ("use_initial_guess", I32), ("mg_coarse_solver", I32)]
 
 
 class SolveStats(ct.Structure):

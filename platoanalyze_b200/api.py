@@ -169,9 +169,16 @@ class Mesh:
 
 
 class SolveOptions:
-    def __init__(self, method="fp64", rel_tol=1e-10, max_iters=0, check_every=64, use_initial_guess=False):
+    def __init__(self, method="fp64", rel_tol=1e-10, max_iters=0, check_every=64, use_initial_guess=False,
+                 mg_coarse="auto"):
+        """mg_coarse (method "mg"): "auto" solves the coarsest level of an elastic
+        solve with a dense inverse when it has at most 2048 dofs (J2 tangent
+        solves iterate), "chebyshev" always iterates."""
         self.method, self.rel_tol, self.max_iters = method, rel_tol, max_iters
         self.check_every, self.use_initial_guess = check_every, use_initial_guess
+        if mg_coarse not in ("auto", "chebyshev"):
+            raise ValueError("mg_coarse must be 'auto' or 'chebyshev'")
+        self.mg_coarse = mg_coarse
 
     def c(self):
         o = _abi.SolveOptions()
@@ -182,6 +189,7 @@ class SolveOptions:
         o.max_iters = int(self.max_iters)
         o.check_every = int(self.check_every)
         o.use_initial_guess = int(bool(self.use_initial_guess))
+        o.mg_coarse_solver = _abi.PA_MG_COARSE_AUTO if self.mg_coarse == "auto" else _abi.PA_MG_COARSE_CHEBYSHEV
         return o
 
 

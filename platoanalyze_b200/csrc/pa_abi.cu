@@ -570,6 +570,7 @@ pa_status pa_solve_options_default(pa_solve_options* o) {
     o->max_iters = 0;
     o->check_every = 64;
     o->use_initial_guess = 0;
+    o->mg_coarse_solver = PA_MG_COARSE_AUTO;
   });
 }
 

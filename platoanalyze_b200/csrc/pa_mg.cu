@@ -14,8 +14,11 @@
 //    [lmax/10, 1.15 lmax], lmax from 20 power iterations (FP32, matrix-free
 //    tile kernel, zero-mean start); the same polynomial before and after the coarse correction, so
 //    the V-cycle is a symmetric positive definite operator;
-//  * coarsest level: Chebyshev of degree 40 on [lmax/1000, 1.1 lmax] (linear,
-//    no factorisation).
+//  * coarsest level (10x5x5 hexes for a 160x80x80 box): solved exactly with
+//    a dense FP64 inverse built per solve by blocked Gauss-Jordan elimination
+//    (one matrix-vector product per V-cycle) when it has at most 2048 dofs
+//    and the operator is elastic; otherwise (J2 tangents), or on request,
+//    Chebyshev of degree 40 on [lmax/1000, 1.1 lmax].
 // The outer CG runs in FP64 with the FP64 apply; it stops on the recursive
 // residual and confirms on the true residual b' - K x.  For a J2 tangent
 // solve the fine level (smoothing and outer CG) applies the consistent
@@ -25,6 +28,7 @@
 #include <memory>
 #include <vector>
 
+#include "pa_cell.cuh"
 #include "pa_problem.cuh"
 #include "pa_tiled.cuh"
 
@@ -305,6 +309,187 @@ __global__ void k_mg_set_bc(int64_t nbc, const int32_t* __restrict__ dofs, const
   x_aos[dofs[i]] = scale * vals[i];
 }
 
+// ---- coarsest level: dense inverse ---------------------------------------
+// The coarsest box (10x5x5 hexes for 160x80x80, 1188 dofs) is solved exactly:
+// its masked elastic operator is assembled as a dense FP64 matrix (component-
+// major dofs d*N + v, padded to nd, a multiple of kGJ), Dirichlet and padding
+// dofs carry identity rows/columns (the restricted right-hand side is zero
+// there), and the matrix is inverted in place by blocked Gauss-Jordan
+// elimination without pivoting (symmetric positive definite).  A V-cycle
+// then costs one matrix-vector product at the bottom.
+constexpr int kGJ = 64, kGJc = 32;
+constexpr int64_t kDirectMaxDofs = 2048;
+
+// one thread per tet: A[row, col] += the masked 12x12 stiffness
+__global__ void k_mg_dense_assemble(int64_t C, const int32_t* __restrict__ perm, const int32_t* __restrict__ cells,
+                                    const double* __restrict__ coords, const double* __restrict__ w,
+                                    const uint8_t* __restrict__ mask, Iso<double> iso, int64_t N, int64_t nd,
+                                    double* __restrict__ A) {
+  const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= C) return;
+  const int64_t u = perm[i];
+  int64_t v[4];
+  double x[4][3];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    v[k] = cells[4 * u + k];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) x[k][d] = coords[3 * v[k] + d];
+  }
+  double g[4][3], vol;
+  tet_geometry(x, g, vol);
+  const double s = vol * w[i];
+  for (int a = 0; a < 4; ++a)
+    for (int b = 0; b < 4; ++b) {
+      double k9[9];
+      tet_kblock(iso, s, g[a], g[b], k9);
+      for (int di = 0; di < 3; ++di) {
+        if ((mask[v[a]] >> di) & 1) continue;
+        for (int dj = 0; dj < 3; ++dj) {
+          if ((mask[v[b]] >> dj) & 1) continue;
+          atomicAdd(&A[(di * N + v[a]) * nd + dj * N + v[b]], k9[3 * di + dj]);
+        }
+      }
+    }
+}
+
+// identity on Dirichlet and padding dofs; diag0 = the diagonal before elimination
+__global__ void k_mg_dense_ident(int64_t N, int64_t nd, const uint8_t* __restrict__ mask, double* __restrict__ A,
+                                 double* __restrict__ diag0) {
+  const int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (r >= nd) return;
+  const bool fixed = r >= 3 * N || ((mask[r % N] >> (r / N)) & 1);
+  if (fixed) A[r * nd + r] = 1.0;
+  diag0[r] = A[r * nd + r];
+}
+
+// In-place Gauss-Jordan of the pivot block A[K,K] -> P^-1 (one CTA).  A pivot
+// that is not above 1e-12 of its row's original diagonal marks the matrix as
+// (numerically) singular in *flag.
+__global__ void __launch_bounds__(256) k_gj_pivot(int64_t nd, int64_t k0, const double* __restrict__ A,
+                                                  const double* __restrict__ diag0, double* __restrict__ piv,
+                                                  double* __restrict__ flag) {
+  __shared__ double P[kGJ][kGJ + 1];
+  __shared__ double row[kGJ], col[kGJ];
+  for (int e = threadIdx.x; e < kGJ * kGJ; e += blockDim.x) P[e / kGJ][e % kGJ] = A[(k0 + e / kGJ) * nd + k0 + e % kGJ];
+  __syncthreads();
+  for (int p = 0; p < kGJ; ++p) {
+    if (threadIdx.x < kGJ) {
+      row[threadIdx.x] = P[p][threadIdx.x];
+      col[threadIdx.x] = P[threadIdx.x][p];
+    }
+    __syncthreads();
+    const double pv = row[p];
+    if (threadIdx.x == 0 && !(pv > 1e-12 * diag0[k0 + p])) *flag = 1.0;
+    const double ip = 1.0 / pv;
+    for (int e = threadIdx.x; e < kGJ * kGJ; e += blockDim.x) {
+      const int r = e / kGJ, c = e % kGJ;
+      double val;
+      if (r == p && c == p)
+        val = ip;
+      else if (r == p)
+        val = row[c] * ip;
+      else if (c == p)
+        val = -col[r] * ip;
+      else
+        val = P[r][c] - col[r] * row[c] * ip;
+      P[r][c] = val;
+    }
+    __syncthreads();
+  }
+  for (int e = threadIdx.x; e < kGJ * kGJ; e += blockDim.x) piv[e] = P[e / kGJ][e % kGJ];
+}
+
+// acc (this thread's 4x4 outputs of a 64x64 tile) += L[64 x 64] R[64 x 64];
+// thread t owns rows t/16 + 16p and columns t%16 + 16q.
+__device__ __forceinline__ void gj_tile_mma(const double* __restrict__ L, int64_t ldl, const double* __restrict__ R,
+                                            int64_t ldr, double acc[4][4]) {
+  __shared__ double Ls[kGJ][kGJc + 1];
+  __shared__ double Rs[kGJc][kGJ];
+  const int tr = threadIdx.x / 16, tc = threadIdx.x % 16;
+  for (int k0 = 0; k0 < kGJ; k0 += kGJc) {
+    for (int e = threadIdx.x; e < kGJ * kGJc; e += blockDim.x) {
+      Ls[e / kGJc][e % kGJc] = L[(e / kGJc) * ldl + k0 + e % kGJc];
+      Rs[e / kGJ][e % kGJ] = R[(k0 + e / kGJ) * ldr + e % kGJ];
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int k = 0; k < kGJc; ++k) {
+      double a[4], b[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        a[q] = Ls[tr + 16 * q][k];
+        b[q] = Rs[k][tc + 16 * q];
+      }
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[p][q] = fma(a[p], b[q], acc[p][q]);
+    }
+    __syncthreads();
+  }
+}
+
+// Row panel W = P^-1 A[K, :] and a copy of the column panel Cp = A[:, K]
+// (both read before k_gj_update overwrites them); block j covers columns /
+// rows j*64 .. j*64+63.
+__global__ void __launch_bounds__(256) k_gj_panels(int64_t nd, int64_t k0, const double* __restrict__ A,
+                                                   const double* __restrict__ piv, double* __restrict__ W,
+                                                   double* __restrict__ Cp) {
+  const int64_t j0 = int64_t(blockIdx.x) * kGJ;
+  double acc[4][4] = {};
+  gj_tile_mma(piv, kGJ, A + k0 * nd + j0, nd, acc);
+  const int tr = threadIdx.x / 16, tc = threadIdx.x % 16;
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) W[(tr + 16 * p) * nd + j0 + tc + 16 * q] = acc[p][q];
+  for (int e = threadIdx.x; e < kGJ * kGJ; e += blockDim.x)
+    Cp[(j0 + e / kGJ) * kGJ + e % kGJ] = A[(j0 + e / kGJ) * nd + k0 + e % kGJ];
+}
+
+// One Gauss-Jordan block step on tile (I, J):
+//   I = K, J = K: P^-1;  I = K: W;  J = K: -Cp P^-1;  else A - Cp W.
+__global__ void __launch_bounds__(256) k_gj_update(int64_t nd, int64_t k0, double* __restrict__ A,
+                                                   const double* __restrict__ piv, const double* __restrict__ W,
+                                                   const double* __restrict__ Cp) {
+  const int64_t j0 = int64_t(blockIdx.x) * kGJ, i0 = int64_t(blockIdx.y) * kGJ;
+  const int tr = threadIdx.x / 16, tc = threadIdx.x % 16;
+  const bool ik = i0 == k0, jk = j0 == k0;
+  if (ik) {  // block-uniform
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int r = tr + 16 * p, c = tc + 16 * q;
+        A[(i0 + r) * nd + j0 + c] = jk ? piv[r * kGJ + c] : W[r * nd + j0 + c];
+      }
+    return;
+  }
+  double acc[4][4] = {};
+  gj_tile_mma(Cp + i0 * kGJ, kGJ, jk ? piv : W + j0, jk ? kGJ : nd, acc);
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      double* a = &A[(i0 + tr + 16 * p) * nd + j0 + tc + 16 * q];
+      *a = jk ? -acc[p][q] : *a - acc[p][q];
+    }
+}
+
+// x = A^-1 b on the coarsest level: one warp per row, FP64 sums
+__global__ void k_mg_dense_solve(int64_t n3, int64_t nd, const double* __restrict__ Ainv, const float* __restrict__ b,
+                                 float* __restrict__ x) {
+  const int64_t r = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (r >= n3) return;
+  double s = 0.0;
+  for (int64_t c = lane; c < n3; c += 32) s = fma(Ainv[r * nd + c], double(b[c]), s);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (lane == 0) x[r] = float(s);
+}
+
 }  // namespace
 
 // ------------------------------------------------------------ hierarchy --
@@ -320,12 +505,16 @@ struct MgLevel {
   float lmax = 0.f;
   DevBuf<float> ev;  // the power iteration's last vector: the next elastic solve starts from it
   bool ev_valid = false;  // ev (and lmax) come from an elastic operator
+  // coarsest level, direct solve: the dense inverse (nd x nd) and its scratch
+  int64_t nd = 0;
+  DevBuf<double> dense, gj_w, gj_c, gj_p, diag0, gj_flag;
 };
 
 struct MgHierarchy {
   std::vector<std::unique_ptr<MgLevel>> L;
   int fine_n[3] = {0, 0, 0};
   double fine_l[3] = {0, 0, 0};
+  bool coarse_direct = false;  // this solve's coarsest level uses the dense inverse
 };
 
 void mg_release(Problem& P) {
@@ -344,6 +533,42 @@ double host_dot(cudaStream_t s, DevBuf<double>& acc, int64_t n, const double* a,
   PA_CUDA(cudaMemcpyAsync(&h, acc.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
   PA_CUDA(cudaStreamSynchronize(s));
   return h;
+}
+
+// Dense inverse of the coarsest level's operator for this solve's weights;
+// false when elimination met a non-positive pivot (a singular operator, e.g.
+// no Dirichlet dofs), in which case the level keeps the Chebyshev solve.
+bool coarse_factor(MgLevel& L, cudaStream_t s) {
+  const int64_t n3 = 3 * L.N, nd = (n3 + kGJ - 1) / kGJ * kGJ;
+  if (L.nd != nd) {
+    L.dense.resize(nd * nd);
+    L.gj_w.resize(kGJ * nd);
+    L.gj_c.resize(nd * kGJ);
+    L.gj_p.resize(kGJ * kGJ);
+    L.diag0.resize(nd);
+    L.gj_flag.resize(1);
+    L.nd = nd;
+  }
+  const Mesh& m = *L.P->mesh;
+  PA_CUDA(cudaMemsetAsync(L.dense.get(), 0, sizeof(double) * nd * nd, s));
+  PA_CUDA(cudaMemsetAsync(L.gj_flag.get(), 0, sizeof(double), s));
+  k_mg_dense_assemble<<<grid_all(L.C), kT, 0, s>>>(L.C, m.d_cell_perm.get(), m.d_cells.get(), m.d_coords.get(),
+                                                   L.w64.get(), L.P->d_node_mask.get(), L.P->ep.iso(), L.N, nd,
+                                                   L.dense.get());
+  k_mg_dense_ident<<<grid_all(nd), kT, 0, s>>>(L.N, nd, L.P->d_node_mask.get(), L.dense.get(), L.diag0.get());
+  PA_LAUNCHED();
+  for (int64_t k0 = 0; k0 < nd; k0 += kGJ) {
+    k_gj_pivot<<<1, kT, 0, s>>>(nd, k0, L.dense.get(), L.diag0.get(), L.gj_p.get(), L.gj_flag.get());
+    k_gj_panels<<<int(nd / kGJ), kT, 0, s>>>(nd, k0, L.dense.get(), L.gj_p.get(), L.gj_w.get(), L.gj_c.get());
+    k_gj_update<<<dim3(unsigned(nd / kGJ), unsigned(nd / kGJ)), kT, 0, s>>>(nd, k0, L.dense.get(), L.gj_p.get(),
+                                                                           L.gj_w.get(), L.gj_c.get());
+    PA_LAUNCHED();
+  }
+  g_launches += 2 + 3 * (nd / kGJ);
+  double flag = 0.0;
+  PA_CUDA(cudaMemcpyAsync(&flag, L.gj_flag.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
+  PA_CUDA(cudaStreamSynchronize(s));
+  return flag == 0.0;
 }
 
 // Dirichlet masks of a coarse level by injection from the fine level's node mask.
@@ -378,7 +603,8 @@ void coarse_bcs(const MgLevel& f, MgLevel& c, const std::vector<uint8_t>& fmask,
 
 // Build (first use) or refresh the hierarchy for the problem's box mesh,
 // weights w64 / w32 (tile order) and Dirichlet set.
-void mg_setup(Problem& P, const double* w64, const float* w32, const double* diag_aos, const float* plas32) {
+void mg_setup(Problem& P, const double* w64, const float* w32, const double* diag_aos, const float* plas32,
+              bool coarse_direct) {
   const Mesh& m = *P.mesh;
   PA_CHECK(m.box_n[0] > 0, "PA_SOLVER_PCG_MG needs a structured box mesh (pa_mesh_create_box)");
   PA_CHECK(m.box_n[0] % 2 == 0 && m.box_n[1] % 2 == 0 && m.box_n[2] % 2 == 0,
@@ -433,6 +659,8 @@ void mg_setup(Problem& P, const double* w64, const float* w32, const double* dia
   }
   MgHierarchy& H = *P.mg;
   H.L[0]->plas = plas32;  // the coarse levels carry the elastic operator
+  // of the fine problem's current material (a J2 solve sets its own E, nu)
+  for (size_t l = 1; l < H.L.size(); ++l) H.L[l]->own_prob->ep = P.ep;
   // Dirichlet sets by injection
   std::vector<uint8_t> fmask(size_t(P.N()), 0);
   for (int32_t dof : P.bc_dofs) fmask[size_t(dof / 3)] |= uint8_t(1u << (dof % 3));
@@ -459,6 +687,8 @@ void mg_setup(Problem& P, const double* w64, const float* w32, const double* dia
     PA_LAUNCHED();
     g_launches += 1;
   }
+  MgLevel& Lc = *H.L.back();
+  H.coarse_direct = coarse_direct && 3 * Lc.N <= kDirectMaxDofs && coarse_factor(Lc, s);
   // lmax of D^-1 K per level: power iteration, all on the device (each
   // step's squared norm lands in norms[level][step]; the scaling kernel reads
   // it there), one host read for every level at the end.  An elastic solve
@@ -469,9 +699,10 @@ void mg_setup(Problem& P, const double* w64, const float* w32, const double* dia
   // measured, the 80x40x40 bar then stopped converging).
   constexpr int kPower = 20, kPowerWarm = 5;
   const size_t NL = H.L.size();
+  const size_t NP = H.coarse_direct ? NL - 1 : NL;  // levels that smooth (need lmax)
   DevBuf<double> norms(NL * (kPower + 1));
   PA_CUDA(cudaMemsetAsync(norms.get(), 0, sizeof(double) * NL * (kPower + 1), s));
-  for (size_t l = 0; l < NL; ++l) {
+  for (size_t l = 0; l < NP; ++l) {
     MgLevel& L = *H.L[l];
     const float* lw32 = l == 0 ? w32 : L.w32.get();
     const int64_t n3 = 3 * L.N;
@@ -502,7 +733,7 @@ void mg_setup(Problem& P, const double* w64, const float* w32, const double* dia
   std::vector<double> h(NL * (kPower + 1));
   PA_CUDA(cudaMemcpyAsync(h.data(), norms.get(), sizeof(double) * h.size(), cudaMemcpyDeviceToHost, s));
   PA_CUDA(cudaStreamSynchronize(s));
-  for (size_t l = 0; l < NL; ++l) {
+  for (size_t l = 0; l < NP; ++l) {
     PA_CHECK(h[l * (kPower + 1)] > 0.0, "multigrid level without free dofs");
     double lam = 0.0;  // ||D^-1 K x|| with ||x|| = 1 approaches lmax from below
     for (int it = 1; it <= kPower; ++it) {
@@ -568,6 +799,13 @@ void vcycle(MgHierarchy& H, size_t l, const float* w32_fine, cudaStream_t s) {
   MgLevel& L = *H.L[l];
   const float* w32 = l == 0 ? w32_fine : L.w32.get();
   if (l + 1 == H.L.size()) {
+    if (H.coarse_direct) {
+      const int64_t n3 = 3 * L.N;
+      k_mg_dense_solve<<<grid_all(32 * n3), kT, 0, s>>>(n3, L.nd, L.dense.get(), L.b.get(), L.x.get());
+      PA_LAUNCHED();
+      g_launches += 1;
+      return;
+    }
     const Cheb c = cheb_coeffs(L.lmax * 1.1f / 1000.f, L.lmax * 1.1f, kCoarseDeg);
     cheb(L, w32, L.b.get(), L.x.get(), true, c, kCoarseDeg, s);
     return;
@@ -607,7 +845,16 @@ pa_status solve_mg(Problem& P, const SolveOperator& op, const double* b, double*
   if (!P.ev0) { PA_CUDA(cudaEventCreate(&P.ev0)); PA_CUDA(cudaEventCreate(&P.ev1)); }
   g_launches = 0;
   P.ws.ensure(n, P.C(), 1, true);
-  mg_setup(P, op.w64, op.w32, op.diag_aos, op.plas32);
+  PA_CHECK(o.mg_coarse_solver == PA_MG_COARSE_AUTO || o.mg_coarse_solver == PA_MG_COARSE_CHEBYSHEV,
+           "mg_coarse_solver must be PA_MG_COARSE_AUTO or PA_MG_COARSE_CHEBYSHEV");
+  // AUTO: the dense coarse inverse for elastic operators.  A J2 tangent
+  // solve keeps the Chebyshev coarse solve: its coarse levels carry the
+  // elastic operator, only a model of the plastic tangent, and with
+  // Eisenstat-Walker tolerances the exact coarse solve left one load step of
+  // the 80x40x40 bar unconverged (measured; with tight tolerances both
+  // coarse solves give the same Newton iterations).
+  mg_setup(P, op.w64, op.w32, op.diag_aos, op.plas32,
+           o.mg_coarse_solver == PA_MG_COARSE_AUTO && op.plas32 == nullptr);
   MgHierarchy& H = *P.mg;
   MgLevel& F = *H.L[0];
   const uint8_t* mask = P.d_node_mask.get();

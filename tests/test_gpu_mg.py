@@ -41,6 +41,22 @@ def test_mg_matches_the_oracle_and_fp64_pcg(pa, oracle_lib, dims):
     assert s64["iterations"] > 5 * st["iterations"]
 
 
+@pytest.mark.parametrize("dims", [(16, 8, 8), (40, 20, 20)])
+def test_mg_coarse_direct_matches_chebyshev(pa, dims):
+    """The dense Gauss-Jordan inverse on the coarsest level (4x2x2 hexes:
+    135 dofs, 3 elimination blocks; 10x5x5 as for 160x80x80: 1188 dofs, 19
+    blocks) against the degree-40 Chebyshev coarse solve: the same solution,
+    no more outer iterations (an exact coarse solve), far fewer launches."""
+    mesh, prob, faces, dofs, z = _cantilever(pa, dims, 7)
+    u_d, st_d = prob.solution(z, options=pa.SolveOptions("mg", rel_tol=1e-10))
+    u_c, st_c = prob.solution(z, options=pa.SolveOptions("mg", rel_tol=1e-10, mg_coarse="chebyshev"))
+    assert st_d["converged"] and st_c["converged"], (st_d, st_c)
+    assert rel_inf(u_d, u_c) <= 1e-7
+    assert st_d["iterations"] <= st_c["iterations"], (st_d, st_c)
+    # 80 launches of the Chebyshev coarse solve per V-cycle become one
+    assert st_d["kernel_launches"] < st_c["kernel_launches"] - 40 * st_d["iterations"], (st_d, st_c)
+
+
 def test_mg_inhomogeneous_dirichlet_and_reuse(pa):
     mesh, prob, faces, dofs, z = _cantilever(pa, (16, 8, 8), 5)
     vals = 0.01 * np.sin(np.arange(dofs.size))
