@@ -63,9 +63,10 @@ def parse():
     ap.add_argument("--mg-coarse", default="auto", choices=["auto", "chebyshev"],
                     help="multigrid coarsest level: dense inverse when small enough, or Chebyshev iteration")
     ap.add_argument("--boxes", type=int, default=64, help="batched: number of boxes")
-    ap.add_argument("--workload", default="cantilever", choices=["cantilever", "j2", "learned", "batched"],
+    ap.add_argument("--workload", default="cantilever", choices=["cantilever", "j2", "learned", "batched", "kernels"],
                     help="cantilever: the SIMP solve (default); j2: the elasto-plastic bar; learned: the "
-                         "learned-preconditioner solve on 64^3 after SIMP-pair training")
+                         "learned-preconditioner solve on 64^3 after SIMP-pair training; kernels: every "
+                         "per-cell entry point timed against its roofline")
     ap.add_argument("--simp-iterations", type=int, default=30)
     ap.add_argument("--train-steps", type=int, default=400)
     return ap.parse_args()
@@ -337,6 +338,98 @@ def profile_kernel(args):
                          "algorithmic_bytes": nb.value}
     print(json.dumps(out), flush=True)
     return 0
+
+
+def run_kernels(args):
+    """Every per-cell entry point of the path on the 160x80x80 box (FP64,
+    per-cell controls, device buffers through the C ABI), each timed with CUDA
+    events on the problem's stream after an L2 flush (256 MB written, untimed):
+    cells/s and GB/s of its algorithmic bytes (s = 8, index 4 B; B = CRS
+    blocks), the fraction of the measured HBM bandwidth, and the CPU oracle's
+    cells/s for the same function on an 80x40x40 sample with all host threads."""
+    import torch
+    import platoanalyze_b200 as pa
+    from platoanalyze_b200.workloads import cantilever, cell_density
+
+    torch.cuda.set_device(0)
+    dims = dims_of(args.dims)
+    C, N = counts(dims)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    mesh, prob, faces, dofs = cantilever(dims, stream=stream.cuda_stream)
+    B = mesh.num_blocks
+    z = torch.from_numpy(cell_density(dims, SEED, kind="smoothed", sigma=3.0, lo=0.01, hi=1.0)).cuda()
+    u, _ = prob.solution(z, options=pa.SolveOptions("mg", rel_tol=1e-8))
+    vf, sf = prob.vector_function(), prob.scalar_function()
+    r = torch.empty(3 * N, dtype=torch.float64, device="cuda")
+    gz = torch.empty(C, dtype=torch.float64, device="cuda")
+    gzc = torch.empty(12 * C, dtype=torch.float64, device="cuda")
+    crs = torch.empty(9 * B, dtype=torch.float64, device="cuda")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    cases = [  # name, call, algorithmic bytes, reference function
+        ("vf_value (residual)", lambda: vf.value(u, z, r), C * 24 + N * 72,
+         "Elliptic::VectorFunction::value, src/elliptic/VectorFunction.hpp:231"),
+        ("sf_value (compliance)", lambda: sf.value(u, z), C * 24 + N * 48,
+         "PhysicsScalarFunction::value, src/elliptic/PhysicsScalarFunction.hpp:225"),
+        ("sf_gradient_u", lambda: sf.gradient_u(u, z, r), C * 24 + N * 72,
+         "PhysicsScalarFunction::gradient_u, :365"),
+        ("sf_gradient_z (self-adjoint dF/dz)", lambda: sf.gradient_z(u, z, gz), C * 32 + N * 48,
+         "PhysicsScalarFunction::gradient_z, :432"),
+        ("vf_gradient_z (dR/dz, 12 per cell)", lambda: vf.gradient_z(u, z, gzc), C * 120 + N * 48,
+         "VectorFunction::gradient_z, src/elliptic/VectorFunction.hpp:598"),
+        ("vf_gradient_u (assembled block CRS)", lambda: vf.gradient_u(u, z, crs), C * 88 + N * 24 + B * 76,
+         "VectorFunction::gradient_u, :505"),
+        ("vf_gradient_x (dR/dx, block CRS)", lambda: vf.gradient_x(u, z, crs), C * 88 + N * 48 + B * 76,
+         "VectorFunction::gradient_x, :317"),
+    ]
+    peak, peak_kind = peaks()
+    rows = []
+    for name, fn, nbytes, ref in cases:
+        for _ in range(max(args.warmup, 3)):
+            fn()
+        tot = 0.0
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            tot += e0.elapsed_time(e1)
+        ms = tot / args.steps
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        rows.append({"function": name, "reference": ref, "ms": ms, "cells_per_s": C / (ms * 1e-3),
+                     "algorithmic_bytes": nbytes, "GB/s": gbs, "frac": gbs / peak})
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import cpu as ocpu
+        threads = host_cores()
+        ocpu.set_threads(threads)
+        sd = (80, 40, 40)
+        cells, coords = ocpu.box_mesh(*sd, float(sd[0]), float(sd[1]), float(sd[2]))
+        O = ocpu.Oracle(cells, coords, E=1.0, nu=0.3, p=3.0, pmin=1e-9, layout=1)
+        zc = cell_density(sd, SEED, kind="smoothed", sigma=3.0, lo=0.01, hi=1.0)
+        uc = np.random.default_rng(SEED).standard_normal(3 * O.N) * 1e-3
+        g = O.graph()
+        cpu = {"cores": threads, "kind": "port", "sample": f"oracle (C++/OpenMP FP64) on {sd[0]}x{sd[1]}x{sd[2]}",
+               "cells_per_s": {}}
+        for name, fn in [("vf_value (residual)", lambda: O.residual(uc, zc)),
+                         ("sf_value+gradients (compliance, dF/du, dF/dz)", lambda: O.energy(uc, zc)),
+                         ("vf_gradient_z (dR/dz, 12 per cell)", lambda: O.gradient_z(uc, zc, g)),
+                         ("vf_gradient_u (assembled block CRS)", lambda: O.jacobian(uc, zc, g)),
+                         ("vf_gradient_x (dR/dx, block CRS)", lambda: O.gradient_x(uc, zc, graph=g))]:
+            fn()
+            t = time.perf_counter()
+            reps = 0
+            while reps < 3 or time.perf_counter() - t < 1.0:
+                fn()
+                reps += 1
+            cpu["cells_per_s"][name] = O.C * reps / (time.perf_counter() - t)
+    print(json.dumps({"workload": f"per-cell entry points, {dims[0]}x{dims[1]}x{dims[2]} box ({C} tets, {N} nodes, "
+                                  f"{B} CRS blocks), FP64, per-cell control",
+                      "steps": args.steps, "warmup": max(args.warmup, 3), "peak_gbs": peak, "peak_kind": peak_kind,
+                      "l2": "256 MB buffer written before each timed call", "kernels": rows,
+                      "cpu_baseline": cpu}), flush=True)
 
 
 def run_ours(args):
@@ -869,6 +962,8 @@ def main():
         return run_learned(args)
     if args.workload == "batched":
         return run_batched(args)
+    if args.workload == "kernels":
+        return run_kernels(args)
     return run_ours(args)
 
 

@@ -405,6 +405,22 @@ pa_status pa_problem_set_dirichlet(pa_problem* problem, const int32_t* dofs, con
   });
 }
 
+// y = K(z) u (interleaved, unconstrained) through the FP64 tile kernel: the
+// tets of a tile sum into shared memory and only nodes shared with other
+// tiles are added globally, instead of 12 global atomics per tet.
+static void apply_k64(Problem& P, const double* du, const double* dz, double* dy) {
+  const int64_t n = P.ndof();
+  P.ws.w64.resize(P.C());
+  pa::launch_cell_weights(P, dz, P.ws.w64.get(), nullptr, P.stream);
+  pa::DevBuf<double>& xs = P.ws.x;
+  pa::DevBuf<double>& ys = P.ws.t;
+  if (xs.n < size_t(n)) xs.resize(n);
+  if (ys.n < size_t(n)) ys.resize(n);
+  pa::launch_aos_to_soa<double, double>(du, xs.get(), P.N(), P.stream);
+  pa::launch_apply_tiled<double>(P, P.ws.w64.get(), xs.get(), ys.get(), false, P.stream);
+  pa::launch_soa_to_aos<double, double>(ys.get(), dy, P.N(), P.stream);
+}
+
 pa_status pa_vf_value(pa_problem* problem, const double* u, const double* z, double* r) {
   return guard([&] {
     Problem& P = prob(problem);
@@ -412,7 +428,7 @@ pa_status pa_vf_value(pa_problem* problem, const double* u, const double* z, dou
     const double* du = st.in(u, P.ndof(), "u");
     const double* dz = st.in(z, P.nz(), "z");
     double* dr = st.out(r, P.ndof(), "r");
-    pa::launch_value(P, du, dz, dr, P.stream);
+    apply_k64(P, du, dz, dr);  // linear elasticity: the volume term is K(z) u
     pa::launch_traction(P, dr, -1.0, P.stream);
     st.finish();
   });
@@ -500,7 +516,14 @@ pa_status pa_sf_value(pa_problem* problem, const double* u, const double* z, dou
 pa_status pa_sf_gradient_u(pa_problem* problem, const double* u, const double* z, double* grad) {
   return guard([&] {
     PA_CHECK(grad, "null grad pointer");
-    energy_call(problem, u, z, nullptr, grad, nullptr);
+    // f = 1/2 u^T K(z) u, so df/du = K(z) u
+    Problem& P = prob(problem);
+    pa::Stage st(P);
+    const double* du = st.in(u, P.ndof(), "u");
+    const double* dz = st.in(z, P.nz(), "z");
+    double* dg = st.out(grad, P.ndof(), "grad");
+    apply_k64(P, du, dz, dg);
+    st.finish();
   });
 }
 

@@ -85,13 +85,28 @@ __device__ __forceinline__ T voigt_dot(const T a[6], const T b[6]) {
   return a[0] * b[0] + a[1] * b[1] + a[2] * b[2] + a[3] * b[3] + a[4] * b[4] + a[5] * b[5];
 }
 
+// x^p; integer exponents 0..4 (the reference's default p is 3) as products,
+// which agree with pow to an ulp or two: an FP64 pow costs an exp/log pair,
+// and one or two of them per tet made the per-cell kernels FP64-bound.
+__device__ __forceinline__ double simp_pow(double x, double p) {
+  if (p == 3.0) return x * x * x;
+  if (p == 2.0) return x * x;
+  if (p == 1.0) return x;
+  if (p == 4.0) {
+    const double x2 = x * x;
+    return x2 * x2;
+  }
+  if (p == 0.0) return 1.0;
+  return pow(x, p);
+}
+
 // SIMP penalty and its derivative (src/Simp.hpp:130-134).
 __device__ __forceinline__ double simp(double rho, double p, double pmin) {
-  return pmin + (1.0 - pmin) * pow(rho, p);
+  return pmin + (1.0 - pmin) * simp_pow(rho, p);
 }
 __device__ __forceinline__ double simp_deriv(double rho, double p, double pmin) {
   if (rho == 0.0) return p == 1.0 ? (1.0 - pmin) : 0.0;
-  return (1.0 - pmin) * p * pow(rho, p - 1.0);
+  return (1.0 - pmin) * p * simp_pow(rho, p - 1.0);
 }
 
 // Closed-form 3x3 block (a,b) of the isotropic cell stiffness

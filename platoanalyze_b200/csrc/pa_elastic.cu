@@ -5,7 +5,8 @@
 // These entry points are called once per design iteration (not inside the
 // Krylov loop), so they use one thread per cell in the caller's cell order
 // with global atomics for the scatter; the Krylov hot loop uses the
-// tile-staged kernel of pa_tiled.cuh.
+// tile-staged kernel of pa_tiled.cuh, and so do the residual and dF/du entry
+// points (K(z) u, pa_abi.cu), which would otherwise add 12 atomics per tet.
 #include <algorithm>
 
 #include "pa_problem.cuh"
