@@ -58,26 +58,6 @@ struct Mat64 {
   int layout;
 };
 
-// VectorFunction::value volume term: r += vol p(rho) B^T C B u_e.
-__global__ void k_value(CellIn m, Mat64 mat, const double* __restrict__ u, const double* __restrict__ z,
-                        double* __restrict__ r) {
-  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  if (c >= m.C) return;
-  int v[4];
-  double x[4][3], g[4][3], vol, ue[12], e[6], sig[6], re[12];
-  load_cell(m, c, v, x);
-  load_u(u, v, ue);
-  tet_geometry(x, g, vol);
-  tet_strain(g, ue, e);
-  const double w = simp(cell_density(z, mat.layout, c, v), mat.p, mat.pmin);
-  tet_stress(mat.iso, vol * w, e, sig);
-  tet_divergence(g, sig, re);
-#pragma unroll
-  for (int n = 0; n < 4; ++n)
-#pragma unroll
-    for (int d = 0; d < 3; ++d) atomicAdd(&r[3 * int64_t(v[n]) + d], re[3 * n + d]);
-}
-
 // SurfaceLoadIntegral (src/SurfaceLoadIntegral.hpp:96-160): per face node
 // weight = scale * (1/6) |(x0 - x2) x (x1 - x2)|, times the face's flux.
 __global__ void k_traction(const int32_t* __restrict__ faces, const double* __restrict__ flux, int64_t nf,
@@ -425,12 +405,6 @@ CellIn cell_in(const Problem& P) { return CellIn{P.mesh->d_cells.get(), P.mesh->
 Mat64 mat64(const Problem& P) { return Mat64{P.ep.iso(), P.ep.p, P.ep.pmin, P.ep.layout}; }
 
 }  // namespace
-
-void launch_value(const Problem& P, const double* u, const double* z, double* r, cudaStream_t s) {
-  PA_CUDA(cudaMemsetAsync(r, 0, sizeof(double) * P.ndof(), s));
-  k_value<<<grid_for(P.C()), kThreads, 0, s>>>(cell_in(P), mat64(P), u, z, r);
-  PA_LAUNCHED();
-}
 
 void launch_traction(const Problem& P, double* r, double scale, cudaStream_t s) {
   const int64_t nf = int64_t(P.faces.size() / 3);

@@ -201,7 +201,6 @@ struct Problem;
 
 // ------------------------------------------------------------ kernel APIs --
 // (implemented in pa_elastic.cu)
-void launch_value(const Problem& P, const double* u, const double* z, double* r, cudaStream_t s);
 void launch_traction(const Problem& P, double* r, double scale, cudaStream_t s);
 void launch_gradient_u(const Problem& P, const double* z, double* entries, cudaStream_t s);
 void launch_gradient_z(const Problem& P, const double* u, const double* z, double* entries, cudaStream_t s);
