@@ -65,7 +65,8 @@ def coarse_operator(n3, nd, fixed, seed):
 
 
 def test_blocked_inverse_of_padded_operators():
-    # 135 dofs (4x2x2 coarsest box) and 1188 dofs (10x5x5, cfg2) -> 192 / 1216
+    # 135 dofs (the 4x2x2 coarsest box: 3 blocks) and 300 dofs (5 blocks); the
+    # 1,188-dof bottom level of 160x80x80 runs in the GPU multigrid tests
     for n3, seed in ((135, 1), (300, 2)):
         nd = (n3 + NB - 1) // NB * NB
         A = coarse_operator(n3, nd, fixed=range(0, n3, 7), seed=seed)
@@ -80,7 +81,7 @@ def test_blocked_inverse_of_padded_operators():
 
 
 def test_high_contrast_operator_is_inverted_accurately():
-    """Void-like dofs (weights ~1e-9 of the solid's) keep pivots far above the
+    """Void-like dofs (stiffness 1e-8 of the solid's) keep pivots far above the
     1e-12 relative threshold of their own rows."""
     n3, nd = 120, 128
     A = coarse_operator(n3, nd, fixed=range(0, 12), seed=3)
