@@ -200,7 +200,11 @@ pa_status pa_sf_gradient_x(pa_problem* problem, const double* u, const double* z
  * __device__ array, which limits a call to 8,388,608 cells (larger meshes are
  * rejected with PA_ERR_INVALID_ARG).  The first call on a device looks up that
  * array's address (do it before any stream capture); calls whose kernels
- * overlap on the GPU race on the shared array, so serialise them on one stream. */
+ * overlap on the GPU race on the shared array, so serialise them on one stream.
+ * All arrays must belong to the current device.  A node id outside
+ * [0, num_nodes) makes *value NaN (the kernel skips that cell's reads); the
+ * lengths of coords, u and z cannot be checked from the host, and arrays
+ * shorter than stated are undefined behaviour. */
 pa_status pa_sf_value_noalloc(const int32_t* cells2nodes, int64_t num_cells, const double* coords,
                               int64_t num_nodes, const double* u, const double* z,
                               const pa_elastic_params* params, double* value, void* stream);

@@ -4,6 +4,7 @@ TEST INFRASTRUCTURE ONLY (see oracle/__init__.py).
 """
 import ctypes as ct
 import os
+import time
 
 import numpy as np
 
@@ -33,6 +34,7 @@ def lib():
         L.pao_block_spmv.argtypes = [I64, P, P, P, P, P]
         L.pao_pcg.argtypes = [I64, P, P, P, P, P, F64, ct.c_int, P]
         L.pao_pcg.restype = ct.c_int
+        L.pao_pcg_run.argtypes = [I64, P, P, P, P, P, F64, F64, ct.c_int, P]
         L.pao_apply.argtypes = [I64, I64, P, P, P, P, ct.c_int, F64, F64, F64, F64, P]
         L.pao_j2_update.argtypes = [I64, P, P, P, P] + [F64] * 8 + [P, P]
         L.pao_j2_plastic_step.argtypes = [I64, P, P, F64, P]
@@ -168,6 +170,39 @@ class Oracle:
         rel = ct.c_double(0)
         it = L.pao_pcg(self.N, _p(rowmap), _p(cols), _p(vals), _p(rhs), _p(x), rel_tol, max_iters, ct.byref(rel))
         return x, it, rel.value
+
+    def constrained_system(self, z, F, bc_dofs, bc_values=None, graph=None):
+        """The linear system of Elliptic::Problem::solution (src/elliptic/Problem.hpp:259-311):
+        K assembled with dual numbers (gradient_u at u = 0) and constrained
+        symmetrically (applyBlockConstraints, src/ApplyConstraints.hpp:11-79).
+        Returns (rowmap, cols, vals, rhs) and the seconds of assembly and of
+        elimination."""
+        rowmap, cols = graph if graph is not None else self.graph()
+        rowmap, cols = _c(rowmap, np.int32), _c(cols, np.int32)
+        z = _c(z, np.float64)
+        t0 = time.perf_counter()
+        vals = self.jacobian(np.zeros(3 * self.N), z, (rowmap, cols))
+        t1 = time.perf_counter()
+        rhs = _c(F, np.float64).copy()
+        bc_dofs = _c(bc_dofs, np.int32)
+        bcv = np.zeros(len(bc_dofs)) if bc_values is None else _c(bc_values, np.float64)
+        lib().pao_apply_block_constraints(self.N, _p(rowmap), _p(cols), _p(vals), _p(rhs), len(bc_dofs),
+                                          _p(bc_dofs), _p(bcv), 1.0)
+        t2 = time.perf_counter()
+        return (rowmap, cols, vals, rhs), t1 - t0, t2 - t1
+
+    def pcg_run(self, system, x=None, rel_tol=1e-8, report_tol=None, max_iters=0):
+        """Jacobi-PCG on a constrained system from x (zero if None), to rel_tol,
+        noting when the residual first reaches report_tol.  Returns x and a dict
+        (iterations, seconds, relres and the checkpoint's iterations/seconds)."""
+        rowmap, cols, vals, rhs = system
+        x = np.zeros(3 * self.N) if x is None else _c(x, np.float64).copy()
+        info = np.zeros(5)
+        rt = rel_tol if report_tol is None else report_tol
+        lib().pao_pcg_run(self.N, _p(rowmap), _p(cols), _p(vals), _p(rhs), _p(x), float(rt), float(rel_tol),
+                          int(max_iters), _p(info))
+        return x, {"report_iterations": int(info[0]), "report_seconds": float(info[1]), "iterations": int(info[2]),
+                   "seconds": float(info[3]), "rel_residual": float(info[4])}
 
     def j2_update(self, u, z, prev, mu, sigma_y0, h_iso, h_kin, pe=3.0, pe_min=1e-9, pp=2.5, pp_min=1e-9):
         u, z, prev = _c(u, np.float64), _c(z, np.float64), _c(prev, np.float64)

@@ -493,6 +493,67 @@ int pao_pcg(int64_t N, const int32_t* rowmap, const int32_t* cols, const double*
   return it;
 }
 
+// The same Jacobi-PCG as pao_pcg, started from x, with a checkpoint: when the
+// relative recursive residual first reaches report_tol, the iteration count
+// and the wall time since entry are stored (info[0], info[1]); the loop goes
+// on to rel_tol (info[2] = iterations, info[3] = total seconds, info[4] =
+// true relative residual ||b - A x|| / ||b||).  max_iters <= 0 means 10*ndof;
+// max_iters caps a bounded run (a timing sample of a longer solve).
+void pao_pcg_run(int64_t N, const int32_t* rowmap, const int32_t* cols, const double* vals, const double* b,
+                 double* x, double report_tol, double rel_tol, int max_iters, double* info) {
+  const double t0 = omp_get_wtime();
+  int64_t n = 3 * N;
+  std::vector<double> dinv(n), r(n), zz(n), pp(n), ap(n);
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < N; ++i)
+    for (int32_t k = rowmap[i]; k < rowmap[i + 1]; ++k)
+      if (cols[k] == i)
+        for (int d = 0; d < 3; ++d) dinv[3 * i + d] = 1.0 / vals[9LL * k + 4 * d];
+  pao_block_spmv(N, rowmap, cols, vals, x, ap.data());
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n; ++i) {
+    r[i] = b[i] - ap[i];
+    zz[i] = r[i] * dinv[i];
+    pp[i] = zz[i];
+  }
+  double bn = std::sqrt(dot(n, b, b));
+  if (bn == 0) bn = 1;
+  double rz = dot(n, r.data(), zz.data());
+  if (max_iters <= 0) max_iters = int(10 * n);
+  int it = 0;
+  double rr = std::sqrt(dot(n, r.data(), r.data()));
+  info[0] = -1.0;
+  info[1] = 0.0;
+  if (rr / bn <= report_tol) { info[0] = 0.0; info[1] = omp_get_wtime() - t0; }
+  while (it < max_iters && rr / bn > rel_tol) {
+    pao_block_spmv(N, rowmap, cols, vals, pp.data(), ap.data());
+    const double alpha = rz / dot(n, pp.data(), ap.data());
+    double rz1 = 0.0, rr2 = 0.0;
+#pragma omp parallel for schedule(static) reduction(+ : rz1, rr2)
+    for (int64_t i = 0; i < n; ++i) {
+      x[i] += alpha * pp[i];
+      r[i] -= alpha * ap[i];
+      zz[i] = r[i] * dinv[i];
+      rz1 += r[i] * zz[i];
+      rr2 += r[i] * r[i];
+    }
+    const double beta = rz1 / rz;
+    rz = rz1;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) pp[i] = zz[i] + beta * pp[i];
+    rr = std::sqrt(rr2);
+    ++it;
+    if (info[0] < 0.0 && rr / bn <= report_tol) { info[0] = it; info[1] = omp_get_wtime() - t0; }
+  }
+  pao_block_spmv(N, rowmap, cols, vals, x, ap.data());
+  double tr = 0;
+#pragma omp parallel for schedule(static) reduction(+ : tr)
+  for (int64_t i = 0; i < n; ++i) tr += (b[i] - ap[i]) * (b[i] - ap[i]);
+  info[2] = it;
+  info[3] = omp_get_wtime() - t0;
+  info[4] = std::sqrt(tr) / bn;
+}
+
 // Matrix-free K u (no constraints) with hand-derived cell operator; used to
 // cross-check the dual-number Jacobian and as a CPU timing of one apply.
 void pao_apply(int64_t C, int64_t N, const int32_t* cells, const double* coords, const double* u,

@@ -19,6 +19,12 @@
 // kernels overlap on the GPU (different streams, or different host threads)
 // race on it.  Serialise such calls on one stream.
 //
+// Inputs live on the device, so the host cannot validate them: a node id in
+// cells2nodes outside [0, num_nodes) is caught in the kernel (that cell reads
+// nothing through it and the value comes out NaN), but the lengths of coords,
+// u and z (N or C per the control layout) cannot be checked; arrays shorter
+// than the stated sizes are undefined behaviour.
+//
 // Host code must not pass `g_noalloc_partials` to a kernel: in host code that
 // name is a host-side stand-in, not the device address.  The address is
 // obtained with cudaGetSymbolAddress once per device, the first time the entry
@@ -64,17 +70,28 @@ __device__ __forceinline__ double noalloc_block_sum(double v, double* smem) {
 
 // Per-cell 1/2 vol p(rho) eps:C:eps (src/elliptic/InternalElasticEnergy.hpp:100-158),
 // one partial sum per block into the scratch array.
+// A cell with a node id outside [0, N) reads nothing through it and
+// contributes NaN, so the value comes out NaN instead of an out-of-bounds read.
 __global__ void __launch_bounds__(kNoAllocThreads) k_energy_noalloc(const int32_t* __restrict__ cells,
                                                                     const double* __restrict__ coords, int64_t C,
-                                                                    NoAllocMat m, const double* __restrict__ u,
+                                                                    int64_t N, NoAllocMat m,
+                                                                    const double* __restrict__ u,
                                                                     const double* __restrict__ z,
                                                                     double* __restrict__ partials) {
   __shared__ double s_red[32];
   const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   double f = 0.0;
+  int v[4] = {0, 0, 0, 0};
+  bool in_range = false;
   if (c < C) {
     const int4 q = reinterpret_cast<const int4*>(cells)[c];
-    const int v[4] = {q.x, q.y, q.z, q.w};
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+    in_range = true;
+#pragma unroll
+    for (int n = 0; n < 4; ++n) in_range = in_range && v[n] >= 0 && int64_t(v[n]) < N;
+    if (!in_range) f = __longlong_as_double(0x7ff8000000000000LL);  // quiet NaN
+  }
+  if (in_range) {
     double x[4][3], ue[12], g[4][3], vol, e[6], sig[6];
 #pragma unroll
     for (int n = 0; n < 4; ++n)
@@ -102,13 +119,18 @@ __global__ void __launch_bounds__(1024) k_sum_noalloc(const double* __restrict__
   if (threadIdx.x == 0) *out = v;
 }
 
-bool on_device(const void* p) {
+// True for memory of device `dev` (or managed memory).  A pointer that
+// cudaPointerGetAttributes rejects is reported as not on the device; that
+// error is its own (the call returns it synchronously) and is cleared.
+bool on_device(const void* p, int dev) {
   cudaPointerAttributes a{};
-  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-    cudaGetLastError();
+  const cudaError_t e = cudaPointerGetAttributes(&a, p);
+  if (e != cudaSuccess) {
+    if (cudaPeekAtLastError() == e) cudaGetLastError();
     return false;
   }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  if (a.type == cudaMemoryTypeManaged) return true;
+  return a.type == cudaMemoryTypeDevice && a.device == dev;
 }
 
 }  // namespace
@@ -126,12 +148,13 @@ extern "C" pa_status pa_sf_value_noalloc(const int32_t* cells2nodes, int64_t num
       throw pa::Error(PA_ERR_INVALID_ARG, "unknown control layout");
     if (reinterpret_cast<uintptr_t>(cells2nodes) % 16 != 0)
       throw pa::Error(PA_ERR_INVALID_ARG, "cells2nodes must be 16-byte aligned");
-    const void* arrays[] = {cells2nodes, coords, u, z, value};
-    for (const void* a : arrays)
-      if (!on_device(a)) throw pa::Error(PA_ERR_INVALID_ARG, "pa_sf_value_noalloc takes device pointers only");
     int dev = 0;
     PA_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kNoAllocMaxDevices) throw pa::Error(PA_ERR_UNSUPPORTED, "device ordinal too large");
+    const void* arrays[] = {cells2nodes, coords, u, z, value};
+    for (const void* a : arrays)
+      if (!on_device(a, dev))
+        throw pa::Error(PA_ERR_INVALID_ARG, "pa_sf_value_noalloc takes device pointers of the current device only");
     double* scratch = nullptr;
     {
       std::lock_guard<std::mutex> lock(g_noalloc_mutex);
@@ -147,7 +170,8 @@ extern "C" pa_status pa_sf_value_noalloc(const int32_t* cells2nodes, int64_t num
                  params->simp_exponent, params->simp_min, params->control_layout};
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const int blocks = int((num_cells + kNoAllocThreads - 1) / kNoAllocThreads);
-    k_energy_noalloc<<<blocks, kNoAllocThreads, 0, s>>>(cells2nodes, coords, num_cells, m, u, z, scratch);
+    k_energy_noalloc<<<blocks, kNoAllocThreads, 0, s>>>(cells2nodes, coords, num_cells, num_nodes, m, u, z,
+                                                        scratch);
     PA_LAUNCHED();
     k_sum_noalloc<<<1, 1024, 0, s>>>(scratch, blocks, value);
     PA_LAUNCHED();

@@ -10,6 +10,7 @@ generated from a seed.
 import numpy as np
 
 from .api import Mesh, Problem
+from .fields import HEX_TETS, box_arrays, cell_density, hex_density  # noqa: F401  (re-exported)
 
 CONFIGS = {
     # 20x10x10 hexes, i.i.d. U[0.3, 1] densities, FP64 Jacobi-PCG to 1e-10
@@ -19,28 +20,6 @@ CONFIGS = {
     "cantilever_160x80x80_mg": dict(dims=(160, 80, 80), density="smoothed", sigma=3.0, lo=0.01, hi=1.0,
                                     rel_tol=1e-8, method="mg"),
 }
-
-
-def hex_density(dims, seed, kind="smoothed", sigma=3.0, lo=0.01, hi=1.0):
-    """Per-hex density on the (nz, ny, nx) grid, flattened x fastest.
-
-    smoothed: white noise U[0,1] (numpy PCG64, `seed`), separable Gaussian
-    filter with sigma cells truncated at 3 sigma (reflecting borders), affine
-    rescale to [0, 1], clip to [lo, hi].  uniform: i.i.d. U[lo, hi]."""
-    nx, ny, nz = dims
-    rng = np.random.default_rng(seed)
-    if kind == "uniform":
-        return rng.uniform(lo, hi, nx * ny * nz)
-    from scipy.ndimage import gaussian_filter
-    noise = rng.uniform(0.0, 1.0, (nz, ny, nx))
-    f = gaussian_filter(noise, sigma=sigma, truncate=3.0, mode="reflect")
-    f = (f - f.min()) / max(f.max() - f.min(), 1e-300)
-    return np.clip(f, lo, hi).ravel()
-
-
-def cell_density(dims, seed, **kw):
-    """Per-tet density: each hex value repeated for its 6 tets."""
-    return np.repeat(hex_density(dims, seed, **kw), 6)
 
 
 def cantilever(dims, youngs_modulus=1.0, poissons_ratio=0.3, simp_exponent=3.0, simp_min=1e-9, stream=None,
@@ -153,34 +132,7 @@ def simp_training_pairs(prob, dims, iterations=30, snapshots=(8, 32, 128, 512), 
 # parted mesh (one CG per box).
 
 def _box(nx, ny, nz):
-    px, py = nx + 1, ny + 1
-    k, j, i = np.meshgrid(np.arange(nz + 1), np.arange(ny + 1), np.arange(nx + 1), indexing="ij")
-    coords = np.stack([i.ravel(), j.ravel(), k.ravel()], axis=1).astype(np.float64)
-    hk, hj, hi = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
-    hi, hj, hk = hi.ravel(), hj.ravel(), hk.ravel()
-    cells = np.empty((hi.size, 6, 4), dtype=np.int32)
-    for t, tet in enumerate(HEX_TETS):
-        for n, (a, b, c) in enumerate(tet):
-            cells[:, t, n] = (hi + a) + px * ((hj + b) + py * (hk + c))
-    # x = nx faces: tets 4 and 5 of the hexes with i = nx - 1
-    last = hi == nx - 1
-    node = lambda a, b, c: (hi[last] + a) + px * ((hj[last] + b) + py * (hk[last] + c))
-    faces = np.concatenate([np.stack([node(1, 0, 0), node(1, 0, 1), node(1, 1, 1)], 1),
-                            np.stack([node(1, 0, 0), node(1, 1, 1), node(1, 1, 0)], 1)]).astype(np.int32)
-    jj, kk = np.meshgrid(np.arange(py), np.arange(nz + 1), indexing="ij")
-    clamp = (px * (jj + py * kk)).ravel()
-    return cells.reshape(-1, 4), coords, faces, clamp
-
-
-# Six tets of a unit hex (vertex offsets), the split of pa_mesh_create_box.
-HEX_TETS = (
-    ((0, 0, 0), (1, 1, 0), (0, 1, 0), (1, 1, 1)),
-    ((0, 0, 0), (0, 1, 0), (0, 1, 1), (1, 1, 1)),
-    ((0, 0, 0), (0, 1, 1), (0, 0, 1), (1, 1, 1)),
-    ((0, 0, 0), (1, 0, 1), (1, 1, 1), (0, 0, 1)),
-    ((1, 0, 0), (1, 0, 1), (1, 1, 1), (0, 0, 0)),
-    ((1, 0, 0), (1, 1, 1), (1, 1, 0), (0, 0, 0)),
-)
+    return box_arrays(nx, ny, nz)
 
 
 def batch_specs(count=64, seed=1234, lo=16, hi=48):

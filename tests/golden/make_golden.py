@@ -1,9 +1,9 @@
 """Generate the golden fixtures in tests/golden/ from the reference's own tests.
 
-Run from the repository root in a container where the platoanalyze source tree
-is mounted (default /root/reference; override with PA_REFERENCE):
+Run from the repository root with the path of a platoanalyze source tree,
+as an argument or in the PA_REFERENCE environment variable:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py <platoanalyze source tree>
 
 The reference cannot be built here (it needs Trilinos, Omega_h and Kokkos), so
 its unit tests are read as text and their gold arrays extracted:
@@ -44,7 +44,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
 sys.path.insert(0, ROOT)
 from oracle import np_ref  # noqa: E402
 
-REF = os.environ.get("PA_REFERENCE", "/root/reference")
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PA_REFERENCE", "")
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 
@@ -245,6 +245,8 @@ def up_residual_3d():
 
 
 def main():
+    if not REF or not os.path.isdir(os.path.join(REF, "unit_tests")):
+        sys.exit("usage: make_golden.py <platoanalyze source tree> (or set PA_REFERENCE)")
     with open(os.path.join(OUT, "derivative_tests_3d.json"), "w") as f:
         json.dump(derivative_tests(), f, indent=1)
     with open(os.path.join(OUT, "j2_plastic_step_3d.json"), "w") as f:

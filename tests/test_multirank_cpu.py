@@ -63,6 +63,6 @@ def test_reference_arm_nonzero_rank_exits_without_work(monkeypatch):
         dims, warmup, steps, gpus, rel_tol = "4x2x2", 1, 1, 2, 1e-8
 
     called = []
-    monkeypatch.setattr(bench, "cpu_solve_estimate", lambda *a, **k: called.append(1))
+    monkeypatch.setattr(bench, "CpuCantilever", lambda *a, **k: called.append(1))
     assert bench.run_reference(Args()) == 0
     assert not called
