@@ -29,6 +29,7 @@
 #include <vector>
 
 #include "pa_cell.cuh"
+#include "pa_dense.cuh"
 #include "pa_problem.cuh"
 #include "pa_tiled.cuh"
 
@@ -317,7 +318,6 @@ __global__ void k_mg_set_bc(int64_t nbc, const int32_t* __restrict__ dofs, const
 // there), and the matrix is inverted in place by blocked Gauss-Jordan
 // elimination without pivoting (symmetric positive definite).  A V-cycle
 // then costs one matrix-vector product at the bottom.
-constexpr int kGJ = 64, kGJc = 32;
 constexpr int64_t kDirectMaxDofs = 2048;
 
 // one thread per tet: A[row, col] += the masked 12x12 stiffness
@@ -361,133 +361,6 @@ __global__ void k_mg_dense_ident(int64_t N, int64_t nd, const uint8_t* __restric
   const bool fixed = r >= 3 * N || ((mask[r % N] >> (r / N)) & 1);
   if (fixed) A[r * nd + r] = 1.0;
   diag0[r] = A[r * nd + r];
-}
-
-// In-place Gauss-Jordan of the pivot block A[K,K] -> P^-1 (one CTA).  A pivot
-// that is not above 1e-12 of its row's original diagonal marks the matrix as
-// (numerically) singular in *flag.
-__global__ void __launch_bounds__(256) k_gj_pivot(int64_t nd, int64_t k0, const double* __restrict__ A,
-                                                  const double* __restrict__ diag0, double* __restrict__ piv,
-                                                  double* __restrict__ flag) {
-  __shared__ double P[kGJ][kGJ + 1];
-  __shared__ double row[kGJ], col[kGJ];
-  for (int e = threadIdx.x; e < kGJ * kGJ; e += blockDim.x) P[e / kGJ][e % kGJ] = A[(k0 + e / kGJ) * nd + k0 + e % kGJ];
-  __syncthreads();
-  for (int p = 0; p < kGJ; ++p) {
-    if (threadIdx.x < kGJ) {
-      row[threadIdx.x] = P[p][threadIdx.x];
-      col[threadIdx.x] = P[threadIdx.x][p];
-    }
-    __syncthreads();
-    const double pv = row[p];
-    if (threadIdx.x == 0 && !(pv > 1e-12 * diag0[k0 + p])) *flag = 1.0;
-    const double ip = 1.0 / pv;
-    for (int e = threadIdx.x; e < kGJ * kGJ; e += blockDim.x) {
-      const int r = e / kGJ, c = e % kGJ;
-      double val;
-      if (r == p && c == p)
-        val = ip;
-      else if (r == p)
-        val = row[c] * ip;
-      else if (c == p)
-        val = -col[r] * ip;
-      else
-        val = P[r][c] - col[r] * row[c] * ip;
-      P[r][c] = val;
-    }
-    __syncthreads();
-  }
-  for (int e = threadIdx.x; e < kGJ * kGJ; e += blockDim.x) piv[e] = P[e / kGJ][e % kGJ];
-}
-
-// acc (this thread's 4x4 outputs of a 64x64 tile) += L[64 x 64] R[64 x 64];
-// thread t owns rows t/16 + 16p and columns t%16 + 16q.
-__device__ __forceinline__ void gj_tile_mma(const double* __restrict__ L, int64_t ldl, const double* __restrict__ R,
-                                            int64_t ldr, double acc[4][4]) {
-  __shared__ double Ls[kGJ][kGJc + 1];
-  __shared__ double Rs[kGJc][kGJ];
-  const int tr = threadIdx.x / 16, tc = threadIdx.x % 16;
-  for (int k0 = 0; k0 < kGJ; k0 += kGJc) {
-    for (int e = threadIdx.x; e < kGJ * kGJc; e += blockDim.x) {
-      Ls[e / kGJc][e % kGJc] = L[(e / kGJc) * ldl + k0 + e % kGJc];
-      Rs[e / kGJ][e % kGJ] = R[(k0 + e / kGJ) * ldr + e % kGJ];
-    }
-    __syncthreads();
-#pragma unroll 4
-    for (int k = 0; k < kGJc; ++k) {
-      double a[4], b[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        a[q] = Ls[tr + 16 * q][k];
-        b[q] = Rs[k][tc + 16 * q];
-      }
-#pragma unroll
-      for (int p = 0; p < 4; ++p)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) acc[p][q] = fma(a[p], b[q], acc[p][q]);
-    }
-    __syncthreads();
-  }
-}
-
-// Row panel W = P^-1 A[K, :] and a copy of the column panel Cp = A[:, K]
-// (both read before k_gj_update overwrites them); block j covers columns /
-// rows j*64 .. j*64+63.
-__global__ void __launch_bounds__(256) k_gj_panels(int64_t nd, int64_t k0, const double* __restrict__ A,
-                                                   const double* __restrict__ piv, double* __restrict__ W,
-                                                   double* __restrict__ Cp) {
-  const int64_t j0 = int64_t(blockIdx.x) * kGJ;
-  double acc[4][4] = {};
-  gj_tile_mma(piv, kGJ, A + k0 * nd + j0, nd, acc);
-  const int tr = threadIdx.x / 16, tc = threadIdx.x % 16;
-#pragma unroll
-  for (int p = 0; p < 4; ++p)
-#pragma unroll
-    for (int q = 0; q < 4; ++q) W[(tr + 16 * p) * nd + j0 + tc + 16 * q] = acc[p][q];
-  for (int e = threadIdx.x; e < kGJ * kGJ; e += blockDim.x)
-    Cp[(j0 + e / kGJ) * kGJ + e % kGJ] = A[(j0 + e / kGJ) * nd + k0 + e % kGJ];
-}
-
-// One Gauss-Jordan block step on tile (I, J):
-//   I = K, J = K: P^-1;  I = K: W;  J = K: -Cp P^-1;  else A - Cp W.
-__global__ void __launch_bounds__(256) k_gj_update(int64_t nd, int64_t k0, double* __restrict__ A,
-                                                   const double* __restrict__ piv, const double* __restrict__ W,
-                                                   const double* __restrict__ Cp) {
-  const int64_t j0 = int64_t(blockIdx.x) * kGJ, i0 = int64_t(blockIdx.y) * kGJ;
-  const int tr = threadIdx.x / 16, tc = threadIdx.x % 16;
-  const bool ik = i0 == k0, jk = j0 == k0;
-  if (ik) {  // block-uniform
-#pragma unroll
-    for (int p = 0; p < 4; ++p)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int r = tr + 16 * p, c = tc + 16 * q;
-        A[(i0 + r) * nd + j0 + c] = jk ? piv[r * kGJ + c] : W[r * nd + j0 + c];
-      }
-    return;
-  }
-  double acc[4][4] = {};
-  gj_tile_mma(Cp + i0 * kGJ, kGJ, jk ? piv : W + j0, jk ? kGJ : nd, acc);
-#pragma unroll
-  for (int p = 0; p < 4; ++p)
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      double* a = &A[(i0 + tr + 16 * p) * nd + j0 + tc + 16 * q];
-      *a = jk ? -acc[p][q] : *a - acc[p][q];
-    }
-}
-
-// x = A^-1 b on the coarsest level: one warp per row, FP64 sums
-__global__ void k_mg_dense_solve(int64_t n3, int64_t nd, const double* __restrict__ Ainv, const float* __restrict__ b,
-                                 float* __restrict__ x) {
-  const int64_t r = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (r >= n3) return;
-  double s = 0.0;
-  for (int64_t c = lane; c < n3; c += 32) s = fma(Ainv[r * nd + c], double(b[c]), s);
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-  if (lane == 0) x[r] = float(s);
 }
 
 }  // namespace
@@ -557,13 +430,7 @@ bool coarse_factor(MgLevel& L, cudaStream_t s) {
                                                    L.dense.get());
   k_mg_dense_ident<<<grid_all(nd), kT, 0, s>>>(L.N, nd, L.P->d_node_mask.get(), L.dense.get(), L.diag0.get());
   PA_LAUNCHED();
-  for (int64_t k0 = 0; k0 < nd; k0 += kGJ) {
-    k_gj_pivot<<<1, kT, 0, s>>>(nd, k0, L.dense.get(), L.diag0.get(), L.gj_p.get(), L.gj_flag.get());
-    k_gj_panels<<<int(nd / kGJ), kT, 0, s>>>(nd, k0, L.dense.get(), L.gj_p.get(), L.gj_w.get(), L.gj_c.get());
-    k_gj_update<<<dim3(unsigned(nd / kGJ), unsigned(nd / kGJ)), kT, 0, s>>>(nd, k0, L.dense.get(), L.gj_p.get(),
-                                                                           L.gj_w.get(), L.gj_c.get());
-    PA_LAUNCHED();
-  }
+  gj_invert(s, nd, L.dense.get(), L.diag0.get(), L.gj_w.get(), L.gj_c.get(), L.gj_p.get(), L.gj_flag.get());
   g_launches += 2 + 3 * (nd / kGJ);
   double flag = 0.0;
   PA_CUDA(cudaMemcpyAsync(&flag, L.gj_flag.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
