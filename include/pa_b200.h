@@ -103,6 +103,17 @@ pa_status pa_mesh_set_graph(pa_mesh* mesh, const int32_t* rowmap, const int32_t*
  * allowed only before problems are created on the mesh. */
 pa_status pa_mesh_uniform_geometry(pa_mesh* mesh, int32_t enable, int32_t* active);
 
+/* Box kernels.  On a box made by pa_mesh_create_box the matrix-free operator
+ * (pa_apply) and every level of the multigrid solve (PA_SOLVER_PCG_MG) run on
+ * a kernel that derives node ids from the lattice and works on the tets as
+ * edge differences of their hex (no connectivity, coordinates or geometry
+ * arithmetic), with the vector updates fused into it.  No reference
+ * counterpart (the reference gathers through cells2nodes,
+ * src/ImplicitFunctors.hpp:15-58).  enable = 1 (the default) uses them when
+ * the mesh qualifies, 0 keeps the tile kernels, -1 only queries; *active (may
+ * be NULL) receives 1 when they are in use.  Takes effect on the next call. */
+pa_status pa_mesh_box_kernels(pa_mesh* mesh, int32_t enable, int32_t* active);
+
 /* Visualisation output: the mesh, the displacement u (3N, interleaved; may be
  * NULL) and the control (N nodal or C per-cell values by control_layout; may
  * be NULL) as a VTK XML unstructured grid (.vtu, base64 binary arrays,

@@ -120,6 +120,7 @@ SIGNATURES = [
     ("pa_up_residual", I32, [P, ct.POINTER(UpParams), P, P, P, I32, P, P, I32]),
     ("pa_mesh_set_parts", I32, [P, I32, P]),
     ("pa_mesh_uniform_geometry", I32, [P, I32, P]),
+    ("pa_mesh_box_kernels", I32, [P, I32, P]),
     ("pa_write_vtu", I32, [P, ct.c_char_p, P, P, I32]),
     ("pa_problem_part_stats", I32, [P, P, P]),
     ("pa_problem_autotune_tiles", I32, [P, P, P, P]),

@@ -149,6 +149,17 @@ class Mesh:
         _abi.check(self._lib.pa_mesh_uniform_geometry(self._h, 1 if enable else 0, ct.byref(a)))
         return bool(a.value)
 
+    @property
+    def box_kernels(self):
+        """True when pa_apply and the multigrid solve run on the box kernel."""
+        a = ct.c_int32()
+        _abi.check(self._lib.pa_mesh_box_kernels(self._h, -1, ct.byref(a)))
+        return bool(a.value)
+
+    def set_box_kernels(self, enable):
+        """Use (True, the default) or bypass the box kernel on a structured box."""
+        _abi.check(self._lib.pa_mesh_box_kernels(self._h, int(bool(enable)), None))
+
     def boundary_faces(self, axis, value):
         n = ct.c_int64()
         _abi.check(self._lib.pa_mesh_boundary_faces(self._h, axis, float(value), None, ct.byref(n)))

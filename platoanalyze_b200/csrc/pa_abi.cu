@@ -361,6 +361,7 @@ pa_status pa_problem_destroy(pa_problem* problem) {
     cudaStream_t s = P.own_stream ? P.stream : nullptr;
     pa_pc* pc = problem->pc;
     pa::mg_release(P);
+    pa::boxmg_release(P);
     delete problem;
     if (s) cudaStreamDestroy(s);
     mh->m.live_problems -= 1;
@@ -546,6 +547,7 @@ pa_status pa_apply(pa_problem* problem, const double* z, const void* x, void* y,
     if (precision == PA_FP32) P.ws.w32.resize(P.C());
     pa::launch_cell_weights(P, dz, P.ws.w64.get(), precision == PA_FP32 ? P.ws.w32.get() : nullptr, P.stream);
     const int64_t nbc = constrained ? int64_t(P.bc_dofs.size()) : 0;
+    const bool box = pa::box_apply_eligible(P);
     if (precision == PA_FP64) {
       const double* dx = st.in(static_cast<const double*>(x), n, "x");
       double* dy = st.out(static_cast<double*>(y), n, "y");
@@ -554,7 +556,10 @@ pa_status pa_apply(pa_problem* problem, const double* z, const void* x, void* y,
       if (xs.n < size_t(n)) xs.resize(n);
       if (ys.n < size_t(n)) ys.resize(n);
       pa::launch_aos_to_soa<double, double>(dx, xs.get(), P.N(), P.stream);
-      pa::launch_apply_tiled<double>(P, P.ws.w64.get(), xs.get(), ys.get(), constrained != 0, P.stream);
+      if (box)
+        pa::box_apply<double>(P, dz, xs.get(), ys.get(), constrained != 0);
+      else
+        pa::launch_apply_tiled<double>(P, P.ws.w64.get(), xs.get(), ys.get(), constrained != 0, P.stream);
       pa::launch_soa_to_aos<double, double>(ys.get(), dy, P.N(), P.stream);
       pa::launch_copy_dofs<double>(P.d_bc_dofs.get(), nbc, dx, dy, P.stream);  // identity rows
     } else {
@@ -565,7 +570,10 @@ pa_status pa_apply(pa_problem* problem, const double* z, const void* x, void* y,
       if (xs.n < size_t(n)) xs.resize(n);
       if (ys.n < size_t(n)) ys.resize(n);
       pa::launch_aos_to_soa<float, float>(dx, xs.get(), P.N(), P.stream);
-      pa::launch_apply_tiled<float>(P, P.ws.w32.get(), xs.get(), ys.get(), constrained != 0, P.stream);
+      if (box)
+        pa::box_apply<float>(P, dz, xs.get(), ys.get(), constrained != 0);
+      else
+        pa::launch_apply_tiled<float>(P, P.ws.w32.get(), xs.get(), ys.get(), constrained != 0, P.stream);
       pa::launch_soa_to_aos<float, float>(ys.get(), dy, P.N(), P.stream);
       pa::launch_copy_dofs<float>(P.d_bc_dofs.get(), nbc, dx, dy, P.stream);
     }
@@ -695,11 +703,19 @@ pa_status pa_time_apply(pa_problem* problem, const double* z, int32_t precision,
     PA_CHECK(reps > 0 && ms_per_launch, "need reps > 0 and an output");
     pa::Stage st(P);
     const double* dz = st.in(z, P.nz(), "z");
-    *ms_per_launch = pa::time_apply(P, dz, precision == PA_FP32, reps);
-    if (algorithmic_bytes) {
-      const int64_t sv = precision == PA_FP32 ? 4 : 8;
-      // cells: 4 int32 node ids + penalty weight; nodes: coords, x in, y out
-      *algorithmic_bytes = P.C() * (16 + sv) + P.N() * (3 * sv) * 3;
+    if (pa::box_apply_eligible(P)) {
+      // the box kernel: weights (one per hex when the six tets share it), x in,
+      // y out and the node's Dirichlet mask; no connectivity, no coordinates
+      int64_t nb = 0;
+      *ms_per_launch = pa::time_box_apply(P, dz, precision == PA_FP32, reps, &nb);
+      if (algorithmic_bytes) *algorithmic_bytes = nb;
+    } else {
+      *ms_per_launch = pa::time_apply(P, dz, precision == PA_FP32, reps);
+      if (algorithmic_bytes) {
+        const int64_t sv = precision == PA_FP32 ? 4 : 8;
+        // cells: 4 int32 node ids + penalty weight; nodes: coords, x in, y out
+        *algorithmic_bytes = P.C() * (16 + sv) + P.N() * (3 * sv) * 3;
+      }
     }
     st.finish();
   });
@@ -1016,6 +1032,15 @@ pa_status pa_mesh_uniform_geometry(pa_mesh* mesh, int32_t enable, int32_t* activ
       pa::mesh_rebuild_tiles(m);
     }
     if (active) *active = m.uniform_hex ? 1 : 0;
+  });
+}
+
+pa_status pa_mesh_box_kernels(pa_mesh* mesh, int32_t enable, int32_t* active) {
+  return guard([&] {
+    PA_CHECK(mesh, "null pa_mesh");
+    pa::Mesh& m = mesh->m;
+    if (enable >= 0) m.box_kernels = enable != 0;
+    if (active) *active = (m.box_kernels && m.box_n[0] > 0) ? 1 : 0;
   });
 }
 

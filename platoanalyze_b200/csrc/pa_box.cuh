@@ -30,7 +30,8 @@
 // the epilogue sees the final y of its node, so vector updates (Chebyshev
 // steps, residuals, CG dot products) fuse into the same kernel.  The input
 // vector is formed once per node and plane into shared memory (three plane
-// buffers, one barrier per hex layer).
+// buffers, one barrier per hex layer), its global loads issued a layer
+// before they are needed.
 #pragma once
 
 #include <cstdint>
@@ -145,13 +146,20 @@ __device__ __forceinline__ void box_hex(const T (&u)[8][3], const T (&w)[WM ? 6 
   box_tet<0, 1, 2, CUBE>(u, W(5) * g.lam, W(5) * g.mu, g.ih, f);
 }
 
-// y = K x on the box with a fused input former and epilogue.
-//   In:  __device__ void operator()(int64_t v, int i, int j, int k, bool owned, T (&x)[3]) const
-//        the input vector at node v = (i, j, k) (called once per CTA, node
-//        and plane; `owned`: this CTA owns v, for side outputs);
-//   Out: __device__ double operator()(int64_t v, int i, int j, int k, const T (&y)[3]) const
-//        consumes (K x)_v at an owned node, returns its part of the reduction;
-//        static constexpr bool kReduce; __device__ void finish(double) const.
+// y = K x on the box with a fused input former and epilogue.  Both are split
+// into a load part (global loads into registers, issued a hex layer before
+// the values are needed) and a compute part:
+//   In:  struct Raw;
+//        __device__ Raw load(int64_t v, bool owned) const;
+//        __device__ void make(const Raw&, int64_t v, int i, int j, int k, bool owned, T (&x)[3]) const;
+//        the input vector at node v = (i, j, k), once per CTA, node and plane
+//        (`owned`: this CTA owns v, for side outputs);
+//   Out: struct Pre;
+//        __device__ Pre load(int64_t v) const;
+//        __device__ double store(const Pre&, int64_t v, int i, int j, int k, const T (&y)[3]) const;
+//        consumes (K x)_v at an owned node and returns its part of the
+//        reduction; static constexpr bool kReduce; __device__ void finish(double) const.
+// Node plane p is formed three hex layers ahead into buffer (p - k0 + 1) % 3.
 // Grid: (ceil(px / 31), ceil(py / 7), ceil(pz / kz)) CTAs of 256 threads.
 template <typename T, int WM, bool CUBE, class In, class Out>
 __global__ void __launch_bounds__(kBoxThreads) k_box(BoxDims d, BoxGeo<T> g, BoxW<T, WM> bw, int kz, In in,
@@ -166,15 +174,37 @@ __global__ void __launch_bounds__(kBoxThreads) k_box(BoxDims d, BoxGeo<T> g, Box
   const bool hex_ij = i >= 0 && i < d.nx && j >= 0 && j < d.ny;
   const bool own_ij = L >= 1 && wp >= 1 && i < d.px && j < d.py;
 
-  // form node plane `plane` into buffer b
-  auto form = [&](int plane, int b) {
-    for (int e = threadIdx.x; e < kBoxPlane; e += kBoxThreads) {
-      const int r = e / kBoxCols, c = e - r * kBoxCols;
-      const int ni = i0 - 1 + c, nj = j0 - 1 + r;
+  // the (at most two) plane entries this thread forms: e = tid, tid + 256
+  constexpr int kSlots = (kBoxPlane + kBoxThreads - 1) / kBoxThreads;
+  int fi[kSlots], fj[kSlots];
+  bool fin[kSlots], fown[kSlots];
+#pragma unroll
+  for (int q = 0; q < kSlots; ++q) {
+    const int e = threadIdx.x + q * kBoxThreads;
+    const int r = e / kBoxCols, c = e - r * kBoxCols;
+    fi[q] = i0 - 1 + c;
+    fj[q] = j0 - 1 + r;
+    fin[q] = e < kBoxPlane && fi[q] >= 0 && fi[q] < d.px && fj[q] >= 0 && fj[q] < d.py;
+    fown[q] = e < kBoxPlane && c >= 1 && c <= kBoxX && r >= 1 && r <= kBoxY;
+  }
+  auto node_of = [&](int ni, int nj, int nk) { return int64_t(ni) + int64_t(d.px) * (nj + int64_t(d.py) * nk); };
+  typename In::Raw raw[kSlots];
+  // issue the loads of node plane p
+  auto form_load = [&](int p) {
+#pragma unroll
+    for (int q = 0; q < kSlots; ++q)
+      if (fin[q] && p >= 0 && p < d.pz) raw[q] = in.load(node_of(fi[q], fj[q], p), fown[q] && p >= k0 && p < k1);
+  };
+  // finish node plane p into buffer b
+  auto form_store = [&](int p, int b) {
+#pragma unroll
+    for (int q = 0; q < kSlots; ++q) {
+      const int e = threadIdx.x + q * kBoxThreads;
+      if (e >= kBoxPlane) continue;
       T v[3] = {T(0), T(0), T(0)};
-      if (ni >= 0 && ni < d.px && nj >= 0 && nj < d.py && plane >= 0 && plane < d.pz) {
-        const bool owned = c >= 1 && c <= kBoxX && r >= 1 && r <= kBoxY && plane >= k0 && plane < k1;
-        in(int64_t(ni) + int64_t(d.px) * (nj + int64_t(d.py) * plane), ni, nj, plane, owned, v);
+      if (fin[q] && p >= 0 && p < d.pz) {
+        const int64_t nv = node_of(fi[q], fj[q], p);
+        in.make(raw[q], nv, fi[q], fj[q], p, fown[q] && p >= k0 && p < k1, v);
       }
       xs[b][e][0] = v[0];
       xs[b][e][1] = v[1];
@@ -189,19 +219,47 @@ __global__ void __launch_bounds__(kBoxThreads) k_box(BoxDims d, BoxGeo<T> g, Box
     v[2] = xs[pb][e][2];
   };
 
-  // buffers rotate: plane p lives in xs[(p - (k0 - 1)) % 3]
-  form(k0 - 1, 0);
-  form(k0, 1);
+  for (int p = 0; p < 3; ++p) {
+    form_load(k0 - 1 + p);
+    form_store(k0 - 1 + p, p);
+  }
   __syncthreads();
   T xb[4][3];  // bottom corners (a + 2b) of the current hex layer
 #pragma unroll
   for (int q = 0; q < 4; ++q) corner(0, q & 1, q >> 1, xb[q]);
+  __syncthreads();  // the first layer refills buffer 0
   T carry[4][3];
 #pragma unroll
   for (int q = 0; q < 4; ++q) carry[q][0] = carry[q][1] = carry[q][2] = T(0);
   double acc = 0.0;
-  int bt = 1, bf = 2;  // buffer of the top plane (k + 1), buffer to form (k + 2)
+  int bt = 1, bf = 0;  // buffer of the top plane (k + 1), buffer to form (k + 3)
+  // hex weights, loaded one layer ahead; hex (i, j, k) = h0 + k * layer
+  const int64_t layer = int64_t(d.nx) * d.ny, h0 = hex_ij ? int64_t(i) + int64_t(d.nx) * j : 0;
+  auto load_w = [&](int k, T (&w)[WM ? 6 : 1]) {
+    if (hex_ij && k >= 0 && k < d.nz) {
+      const int64_t h = h0 + k * layer;
+      if constexpr (WM) {
+#pragma unroll
+        for (int t = 0; t < 6; ++t) w[t] = bw.w[t * bw.H + h];
+      } else {
+        w[0] = bw.w[h];
+      }
+    }
+  };
+  T wn[WM ? 6 : 1];
+  load_w(k0 - 1, wn);
+  const int64_t plane = int64_t(d.px) * d.py, v0 = int64_t(i) + int64_t(d.px) * j;
   for (int k = k0 - 1; k < k1; ++k) {
+    const bool fwd = k + 3 <= k1;  // plane k + 3 is read by a later layer
+    if (fwd) form_load(k + 3);
+    const bool own = own_ij && k >= k0;
+    const int64_t v = v0 + k * plane;
+    typename Out::Pre pre;
+    if (own) pre = out.load(v);
+    T w[WM ? 6 : 1];
+#pragma unroll
+    for (int t = 0; t < (WM ? 6 : 1); ++t) w[t] = wn[t];
+    load_w(k + 1, wn);
     T u[8][3];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
@@ -215,14 +273,6 @@ __global__ void __launch_bounds__(kBoxThreads) k_box(BoxDims d, BoxGeo<T> g, Box
     }
     T f[8][3];
     if (hex_ij && k >= 0 && k < d.nz) {
-      const int64_t h = int64_t(i) + int64_t(d.nx) * (j + int64_t(d.ny) * k);
-      T w[WM ? 6 : 1];
-      if constexpr (WM) {
-#pragma unroll
-        for (int t = 0; t < 6; ++t) w[t] = bw.w[t * bw.H + h];
-      } else {
-        w[0] = bw.w[h];
-      }
       box_hex<CUBE, WM>(u, w, g, f);
     } else {
 #pragma unroll
@@ -247,14 +297,14 @@ __global__ void __launch_bounds__(kBoxThreads) k_box(BoxDims d, BoxGeo<T> g, Box
     const int yi = (k - k0 + 1) & 1;
 #pragma unroll
     for (int c = 0; c < 3; ++c) yb[yi][wp][L][c] = G1[c];
-    if (k + 2 < k1 + 1) form(k + 2, bf);
+    if (fwd) form_store(k + 3, bf);
     __syncthreads();
     // along y: node j gets corner b = 0 of row j and corner b = 1 of row j - 1
-    if (own_ij && k >= k0) {
+    if (own) {
       T y[3];
 #pragma unroll
       for (int c = 0; c < 3; ++c) y[c] = G0[c] + yb[yi][wp - 1][L][c];
-      acc += out(int64_t(i) + int64_t(d.px) * (j + int64_t(d.py) * k), i, j, k, y);
+      acc += out.store(pre, v, i, j, k, y);
     }
     bt = bt == 2 ? 0 : bt + 1;
     bf = bf == 2 ? 0 : bf + 1;
@@ -272,12 +322,12 @@ __global__ void __launch_bounds__(kBoxThreads) k_box(BoxDims d, BoxGeo<T> g, Box
     __syncthreads();
     if (s_last) {
       __threadfence();
-      double v = 0.0;
-      for (unsigned p = threadIdx.x; p < nb; p += kBoxThreads) v += __ldcg(&red.partials[p]);
-      v = block_sum_box(v, s_red);
+      double t = 0.0;
+      for (unsigned p = threadIdx.x; p < nb; p += kBoxThreads) t += __ldcg(&red.partials[p]);
+      t = block_sum_box(t, s_red);
       if (threadIdx.x == 0) {
         *red.counter = 0u;
-        out.finish(v);
+        out.finish(t);
       }
     }
   }

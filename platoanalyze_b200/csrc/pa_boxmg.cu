@@ -1,0 +1,1366 @@
+// pa_boxmg.cu -- CG preconditioned by a geometric multigrid V-cycle on
+// structured boxes, every level applied by the box kernel (pa_box.cuh).
+//
+// The same method as pa_mg.cu (the reference's AMG-preconditioned Krylov
+// solve, src/alg/AmgXLinearSolver.cpp:34-73, replaced on boxes by a
+// geometric hierarchy): levels of half the hexes per axis with the mean SIMP
+// weight of their children, Dirichlet dofs by injection, trilinear transfers,
+// Chebyshev(2) smoothing in D^-1 K on [lmax/10, 1.15 lmax] before and after
+// the coarse correction, a dense FP64 inverse on the coarsest level and an
+// FP64 outer CG.  What changes is the data path:
+//  * every operator application is the box kernel, with the vector updates
+//    of the Chebyshev steps, residuals and CG dot products fused into its
+//    epilogue; one V-cycle on a level is four kernels plus the restriction:
+//      pre   x = dinv (ca b - c2 K d0), d0 = dinv b / theta      (x0 = 0)
+//      res   r = b - K x
+//      post1 r0 = dinv (b - K xi),    xi = x + P e (prolongation formed in the input)
+//      post2 x = xi + ca r0 - c2 dinv K (r0 / theta)
+//    with ca = (1 + c1) / theta + c2 and (c1, c2) the degree-2 Chebyshev
+//    coefficients: exactly the two-step Chebyshev recurrence of pa_mg.cu;
+//  * the finest level reads the outer CG's FP64 residual and writes the FP64
+//    preconditioned residual (no conversion kernels) and accumulates r . z;
+//  * the outer iteration (V-cycle, p = z + beta p with K p and p . Kp in one
+//    kernel, x and r updates with r . r) is one CUDA graph, launched once per
+//    iteration; every scalar stays on the device;
+//  * weights, diagonals and the Dirichlet masks are computed in box order from
+//    the lattice (no cell permutation, no atomics), and a fine level whose six
+//    tets of every hex share one weight (per-hex densities) reads one weight
+//    per hex.
+// Requirements: a box from mesh_make_box (even hex counts), an elastic
+// operator (J2 tangent solves keep pa_mg.cu), one part.
+#include <cmath>
+#include <memory>
+#include <vector>
+
+#include "pa_box.cuh"
+#include "pa_cell.cuh"
+#include "pa_dense.cuh"
+#include "pa_problem.cuh"
+
+namespace pa {
+
+namespace {
+
+constexpr int kVT = 256;
+int vec_blocks(int64_t n) { return int(std::min<int64_t>((n + kVT - 1) / kVT, 148 * 8)); }
+
+// device scalars of the outer CG
+enum : int { kRz = 0, kPq, kAlpha, kBeta, kRr, kBreak, kFirst, kScalars };
+
+// Axis paths of the six tets (pa_box.cuh): (y,x,z) (y,z,x) (z,y,x) (z,x,y)
+// (x,z,y) (x,y,z), two bits per axis, tet t at bits 6t.
+constexpr uint64_t kPathCode = (1ull << 0) | (0ull << 2) | (2ull << 4) |     // t0
+                               (1ull << 6) | (2ull << 8) | (0ull << 10) |    // t1
+                               (2ull << 12) | (1ull << 14) | (0ull << 16) |  // t2
+                               (2ull << 18) | (0ull << 20) | (1ull << 22) |  // t3
+                               (0ull << 24) | (2ull << 26) | (1ull << 28) |  // t4
+                               (0ull << 30) | (1ull << 32) | (2ull << 34);   // t5
+
+// m-th axis of the path of tet t
+__host__ __device__ __forceinline__ int path_axis(int t, int m) { return int((kPathCode >> (6 * t + 2 * m)) & 3u); }
+
+// corner of vertex m of path tet t (v0 = 0, v3 = 7)
+__host__ __device__ __forceinline__ int path_vertex(int t, int m) {
+  int c = 0;
+  for (int q = 0; q < m; ++q) c |= 1 << path_axis(t, q);
+  return c;
+}
+
+// ------------------------------------------------------------- functors --
+// Input formers (In: load + make) and epilogues (Out: load + store) of the
+// box kernel; the loads run a hex layer before their values are used.
+
+template <typename S, typename T>
+struct InVec {  // x, with the masked dofs zero (mask may be null)
+  const S* x;
+  const uint8_t* mask;
+  int64_t N;
+  struct Raw {
+    S x[3];
+    uint8_t mk;
+  };
+  __device__ Raw load(int64_t v, bool) const {
+    Raw r;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) r.x[c] = x[c * N + v];
+    r.mk = mask ? mask[v] : 0;
+    return r;
+  }
+  __device__ void make(const Raw& r, int64_t, int, int, int, bool, T (&o)[3]) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) o[c] = ((r.mk >> c) & 1) ? T(0) : T(r.x[c]);
+  }
+};
+
+template <typename T>
+struct OutPlain {  // y = K x, masked dofs zero (mask may be null)
+  T* y;
+  const uint8_t* mask;
+  int64_t N;
+  static constexpr bool kReduce = false;
+  struct Pre {
+    uint8_t mk;
+  };
+  __device__ Pre load(int64_t v) const { return Pre{mask ? mask[v] : uint8_t(0)}; }
+  __device__ double store(const Pre& p, int64_t v, int, int, int, const T (&k)[3]) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) y[c * N + v] = ((p.mk >> c) & 1) ? T(0) : k[c];
+    return 0.0;
+  }
+  __device__ void finish(double) const {}
+};
+
+template <typename B>
+struct InDinvB {  // d0 = dinv b / theta
+  const B* b;
+  const float* dinv;
+  float s;
+  int64_t N;
+  struct Raw {
+    float d[3];
+    B b[3];
+  };
+  __device__ Raw load(int64_t v, bool) const {
+    Raw r;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      r.d[c] = dinv[c * N + v];
+      r.b[c] = b[c * N + v];
+    }
+    return r;
+  }
+  __device__ void make(const Raw& r, int64_t, int, int, int, bool, float (&o)[3]) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) o[c] = s * r.d[c] * float(r.b[c]);
+  }
+};
+
+template <typename B>
+struct OutPre {  // x = dinv (ca b - c2 K d0)
+  float* x;
+  const B* b;
+  const float* dinv;
+  float ca, c2;
+  int64_t N;
+  static constexpr bool kReduce = false;
+  struct Pre {
+    float d[3];
+    B b[3];
+  };
+  __device__ Pre load(int64_t v) const {
+    Pre p;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      p.d[c] = dinv[c * N + v];
+      p.b[c] = b[c * N + v];
+    }
+    return p;
+  }
+  __device__ double store(const Pre& p, int64_t v, int, int, int, const float (&k)[3]) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) x[c * N + v] = p.d[c] * (ca * float(p.b[c]) - c2 * k[c]);
+    return 0.0;
+  }
+  __device__ void finish(double) const {}
+};
+
+template <typename B>
+struct OutRes {  // r = b - K x, masked dofs zero
+  float* r;
+  const B* b;
+  const uint8_t* mask;
+  int64_t N;
+  static constexpr bool kReduce = false;
+  struct Pre {
+    B b[3];
+    uint8_t mk;
+  };
+  __device__ Pre load(int64_t v) const {
+    Pre p;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) p.b[c] = b[c * N + v];
+    p.mk = mask[v];
+    return p;
+  }
+  __device__ double store(const Pre& p, int64_t v, int, int, int, const float (&k)[3]) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) r[c * N + v] = ((p.mk >> c) & 1) ? 0.f : float(p.b[c]) - k[c];
+    return 0.0;
+  }
+  __device__ void finish(double) const {}
+};
+
+// Trilinear interpolation from the coarse lattice (cpx x cpy x ...) at fine
+// node (i, j, k); the coarse vector is small and read from L2.
+struct Prolong {
+  const float* e;
+  int cpx, cpy;
+  int64_t Nc;
+  __device__ __forceinline__ void add(int i, int j, int k, float (&o)[3]) const {
+    const int ia = i >> 1, ja = j >> 1, ka = k >> 1;
+    const int ni = (i & 1) + 1, nj = (j & 1) + 1, nk = (k & 1) + 1;
+    const float wi = ni == 1 ? 1.f : 0.5f, wj = nj == 1 ? 1.f : 0.5f, wk = nk == 1 ? 1.f : 0.5f;
+    const float w = wi * wj * wk;
+    float s[3] = {0.f, 0.f, 0.f};
+    for (int c = 0; c < nk; ++c)
+      for (int b = 0; b < nj; ++b)
+        for (int a = 0; a < ni; ++a) {
+          const int64_t cv = (ia + a) + int64_t(cpx) * ((ja + b) + int64_t(cpy) * (ka + c));
+#pragma unroll
+          for (int d = 0; d < 3; ++d) s[d] += e[d * Nc + cv];
+        }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) o[d] += w * s[d];
+  }
+};
+
+struct InProlong {  // xi = x + P e, masked dofs zero
+  const float* x;
+  Prolong P;
+  const uint8_t* mask;
+  int64_t N;
+  struct Raw {
+    float x[3];
+    uint8_t mk;
+  };
+  __device__ Raw load(int64_t v, bool) const {
+    Raw r;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) r.x[c] = x[c * N + v];
+    r.mk = mask[v];
+    return r;
+  }
+  __device__ void make(const Raw& r, int64_t, int i, int j, int k, bool, float (&o)[3]) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) o[c] = r.x[c];
+    P.add(i, j, k, o);
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      if ((r.mk >> c) & 1) o[c] = 0.f;
+  }
+};
+
+template <typename B>
+struct OutPost1 {  // r0 = dinv (b - K xi)
+  float* r0;
+  const B* b;
+  const float* dinv;
+  int64_t N;
+  static constexpr bool kReduce = false;
+  struct Pre {
+    float d[3];
+    B b[3];
+  };
+  __device__ Pre load(int64_t v) const {
+    Pre p;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      p.d[c] = dinv[c * N + v];
+      p.b[c] = b[c * N + v];
+    }
+    return p;
+  }
+  __device__ double store(const Pre& p, int64_t v, int, int, int, const float (&k)[3]) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) r0[c * N + v] = p.d[c] * (float(p.b[c]) - k[c]);
+    return 0.0;
+  }
+  __device__ void finish(double) const {}
+};
+
+struct InScaled {  // d0 = s r0
+  const float* r;
+  float s;
+  int64_t N;
+  struct Raw {
+    float r[3];
+  };
+  __device__ Raw load(int64_t v, bool) const {
+    Raw q;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) q.r[c] = r[c * N + v];
+    return q;
+  }
+  __device__ void make(const Raw& q, int64_t, int, int, int, bool, float (&o)[3]) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) o[c] = s * q.r[c];
+  }
+};
+
+// x_out = xi + ca r0 - c2 dinv K d0, xi = x + P e (masked); on the finest level
+// (RZ) the output is the FP64 preconditioned residual z and r . z is reduced
+// (finish: beta = r.z_new / r.z_old, or 0 on the first iteration).
+template <typename O, bool RZ>
+struct OutPost2 {
+  O* xo;
+  const float* x;
+  Prolong P;
+  const uint8_t* mask;
+  const float* r0;
+  const float* dinv;
+  float ca, c2;
+  int64_t N;
+  const double* rvec;  // RZ: the outer residual
+  double* sc;          // RZ: the outer CG scalars
+  static constexpr bool kReduce = RZ;
+  struct Pre {
+    float x[3], r0[3], d[3];
+    double rv[RZ ? 3 : 1];
+    uint8_t mk;
+  };
+  __device__ Pre load(int64_t v) const {
+    Pre p;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int64_t q = c * N + v;
+      p.x[c] = x[q];
+      p.r0[c] = r0[q];
+      p.d[c] = dinv[q];
+      if constexpr (RZ) p.rv[c] = rvec[q];
+    }
+    p.mk = mask[v];
+    return p;
+  }
+  __device__ double store(const Pre& p, int64_t v, int i, int j, int k, const float (&kd)[3]) const {
+    float xi[3] = {p.x[0], p.x[1], p.x[2]};
+    P.add(i, j, k, xi);
+    double acc = 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float xin = ((p.mk >> c) & 1) ? 0.f : xi[c];
+      const float z = xin + ca * p.r0[c] - c2 * p.d[c] * kd[c];
+      xo[c * N + v] = O(z);
+      if constexpr (RZ) acc += double(z) * p.rv[c];
+    }
+    return acc;
+  }
+  __device__ void finish(double t) const {
+    if constexpr (RZ) {
+      const double old = sc[kRz];
+      sc[kBeta] = sc[kFirst] != 0.0 ? 0.0 : t / old;
+      sc[kFirst] = 0.0;
+      sc[kRz] = t;
+      if (!(t > 0.0) || !isfinite(t)) sc[kBreak] = 1.0;
+    }
+  }
+};
+
+// power iteration: x_next = dinv K x / ||x||, ||x_next||^2 reduced
+struct OutPower {
+  float* xn;
+  const float* dinv;
+  const double* nrm_in;
+  double* nrm_out;
+  int64_t N;
+  static constexpr bool kReduce = true;
+  struct Pre {
+    float d[3];
+  };
+  __device__ Pre load(int64_t v) const {
+    Pre p;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) p.d[c] = dinv[c * N + v];
+    return p;
+  }
+  __device__ double store(const Pre& p, int64_t v, int, int, int, const float (&k)[3]) const {
+    const double q = *nrm_in;
+    const float sc = (q > 0.0 && isfinite(q)) ? float(1.0 / sqrt(q)) : 1.f;
+    double acc = 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float val = p.d[c] * k[c] * sc;
+      xn[c * N + v] = val;
+      acc += double(val) * val;
+    }
+    return acc;
+  }
+  __device__ void finish(double t) const { *nrm_out = t; }
+};
+
+// outer CG: p = z + beta p_old formed in the input (the owner stores p_new);
+// q = K p (masked), p . q reduced, alpha = r.z / p.q
+struct InCgP {
+  const double* z;
+  const double* pold;
+  double* pnew;
+  const double* sc;
+  int64_t N;
+  struct Raw {
+    double z[3], p[3];
+  };
+  __device__ Raw load(int64_t v, bool) const {
+    Raw r;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      r.z[c] = z[c * N + v];
+      r.p[c] = pold[c * N + v];
+    }
+    return r;
+  }
+  __device__ void make(const Raw& r, int64_t v, int, int, int, bool owned, double (&o)[3]) const {
+    const double beta = sc[kBeta];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      o[c] = r.z[c] + beta * r.p[c];
+      if (owned) pnew[c * N + v] = o[c];
+    }
+  }
+};
+struct OutCgQ {
+  double* q;
+  const double* z;
+  const double* pold;
+  const uint8_t* mask;
+  double* sc;
+  int64_t N;
+  static constexpr bool kReduce = true;
+  struct Pre {
+    double z[3], p[3];
+    uint8_t mk;
+  };
+  __device__ Pre load(int64_t v) const {
+    Pre r;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      r.z[c] = z[c * N + v];
+      r.p[c] = pold[c * N + v];
+    }
+    r.mk = mask[v];
+    return r;
+  }
+  __device__ double store(const Pre& r, int64_t v, int, int, int, const double (&k)[3]) const {
+    const double beta = sc[kBeta];
+    double acc = 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const double qv = ((r.mk >> c) & 1) ? 0.0 : k[c];
+      q[c * N + v] = qv;
+      acc += (r.z[c] + beta * r.p[c]) * qv;
+    }
+    return acc;
+  }
+  __device__ void finish(double t) const {
+    sc[kPq] = t;
+    if (!(t > 0.0) || !isfinite(t)) {
+      sc[kBreak] = 1.0;
+      sc[kAlpha] = 0.0;
+    } else {
+      sc[kAlpha] = sc[kRz] / t;
+    }
+  }
+};
+
+// ------------------------------------------------------- vector kernels --
+__device__ __forceinline__ void grid_reduce_finish(double v, double* partials, unsigned int* counter, double* out) {
+  __shared__ double s_red[32];
+  __shared__ bool s_last;
+  const double b = block_sum_box(v, s_red);
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = b;
+    __threadfence();
+    s_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (s_last) {
+    __threadfence();
+    double t = 0.0;
+    for (unsigned p = threadIdx.x; p < gridDim.x; p += blockDim.x) t += __ldcg(&partials[p]);
+    t = block_sum_box(t, s_red);
+    if (threadIdx.x == 0) {
+      *counter = 0u;
+      *out = t;
+    }
+  }
+}
+
+// x += alpha p; r -= alpha q; r . r
+__global__ void __launch_bounds__(kVT) k_bcg_update(int64_t n, const double* __restrict__ sc_in,
+                                                    const double* __restrict__ p, const double* __restrict__ q,
+                                                    double* __restrict__ x, double* __restrict__ r,
+                                                    double* partials, unsigned int* counter, double* rr_out) {
+  const double a = sc_in[kAlpha];
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    x[i] += a * p[i];
+    const double ri = r[i] - a * q[i];
+    r[i] = ri;
+    s += ri * ri;
+  }
+  grid_reduce_finish(s, partials, counter, rr_out);
+}
+
+// out = mask ? 0 : a - b (b may be null), and out . out
+__global__ void __launch_bounds__(kVT) k_bres64(int64_t N, const double* __restrict__ a, const double* __restrict__ b,
+                                                const uint8_t* __restrict__ mask, double* __restrict__ out,
+                                                double* partials, unsigned int* counter, double* nrm_out) {
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < 3 * N; i += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t v = i % N, d = i / N;
+    const double o = ((mask[v] >> d) & 1) ? 0.0 : a[i] - (b ? b[i] : 0.0);
+    out[i] = o;
+    s += o * o;
+  }
+  grid_reduce_finish(s, partials, counter, nrm_out);
+}
+
+__global__ void k_bcg_reset(double* sc) {
+  sc[kRz] = 0.0;
+  sc[kPq] = 0.0;
+  sc[kAlpha] = 0.0;
+  sc[kBeta] = 0.0;
+  sc[kBreak] = 0.0;
+  sc[kFirst] = 1.0;
+}
+
+// x_soa[d N + v] = scale * value for each Dirichlet dof (dof = 3 v + d)
+__global__ void k_bscatter_bc(int64_t nbc, const int32_t* __restrict__ dofs, const double* __restrict__ vals,
+                              double scale, int64_t N, double* __restrict__ x) {
+  const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= nbc) return;
+  const int32_t dof = dofs[i];
+  x[(dof % 3) * N + dof / 3] = scale * vals[i];
+}
+__global__ void k_bset_bc(int64_t nbc, const int32_t* __restrict__ dofs, const double* __restrict__ vals, double scale,
+                          double* __restrict__ x_aos) {
+  const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= nbc) return;
+  x_aos[dofs[i]] = scale * vals[i];
+}
+
+// Restriction (R = P^T of trilinear interpolation), coarse masked dofs zero.
+__global__ void k_brestrict(int cnx, int cny, int cnz, const float* __restrict__ f, int64_t Nf,
+                            const uint8_t* __restrict__ cmask, float* __restrict__ c, int64_t Nc) {
+  const int64_t v = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (v >= Nc) return;
+  const int cpx = cnx + 1, cpy = cny + 1;
+  const int I = int(v % cpx), J = int((v / cpx) % cpy), K = int(v / (int64_t(cpx) * cpy));
+  const int fpx = 2 * cnx + 1, fpy = 2 * cny + 1, fpz = 2 * cnz + 1;
+  float s[3] = {0.f, 0.f, 0.f};
+  for (int dc = -1; dc <= 1; ++dc) {
+    const int k = 2 * K + dc;
+    if (k < 0 || k >= fpz) continue;
+    const float wc = dc ? 0.5f : 1.0f;
+    for (int db = -1; db <= 1; ++db) {
+      const int j = 2 * J + db;
+      if (j < 0 || j >= fpy) continue;
+      const float wb = wc * (db ? 0.5f : 1.0f);
+      for (int da = -1; da <= 1; ++da) {
+        const int i = 2 * I + da;
+        if (i < 0 || i >= fpx) continue;
+        const float w = wb * (da ? 0.5f : 1.0f);
+        const int64_t fv = i + int64_t(fpx) * (j + int64_t(fpy) * k);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) s[d] += w * f[d * Nf + fv];
+      }
+    }
+  }
+  const uint8_t mk = cmask[v];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) c[d * Nc + v] = ((mk >> d) & 1) ? 0.f : s[d];
+}
+
+// deterministic zero-mean start vector in [-1, 1], masked; ||x||^2 reduced
+__global__ void __launch_bounds__(kVT) k_bseed(int64_t N, const uint8_t* __restrict__ mask, float* __restrict__ x,
+                                               double* partials, unsigned int* counter, double* nrm_out) {
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < 3 * N; i += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t v = i % N, d = i / N;
+    uint32_t h = uint32_t(i) * 2654435761u + 0x9e3779b9u;
+    h ^= h >> 16;
+    h *= 0x85ebca6bu;
+    h ^= h >> 13;
+    const float val = ((mask[v] >> d) & 1) ? 0.f : float(int(h % 2001u) - 1000) * 1e-3f;
+    x[i] = val;
+    s += double(val) * val;
+  }
+  grid_reduce_finish(s, partials, counter, nrm_out);
+}
+
+// ||x||^2
+__global__ void __launch_bounds__(kVT) k_bnorm2(int64_t n, const float* __restrict__ x, double* partials,
+                                                unsigned int* counter, double* nrm_out) {
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    s += double(x[i]) * x[i];
+  grid_reduce_finish(s, partials, counter, nrm_out);
+}
+
+// ------------------------------------------------ weights and diagonals --
+// SIMP weight of every tet of the fine box from the control (per cell: user
+// cell 6h + t; nodal: the mean of the tet's four nodes, src/ApplyWeighting.hpp:49-62),
+// tet-major; the per-hex copy and a flag when the six tets of a hex differ.
+__global__ void k_bweights(BoxDims d, const double* __restrict__ z, int layout, double p, double pmin,
+                           double* __restrict__ w64t, float* __restrict__ w32t, double* __restrict__ w64h,
+                           float* __restrict__ w32h, unsigned int* __restrict__ differ) {
+  const int64_t h = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (h >= d.H) return;
+  const int i = int(h % d.nx), j = int((h / d.nx) % d.ny), k = int(h / (int64_t(d.nx) * d.ny));
+  double w[6];
+#pragma unroll
+  for (int t = 0; t < 6; ++t) {
+    double rho;
+    if (layout == PA_CONTROL_CELL) {
+      rho = z[6 * h + t];
+    } else {
+      rho = 0.0;
+      for (int m = 0; m < 4; ++m) {
+        const int c = path_vertex(t, m);
+        rho += z[(i + (c & 1)) + int64_t(d.px) * ((j + ((c >> 1) & 1)) + int64_t(d.py) * (k + (c >> 2)))];
+      }
+      rho *= 0.25;
+    }
+    w[t] = simp(rho, p, pmin);
+    w64t[t * d.H + h] = w[t];
+    w32t[t * d.H + h] = float(w[t]);
+  }
+  bool same = true;
+#pragma unroll
+  for (int t = 1; t < 6; ++t) same = same && w[t] == w[0];
+  w64h[h] = w[0];
+  w32h[h] = float(w[0]);
+  if (!same) atomicOr(differ, 1u);
+}
+
+// Coarse hex weight = mean of the 48 child tets (per-hex or tet-major fine weights).
+__global__ void k_bcoarse_w(BoxDims c, BoxDims f, const double* __restrict__ wf, int wm, double* __restrict__ w64,
+                            float* __restrict__ w32) {
+  const int64_t h = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (h >= c.H) return;
+  const int I = int(h % c.nx), J = int((h / c.nx) % c.ny), K = int(h / (int64_t(c.nx) * c.ny));
+  double s = 0.0;
+  for (int cc = 0; cc < 2; ++cc)
+    for (int b = 0; b < 2; ++b)
+      for (int a = 0; a < 2; ++a) {
+        const int64_t fh = (2 * I + a) + int64_t(f.nx) * ((2 * J + b) + int64_t(f.ny) * (2 * K + cc));
+        if (wm)
+          for (int t = 0; t < 6; ++t) s += wf[t * f.H + fh];
+        else
+          s += 6.0 * wf[fh];
+      }
+  const double w = s / 48.0;
+  w64[h] = w;
+  w32[h] = float(w);
+}
+
+// dinv = masked ? 0 : 1 / diag(K), diag from the tets around each node:
+// K_vv,dd = s [lam g_d^2 + mu g_d^2 + mu |g|^2], g the vertex's barycentric gradient.
+__global__ void k_bdinv(BoxDims d, double hx, double hy, double hz, double lam, double mu, const double* __restrict__ w,
+                        int wm, const uint8_t* __restrict__ mask, float* __restrict__ dinv) {
+  const int64_t v = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (v >= d.N) return;
+  const int i = int(v % d.px), j = int((v / d.px) % d.py), k = int(v / (int64_t(d.px) * d.py));
+  const double ih[3] = {1.0 / hx, 1.0 / hy, 1.0 / hz};
+  const double vol = hx * hy * hz / 6.0;
+  double dg[3] = {0.0, 0.0, 0.0};
+  for (int q = 0; q < 8; ++q) {  // this node is corner q of hex (i, j, k) - offset(q)
+    const int hi = i - (q & 1), hj = j - ((q >> 1) & 1), hk = k - (q >> 2);
+    if (hi < 0 || hi >= d.nx || hj < 0 || hj >= d.ny || hk < 0 || hk >= d.nz) continue;
+    const int64_t h = hi + int64_t(d.nx) * (hj + int64_t(d.ny) * hk);
+    for (int t = 0; t < 6; ++t)
+      for (int m = 0; m < 4; ++m) {
+        if (path_vertex(t, m) != q) continue;
+        double g[3] = {0.0, 0.0, 0.0};
+        if (m >= 1) g[path_axis(t, m - 1)] += ih[path_axis(t, m - 1)];
+        if (m <= 2) g[path_axis(t, m)] -= ih[path_axis(t, m)];
+        const double s = vol * (wm ? w[t * d.H + h] : w[h]);
+        const double gg = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) dg[c] += s * ((lam + mu) * g[c] * g[c] + mu * gg);
+      }
+  }
+  const uint8_t mk = mask[v];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) dinv[c * d.N + v] = ((mk >> c) & 1) || !(dg[c] > 0.0) ? 0.f : float(1.0 / dg[c]);
+}
+
+// Coarsest level: A += masked 12x12 stiffness of every tet (one thread per
+// tet; component-major dofs c N + v, row stride nd).
+__global__ void k_bdense_assemble(BoxDims d, double hx, double hy, double hz, Iso<double> iso,
+                                  const double* __restrict__ w, const uint8_t* __restrict__ mask, int64_t nd,
+                                  double* __restrict__ A) {
+  const int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (e >= 6 * d.H) return;
+  const int64_t h = e / 6;
+  const int t = int(e % 6);
+  const int i = int(h % d.nx), j = int((h / d.nx) % d.ny), k = int(h / (int64_t(d.nx) * d.ny));
+  const double ih[3] = {1.0 / hx, 1.0 / hy, 1.0 / hz};
+  double g[4][3];
+  int64_t vv[4];
+  for (int m = 0; m < 4; ++m) {
+    g[m][0] = g[m][1] = g[m][2] = 0.0;
+    if (m >= 1) g[m][path_axis(t, m - 1)] += ih[path_axis(t, m - 1)];
+    if (m <= 2) g[m][path_axis(t, m)] -= ih[path_axis(t, m)];
+    const int c = path_vertex(t, m);
+    vv[m] = (i + (c & 1)) + int64_t(d.px) * ((j + ((c >> 1) & 1)) + int64_t(d.py) * (k + (c >> 2)));
+  }
+  const double s = hx * hy * hz / 6.0 * w[h];
+  for (int a = 0; a < 4; ++a)
+    for (int b = 0; b < 4; ++b) {
+      double k9[9];
+      tet_kblock(iso, s, g[a], g[b], k9);
+      for (int di = 0; di < 3; ++di) {
+        if ((mask[vv[a]] >> di) & 1) continue;
+        for (int dj = 0; dj < 3; ++dj) {
+          if ((mask[vv[b]] >> dj) & 1) continue;
+          atomicAdd(&A[(di * d.N + vv[a]) * nd + dj * d.N + vv[b]], k9[3 * di + dj]);
+        }
+      }
+    }
+}
+
+// identity on Dirichlet and padding dofs; diag0 = the diagonal before elimination
+__global__ void k_bdense_ident(int64_t N, int64_t nd, const uint8_t* __restrict__ mask, double* __restrict__ A,
+                               double* __restrict__ diag0) {
+  const int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (r >= nd) return;
+  const bool fixed = r >= 3 * N || ((mask[r % N] >> (r / N)) & 1);
+  if (fixed) A[r * nd + r] = 1.0;
+  diag0[r] = A[r * nd + r];
+}
+
+}  // namespace
+
+// ---------------------------------------------------------- hierarchy --
+struct BoxLevel {
+  BoxDims d{};
+  double h[3] = {1, 1, 1};
+  bool cube = true;
+  int wm = 0;  // 1: tet-major weights (finest level only)
+  DevBuf<double> w64;
+  DevBuf<float> w32;
+  DevBuf<uint8_t> own_mask;
+  const uint8_t* mask = nullptr;
+  DevBuf<float> dinv, x, b, r, pw0, pw1;
+  float lmax = 0.f;
+  bool pw_valid = false;
+  // coarsest level: dense inverse
+  int64_t nd = 0;
+  DevBuf<double> dense, gj_w, gj_c, gj_p, diag0, flag;
+};
+
+struct BoxHierarchy {
+  std::vector<std::unique_ptr<BoxLevel>> L;
+  int fine_n[3] = {0, 0, 0};
+  double fine_l[3] = {0, 0, 0};
+  DevBuf<double> w64t, w64h;
+  DevBuf<float> w32t, w32h;
+  DevBuf<unsigned int> differ;
+  DevBuf<double> partials, sc, norms;
+  DevBuf<unsigned int> counter;
+  DevBuf<double> p0, p1, q;  // outer CG directions (ping-pong) and K p
+};
+
+void boxmg_release(Problem& P) {
+  delete P.boxmg;
+  P.boxmg = nullptr;
+}
+
+namespace {
+
+thread_local int64_t g_box_launches = 0;
+
+template <typename T>
+BoxGeo<T> box_geo(const BoxLevel& L, const ElasticParams& ep) {
+  const Iso<double> iso = ep.iso();
+  const double vol = L.h[0] * L.h[1] * L.h[2] / 6.0;
+  BoxGeo<T> g;
+  const double s = L.cube ? 1.0 / (L.h[0] * L.h[0]) : 1.0;
+  g.lam = T(iso.lam * vol * s);
+  g.mu = T(iso.mu * vol * s);
+  for (int a = 0; a < 3; ++a) g.ih[a] = T(1.0 / L.h[a]);
+  return g;
+}
+
+// CTAs of a box launch: a brick column per (31 x 7) node block, the z range
+// cut into as many chunks as fill the resident CTA slots once (at least two
+// node planes per chunk).
+dim3 box_grid(const BoxDims& d, int slots, int* kz_out) {
+  const int gx = (d.px + kBoxX - 1) / kBoxX, gy = (d.py + kBoxY - 1) / kBoxY;
+  const int gz_want = std::max(1, slots / (gx * gy));
+  int kz = std::max(2, (d.pz + gz_want - 1) / gz_want);
+  const int gz = (d.pz + kz - 1) / kz;
+  *kz_out = kz;
+  return dim3(unsigned(gx), unsigned(gy), unsigned(gz));
+}
+
+void set_dims(BoxLevel& L, int nx, int ny, int nz, double lx, double ly, double lz) {
+  L.d.nx = nx;
+  L.d.ny = ny;
+  L.d.nz = nz;
+  L.d.px = nx + 1;
+  L.d.py = ny + 1;
+  L.d.pz = nz + 1;
+  L.d.N = int64_t(L.d.px) * L.d.py * L.d.pz;
+  L.d.H = int64_t(nx) * ny * nz;
+  L.h[0] = lx / nx;
+  L.h[1] = ly / ny;
+  L.h[2] = lz / nz;
+  const double hmax = std::max(std::max(L.h[0], L.h[1]), L.h[2]);
+  L.cube = std::fabs(L.h[0] - L.h[1]) <= 1e-12 * hmax && std::fabs(L.h[0] - L.h[2]) <= 1e-12 * hmax;
+}
+
+template <typename T, int WM, bool CUBE, class In, class Out>
+void launch_box_t(const BoxLevel& L, const BoxGeo<T>& g, const T* w, const In& in, const Out& out, BoxRed red,
+                  cudaStream_t s) {
+  static int occupancy = 0;  // resident CTAs per SM of this instance
+  if (occupancy == 0) {
+    int o = 0;
+    PA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_box<T, WM, CUBE, In, Out>, kBoxThreads, 0));
+    occupancy = std::max(1, o);
+  }
+  int kz = 2;
+  const dim3 grid = box_grid(L.d, occupancy * num_sms(), &kz);
+  k_box<T, WM, CUBE, In, Out><<<grid, kBoxThreads, 0, s>>>(L.d, g, BoxW<T, WM>{w, L.d.H}, kz, in, out, red);
+  PA_LAUNCHED();
+  g_box_launches += 1;
+}
+
+// dispatch on the level's weight layout and hex shape
+template <typename T, class In, class Out>
+void launch_box(const BoxLevel& L, const BoxGeo<T>& g, const T* w, const In& in, const Out& out, BoxRed red,
+                cudaStream_t s) {
+  if (L.wm) {
+    if (L.cube)
+      launch_box_t<T, 1, true>(L, g, w, in, out, red, s);
+    else
+      launch_box_t<T, 1, false>(L, g, w, in, out, red, s);
+  } else {
+    if (L.cube)
+      launch_box_t<T, 0, true>(L, g, w, in, out, red, s);
+    else
+      launch_box_t<T, 0, false>(L, g, w, in, out, red, s);
+  }
+}
+
+// an upper bound on the CTAs of any box launch on the hierarchy (chunks of
+// at least two planes) and of the vector kernels
+int64_t max_grid_blocks(const BoxHierarchy& H) {
+  int64_t m = 148 * 8;
+  for (const auto& L : H.L)
+    m = std::max<int64_t>(m, int64_t((L->d.px + kBoxX - 1) / kBoxX) * ((L->d.py + kBoxY - 1) / kBoxY) *
+                                 ((L->d.pz + 1) / 2));
+  return m;
+}
+
+// coarse masks by injection (fine node (2I, 2J, 2K))
+void coarse_mask(const BoxLevel& f, BoxLevel& c, const std::vector<uint8_t>& fmask, std::vector<uint8_t>& cmask) {
+  cmask.assign(size_t(c.d.N), 0);
+  for (int64_t K = 0; K < c.d.pz; ++K)
+    for (int64_t J = 0; J < c.d.py; ++J)
+      for (int64_t I = 0; I < c.d.px; ++I)
+        cmask[size_t(I + c.d.px * (J + c.d.py * K))] = fmask[size_t(2 * I + f.d.px * (2 * J + f.d.py * 2 * K))];
+}
+
+}  // namespace
+
+// True when the box kernels can run this problem's multigrid solve.
+// True when the box kernels can run this problem's multigrid solve: a box
+// of mesh_make_box with even hex counts, one part, and a coarsest level (the
+// box halved while every axis stays even with at least 4 hexes) of at most
+// 2048 dofs for the dense inverse.
+bool boxmg_eligible(const Problem& P) {
+  const Mesh& m = *P.mesh;
+  if (!box_apply_eligible(P) || m.box_n[0] % 2 || m.box_n[1] % 2 || m.box_n[2] % 2) return false;
+  int n[3] = {m.box_n[0], m.box_n[1], m.box_n[2]};
+  while (!(n[0] % 2 || n[1] % 2 || n[2] % 2 || std::min(std::min(n[0], n[1]), n[2]) < 4))
+    for (int a = 0; a < 3; ++a) n[a] /= 2;
+  return 3LL * (n[0] + 1) * (n[1] + 1) * (n[2] + 1) <= 2048;
+}
+
+// True when the box kernel can apply this problem's operator (pa_apply).
+bool box_apply_eligible(const Problem& P) {
+  const Mesh& m = *P.mesh;
+  return m.box_kernels && m.box_n[0] > 0 && m.num_parts == 1;
+}
+
+namespace {
+
+// Build the hierarchy for the problem's box (first use or a new box), then
+// refresh weights, masks, diagonals, spectral estimates and the coarsest
+// inverse for control z.  False when the coarsest operator is singular (no
+// dense inverse): the caller then solves with pa_mg.cu, whose coarsest
+// level falls back to Chebyshev.
+// The hierarchy's levels and device buffers for the problem's box.
+void boxmg_setup_levels(Problem& P) {
+  const Mesh& m = *P.mesh;
+  cudaStream_t s = P.stream;
+  boxmg_release(P);
+  std::unique_ptr<BoxHierarchy> H(new BoxHierarchy());
+  int n[3] = {m.box_n[0], m.box_n[1], m.box_n[2]};
+  for (int a = 0; a < 3; ++a) {
+    H->fine_n[a] = n[a];
+    H->fine_l[a] = m.box_l[a];
+  }
+  for (int l = 0;; ++l) {
+    std::unique_ptr<BoxLevel> L(new BoxLevel());
+    set_dims(*L, n[0], n[1], n[2], m.box_l[0], m.box_l[1], m.box_l[2]);
+    const int64_t n3 = 3 * L->d.N;
+    L->dinv.resize(n3);
+    L->x.resize(n3);
+    L->r.resize(n3);
+    if (l > 0) {
+      L->b.resize(n3);
+      L->w64.resize(L->d.H);
+      L->w32.resize(L->d.H);
+      L->own_mask.resize(L->d.N);
+      L->mask = L->own_mask.get();
+    }
+    H->L.push_back(std::move(L));
+    if (n[0] % 2 || n[1] % 2 || n[2] % 2 || std::min(std::min(n[0], n[1]), n[2]) < 4) break;
+    for (int a = 0; a < 3; ++a) n[a] /= 2;
+  }
+  const BoxLevel& F = *H->L[0];
+  H->w64t.resize(6 * F.d.H);
+  H->w32t.resize(6 * F.d.H);
+  H->w64h.resize(F.d.H);
+  H->w32h.resize(F.d.H);
+  H->differ.resize(1);
+  H->partials.resize(size_t(max_grid_blocks(*H)));
+  H->counter.resize(1);
+  PA_CUDA(cudaMemsetAsync(H->counter.get(), 0, sizeof(unsigned int), s));
+  H->sc.resize(kScalars);
+  H->norms.resize(H->L.size() * 21);
+  const int64_t n3 = 3 * F.d.N;
+  H->p0.resize(n3);
+  H->p1.resize(n3);
+  H->q.resize(n3);
+  P.boxmg = H.release();
+}
+
+// True when the hierarchy must be (re)built for the problem's box.
+bool boxmg_stale(const Problem& P) {
+  const Mesh& m = *P.mesh;
+  if (P.boxmg == nullptr) return true;
+  for (int a = 0; a < 3; ++a)
+    if (P.boxmg->fine_n[a] != m.box_n[a] || P.boxmg->fine_l[a] != m.box_l[a]) return true;
+  return false;
+}
+
+bool boxmg_setup(Problem& P, const double* z) {
+  cudaStream_t s = P.stream;
+  if (boxmg_stale(P)) boxmg_setup_levels(P);
+  PA_CHECK(P.boxmg->L.size() >= 2, "PA_SOLVER_PCG_MG needs at least one coarse level");
+  BoxHierarchy& H = *P.boxmg;
+  BoxLevel& F = *H.L[0];
+  F.mask = P.d_node_mask.get();
+  // fine weights in box order
+  PA_CUDA(cudaMemsetAsync(H.differ.get(), 0, sizeof(unsigned int), s));
+  k_bweights<<<int((F.d.H + kVT - 1) / kVT), kVT, 0, s>>>(F.d, z, P.ep.layout, P.ep.p, P.ep.pmin, H.w64t.get(),
+                                                          H.w32t.get(), H.w64h.get(), H.w32h.get(), H.differ.get());
+  PA_LAUNCHED();
+  // masks by injection (host, from the problem's Dirichlet dofs)
+  std::vector<uint8_t> fmask(size_t(F.d.N), 0);
+  for (int32_t dof : P.bc_dofs) fmask[size_t(dof / 3)] |= uint8_t(1u << (dof % 3));
+  for (size_t l = 1; l < H.L.size(); ++l) {
+    std::vector<uint8_t> cmask;
+    coarse_mask(*H.L[l - 1], *H.L[l], fmask, cmask);
+    H.L[l]->own_mask.upload(cmask.data(), cmask.size(), s);
+    fmask.swap(cmask);
+  }
+  unsigned int differ = 0;
+  PA_CUDA(cudaMemcpyAsync(&differ, H.differ.get(), sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+  PA_CUDA(cudaStreamSynchronize(s));
+  F.wm = differ ? 1 : 0;
+  const double* fw64 = F.wm ? H.w64t.get() : H.w64h.get();
+  g_box_launches += 1;
+  // coarse weights and every level's inverse diagonal
+  const Iso<double> iso = P.ep.iso();
+  for (size_t l = 0; l < H.L.size(); ++l) {
+    BoxLevel& L = *H.L[l];
+    const double* lw = l == 0 ? fw64 : L.w64.get();
+    if (l > 0) {
+      const BoxLevel& Fl = *H.L[l - 1];
+      k_bcoarse_w<<<int((L.d.H + kVT - 1) / kVT), kVT, 0, s>>>(L.d, Fl.d, l == 1 ? fw64 : Fl.w64.get(),
+                                                               l == 1 ? F.wm : 0, L.w64.get(), L.w32.get());
+      PA_LAUNCHED();
+      g_box_launches += 1;
+    }
+    k_bdinv<<<int((L.d.N + kVT - 1) / kVT), kVT, 0, s>>>(L.d, L.h[0], L.h[1], L.h[2], iso.lam, iso.mu, lw,
+                                                         l == 0 ? F.wm : 0, L.mask, L.dinv.get());
+    PA_LAUNCHED();
+    g_box_launches += 1;
+  }
+  // coarsest level: dense inverse (eligibility guarantees at most 2048 dofs)
+  BoxLevel& Lc = *H.L.back();
+  {
+    const int64_t n3 = 3 * Lc.d.N, nd = (n3 + kGJ - 1) / kGJ * kGJ;
+    if (Lc.nd != nd) {
+      Lc.dense.resize(nd * nd);
+      Lc.gj_w.resize(kGJ * nd);
+      Lc.gj_c.resize(nd * kGJ);
+      Lc.gj_p.resize(kGJ * kGJ);
+      Lc.diag0.resize(nd);
+      Lc.flag.resize(1);
+      Lc.nd = nd;
+    }
+    PA_CUDA(cudaMemsetAsync(Lc.dense.get(), 0, sizeof(double) * nd * nd, s));
+    PA_CUDA(cudaMemsetAsync(Lc.flag.get(), 0, sizeof(double), s));
+    k_bdense_assemble<<<int((6 * Lc.d.H + kVT - 1) / kVT), kVT, 0, s>>>(Lc.d, Lc.h[0], Lc.h[1], Lc.h[2], iso,
+                                                                        Lc.w64.get(), Lc.mask, nd, Lc.dense.get());
+    k_bdense_ident<<<int((nd + kVT - 1) / kVT), kVT, 0, s>>>(Lc.d.N, nd, Lc.mask, Lc.dense.get(), Lc.diag0.get());
+    PA_LAUNCHED();
+    gj_invert(s, nd, Lc.dense.get(), Lc.diag0.get(), Lc.gj_w.get(), Lc.gj_c.get(), Lc.gj_p.get(), Lc.flag.get());
+    g_box_launches += 2 + 3 * (nd / kGJ);
+  }
+  // lmax of D^-1 K per smoothed level by power iteration, on the device
+  // (the norm of each step lands in norms[level][step]); an elastic solve
+  // after an elastic solve starts from the previous vector and takes 5 steps
+  constexpr int kPower = 20, kPowerWarm = 5;
+  const size_t NL = H.L.size();
+  const size_t NS = NL - 1;  // smoothed levels (the coarsest is solved exactly)
+  PA_CUDA(cudaMemsetAsync(H.norms.get(), 0, sizeof(double) * NL * (kPower + 1), s));
+  BoxRed red{H.partials.get(), H.counter.get()};
+  for (size_t l = 0; l < NS; ++l) {
+    BoxLevel& L = *H.L[l];
+    const int64_t n3 = 3 * L.d.N;
+    double* nl = H.norms.get() + l * (kPower + 1);
+    if (L.pw0.n != size_t(n3)) {
+      L.pw0.resize(n3);
+      L.pw1.resize(n3);
+      L.pw_valid = false;
+    }
+    const bool warm = L.pw_valid;
+    if (!warm)
+      k_bseed<<<vec_blocks(n3), kVT, 0, s>>>(L.d.N, L.mask, L.pw0.get(), H.partials.get(), H.counter.get(), nl);
+    else
+      k_bnorm2<<<vec_blocks(n3), kVT, 0, s>>>(n3, L.pw0.get(), H.partials.get(), H.counter.get(), nl);
+    PA_LAUNCHED();
+    g_box_launches += 1;
+    const int steps = warm ? kPowerWarm : kPower;
+    const BoxGeo<float> g = box_geo<float>(L, P.ep);
+    const float* lw32 = l == 0 ? (F.wm ? H.w32t.get() : H.w32h.get()) : L.w32.get();
+    for (int it = 1; it <= steps; ++it) {
+      float* xin = (it & 1) ? L.pw0.get() : L.pw1.get();
+      float* xout = (it & 1) ? L.pw1.get() : L.pw0.get();
+      launch_box<float>(L, g, lw32, InVec<float, float>{xin, nullptr, L.d.N},
+                        OutPower{xout, L.dinv.get(), nl + it - 1, nl + it, L.d.N}, red, s);
+    }
+    if (steps & 1) {  // the last vector in pw0
+      std::swap(L.pw0.p, L.pw1.p);
+      std::swap(L.pw0.n, L.pw1.n);
+    }
+  }
+  std::vector<double> h(NL * (kPower + 1));
+  PA_CUDA(cudaMemcpyAsync(h.data(), H.norms.get(), sizeof(double) * h.size(), cudaMemcpyDeviceToHost, s));
+  double flag = 0.0;
+  PA_CUDA(cudaMemcpyAsync(&flag, Lc.flag.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
+  PA_CUDA(cudaStreamSynchronize(s));
+  if (flag != 0.0) return false;
+  for (size_t l = 0; l < NS; ++l) {
+    BoxLevel& L = *H.L[l];
+    const bool warm = L.pw_valid;
+    const int steps = warm ? kPowerWarm : kPower;
+    PA_CHECK(h[l * (kPower + 1)] > 0.0, "multigrid level without free dofs");
+    double lam = 0.0;
+    for (int it = 1; it <= steps; ++it) {
+      const double v = h[l * (kPower + 1) + it];
+      if (std::isfinite(v)) lam = std::max(lam, std::sqrt(v));
+    }
+    PA_CHECK(lam > 0.0, "multigrid: no spectral estimate (zero operator?)");
+    if (warm) lam = std::max(lam, 0.95 * double(L.lmax));
+    L.lmax = float(lam);
+    L.pw_valid = true;
+  }
+  return true;
+}
+
+}  // namespace
+}  // namespace pa
+
+namespace pa {
+namespace {
+
+struct ChebStep {
+  float inv_theta, ca, c2;
+};
+
+// Degree-2 Chebyshev on [lmax / 10, lmax] (lmax = 1.15 x the estimate): the
+// first-step coefficients of the recurrence of pa_mg.cu (cheb_coeffs).
+ChebStep cheb2(float lmax_est) {
+  const double lmax = 1.15 * double(lmax_est), lmin = lmax / 10.0;
+  const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin), sigma = theta / delta;
+  const double rho = 1.0 / sigma;
+  const double rn = 1.0 / (2.0 * sigma - rho);
+  const double c1 = rn * rho, c2 = 2.0 * rn / delta;
+  return ChebStep{float(1.0 / theta), float((1.0 + c1) / theta + c2), float(c2)};
+}
+
+const float* level_w32(const BoxHierarchy& H, size_t l) {
+  const BoxLevel& L = *H.L[l];
+  if (l > 0) return L.w32.get();
+  return L.wm ? H.w32t.get() : H.w32h.get();
+}
+const double* level_w64(const BoxHierarchy& H, size_t l) {
+  const BoxLevel& L = *H.L[l];
+  if (l > 0) return L.w64.get();
+  return L.wm ? H.w64t.get() : H.w64h.get();
+}
+
+// the part of the V-cycle on level l and below that reads b (B) and writes x_out (O)
+template <typename B, typename O, bool RZ>
+void vcycle_level(const Problem& P, BoxHierarchy& H, size_t l, const B* b, O* xo, const double* rvec, double* sc,
+                  cudaStream_t s);
+
+void vcycle(const Problem& P, BoxHierarchy& H, size_t l, cudaStream_t s) {
+  // levels >= 1: b and x in the level's FP32 buffers
+  BoxLevel& L = *H.L[l];
+  if (l + 1 == H.L.size()) {
+    const int64_t n3 = 3 * L.d.N;
+    k_mg_dense_solve<<<int((32 * n3 + kVT - 1) / kVT), kVT, 0, s>>>(n3, L.nd, L.dense.get(), L.b.get(), L.x.get());
+    PA_LAUNCHED();
+    g_box_launches += 1;
+    return;
+  }
+  vcycle_level<float, float, false>(P, H, l, L.b.get(), L.x.get(), nullptr, nullptr, s);
+}
+
+template <typename B, typename O, bool RZ>
+void vcycle_level(const Problem& P, BoxHierarchy& H, size_t l, const B* b, O* xo, const double* rvec, double* sc,
+                  cudaStream_t s) {
+  BoxLevel& L = *H.L[l];
+  BoxLevel& C = *H.L[l + 1];
+  const ChebStep ch = cheb2(L.lmax);
+  const BoxGeo<float> g = box_geo<float>(L, P.ep);
+  const float* w = level_w32(H, l);
+  const BoxRed red{H.partials.get(), H.counter.get()};
+  const int64_t N = L.d.N;
+  // pre-smoothing from x = 0
+  launch_box<float>(L, g, w, InDinvB<B>{b, L.dinv.get(), ch.inv_theta, N},
+                    OutPre<B>{L.x.get(), b, L.dinv.get(), ch.ca, ch.c2, N}, red, s);
+  // residual, restricted to the coarse right-hand side
+  launch_box<float>(L, g, w, InVec<float, float>{L.x.get(), nullptr, N}, OutRes<B>{L.r.get(), b, L.mask, N}, red,
+                    s);
+  k_brestrict<<<int((C.d.N + kVT - 1) / kVT), kVT, 0, s>>>(C.d.nx, C.d.ny, C.d.nz, L.r.get(), N, C.mask, C.b.get(),
+                                                           C.d.N);
+  PA_LAUNCHED();
+  g_box_launches += 1;
+  vcycle(P, H, l + 1, s);
+  // post-smoothing from x + P e
+  const Prolong Pe{C.x.get(), C.d.px, C.d.py, C.d.N};
+  launch_box<float>(L, g, w, InProlong{L.x.get(), Pe, L.mask, N}, OutPost1<B>{L.r.get(), b, L.dinv.get(), N}, red,
+                    s);
+  launch_box<float>(L, g, w, InScaled{L.r.get(), ch.inv_theta, N},
+                    OutPost2<O, RZ>{xo, L.x.get(), Pe, L.mask, L.r.get(), L.dinv.get(), ch.ca, ch.c2, N, rvec, sc},
+                    red, s);
+}
+
+// y = K x (FP64, box kernel) with optional masks on input and output
+void box_apply64(const BoxLevel& L, const ElasticParams& ep, const double* w, const double* x, double* y,
+                 const uint8_t* mask, BoxRed red, cudaStream_t s) {
+  launch_box<double>(L, box_geo<double>(L, ep), w, InVec<double, double>{x, mask, L.d.N},
+                     OutPlain<double>{y, mask, L.d.N}, red, s);
+}
+
+// The hierarchy's levels and buffers (no device work besides allocation).
+void boxmg_ensure(Problem& P) {
+  if (boxmg_stale(P)) boxmg_setup_levels(P);
+}
+
+}  // namespace
+
+// Solve K x = b with the box multigrid-preconditioned CG for control z.
+// Returns false (nothing written) when the coarsest operator is singular.
+bool solve_boxmg(Problem& P, const double* z, const double* b, double* x_out, const pa_solve_options& o,
+                 pa_solve_stats* st, pa_status* status) {
+  cudaStream_t s = P.stream;
+  PA_CHECK(o.rel_tol > 0.0, "rel_tol must be positive");
+  g_box_launches = 0;
+  if (!boxmg_setup(P, z)) return false;
+  BoxHierarchy& H = *P.boxmg;
+  BoxLevel& F = *H.L[0];
+  const int64_t N = F.d.N, n = 3 * N;
+  SolverWorkspace& ws = P.ws;
+  const uint8_t* mask = F.mask;
+  const double* w64 = level_w64(H, 0);
+  const BoxRed red{H.partials.get(), H.counter.get()};
+  double* sc = H.sc.get();
+  double* bp = ws.b.get();
+  double* x = ws.x.get();
+  double* r = ws.r.get();
+  double* t = ws.t.get();
+  double* zv = ws.p0.get();
+  // b' = mask(b - K x_D), component-major, and ||b'||^2
+  const int64_t nbc = int64_t(P.bc_dofs.size());
+  launch_aos_to_soa<double, double>(b, t, N, s);
+  if (nbc) {
+    PA_CUDA(cudaMemsetAsync(zv, 0, sizeof(double) * n, s));
+    k_bscatter_bc<<<int((nbc + 255) / 256), 256, 0, s>>>(nbc, P.d_bc_dofs.get(), P.d_bc_vals.get(), 1.0, N, zv);
+    PA_LAUNCHED();
+    box_apply64(F, P.ep, w64, zv, H.q.get(), nullptr, red, s);
+    k_bres64<<<vec_blocks(n), kVT, 0, s>>>(N, t, H.q.get(), mask, bp, H.partials.get(), H.counter.get(), sc + kRr);
+  } else {
+    k_bres64<<<vec_blocks(n), kVT, 0, s>>>(N, t, nullptr, mask, bp, H.partials.get(), H.counter.get(), sc + kRr);
+  }
+  PA_LAUNCHED();
+  double bb = 0.0;
+  PA_CUDA(cudaMemcpyAsync(&bb, sc + kRr, sizeof(double), cudaMemcpyDeviceToHost, s));
+  PA_CUDA(cudaStreamSynchronize(s));
+  if (!(bb > 0.0)) bb = 1.0;
+  const double tol2 = o.rel_tol * o.rel_tol * bb;
+  const int max_iters = o.max_iters > 0 ? o.max_iters : 1000;
+  PA_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, s));
+  PA_CUDA(cudaMemcpyAsync(r, bp, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  PA_CUDA(cudaMemsetAsync(H.p0.get(), 0, sizeof(double) * n, s));
+  k_bcg_reset<<<1, 1, 0, s>>>(sc);
+  PA_LAUNCHED();
+  // one outer iteration as a graph; two variants alternate the p buffers
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  cudaGraph_t graph[2] = {nullptr, nullptr};
+  struct GraphGuard {
+    cudaGraph_t* g;
+    cudaGraphExec_t* e;
+    ~GraphGuard() {
+      for (int k = 0; k < 2; ++k) {
+        if (e[k]) cudaGraphExecDestroy(e[k]);
+        if (g[k]) cudaGraphDestroy(g[k]);
+      }
+    }
+  } guard{graph, gexec};
+  int64_t per_iter = 0;
+  for (int k = 0; k < 2; ++k) {
+    double* pold = k == 0 ? H.p0.get() : H.p1.get();
+    double* pnew = k == 0 ? H.p1.get() : H.p0.get();
+    const int64_t before = g_box_launches;
+    PA_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    vcycle_level<double, double, true>(P, H, 0, r, zv, r, sc, s);
+    launch_box<double>(F, box_geo<double>(F, P.ep), w64, InCgP{zv, pold, pnew, sc, N},
+                       OutCgQ{H.q.get(), zv, pold, mask, sc, N}, red, s);
+    k_bcg_update<<<vec_blocks(n), kVT, 0, s>>>(n, sc, pnew, H.q.get(), x, r, H.partials.get(), H.counter.get(),
+                                               sc + kRr);
+    g_box_launches += 1;
+    const cudaError_t ce = cudaStreamEndCapture(s, &graph[k]);
+    if (ce != cudaSuccess) throw Error(PA_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+    PA_CUDA(cudaGraphInstantiate(&gexec[k], graph[k], 0));
+    per_iter = g_box_launches - before;
+    g_box_launches = before;
+  }
+  int iters = 0, restarts = 0;
+  double rr_true = bb;
+  bool converged = false, breakdown = false;
+  double h2[2];
+  while (!converged && iters < max_iters && !breakdown) {
+    double rr = bb;
+    while (iters < max_iters) {
+      PA_CUDA(cudaGraphLaunch(gexec[iters & 1], s));
+      g_box_launches += per_iter;
+      ++iters;
+      PA_CUDA(cudaMemcpyAsync(h2, sc + kRr, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+      PA_CUDA(cudaStreamSynchronize(s));
+      rr = h2[0];
+      if (h2[1] != 0.0) {
+        breakdown = true;
+        break;
+      }
+      if (rr <= tol2) break;
+    }
+    if (breakdown) break;
+    // confirm on the true residual r = b' - K x (p and the scalars restart)
+    box_apply64(F, P.ep, w64, x, H.q.get(), mask, red, s);
+    k_bres64<<<vec_blocks(n), kVT, 0, s>>>(N, bp, H.q.get(), mask, r, H.partials.get(), H.counter.get(), sc + kRr);
+    PA_LAUNCHED();
+    g_box_launches += 1;
+    PA_CUDA(cudaMemcpyAsync(&rr_true, sc + kRr, sizeof(double), cudaMemcpyDeviceToHost, s));
+    PA_CUDA(cudaStreamSynchronize(s));
+    converged = rr_true <= tol2;
+    if (!converged && iters < max_iters) {
+      ++restarts;
+      k_bcg_reset<<<1, 1, 0, s>>>(sc);
+      PA_LAUNCHED();
+    }
+  }
+  // x_out = x + x_D (interleaved)
+  launch_soa_to_aos<double, double>(x, x_out, N, s);
+  if (nbc) {
+    k_bset_bc<<<int((nbc + 255) / 256), 256, 0, s>>>(nbc, P.d_bc_dofs.get(), P.d_bc_vals.get(), 1.0, x_out);
+    PA_LAUNCHED();
+  }
+  PA_CUDA(cudaEventRecord(P.ev1, s));
+  PA_CUDA(cudaEventSynchronize(P.ev1));
+  const double relres = std::sqrt(rr_true / bb);
+  if (st) {
+    st->iterations = iters;
+    st->replacements = restarts;
+    st->rel_residual = relres;
+    st->converged = converged ? 1 : 0;
+    st->kernel_launches = g_box_launches + 6;
+    st->fallback_iterations = 0;
+  }
+  *status = breakdown ? PA_ERR_BREAKDOWN : !std::isfinite(relres) ? PA_ERR_NONFINITE
+                                         : converged ? PA_OK : PA_ERR_NOT_CONVERGED;
+  return true;
+}
+
+// y = K(z) x on the box (component-major x, y; T = float or double), masked
+// when `constrained` (masked rows and columns zero), for pa_apply.
+template <typename T>
+void box_apply(Problem& P, const double* z, const T* x, T* y, bool constrained) {
+  cudaStream_t s = P.stream;
+  boxmg_ensure(P);
+  BoxHierarchy& H = *P.boxmg;
+  BoxLevel& F = *H.L[0];
+  PA_CUDA(cudaMemsetAsync(H.differ.get(), 0, sizeof(unsigned int), s));
+  k_bweights<<<int((F.d.H + kVT - 1) / kVT), kVT, 0, s>>>(F.d, z, P.ep.layout, P.ep.p, P.ep.pmin, H.w64t.get(),
+                                                          H.w32t.get(), H.w64h.get(), H.w32h.get(), H.differ.get());
+  PA_LAUNCHED();
+  unsigned int differ = 0;
+  PA_CUDA(cudaMemcpyAsync(&differ, H.differ.get(), sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+  PA_CUDA(cudaStreamSynchronize(s));
+  F.wm = differ ? 1 : 0;
+  const uint8_t* mask = constrained ? P.d_node_mask.get() : nullptr;
+  const BoxRed red{H.partials.get(), H.counter.get()};
+  if constexpr (std::is_same<T, double>::value) {
+    box_apply64(F, P.ep, level_w64(H, 0), x, y, mask, red, s);
+  } else {
+    launch_box<float>(F, box_geo<float>(F, P.ep), level_w32(H, 0), InVec<float, float>{x, mask, F.d.N},
+                      OutPlain<float>{y, mask, F.d.N}, red, s);
+  }
+}
+template void box_apply<double>(Problem&, const double*, const double*, double*, bool);
+template void box_apply<float>(Problem&, const double*, const float*, float*, bool);
+
+// Device time of the plain FP32 (or FP64) box apply over `reps` launches
+// (weights from z, random x), and its algorithmic bytes per launch: weights
+// (one per hex when the tets of every hex share it), x in and y out.
+double time_box_apply(Problem& P, const double* z, bool fp32, int reps, int64_t* bytes) {
+  cudaStream_t s = P.stream;
+  const int64_t n = P.ndof();
+  DevBuf<float> x32, y32;
+  DevBuf<double> x64, y64;
+  if (fp32) {
+    x32.resize(n);
+    y32.resize(n);
+    PA_CUDA(cudaMemsetAsync(x32.get(), 0, sizeof(float) * n, s));
+    box_apply<float>(P, z, x32.get(), y32.get(), true);
+  } else {
+    x64.resize(n);
+    y64.resize(n);
+    PA_CUDA(cudaMemsetAsync(x64.get(), 0, sizeof(double) * n, s));
+    box_apply<double>(P, z, x64.get(), y64.get(), true);
+  }
+  BoxHierarchy& H = *P.boxmg;
+  BoxLevel& F = *H.L[0];
+  const BoxRed red{H.partials.get(), H.counter.get()};
+  const uint8_t* mask = P.d_node_mask.get();
+  cudaEvent_t e0, e1;
+  PA_CUDA(cudaEventCreate(&e0));
+  PA_CUDA(cudaEventCreate(&e1));
+  PA_CUDA(cudaEventRecord(e0, s));
+  for (int k = 0; k < reps; ++k) {
+    if (fp32)
+      launch_box<float>(F, box_geo<float>(F, P.ep), level_w32(H, 0), InVec<float, float>{x32.get(), mask, F.d.N},
+                        OutPlain<float>{y32.get(), mask, F.d.N}, red, s);
+    else
+      box_apply64(F, P.ep, level_w64(H, 0), x64.get(), y64.get(), mask, red, s);
+  }
+  PA_CUDA(cudaEventRecord(e1, s));
+  PA_CUDA(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  PA_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  const int64_t sv = fp32 ? 4 : 8;
+  if (bytes) *bytes = (F.wm ? 6 * F.d.H : F.d.H) * sv + F.d.N * (6 * sv + 1);
+  return double(ms) / reps;
+}
+
+}  // namespace pa

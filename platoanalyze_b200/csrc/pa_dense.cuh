@@ -14,45 +14,58 @@ namespace {
 
 constexpr int kGJ = 64, kGJc = 32;
 
-// In-place Gauss-Jordan of the pivot block A[K,K] -> P^-1 (one CTA).  A pivot
-// that is not above 1e-12 of its row's original diagonal marks the matrix as
-// (numerically) singular in *flag.  The pivots and original diagonals stay in
-// shared memory and are checked once after the loop, so no column waits on a
-// global load.
+// In-place Gauss-Jordan of the pivot block A[K,K] -> P^-1 (one CTA of 256
+// threads).  Thread t keeps the 4 x 4 sub-block (rows 4 (t / 16) + i, columns
+// 4 (t % 16) + j) in registers; for each pivot p the owners of row p and
+// column p publish them in shared memory (double-buffered, one barrier per
+// pivot) and every thread updates its sub-block.  A pivot that is not above
+// 1e-12 of its row's original diagonal marks the matrix as (numerically)
+// singular in *flag, checked once after the loop.
 __global__ void __launch_bounds__(256) k_gj_pivot(int64_t nd, int64_t k0, const double* __restrict__ A,
                                                   const double* __restrict__ diag0, double* __restrict__ piv,
                                                   double* __restrict__ flag) {
-  __shared__ double P[kGJ][kGJ + 1];
-  __shared__ double row[kGJ], col[kGJ], pivots[kGJ], d0[kGJ];
-  for (int e = threadIdx.x; e < kGJ * kGJ; e += blockDim.x) P[e / kGJ][e % kGJ] = A[(k0 + e / kGJ) * nd + k0 + e % kGJ];
-  if (threadIdx.x < kGJ) d0[threadIdx.x] = diag0[k0 + threadIdx.x];
-  __syncthreads();
+  __shared__ double rowb[2][kGJ], colb[2][kGJ], pivots[kGJ];
+  const int a = threadIdx.x >> 4, b = threadIdx.x & 15;
+  double R[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) R[i][j] = A[(k0 + 4 * a + i) * nd + k0 + 4 * b + j];
   for (int p = 0; p < kGJ; ++p) {
-    if (threadIdx.x < kGJ) {
-      row[threadIdx.x] = P[p][threadIdx.x];
-      col[threadIdx.x] = P[threadIdx.x][p];
+    const int q = p & 1, pr = p >> 2, pc = p & 3;
+    if (b == pr) {  // this thread holds column p for its four rows
+#pragma unroll
+      for (int i = 0; i < 4; ++i) colb[q][4 * a + i] = pc == 0 ? R[i][0] : pc == 1 ? R[i][1] : pc == 2 ? R[i][2] : R[i][3];
+    }
+    if (a == pr) {  // and row p for its four columns
+#pragma unroll
+      for (int j = 0; j < 4; ++j) rowb[q][4 * b + j] = pc == 0 ? R[0][j] : pc == 1 ? R[1][j] : pc == 2 ? R[2][j] : R[3][j];
     }
     __syncthreads();
-    const double pv = row[p];
+    const double pv = rowb[q][p];
     if (threadIdx.x == 0) pivots[p] = pv;
     const double ip = 1.0 / pv;
-    for (int e = threadIdx.x; e < kGJ * kGJ; e += blockDim.x) {
-      const int r = e / kGJ, c = e % kGJ;
-      double val;
-      if (r == p && c == p)
-        val = ip;
-      else if (r == p)
-        val = row[c] * ip;
-      else if (c == p)
-        val = -col[r] * ip;
-      else
-        val = P[r][c] - col[r] * row[c] * ip;
-      P[r][c] = val;
+    double cr[4], rc[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      cr[i] = colb[q][4 * a + i] * ip;
+      rc[i] = rowb[q][4 * b + i];
     }
-    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const bool rp = 4 * a + i == p, cp = 4 * b + j == p;
+        const double gen = R[i][j] - cr[i] * rc[j];
+        R[i][j] = rp ? (cp ? ip : rc[j] * ip) : (cp ? -cr[i] : gen);
+      }
   }
-  if (threadIdx.x < kGJ && !(pivots[threadIdx.x] > 1e-12 * d0[threadIdx.x])) *flag = 1.0;
-  for (int e = threadIdx.x; e < kGJ * kGJ; e += blockDim.x) piv[e] = P[e / kGJ][e % kGJ];
+  __syncthreads();
+  if (threadIdx.x < kGJ && !(pivots[threadIdx.x] > 1e-12 * diag0[k0 + threadIdx.x])) *flag = 1.0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) piv[(4 * a + i) * kGJ + 4 * b + j] = R[i][j];
 }
 
 // acc (this thread's 4x4 outputs of a 64x64 tile) += L[64 x 64] R[64 x 64];

@@ -130,6 +130,7 @@ struct Mesh {
   // structured box (mesh_make_box): hex counts and lengths; 0 for other meshes
   int box_n[3] = {0, 0, 0};
   double box_l[3] = {0.0, 0.0, 0.0};
+  bool box_kernels = true;  // structured boxes: apply and multigrid on the box kernel (pa_box.cuh)
   DevBuf<int32_t> d_tile_cluster_start, d_tile_cell_start, d_tile_hex_count, d_tile_node_start, d_cell_perm;
   DevBuf<int32_t> d_cell_iperm;  // user -> internal cell id
   DevBuf<uint32_t> d_tile_nodes;

@@ -38,11 +38,13 @@ struct SolveOperator {
 
 struct LearnedPC;
 struct MgHierarchy;
+struct BoxHierarchy;
 
 struct Problem {
   Mesh* mesh = nullptr;
   LearnedPC* pc = nullptr;  // network of PA_SOLVER_FCG_LEARNED (not owned)
   MgHierarchy* mg = nullptr;  // coarse levels of PA_SOLVER_PCG_MG (owned; mg_release)
+  BoxHierarchy* boxmg = nullptr;  // the same on box kernels (owned; boxmg_release)
   ElasticParams ep{};
   cudaStream_t stream = nullptr;
   bool own_stream = false;
@@ -82,5 +84,17 @@ pa_status solve_batched(Problem& P, const SolveOperator& op, const double* b, do
 pa_status solve_mg(Problem& P, const SolveOperator& op, const double* b, double* x_out, const pa_solve_options& o,
                    pa_solve_stats* st);
 void mg_release(Problem& P);
+
+// Structured boxes (pa_boxmg.cu): the box kernel of pa_box.cuh applies the
+// operator; multigrid CG with every level on it.
+bool box_apply_eligible(const Problem& P);
+bool boxmg_eligible(const Problem& P);
+// false (nothing written) when the coarsest operator is singular
+bool solve_boxmg(Problem& P, const double* z, const double* b, double* x_out, const pa_solve_options& o,
+                 pa_solve_stats* st, pa_status* status);
+template <typename T>
+void box_apply(Problem& P, const double* z, const T* x, T* y, bool constrained);
+double time_box_apply(Problem& P, const double* z, bool fp32, int reps, int64_t* bytes);
+void boxmg_release(Problem& P);
 
 }  // namespace pa

@@ -1017,6 +1017,22 @@ pa_status solve_device(Problem& P, const double* z, const double* b, double* x_o
   P.ws.ensure(n, P.C(), grid_need, mixed || mg);
   SolverWorkspace& ws = P.ws;
   if (!P.ev0) { PA_CUDA(cudaEventCreate(&P.ev0)); PA_CUDA(cudaEventCreate(&P.ev1)); }
+  if (mg && o.mg_coarse_solver == PA_MG_COARSE_AUTO && boxmg_eligible(P)) {
+    // structured box: every level on the box kernel
+    cudaEvent_t t0;
+    PA_CUDA(cudaEventCreate(&t0));
+    PA_CUDA(cudaEventRecord(t0, P.stream));
+    pa_status status = PA_OK;
+    const bool done = solve_boxmg(P, z, b, x_out, o, st, &status);
+    if (done) {
+      float ms = 0.f;
+      PA_CUDA(cudaEventElapsedTime(&ms, t0, P.ev1));
+      cudaEventDestroy(t0);
+      if (st) st->seconds = ms * 1e-3;  // weights, diagonals and the hierarchy's set-up included
+      return status;
+    }
+    cudaEventDestroy(t0);  // singular coarsest operator: the tile-kernel hierarchy below
+  }
   if (mg) {
     PA_CHECK(P.mesh->num_parts == 1, "PA_SOLVER_PCG_MG solves one box (not a parted mesh)");
     cudaEvent_t t0;

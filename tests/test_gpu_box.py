@@ -1,0 +1,151 @@
+"""The box kernel (structured boxes of pa_mesh_create_box): K x through
+pa_apply against the FP64 oracle and against the tile kernel, and the
+multigrid solve whose every level runs on it against the oracle and the
+tile-kernel multigrid.
+
+Tolerances: FP64 apply 1e-12 relative (infinity norm) against the oracle;
+FP32 apply 1e-5; solves to relres 1e-10 checked by the oracle's own
+operator, and within 1e-7 of the FP64 Jacobi-PCG solution."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_inf(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+# (hexes, lengths, control layout, per-hex densities?) -- sizes cross the
+# CTA brick edges (31 nodes along x, 7 along y, kz planes along z)
+APPLY_CASES = [
+    ((12, 8, 6), (12.0, 8.0, 6.0), "cell", True),
+    ((40, 9, 17), (40.0, 9.0, 17.0), "cell", False),
+    ((33, 15, 10), (1.0, 2.0, 3.0), "nodal", False),  # non-cubic hexes
+    ((2, 2, 2), (2.0, 2.0, 2.0), "cell", False),
+    ((64, 8, 8), (64.0, 8.0, 8.0), "cell", True),
+]
+
+
+@pytest.mark.parametrize("case", APPLY_CASES, ids=lambda c: f"{c[0][0]}x{c[0][1]}x{c[0][2]}-{c[2]}-{'hex' if c[3] else 'tet'}")
+def test_box_apply_matches_oracle_and_tile_kernel(pa, oracle_lib, case):
+    from oracle import np_ref
+    (nx, ny, nz), (lx, ly, lz), layout, per_hex = case
+    rng = np.random.default_rng(nx * 100 + nz)
+    mesh = pa.Mesh.box(nx, ny, nz, lx, ly, lz)
+    assert mesh.box_kernels
+    E, nu, p, pmin = 2.5, 0.31, 3.0, 1e-6
+    prob = pa.Problem(mesh, E, nu, p, pmin, control_layout=layout)
+    cells, coords = np_ref.box_mesh(nx, ny, nz, lx, ly, lz)
+    lay = 1 if layout == "cell" else 0
+    O = oracle_lib.Oracle(cells, coords, E=E, nu=nu, p=p, pmin=pmin, layout=lay)
+    if layout == "cell":
+        z = np.repeat(rng.uniform(0.05, 1.0, nx * ny * nz), 6) if per_hex else rng.uniform(0.05, 1.0, O.C)
+    else:
+        z = rng.uniform(0.05, 1.0, O.N)
+    x = rng.standard_normal(3 * O.N)
+    y_ref = O.apply(x, z)
+    y_box = prob.apply(z, x)
+    assert rel_inf(y_box, y_ref) <= 1e-12
+    # constrained: x = 0 face clamped (identity rows) and one more node's y dof
+    clamp = np.where(coords[:, 0] == 0.0)[0]
+    dofs = np.sort(np.concatenate([3 * clamp, 3 * clamp + 1, 3 * clamp + 2, [3 * (O.N - 1) + 1]])).astype(np.int32)
+    prob.set_dirichlet(dofs)
+    yc_box = prob.apply(z, x, constrained=True)
+    free = np.ones(3 * O.N, bool)
+    free[dofs] = False
+    yc_ref = O.apply(np.where(free, x, 0.0), z)
+    yc_ref[~free] = x[~free]
+    assert rel_inf(yc_box, yc_ref) <= 1e-12
+    # FP32 box kernel, and the tile kernel on the same mesh
+    y32 = prob.apply(z, x.astype(np.float32), constrained=True)
+    assert rel_inf(y32, yc_ref) <= 1e-5
+    mesh.set_box_kernels(False)
+    assert not mesh.box_kernels
+    yc_tile = prob.apply(z, x, constrained=True)
+    assert rel_inf(yc_tile, yc_box) <= 1e-12
+
+
+def _cantilever(dims, seed, lengths=None):
+    from platoanalyze_b200.workloads import cantilever, cell_density
+    mesh, prob, faces, dofs = cantilever(dims)
+    z = cell_density(dims, seed, kind="smoothed", sigma=1.5, lo=0.01, hi=1.0)
+    return mesh, prob, faces, dofs, z
+
+
+@pytest.mark.parametrize("dims", [(16, 8, 8), (24, 12, 12), (64, 16, 16)])
+def test_box_mg_matches_oracle_and_tile_mg(pa, oracle_lib, dims):
+    from oracle import np_ref
+    mesh, prob, faces, dofs, z = _cantilever(dims, 3)
+    u, st = prob.solution(z, options=pa.SolveOptions("mg", rel_tol=1e-10))
+    assert st["converged"] and st["rel_residual"] <= 1e-10, st
+    nx, ny, nz = dims
+    cells, coords = np_ref.box_mesh(nx, ny, nz, float(nx), float(ny), float(nz))
+    O = oracle_lib.Oracle(cells, coords, E=1.0, nu=0.3, p=3.0, pmin=1e-9, layout=1)
+    flux = np.array([0.0, 0.0, -1.0 / (ny * nz)])
+    F = -O.residual(np.zeros_like(u), z, faces, flux)
+    res = F - O.apply(u, z)
+    res[dofs] = 0.0
+    assert np.linalg.norm(res) <= 1.01e-10 * np.linalg.norm(F)
+    u64, _ = prob.solution(z, options=pa.SolveOptions("fp64", rel_tol=1e-11))
+    assert rel_inf(u, u64) <= 1e-7
+    # the same method on the tile kernels: the same iteration count (to one)
+    mesh.set_box_kernels(False)
+    ut, stt = prob.solution(z, options=pa.SolveOptions("mg", rel_tol=1e-10))
+    assert stt["converged"], stt
+    assert abs(stt["iterations"] - st["iterations"]) <= 1, (st, stt)
+    assert rel_inf(ut, u) <= 1e-7
+    # deterministic (no atomics): a fresh problem's first solve gives the same
+    # bits (a later solve on the same problem starts its spectral estimates
+    # from the previous solve's vector)
+    mesh.set_box_kernels(True)
+    from platoanalyze_b200.workloads import cantilever
+    _, prob2, _, _ = cantilever(dims)
+    u2, st2 = prob2.solution(z, options=pa.SolveOptions("mg", rel_tol=1e-10))
+    assert st2["iterations"] == st["iterations"] and np.array_equal(u2, u)
+
+
+def test_box_mg_nodal_per_tet_noncubic_inhomogeneous(pa, oracle_lib):
+    """Nodal controls (per-tet weights), non-cubic hexes (lengths 2 x 1 x 1.5
+    over 16 x 8 x 8) and prescribed nonzero Dirichlet values."""
+    from oracle import np_ref
+    nx, ny, nz = 16, 8, 8
+    lx, ly, lz = 2.0, 1.0, 1.5
+    mesh = pa.Mesh.box(nx, ny, nz, lx, ly, lz)
+    prob = pa.Problem(mesh, 1.0, 0.3, 3.0, 1e-9, control_layout="nodal")
+    cells, coords = np_ref.box_mesh(nx, ny, nz, lx, ly, lz)
+    faces = mesh.boundary_faces(0, lx)
+    flux = np.array([0.0, 0.3, -1.0])
+    prob.add_traction(faces, flux)
+    clamp = np.where(coords[:, 0] == 0.0)[0]
+    dofs = np.sort(np.concatenate([3 * clamp, 3 * clamp + 1, 3 * clamp + 2])).astype(np.int32)
+    vals = 0.01 * np.cos(np.arange(dofs.size))
+    prob.set_dirichlet(dofs, vals)
+    rng = np.random.default_rng(9)
+    z = rng.uniform(0.1, 1.0, coords.shape[0])
+    u, st = prob.solution(z, options=pa.SolveOptions("mg", rel_tol=1e-10))
+    assert st["converged"], st
+    assert np.array_equal(u[dofs], vals)
+    O = oracle_lib.Oracle(cells, coords, E=1.0, nu=0.3, p=3.0, pmin=1e-9, layout=0)
+    F = -O.residual(np.zeros_like(u), z, faces, flux)
+    res = F - O.apply(u, z)
+    res[dofs] = 0.0
+    ud = np.zeros_like(u)
+    ud[dofs] = vals
+    Fb = F - O.apply(ud, z)
+    Fb[dofs] = 0.0
+    assert np.linalg.norm(res) <= 1.01e-10 * np.linalg.norm(Fb)
+    u64, _ = prob.solution(z, options=pa.SolveOptions("fp64", rel_tol=1e-11))
+    assert rel_inf(u, u64) <= 1e-7
+
+
+def test_box_mg_density_change_reuses_hierarchy(pa):
+    mesh, prob, faces, dofs, z = _cantilever((32, 16, 16), 11)
+    from platoanalyze_b200.workloads import cell_density
+    for seed in (11, 12, 13):
+        zz = cell_density((32, 16, 16), seed, kind="smoothed", sigma=2.0, lo=0.01, hi=1.0)
+        u, st = prob.solution(zz, options=pa.SolveOptions("mg", rel_tol=1e-10))
+        u64, _ = prob.solution(zz, options=pa.SolveOptions("fp64", rel_tol=1e-11))
+        assert st["converged"], st
+        assert rel_inf(u, u64) <= 1e-7
