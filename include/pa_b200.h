@@ -103,7 +103,10 @@ pa_status pa_mesh_set_graph(pa_mesh* mesh, const int32_t* rowmap, const int32_t*
  * allowed only before problems are created on the mesh. */
 pa_status pa_mesh_uniform_geometry(pa_mesh* mesh, int32_t enable, int32_t* active);
 
-/* Box kernels.  On a box made by pa_mesh_create_box the matrix-free operator
+/* Box kernels.  On a box lattice (made by pa_mesh_create_box, or given to
+ * pa_mesh_create as arrays that form such a box -- equal axis-aligned hexes
+ * split into the same six tets along one cube diagonal, as Omega_h build_box
+ * does -- under any node, cell and vertex order) the matrix-free operator
  * (pa_apply) and every level of the multigrid solve (PA_SOLVER_PCG_MG) run on
  * a kernel that derives node ids from the lattice and works on the tets as
  * edge differences of their hex (no connectivity, coordinates or geometry

@@ -555,12 +555,13 @@ pa_status pa_apply(pa_problem* problem, const double* z, const void* x, void* y,
       pa::DevBuf<double>& ys = P.ws.t;
       if (xs.n < size_t(n)) xs.resize(n);
       if (ys.n < size_t(n)) ys.resize(n);
-      pa::launch_aos_to_soa<double, double>(dx, xs.get(), P.N(), P.stream);
-      if (box)
-        pa::box_apply<double>(P, dz, xs.get(), ys.get(), constrained != 0);
-      else
+      if (box) {
+        pa::box_apply<double>(P, dz, dx, dy, constrained != 0, xs.get(), ys.get());
+      } else {
+        pa::launch_aos_to_soa<double, double>(dx, xs.get(), P.N(), P.stream);
         pa::launch_apply_tiled<double>(P, P.ws.w64.get(), xs.get(), ys.get(), constrained != 0, P.stream);
-      pa::launch_soa_to_aos<double, double>(ys.get(), dy, P.N(), P.stream);
+        pa::launch_soa_to_aos<double, double>(ys.get(), dy, P.N(), P.stream);
+      }
       pa::launch_copy_dofs<double>(P.d_bc_dofs.get(), nbc, dx, dy, P.stream);  // identity rows
     } else {
       const float* dx = st.in(static_cast<const float*>(x), n, "x");
@@ -569,12 +570,13 @@ pa_status pa_apply(pa_problem* problem, const double* z, const void* x, void* y,
       pa::DevBuf<float>& ys = P.ws.ap32;
       if (xs.n < size_t(n)) xs.resize(n);
       if (ys.n < size_t(n)) ys.resize(n);
-      pa::launch_aos_to_soa<float, float>(dx, xs.get(), P.N(), P.stream);
-      if (box)
-        pa::box_apply<float>(P, dz, xs.get(), ys.get(), constrained != 0);
-      else
+      if (box) {
+        pa::box_apply<float>(P, dz, dx, dy, constrained != 0, xs.get(), ys.get());
+      } else {
+        pa::launch_aos_to_soa<float, float>(dx, xs.get(), P.N(), P.stream);
         pa::launch_apply_tiled<float>(P, P.ws.w32.get(), xs.get(), ys.get(), constrained != 0, P.stream);
-      pa::launch_soa_to_aos<float, float>(ys.get(), dy, P.N(), P.stream);
+        pa::launch_soa_to_aos<float, float>(ys.get(), dy, P.N(), P.stream);
+      }
       pa::launch_copy_dofs<float>(P.d_bc_dofs.get(), nbc, dx, dy, P.stream);
     }
     st.finish();
@@ -1040,7 +1042,7 @@ pa_status pa_mesh_box_kernels(pa_mesh* mesh, int32_t enable, int32_t* active) {
     PA_CHECK(mesh, "null pa_mesh");
     pa::Mesh& m = mesh->m;
     if (enable >= 0) m.box_kernels = enable != 0;
-    if (active) *active = (m.box_kernels && m.box_n[0] > 0) ? 1 : 0;
+    if (active) *active = (m.box_kernels && m.lat_n[0] > 0) ? 1 : 0;
   });
 }
 

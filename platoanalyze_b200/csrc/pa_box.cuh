@@ -29,7 +29,7 @@
 // by exactly one thread, in a fixed order: no atomics, deterministic, and
 // the epilogue sees the final y of its node, so vector updates (Chebyshev
 // steps, residuals, CG dot products) fuse into the same kernel.  The input
-// vector is formed once per node and plane into shared memory (three plane
+// vector is formed once per node and plane into shared memory (four plane
 // buffers, one barrier per hex layer), its global loads issued a layer
 // before they are needed.
 #pragma once
@@ -90,82 +90,135 @@ __device__ __forceinline__ double block_sum_box(double v, double* smem /*>= 32*/
   return v;
 }
 
-// One path tet: forces of corner displacements u into f.
-template <int P1, int P2, int P3, bool CUBE, typename T>
-__device__ __forceinline__ void box_tet(const T (&u)[8][3], T lam, T mu, const T (&ih)[3], T (&f)[8][3]) {
-  constexpr int v1 = 1 << P1, v2 = v1 | (1 << P2);
-  T G[3][3];
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    G[c][P1] = u[v1][c] - u[0][c];
-    G[c][P2] = u[v2][c] - u[v1][c];
-    G[c][P3] = u[7][c] - u[v2][c];
-    if constexpr (!CUBE) {
-      G[c][P1] *= ih[P1];
-      G[c][P2] *= ih[P2];
-      G[c][P3] *= ih[P3];
-    }
-  }
-  const T lt = lam * (G[0][0] + G[1][1] + G[2][2]);
-  const T m2 = mu + mu;
-  T s[3][3];
-  s[0][0] = fma(m2, G[0][0], lt);
-  s[1][1] = fma(m2, G[1][1], lt);
-  s[2][2] = fma(m2, G[2][2], lt);
-  s[0][1] = s[1][0] = mu * (G[0][1] + G[1][0]);
-  s[0][2] = s[2][0] = mu * (G[0][2] + G[2][0]);
-  s[1][2] = s[2][1] = mu * (G[1][2] + G[2][1]);
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    T S1 = s[c][P1], S2 = s[c][P2], S3 = s[c][P3];
-    if constexpr (!CUBE) {
-      S1 *= ih[P1];
-      S2 *= ih[P2];
-      S3 *= ih[P3];
-    }
-    f[0][c] -= S1;
-    f[v1][c] += S1 - S2;
-    f[v2][c] += S2 - S3;
-    f[7][c] += S3;
-  }
-}
+// Shared-memory node record: FP32 (x, y, z, unused) in one 16-byte access;
+// FP64 (x, y, z) in three 8-byte accesses (24 bytes keep the FP64 kernel's
+// plane buffers within 48 KB).
+template <typename T>
+struct BoxV4;
+template <>
+struct alignas(16) BoxV4<float> {
+  float x, y, z, w;
+  __device__ BoxV4() {}
+  __device__ BoxV4(float a, float b, float c) : x(a), y(b), z(c), w(0.f) {}
+};
+template <>
+struct BoxV4<double> {
+  double x, y, z;
+  __device__ BoxV4() {}
+  __device__ BoxV4(double a, double b, double c) : x(a), y(b), z(c) {}
+};
 
-// Forces of one hex (six tets) for corner displacements u; w: the hex's
-// weight (WM = 0) or its six tet weights.
-template <bool CUBE, int WM, typename T>
-__device__ __forceinline__ void box_hex(const T (&u)[8][3], const T (&w)[WM ? 6 : 1], const BoxGeo<T>& g,
+// Forces of one hex for corner displacements u (corner c = a + 2b + 4c).
+// The twelve hex edges carry the displacement differences; tet t (its path
+// edges listed below) takes its displacement gradient columns from its three
+// edges, and its edge fluxes (stress columns) accumulate per edge; a corner's
+// force is the sum of the fluxes of the edges that end there minus those that
+// start there:
+//   t0 Y00 X10 Z11   t1 Y00 Z01 X11   t2 Z00 Y01 X11
+//   t3 Z00 X01 Y11   t4 X00 Z10 Y11   t5 X00 Y10 Z11
+// (X_bc: x-edge from corner 2b + 4c; Y_ac: y-edge from a + 4c; Z_ab: z-edge
+// from a + 2b).  lw, mw: the six tets' Lame parameters times weight and
+// volume (and 1/h^2 for cubes).
+template <bool CUBE, typename T>
+__device__ __forceinline__ void box_hex(const T (&u)[8][3], const T (&lw)[6], const T (&mw)[6], const T (&ih)[3],
                                         T (&f)[8][3]) {
+  T X00[3], X10[3], X01[3], X11[3], Y00[3], Y10[3], Y01[3], Y11[3], Z00[3], Z10[3], Z01[3], Z11[3];
 #pragma unroll
-  for (int c = 0; c < 8; ++c) f[c][0] = f[c][1] = f[c][2] = T(0);
-  auto W = [&](int t) { return WM ? w[WM ? t : 0] : w[0]; };
-  box_tet<1, 0, 2, CUBE>(u, W(0) * g.lam, W(0) * g.mu, g.ih, f);
-  box_tet<1, 2, 0, CUBE>(u, W(1) * g.lam, W(1) * g.mu, g.ih, f);
-  box_tet<2, 1, 0, CUBE>(u, W(2) * g.lam, W(2) * g.mu, g.ih, f);
-  box_tet<2, 0, 1, CUBE>(u, W(3) * g.lam, W(3) * g.mu, g.ih, f);
-  box_tet<0, 2, 1, CUBE>(u, W(4) * g.lam, W(4) * g.mu, g.ih, f);
-  box_tet<0, 1, 2, CUBE>(u, W(5) * g.lam, W(5) * g.mu, g.ih, f);
+  for (int c = 0; c < 3; ++c) {
+    X00[c] = u[1][c] - u[0][c];
+    X10[c] = u[3][c] - u[2][c];
+    X01[c] = u[5][c] - u[4][c];
+    X11[c] = u[7][c] - u[6][c];
+    Y00[c] = u[2][c] - u[0][c];
+    Y10[c] = u[3][c] - u[1][c];
+    Y01[c] = u[6][c] - u[4][c];
+    Y11[c] = u[7][c] - u[5][c];
+    Z00[c] = u[4][c] - u[0][c];
+    Z10[c] = u[5][c] - u[1][c];
+    Z01[c] = u[6][c] - u[2][c];
+    Z11[c] = u[7][c] - u[3][c];
+    if constexpr (!CUBE) {
+      X00[c] *= ih[0]; X10[c] *= ih[0]; X01[c] *= ih[0]; X11[c] *= ih[0];
+      Y00[c] *= ih[1]; Y10[c] *= ih[1]; Y01[c] *= ih[1]; Y11[c] *= ih[1];
+      Z00[c] *= ih[2]; Z10[c] *= ih[2]; Z01[c] *= ih[2]; Z11[c] *= ih[2];
+    }
+  }
+  // stress columns (edge fluxes) of a tet with gradient columns gx, gy, gz
+  auto tet = [&](const T (&gx)[3], const T (&gy)[3], const T (&gz)[3], T l, T m, T (&sx)[3], T (&sy)[3],
+                 T (&sz)[3]) {
+    const T lt = l * (gx[0] + gy[1] + gz[2]);
+    const T m2 = m + m;
+    const T sxy = m * (gy[0] + gx[1]), sxz = m * (gz[0] + gx[2]), syz = m * (gz[1] + gy[2]);
+    sx[0] = fma(m2, gx[0], lt);
+    sy[1] = fma(m2, gy[1], lt);
+    sz[2] = fma(m2, gz[2], lt);
+    sx[1] = sy[0] = sxy;
+    sx[2] = sz[0] = sxz;
+    sy[2] = sz[1] = syz;
+    if constexpr (!CUBE) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        sx[c] *= ih[0];
+        sy[c] *= ih[1];
+        sz[c] *= ih[2];
+      }
+    }
+  };
+  T qX00[3], qX10[3], qX01[3], qX11[3], qY00[3], qY10[3], qY01[3], qY11[3], qZ00[3], qZ10[3], qZ01[3], qZ11[3];
+  T a[3], b[3], c3[3];
+  tet(X10, Y00, Z11, lw[0], mw[0], qX10, qY00, qZ11);  // t0
+  tet(X11, Y00, Z01, lw[1], mw[1], qX11, a, qZ01);      // t1
+#pragma unroll
+  for (int c = 0; c < 3; ++c) qY00[c] += a[c];
+  tet(X11, Y01, Z00, lw[2], mw[2], a, qY01, qZ00);      // t2
+#pragma unroll
+  for (int c = 0; c < 3; ++c) qX11[c] += a[c];
+  tet(X01, Y11, Z00, lw[3], mw[3], qX01, qY11, a);      // t3
+#pragma unroll
+  for (int c = 0; c < 3; ++c) qZ00[c] += a[c];
+  tet(X00, Y11, Z10, lw[4], mw[4], qX00, a, qZ10);      // t4
+#pragma unroll
+  for (int c = 0; c < 3; ++c) qY11[c] += a[c];
+  tet(X00, Y10, Z11, lw[5], mw[5], b, qY10, c3);        // t5
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    qX00[c] += b[c];
+    qZ11[c] += c3[c];
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    f[0][c] = -(qX00[c] + qY00[c]) - qZ00[c];
+    f[1][c] = qX00[c] - qY10[c] - qZ10[c];
+    f[2][c] = qY00[c] - qX10[c] - qZ01[c];
+    f[3][c] = qX10[c] + qY10[c] - qZ11[c];
+    f[4][c] = qZ00[c] - qX01[c] - qY01[c];
+    f[5][c] = qX01[c] + qZ10[c] - qY11[c];
+    f[6][c] = qY01[c] + qZ01[c] - qX11[c];
+    f[7][c] = qX11[c] + qY11[c] + qZ11[c];
+  }
 }
 
 // y = K x on the box with a fused input former and epilogue.  Both are split
 // into a load part (global loads into registers, issued a hex layer before
 // the values are needed) and a compute part:
 //   In:  struct Raw;
-//        __device__ Raw load(int64_t v, bool owned) const;
-//        __device__ void make(const Raw&, int64_t v, int i, int j, int k, bool owned, T (&x)[3]) const;
-//        the input vector at node v = (i, j, k), once per CTA, node and plane
-//        (`owned`: this CTA owns v, for side outputs);
+//        __device__ Raw load(int v, bool owned) const;
+//        __device__ void make(const Raw&, int v, bool owned, T (&x)[3]) const;
+//        the input vector at node v, once per CTA, node and plane (`owned`:
+//        this CTA owns v, for side outputs);
 //   Out: struct Pre;
-//        __device__ Pre load(int64_t v) const;
-//        __device__ double store(const Pre&, int64_t v, int i, int j, int k, const T (&y)[3]) const;
+//        __device__ Pre load(int v) const;
+//        __device__ double store(const Pre&, int v, const T (&y)[3]) const;
 //        consumes (K x)_v at an owned node and returns its part of the
 //        reduction; static constexpr bool kReduce; __device__ void finish(double) const.
-// Node plane p is formed three hex layers ahead into buffer (p - k0 + 1) % 3.
+// Node indices are 32-bit (3 N < 2^31).  Node plane p is formed three hex
+// layers ahead into buffer (p - k0 + 1) % 4.
 // Grid: (ceil(px / 31), ceil(py / 7), ceil(pz / kz)) CTAs of 256 threads.
 template <typename T, int WM, bool CUBE, class In, class Out>
 __global__ void __launch_bounds__(kBoxThreads) k_box(BoxDims d, BoxGeo<T> g, BoxW<T, WM> bw, int kz, In in,
                                                      Out out, BoxRed red) {
-  __shared__ T xs[3][kBoxPlane][3];
-  __shared__ T yb[2][8][32][3];
+  __shared__ BoxV4<T> xs[4][kBoxPlane];
+  __shared__ BoxV4<T> yb[2][8][32];
   __shared__ double s_red[32];
   const int L = threadIdx.x & 31, wp = threadIdx.x >> 5;
   const int i0 = blockIdx.x * kBoxX, j0 = blockIdx.y * kBoxY, k0 = blockIdx.z * kz;
@@ -173,50 +226,36 @@ __global__ void __launch_bounds__(kBoxThreads) k_box(BoxDims d, BoxGeo<T> g, Box
   const int i = i0 - 1 + L, j = j0 - 1 + wp;
   const bool hex_ij = i >= 0 && i < d.nx && j >= 0 && j < d.ny;
   const bool own_ij = L >= 1 && wp >= 1 && i < d.px && j < d.py;
+  const int plane = d.px * d.py;
 
   // the (at most two) plane entries this thread forms: e = tid, tid + 256
   constexpr int kSlots = (kBoxPlane + kBoxThreads - 1) / kBoxThreads;
-  int fi[kSlots], fj[kSlots];
+  int fv[kSlots];
   bool fin[kSlots], fown[kSlots];
 #pragma unroll
   for (int q = 0; q < kSlots; ++q) {
     const int e = threadIdx.x + q * kBoxThreads;
     const int r = e / kBoxCols, c = e - r * kBoxCols;
-    fi[q] = i0 - 1 + c;
-    fj[q] = j0 - 1 + r;
-    fin[q] = e < kBoxPlane && fi[q] >= 0 && fi[q] < d.px && fj[q] >= 0 && fj[q] < d.py;
+    const int fi = i0 - 1 + c, fj = j0 - 1 + r;
+    fin[q] = e < kBoxPlane && fi >= 0 && fi < d.px && fj >= 0 && fj < d.py;
     fown[q] = e < kBoxPlane && c >= 1 && c <= kBoxX && r >= 1 && r <= kBoxY;
+    fv[q] = fin[q] ? fi + d.px * fj : 0;  // node of the entry in plane 0
   }
-  auto node_of = [&](int ni, int nj, int nk) { return int64_t(ni) + int64_t(d.px) * (nj + int64_t(d.py) * nk); };
   typename In::Raw raw[kSlots];
-  // issue the loads of node plane p
   auto form_load = [&](int p) {
 #pragma unroll
     for (int q = 0; q < kSlots; ++q)
-      if (fin[q] && p >= 0 && p < d.pz) raw[q] = in.load(node_of(fi[q], fj[q], p), fown[q] && p >= k0 && p < k1);
+      if (fin[q] && p >= 0 && p < d.pz) raw[q] = in.load(fv[q] + p * plane, fown[q] && p >= k0 && p < k1);
   };
-  // finish node plane p into buffer b
   auto form_store = [&](int p, int b) {
 #pragma unroll
     for (int q = 0; q < kSlots; ++q) {
       const int e = threadIdx.x + q * kBoxThreads;
       if (e >= kBoxPlane) continue;
       T v[3] = {T(0), T(0), T(0)};
-      if (fin[q] && p >= 0 && p < d.pz) {
-        const int64_t nv = node_of(fi[q], fj[q], p);
-        in.make(raw[q], nv, fi[q], fj[q], p, fown[q] && p >= k0 && p < k1, v);
-      }
-      xs[b][e][0] = v[0];
-      xs[b][e][1] = v[1];
-      xs[b][e][2] = v[2];
+      if (fin[q] && p >= 0 && p < d.pz) in.make(raw[q], fv[q] + p * plane, fown[q] && p >= k0 && p < k1, v);
+      xs[b][e] = BoxV4<T>(v[0], v[1], v[2]);
     }
-  };
-  // corner (a, b) of this thread's hex from plane buffer pb
-  auto corner = [&](int pb, int a, int b, T (&v)[3]) {
-    const int e = (wp + b) * kBoxCols + L + a;
-    v[0] = xs[pb][e][0];
-    v[1] = xs[pb][e][1];
-    v[2] = xs[pb][e][2];
   };
 
   for (int p = 0; p < 3; ++p) {
@@ -224,56 +263,63 @@ __global__ void __launch_bounds__(kBoxThreads) k_box(BoxDims d, BoxGeo<T> g, Box
     form_store(k0 - 1 + p, p);
   }
   __syncthreads();
-  T xb[4][3];  // bottom corners (a + 2b) of the current hex layer
+
+  // hex weights, loaded one layer ahead; hex (i, j, k) = h0 + k * layer
+  const int layer = d.nx * d.ny, h0 = hex_ij ? i + d.nx * j : 0;
+  T wn[WM ? 6 : 1];
+  auto load_w = [&](int k) {
+    if (hex_ij && k >= 0 && k < d.nz) {
+      if constexpr (WM) {
 #pragma unroll
-  for (int q = 0; q < 4; ++q) corner(0, q & 1, q >> 1, xb[q]);
-  __syncthreads();  // the first layer refills buffer 0
+        for (int t = 0; t < 6; ++t) wn[t] = bw.w[int64_t(t) * bw.H + h0 + k * layer];
+      } else {
+        wn[0] = bw.w[h0 + k * layer];
+      }
+    }
+  };
+  load_w(k0 - 1);
+  const int v0 = i + d.px * j;
   T carry[4][3];
 #pragma unroll
   for (int q = 0; q < 4; ++q) carry[q][0] = carry[q][1] = carry[q][2] = T(0);
   double acc = 0.0;
-  int bt = 1, bf = 0;  // buffer of the top plane (k + 1), buffer to form (k + 3)
-  // hex weights, loaded one layer ahead; hex (i, j, k) = h0 + k * layer
-  const int64_t layer = int64_t(d.nx) * d.ny, h0 = hex_ij ? int64_t(i) + int64_t(d.nx) * j : 0;
-  auto load_w = [&](int k, T (&w)[WM ? 6 : 1]) {
-    if (hex_ij && k >= 0 && k < d.nz) {
-      const int64_t h = h0 + k * layer;
-      if constexpr (WM) {
-#pragma unroll
-        for (int t = 0; t < 6; ++t) w[t] = bw.w[t * bw.H + h];
-      } else {
-        w[0] = bw.w[h];
-      }
-    }
-  };
-  T wn[WM ? 6 : 1];
-  load_w(k0 - 1, wn);
-  const int64_t plane = int64_t(d.px) * d.py, v0 = int64_t(i) + int64_t(d.px) * j;
+  int bb = 0;  // buffer of the bottom plane k; top k + 1 in bb + 1, plane k + 3 formed into bb + 3 (mod 4)
+#pragma unroll 2
   for (int k = k0 - 1; k < k1; ++k) {
     const bool fwd = k + 3 <= k1;  // plane k + 3 is read by a later layer
     if (fwd) form_load(k + 3);
     const bool own = own_ij && k >= k0;
-    const int64_t v = v0 + k * plane;
+    const int v = v0 + k * plane;
     typename Out::Pre pre;
     if (own) pre = out.load(v);
-    T w[WM ? 6 : 1];
+    T lw[6], mw[6];
+    {
+      T w[WM ? 6 : 1];
 #pragma unroll
-    for (int t = 0; t < (WM ? 6 : 1); ++t) w[t] = wn[t];
-    load_w(k + 1, wn);
-    T u[8][3];
+      for (int t = 0; t < (WM ? 6 : 1); ++t) w[t] = wn[t];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      u[q][0] = xb[q][0];
-      u[q][1] = xb[q][1];
-      u[q][2] = xb[q][2];
-      corner(bt, q & 1, q >> 1, xb[q]);  // top plane, next layer's bottom
-      u[q + 4][0] = xb[q][0];
-      u[q + 4][1] = xb[q][1];
-      u[q + 4][2] = xb[q][2];
+      for (int t = 0; t < 6; ++t) {
+        lw[t] = w[WM ? t : 0] * g.lam;
+        mw[t] = w[WM ? t : 0] * g.mu;
+      }
     }
+    load_w(k + 1);
     T f[8][3];
     if (hex_ij && k >= 0 && k < d.nz) {
-      box_hex<CUBE, WM>(u, w, g, f);
+      T u[8][3];
+      const int bt = (bb + 1) & 3;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int e = (wp + (q >> 1)) * kBoxCols + L + (q & 1);
+        const BoxV4<T> lo = xs[bb][e], hi = xs[bt][e];
+        u[q][0] = lo.x;
+        u[q][1] = lo.y;
+        u[q][2] = lo.z;
+        u[q + 4][0] = hi.x;
+        u[q + 4][1] = hi.y;
+        u[q + 4][2] = hi.z;
+      }
+      box_hex<CUBE>(u, lw, mw, g.ih, f);
     } else {
 #pragma unroll
       for (int c = 0; c < 8; ++c) f[c][0] = f[c][1] = f[c][2] = T(0);
@@ -295,19 +341,16 @@ __global__ void __launch_bounds__(kBoxThreads) k_box(BoxDims d, BoxGeo<T> g, Box
       G1[c] = P[2][c] + __shfl_up_sync(0xffffffffu, P[3][c], 1);
     }
     const int yi = (k - k0 + 1) & 1;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) yb[yi][wp][L][c] = G1[c];
-    if (fwd) form_store(k + 3, bf);
+    yb[yi][wp][L] = BoxV4<T>(G1[0], G1[1], G1[2]);
+    if (fwd) form_store(k + 3, (bb + 3) & 3);
     __syncthreads();
     // along y: node j gets corner b = 0 of row j and corner b = 1 of row j - 1
     if (own) {
-      T y[3];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) y[c] = G0[c] + yb[yi][wp - 1][L][c];
-      acc += out.store(pre, v, i, j, k, y);
+      const BoxV4<T> o = yb[yi][wp - 1][L];
+      const T y[3] = {G0[0] + o.x, G0[1] + o.y, G0[2] + o.z};
+      acc += out.store(pre, v, y);
     }
-    bt = bt == 2 ? 0 : bt + 1;
-    bf = bf == 2 ? 0 : bf + 1;
+    bb = (bb + 1) & 3;
   }
   if constexpr (Out::kReduce) {
     const double b = block_sum_box(acc, s_red);

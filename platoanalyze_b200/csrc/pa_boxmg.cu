@@ -6,8 +6,13 @@
 // geometric hierarchy): levels of half the hexes per axis with the mean SIMP
 // weight of their children, Dirichlet dofs by injection, trilinear transfers,
 // Chebyshev(2) smoothing in D^-1 K on [lmax/10, 1.15 lmax] before and after
-// the coarse correction, a dense FP64 inverse on the coarsest level and an
-// FP64 outer CG.  What changes is the data path:
+// the coarse correction, a dense FP64 inverse on the coarsest level, and an
+// FP64 outer CG whose convergence is confirmed on the true residual b - K x
+// (it restarts from it otherwise).  An outer CG with the FP32 operator and
+// FP64 vectors was measured on the 160x80x80 cantilever: its recursion ran
+// ahead of the true residual, one restart was needed and it took 25
+// iterations (12.0 ms) against 19 (10.2 ms) for the FP64 operator, so the
+// outer operator stays FP64.  What changes against pa_mg.cu is the data path:
 //  * every operator application is the box kernel, with the vector updates
 //    of the Chebyshev steps, residuals and CG dot products fused into its
 //    epilogue; one V-cycle on a level is four kernels plus the restriction:
@@ -26,8 +31,9 @@
 //    the lattice (no cell permutation, no atomics), and a fine level whose six
 //    tets of every hex share one weight (per-hex densities) reads one weight
 //    per hex.
-// Requirements: a box from mesh_make_box (even hex counts), an elastic
-// operator (J2 tangent solves keep pa_mg.cu), one part.
+// Requirements: a box lattice (mesh_make_box, or arrays recognised by
+// detect_lattice: the solver permutes b and x at its boundary) with even hex
+// counts, an elastic operator (J2 tangent solves keep pa_mg.cu), one part.
 #include <cmath>
 #include <memory>
 #include <vector>
@@ -79,14 +85,14 @@ struct InVec {  // x, with the masked dofs zero (mask may be null)
     S x[3];
     uint8_t mk;
   };
-  __device__ Raw load(int64_t v, bool) const {
+  __device__ Raw load(int v, bool) const {
     Raw r;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) r.x[c] = x[c * N + v];
+    for (int c = 0; c < 3; ++c) r.x[c] = x[c * int(N) + v];
     r.mk = mask ? mask[v] : 0;
     return r;
   }
-  __device__ void make(const Raw& r, int64_t, int, int, int, bool, T (&o)[3]) const {
+  __device__ void make(const Raw& r, int, bool, T (&o)[3]) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) o[c] = ((r.mk >> c) & 1) ? T(0) : T(r.x[c]);
   }
@@ -101,10 +107,10 @@ struct OutPlain {  // y = K x, masked dofs zero (mask may be null)
   struct Pre {
     uint8_t mk;
   };
-  __device__ Pre load(int64_t v) const { return Pre{mask ? mask[v] : uint8_t(0)}; }
-  __device__ double store(const Pre& p, int64_t v, int, int, int, const T (&k)[3]) const {
+  __device__ Pre load(int v) const { return Pre{mask ? mask[v] : uint8_t(0)}; }
+  __device__ double store(const Pre& p, int v, const T (&k)[3]) const {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) y[c * N + v] = ((p.mk >> c) & 1) ? T(0) : k[c];
+    for (int c = 0; c < 3; ++c) y[c * int(N) + v] = ((p.mk >> c) & 1) ? T(0) : k[c];
     return 0.0;
   }
   __device__ void finish(double) const {}
@@ -120,16 +126,16 @@ struct InDinvB {  // d0 = dinv b / theta
     float d[3];
     B b[3];
   };
-  __device__ Raw load(int64_t v, bool) const {
+  __device__ Raw load(int v, bool) const {
     Raw r;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      r.d[c] = dinv[c * N + v];
-      r.b[c] = b[c * N + v];
+      r.d[c] = dinv[c * int(N) + v];
+      r.b[c] = b[c * int(N) + v];
     }
     return r;
   }
-  __device__ void make(const Raw& r, int64_t, int, int, int, bool, float (&o)[3]) const {
+  __device__ void make(const Raw& r, int, bool, float (&o)[3]) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) o[c] = s * r.d[c] * float(r.b[c]);
   }
@@ -147,18 +153,18 @@ struct OutPre {  // x = dinv (ca b - c2 K d0)
     float d[3];
     B b[3];
   };
-  __device__ Pre load(int64_t v) const {
+  __device__ Pre load(int v) const {
     Pre p;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      p.d[c] = dinv[c * N + v];
-      p.b[c] = b[c * N + v];
+      p.d[c] = dinv[c * int(N) + v];
+      p.b[c] = b[c * int(N) + v];
     }
     return p;
   }
-  __device__ double store(const Pre& p, int64_t v, int, int, int, const float (&k)[3]) const {
+  __device__ double store(const Pre& p, int v, const float (&k)[3]) const {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) x[c * N + v] = p.d[c] * (ca * float(p.b[c]) - c2 * k[c]);
+    for (int c = 0; c < 3; ++c) x[c * int(N) + v] = p.d[c] * (ca * float(p.b[c]) - c2 * k[c]);
     return 0.0;
   }
   __device__ void finish(double) const {}
@@ -175,69 +181,19 @@ struct OutRes {  // r = b - K x, masked dofs zero
     B b[3];
     uint8_t mk;
   };
-  __device__ Pre load(int64_t v) const {
+  __device__ Pre load(int v) const {
     Pre p;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) p.b[c] = b[c * N + v];
+    for (int c = 0; c < 3; ++c) p.b[c] = b[c * int(N) + v];
     p.mk = mask[v];
     return p;
   }
-  __device__ double store(const Pre& p, int64_t v, int, int, int, const float (&k)[3]) const {
+  __device__ double store(const Pre& p, int v, const float (&k)[3]) const {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) r[c * N + v] = ((p.mk >> c) & 1) ? 0.f : float(p.b[c]) - k[c];
+    for (int c = 0; c < 3; ++c) r[c * int(N) + v] = ((p.mk >> c) & 1) ? 0.f : float(p.b[c]) - k[c];
     return 0.0;
   }
   __device__ void finish(double) const {}
-};
-
-// Trilinear interpolation from the coarse lattice (cpx x cpy x ...) at fine
-// node (i, j, k); the coarse vector is small and read from L2.
-struct Prolong {
-  const float* e;
-  int cpx, cpy;
-  int64_t Nc;
-  __device__ __forceinline__ void add(int i, int j, int k, float (&o)[3]) const {
-    const int ia = i >> 1, ja = j >> 1, ka = k >> 1;
-    const int ni = (i & 1) + 1, nj = (j & 1) + 1, nk = (k & 1) + 1;
-    const float wi = ni == 1 ? 1.f : 0.5f, wj = nj == 1 ? 1.f : 0.5f, wk = nk == 1 ? 1.f : 0.5f;
-    const float w = wi * wj * wk;
-    float s[3] = {0.f, 0.f, 0.f};
-    for (int c = 0; c < nk; ++c)
-      for (int b = 0; b < nj; ++b)
-        for (int a = 0; a < ni; ++a) {
-          const int64_t cv = (ia + a) + int64_t(cpx) * ((ja + b) + int64_t(cpy) * (ka + c));
-#pragma unroll
-          for (int d = 0; d < 3; ++d) s[d] += e[d * Nc + cv];
-        }
-#pragma unroll
-    for (int d = 0; d < 3; ++d) o[d] += w * s[d];
-  }
-};
-
-struct InProlong {  // xi = x + P e, masked dofs zero
-  const float* x;
-  Prolong P;
-  const uint8_t* mask;
-  int64_t N;
-  struct Raw {
-    float x[3];
-    uint8_t mk;
-  };
-  __device__ Raw load(int64_t v, bool) const {
-    Raw r;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) r.x[c] = x[c * N + v];
-    r.mk = mask[v];
-    return r;
-  }
-  __device__ void make(const Raw& r, int64_t, int i, int j, int k, bool, float (&o)[3]) const {
-#pragma unroll
-    for (int c = 0; c < 3; ++c) o[c] = r.x[c];
-    P.add(i, j, k, o);
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-      if ((r.mk >> c) & 1) o[c] = 0.f;
-  }
 };
 
 template <typename B>
@@ -251,18 +207,18 @@ struct OutPost1 {  // r0 = dinv (b - K xi)
     float d[3];
     B b[3];
   };
-  __device__ Pre load(int64_t v) const {
+  __device__ Pre load(int v) const {
     Pre p;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      p.d[c] = dinv[c * N + v];
-      p.b[c] = b[c * N + v];
+      p.d[c] = dinv[c * int(N) + v];
+      p.b[c] = b[c * int(N) + v];
     }
     return p;
   }
-  __device__ double store(const Pre& p, int64_t v, int, int, int, const float (&k)[3]) const {
+  __device__ double store(const Pre& p, int v, const float (&k)[3]) const {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) r0[c * N + v] = p.d[c] * (float(p.b[c]) - k[c]);
+    for (int c = 0; c < 3; ++c) r0[c * int(N) + v] = p.d[c] * (float(p.b[c]) - k[c]);
     return 0.0;
   }
   __device__ void finish(double) const {}
@@ -275,27 +231,26 @@ struct InScaled {  // d0 = s r0
   struct Raw {
     float r[3];
   };
-  __device__ Raw load(int64_t v, bool) const {
+  __device__ Raw load(int v, bool) const {
     Raw q;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) q.r[c] = r[c * N + v];
+    for (int c = 0; c < 3; ++c) q.r[c] = r[c * int(N) + v];
     return q;
   }
-  __device__ void make(const Raw& q, int64_t, int, int, int, bool, float (&o)[3]) const {
+  __device__ void make(const Raw& q, int, bool, float (&o)[3]) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) o[c] = s * q.r[c];
   }
 };
 
-// x_out = xi + ca r0 - c2 dinv K d0, xi = x + P e (masked); on the finest level
+// x_out = xi + ca r0 - c2 dinv K d0 (xi = x + P e, prolongated in place
+// before post1; masked dofs are zero in xi, r0 and dinv); on the finest level
 // (RZ) the output is the FP64 preconditioned residual z and r . z is reduced
 // (finish: beta = r.z_new / r.z_old, or 0 on the first iteration).
 template <typename O, bool RZ>
 struct OutPost2 {
   O* xo;
   const float* x;
-  Prolong P;
-  const uint8_t* mask;
   const float* r0;
   const float* dinv;
   float ca, c2;
@@ -306,30 +261,25 @@ struct OutPost2 {
   struct Pre {
     float x[3], r0[3], d[3];
     double rv[RZ ? 3 : 1];
-    uint8_t mk;
   };
-  __device__ Pre load(int64_t v) const {
+  __device__ Pre load(int v) const {
     Pre p;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const int64_t q = c * N + v;
+      const int q = c * int(N) + v;
       p.x[c] = x[q];
       p.r0[c] = r0[q];
       p.d[c] = dinv[q];
       if constexpr (RZ) p.rv[c] = rvec[q];
     }
-    p.mk = mask[v];
     return p;
   }
-  __device__ double store(const Pre& p, int64_t v, int i, int j, int k, const float (&kd)[3]) const {
-    float xi[3] = {p.x[0], p.x[1], p.x[2]};
-    P.add(i, j, k, xi);
+  __device__ double store(const Pre& p, int v, const float (&kd)[3]) const {
     double acc = 0.0;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const float xin = ((p.mk >> c) & 1) ? 0.f : xi[c];
-      const float z = xin + ca * p.r0[c] - c2 * p.d[c] * kd[c];
-      xo[c * N + v] = O(z);
+      const float z = p.x[c] + ca * p.r0[c] - c2 * p.d[c] * kd[c];
+      xo[c * int(N) + v] = O(z);
       if constexpr (RZ) acc += double(z) * p.rv[c];
     }
     return acc;
@@ -356,20 +306,20 @@ struct OutPower {
   struct Pre {
     float d[3];
   };
-  __device__ Pre load(int64_t v) const {
+  __device__ Pre load(int v) const {
     Pre p;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) p.d[c] = dinv[c * N + v];
+    for (int c = 0; c < 3; ++c) p.d[c] = dinv[c * int(N) + v];
     return p;
   }
-  __device__ double store(const Pre& p, int64_t v, int, int, int, const float (&k)[3]) const {
+  __device__ double store(const Pre& p, int v, const float (&k)[3]) const {
     const double q = *nrm_in;
     const float sc = (q > 0.0 && isfinite(q)) ? float(1.0 / sqrt(q)) : 1.f;
     double acc = 0.0;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const float val = p.d[c] * k[c] * sc;
-      xn[c * N + v] = val;
+      xn[c * int(N) + v] = val;
       acc += double(val) * val;
     }
     return acc;
@@ -388,21 +338,21 @@ struct InCgP {
   struct Raw {
     double z[3], p[3];
   };
-  __device__ Raw load(int64_t v, bool) const {
+  __device__ Raw load(int v, bool) const {
     Raw r;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      r.z[c] = z[c * N + v];
-      r.p[c] = pold[c * N + v];
+      r.z[c] = z[c * int(N) + v];
+      r.p[c] = pold[c * int(N) + v];
     }
     return r;
   }
-  __device__ void make(const Raw& r, int64_t v, int, int, int, bool owned, double (&o)[3]) const {
+  __device__ void make(const Raw& r, int v, bool owned, double (&o)[3]) const {
     const double beta = sc[kBeta];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       o[c] = r.z[c] + beta * r.p[c];
-      if (owned) pnew[c * N + v] = o[c];
+      if (owned) pnew[c * int(N) + v] = o[c];
     }
   }
 };
@@ -418,23 +368,23 @@ struct OutCgQ {
     double z[3], p[3];
     uint8_t mk;
   };
-  __device__ Pre load(int64_t v) const {
+  __device__ Pre load(int v) const {
     Pre r;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      r.z[c] = z[c * N + v];
-      r.p[c] = pold[c * N + v];
+      r.z[c] = z[c * int(N) + v];
+      r.p[c] = pold[c * int(N) + v];
     }
     r.mk = mask[v];
     return r;
   }
-  __device__ double store(const Pre& r, int64_t v, int, int, int, const double (&k)[3]) const {
+  __device__ double store(const Pre& r, int v, const double (&k)[3]) const {
     const double beta = sc[kBeta];
     double acc = 0.0;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const double qv = ((r.mk >> c) & 1) ? 0.0 : k[c];
-      q[c * N + v] = qv;
+      q[c * int(N) + v] = qv;
       acc += (r.z[c] + beta * r.p[c]) * qv;
     }
     return acc;
@@ -512,13 +462,15 @@ __global__ void k_bcg_reset(double* sc) {
   sc[kFirst] = 1.0;
 }
 
-// x_soa[d N + v] = scale * value for each Dirichlet dof (dof = 3 v + d)
+// x_soa[d N + lattice(v)] = scale * value for each Dirichlet dof (dof = 3 v + d)
 __global__ void k_bscatter_bc(int64_t nbc, const int32_t* __restrict__ dofs, const double* __restrict__ vals,
-                              double scale, int64_t N, double* __restrict__ x) {
+                              double scale, int64_t N, const int32_t* __restrict__ lat_of, int flip,
+                              double* __restrict__ x) {
   const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i >= nbc) return;
   const int32_t dof = dofs[i];
-  x[(dof % 3) * N + dof / 3] = scale * vals[i];
+  const int32_t v = dof / 3, d = dof % 3;
+  x[d * N + (lat_of ? lat_of[v] : v)] = (((flip >> d) & 1) ? -scale : scale) * vals[i];
 }
 __global__ void k_bset_bc(int64_t nbc, const int32_t* __restrict__ dofs, const double* __restrict__ vals, double scale,
                           double* __restrict__ x_aos) {
@@ -559,6 +511,32 @@ __global__ void k_brestrict(int cnx, int cny, int cnz, const float* __restrict__
   for (int d = 0; d < 3; ++d) c[d * Nc + v] = ((mk >> d) & 1) ? 0.f : s[d];
 }
 
+// x_fine += P e (trilinear interpolation of the coarse correction), fine
+// masked dofs untouched (they stay zero).
+__global__ void k_bprolong_add(int cnx, int cny, const float* __restrict__ e, int64_t Nc,
+                               const uint8_t* __restrict__ fmask, float* __restrict__ x, int64_t Nf) {
+  const int64_t v = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (v >= Nf) return;
+  const int fpx = 2 * cnx + 1, fpy = 2 * cny + 1;
+  const int i = int(v % fpx), j = int((v / fpx) % fpy), k = int(v / (int64_t(fpx) * fpy));
+  const int cpx = cnx + 1, cpy = cny + 1;
+  const int ia = i >> 1, ja = j >> 1, ka = k >> 1;
+  const int ni = (i & 1) + 1, nj = (j & 1) + 1, nk = (k & 1) + 1;
+  const float w = (ni == 1 ? 1.f : 0.5f) * (nj == 1 ? 1.f : 0.5f) * (nk == 1 ? 1.f : 0.5f);
+  float s[3] = {0.f, 0.f, 0.f};
+  for (int c = 0; c < nk; ++c)
+    for (int b = 0; b < nj; ++b)
+      for (int a = 0; a < ni; ++a) {
+        const int64_t cv = (ia + a) + int64_t(cpx) * ((ja + b) + int64_t(cpy) * (ka + c));
+#pragma unroll
+        for (int d = 0; d < 3; ++d) s[d] += e[d * Nc + cv];
+      }
+  const uint8_t mk = fmask[v];
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+    if (!((mk >> d) & 1)) x[d * Nf + v] += w * s[d];
+}
+
 // deterministic zero-mean start vector in [-1, 1], masked; ||x||^2 reduced
 __global__ void __launch_bounds__(kVT) k_bseed(int64_t N, const uint8_t* __restrict__ mask, float* __restrict__ x,
                                                double* partials, unsigned int* counter, double* nrm_out) {
@@ -576,6 +554,34 @@ __global__ void __launch_bounds__(kVT) k_bseed(int64_t N, const uint8_t* __restr
   grid_reduce_finish(s, partials, counter, nrm_out);
 }
 
+// interleaved caller's order -> component-major lattice order (node_of null:
+// same order; flip bit d: component d changes sign)
+template <typename S, typename T>
+__global__ void k_bperm_in(int64_t N, const int32_t* __restrict__ node_of, int flip, const S* __restrict__ aos,
+                           T* __restrict__ soa) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < 3 * N; i += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t b = i % N, d = i / N;
+    const T v = T(aos[3 * int64_t(node_of ? node_of[b] : b) + d]);
+    soa[i] = ((flip >> d) & 1) ? -v : v;
+  }
+}
+// component-major lattice order -> interleaved caller's order
+template <typename T, typename S>
+__global__ void k_bperm_out(int64_t N, const int32_t* __restrict__ node_of, int flip, const T* __restrict__ soa,
+                            S* __restrict__ aos) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < 3 * N; i += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t b = i % N, d = i / N;
+    const S v = S(soa[i]);
+    aos[3 * int64_t(node_of ? node_of[b] : b) + d] = ((flip >> d) & 1) ? -v : v;
+  }
+}
+// node mask in lattice order
+__global__ void k_bperm_mask(int64_t N, const int32_t* __restrict__ node_of, const uint8_t* __restrict__ in,
+                             uint8_t* __restrict__ out) {
+  const int64_t b = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (b < N) out[b] = in[node_of[b]];
+}
+
 // ||x||^2
 __global__ void __launch_bounds__(kVT) k_bnorm2(int64_t n, const float* __restrict__ x, double* partials,
                                                 unsigned int* counter, double* nrm_out) {
@@ -590,6 +596,7 @@ __global__ void __launch_bounds__(kVT) k_bnorm2(int64_t n, const float* __restri
 // cell 6h + t; nodal: the mean of the tet's four nodes, src/ApplyWeighting.hpp:49-62),
 // tet-major; the per-hex copy and a flag when the six tets of a hex differ.
 __global__ void k_bweights(BoxDims d, const double* __restrict__ z, int layout, double p, double pmin,
+                           const int32_t* __restrict__ cell_of_slot, const int32_t* __restrict__ node_of,
                            double* __restrict__ w64t, float* __restrict__ w32t, double* __restrict__ w64h,
                            float* __restrict__ w32h, unsigned int* __restrict__ differ) {
   const int64_t h = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
@@ -600,12 +607,13 @@ __global__ void k_bweights(BoxDims d, const double* __restrict__ z, int layout, 
   for (int t = 0; t < 6; ++t) {
     double rho;
     if (layout == PA_CONTROL_CELL) {
-      rho = z[6 * h + t];
+      rho = z[cell_of_slot ? cell_of_slot[6 * h + t] : 6 * h + t];
     } else {
       rho = 0.0;
       for (int m = 0; m < 4; ++m) {
         const int c = path_vertex(t, m);
-        rho += z[(i + (c & 1)) + int64_t(d.px) * ((j + ((c >> 1) & 1)) + int64_t(d.py) * (k + (c >> 2)))];
+        const int64_t b = (i + (c & 1)) + int64_t(d.px) * ((j + ((c >> 1) & 1)) + int64_t(d.py) * (k + (c >> 2)));
+        rho += z[node_of ? node_of[b] : b];
       }
       rho *= 0.25;
     }
@@ -748,6 +756,7 @@ struct BoxHierarchy {
   DevBuf<double> partials, sc, norms;
   DevBuf<unsigned int> counter;
   DevBuf<double> p0, p1, q;  // outer CG directions (ping-pong) and K p
+  DevBuf<uint8_t> mask0;     // the finest level's Dirichlet mask in lattice order (permuted meshes)
 };
 
 void boxmg_release(Problem& P) {
@@ -860,8 +869,8 @@ void coarse_mask(const BoxLevel& f, BoxLevel& c, const std::vector<uint8_t>& fma
 // 2048 dofs for the dense inverse.
 bool boxmg_eligible(const Problem& P) {
   const Mesh& m = *P.mesh;
-  if (!box_apply_eligible(P) || m.box_n[0] % 2 || m.box_n[1] % 2 || m.box_n[2] % 2) return false;
-  int n[3] = {m.box_n[0], m.box_n[1], m.box_n[2]};
+  if (!box_apply_eligible(P) || m.lat_n[0] % 2 || m.lat_n[1] % 2 || m.lat_n[2] % 2) return false;
+  int n[3] = {m.lat_n[0], m.lat_n[1], m.lat_n[2]};
   while (!(n[0] % 2 || n[1] % 2 || n[2] % 2 || std::min(std::min(n[0], n[1]), n[2]) < 4))
     for (int a = 0; a < 3; ++a) n[a] /= 2;
   return 3LL * (n[0] + 1) * (n[1] + 1) * (n[2] + 1) <= 2048;
@@ -870,7 +879,7 @@ bool boxmg_eligible(const Problem& P) {
 // True when the box kernel can apply this problem's operator (pa_apply).
 bool box_apply_eligible(const Problem& P) {
   const Mesh& m = *P.mesh;
-  return m.box_kernels && m.box_n[0] > 0 && m.num_parts == 1;
+  return m.box_kernels && m.lat_n[0] > 0 && m.num_parts == 1 && 3 * m.N < (int64_t(1) << 31);
 }
 
 namespace {
@@ -886,14 +895,14 @@ void boxmg_setup_levels(Problem& P) {
   cudaStream_t s = P.stream;
   boxmg_release(P);
   std::unique_ptr<BoxHierarchy> H(new BoxHierarchy());
-  int n[3] = {m.box_n[0], m.box_n[1], m.box_n[2]};
+  int n[3] = {m.lat_n[0], m.lat_n[1], m.lat_n[2]};
   for (int a = 0; a < 3; ++a) {
     H->fine_n[a] = n[a];
-    H->fine_l[a] = m.box_l[a];
+    H->fine_l[a] = m.lat_l[a];
   }
   for (int l = 0;; ++l) {
     std::unique_ptr<BoxLevel> L(new BoxLevel());
-    set_dims(*L, n[0], n[1], n[2], m.box_l[0], m.box_l[1], m.box_l[2]);
+    set_dims(*L, n[0], n[1], n[2], m.lat_l[0], m.lat_l[1], m.lat_l[2]);
     const int64_t n3 = 3 * L->d.N;
     L->dinv.resize(n3);
     L->x.resize(n3);
@@ -927,12 +936,25 @@ void boxmg_setup_levels(Problem& P) {
   P.boxmg = H.release();
 }
 
+// The problem's Dirichlet mask in lattice order (a gather on permuted meshes).
+const uint8_t* lattice_mask(Problem& P) {
+  const Mesh& m = *P.mesh;
+  if (!m.lat_permuted) return P.d_node_mask.get();
+  BoxHierarchy& H = *P.boxmg;
+  H.mask0.resize(m.N);
+  k_bperm_mask<<<int((m.N + kVT - 1) / kVT), kVT, 0, P.stream>>>(m.N, m.d_lat_node.get(), P.d_node_mask.get(),
+                                                               H.mask0.get());
+  PA_LAUNCHED();
+  g_box_launches += 1;
+  return H.mask0.get();
+}
+
 // True when the hierarchy must be (re)built for the problem's box.
 bool boxmg_stale(const Problem& P) {
   const Mesh& m = *P.mesh;
   if (P.boxmg == nullptr) return true;
   for (int a = 0; a < 3; ++a)
-    if (P.boxmg->fine_n[a] != m.box_n[a] || P.boxmg->fine_l[a] != m.box_l[a]) return true;
+    if (P.boxmg->fine_n[a] != m.lat_n[a] || P.boxmg->fine_l[a] != m.lat_l[a]) return true;
   return false;
 }
 
@@ -942,15 +964,21 @@ bool boxmg_setup(Problem& P, const double* z) {
   PA_CHECK(P.boxmg->L.size() >= 2, "PA_SOLVER_PCG_MG needs at least one coarse level");
   BoxHierarchy& H = *P.boxmg;
   BoxLevel& F = *H.L[0];
-  F.mask = P.d_node_mask.get();
-  // fine weights in box order
+  const Mesh& m = *P.mesh;
+  F.mask = lattice_mask(P);
+  // fine weights in lattice order
   PA_CUDA(cudaMemsetAsync(H.differ.get(), 0, sizeof(unsigned int), s));
-  k_bweights<<<int((F.d.H + kVT - 1) / kVT), kVT, 0, s>>>(F.d, z, P.ep.layout, P.ep.p, P.ep.pmin, H.w64t.get(),
-                                                          H.w32t.get(), H.w64h.get(), H.w32h.get(), H.differ.get());
+  k_bweights<<<int((F.d.H + kVT - 1) / kVT), kVT, 0, s>>>(
+      F.d, z, P.ep.layout, P.ep.p, P.ep.pmin, m.lat_permuted ? m.d_lat_cell.get() : nullptr,
+      m.lat_permuted ? m.d_lat_node.get() : nullptr, H.w64t.get(), H.w32t.get(), H.w64h.get(), H.w32h.get(),
+      H.differ.get());
   PA_LAUNCHED();
   // masks by injection (host, from the problem's Dirichlet dofs)
   std::vector<uint8_t> fmask(size_t(F.d.N), 0);
-  for (int32_t dof : P.bc_dofs) fmask[size_t(dof / 3)] |= uint8_t(1u << (dof % 3));
+  for (int32_t dof : P.bc_dofs) {
+    const int32_t v = dof / 3;
+    fmask[size_t(m.lat_permuted ? m.h_lat_of_node[size_t(v)] : v)] |= uint8_t(1u << (dof % 3));
+  }
   for (size_t l = 1; l < H.L.size(); ++l) {
     std::vector<uint8_t> cmask;
     coarse_mask(*H.L[l - 1], *H.L[l], fmask, cmask);
@@ -1136,12 +1164,13 @@ void vcycle_level(const Problem& P, BoxHierarchy& H, size_t l, const B* b, O* xo
   g_box_launches += 1;
   vcycle(P, H, l + 1, s);
   // post-smoothing from x + P e
-  const Prolong Pe{C.x.get(), C.d.px, C.d.py, C.d.N};
-  launch_box<float>(L, g, w, InProlong{L.x.get(), Pe, L.mask, N}, OutPost1<B>{L.r.get(), b, L.dinv.get(), N}, red,
-                    s);
-  launch_box<float>(L, g, w, InScaled{L.r.get(), ch.inv_theta, N},
-                    OutPost2<O, RZ>{xo, L.x.get(), Pe, L.mask, L.r.get(), L.dinv.get(), ch.ca, ch.c2, N, rvec, sc},
+  k_bprolong_add<<<int((N + kVT - 1) / kVT), kVT, 0, s>>>(C.d.nx, C.d.ny, C.x.get(), C.d.N, L.mask, L.x.get(), N);
+  PA_LAUNCHED();
+  g_box_launches += 1;
+  launch_box<float>(L, g, w, InVec<float, float>{L.x.get(), nullptr, N}, OutPost1<B>{L.r.get(), b, L.dinv.get(), N},
                     red, s);
+  launch_box<float>(L, g, w, InScaled{L.r.get(), ch.inv_theta, N},
+                    OutPost2<O, RZ>{xo, L.x.get(), L.r.get(), L.dinv.get(), ch.ca, ch.c2, N, rvec, sc}, red, s);
 }
 
 // y = K x (FP64, box kernel) with optional masks on input and output
@@ -1181,10 +1210,15 @@ bool solve_boxmg(Problem& P, const double* z, const double* b, double* x_out, co
   double* zv = ws.p0.get();
   // b' = mask(b - K x_D), component-major, and ||b'||^2
   const int64_t nbc = int64_t(P.bc_dofs.size());
-  launch_aos_to_soa<double, double>(b, t, N, s);
+  const Mesh& m = *P.mesh;
+  const int32_t* node_of = m.lat_permuted ? m.d_lat_node.get() : nullptr;
+  k_bperm_in<double, double><<<vec_blocks(n), kVT, 0, s>>>(N, node_of, m.lat_flip, b, t);
+  PA_LAUNCHED();
   if (nbc) {
     PA_CUDA(cudaMemsetAsync(zv, 0, sizeof(double) * n, s));
-    k_bscatter_bc<<<int((nbc + 255) / 256), 256, 0, s>>>(nbc, P.d_bc_dofs.get(), P.d_bc_vals.get(), 1.0, N, zv);
+    k_bscatter_bc<<<int((nbc + 255) / 256), 256, 0, s>>>(nbc, P.d_bc_dofs.get(), P.d_bc_vals.get(), 1.0, N,
+                                                         m.lat_permuted ? m.d_lat_of_node.get() : nullptr,
+                                                         m.lat_flip, zv);
     PA_LAUNCHED();
     box_apply64(F, P.ep, w64, zv, H.q.get(), nullptr, red, s);
     k_bres64<<<vec_blocks(n), kVT, 0, s>>>(N, t, H.q.get(), mask, bp, H.partials.get(), H.counter.get(), sc + kRr);
@@ -1268,8 +1302,9 @@ bool solve_boxmg(Problem& P, const double* z, const double* b, double* x_out, co
       PA_LAUNCHED();
     }
   }
-  // x_out = x + x_D (interleaved)
-  launch_soa_to_aos<double, double>(x, x_out, N, s);
+  // x_out = x + x_D (interleaved, caller's order)
+  k_bperm_out<double, double><<<vec_blocks(n), kVT, 0, s>>>(N, node_of, m.lat_flip, x, x_out);
+  PA_LAUNCHED();
   if (nbc) {
     k_bset_bc<<<int((nbc + 255) / 256), 256, 0, s>>>(nbc, P.d_bc_dofs.get(), P.d_bc_vals.get(), 1.0, x_out);
     PA_LAUNCHED();
@@ -1290,33 +1325,43 @@ bool solve_boxmg(Problem& P, const double* z, const double* b, double* x_out, co
   return true;
 }
 
-// y = K(z) x on the box (component-major x, y; T = float or double), masked
-// when `constrained` (masked rows and columns zero), for pa_apply.
+// y = K(z) x on the box (interleaved x, y in the caller's node order; T =
+// float or double), masked when `constrained` (masked rows and columns zero;
+// the caller restores identity rows), for pa_apply.  xs, ys: 3N scratch.
 template <typename T>
-void box_apply(Problem& P, const double* z, const T* x, T* y, bool constrained) {
+void box_apply(Problem& P, const double* z, const T* x, T* y, bool constrained, T* xs, T* ys) {
   cudaStream_t s = P.stream;
   boxmg_ensure(P);
   BoxHierarchy& H = *P.boxmg;
   BoxLevel& F = *H.L[0];
+  const Mesh& m = *P.mesh;
   PA_CUDA(cudaMemsetAsync(H.differ.get(), 0, sizeof(unsigned int), s));
-  k_bweights<<<int((F.d.H + kVT - 1) / kVT), kVT, 0, s>>>(F.d, z, P.ep.layout, P.ep.p, P.ep.pmin, H.w64t.get(),
-                                                          H.w32t.get(), H.w64h.get(), H.w32h.get(), H.differ.get());
+  k_bweights<<<int((F.d.H + kVT - 1) / kVT), kVT, 0, s>>>(
+      F.d, z, P.ep.layout, P.ep.p, P.ep.pmin, m.lat_permuted ? m.d_lat_cell.get() : nullptr,
+      m.lat_permuted ? m.d_lat_node.get() : nullptr, H.w64t.get(), H.w32t.get(), H.w64h.get(), H.w32h.get(),
+      H.differ.get());
   PA_LAUNCHED();
   unsigned int differ = 0;
   PA_CUDA(cudaMemcpyAsync(&differ, H.differ.get(), sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
   PA_CUDA(cudaStreamSynchronize(s));
   F.wm = differ ? 1 : 0;
-  const uint8_t* mask = constrained ? P.d_node_mask.get() : nullptr;
+  const uint8_t* mask = constrained ? lattice_mask(P) : nullptr;
+  const int32_t* node_of = m.lat_permuted ? m.d_lat_node.get() : nullptr;
+  const int64_t n = 3 * F.d.N;
+  k_bperm_in<T, T><<<vec_blocks(n), kVT, 0, s>>>(F.d.N, node_of, m.lat_flip, x, xs);
+  PA_LAUNCHED();
   const BoxRed red{H.partials.get(), H.counter.get()};
   if constexpr (std::is_same<T, double>::value) {
-    box_apply64(F, P.ep, level_w64(H, 0), x, y, mask, red, s);
+    box_apply64(F, P.ep, level_w64(H, 0), xs, ys, mask, red, s);
   } else {
-    launch_box<float>(F, box_geo<float>(F, P.ep), level_w32(H, 0), InVec<float, float>{x, mask, F.d.N},
-                      OutPlain<float>{y, mask, F.d.N}, red, s);
+    launch_box<float>(F, box_geo<float>(F, P.ep), level_w32(H, 0), InVec<float, float>{xs, mask, F.d.N},
+                      OutPlain<float>{ys, mask, F.d.N}, red, s);
   }
+  k_bperm_out<T, T><<<vec_blocks(n), kVT, 0, s>>>(F.d.N, node_of, m.lat_flip, ys, y);
+  PA_LAUNCHED();
 }
-template void box_apply<double>(Problem&, const double*, const double*, double*, bool);
-template void box_apply<float>(Problem&, const double*, const float*, float*, bool);
+template void box_apply<double>(Problem&, const double*, const double*, double*, bool, double*, double*);
+template void box_apply<float>(Problem&, const double*, const float*, float*, bool, float*, float*);
 
 // Device time of the plain FP32 (or FP64) box apply over `reps` launches
 // (weights from z, random x), and its algorithmic bytes per launch: weights
@@ -1326,21 +1371,27 @@ double time_box_apply(Problem& P, const double* z, bool fp32, int reps, int64_t*
   const int64_t n = P.ndof();
   DevBuf<float> x32, y32;
   DevBuf<double> x64, y64;
+  DevBuf<float> s32a, s32b;
+  DevBuf<double> s64a, s64b;
   if (fp32) {
     x32.resize(n);
     y32.resize(n);
+    s32a.resize(n);
+    s32b.resize(n);
     PA_CUDA(cudaMemsetAsync(x32.get(), 0, sizeof(float) * n, s));
-    box_apply<float>(P, z, x32.get(), y32.get(), true);
+    box_apply<float>(P, z, x32.get(), y32.get(), true, s32a.get(), s32b.get());
   } else {
     x64.resize(n);
     y64.resize(n);
+    s64a.resize(n);
+    s64b.resize(n);
     PA_CUDA(cudaMemsetAsync(x64.get(), 0, sizeof(double) * n, s));
-    box_apply<double>(P, z, x64.get(), y64.get(), true);
+    box_apply<double>(P, z, x64.get(), y64.get(), true, s64a.get(), s64b.get());
   }
   BoxHierarchy& H = *P.boxmg;
   BoxLevel& F = *H.L[0];
   const BoxRed red{H.partials.get(), H.counter.get()};
-  const uint8_t* mask = P.d_node_mask.get();
+  const uint8_t* mask = lattice_mask(P);
   cudaEvent_t e0, e1;
   PA_CUDA(cudaEventCreate(&e0));
   PA_CUDA(cudaEventCreate(&e1));

@@ -131,6 +131,18 @@ struct Mesh {
   int box_n[3] = {0, 0, 0};
   double box_l[3] = {0.0, 0.0, 0.0};
   bool box_kernels = true;  // structured boxes: apply and multigrid on the box kernel (pa_box.cuh)
+  // Lattice of the box kernels: set for mesh_make_box boxes (identity
+  // numbering) and for meshes given as arrays that are such a box under some
+  // numbering (detect_lattice, pa_lattice.cu); lat_n[0] == 0 otherwise.
+  int lat_n[3] = {0, 0, 0};
+  double lat_l[3] = {0.0, 0.0, 0.0};
+  bool lat_permuted = false;           // the caller's numbering differs from the lattice order
+  int lat_flip = 0;                    // bit a: lattice axis a runs against the caller's axis a
+                                       // (vector components along it change sign)
+  DevBuf<int32_t> d_lat_node;          // lattice node -> caller's node (permuted only)
+  DevBuf<int32_t> d_lat_of_node;       // caller's node -> lattice node (permuted only)
+  DevBuf<int32_t> d_lat_cell;          // 6 h + t (hex h, box template tet t) -> caller's cell (permuted only)
+  std::vector<int32_t> h_lat_of_node;  // caller's node -> lattice node (permuted only)
   DevBuf<int32_t> d_tile_cluster_start, d_tile_cell_start, d_tile_hex_count, d_tile_node_start, d_cell_perm;
   DevBuf<int32_t> d_cell_iperm;  // user -> internal cell id
   DevBuf<uint32_t> d_tile_nodes;
@@ -154,6 +166,10 @@ struct Mesh {
 };
 
 void mesh_build(Mesh& m);  // tiles + graph + device upload
+// Recognise a mesh given as arrays as a box of equal axis-aligned hexes, each
+// split into the six tets of mesh_make_box (up to a reflection of the axes),
+// under any node, cell and vertex numbering; sets lat_* (pa_lattice.cu).
+void detect_lattice(Mesh& m);
 // Structured box [0,lx]x[0,ly]x[0,lz] of nx*ny*nz hexes x 6 tets (nodes and
 // hexes numbered x fastest), then mesh_build.
 void mesh_make_box(Mesh& m, int nx, int ny, int nz, double lx, double ly, double lz);

@@ -464,6 +464,12 @@ void mesh_make_box(Mesh& m, int nx, int ny, int nz, double lx, double ly, double
   m.box_l[0] = lx;
   m.box_l[1] = ly;
   m.box_l[2] = lz;
+  for (int a = 0; a < 3; ++a) {
+    m.lat_n[a] = m.box_n[a];
+    m.lat_l[a] = m.box_l[a];
+  }
+  m.lat_permuted = false;
+  m.lat_flip = 0;
   mesh_build(m);
 }
 
@@ -479,6 +485,7 @@ void mesh_build(Mesh& m) {
            "tile size (clusters per tile) must be 64, 128 or 256");
   build_graph(m);
   build_tiles(m);
+  if (m.box_n[0] == 0) detect_lattice(m);
   m.d_cells.upload(m.cells.data(), m.cells.size());
   m.d_coords.upload(m.coords.data(), m.coords.size());
   std::vector<double> soa(3 * m.N);

@@ -92,8 +92,9 @@ bool boxmg_eligible(const Problem& P);
 // false (nothing written) when the coarsest operator is singular
 bool solve_boxmg(Problem& P, const double* z, const double* b, double* x_out, const pa_solve_options& o,
                  pa_solve_stats* st, pa_status* status);
+// interleaved x, y in the caller's order; xs, ys: 3N scratch
 template <typename T>
-void box_apply(Problem& P, const double* z, const T* x, T* y, bool constrained);
+void box_apply(Problem& P, const double* z, const T* x, T* y, bool constrained, T* xs, T* ys);
 double time_box_apply(Problem& P, const double* z, bool fp32, int reps, int64_t* bytes);
 void boxmg_release(Problem& P);
 

@@ -149,3 +149,105 @@ def test_box_mg_density_change_reuses_hierarchy(pa):
         u64, _ = prob.solution(zz, options=pa.SolveOptions("fp64", rel_tol=1e-11))
         assert st["converged"], st
         assert rel_inf(u, u64) <= 1e-7
+
+
+def _scrambled(nx, ny, nz, seed, mirror_x=False):
+    """The box of pa_mesh_create_box as caller arrays: nodes and cells in
+    random order, each tet's vertices in random order, optionally mirrored in
+    x (the split then runs along another cube diagonal).  Returns the arrays,
+    the new node id of each box node, the box slot (6 h + t) of each cell, the
+    load faces and the clamped nodes."""
+    from platoanalyze_b200.fields import box_arrays
+    cells, coords, faces, clamp = box_arrays(nx, ny, nz)
+    rng = np.random.default_rng(seed)
+    N, C = coords.shape[0], cells.shape[0]
+    new_of_old = rng.permutation(N).astype(np.int32)
+    X = np.empty_like(coords)
+    X[new_of_old] = coords
+    if mirror_x:
+        X[:, 0] = nx - X[:, 0]
+    order = rng.permutation(C)
+    cl = new_of_old[cells][order]
+    cl = np.array([row[rng.permutation(4)] for row in cl], dtype=np.int32)
+    return cl, X, new_of_old, order, new_of_old[faces], new_of_old[clamp]
+
+
+def test_box_kernels_on_reference_numbered_meshes(pa, oracle_lib):
+    """The reference's own 2x2x2 Omega_h box (golden DerivativeTests mesh) and
+    a scrambled, x-mirrored 12x8x6 box enter through pa_mesh_create, are
+    recognised as lattices, and the box kernel's K x matches the oracle."""
+    from golden_util import derivative_case
+    d, cells, coords, u, z = derivative_case()
+    m = pa.Mesh.from_arrays(cells, coords)
+    assert m.box_kernels
+    prob = pa.Problem(m, 1.0, 0.3, 3.0, 1e-9, control_layout="nodal")
+    rng = np.random.default_rng(2)
+    zz = rng.uniform(0.2, 1.0, coords.shape[0])
+    O = oracle_lib.Oracle(cells, coords, E=1.0, nu=0.3, p=3.0, pmin=1e-9, layout=0)
+    assert rel_inf(prob.apply(zz, u), O.apply(u, zz)) <= 1e-12
+    cl, X, _, _, _, _ = _scrambled(12, 8, 6, 5, mirror_x=True)
+    m2 = pa.Mesh.from_arrays(cl, X)
+    assert m2.box_kernels
+    p2 = pa.Problem(m2, 2.0, 0.25, 3.0, 1e-6, control_layout="cell")
+    z2 = rng.uniform(0.05, 1.0, cl.shape[0])
+    x2 = rng.standard_normal(3 * X.shape[0])
+    O2 = oracle_lib.Oracle(cl, X, E=2.0, nu=0.25, p=3.0, pmin=1e-6, layout=1)
+    assert rel_inf(p2.apply(z2, x2), O2.apply(x2, z2)) <= 1e-12
+    assert rel_inf(p2.apply(z2, x2.astype(np.float32)), O2.apply(x2, z2)) <= 1e-5
+
+
+def test_box_mg_through_pa_mesh_create_at_64x32x32(pa, oracle_lib):
+    """The drop-in path: a 64x32x32 box handed over as scrambled arrays (node,
+    cell and vertex order random) solves with the multigrid method on the box
+    kernels, to the same solution and iteration count (within 10 %) as the
+    pa_mesh_create_box mesh, with its residual checked by the oracle."""
+    from platoanalyze_b200.workloads import cantilever, cell_density
+    dims = (64, 32, 32)
+    nx, ny, nz = dims
+    mesh_b, prob_b, faces_b, dofs_b = cantilever(dims)
+    z_box = cell_density(dims, 21, kind="smoothed", sigma=2.0, lo=0.01, hi=1.0)
+    ub, stb = prob_b.solution(z_box, options=pa.SolveOptions("mg", rel_tol=1e-10))
+    assert stb["converged"], stb
+    cl, X, new_of_old, order, faces, clamp = _scrambled(nx, ny, nz, 8)
+    m = pa.Mesh.from_arrays(cl, X)
+    assert m.box_kernels
+    prob = pa.Problem(m, 1.0, 0.3, 3.0, 1e-9, control_layout="cell")
+    flux = np.array([0.0, 0.0, -1.0 / (ny * nz)])
+    prob.add_traction(faces, flux)
+    dofs = np.sort(np.concatenate([3 * clamp, 3 * clamp + 1, 3 * clamp + 2])).astype(np.int32)
+    prob.set_dirichlet(dofs)
+    z = z_box[order]
+    u, st = prob.solution(z, options=pa.SolveOptions("mg", rel_tol=1e-10))
+    assert st["converged"], st
+    assert abs(st["iterations"] - stb["iterations"]) <= max(1, 0.1 * stb["iterations"]), (st, stb)
+    ub_mapped = np.empty_like(ub)
+    for dd in range(3):
+        ub_mapped[3 * new_of_old + dd] = ub[dd::3]
+    assert rel_inf(u, ub_mapped) <= 1e-9
+    O = oracle_lib.Oracle(cl, X, E=1.0, nu=0.3, p=3.0, pmin=1e-9, layout=1)
+    F = -O.residual(np.zeros_like(u), z, faces, flux)
+    res = F - O.apply(u, z)
+    res[dofs] = 0.0
+    assert np.linalg.norm(res) <= 1.01e-10 * np.linalg.norm(F)
+
+
+def test_box_mg_mirrored_scrambled_with_dirichlet_values(pa):
+    """A mirrored (split along another cube diagonal), scrambled 16x8x8 box
+    with prescribed nonzero Dirichlet values: the multigrid solve on the box
+    kernels equals the FP64 Jacobi-PCG solve on the caller's numbering."""
+    nx, ny, nz = 16, 8, 8
+    cl, X, new_of_old, order, faces, clamp = _scrambled(nx, ny, nz, 13, mirror_x=True)
+    m = pa.Mesh.from_arrays(cl, X)
+    assert m.box_kernels
+    prob = pa.Problem(m, 1.0, 0.3, 3.0, 1e-9, control_layout="cell")
+    prob.add_traction(faces, np.array([0.2, 0.0, -1.0 / (ny * nz)]))
+    dofs = np.sort(np.concatenate([3 * clamp, 3 * clamp + 1, 3 * clamp + 2])).astype(np.int32)
+    vals = 0.01 * np.sin(np.arange(dofs.size))
+    prob.set_dirichlet(dofs, vals)
+    rng = np.random.default_rng(4)
+    z = rng.uniform(0.05, 1.0, cl.shape[0])
+    u, st = prob.solution(z, options=pa.SolveOptions("mg", rel_tol=1e-10))
+    u64, _ = prob.solution(z, options=pa.SolveOptions("fp64", rel_tol=1e-11))
+    assert st["converged"], st
+    assert np.array_equal(u[dofs], vals)
+    assert rel_inf(u, u64) <= 1e-7

@@ -71,12 +71,22 @@ def test_mg_inhomogeneous_dirichlet_and_reuse(pa):
         assert rel_inf(u, u64) <= 1e-7
 
 
-def test_mg_refuses_unsupported_meshes(pa):
+def test_mg_accepts_array_boxes_and_refuses_unsupported_meshes(pa):
+    """A box given as arrays is recognised as a lattice (the box kernels solve
+    it); with the box kernels switched off, and with an odd hex count, the
+    multigrid method refuses."""
     from oracle import np_ref
     from platoanalyze_b200._abi import PaError
     cells, coords = np_ref.box_mesh(8, 4, 4, 8.0, 4.0, 4.0)
-    m = pa.Mesh.from_arrays(cells, coords)  # not made by the box generator
+    m = pa.Mesh.from_arrays(cells, coords)
+    assert m.box_kernels
     prob = pa.Problem(m, 1.0, 0.3, 3.0, 1e-9, control_layout="cell")
+    clamp = np.where(coords[:, 0] == 0.0)[0]
+    prob.set_dirichlet(np.sort(np.concatenate([3 * clamp, 3 * clamp + 1, 3 * clamp + 2])).astype(np.int32))
+    prob.add_traction(m.boundary_faces(0, 8.0), np.array([0.0, 0.0, -1.0 / 16]))
+    u, st = prob.solution(np.ones(m.num_cells), options=pa.SolveOptions("mg"))
+    assert st["converged"], st
+    m.set_box_kernels(False)
     with pytest.raises(PaError):
         prob.solution(np.ones(m.num_cells), options=pa.SolveOptions("mg"))
     m2 = pa.Mesh.box(7, 4, 4, 7.0, 4.0, 4.0)  # odd hex count
