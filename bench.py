@@ -551,16 +551,28 @@ def run_ours(args):
                                                                      check_every=args.check_every))
 
     # roofline of the dominant kernel timed live on this stream: the plain
-    # FP32 apply of the multigrid smoother, or the fused CG apply of Jacobi-PCG
+    # FP32 apply of the multigrid smoother (on a box: the box kernel, whose
+    # fused variants run every level of the V-cycle), or the fused CG apply
+    # of Jacobi-PCG.  `achieved` uses the per-cell/per-node algorithmic bytes
+    # of the matrix-free apply (4 node ids + penalty per tet, coordinates, x
+    # in and y out per node); the box kernel reads no ids and no coordinates
+    # (the lattice implies them), so the bytes it must move are reported too.
     import ctypes as ct
     from platoanalyze_b200 import _abi
     ms_launch, nbytes = ct.c_double(), ct.c_int64()
+    lattice_bytes = None
     if args.method == "mg":
         precision = 1
-        kernel = "k_apply_tiled (plain FP32 apply: multigrid smoothing and residuals)"
         _abi.check(_abi.load().pa_time_apply(prob._h, ct.c_void_p(z.data_ptr()), precision, 50, ct.byref(ms_launch),
                                              ct.byref(nbytes)))
-        tag = f"k_apply_tiled_plain_fp32_{dims[0]}x{dims[1]}x{dims[2]}"
+        if mesh.box_kernels:
+            kernel = "k_box (plain FP32 box apply; the multigrid levels run this kernel with fused epilogues)"
+            lattice_bytes = nbytes.value
+            nbytes.value = C * (16 + 4) + N * (3 * 4) * 3
+            tag = f"k_box_plain_fp32_{dims[0]}x{dims[1]}x{dims[2]}"
+        else:
+            kernel = "k_apply_tiled (plain FP32 apply: multigrid smoothing and residuals)"
+            tag = f"k_apply_tiled_plain_fp32_{dims[0]}x{dims[1]}x{dims[2]}"
     else:
         precision = 1 if args.method == "mixed" else 0
         kernel = "k_apply_tiled (fused CG: p update + K p + p.Kp)"
@@ -588,9 +600,12 @@ def run_ours(args):
                                f"Problem::solution to relres {args.rel_tol:g}",
                    "cells": C, "nodes": N, "dofs": ndof, "method": args.method, "mg_coarse": args.mg_coarse, "parallelism": f"replicas x{world}",
                    "preconditioner": ("geometric multigrid V-cycle: box hierarchy to the coarsest even level, "
-                                      "Chebyshev(2) smoothing in D^-1 K, Chebyshev(40) coarsest, trilinear transfers")
+                                      "Chebyshev(2) smoothing in D^-1 K before and after the coarse correction, "
+                                      "trilinear transfers, dense FP64 inverse on the coarsest level")
                    if args.method == "mg" else "Jacobi",
-                   "tile_clusters": tile, "autotune_ms_per_apply": tile_ms,
+                   "kernels": ("box kernels (lattice node ids, fused Chebyshev/residual/CG epilogues)"
+                               if args.method == "mg" and mesh.box_kernels else
+                               f"tile kernels, {tile} clusters per tile (autotuned: {tile_ms})"),
                    "geometry": "hex geometry table (uniform hexes)" if mesh.uniform_geometry else "per tet",
                    "l2": "256 MB buffer written between timed steps"},
         "solve_s": max_ms / args.steps * 1e-3, "iterations": iters, "fp64_solve_s": st64["seconds"],
@@ -606,6 +621,13 @@ def run_ours(args):
                      "peak_kind": peak_kind, "traffic": traffic, "algorithmic_bytes_per_launch": nbytes.value,
                      "ms_per_launch": ms_launch.value},
     }
+    if lattice_bytes is not None:
+        lat_gbs = lattice_bytes / (ms_launch.value * 1e-3) / 1e9
+        line["roofline"]["lattice_bytes_per_launch"] = lattice_bytes
+        line["roofline"]["lattice_bytes_frac"] = lat_gbs / peak
+        line["roofline"]["note"] = ("achieved/frac on the apply's per-cell/per-node algorithmic bytes; the box "
+                                    "kernel moves only weights, x, y and masks (lattice_bytes), and is bound by "
+                                    "instruction issue, not HBM")
     if world == 1 and not args.no_cpu_baseline:
         line.update(cpu_leg(args, dims, prob, z, u, st64))
     print(json.dumps(line), flush=True)
@@ -894,8 +916,8 @@ def run_batched(args):
     its own smoothed density (seed + i) and unit traction direction, solved
     as one parted mesh (one CG per box, all boxes in the same kernels and
     one CUDA graph per chunk) to relres 1e-8 in mixed precision, after the
-    tile-size autotuner.  Under torchrun the boxes are dealt round-robin to
-    the ranks (strong scaling; no collective on the data path)."""
+    tile-size autotuner.  Under torchrun the boxes are dealt to the ranks by
+    estimated work (strong scaling; no collective on the data path)."""
     import torch
     import torch.distributed as dist
     import platoanalyze_b200 as pa
@@ -909,11 +931,12 @@ def run_batched(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
     specs, dirs = batch_specs(args.boxes, SEED)
-    mine = dealt_boxes(args.boxes, world, rank)
+    mine = dealt_boxes(specs, world, rank)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     t0 = time.perf_counter()
-    mesh, prob, z_host, offs = batched_boxes([specs[i] for i in mine], dirs[mine], seed=SEED, stream=stream.cuda_stream)
+    mesh, prob, z_host, offs = batched_boxes([specs[i] for i in mine], dirs[mine], seed=SEED, stream=stream.cuda_stream,
+                                             box_ids=mine)
     t_build = time.perf_counter() - t0
     z = torch.tensor(z_host, device="cuda")
     tile, tile_ms = prob.autotune_tiles(z)
@@ -1009,11 +1032,13 @@ def run_batched(args):
     return 0
 
 
-def dealt_boxes(count, world, rank):
-    """Boxes of this rank in the batched workload: round-robin, so that every
-    box is solved by exactly one rank and the ranks' cell counts differ by at
-    most one box."""
-    return list(range(rank, count, world))
+def dealt_boxes(specs, world, rank):
+    """Boxes of this rank in the batched workload: dealt by estimated work
+    (tets x longest edge), longest first, each to the least-loaded rank, so
+    that every box is solved by exactly one rank and the largest rank load is
+    within one box of the mean."""
+    from platoanalyze_b200.partition import deal_boxes
+    return deal_boxes(specs, world)[rank]
 
 
 def offs_cells(offs, specs, mine, k):

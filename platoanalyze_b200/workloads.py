@@ -145,10 +145,11 @@ def batch_specs(count=64, seed=1234, lo=16, hi=48):
     return [tuple(int(v) for v in row) for row in dims], d
 
 
-def batched_boxes(specs, directions, seed=1234, stream=None, sigma=3.0):
+def batched_boxes(specs, directions, seed=1234, stream=None, sigma=3.0, box_ids=None):
     """One parted mesh + Problem holding every box (each clamped at its x = 0
     face, unit total traction along its direction on its x = max face) and
-    the per-cell densities (smoothed field, seed + i).  Boxes are laid out
+    the per-cell densities (smoothed field, seed + i, or seed + box_ids[i]
+    when the boxes are a subset of a larger batch).  Boxes are laid out
     along x with a gap, parts = boxes."""
     cells_l, coords_l, z_l, faces_l, clamp_l, offs = [], [], [], [], [], [0]
     x0, nn = 0.0, 0
@@ -159,7 +160,8 @@ def batched_boxes(specs, directions, seed=1234, stream=None, sigma=3.0):
         coords_l.append(X)
         faces_l.append(f + nn)
         clamp_l.append(cl + nn)
-        z_l.append(cell_density((nx, ny, nz), seed + i, kind="smoothed", sigma=sigma, lo=0.01, hi=1.0))
+        bid = i if box_ids is None else int(box_ids[i])
+        z_l.append(cell_density((nx, ny, nz), seed + bid, kind="smoothed", sigma=sigma, lo=0.01, hi=1.0))
         nn += X.shape[0]
         offs.append(nn)
         x0 += nx + 4.0
