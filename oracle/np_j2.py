@@ -148,21 +148,37 @@ class J2Problem:
 
     def solve(self, bc_dofs, bc_final, steps, tol=1e-10, max_newton=25):
         """Pseudo-time load stepping, Dirichlet values ramped linearly; Newton
-        with a dense solve of the constrained tangent.  Returns u and states."""
+        with a dense solve of the constrained tangent and a backtracking line
+        search on ||R_free|| (steps halved while the residual does not
+        decrease; the converged increment does not depend on it).  Returns u
+        and states; self.converged tells whether every step met tol."""
         u = np.zeros(3 * self.N)
         prev = np.zeros((self.C, 14))
         free = np.setdiff1d(np.arange(3 * self.N), bc_dofs)
+        self.converged = True
         for k in range(steps):
             u[bc_dofs] = bc_final * (k + 1) / steps
+            ok = False
             for it in range(max_newton):
                 R, cur = self.residual(u, prev)
-                if np.linalg.norm(R[free]) <= tol * max(1.0, np.linalg.norm(R)):
+                rn = np.linalg.norm(R[free])
+                if rn <= tol * max(1.0, np.linalg.norm(R)):
+                    ok = True
                     break
                 K = self.tangent(u, prev)
                 du = np.linalg.solve(K[np.ix_(free, free)], -R[free])
-                u[free] += du
-                if np.linalg.norm(du) <= 1e-14 * max(1.0, np.linalg.norm(u)):
+                a = 1.0
+                for _ in range(30):
+                    trial = u.copy()
+                    trial[free] += a * du
+                    if np.linalg.norm(self.residual(trial, prev)[0][free]) < rn:
+                        break
+                    a *= 0.5
+                u[free] += a * du
+                if np.linalg.norm(a * du) <= 1e-14 * max(1.0, np.linalg.norm(u)):
+                    ok = True
                     break
+            self.converged = self.converged and ok
             R, cur = self.residual(u, prev)
             prev = cur
         return u, prev

@@ -117,3 +117,52 @@ def test_inexact_newton_cuts_cg_work(pa):
     assert np.abs(u1 - u0).max() <= 1e-6 * np.abs(u0).max()
     assert np.abs(l1 - l0).max() <= 1e-5 * max(np.abs(l0).max(), 1e-12)
     assert s1["cg_iterations"] < s0["cg_iterations"], (s0, s1)
+
+
+@pytest.fixture(scope="module")
+def bar_8x4x4_oracle():
+    """The 8x4x4 bar (768 tets) to 2% axial strain in 4 steps, solved by the
+    NumPy J2 oracle (dense Newton, finite-difference tangent, tolerance 1e-12)."""
+    from oracle import np_j2
+    from platoanalyze_b200.fields import box_arrays
+    nx, ny, nz = 8, 4, 4
+    cells, coords, _, _ = box_arrays(nx, ny, nz)  # the numbering of pa_mesh_create_box
+    x0 = np.where(coords[:, 0] < 1e-9)[0]
+    x1 = np.where(coords[:, 0] > nx - 1e-9)[0]
+    dofs = np.concatenate([3 * x0, 3 * x0 + 1, 3 * x0 + 2, 3 * x1])
+    vals = np.concatenate([np.zeros(3 * x0.size), np.full(x1.size, 0.02 * nx)])
+    order = np.argsort(dofs)
+    prm = np_j2.J2Params(200e3, 0.3, 250.0, 1000.0, 0.0, pe=1.0, pe_min=1e-9, pp=0.5, pp_min=1e-4)
+    J = np_j2.J2Problem(cells, coords, prm, np.ones(coords.shape[0]))
+    u_ref, loc_ref = J.solve(dofs[order], vals[order], 4, tol=1e-12)
+    assert J.converged
+    return u_ref, loc_ref
+
+
+@pytest.mark.parametrize("method,forcing", [("mg", True), ("fp64", False)])
+def test_j2_mid_size_bar_matches_oracle(pa, bar_8x4x4_oracle, method, forcing):
+    """The benchmark's J2 setting (box mesh; multigrid tangent solves with
+    Eisenstat-Walker tolerances, as bench.py --workload j2 runs it, and FP64
+    Jacobi-PCG) on a bar where nearly every cell yields: displacements within
+    1e-7 and local states within 1e-6 of the oracle."""
+    u_ref, loc_ref = bar_8x4x4_oracle
+    nx, ny, nz = 8, 4, 4
+    mesh = pa.Mesh.box(nx, ny, nz, float(nx), float(ny), float(nz))
+    prob = pa.Problem(mesh, 200e3, 0.3)
+    cells, coords = mesh.arrays()
+    x0 = np.where(coords[:, 0] < 1e-9)[0]
+    x1 = np.where(coords[:, 0] > nx - 1e-9)[0]
+    dofs = np.concatenate([3 * x0, 3 * x0 + 1, 3 * x0 + 2, 3 * x1])
+    vals = np.concatenate([np.zeros(3 * x0.size), np.full(x1.size, 0.02 * nx)])
+    order = np.argsort(dofs)
+    prob.set_dirichlet(dofs[order].astype(np.int32), vals[order])
+    params = dict(youngs_modulus=200e3, poissons_ratio=0.3, initial_yield_stress=250.0,
+                  hardening_modulus_isotropic=1000.0, hardening_modulus_kinematic=0.0, elastic_penalty_exponent=1.0,
+                  elastic_min_ersatz=1e-9, plastic_penalty_exponent=0.5, plastic_min_ersatz=1e-4)
+    u, local, st = prob.j2_solve(params, np.ones(coords.shape[0]), steps=4, max_newton=30, newton_tol=1e-10,
+                                 options=pa.SolveOptions(method, rel_tol=1e-12), adaptive_forcing=forcing)
+    assert st["converged"], st
+    loc = np.asarray(local).reshape(-1, 14)
+    assert (loc_ref[:, 0] > 0).mean() > 0.95  # nearly every cell plastic at 2 %
+    assert np.abs(u - u_ref).max() <= 1e-7 * np.abs(u_ref).max()
+    assert np.abs(loc - loc_ref).max() <= 1e-6 * np.abs(loc_ref).max()
