@@ -439,16 +439,21 @@ __global__ void __launch_bounds__(kVT) k_bcg_update(int64_t n, const double* __r
   grid_reduce_finish(s, partials, counter, rr_out);
 }
 
-// out = mask ? 0 : a - b (b may be null), and out . out
-__global__ void __launch_bounds__(kVT) k_bres64(int64_t N, const double* __restrict__ a, const double* __restrict__ b,
+// out = mask ? 0 : a - b (b may be null), and out . out (one thread per node,
+// 32-bit node ids: 3 N < 2^31 on the box path)
+__global__ void __launch_bounds__(kVT) k_bres64(int N, const double* __restrict__ a, const double* __restrict__ b,
                                                 const uint8_t* __restrict__ mask, double* __restrict__ out,
                                                 double* partials, unsigned int* counter, double* nrm_out) {
   double s = 0.0;
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < 3 * N; i += int64_t(gridDim.x) * blockDim.x) {
-    const int64_t v = i % N, d = i / N;
-    const double o = ((mask[v] >> d) & 1) ? 0.0 : a[i] - (b ? b[i] : 0.0);
-    out[i] = o;
-    s += o * o;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < N; v += gridDim.x * blockDim.x) {
+    const uint8_t mk = mask[v];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const int i = d * N + v;
+      const double o = ((mk >> d) & 1) ? 0.0 : a[i] - (b ? b[i] : 0.0);
+      out[i] = o;
+      s += o * o;
+    }
   }
   grid_reduce_finish(s, partials, counter, nrm_out);
 }
@@ -480,12 +485,12 @@ __global__ void k_bset_bc(int64_t nbc, const int32_t* __restrict__ dofs, const d
 }
 
 // Restriction (R = P^T of trilinear interpolation), coarse masked dofs zero.
-__global__ void k_brestrict(int cnx, int cny, int cnz, const float* __restrict__ f, int64_t Nf,
-                            const uint8_t* __restrict__ cmask, float* __restrict__ c, int64_t Nc) {
-  const int64_t v = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+__global__ void k_brestrict(int cnx, int cny, int cnz, const float* __restrict__ f, int Nf,
+                            const uint8_t* __restrict__ cmask, float* __restrict__ c, int Nc) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= Nc) return;
   const int cpx = cnx + 1, cpy = cny + 1;
-  const int I = int(v % cpx), J = int((v / cpx) % cpy), K = int(v / (int64_t(cpx) * cpy));
+  const int I = v % cpx, J = (v / cpx) % cpy, K = v / (cpx * cpy);
   const int fpx = 2 * cnx + 1, fpy = 2 * cny + 1, fpz = 2 * cnz + 1;
   float s[3] = {0.f, 0.f, 0.f};
   for (int dc = -1; dc <= 1; ++dc) {
@@ -500,7 +505,7 @@ __global__ void k_brestrict(int cnx, int cny, int cnz, const float* __restrict__
         const int i = 2 * I + da;
         if (i < 0 || i >= fpx) continue;
         const float w = wb * (da ? 0.5f : 1.0f);
-        const int64_t fv = i + int64_t(fpx) * (j + int64_t(fpy) * k);
+        const int fv = i + fpx * (j + fpy * k);
 #pragma unroll
         for (int d = 0; d < 3; ++d) s[d] += w * f[d * Nf + fv];
       }
@@ -513,12 +518,12 @@ __global__ void k_brestrict(int cnx, int cny, int cnz, const float* __restrict__
 
 // x_fine += P e (trilinear interpolation of the coarse correction), fine
 // masked dofs untouched (they stay zero).
-__global__ void k_bprolong_add(int cnx, int cny, const float* __restrict__ e, int64_t Nc,
-                               const uint8_t* __restrict__ fmask, float* __restrict__ x, int64_t Nf) {
-  const int64_t v = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+__global__ void k_bprolong_add(int cnx, int cny, const float* __restrict__ e, int Nc,
+                               const uint8_t* __restrict__ fmask, float* __restrict__ x, int Nf) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= Nf) return;
   const int fpx = 2 * cnx + 1, fpy = 2 * cny + 1;
-  const int i = int(v % fpx), j = int((v / fpx) % fpy), k = int(v / (int64_t(fpx) * fpy));
+  const int i = v % fpx, j = (v / fpx) % fpy, k = v / (fpx * fpy);
   const int cpx = cnx + 1, cpy = cny + 1;
   const int ia = i >> 1, ja = j >> 1, ka = k >> 1;
   const int ni = (i & 1) + 1, nj = (j & 1) + 1, nk = (k & 1) + 1;
@@ -527,7 +532,7 @@ __global__ void k_bprolong_add(int cnx, int cny, const float* __restrict__ e, in
   for (int c = 0; c < nk; ++c)
     for (int b = 0; b < nj; ++b)
       for (int a = 0; a < ni; ++a) {
-        const int64_t cv = (ia + a) + int64_t(cpx) * ((ja + b) + int64_t(cpy) * (ka + c));
+        const int cv = (ia + a) + cpx * ((ja + b) + cpy * (ka + c));
 #pragma unroll
         for (int d = 0; d < 3; ++d) s[d] += e[d * Nc + cv];
       }
@@ -538,18 +543,22 @@ __global__ void k_bprolong_add(int cnx, int cny, const float* __restrict__ e, in
 }
 
 // deterministic zero-mean start vector in [-1, 1], masked; ||x||^2 reduced
-__global__ void __launch_bounds__(kVT) k_bseed(int64_t N, const uint8_t* __restrict__ mask, float* __restrict__ x,
+__global__ void __launch_bounds__(kVT) k_bseed(int N, const uint8_t* __restrict__ mask, float* __restrict__ x,
                                                double* partials, unsigned int* counter, double* nrm_out) {
   double s = 0.0;
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < 3 * N; i += int64_t(gridDim.x) * blockDim.x) {
-    const int64_t v = i % N, d = i / N;
-    uint32_t h = uint32_t(i) * 2654435761u + 0x9e3779b9u;
-    h ^= h >> 16;
-    h *= 0x85ebca6bu;
-    h ^= h >> 13;
-    const float val = ((mask[v] >> d) & 1) ? 0.f : float(int(h % 2001u) - 1000) * 1e-3f;
-    x[i] = val;
-    s += double(val) * val;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < N; v += gridDim.x * blockDim.x) {
+    const uint8_t mk = mask[v];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const int i = d * N + v;
+      uint32_t h = uint32_t(i) * 2654435761u + 0x9e3779b9u;
+      h ^= h >> 16;
+      h *= 0x85ebca6bu;
+      h ^= h >> 13;
+      const float val = ((mk >> d) & 1) ? 0.f : float(int(h % 2001u) - 1000) * 1e-3f;
+      x[i] = val;
+      s += double(val) * val;
+    }
   }
   grid_reduce_finish(s, partials, counter, nrm_out);
 }
@@ -557,22 +566,28 @@ __global__ void __launch_bounds__(kVT) k_bseed(int64_t N, const uint8_t* __restr
 // interleaved caller's order -> component-major lattice order (node_of null:
 // same order; flip bit d: component d changes sign)
 template <typename S, typename T>
-__global__ void k_bperm_in(int64_t N, const int32_t* __restrict__ node_of, int flip, const S* __restrict__ aos,
+__global__ void k_bperm_in(int N, const int32_t* __restrict__ node_of, int flip, const S* __restrict__ aos,
                            T* __restrict__ soa) {
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < 3 * N; i += int64_t(gridDim.x) * blockDim.x) {
-    const int64_t b = i % N, d = i / N;
-    const T v = T(aos[3 * int64_t(node_of ? node_of[b] : b) + d]);
-    soa[i] = ((flip >> d) & 1) ? -v : v;
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < N; b += gridDim.x * blockDim.x) {
+    const int64_t u = 3 * int64_t(node_of ? node_of[b] : b);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const T v = T(aos[u + d]);
+      soa[d * N + b] = ((flip >> d) & 1) ? -v : v;
+    }
   }
 }
 // component-major lattice order -> interleaved caller's order
 template <typename T, typename S>
-__global__ void k_bperm_out(int64_t N, const int32_t* __restrict__ node_of, int flip, const T* __restrict__ soa,
+__global__ void k_bperm_out(int N, const int32_t* __restrict__ node_of, int flip, const T* __restrict__ soa,
                             S* __restrict__ aos) {
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < 3 * N; i += int64_t(gridDim.x) * blockDim.x) {
-    const int64_t b = i % N, d = i / N;
-    const S v = S(soa[i]);
-    aos[3 * int64_t(node_of ? node_of[b] : b) + d] = ((flip >> d) & 1) ? -v : v;
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < N; b += gridDim.x * blockDim.x) {
+    const int64_t u = 3 * int64_t(node_of ? node_of[b] : b);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const S v = S(soa[d * N + b]);
+      aos[u + d] = ((flip >> d) & 1) ? -v : v;
+    }
   }
 }
 // node mask in lattice order
@@ -1049,7 +1064,7 @@ bool boxmg_setup(Problem& P, const double* z) {
     }
     const bool warm = L.pw_valid;
     if (!warm)
-      k_bseed<<<vec_blocks(n3), kVT, 0, s>>>(L.d.N, L.mask, L.pw0.get(), H.partials.get(), H.counter.get(), nl);
+      k_bseed<<<vec_blocks(L.d.N), kVT, 0, s>>>(int(L.d.N), L.mask, L.pw0.get(), H.partials.get(), H.counter.get(), nl);
     else
       k_bnorm2<<<vec_blocks(n3), kVT, 0, s>>>(n3, L.pw0.get(), H.partials.get(), H.counter.get(), nl);
     PA_LAUNCHED();
@@ -1158,13 +1173,14 @@ void vcycle_level(const Problem& P, BoxHierarchy& H, size_t l, const B* b, O* xo
   // residual, restricted to the coarse right-hand side
   launch_box<float>(L, g, w, InVec<float, float>{L.x.get(), nullptr, N}, OutRes<B>{L.r.get(), b, L.mask, N}, red,
                     s);
-  k_brestrict<<<int((C.d.N + kVT - 1) / kVT), kVT, 0, s>>>(C.d.nx, C.d.ny, C.d.nz, L.r.get(), N, C.mask, C.b.get(),
+  k_brestrict<<<int((C.d.N + kVT - 1) / kVT), kVT, 0, s>>>(C.d.nx, C.d.ny, C.d.nz, L.r.get(), int(N), C.mask, C.b.get(),
                                                            C.d.N);
   PA_LAUNCHED();
   g_box_launches += 1;
   vcycle(P, H, l + 1, s);
   // post-smoothing from x + P e
-  k_bprolong_add<<<int((N + kVT - 1) / kVT), kVT, 0, s>>>(C.d.nx, C.d.ny, C.x.get(), C.d.N, L.mask, L.x.get(), N);
+  k_bprolong_add<<<int((N + kVT - 1) / kVT), kVT, 0, s>>>(C.d.nx, C.d.ny, C.x.get(), int(C.d.N), L.mask, L.x.get(),
+                                                          int(N));
   PA_LAUNCHED();
   g_box_launches += 1;
   launch_box<float>(L, g, w, InVec<float, float>{L.x.get(), nullptr, N}, OutPost1<B>{L.r.get(), b, L.dinv.get(), N},
@@ -1212,7 +1228,7 @@ bool solve_boxmg(Problem& P, const double* z, const double* b, double* x_out, co
   const int64_t nbc = int64_t(P.bc_dofs.size());
   const Mesh& m = *P.mesh;
   const int32_t* node_of = m.lat_permuted ? m.d_lat_node.get() : nullptr;
-  k_bperm_in<double, double><<<vec_blocks(n), kVT, 0, s>>>(N, node_of, m.lat_flip, b, t);
+  k_bperm_in<double, double><<<vec_blocks(N), kVT, 0, s>>>(int(N), node_of, m.lat_flip, b, t);
   PA_LAUNCHED();
   if (nbc) {
     PA_CUDA(cudaMemsetAsync(zv, 0, sizeof(double) * n, s));
@@ -1221,9 +1237,9 @@ bool solve_boxmg(Problem& P, const double* z, const double* b, double* x_out, co
                                                          m.lat_flip, zv);
     PA_LAUNCHED();
     box_apply64(F, P.ep, w64, zv, H.q.get(), nullptr, red, s);
-    k_bres64<<<vec_blocks(n), kVT, 0, s>>>(N, t, H.q.get(), mask, bp, H.partials.get(), H.counter.get(), sc + kRr);
+    k_bres64<<<vec_blocks(N), kVT, 0, s>>>(int(N), t, H.q.get(), mask, bp, H.partials.get(), H.counter.get(), sc + kRr);
   } else {
-    k_bres64<<<vec_blocks(n), kVT, 0, s>>>(N, t, nullptr, mask, bp, H.partials.get(), H.counter.get(), sc + kRr);
+    k_bres64<<<vec_blocks(N), kVT, 0, s>>>(int(N), t, nullptr, mask, bp, H.partials.get(), H.counter.get(), sc + kRr);
   }
   PA_LAUNCHED();
   double bb = 0.0;
@@ -1290,7 +1306,7 @@ bool solve_boxmg(Problem& P, const double* z, const double* b, double* x_out, co
     if (breakdown) break;
     // confirm on the true residual r = b' - K x (p and the scalars restart)
     box_apply64(F, P.ep, w64, x, H.q.get(), mask, red, s);
-    k_bres64<<<vec_blocks(n), kVT, 0, s>>>(N, bp, H.q.get(), mask, r, H.partials.get(), H.counter.get(), sc + kRr);
+    k_bres64<<<vec_blocks(N), kVT, 0, s>>>(int(N), bp, H.q.get(), mask, r, H.partials.get(), H.counter.get(), sc + kRr);
     PA_LAUNCHED();
     g_box_launches += 1;
     PA_CUDA(cudaMemcpyAsync(&rr_true, sc + kRr, sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -1303,7 +1319,7 @@ bool solve_boxmg(Problem& P, const double* z, const double* b, double* x_out, co
     }
   }
   // x_out = x + x_D (interleaved, caller's order)
-  k_bperm_out<double, double><<<vec_blocks(n), kVT, 0, s>>>(N, node_of, m.lat_flip, x, x_out);
+  k_bperm_out<double, double><<<vec_blocks(N), kVT, 0, s>>>(int(N), node_of, m.lat_flip, x, x_out);
   PA_LAUNCHED();
   if (nbc) {
     k_bset_bc<<<int((nbc + 255) / 256), 256, 0, s>>>(nbc, P.d_bc_dofs.get(), P.d_bc_vals.get(), 1.0, x_out);
@@ -1347,8 +1363,7 @@ void box_apply(Problem& P, const double* z, const T* x, T* y, bool constrained, 
   F.wm = differ ? 1 : 0;
   const uint8_t* mask = constrained ? lattice_mask(P) : nullptr;
   const int32_t* node_of = m.lat_permuted ? m.d_lat_node.get() : nullptr;
-  const int64_t n = 3 * F.d.N;
-  k_bperm_in<T, T><<<vec_blocks(n), kVT, 0, s>>>(F.d.N, node_of, m.lat_flip, x, xs);
+  k_bperm_in<T, T><<<vec_blocks(F.d.N), kVT, 0, s>>>(int(F.d.N), node_of, m.lat_flip, x, xs);
   PA_LAUNCHED();
   const BoxRed red{H.partials.get(), H.counter.get()};
   if constexpr (std::is_same<T, double>::value) {
@@ -1357,7 +1372,7 @@ void box_apply(Problem& P, const double* z, const T* x, T* y, bool constrained, 
     launch_box<float>(F, box_geo<float>(F, P.ep), level_w32(H, 0), InVec<float, float>{xs, mask, F.d.N},
                       OutPlain<float>{ys, mask, F.d.N}, red, s);
   }
-  k_bperm_out<T, T><<<vec_blocks(n), kVT, 0, s>>>(F.d.N, node_of, m.lat_flip, ys, y);
+  k_bperm_out<T, T><<<vec_blocks(F.d.N), kVT, 0, s>>>(int(F.d.N), node_of, m.lat_flip, ys, y);
   PA_LAUNCHED();
 }
 template void box_apply<double>(Problem&, const double*, const double*, double*, bool, double*, double*);
