@@ -120,7 +120,7 @@ template <typename B>
 struct InDinvB {  // d0 = dinv b / theta
   const B* b;
   const float* dinv;
-  float s;
+  const float* ch;  // the level's Chebyshev coefficients (1 / theta, ca, c2)
   int64_t N;
   struct Raw {
     float d[3];
@@ -136,6 +136,7 @@ struct InDinvB {  // d0 = dinv b / theta
     return r;
   }
   __device__ void make(const Raw& r, int, bool, float (&o)[3]) const {
+    const float s = __ldg(ch);
 #pragma unroll
     for (int c = 0; c < 3; ++c) o[c] = s * r.d[c] * float(r.b[c]);
   }
@@ -146,7 +147,7 @@ struct OutPre {  // x = dinv (ca b - c2 K d0)
   float* x;
   const B* b;
   const float* dinv;
-  float ca, c2;
+  const float* ch;
   int64_t N;
   static constexpr bool kReduce = false;
   struct Pre {
@@ -163,6 +164,7 @@ struct OutPre {  // x = dinv (ca b - c2 K d0)
     return p;
   }
   __device__ double store(const Pre& p, int v, const float (&k)[3]) const {
+    const float ca = __ldg(ch + 1), c2 = __ldg(ch + 2);
 #pragma unroll
     for (int c = 0; c < 3; ++c) x[c * int(N) + v] = p.d[c] * (ca * float(p.b[c]) - c2 * k[c]);
     return 0.0;
@@ -224,9 +226,9 @@ struct OutPost1 {  // r0 = dinv (b - K xi)
   __device__ void finish(double) const {}
 };
 
-struct InScaled {  // d0 = s r0
+struct InScaled {  // d0 = r0 / theta
   const float* r;
-  float s;
+  const float* ch;
   int64_t N;
   struct Raw {
     float r[3];
@@ -239,7 +241,7 @@ struct InScaled {  // d0 = s r0
   }
   __device__ void make(const Raw& q, int, bool, float (&o)[3]) const {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) o[c] = s * q.r[c];
+    for (int c = 0; c < 3; ++c) o[c] = __ldg(ch) * q.r[c];
   }
 };
 
@@ -253,7 +255,7 @@ struct OutPost2 {
   const float* x;
   const float* r0;
   const float* dinv;
-  float ca, c2;
+  const float* ch;
   int64_t N;
   const double* rvec;  // RZ: the outer residual
   double* sc;          // RZ: the outer CG scalars
@@ -276,6 +278,7 @@ struct OutPost2 {
   }
   __device__ double store(const Pre& p, int v, const float (&kd)[3]) const {
     double acc = 0.0;
+    const float ca = __ldg(ch + 1), c2 = __ldg(ch + 2);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const float z = p.x[c] + ca * p.r0[c] - c2 * p.d[c] * kd[c];
@@ -758,7 +761,8 @@ struct BoxLevel {
   bool pw_valid = false;
   // coarsest level: dense inverse
   int64_t nd = 0;
-  DevBuf<double> dense, gj_w, gj_c, gj_p, diag0, flag;
+  DevBuf<double> dense, gj_c, gj_p, diag0, flag;
+  DevBuf<unsigned> gj_sync;
 };
 
 struct BoxHierarchy {
@@ -772,6 +776,33 @@ struct BoxHierarchy {
   DevBuf<unsigned int> counter;
   DevBuf<double> p0, p1, q;  // outer CG directions (ping-pong) and K p
   DevBuf<uint8_t> mask0;     // the finest level's Dirichlet mask in lattice order (permuted meshes)
+  std::vector<int32_t> mask_dofs;  // the Dirichlet set the coarse masks were built for
+  bool masks_valid = false;
+  DevBuf<float> cheb;  // per smoothed level: 1 / theta, ca, c2 (read by the captured iteration)
+  // the captured outer iteration (two variants alternate the p buffers),
+  // reused while every pointer and constant it captured is unchanged
+  struct GraphKey {
+    const void* ptr[6] = {};
+    int wm = -1;
+    double lam = 0.0, mu = 0.0;
+    bool operator==(const GraphKey& o) const {
+      for (int k = 0; k < 6; ++k)
+        if (ptr[k] != o.ptr[k]) return false;
+      return wm == o.wm && lam == o.lam && mu == o.mu;
+    }
+  } key;
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  int64_t per_iter = 0;
+  BoxHierarchy() = default;
+  BoxHierarchy(const BoxHierarchy&) = delete;
+  BoxHierarchy& operator=(const BoxHierarchy&) = delete;
+  ~BoxHierarchy() { drop_graphs(); }
+  void drop_graphs() {
+    for (auto& e : gexec) {
+      if (e) cudaGraphExecDestroy(e);
+      e = nullptr;
+    }
+  }
 };
 
 void boxmg_release(Problem& P) {
@@ -877,7 +908,6 @@ void coarse_mask(const BoxLevel& f, BoxLevel& c, const std::vector<uint8_t>& fma
 
 }  // namespace
 
-// True when the box kernels can run this problem's multigrid solve.
 // True when the box kernels can run this problem's multigrid solve: a box
 // of mesh_make_box with even hex counts, one part, and a coarsest level (the
 // box halved while every axis stays even with at least 4 hexes) of at most
@@ -988,17 +1018,22 @@ bool boxmg_setup(Problem& P, const double* z) {
       m.lat_permuted ? m.d_lat_node.get() : nullptr, H.w64t.get(), H.w32t.get(), H.w64h.get(), H.w32h.get(),
       H.differ.get());
   PA_LAUNCHED();
-  // masks by injection (host, from the problem's Dirichlet dofs)
-  std::vector<uint8_t> fmask(size_t(F.d.N), 0);
-  for (int32_t dof : P.bc_dofs) {
-    const int32_t v = dof / 3;
-    fmask[size_t(m.lat_permuted ? m.h_lat_of_node[size_t(v)] : v)] |= uint8_t(1u << (dof % 3));
-  }
-  for (size_t l = 1; l < H.L.size(); ++l) {
-    std::vector<uint8_t> cmask;
-    coarse_mask(*H.L[l - 1], *H.L[l], fmask, cmask);
-    H.L[l]->own_mask.upload(cmask.data(), cmask.size(), s);
-    fmask.swap(cmask);
+  // coarse masks by injection (host, from the problem's Dirichlet dofs),
+  // rebuilt only when the Dirichlet set changed since the last solve
+  if (!H.masks_valid || H.mask_dofs != P.bc_dofs) {
+    std::vector<uint8_t> fmask(size_t(F.d.N), 0);
+    for (int32_t dof : P.bc_dofs) {
+      const int32_t v = dof / 3;
+      fmask[size_t(m.lat_permuted ? m.h_lat_of_node[size_t(v)] : v)] |= uint8_t(1u << (dof % 3));
+    }
+    for (size_t l = 1; l < H.L.size(); ++l) {
+      std::vector<uint8_t> cmask;
+      coarse_mask(*H.L[l - 1], *H.L[l], fmask, cmask);
+      H.L[l]->own_mask.upload(cmask.data(), cmask.size(), s);
+      fmask.swap(cmask);
+    }
+    H.mask_dofs = P.bc_dofs;
+    H.masks_valid = true;
   }
   unsigned int differ = 0;
   PA_CUDA(cudaMemcpyAsync(&differ, H.differ.get(), sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
@@ -1029,9 +1064,9 @@ bool boxmg_setup(Problem& P, const double* z) {
     const int64_t n3 = 3 * Lc.d.N, nd = (n3 + kGJ - 1) / kGJ * kGJ;
     if (Lc.nd != nd) {
       Lc.dense.resize(nd * nd);
-      Lc.gj_w.resize(kGJ * nd);
       Lc.gj_c.resize(nd * kGJ);
-      Lc.gj_p.resize(kGJ * kGJ);
+      Lc.gj_p.resize(2 * kGJ * kGJ);
+      Lc.gj_sync.resize(1);
       Lc.diag0.resize(nd);
       Lc.flag.resize(1);
       Lc.nd = nd;
@@ -1042,8 +1077,8 @@ bool boxmg_setup(Problem& P, const double* z) {
                                                                         Lc.w64.get(), Lc.mask, nd, Lc.dense.get());
     k_bdense_ident<<<int((nd + kVT - 1) / kVT), kVT, 0, s>>>(Lc.d.N, nd, Lc.mask, Lc.dense.get(), Lc.diag0.get());
     PA_LAUNCHED();
-    gj_invert(s, nd, Lc.dense.get(), Lc.diag0.get(), Lc.gj_w.get(), Lc.gj_c.get(), Lc.gj_p.get(), Lc.flag.get());
-    g_box_launches += 2 + 3 * (nd / kGJ);
+    gj_invert(s, nd, Lc.dense.get(), Lc.diag0.get(), Lc.gj_c.get(), Lc.gj_p.get(), Lc.gj_sync.get(), Lc.flag.get());
+    g_box_launches += 3;
   }
   // lmax of D^-1 K per smoothed level by power iteration, on the device
   // (the norm of each step lands in norms[level][step]); an elastic solve
@@ -1088,6 +1123,7 @@ bool boxmg_setup(Problem& P, const double* z) {
   double flag = 0.0;
   PA_CUDA(cudaMemcpyAsync(&flag, Lc.flag.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
   PA_CUDA(cudaStreamSynchronize(s));
+  if (flag >= 2.0) throw Error(PA_ERR_CUDA, "coarsest factorization: a grid barrier timed out");
   if (flag != 0.0) return false;
   for (size_t l = 0; l < NS; ++l) {
     BoxLevel& L = *H.L[l];
@@ -1162,14 +1198,14 @@ void vcycle_level(const Problem& P, BoxHierarchy& H, size_t l, const B* b, O* xo
                   cudaStream_t s) {
   BoxLevel& L = *H.L[l];
   BoxLevel& C = *H.L[l + 1];
-  const ChebStep ch = cheb2(L.lmax);
+  const float* ch = H.cheb.get() + 3 * l;
   const BoxGeo<float> g = box_geo<float>(L, P.ep);
   const float* w = level_w32(H, l);
   const BoxRed red{H.partials.get(), H.counter.get()};
   const int64_t N = L.d.N;
   // pre-smoothing from x = 0
-  launch_box<float>(L, g, w, InDinvB<B>{b, L.dinv.get(), ch.inv_theta, N},
-                    OutPre<B>{L.x.get(), b, L.dinv.get(), ch.ca, ch.c2, N}, red, s);
+  launch_box<float>(L, g, w, InDinvB<B>{b, L.dinv.get(), ch, N},
+                    OutPre<B>{L.x.get(), b, L.dinv.get(), ch, N}, red, s);
   // residual, restricted to the coarse right-hand side
   launch_box<float>(L, g, w, InVec<float, float>{L.x.get(), nullptr, N}, OutRes<B>{L.r.get(), b, L.mask, N}, red,
                     s);
@@ -1185,8 +1221,8 @@ void vcycle_level(const Problem& P, BoxHierarchy& H, size_t l, const B* b, O* xo
   g_box_launches += 1;
   launch_box<float>(L, g, w, InVec<float, float>{L.x.get(), nullptr, N}, OutPost1<B>{L.r.get(), b, L.dinv.get(), N},
                     red, s);
-  launch_box<float>(L, g, w, InScaled{L.r.get(), ch.inv_theta, N},
-                    OutPost2<O, RZ>{xo, L.x.get(), L.r.get(), L.dinv.get(), ch.ca, ch.c2, N, rvec, sc}, red, s);
+  launch_box<float>(L, g, w, InScaled{L.r.get(), ch, N},
+                    OutPost2<O, RZ>{xo, L.x.get(), L.r.get(), L.dinv.get(), ch, N, rvec, sc}, red, s);
 }
 
 // y = K x (FP64, box kernel) with optional masks on input and output
@@ -1253,37 +1289,56 @@ bool solve_boxmg(Problem& P, const double* z, const double* b, double* x_out, co
   PA_CUDA(cudaMemsetAsync(H.p0.get(), 0, sizeof(double) * n, s));
   k_bcg_reset<<<1, 1, 0, s>>>(sc);
   PA_LAUNCHED();
-  // one outer iteration as a graph; two variants alternate the p buffers
-  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
-  cudaGraph_t graph[2] = {nullptr, nullptr};
-  struct GraphGuard {
-    cudaGraph_t* g;
-    cudaGraphExec_t* e;
-    ~GraphGuard() {
-      for (int k = 0; k < 2; ++k) {
-        if (e[k]) cudaGraphExecDestroy(e[k]);
-        if (g[k]) cudaGraphDestroy(g[k]);
-      }
+  // this solve's Chebyshev coefficients, read by the captured iteration
+  {
+    const size_t NS = H.L.size() - 1;
+    std::vector<float> ch(3 * NS);
+    for (size_t l = 0; l < NS; ++l) {
+      const ChebStep c = cheb2(H.L[l]->lmax);
+      ch[3 * l] = c.inv_theta;
+      ch[3 * l + 1] = c.ca;
+      ch[3 * l + 2] = c.c2;
     }
-  } guard{graph, gexec};
-  int64_t per_iter = 0;
-  for (int k = 0; k < 2; ++k) {
-    double* pold = k == 0 ? H.p0.get() : H.p1.get();
-    double* pnew = k == 0 ? H.p1.get() : H.p0.get();
-    const int64_t before = g_box_launches;
-    PA_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    vcycle_level<double, double, true>(P, H, 0, r, zv, r, sc, s);
-    launch_box<double>(F, box_geo<double>(F, P.ep), w64, InCgP{zv, pold, pnew, sc, N},
-                       OutCgQ{H.q.get(), zv, pold, mask, sc, N}, red, s);
-    k_bcg_update<<<vec_blocks(n), kVT, 0, s>>>(n, sc, pnew, H.q.get(), x, r, H.partials.get(), H.counter.get(),
-                                               sc + kRr);
-    g_box_launches += 1;
-    const cudaError_t ce = cudaStreamEndCapture(s, &graph[k]);
-    if (ce != cudaSuccess) throw Error(PA_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
-    PA_CUDA(cudaGraphInstantiate(&gexec[k], graph[k], 0));
-    per_iter = g_box_launches - before;
-    g_box_launches = before;
+    if (H.cheb.n != ch.size()) H.cheb.resize(ch.size());
+    PA_CUDA(cudaMemcpyAsync(H.cheb.get(), ch.data(), sizeof(float) * ch.size(), cudaMemcpyHostToDevice, s));
   }
+  // one outer iteration as a graph; two variants alternate the p buffers.
+  // Captured once and relaunched by later solves while the buffers, the
+  // weight layout and the material are the same.
+  BoxHierarchy::GraphKey key;
+  const void* ptrs[6] = {zv, r, x, mask, w64, bp};
+  for (int k = 0; k < 6; ++k) key.ptr[k] = ptrs[k];
+  key.wm = F.wm;
+  key.lam = P.ep.iso().lam;
+  key.mu = P.ep.iso().mu;
+  if (!(H.gexec[0] && H.key == key)) {
+    H.drop_graphs();
+    for (int k = 0; k < 2; ++k) {
+      double* pold = k == 0 ? H.p0.get() : H.p1.get();
+      double* pnew = k == 0 ? H.p1.get() : H.p0.get();
+      const int64_t before = g_box_launches;
+      PA_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      vcycle_level<double, double, true>(P, H, 0, r, zv, r, sc, s);
+      launch_box<double>(F, box_geo<double>(F, P.ep), w64, InCgP{zv, pold, pnew, sc, N},
+                         OutCgQ{H.q.get(), zv, pold, mask, sc, N}, red, s);
+      k_bcg_update<<<vec_blocks(n), kVT, 0, s>>>(n, sc, pnew, H.q.get(), x, r, H.partials.get(), H.counter.get(),
+                                                 sc + kRr);
+      g_box_launches += 1;
+      cudaGraph_t graph = nullptr;
+      const cudaError_t ce = cudaStreamEndCapture(s, &graph);
+      if (ce != cudaSuccess) throw Error(PA_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+      const cudaError_t ie = cudaGraphInstantiate(&H.gexec[k], graph, 0);
+      cudaGraphDestroy(graph);
+      if (ie != cudaSuccess) {
+        H.drop_graphs();
+        throw Error(PA_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+      }
+      H.per_iter = g_box_launches - before;
+      g_box_launches = before;
+    }
+    H.key = key;
+  }
+  const int64_t per_iter = H.per_iter;
   int iters = 0, restarts = 0;
   double rr_true = bb;
   bool converged = false, breakdown = false;
@@ -1291,7 +1346,7 @@ bool solve_boxmg(Problem& P, const double* z, const double* b, double* x_out, co
   while (!converged && iters < max_iters && !breakdown) {
     double rr = bb;
     while (iters < max_iters) {
-      PA_CUDA(cudaGraphLaunch(gexec[iters & 1], s));
+      PA_CUDA(cudaGraphLaunch(H.gexec[iters & 1], s));
       g_box_launches += per_iter;
       ++iters;
       PA_CUDA(cudaMemcpyAsync(h2, sc + kRr, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));

@@ -380,7 +380,8 @@ struct MgLevel {
   bool ev_valid = false;  // ev (and lmax) come from an elastic operator
   // coarsest level, direct solve: the dense inverse (nd x nd) and its scratch
   int64_t nd = 0;
-  DevBuf<double> dense, gj_w, gj_c, gj_p, diag0, gj_flag;
+  DevBuf<double> dense, gj_c, gj_p, diag0, gj_flag;
+  DevBuf<unsigned> gj_sync;
 };
 
 struct MgHierarchy {
@@ -415,9 +416,9 @@ bool coarse_factor(MgLevel& L, cudaStream_t s) {
   const int64_t n3 = 3 * L.N, nd = (n3 + kGJ - 1) / kGJ * kGJ;
   if (L.nd != nd) {
     L.dense.resize(nd * nd);
-    L.gj_w.resize(kGJ * nd);
     L.gj_c.resize(nd * kGJ);
-    L.gj_p.resize(kGJ * kGJ);
+    L.gj_p.resize(2 * kGJ * kGJ);
+    L.gj_sync.resize(1);
     L.diag0.resize(nd);
     L.gj_flag.resize(1);
     L.nd = nd;
@@ -430,11 +431,12 @@ bool coarse_factor(MgLevel& L, cudaStream_t s) {
                                                    L.dense.get());
   k_mg_dense_ident<<<grid_all(nd), kT, 0, s>>>(L.N, nd, L.P->d_node_mask.get(), L.dense.get(), L.diag0.get());
   PA_LAUNCHED();
-  gj_invert(s, nd, L.dense.get(), L.diag0.get(), L.gj_w.get(), L.gj_c.get(), L.gj_p.get(), L.gj_flag.get());
-  g_launches += 2 + 3 * (nd / kGJ);
+  gj_invert(s, nd, L.dense.get(), L.diag0.get(), L.gj_c.get(), L.gj_p.get(), L.gj_sync.get(), L.gj_flag.get());
+  g_launches += 3;
   double flag = 0.0;
   PA_CUDA(cudaMemcpyAsync(&flag, L.gj_flag.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
   PA_CUDA(cudaStreamSynchronize(s));
+  if (flag >= 2.0) throw Error(PA_ERR_CUDA, "coarsest factorization: a grid barrier timed out");
   return flag == 0.0;
 }
 
