@@ -398,6 +398,27 @@ pa_status pa_up_residual(pa_problem* problem, const pa_up_params* params, const 
                          const double* ppg, int32_t ppg_per_cell, const double* z, double* residual,
                          int32_t assembled);
 
+/* Stabilized u-p J2 plasticity solve, PlasticityProblem::solution's forward
+ * problem (src/PlasticityProblem.hpp:791-846) with NewtonRaphsonSolver::solve
+ * (src/NewtonRaphsonSolver.hpp:570-640): load steps over the problem's
+ * Dirichlet values (displacement dofs 3 v + i, the final values; the
+ * pressures are free), each Newton iterate returning the local states from
+ * the previous step's (the J2 return mapping of `params`) and solving with the
+ * condensed tangent dR/du - dR/dc (dH/dc)^-1 dH/du; the projected pressure
+ * gradient of step k+1 is the lumped projection of step k's pressure
+ * (PlasticityProblem::updateProjectedPressureGradient, :877-897), zero in the
+ * first step.  The tangent is symmetric indefinite: MINRES with the inverse
+ * absolute diagonal, to linear->rel_tol (default 1e-12) within
+ * linear->max_iters (0: 100000); linear->method is ignored.  A step ends when
+ * ||R_free|| <= newton_tol x ||R_free|| of the new boundary values on the
+ * previous field (backtracking line search as pa_j2_solve).  Outputs the
+ * state (u_x, u_y, u_z, p per node; 4N), the local states (C x 14) and, when
+ * ppg is not NULL, the projected pressure gradient of the last step (3N).
+ * stats->cg_iterations counts MINRES iterations. */
+pa_status pa_up_solve(pa_problem* problem, const pa_up_params* up, const pa_j2_params* params, const double* z,
+                      const pa_j2_solve_options* options, const pa_solve_options* linear, double* state,
+                      double* local, double* ppg, pa_j2_stats* stats);
+
 /* ------------------------------------------------------ batched solves --- */
 /* No counterpart in the reference (one Problem solves one mesh).  A parted
  * mesh is the disjoint union of independent sub-meshes: part p owns the nodes

@@ -348,15 +348,45 @@ class Problem:
         state, local, ppg, z = (_as(a, np.float64) for a in (state, local, ppg, z))
         n_out = 4 * N if assembled else 16 * C
         out = _empty(state, n_out) if out is None else out
-        up = _abi.UpParams(*[float(params.get(k, d)) for k, d in (
-            ("youngs_modulus", None), ("poissons_ratio", None), ("penalty_exponent", 3.0), ("penalty_min", 1e-9),
-            ("pressure_scaling", 1.0))])
+        up = self._up_params(params)
         _abi.check(self._lib.pa_up_residual(self._h, ct.byref(up), _ptr(state, np.float64, 4 * N, "state"),
                                             _ptr(local, np.float64, 14 * C, "local"),
                                             _ptr(ppg, np.float64, 12 * C if per_cell_ppg else 3 * N, "ppg"),
                                             int(bool(per_cell_ppg)), _ptr(z, np.float64, N, "z"),
                                             _ptr(out, np.float64, n_out, "residual"), int(bool(assembled))))
         return out
+
+    @staticmethod
+    def _up_params(params):
+        return _abi.UpParams(*[float(params.get(k, d)) for k, d in (
+            ("youngs_modulus", None), ("poissons_ratio", None), ("penalty_exponent", 3.0), ("penalty_min", 1e-9),
+            ("pressure_scaling", 1.0))])
+
+    def up_solve(self, up_params, j2_params, z, steps=1, max_newton=20, newton_tol=1e-10, rel_tol=1e-12,
+                 max_iters=0, state=None, local=None, ppg=None, allow_not_converged=False):
+        """Stabilized u-p J2 plasticity solve (pa_up_solve): returns the state
+        (u_x, u_y, u_z, p per node), the local states (C x 14), the projected
+        pressure gradient of the last step (3N) and the solve statistics."""
+        C, N = self.mesh.num_cells, self.mesh.num_nodes
+        z = _as(z, np.float64)
+        state = _empty(z, 4 * N) if state is None else state
+        local = _empty(z, 14 * C) if local is None else local
+        ppg = _empty(z, 3 * N) if ppg is None else ppg
+        up = self._up_params(up_params)
+        jp = self._j2_params(j2_params)
+        jo = _abi.J2SolveOptions(int(steps), int(max_newton), float(newton_tol), 0)
+        lo = SolveOptions("fp64", rel_tol=rel_tol, max_iters=max_iters).c()
+        js = _abi.J2Stats()
+        status = self._lib.pa_up_solve(self._h, ct.byref(up), ct.byref(jp), _ptr(z, np.float64, N, "z"), ct.byref(jo),
+                                       ct.byref(lo), _ptr(state, np.float64, 4 * N, "state"),
+                                       _ptr(local, np.float64, 14 * C, "local"), _ptr(ppg, np.float64, 3 * N, "ppg"),
+                                       ct.byref(js))
+        _abi.check(status, allow=(3,) if allow_not_converged else ())
+        return state, local, ppg, {"steps": js.steps, "newton_iterations": js.newton_iterations,
+                                   "minres_iterations": js.cg_iterations, "seconds": js.seconds,
+                                   "final_rel_residual": js.final_rel_residual, "converged": bool(js.converged),
+                                   "linear_unconverged": js.linear_unconverged,
+                                   "line_search_halvings": js.line_search_halvings}
 
     @staticmethod
     def _j2_params(params):

@@ -25,6 +25,9 @@ void launch_j2_local_residual(const Problem& P, const pa_j2_params& jp, const do
                               const double* loc, const double* prev, double* H, cudaStream_t s);
 pa_status j2_solve(Problem& P, const pa_j2_params& jp, const double* z, const pa_j2_solve_options& jo,
                    const pa_solve_options& lo, double* u, double* local, pa_j2_stats* js);
+pa_status up_solve(Problem& P, const pa_up_params& up, const pa_j2_params& jp, const double* z,
+                   const pa_j2_solve_options& jo, const pa_solve_options& lo, double* state, double* local,
+                   double* ppg, pa_j2_stats* js);
 
 namespace {
 thread_local std::string g_last_error;
@@ -792,6 +795,31 @@ pa_status pa_j2_solve(pa_problem* problem, const pa_j2_params* params, const dou
     double* du = st.out(u, P.ndof(), "u");
     double* dl = st.out(local, 14 * P.C(), "local");
     pa_status s = pa::j2_solve(P, *params, dz, *options, lo, du, dl, stats);
+    st.finish();
+    return s;
+  });
+}
+
+pa_status pa_up_solve(pa_problem* problem, const pa_up_params* up, const pa_j2_params* params, const double* z,
+                      const pa_j2_solve_options* options, const pa_solve_options* linear, double* state,
+                      double* local, double* ppg, pa_j2_stats* stats) {
+  return pa::guard_status([&] {
+    Problem& P = prob(problem);
+    PA_CHECK(up && params && options, "null u-p parameters or options");
+    PA_CHECK(up->youngs_modulus > 0 && up->poissons_ratio > -1.0 && up->poissons_ratio < 0.5,
+             "u-p moduli out of range");
+    PA_CHECK(params->youngs_modulus > 0 && params->initial_yield_stress > 0, "J2 moduli must be positive");
+    pa_solve_options lo;
+    pa_solve_options_default(&lo);
+    lo.rel_tol = 1e-12;
+    lo.max_iters = 0;
+    if (linear) lo = *linear;
+    pa::Stage st(P);
+    const double* dz = st.in(z, P.N(), "z");
+    double* ds = st.out(state, 4 * P.N(), "state");
+    double* dl = st.out(local, 14 * P.C(), "local");
+    double* dp = ppg ? st.out(ppg, 3 * P.N(), "projected pressure gradient") : nullptr;
+    pa_status s = pa::up_solve(P, *up, *params, dz, *options, lo, ds, dl, dp, stats);
     st.finish();
     return s;
   });

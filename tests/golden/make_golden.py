@@ -13,7 +13,9 @@ its unit tests are read as text and their gold arrays extracted:
   z = 1, u_i = 1e-4 (i+1).
 * unit_tests/PlasticityTests.cpp, J2PlasticityUtils_UpdatePlasticStep3D.
 * unit_tests/ElastoPlasticityTests.cpp, ElastoPlasticity_Residual3D_Elastic
-  (stabilized u-p residual on the single-hex box).
+  (stabilized u-p residual on the single-hex box) and
+  ElastoPlasticity_ElasticSolution3D (the u-p plasticity solve on the same
+  box: one pseudo-time step, x = 0 face fixed, u_y = -1e-3 on x = 1).
 
 The gold values depend on the vertex numbering of Omega_h's build_box, whose
 source is not available.  It is identified here by search rather than
@@ -244,6 +246,48 @@ def up_residual_3d():
     }
 
 
+def up_elastic_solution_3d(box):
+    """ElastoPlasticity_ElasticSolution3D (unit_tests/ElastoPlasticityTests.cpp:2101-2233):
+    PlasticityProblem::solution on the single-hex box of up_residual_3d (same
+    Omega_h build_box mesh), controls 1, one pseudo-time step; the state
+    (u_x, u_y, u_z, p per vertex) after the Newton solve, tolerance 1e-4."""
+    src = open(os.path.join(REF, "unit_tests/ElastoPlasticityTests.cpp")).read()
+    s = src.index("ElastoPlasticity_ElasticSolution3D")
+    e = src.index("TEUCHOS_UNIT_TEST", s)
+    body = src[s:e]
+
+    def param(name):
+        m = re.search(r"name='" + re.escape(name) + r"'\s+type='double'\s+value='([^']+)'", body)
+        return float(m.group(1))
+
+    i = body.index("tGold")
+    j = body.index("{", i)
+    k = body.index("};", j)
+    rows = re.findall(r"\{([^{}]*)\}", body[j + 1:k + 1])
+    gold = [float(t) for t in re.findall(r"[-+]?[0-9]*\.?[0-9]+(?:[eE][-+]?[0-9]+)?", rows[0])]
+    assert len(gold) == 32, len(gold)
+    assert "-0.001*t" in body and "Initial Num. Pseudo Time Steps' type='int' value='1'" in body
+    return {
+        "source": "unit_tests/ElastoPlasticityTests.cpp:2101-2233 (ElastoPlasticity_ElasticSolution3D)",
+        "mesh": box["mesh"],
+        "material": {"youngs_modulus": param("Youngs Modulus"), "poissons_ratio": param("Poissons Ratio"),
+                     "simp_exponent": param("Exponent"), "simp_min": param("Minimum Value"), "pressure_scaling": 1.0},
+        "j2": {"initial_yield_stress": param("Initial Yield Stress"),
+               "hardening_modulus_isotropic": param("Hardening Modulus Isotropic"),
+               "hardening_modulus_kinematic": param("Hardening Modulus Kinematic"),
+               "elastic_penalty_exponent": param("Elastic Properties Penalty Exponent"),
+               "elastic_min_ersatz": param("Elastic Properties Minimum Ersatz"),
+               "plastic_penalty_exponent": param("Plastic Properties Penalty Exponent"),
+               "plastic_min_ersatz": param("Plastic Properties Minimum Ersatz")},
+        "steps": 1,
+        "boundary": "x = 0 vertices: u_x = u_y = u_z = 0; x = 1 vertices: u_y = -0.001 t at t = 1",
+        "tolerance": 1e-4,
+        "cells": box["cells"],
+        "coords": box["coords"],
+        "gold": gold,
+    }
+
+
 def main():
     if not REF or not os.path.isdir(os.path.join(REF, "unit_tests")):
         sys.exit("usage: make_golden.py <platoanalyze source tree> (or set PA_REFERENCE)")
@@ -251,8 +295,11 @@ def main():
         json.dump(derivative_tests(), f, indent=1)
     with open(os.path.join(OUT, "j2_plastic_step_3d.json"), "w") as f:
         json.dump(j2_plastic_step(), f, indent=1)
+    box = up_residual_3d()
     with open(os.path.join(OUT, "up_residual_3d.json"), "w") as f:
-        json.dump(up_residual_3d(), f, indent=1)
+        json.dump(box, f, indent=1)
+    with open(os.path.join(OUT, "up_elastic_solution_3d.json"), "w") as f:
+        json.dump(up_elastic_solution_3d(box), f, indent=1)
     print("wrote fixtures to", OUT)
 
 
