@@ -419,6 +419,23 @@ pa_status pa_up_solve(pa_problem* problem, const pa_up_params* up, const pa_j2_p
                       const pa_j2_solve_options* options, const pa_solve_options* linear, double* state,
                       double* local, double* ppg, pa_j2_stats* stats);
 
+/* The "Elastic Work" criterion of the u-p plasticity problem and its
+ * gradient with respect to the nodal controls (PlasticityProblem::
+ * criterionValue / criterionGradient, src/PlasticityProblem.hpp:411-560, with
+ * ElasticWorkCriterion, src/ElasticWorkCriterion.hpp, and the path-dependent
+ * adjoint, src/PathDependentAdjointSolver.hpp:154-940).  Runs pa_up_solve
+ * (same arguments and outputs), then *value = sum over the steps of each
+ * step's elastic work V (sigma_n + sigma_{n-1}) . (e_n - e_{n-1}) / 2, with
+ * e = eps(u) - eps_p and sigma the isotropic stress of up's moduli penalized
+ * by the criterion's own SIMP (penalty_exponent, penalty_min), and gradient
+ * (N) = d value / d z through every step (local states, pressures and the
+ * lagged projection included).  The adjoint solves use MINRES like the
+ * forward ones; stats->cg_iterations counts both. */
+pa_status pa_up_elastic_work(pa_problem* problem, const pa_up_params* up, const pa_j2_params* params,
+                             double penalty_exponent, double penalty_min, const double* z,
+                             const pa_j2_solve_options* options, const pa_solve_options* linear, double* value,
+                             double* gradient, double* state, double* local, pa_j2_stats* stats);
+
 /* ------------------------------------------------------ batched solves --- */
 /* No counterpart in the reference (one Problem solves one mesh).  A parted
  * mesh is the disjoint union of independent sub-meshes: part p owns the nodes

@@ -206,6 +206,16 @@ class UpProblem:
             K[:, j] = (self.cell_residual(c, xp, prev_c, ppg_c)[0] - self.cell_residual(c, xm, prev_c, ppg_c)[0]) / (2 * h)
         return K
 
+    def elastic_work(self, pe=3.0, pe_min=1e-9):
+        """The "Elastic Work" criterion of the last solve: the steps' elastic
+        work summed (PlasticityProblem::evaluateCriterion,
+        src/PlasticityProblem.hpp:929-953)."""
+        total, ps, pl = 0.0, np.zeros(4 * self.N), np.zeros((self.C, 14))
+        for st, loc in self.history:
+            total += elastic_work(self.cells, self.coords, st, loc, ps, pl, self.z, self.E, self.nu, pe, pe_min)
+            ps, pl = st, loc
+        return total
+
     def tangent(self, x, prev, ppg):
         n = 4 * self.N
         K = np.zeros((n, n))
@@ -218,12 +228,14 @@ class UpProblem:
         """bc_dofs in the 4-dof numbering (4 node + component).  Returns the
         state (4N), the local states (C x 14) and the projected pressure
         gradient of the last step (N x 3); self.converged tells whether every
-        step met tol (||R_free|| <= tol max(1, ||R||))."""
+        step met tol (||R_free|| <= tol max(1, ||R||)); self.history holds
+        every step's state and local states."""
         x = np.zeros(4 * self.N)
         prev = np.zeros((self.C, 14))
         ppg = np.zeros((self.N, 3))
         free = np.setdiff1d(np.arange(4 * self.N), bc_dofs)
         self.converged = True
+        self.history = []  # (state, local states) after every step
         for k in range(steps):
             x[bc_dofs] = np.asarray(bc_final) * (k + 1) / steps
             ok = False
@@ -246,6 +258,33 @@ class UpProblem:
             self.converged = self.converged and ok
             R, cur = self.residual(x, prev, ppg)
             prev = cur
+            self.history.append((x.copy(), cur.copy()))
             if k + 1 < steps:
                 ppg = project_pressure_gradient(self.cells, self.coords, x, self.z, self.pe, self.pe_min, self.ps)
         return x, prev, ppg
+
+
+def elastic_work(cells, coords, state, local, prev_state, prev_local, z, E, nu, pe=3.0, pe_min=1e-9):
+    """One step's elastic work, ElasticWorkCriterion::evaluate
+    (src/ElasticWorkCriterion.hpp): per cell V (sigma_n + sigma_{n-1}) / 2 .
+    (e_n - e_{n-1}) with e = eps(u) - eps_p and sigma the penalized isotropic
+    Cauchy stress of e (shear strains engineering, so sigma . e counts them
+    once).  PlasticityProblem::evaluateCriterion sums it over the steps."""
+    mu, kappa = moduli(E, nu)
+    total = 0.0
+    for c, v in enumerate(np.asarray(cells)):
+        g, vol = cell_gradients(coords[v])
+        pen = pe_min + (1.0 - pe_min) * np.mean(np.asarray(z)[v]) ** pe
+        es = []
+        for st, loc in ((state, local), (prev_state, prev_local)):
+            u = np.asarray(st).reshape(-1, 4)[v, :3]
+            du = g.T @ u
+            eps = np.array([du[0, 0], du[1, 1], du[2, 2], du[1, 2] + du[2, 1], du[0, 2] + du[2, 0],
+                            du[0, 1] + du[1, 0]])
+            es.append(eps - np.asarray(loc)[c, 2:8])
+        sig = []
+        for e in es:
+            tr = e[:3].sum()
+            sig.append(pen * np.concatenate([kappa * tr + 2 * mu * (e[:3] - tr / 3.0), mu * e[3:]]))
+        total += vol * 0.5 * (sig[0] + sig[1]) @ (es[0] - es[1])
+    return total

@@ -120,6 +120,8 @@ SIGNATURES = [
     ("pa_up_residual", I32, [P, ct.POINTER(UpParams), P, P, P, I32, P, P, I32]),
     ("pa_up_solve", I32, [P, ct.POINTER(UpParams), ct.POINTER(J2Params), P, ct.POINTER(J2SolveOptions),
                           ct.POINTER(SolveOptions), P, P, P, ct.POINTER(J2Stats)]),
+    ("pa_up_elastic_work", I32, [P, ct.POINTER(UpParams), ct.POINTER(J2Params), F64, F64, P, ct.POINTER(J2SolveOptions),
+                                 ct.POINTER(SolveOptions), ct.POINTER(F64), P, P, P, ct.POINTER(J2Stats)]),
     ("pa_mesh_set_parts", I32, [P, I32, P]),
     ("pa_mesh_uniform_geometry", I32, [P, I32, P]),
     ("pa_mesh_box_kernels", I32, [P, I32, P]),

@@ -388,6 +388,32 @@ class Problem:
                                    "linear_unconverged": js.linear_unconverged,
                                    "line_search_halvings": js.line_search_halvings}
 
+    def up_elastic_work(self, up_params, j2_params, z, steps=1, max_newton=20, newton_tol=1e-10, rel_tol=1e-12,
+                        max_iters=0, penalty_exponent=3.0, penalty_min=1e-9, gradient=None, state=None, local=None):
+        """"Elastic Work" of the u-p plasticity problem summed over the load
+        steps and its gradient with respect to the nodal controls by the
+        path-dependent adjoint (pa_up_elastic_work).  Returns (value,
+        gradient, state, local states, statistics)."""
+        C, N = self.mesh.num_cells, self.mesh.num_nodes
+        z = _as(z, np.float64)
+        gradient = _empty(z, N) if gradient is None else gradient
+        state = _empty(z, 4 * N) if state is None else state
+        local = _empty(z, 14 * C) if local is None else local
+        up = self._up_params(up_params)
+        jp = self._j2_params(j2_params)
+        jo = _abi.J2SolveOptions(int(steps), int(max_newton), float(newton_tol), 0)
+        lo = SolveOptions("fp64", rel_tol=rel_tol, max_iters=max_iters).c()
+        js = _abi.J2Stats()
+        value = ct.c_double()
+        _abi.check(self._lib.pa_up_elastic_work(self._h, ct.byref(up), ct.byref(jp), float(penalty_exponent),
+                                                float(penalty_min), _ptr(z, np.float64, N, "z"), ct.byref(jo),
+                                                ct.byref(lo), ct.byref(value), _ptr(gradient, np.float64, N, "gradient"),
+                                                _ptr(state, np.float64, 4 * N, "state"),
+                                                _ptr(local, np.float64, 14 * C, "local"), ct.byref(js)))
+        return value.value, gradient, state, local, {"newton_iterations": js.newton_iterations,
+                                                     "minres_iterations": js.cg_iterations, "seconds": js.seconds,
+                                                     "converged": bool(js.converged)}
+
     @staticmethod
     def _j2_params(params):
         return _abi.J2Params(*[float(params[k]) for k in (

@@ -28,6 +28,9 @@ pa_status j2_solve(Problem& P, const pa_j2_params& jp, const double* z, const pa
 pa_status up_solve(Problem& P, const pa_up_params& up, const pa_j2_params& jp, const double* z,
                    const pa_j2_solve_options& jo, const pa_solve_options& lo, double* state, double* local,
                    double* ppg, pa_j2_stats* js);
+pa_status up_elastic_work(Problem& P, const pa_up_params& up, const pa_j2_params& jp, double fpe, double fpmin,
+                          const double* z, const pa_j2_solve_options& jo, const pa_solve_options& lo, double* value,
+                          double* grad, double* state, double* local, pa_j2_stats* js);
 
 namespace {
 thread_local std::string g_last_error;
@@ -820,6 +823,33 @@ pa_status pa_up_solve(pa_problem* problem, const pa_up_params* up, const pa_j2_p
     double* dl = st.out(local, 14 * P.C(), "local");
     double* dp = ppg ? st.out(ppg, 3 * P.N(), "projected pressure gradient") : nullptr;
     pa_status s = pa::up_solve(P, *up, *params, dz, *options, lo, ds, dl, dp, stats);
+    st.finish();
+    return s;
+  });
+}
+
+pa_status pa_up_elastic_work(pa_problem* problem, const pa_up_params* up, const pa_j2_params* params,
+                             double penalty_exponent, double penalty_min, const double* z,
+                             const pa_j2_solve_options* options, const pa_solve_options* linear, double* value,
+                             double* gradient, double* state, double* local, pa_j2_stats* stats) {
+  return pa::guard_status([&] {
+    Problem& P = prob(problem);
+    PA_CHECK(up && params && options && value, "null u-p parameters, options or value");
+    PA_CHECK(up->youngs_modulus > 0 && up->poissons_ratio > -1.0 && up->poissons_ratio < 0.5,
+             "u-p moduli out of range");
+    PA_CHECK(params->youngs_modulus > 0 && params->initial_yield_stress > 0, "J2 moduli must be positive");
+    pa_solve_options lo;
+    pa_solve_options_default(&lo);
+    lo.rel_tol = 1e-12;
+    lo.max_iters = 0;
+    if (linear) lo = *linear;
+    pa::Stage st(P);
+    const double* dz = st.in(z, P.N(), "z");
+    double* dg = st.out(gradient, P.N(), "gradient");
+    double* ds = st.out(state, 4 * P.N(), "state");
+    double* dl = st.out(local, 14 * P.C(), "local");
+    pa_status s = pa::up_elastic_work(P, *up, *params, penalty_exponent, penalty_min, dz, *options, lo, value, dg, ds,
+                                      dl, stats);
     st.finish();
     return s;
   });

@@ -167,9 +167,9 @@ __global__ void __launch_bounds__(kUpT) k_up_cells(const int32_t* __restrict__ c
   }
 }
 
-// R[4n + i] = sum over the cells around node n of their entry (vertex, i)
+// R[4n + i] (+)= sum over the cells around node n of their entry (vertex, i)
 __global__ void k_up_gather(int64_t N, const int32_t* __restrict__ ptr, const int64_t* __restrict__ adj, int64_t C,
-                            const double* __restrict__ rc, double* __restrict__ R) {
+                            const double* __restrict__ rc, double* __restrict__ R, int accumulate = 0) {
   const int64_t n = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (n >= N) return;
   double r[4] = {0.0, 0.0, 0.0, 0.0};
@@ -180,7 +180,7 @@ __global__ void k_up_gather(int64_t N, const int32_t* __restrict__ ptr, const in
     for (int i = 0; i < 4; ++i) r[i] += rc[(4 * a + i) * C + c];
   }
 #pragma unroll
-  for (int i = 0; i < 4; ++i) R[4 * n + i] = r[i];
+  for (int i = 0; i < 4; ++i) R[4 * n + i] = (accumulate ? R[4 * n + i] : 0.0) + r[i];
 }
 
 __device__ __forceinline__ bool up_masked(const uint8_t* mask, int64_t node, int comp) {
@@ -329,6 +329,386 @@ __global__ void k_up_set(int64_t m, const int32_t* __restrict__ dofs, const doub
   if (i < m) x[dofs[i]] = scale * vals[i];
 }
 
+// ---------------------------------------------------------------- adjoint --
+// Forward-mode number with one direction, for the pullbacks through the
+// return mapping (one pass per input direction).
+struct D1 {
+  double v, d;
+};
+__device__ __forceinline__ D1 operator+(D1 a, D1 b) { return {a.v + b.v, a.d + b.d}; }
+__device__ __forceinline__ D1 operator-(D1 a, D1 b) { return {a.v - b.v, a.d - b.d}; }
+__device__ __forceinline__ D1 operator*(D1 a, D1 b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
+__device__ __forceinline__ D1 operator*(double a, D1 b) { return {a * b.v, a * b.d}; }
+__device__ __forceinline__ D1 operator/(D1 a, D1 b) { return {a.v / b.v, (a.d * b.v - a.v * b.d) / (b.v * b.v)}; }
+__device__ __forceinline__ double val(D1 a) { return a.v; }
+__device__ __forceinline__ D1 sqrt_t(D1 a) {
+  const double r = sqrt(a.v);
+  return {r, r > 0.0 ? a.d / (2.0 * r) : 0.0};
+}
+__device__ __forceinline__ D1 simp_t(D1 rho, double p, double pmin) {
+  return {pmin + (1.0 - pmin) * pow(rho.v, p), (1.0 - pmin) * p * pow(rho.v, p - 1.0) * rho.d};
+}
+__device__ __forceinline__ double dsimp(double rho, double p, double pmin) {
+  return (1.0 - pmin) * p * pow(rho, p - 1.0);
+}
+
+// The J2 return mapping c_n = Phi(eps, c_{n-1}, rho) of j2_cell (the local
+// state update only) on forward-mode numbers.
+template <typename T>
+__device__ void j2_phi(const J2Dev& p, T rho, const T e[6], const T prev[kLocal], T cur[kLocal]) {
+  const T pe = simp_t(rho, p.pe, p.pe_min);
+  const T mu_p = p.mu * pe;
+  const T ppen = simp_t(rho, p.pp, p.pp_min);
+  const T hi = p.hiso * ppen, hk = p.hkin * ppen;
+#pragma unroll
+  for (int i = 0; i < kLocal; ++i) cur[i] = prev[i];
+  T ee[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) ee[i] = e[i] - prev[2 + i];
+  const T tr3 = (1.0 / 3.0) * (ee[0] + ee[1] + ee[2]);
+  T n[6];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) n[i] = 2.0 * mu_p * (ee[i] - tr3) - prev[8 + i];
+#pragma unroll
+  for (int i = 3; i < 6; ++i) n[i] = mu_p * ee[i] - prev[8 + i];
+  const T norm = sqrt_t(n[0] * n[0] + n[1] * n[1] + n[2] * n[2] + 2.0 * (n[3] * n[3] + n[4] * n[4] + n[5] * n[5]));
+  const double s32 = 1.2247448713915890491, s23 = 0.81649658092772603273;
+  const T sy = p.sy0 * ppen + hi * prev[0];
+  const T ftr = s32 * norm - sy;
+  cur[1] = 0.0 * prev[1];
+  if (val(ftr) > 1.0e-10) {
+    const T dg = ftr / (3.0 * mu_p + hi + hk);
+    cur[1] = dg;
+    cur[0] = prev[0] + dg;
+    const T m1 = s32 * dg / norm, m2 = s23 * dg * hk / norm;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) cur[2 + i] = prev[2 + i] + m1 * n[i];
+#pragma unroll
+    for (int i = 3; i < 6; ++i) cur[2 + i] = prev[2 + i] + 2.0 * m1 * n[i];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) cur[8 + i] = prev[8 + i] + m2 * n[i];
+  }
+}
+
+struct UpCell {
+  int v[4];
+  double g[4][3], vol, rho, eps[6];
+};
+
+__device__ __forceinline__ void up_cell_load(const int32_t* cells, const double* coords, const double* x,
+                                             const double* z, int64_t c, UpCell& k) {
+  const int4 qv = reinterpret_cast<const int4*>(cells)[c];
+  k.v[0] = qv.x;
+  k.v[1] = qv.y;
+  k.v[2] = qv.z;
+  k.v[3] = qv.w;
+  double xc[4][3], ue[12];
+  k.rho = 0.0;
+#pragma unroll
+  for (int n = 0; n < 4; ++n) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      xc[n][d] = coords[3 * int64_t(k.v[n]) + d];
+      ue[3 * n + d] = x[4 * int64_t(k.v[n]) + d];
+    }
+    k.rho += 0.25 * z[k.v[n]];
+  }
+  tet_geometry(xc, k.g, k.vol);
+  tet_strain(k.g, ue, k.eps);
+}
+
+// xc (16 per cell, component-major) = B^T t on the displacement entries, 0 on the pressures
+__device__ __forceinline__ void up_store_bt(const UpCell& k, const double t[6], double scale, int64_t C, int64_t c,
+                                            double* xc) {
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      double b[6];
+      bcol(k.g[a], i, b);
+      xc[(4 * a + i) * C + c] =
+          scale * (b[0] * t[0] + b[1] * t[1] + b[2] * t[2] + b[3] * t[3] + b[4] * t[4] + b[5] * t[5]);
+    }
+    xc[(4 * a + 3) * C + c] = 0.0;
+  }
+}
+
+// The criterion at the last step: f_c = V sigma . e / 2 (the steps' elastic
+// work summed telescopes to the final stored energy), its value per cell,
+// and its partials: x (per cell), c_S (cbar) and rho (rbar, written).
+__global__ void k_upa_final(const int32_t* __restrict__ cells, const double* __restrict__ coords, int64_t C, UpDev q,
+                            double fpe, double fpmin, const double* __restrict__ x, const double* __restrict__ loc,
+                            const double* __restrict__ z, double* __restrict__ fcell, double* __restrict__ xc,
+                            double* __restrict__ cbar, double* __restrict__ rbar) {
+  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (c >= C) return;
+  UpCell k;
+  up_cell_load(cells, coords, x, z, c, k);
+  double e[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) e[i] = k.eps[i] - loc[kLocal * c + 2 + i];
+  const double pen = simp(k.rho, fpe, fpmin);
+  const double tr = e[0] + e[1] + e[2];
+  double sg[6];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) sg[i] = pen * (q.kappa * tr + 2.0 * q.mu * (e[i] - tr / 3.0));
+#pragma unroll
+  for (int i = 3; i < 6; ++i) sg[i] = pen * q.mu * e[i];
+  double se = 0.0;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) se += sg[i] * e[i];
+  const double f = 0.5 * k.vol * se;
+  fcell[c] = f;
+  up_store_bt(k, sg, k.vol, C, c, xc);
+#pragma unroll
+  for (int i = 0; i < kLocal; ++i) cbar[kLocal * c + i] = (i >= 2 && i < 8) ? -k.vol * sg[i - 2] : 0.0;
+  rbar[c] = f * dsimp(k.rho, fpe, fpmin) / pen;
+}
+
+// Pullback of cbar (the cotangent of c_n) through c_n = Phi(eps(x_n), c_{n-1}, rho)
+// onto eps: xc (per cell) = B^T (dPhi/deps)^T cbar.
+__global__ void k_upa_phi_eps(const int32_t* __restrict__ cells, const double* __restrict__ coords, int64_t C,
+                              J2Dev jd, const double* __restrict__ x, const double* __restrict__ prev,
+                              const double* __restrict__ z, const double* __restrict__ cbar, double* __restrict__ xc) {
+  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (c >= C) return;
+  UpCell k;
+  up_cell_load(cells, coords, x, z, c, k);
+  double cb[kLocal];
+  bool any = false;
+#pragma unroll
+  for (int i = 0; i < kLocal; ++i) {
+    cb[i] = cbar[kLocal * c + i];
+    any = any || cb[i] != 0.0;
+  }
+  double eb[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  if (any) {
+    D1 pv[kLocal], cur[kLocal];
+#pragma unroll
+    for (int i = 0; i < kLocal; ++i) pv[i] = D1{prev[kLocal * c + i], 0.0};
+    const D1 rho{k.rho, 0.0};
+#pragma unroll 1
+    for (int dir = 0; dir < 6; ++dir) {
+      D1 e[6];
+#pragma unroll
+      for (int i = 0; i < 6; ++i) e[i] = D1{k.eps[i], i == dir ? 1.0 : 0.0};
+      j2_phi(jd, rho, e, pv, cur);
+      double acc = 0.0;
+#pragma unroll
+      for (int i = 0; i < kLocal; ++i) acc += cb[i] * cur[i].d;
+      eb[dir] = acc;
+    }
+  }
+  up_store_bt(k, eb, 1.0, C, c, xc);
+}
+
+// Pullbacks of step n given its adjoint lam (lam^T R_n): the cotangent of
+// c_n seen by R (through eps_p) plus cbar_n, pulled back through Phi onto
+// c_{n-1} (cprev, written) and rho; R's explicit dependence on rho (rbar,
+// accumulated); and the cotangent of the projected pressure gradient, the same
+// 3-vector for every vertex of the cell (pib, component-major 3 per cell).
+__global__ void k_upa_resid(const int32_t* __restrict__ cells, const double* __restrict__ coords, int64_t C, UpDev q,
+                            J2Dev jd, const double* __restrict__ x, const double* __restrict__ prev,
+                            const double* __restrict__ cur_loc, const double* __restrict__ pi,
+                            const double* __restrict__ z, const double* __restrict__ lam,
+                            const double* __restrict__ cbar, double* __restrict__ cprev, double* __restrict__ rbar,
+                            double* __restrict__ pib) {
+  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (c >= C) return;
+  UpCell k;
+  up_cell_load(cells, coords, x, z, c, k);
+  double lu[12], lp[4], p[4], pic[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      lu[3 * a + i] = lam[4 * int64_t(k.v[a]) + i];
+      pic[i] += 0.25 * pi[3 * int64_t(k.v[a]) + i];
+    }
+    lp[a] = lam[4 * int64_t(k.v[a]) + 3];
+    p[a] = x[4 * int64_t(k.v[a]) + 3];
+  }
+  double el[6];
+  tet_strain(k.g, lu, el);  // engineering strain of lam's displacement part
+  const double pen = simp(k.rho, q.pe, q.pe_min);
+  const double mu_g = pen * q.mu;
+  // cotangent of c_n: cbar + (dR/d eps_p)^T lam = cbar - V D_dev eps(lam_u)
+  double cb[kLocal];
+#pragma unroll
+  for (int i = 0; i < kLocal; ++i) cb[i] = cbar[kLocal * c + i];
+  {
+    const double tl = (el[0] + el[1] + el[2]) / 3.0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) cb[2 + i] -= k.vol * 2.0 * mu_g * (el[i] - tl);
+#pragma unroll
+    for (int i = 3; i < 6; ++i) cb[2 + i] -= k.vol * mu_g * el[i];
+  }
+  // pull back through Phi onto c_{n-1} (entry 1 is not read by Phi) and rho
+  double cp[kLocal], rb = 0.0;
+  {
+    D1 e[6], pv[kLocal], cur[kLocal];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) e[i] = D1{k.eps[i], 0.0};
+#pragma unroll 1
+    for (int dir = 0; dir <= kLocal; ++dir) {  // dir < 14: c_{n-1} entry; dir == 14: rho
+#pragma unroll
+      for (int i = 0; i < kLocal; ++i) pv[i] = D1{prev[kLocal * c + i], i == dir ? 1.0 : 0.0};
+      const D1 rho{k.rho, dir == kLocal ? 1.0 : 0.0};
+      double acc = 0.0;
+      if (dir != 1) {
+        j2_phi(jd, rho, e, pv, cur);
+#pragma unroll
+        for (int i = 0; i < kLocal; ++i) acc += cb[i] * cur[i].d;
+      }
+      if (dir < kLocal)
+        cp[dir] = acc;
+      else
+        rb = acc;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < kLocal; ++i) cprev[kLocal * c + i] = cp[i];
+  // R's explicit dependence on the penalty of the u-p residual
+  double e[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) e[i] = k.eps[i] - cur_loc[kLocal * c + 2 + i];
+  const double tr3 = (e[0] + e[1] + e[2]) / 3.0;
+  const double s1[6] = {2.0 * q.mu * (e[0] - tr3), 2.0 * q.mu * (e[1] - tr3), 2.0 * q.mu * (e[2] - tr3),
+                        q.mu * e[3], q.mu * e[4], q.mu * e[5]};
+  double gp[3] = {0.0, 0.0, 0.0}, gl[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      gp[d] += p[a] * k.g[a][d];
+      gl[d] += lp[a] * k.g[a][d];
+    }
+  const double ps = q.ps;
+  const double pc = ps * 0.25 * (p[0] + p[1] + p[2] + p[3]);
+  const double cv = cbrt(k.vol);
+  const double tau = cv * cv / (2.0 * q.mu);
+  double dR = 0.0;  // lam . dR/dpen
+#pragma unroll
+  for (int i = 0; i < 6; ++i) dR += k.vol * s1[i] * el[i];
+  double st1l = 0.0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) st1l += ps * tau * (ps * gp[d] - pic[d]) * gl[d];
+  dR += -k.vol * st1l + k.vol * 0.25 * ps * pc / (pen * pen * q.kappa) * (lp[0] + lp[1] + lp[2] + lp[3]);
+  rbar[c] += rb + dR * dsimp(k.rho, q.pe, q.pe_min);
+  // projected pressure gradient: dR_p,a / dPi_b = V pen ps tau grad N_a / 4
+#pragma unroll
+  for (int d = 0; d < 3; ++d) pib[d * C + c] = 0.25 * k.vol * pen * ps * tau * gl[d];
+}
+
+// nodal sums of a 3-per-cell quantity (component-major) over the cells around each node
+__global__ void k_upa_gather3(int64_t N, const int32_t* __restrict__ ptr, const int64_t* __restrict__ adj, int64_t C,
+                              const double* __restrict__ v3, double* __restrict__ out) {
+  const int64_t n = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (n >= N) return;
+  double r[3] = {0.0, 0.0, 0.0};
+  for (int32_t e = ptr[n]; e < ptr[n + 1]; ++e) {
+    const int64_t c = adj[e] >> 2;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) r[d] += v3[d * C + c];
+  }
+#pragma unroll
+  for (int d = 0; d < 3; ++d) out[3 * n + d] = r[d];
+}
+
+// W_a = sum over the cells around node a of pen_c V_c (the projection's row sums)
+__global__ void k_upa_weights(int64_t N, const int32_t* __restrict__ ptr, const int64_t* __restrict__ adj,
+                              const int32_t* __restrict__ cells, const double* __restrict__ coords, UpDev q,
+                              const double* __restrict__ z, double* __restrict__ W) {
+  const int64_t n = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (n >= N) return;
+  double w = 0.0;
+  for (int32_t e = ptr[n]; e < ptr[n + 1]; ++e) {
+    const int64_t c = adj[e] >> 2;
+    const int4 qv = reinterpret_cast<const int4*>(cells)[c];
+    const int v[4] = {qv.x, qv.y, qv.z, qv.w};
+    double x[4][3], g[4][3], vol, rho = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) x[k][d] = coords[3 * int64_t(v[k]) + d];
+      rho += 0.25 * z[v[k]];
+    }
+    tet_geometry(x, g, vol);
+    w += simp(rho, q.pe, q.pe_min) * vol;
+  }
+  W[n] = w;
+}
+
+// Pullback of the projection Pi_n = Q(p_{n-1}, z) (Pi_a = ps sum_c w_c grad p_c
+// / W_a, w_c = pen_c V_c) given its cotangent pib (3N): onto the pressures of
+// x_{n-1} (xc, per cell) and rho (rbar, accumulated).
+__global__ void k_upa_proj(const int32_t* __restrict__ cells, const double* __restrict__ coords, int64_t C, UpDev q,
+                           const double* __restrict__ x, const double* __restrict__ z, const double* __restrict__ pi,
+                           const double* __restrict__ W, const double* __restrict__ pib, double* __restrict__ xc,
+                           double* __restrict__ rbar) {
+  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (c >= C) return;
+  UpCell k;
+  up_cell_load(cells, coords, x, z, c, k);
+  double gp[3] = {0.0, 0.0, 0.0}, S[3] = {0.0, 0.0, 0.0}, rr = 0.0;
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const double pa = x[4 * int64_t(k.v[a]) + 3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) gp[d] += pa * k.g[a][d];
+  }
+  const double ps = q.ps, pen = simp(k.rho, q.pe, q.pe_min), w = pen * k.vol;
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const double iw = 1.0 / W[k.v[a]];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double pb = pib[3 * int64_t(k.v[a]) + d];
+      S[d] += pb * iw;
+      rr += pb * (ps * gp[d] - pi[3 * int64_t(k.v[a]) + d]) * iw;
+    }
+  }
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) xc[(4 * b + i) * C + c] = 0.0;
+    xc[(4 * b + 3) * C + c] = ps * w * (k.g[b][0] * S[0] + k.g[b][1] * S[1] + k.g[b][2] * S[2]);
+  }
+  rbar[c] += rr * dsimp(k.rho, q.pe, q.pe_min) * k.vol;
+}
+
+// gradient of the criterion with respect to the nodal controls: rho_c is the
+// mean of its four nodes' controls
+__global__ void k_upa_nodal(int64_t N, const int32_t* __restrict__ ptr, const int64_t* __restrict__ adj,
+                            const double* __restrict__ rbar, double* __restrict__ grad) {
+  const int64_t n = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (n >= N) return;
+  double g = 0.0;
+  for (int32_t e = ptr[n]; e < ptr[n + 1]; ++e) g += 0.25 * rbar[adj[e] >> 2];
+  grad[n] = g;
+}
+
+// b = masked ? 0 : -xbar
+__global__ void k_upa_rhs(int64_t n, const uint8_t* __restrict__ mask, const double* __restrict__ xbar,
+                          double* __restrict__ b) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    b[i] = up_masked(mask, i >> 2, int(i & 3)) ? 0.0 : -xbar[i];
+}
+
+__global__ void k_upa_sum(int64_t n, const double* __restrict__ a, double* __restrict__ partials) {
+  __shared__ double red[256];
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    s += a[i];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partials[blockIdx.x] = red[0];
+}
+
 int blocks_of(int64_t n, int t) { return int(std::max<int64_t>(1, (n + t - 1) / t)); }
 int grid_stride(int64_t n) { return int(std::min<int64_t>(std::max<int64_t>(1, (n + 255) / 256), 148 * 8)); }
 
@@ -473,12 +853,17 @@ struct UpSolver {
 
 }  // namespace
 
-pa_status up_solve(Problem& P, const pa_up_params& up, const pa_j2_params& jp, const double* z,
-                   const pa_j2_solve_options& jo, const pa_solve_options& lo, double* state, double* local,
-                   double* ppg_out, pa_j2_stats* js) {
-  PA_CHECK(jo.steps > 0 && jo.max_newton > 0 && jo.newton_tol > 0, "u-p solve options out of range");
-  PA_CHECK(P.C() < (int64_t(1) << 29) && 4 * P.C() < (int64_t(1) << 31), "u-p solve: mesh too large");
-  UpSolver U(P, up, jp, z);
+// Per-step states kept by the forward solve for the adjoint: state x_n (4N),
+// local states c_n (C x 14) and the projected pressure gradient used in step
+// n (3N), n = 0 .. steps-1.
+struct UpHistory {
+  std::vector<DevBuf<double>> x, c, pi;
+};
+
+pa_status up_forward(UpSolver& U, const pa_j2_solve_options& jo, const pa_solve_options& lo, double* state,
+                     double* local, UpHistory* hist, pa_j2_stats* js) {
+  Problem& P = U.P;
+  const double* z = U.z;
   cudaStream_t s = U.s;
   const int64_t n = U.n, C = U.C;
   PA_CUDA(cudaMemsetAsync(state, 0, sizeof(double) * n, s));
@@ -558,14 +943,24 @@ pa_status up_solve(Problem& P, const pa_up_params& up, const pa_j2_params& jp, c
     // the local states of the accepted iterate, then the next step's projection
     U.residual(state, local);
     PA_CUDA(cudaMemcpyAsync(U.prev.get(), local, sizeof(double) * kLocal * C, cudaMemcpyDeviceToDevice, s));
+    if (hist) {
+      hist->x.emplace_back();
+      hist->c.emplace_back();
+      hist->pi.emplace_back();
+      hist->x.back().resize(n);
+      hist->c.back().resize(kLocal * C);
+      hist->pi.back().resize(3 * U.N);
+      PA_CUDA(cudaMemcpyAsync(hist->x.back().get(), state, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+      PA_CUDA(cudaMemcpyAsync(hist->c.back().get(), local, sizeof(double) * kLocal * C, cudaMemcpyDeviceToDevice, s));
+      PA_CUDA(cudaMemcpyAsync(hist->pi.back().get(), U.ppg.get(), sizeof(double) * 3 * U.N, cudaMemcpyDeviceToDevice,
+                              s));
+    }
     if (step + 1 < jo.steps) {
       k_up_project<<<blocks_of(U.N, 128), 128, 0, s>>>(U.N, U.ptr.get(), U.adj.get(), P.mesh->d_cells.get(),
                                                       P.mesh->d_coords.get(), U.q, state, z, U.ppg.get());
       PA_LAUNCHED();
     }
   }
-  if (ppg_out)
-    PA_CUDA(cudaMemcpyAsync(ppg_out, U.ppg.get(), sizeof(double) * 3 * U.N, cudaMemcpyDeviceToDevice, s));
   PA_CUDA(cudaEventRecord(t1, s));
   PA_CUDA(cudaEventSynchronize(t1));
   float ms = 0.f;
@@ -584,6 +979,108 @@ pa_status up_solve(Problem& P, const pa_up_params& up, const pa_j2_params& jp, c
   }
   if (status != PA_OK) return status;
   return all_converged ? PA_OK : PA_ERR_NOT_CONVERGED;
+}
+
+pa_status up_solve(Problem& P, const pa_up_params& up, const pa_j2_params& jp, const double* z,
+                   const pa_j2_solve_options& jo, const pa_solve_options& lo, double* state, double* local,
+                   double* ppg_out, pa_j2_stats* js) {
+  PA_CHECK(jo.steps > 0 && jo.max_newton > 0 && jo.newton_tol > 0, "u-p solve options out of range");
+  PA_CHECK(P.C() < (int64_t(1) << 29) && 4 * P.C() < (int64_t(1) << 31), "u-p solve: mesh too large");
+  UpSolver U(P, up, jp, z);
+  const pa_status st = up_forward(U, jo, lo, state, local, nullptr, js);
+  if (ppg_out)
+    PA_CUDA(cudaMemcpyAsync(ppg_out, U.ppg.get(), sizeof(double) * 3 * U.N, cudaMemcpyDeviceToDevice, U.s));
+  PA_CUDA(cudaStreamSynchronize(U.s));
+  return st;
+}
+
+// "Elastic Work" (ElasticWorkCriterion summed over the load steps by
+// PlasticityProblem::evaluateCriterion, src/PlasticityProblem.hpp:929-953)
+// and its gradient with respect to the nodal controls by the path-dependent
+// adjoint (PathDependentAdjointSolver, src/PathDependentAdjointSolver.hpp:
+// 154-940).  The steps' elastic work V (sigma_n + sigma_{n-1}) . (e_n -
+// e_{n-1}) / 2 telescopes (sigma = C e, C symmetric) to the last step's
+// stored energy V e_S . C e_S / 2.  The reverse sweep runs the steps
+// backwards with the cotangents of x_n (xbar) and c_n (cbar):
+//   c_n = Phi(eps(x_n), c_{n-1}, rho): xbar_n += B^T dPhi/deps^T cbar_n;
+//   x_n solves R(x_n, Phi(..), Pi_n, rho) = 0: K_n lam_n = -xbar_n (free
+//     dofs; K_n the condensed tangent, symmetric), then cbar_{n-1} =
+//     dPhi/dc_{n-1}^T (cbar_n + dR/dc_n^T lam_n), rhobar += the rho parts,
+//     Pibar_n = dR/dPi^T lam_n;
+//   Pi_n = Q(p_{n-1}, rho) (n > 0): xbar_{n-1} = dQ/dp^T Pibar_n, rhobar +=.
+// The reference solves the same reverse recurrence with the local adjoint
+// kept as an unknown (its local residual H is zero at the returned state, so
+// eliminating it through Phi gives the same gradient).
+pa_status up_elastic_work(Problem& P, const pa_up_params& up, const pa_j2_params& jp, double fpe, double fpmin,
+                          const double* z, const pa_j2_solve_options& jo, const pa_solve_options& lo, double* value,
+                          double* grad, double* state, double* local, pa_j2_stats* js) {
+  PA_CHECK(jo.steps > 0 && jo.max_newton > 0 && jo.newton_tol > 0, "u-p solve options out of range");
+  PA_CHECK(P.C() < (int64_t(1) << 29) && 4 * P.C() < (int64_t(1) << 31), "u-p solve: mesh too large");
+  PA_CHECK(fpmin >= 0.0 && fpmin < 1.0, "criterion penalty minimum out of range");
+  UpSolver U(P, up, jp, z);
+  UpHistory H;
+  const pa_status fst = up_forward(U, jo, lo, state, local, &H, js);
+  if (fst != PA_OK) return fst;
+  cudaStream_t s = U.s;
+  const int64_t N = U.N, C = U.C, n = U.n;
+  const int S = int(H.x.size());
+  const double lin_tol = lo.rel_tol > 0 ? lo.rel_tol : 1e-12;
+  const int64_t lin_max = lo.max_iters > 0 ? lo.max_iters : 100000;
+  const int32_t* cells = P.mesh->d_cells.get();
+  const double* coords = P.mesh->d_coords.get();
+  DevBuf<double> fcell(C), xc(16 * C), xbar(n), cb_cur(kLocal * C), cb_prev(kLocal * C), rbar(C), pib(3 * C),
+      pibn(3 * N), W(N), zeros(kLocal * C), scratch(kLocal * C);
+  PA_CUDA(cudaMemsetAsync(zeros.get(), 0, sizeof(double) * kLocal * C, s));
+  const int cb = blocks_of(C, kUpT), nb = blocks_of(N, 128);
+  // the criterion at the last step and its partials
+  k_upa_final<<<cb, kUpT, 0, s>>>(cells, coords, C, U.q, fpe, fpmin, H.x[S - 1].get(), H.c[S - 1].get(), z,
+                                  fcell.get(), xc.get(), cb_cur.get(), rbar.get());
+  k_upa_sum<<<kRedBlocks, 256, 0, s>>>(C, fcell.get(), U.partials.get());
+  k_up_sum<<<1, 256, 0, s>>>(kRedBlocks, U.partials.get(), U.scal.get());
+  k_up_gather<<<nb, 128, 0, s>>>(N, U.ptr.get(), U.adj.get(), C, xc.get(), xbar.get(), 0);
+  PA_LAUNCHED();
+  PA_CUDA(cudaMemcpyAsync(value, U.scal.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
+  k_upa_weights<<<nb, 128, 0, s>>>(N, U.ptr.get(), U.adj.get(), cells, coords, U.q, z, W.get());
+  PA_LAUNCHED();
+  int64_t lin_total = 0;
+  int lin_unconverged = 0;
+  for (int k = S - 1; k >= 0; --k) {
+    const double* prevc = k > 0 ? H.c[k - 1].get() : zeros.get();
+    // c_k = Phi(eps(x_k), c_{k-1}, rho): onto x_k
+    k_upa_phi_eps<<<cb, kUpT, 0, s>>>(cells, coords, C, U.j.p, H.x[k].get(), prevc, z, cb_cur.get(), xc.get());
+    k_up_gather<<<nb, 128, 0, s>>>(N, U.ptr.get(), U.adj.get(), C, xc.get(), xbar.get(), 1);
+    PA_LAUNCHED();
+    // adjoint of step k with its converged tangent
+    PA_CUDA(cudaMemcpyAsync(U.prev.get(), prevc, sizeof(double) * kLocal * C, cudaMemcpyDeviceToDevice, s));
+    PA_CUDA(cudaMemcpyAsync(U.ppg.get(), H.pi[k].get(), sizeof(double) * 3 * N, cudaMemcpyDeviceToDevice, s));
+    U.cells_eval(H.x[k].get(), scratch.get(), true);
+    k_up_dinv<<<nb, 128, 0, s>>>(N, U.ptr.get(), U.adj.get(), C, U.ke.get(), U.mask.get(), U.dinv.get());
+    k_upa_rhs<<<grid_stride(n), 256, 0, s>>>(n, U.mask.get(), xbar.get(), U.b.get());
+    PA_LAUNCHED();
+    const int64_t its = U.minres(lin_tol, lin_max);
+    lin_total += its < 0 ? -its : its;
+    if (its < 0) ++lin_unconverged;
+    k_upa_resid<<<cb, kUpT, 0, s>>>(cells, coords, C, U.q, U.j.p, H.x[k].get(), prevc, H.c[k].get(), H.pi[k].get(), z,
+                                    U.dx.get(), cb_cur.get(), cb_prev.get(), rbar.get(), pib.get());
+    PA_LAUNCHED();
+    PA_CUDA(cudaMemsetAsync(xbar.get(), 0, sizeof(double) * n, s));
+    if (k > 0) {  // Pi_k = Q(p_{k-1}): onto x_{k-1}
+      k_upa_gather3<<<nb, 128, 0, s>>>(N, U.ptr.get(), U.adj.get(), C, pib.get(), pibn.get());
+      k_upa_proj<<<cb, kUpT, 0, s>>>(cells, coords, C, U.q, H.x[k - 1].get(), z, H.pi[k].get(), W.get(), pibn.get(),
+                                     xc.get(), rbar.get());
+      k_up_gather<<<nb, 128, 0, s>>>(N, U.ptr.get(), U.adj.get(), C, xc.get(), xbar.get(), 0);
+      PA_LAUNCHED();
+    }
+    std::swap(cb_cur.p, cb_prev.p);
+  }
+  k_upa_nodal<<<nb, 128, 0, s>>>(N, U.ptr.get(), U.adj.get(), rbar.get(), grad);
+  PA_LAUNCHED();
+  PA_CUDA(cudaStreamSynchronize(s));
+  if (js) {
+    js->cg_iterations += lin_total;
+    js->linear_unconverged += lin_unconverged;
+  }
+  return lin_unconverged ? PA_ERR_NOT_CONVERGED : PA_OK;
 }
 
 }  // namespace pa

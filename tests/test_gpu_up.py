@@ -131,3 +131,55 @@ def test_up_solve_plastic_bar_matches_oracle(pa, hkin, ps):
     assert np.abs(loc - loc_ref).max() <= 1e-6 * np.abs(loc_ref).max()
     assert np.abs(ppg.reshape(-1, 3) - ppg_ref).max() <= 1e-7 * np.abs(ppg_ref).max()
     assert st["newton_iterations"] <= 15 * steps
+
+
+@pytest.mark.parametrize("steps,strain", [(1, 1e-4), (3, 0.02)])
+def test_up_elastic_work_gradient(pa, steps, strain):
+    """The path-dependent adjoint gradient of the "Elastic Work" criterion
+    (summed over the load steps) against central differences of the NumPy
+    u-p Newton's criterion along random control directions; elastic (one
+    step) and plastic (three steps, most cells yield, kinematic hardening,
+    lagged projection active)."""
+    from oracle import np_j2
+    rng = np.random.default_rng(11)
+    nx = 4
+    cells, coords = np_ref.box_mesh(nx, 1, 1, float(nx), 1.0, 1.0)
+    inner = (coords[:, 0] > 1e-9) & (coords[:, 0] < nx - 1e-9)
+    coords = coords + np.where(inner[:, None], rng.uniform(-0.1, 0.1, coords.shape), 0.0)
+    N = coords.shape[0]
+    z = rng.uniform(0.6, 1.0, N)
+    x0 = np.where(coords[:, 0] < 1e-9)[0]
+    x1 = np.where(coords[:, 0] > nx - 1e-9)[0]
+    dofs3 = np.concatenate([3 * x0, 3 * x0 + 1, 3 * x0 + 2, 3 * x1])
+    vals = np.concatenate([np.zeros(3 * x0.size), np.full(x1.size, strain * nx)])
+    o = np.argsort(dofs3)
+    dofs3, vals = dofs3[o], vals[o]
+    E, nu, ps, fpe = 200e3, 0.3, 1.3, 2.0
+    j2 = dict(youngs_modulus=E, poissons_ratio=nu, initial_yield_stress=250.0, hardening_modulus_isotropic=1000.0,
+              hardening_modulus_kinematic=400.0, elastic_penalty_exponent=3.0, elastic_min_ersatz=1e-9,
+              plastic_penalty_exponent=2.5, plastic_min_ersatz=1e-4)
+    up = dict(youngs_modulus=E, poissons_ratio=nu, penalty_exponent=3.0, penalty_min=1e-9, pressure_scaling=ps)
+    mesh = pa.Mesh.from_arrays(cells, coords)
+    prob = pa.Problem(mesh, E, nu)
+    prob.set_dirichlet(dofs3.astype(np.int32), vals)
+    value, grad, state, local, st = prob.up_elastic_work(up, j2, z, steps=steps, max_newton=30, newton_tol=1e-12,
+                                                         penalty_exponent=fpe)
+    assert st["converged"], st
+    prm = np_j2.J2Params(E, nu, 250.0, 1000.0, 400.0, pe=3.0, pe_min=1e-9, pp=2.5, pp_min=1e-4)
+    dofs4 = 4 * (dofs3 // 3) + dofs3 % 3
+
+    def oracle_value(zz):
+        P = np_up.UpProblem(cells, coords, E, nu, prm, z=zz, pe=3.0, pe_min=1e-9, ps=ps)
+        P.solve(dofs4, vals, steps, tol=1e-13)
+        assert P.converged
+        return P.elastic_work(fpe, 1e-9), P
+
+    w0, P0 = oracle_value(z)
+    assert abs(value - w0) <= 1e-9 * abs(w0)
+    if steps > 1:
+        assert (P0.history[-1][1][:, 1] > 0).mean() > 0.8
+    h = 1e-5
+    for _ in range(3):
+        d = rng.normal(size=N)
+        fd = (oracle_value(z + h * d)[0] - oracle_value(z - h * d)[0]) / (2 * h)
+        assert abs(grad @ d - fd) <= 2e-6 * max(abs(fd), np.abs(grad).sum() * np.abs(d).max() * 1e-3)
