@@ -62,6 +62,28 @@ const char* pa_last_error(void);
 pa_status pa_mesh_create(const int32_t* cells2nodes, int64_t num_cells, const double* coords,
                          int64_t num_nodes, pa_mesh** out);
 
+/* Exodus II mesh input, the mesh and node sets the reference reads with
+ * Omega_h::exodus::read (src/PlatoDriver.hpp:76).  Host-only: a netCDF
+ * classic file (CDF-1, CDF-2 or CDF-5; netCDF-4/HDF5 files are refused with
+ * PA_ERR_INVALID_ARG) with num_dim 3, coordinates coordx/coordy/coordz (or
+ * coord), element blocks connect1..B of 4-node tetrahedra (elem_type TETRA,
+ * TETRA4, TET4 or TET; any other type is refused) concatenated in block
+ * order, and node sets node_ns1..S named by ns_names (else "ns_<id>" from
+ * ns_prop1).  Indices are 0-based on output.  Typical use: open, sizes, mesh
+ * into caller arrays, pa_mesh_create, node sets for the Dirichlet dofs,
+ * close. */
+typedef struct pa_exodus pa_exodus;
+pa_status pa_exodus_open(const char* path, pa_exodus** out);
+pa_status pa_exodus_sizes(const pa_exodus* exodus, int64_t* num_nodes, int64_t* num_cells, int32_t* num_node_sets);
+/* coords: 3 x num_nodes (x, y, z per node); cells2nodes: 4 x num_cells */
+pa_status pa_exodus_mesh(const pa_exodus* exodus, double* coords, int32_t* cells2nodes);
+/* Node set `index` (0 .. num_node_sets - 1): its name (truncated to
+ * name_capacity - 1 characters, NUL-terminated; may be NULL), its size and,
+ * when nodes is not NULL, its node ids. */
+pa_status pa_exodus_node_set(const pa_exodus* exodus, int32_t index, char* name, int32_t name_capacity,
+                             int64_t* count, int32_t* nodes);
+void pa_exodus_close(pa_exodus* exodus);
+
 /* Structured box [0,lx]x[0,ly]x[0,lz] with nx*ny*nz hexes, each split into
  * six tets around its (0,0,0)-(1,1,1) diagonal in the order of the
  * reference's single-hex box (unit_tests/OmegaHUtilitiesTests.cpp:258-287).

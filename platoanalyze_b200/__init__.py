@@ -6,9 +6,9 @@ Problem / VectorFunction / PhysicsScalarFunction interfaces over that ABI.
 Importing it loads the library and fails if it has not been built.
 """
 from . import _abi
-from .api import LearnedPreconditioner, Mesh, PhysicsScalarFunction, Problem, SolveOptions, VectorFunction
+from .api import LearnedPreconditioner, Mesh, PhysicsScalarFunction, Problem, SolveOptions, VectorFunction, read_exodus
 
 _abi.load()
 
 __all__ = ["Mesh", "Problem", "VectorFunction", "PhysicsScalarFunction", "SolveOptions",
-           "LearnedPreconditioner"]
+           "LearnedPreconditioner", "read_exodus"]

@@ -117,6 +117,11 @@ SIGNATURES = [
     ("pa_pc_apply", I32, [P, P, P, P, P]),
     ("pa_pc_train", I32, [P, P, I32, P, I32, P, P, P, ct.POINTER(PcTrainOptions), ct.POINTER(PcTrainStats)]),
     ("pa_problem_set_preconditioner", I32, [P, P]),
+    ("pa_exodus_open", I32, [ct.c_char_p, ct.POINTER(P)]),
+    ("pa_exodus_sizes", I32, [P, ct.POINTER(I64), ct.POINTER(I64), ct.POINTER(I32)]),
+    ("pa_exodus_mesh", I32, [P, P, P]),
+    ("pa_exodus_node_set", I32, [P, I32, ct.c_char_p, I32, ct.POINTER(I64), P]),
+    ("pa_exodus_close", None, [P]),
     ("pa_up_residual", I32, [P, ct.POINTER(UpParams), P, P, P, I32, P, P, I32]),
     ("pa_up_solve", I32, [P, ct.POINTER(UpParams), ct.POINTER(J2Params), P, ct.POINTER(J2SolveOptions),
                           ct.POINTER(SolveOptions), P, P, P, ct.POINTER(J2Stats)]),

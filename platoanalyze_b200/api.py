@@ -95,6 +95,13 @@ class Mesh:
                                       coords.shape[0], ct.byref(h)))
         return cls(h)
 
+    @classmethod
+    def from_exodus(cls, path):
+        """The mesh of an Exodus II file (pa_exodus_*, then pa_mesh_create)
+        and its node sets {name: node ids}."""
+        cells, coords, sets = read_exodus(path)
+        return cls.from_arrays(cells, coords), sets
+
     def arrays(self):
         cells = np.empty((self.num_cells, 4), np.int32)
         coords = np.empty((self.num_nodes, 3), np.float64)
@@ -469,6 +476,31 @@ class Problem:
             self.close()
         except Exception:
             pass
+
+
+def read_exodus(path):
+    """(cells C x 4, coords N x 3, {node set name: node ids}) of an Exodus II
+    file, read by the library's netCDF classic reader (host only)."""
+    lib = _abi.load()
+    h = ct.c_void_p()
+    _abi.check(lib.pa_exodus_open(os.fsencode(path), ct.byref(h)))
+    try:
+        N, C, S = ct.c_int64(), ct.c_int64(), ct.c_int32()
+        _abi.check(lib.pa_exodus_sizes(h, ct.byref(N), ct.byref(C), ct.byref(S)))
+        coords = np.empty((N.value, 3), np.float64)
+        cells = np.empty((C.value, 4), np.int32)
+        _abi.check(lib.pa_exodus_mesh(h, _ptr(coords, np.float64), _ptr(cells, np.int32)))
+        sets = {}
+        for i in range(S.value):
+            name = ct.create_string_buffer(256)
+            n = ct.c_int64()
+            _abi.check(lib.pa_exodus_node_set(h, i, name, 256, ct.byref(n), None))
+            nodes = np.empty(n.value, np.int32)
+            _abi.check(lib.pa_exodus_node_set(h, i, None, 0, None, _ptr(nodes, np.int32) if n.value else None))
+            sets[name.value.decode()] = nodes
+        return cells, coords, sets
+    finally:
+        lib.pa_exodus_close(h)
 
 
 def _stats(st):

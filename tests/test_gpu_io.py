@@ -57,3 +57,31 @@ def test_vtu_without_fields_and_bad_path(pa, tmp_path):
     assert d["C"] == 48 and ("PointData", "Displacements") not in d
     with pytest.raises(PaError):
         mesh.write_vtu(tmp_path / "no_such_dir" / "x.vtu")
+
+
+def test_exodus_mesh_solves_on_the_box_multigrid(pa, tmp_path):
+    """An Exodus II file of a scrambled, x-mirrored 24x12x12 box (two element
+    blocks, named node sets) read with pa_exodus_*: the mesh is recognised as
+    a lattice, the clamped face comes from its node set, and the multigrid
+    solve equals the one of the same arrays handed to pa_mesh_create."""
+    from exodus_writer import exodus_box
+    from test_gpu_box import _scrambled
+    nx, ny, nz = 24, 12, 12
+    cl, X, _, order, faces, clamp = _scrambled(nx, ny, nz, 3, mirror_x=True)
+    path = str(tmp_path / "box.exo")
+    exodus_box(path, cl, X, {"ns_X1": clamp, "load": np.unique(faces)}, version=2)
+    mesh, sets = pa.Mesh.from_exodus(path)
+    assert mesh.box_kernels
+    assert np.array_equal(sets["ns_X1"], clamp)
+    rng = np.random.default_rng(4)
+    z = rng.uniform(0.05, 1.0, cl.shape[0])
+    flux = np.array([0.0, 0.0, -1.0 / (ny * nz)])
+    out = []
+    for m, ns in ((mesh, sets["ns_X1"]), (pa.Mesh.from_arrays(cl, X), clamp)):
+        prob = pa.Problem(m, 1.0, 0.3, 3.0, 1e-9, control_layout="cell")
+        prob.add_traction(faces, flux)
+        prob.set_dirichlet(np.sort(np.concatenate([3 * ns, 3 * ns + 1, 3 * ns + 2])).astype(np.int32))
+        u, st = prob.solution(z, options=pa.SolveOptions("mg", rel_tol=1e-10))
+        assert st["converged"], st
+        out.append(u)
+    assert np.array_equal(out[0], out[1])
