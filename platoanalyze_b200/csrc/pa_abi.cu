@@ -286,6 +286,9 @@ pa_status pa_mesh_set_graph(pa_mesh* mesh, const int32_t* rowmap, const int32_t*
       PA_CHECK(a == b, "row columns differ from the mesh pattern");
     }
     m.cols.assign(cols, cols + num_blocks);
+    m.cols_sorted = true;
+    for (int64_t v = 0; v < m.N && m.cols_sorted; ++v)
+      m.cols_sorted = std::is_sorted(m.cols.begin() + m.rowmap[v], m.cols.begin() + m.rowmap[v + 1]);
     if (m.d_cell_entry.n) m.build_graph_entries();
   });
 }
@@ -416,6 +419,10 @@ pa_status pa_problem_set_dirichlet(pa_problem* problem, const int32_t* dofs, con
 // tets of a tile sum into shared memory and only nodes shared with other
 // tiles are added globally, instead of 12 global atomics per tet.
 static void apply_k64(Problem& P, const double* du, const double* dz, double* dy) {
+  if (pa::box_entry_eligible(P)) {  // the box kernel, penalty and interleaving fused
+    pa::box_entry_apply(P, dz, du, dy);
+    return;
+  }
   const int64_t n = P.ndof();
   P.ws.w64.resize(P.C());
   pa::launch_cell_weights(P, dz, P.ws.w64.get(), nullptr, P.stream);
@@ -449,7 +456,7 @@ pa_status pa_vf_gradient_u(pa_problem* problem, const double* u, const double* z
     pa::Stage st(P);
     const double* dz = st.in(z, P.nz(), "z");
     double* de = st.out(entries, 9 * P.mesh->B, "entries");
-    pa::launch_gradient_u(P, dz, de, P.stream);
+    if (!pa::box_gradient_u(P, dz, de)) pa::launch_gradient_u(P, dz, de, P.stream);
     st.finish();
   });
 }
@@ -505,7 +512,10 @@ static void energy_call(pa_problem* problem, const double* u, const double* z, d
     if (P.d_partials.n < size_t(grid)) P.d_partials.resize(grid);
     if (P.d_scalar.n < 2) P.d_scalar.resize(2);
   }
-  pa::launch_energy(P, du, dz, P.d_partials.get(), value ? P.d_scalar.get() : nullptr, dgu, dgz, P.stream);
+  if (!dgu && pa::box_entry_eligible(P))
+    pa::box_entry_energy(P, dz, du, value ? P.d_scalar.get() : nullptr, dgz);
+  else
+    pa::launch_energy(P, du, dz, P.d_partials.get(), value ? P.d_scalar.get() : nullptr, dgu, dgz, P.stream);
   if (value) {
     PA_CUDA(cudaMemcpyAsync(value, P.d_scalar.get(), sizeof(double), cudaMemcpyDeviceToHost, P.stream));
     PA_CUDA(cudaStreamSynchronize(P.stream));

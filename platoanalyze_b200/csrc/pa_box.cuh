@@ -36,6 +36,7 @@
 
 #include <cstdint>
 
+#include "pa_cell.cuh"
 #include "pa_internal.cuh"
 
 namespace pa {
@@ -58,12 +59,15 @@ struct BoxGeo {
   T ih[3];
 };
 
-// SIMP weights: one per hex (WM = 0) or one per tet, tet-major (WM = 1:
-// w[t H + h]).
+// SIMP weights: one per hex (WM = 0), one per tet, tet-major (WM = 1:
+// w[t H + h]), or (WM = 2) the per-cell controls themselves in box slot
+// order (w[6 h + t]) with the SIMP penalty pmin + (1 - pmin) w^p applied as
+// they are loaded.
 template <typename T, int WM>
 struct BoxW {
   const T* w;
   int64_t H;
+  double p = 0.0, pmin = 0.0;
 };
 
 // Deterministic grid reduction: one partial per CTA, the last CTA to arrive
@@ -269,7 +273,11 @@ __global__ void __launch_bounds__(kBoxThreads) k_box(BoxDims d, BoxGeo<T> g, Box
   T wn[WM ? 6 : 1];
   auto load_w = [&](int k) {
     if (hex_ij && k >= 0 && k < d.nz) {
-      if constexpr (WM) {
+      if constexpr (WM == 2) {
+        const int64_t hh = h0 + int64_t(k) * layer;
+#pragma unroll
+        for (int t = 0; t < 6; ++t) wn[t] = T(simp(double(bw.w[6 * hh + t]), bw.p, bw.pmin));
+      } else if constexpr (WM == 1) {
 #pragma unroll
         for (int t = 0; t < 6; ++t) wn[t] = bw.w[int64_t(t) * bw.H + h0 + k * layer];
       } else {

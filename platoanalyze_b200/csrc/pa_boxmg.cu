@@ -34,6 +34,7 @@
 // Requirements: a box lattice (mesh_make_box, or arrays recognised by
 // detect_lattice: the solver permutes b and x at its boundary) with even hex
 // counts, an elastic operator (J2 tangent solves keep pa_mg.cu), one part.
+#include <algorithm>
 #include <cmath>
 #include <memory>
 #include <vector>
@@ -779,6 +780,9 @@ struct BoxHierarchy {
   std::vector<int32_t> mask_dofs;  // the Dirichlet set the coarse masks were built for
   bool masks_valid = false;
   DevBuf<float> cheb;  // per smoothed level: 1 / theta, ca, c2 (read by the captured iteration)
+  DevBuf<double> e_partials, e_value;  // the per-cell entry points' energy reduction
+  DevBuf<double> gu_k0;                // assembled K on the box: unpenalized blocks per table entry
+  double gu_key[5] = {0, 0, 0, 0, 0};  // the hex sides and Lame constants they were made for
   // the captured outer iteration (two variants alternate the p buffers),
   // reused while every pointer and constant it captured is unchanged
   struct GraphKey {
@@ -856,7 +860,7 @@ void set_dims(BoxLevel& L, int nx, int ny, int nz, double lx, double ly, double 
 
 template <typename T, int WM, bool CUBE, class In, class Out>
 void launch_box_t(const BoxLevel& L, const BoxGeo<T>& g, const T* w, const In& in, const Out& out, BoxRed red,
-                  cudaStream_t s) {
+                  cudaStream_t s, double p = 0.0, double pmin = 0.0) {
   static int occupancy = 0;  // resident CTAs per SM of this instance
   if (occupancy == 0) {
     int o = 0;
@@ -865,7 +869,7 @@ void launch_box_t(const BoxLevel& L, const BoxGeo<T>& g, const T* w, const In& i
   }
   int kz = 2;
   const dim3 grid = box_grid(L.d, occupancy * num_sms(), &kz);
-  k_box<T, WM, CUBE, In, Out><<<grid, kBoxThreads, 0, s>>>(L.d, g, BoxW<T, WM>{w, L.d.H}, kz, in, out, red);
+  k_box<T, WM, CUBE, In, Out><<<grid, kBoxThreads, 0, s>>>(L.d, g, BoxW<T, WM>{w, L.d.H, p, pmin}, kz, in, out, red);
   PA_LAUNCHED();
   g_box_launches += 1;
 }
@@ -1041,20 +1045,13 @@ bool boxmg_setup(Problem& P, const double* z) {
   F.wm = differ ? 1 : 0;
   const double* fw64 = F.wm ? H.w64t.get() : H.w64h.get();
   g_box_launches += 1;
-  // coarse weights and every level's inverse diagonal
+  // coarse weights of every level
   const Iso<double> iso = P.ep.iso();
-  for (size_t l = 0; l < H.L.size(); ++l) {
+  for (size_t l = 1; l < H.L.size(); ++l) {
     BoxLevel& L = *H.L[l];
-    const double* lw = l == 0 ? fw64 : L.w64.get();
-    if (l > 0) {
-      const BoxLevel& Fl = *H.L[l - 1];
-      k_bcoarse_w<<<int((L.d.H + kVT - 1) / kVT), kVT, 0, s>>>(L.d, Fl.d, l == 1 ? fw64 : Fl.w64.get(),
-                                                               l == 1 ? F.wm : 0, L.w64.get(), L.w32.get());
-      PA_LAUNCHED();
-      g_box_launches += 1;
-    }
-    k_bdinv<<<int((L.d.N + kVT - 1) / kVT), kVT, 0, s>>>(L.d, L.h[0], L.h[1], L.h[2], iso.lam, iso.mu, lw,
-                                                         l == 0 ? F.wm : 0, L.mask, L.dinv.get());
+    const BoxLevel& Fl = *H.L[l - 1];
+    k_bcoarse_w<<<int((L.d.H + kVT - 1) / kVT), kVT, 0, s>>>(L.d, Fl.d, l == 1 ? fw64 : Fl.w64.get(),
+                                                             l == 1 ? F.wm : 0, L.w64.get(), L.w32.get());
     PA_LAUNCHED();
     g_box_launches += 1;
   }
@@ -1079,6 +1076,15 @@ bool boxmg_setup(Problem& P, const double* z) {
     PA_LAUNCHED();
     gj_invert(s, nd, Lc.dense.get(), Lc.diag0.get(), Lc.gj_c.get(), Lc.gj_p.get(), Lc.gj_sync.get(), Lc.flag.get());
     g_box_launches += 3;
+  }
+  // every level's inverse diagonal
+  for (size_t l = 0; l < H.L.size(); ++l) {
+    BoxLevel& L = *H.L[l];
+    const double* lw = l == 0 ? fw64 : L.w64.get();
+    k_bdinv<<<int((L.d.N + kVT - 1) / kVT), kVT, 0, s>>>(L.d, L.h[0], L.h[1], L.h[2], iso.lam, iso.mu, lw,
+                                                         l == 0 ? F.wm : 0, L.mask, L.dinv.get());
+    PA_LAUNCHED();
+    g_box_launches += 1;
   }
   // lmax of D^-1 K per smoothed level by power iteration, on the device
   // (the norm of each step lands in norms[level][step]); an elastic solve
@@ -1482,6 +1488,290 @@ double time_box_apply(Problem& P, const double* z, bool fp32, int reps, int64_t*
   const int64_t sv = fp32 ? 4 : 8;
   if (bytes) *bytes = (F.wm ? 6 * F.d.H : F.d.H) * sv + F.d.N * (6 * sv + 1);
   return double(ms) / reps;
+}
+
+
+// ------------------------------------------------------ box entry points --
+// The per-cell entry points (VectorFunction::value, the internal energy and
+// its gradients) on a box mesh in its own numbering (pa_mesh_create_box, or
+// arrays in that order): K(z) u by the box kernel with the SIMP penalty of
+// the per-cell controls applied as the weights load and the interleaved
+// vectors read and written in place; the energy and dF/dz by one thread per
+// hex over its six tets with the lattice's edge-difference gradients.
+namespace {
+
+// x from the interleaved vector (3 per node, lattice node ids)
+struct InAoS64 {
+  const double* x;
+  struct Raw {
+    double v[3];
+  };
+  __device__ Raw load(int v, bool) const {
+    Raw r;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) r.v[c] = x[3 * int64_t(v) + c];
+    return r;
+  }
+  __device__ void make(const Raw& r, int, bool, double (&o)[3]) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) o[c] = r.v[c];
+  }
+};
+
+struct OutAoS64 {  // y = K x, interleaved
+  double* y;
+  static constexpr bool kReduce = false;
+  struct Pre {};
+  __device__ Pre load(int) const { return {}; }
+  __device__ double store(const Pre&, int v, const double (&k)[3]) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) y[3 * int64_t(v) + c] = k[c];
+    return 0.0;
+  }
+};
+
+// Internal energy of every tet (1/2 V sigma(eps) . eps, unpenalized), summed
+// with the SIMP weights of the per-cell controls (box slot order 6 h + t) into
+// one partial per CTA, and dF/dz = dw/dz e0 per cell (grad_z may be null).
+// Path tet t runs 0 -> +axis(t,0) -> +axis(t,1) -> 7, so column axis(t,m) of
+// grad u is the difference of u along edge m over h[axis].
+__global__ void __launch_bounds__(256) k_benergy(BoxDims d, double ih0, double ih1, double ih2, double vol,
+                                                 Iso<double> iso, double p, double pmin, const double* __restrict__ u,
+                                                 const double* __restrict__ z, double* __restrict__ partials,
+                                                 double* __restrict__ grad_z) {
+  __shared__ double red[32];
+  const int64_t h = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  double f = 0.0;
+  if (h < d.H) {
+    const int i = int(h % d.nx), j = int((h / d.nx) % d.ny), k = int(h / (int64_t(d.nx) * d.ny));
+    const double ih[3] = {ih0, ih1, ih2};
+    double uc[8][3];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int64_t v = (i + (q & 1)) + int64_t(d.px) * ((j + ((q >> 1) & 1)) + int64_t(d.py) * (k + (q >> 2)));
+#pragma unroll
+      for (int c = 0; c < 3; ++c) uc[q][c] = u[3 * v + c];
+    }
+#pragma unroll
+    for (int t = 0; t < 6; ++t) {
+      double du[3][3];
+      int prev = 0;
+#pragma unroll
+      for (int m = 0; m < 3; ++m) {
+        const int a = path_axis(t, m), nxt = prev | (1 << a);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) du[c][a] = (uc[nxt][c] - uc[prev][c]) * ih[a];
+        prev = nxt;
+      }
+      const double e[6] = {du[0][0], du[1][1], du[2][2], du[1][2] + du[2][1], du[0][2] + du[2][0],
+                           du[0][1] + du[1][0]};
+      double sig[6];
+      tet_stress(iso, vol, e, sig);
+      const double e0 = 0.5 * voigt_dot(sig, e);
+      const double zt = z[6 * h + t];
+      f += simp(zt, p, pmin) * e0;
+      if (grad_z) grad_z[6 * h + t] = simp_deriv(zt, p, pmin) * e0;
+    }
+  }
+  const double b = block_sum_box(f, red);
+  if (threadIdx.x == 0) partials[blockIdx.x] = b;
+}
+
+__global__ void k_bsum_partials(int n, const double* __restrict__ partials, double* __restrict__ out) {
+  __shared__ double red[32];
+  double v = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) v += partials[i];
+  v = block_sum_box(v, red);
+  if (threadIdx.x == 0) *out = v;
+}
+
+}  // namespace
+
+bool box_entry_eligible(const Problem& P) {
+  const Mesh& m = *P.mesh;
+  return box_apply_eligible(P) && !m.lat_permuted && m.lat_flip == 0 && P.ep.layout == PA_CONTROL_CELL;
+}
+
+void box_entry_apply(Problem& P, const double* z, const double* u, double* y) {
+  boxmg_ensure(P);
+  BoxHierarchy& H = *P.boxmg;
+  const BoxLevel& F = *H.L[0];
+  const BoxRed red{H.partials.get(), H.counter.get()};
+  const BoxGeo<double> g = box_geo<double>(F, P.ep);
+  if (F.cube)
+    launch_box_t<double, 2, true>(F, g, z, InAoS64{u}, OutAoS64{y}, red, P.stream, P.ep.p, P.ep.pmin);
+  else
+    launch_box_t<double, 2, false>(F, g, z, InAoS64{u}, OutAoS64{y}, red, P.stream, P.ep.p, P.ep.pmin);
+}
+
+void box_entry_energy(Problem& P, const double* z, const double* u, double* value, double* grad_z) {
+  boxmg_ensure(P);
+  BoxHierarchy& H = *P.boxmg;
+  const BoxLevel& F = *H.L[0];
+  const int blocks = int((F.d.H + 255) / 256);
+  if (H.e_partials.n < size_t(blocks)) H.e_partials.resize(blocks);
+  const double vol = F.h[0] * F.h[1] * F.h[2] / 6.0;
+  k_benergy<<<blocks, 256, 0, P.stream>>>(F.d, 1.0 / F.h[0], 1.0 / F.h[1], 1.0 / F.h[2], vol, P.ep.iso(), P.ep.p,
+                                          P.ep.pmin, u, z, H.e_partials.get(), grad_z);
+  PA_LAUNCHED();
+  if (value) {
+    k_bsum_partials<<<1, 1024, 0, P.stream>>>(blocks, H.e_partials.get(), value);
+    PA_LAUNCHED();
+  }
+}
+
+
+// ----------------------------------------------- assembled K on the box --
+// VectorFunction::gradient_u as the block-CRS matrix on a box mesh in its own
+// numbering with the mesh's sorted columns: one thread per (neighbour slot,
+// node) block, which sums the tets around that edge and writes its 3 x 3
+// block once (no atomics, no zeroing).  In the six-tet split every tet is a
+// monotone path 0 -> e_a -> e_a + e_b -> (1,1,1) through its hex, so the
+// neighbours of node v are v +- e_S for the seven non-empty axis sets S, and
+// in node-id order they are the fifteen slots of BoxEdges (px, py >= 2).
+// A CTA takes 16 consecutive nodes with one thread per (slot, node), so that a
+// warp shares its slot (the loops over the hexes and tets of an edge are
+// uniform and their table entries, kernel parameters, broadcast), and writes
+// its rows from shared memory as one contiguous range.
+namespace {
+
+struct BoxEdges {
+  int8_t off[15][3];      // neighbour offset of each slot, in node-id order
+  uint8_t count[15][8];   // tets of the edge in the hex at origin v - corner(o)
+  uint8_t tet[15][8][6];  // t | m_v << 3 | m_w << 5
+  int8_t grad[6][4][3];   // gradient of vertex m of tet t on a unit hex (-1, 0, 1 per axis)
+};
+
+BoxEdges make_box_edges() {
+  static const int8_t kOff[15][3] = {{-1, -1, -1}, {0, -1, -1}, {-1, 0, -1}, {0, 0, -1}, {-1, -1, 0},
+                                     {0, -1, 0},   {-1, 0, 0},  {0, 0, 0},   {1, 0, 0},  {0, 1, 0},
+                                     {1, 1, 0},    {0, 0, 1},   {1, 0, 1},   {0, 1, 1},  {1, 1, 1}};
+  BoxEdges E{};
+  for (int t = 0; t < 6; ++t)
+    for (int m = 0; m < 4; ++m) {
+      for (int d = 0; d < 3; ++d) E.grad[t][m][d] = 0;
+      if (m >= 1) E.grad[t][m][path_axis(t, m - 1)] += 1;
+      if (m <= 2) E.grad[t][m][path_axis(t, m)] -= 1;
+    }
+  for (int sl = 0; sl < 15; ++sl) {
+    for (int d = 0; d < 3; ++d) E.off[sl][d] = kOff[sl][d];
+    for (int o = 0; o < 8; ++o) {  // v is corner o of the hex
+      const int wi = (o & 1) + kOff[sl][0], wj = ((o >> 1) & 1) + kOff[sl][1], wk = (o >> 2) + kOff[sl][2];
+      E.count[sl][o] = 0;
+      if (wi < 0 || wi > 1 || wj < 0 || wj > 1 || wk < 0 || wk > 1) continue;
+      const int qw = wi + 2 * wj + 4 * wk;
+      for (int t = 0; t < 6; ++t) {
+        int mv = -1, mw = -1;
+        for (int m = 0; m < 4; ++m) {
+          if (path_vertex(t, m) == o) mv = m;
+          if (path_vertex(t, m) == qw) mw = m;
+        }
+        if (mv >= 0 && mw >= 0) E.tet[sl][o][E.count[sl][o]++] = uint8_t(t | (mv << 3) | (mw << 5));
+      }
+    }
+  }
+  return E;
+}
+
+constexpr int kGuNodes = 16;  // nodes per CTA of k_bgradient_u (15 slots each)
+
+__global__ void __launch_bounds__(15 * kGuNodes) k_bgradient_u(BoxDims d, double vol, double p, double pmin,
+                                                             int layout, BoxEdges E, const double* __restrict__ k0,
+                                                             const double* __restrict__ z,
+                                                             const int32_t* __restrict__ rowmap,
+                                                             double* __restrict__ vals) {
+  // thread (slot, node) = (tid / 16, tid % 16): a warp holds two slots of 16
+  // consecutive nodes; the CTA's blocks are staged in shared memory and its
+  // rows written as one contiguous range
+  __shared__ double stage[15 * kGuNodes * 9];
+  const int64_t v0 = int64_t(blockIdx.x) * kGuNodes;
+  const int64_t v1 = v0 + kGuNodes < d.N ? v0 + kGuNodes : d.N;
+  const int sl = int(threadIdx.x) / kGuNodes;
+  const int64_t v = v0 + int(threadIdx.x) % kGuNodes;
+  const int64_t base = rowmap[v0];
+  if (v < v1) {
+    const int vi = int(v % d.px), vj = int((v / d.px) % d.py), vk = int(v / (int64_t(d.px) * d.py));
+    auto inside = [&](int i, int j, int k) {
+      return i >= 0 && i <= d.nx && j >= 0 && j <= d.ny && k >= 0 && k <= d.nz;
+    };
+    if (inside(vi + E.off[sl][0], vj + E.off[sl][1], vk + E.off[sl][2])) {
+      int rank = 0;
+      for (int q = 0; q < sl; ++q) rank += inside(vi + E.off[q][0], vj + E.off[q][1], vk + E.off[q][2]) ? 1 : 0;
+      double K[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      for (int o = 0; o < 8; ++o) {
+        const int n = E.count[sl][o];
+        if (n == 0) continue;
+        const int oi = vi - (o & 1), oj = vj - ((o >> 1) & 1), ok = vk - (o >> 2);
+        if (oi < 0 || oj < 0 || ok < 0 || oi >= d.nx || oj >= d.ny || ok >= d.nz) continue;
+        const int64_t h = oi + int64_t(d.nx) * (oj + int64_t(d.ny) * ok);
+        for (int e = 0; e < n; ++e) {
+          const int t = E.tet[sl][o][e] & 7;
+          double rho;
+          if (layout == PA_CONTROL_CELL) {
+            rho = z[6 * h + t];
+          } else {
+            rho = 0.0;
+            for (int m = 0; m < 4; ++m) {
+              const int c = path_vertex(t, m);
+              rho += 0.25 * z[(oi + (c & 1)) +
+                              int64_t(d.px) * ((oj + ((c >> 1) & 1)) + int64_t(d.py) * (ok + (c >> 2)))];
+            }
+          }
+          const double w = vol * simp(rho, p, pmin);
+          const double* kb = k0 + 9 * ((sl * 8 + o) * 6 + e);
+#pragma unroll
+          for (int q = 0; q < 9; ++q) K[q] = fma(w, __ldg(kb + q), K[q]);
+        }
+      }
+      double* dst = stage + 9 * (int64_t(rowmap[v]) - base + rank);
+#pragma unroll
+      for (int q = 0; q < 9; ++q) dst[q] = K[q];
+    }
+  }
+  __syncthreads();
+  const int64_t count = 9 * (int64_t(rowmap[v1]) - base);
+  for (int64_t e = threadIdx.x; e < count; e += blockDim.x) vals[9 * base + e] = stage[e];
+}
+
+}  // namespace
+
+bool box_gradient_u(Problem& P, const double* z, double* entries) {
+  const Mesh& m = *P.mesh;
+  if (!(m.box_kernels && m.lat_n[0] > 0 && !m.lat_permuted && m.lat_flip == 0 && m.cols_sorted && m.d_rowmap.n))
+    return false;
+  static const BoxEdges edges = make_box_edges();
+  boxmg_ensure(P);
+  BoxHierarchy& H = *P.boxmg;
+  const BoxLevel& F = *H.L[0];
+  // the unpenalized 3 x 3 block of every (slot, hex corner, tet) entry: on a
+  // uniform box it depends only on the hex sides and the Lame constants
+  const Iso<double> iso = P.ep.iso();
+  const double key[5] = {F.h[0], F.h[1], F.h[2], iso.lam, iso.mu};
+  if (!H.gu_k0.n || !std::equal(key, key + 5, H.gu_key)) {
+    std::vector<double> k0(size_t(15 * 8 * 6 * 9), 0.0);
+    const double ih[3] = {1.0 / F.h[0], 1.0 / F.h[1], 1.0 / F.h[2]};
+    for (int sl = 0; sl < 15; ++sl)
+      for (int o = 0; o < 8; ++o)
+        for (int e = 0; e < edges.count[sl][o]; ++e) {
+          const int code = edges.tet[sl][o][e], t = code & 7, mv = (code >> 3) & 3, mw = code >> 5;
+          double ga[3], gb[3];
+          for (int c = 0; c < 3; ++c) {
+            ga[c] = ih[c] * edges.grad[t][mv][c];
+            gb[c] = ih[c] * edges.grad[t][mw][c];
+          }
+          const double dd = iso.mu * (ga[0] * gb[0] + ga[1] * gb[1] + ga[2] * gb[2]);
+          double* kb = &k0[size_t(9 * ((sl * 8 + o) * 6 + e))];
+          for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) kb[3 * i + j] = iso.lam * ga[i] * gb[j] + iso.mu * ga[j] * gb[i] + (i == j ? dd : 0.0);
+        }
+    H.gu_k0.upload(k0.data(), k0.size(), P.stream);
+    std::copy(key, key + 5, H.gu_key);
+  }
+  k_bgradient_u<<<int((F.d.N + kGuNodes - 1) / kGuNodes), 15 * kGuNodes, 0, P.stream>>>(
+      F.d, F.h[0] * F.h[1] * F.h[2] / 6.0, P.ep.p, P.ep.pmin, P.ep.layout, edges, H.gu_k0.get(), z,
+      m.d_rowmap.get(), entries);
+  PA_LAUNCHED();
+  return true;
 }
 
 }  // namespace pa

@@ -129,6 +129,7 @@ struct Mesh {
   DevBuf<float4> d_coords32_aos4;    // N x (x, y, z, 0): one 16-byte gather per node (FP32 PCG modes)
   DevBuf<int32_t> d_rowmap, d_cols;
   DevBuf<int32_t> d_cell_entry;  // C*16 CRS block index of (a,b) pairs
+  bool cols_sorted = true;       // every row's columns in increasing node order
   int64_t num_clusters = 0, num_hex = 0;
   // every cluster a hex and every hex a translate of the first (edge vectors
   // equal to 1e-9 of the hex size): the FP32 tile kernel then takes the

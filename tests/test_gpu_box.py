@@ -251,3 +251,62 @@ def test_box_mg_mirrored_scrambled_with_dirichlet_values(pa):
     assert st["converged"], st
     assert np.array_equal(u[dofs], vals)
     assert rel_inf(u, u64) <= 1e-7
+
+
+@pytest.mark.parametrize("dims,lengths,p", [((10, 6, 5), (10.0, 6.0, 5.0), 3.0), ((9, 7, 4), (4.5, 5.25, 1.0), 2.5)])
+def test_box_entry_points_match_oracle(pa, oracle_lib, dims, lengths, p):
+    """The per-cell entry points on a box mesh with per-cell controls (the
+    box kernel with the penalty applied as the controls load, and the per-hex
+    energy kernel): residual, internal energy, dF/du and dF/dz against the
+    oracle, on cubic and non-cubic hexes, integer and fractional exponents."""
+    mesh = pa.Mesh.box(*dims, *lengths)
+    assert mesh.box_kernels
+    cells, coords = mesh.arrays()
+    E, nu, pmin = 3.0, 0.27, 1e-6
+    prob = pa.Problem(mesh, E, nu, p, pmin, control_layout="cell")
+    faces = mesh.boundary_faces(0, lengths[0])
+    flux = np.array([0.1, -0.2, 0.7])
+    prob.add_traction(faces, flux)
+    rng = np.random.default_rng(17)
+    u = rng.standard_normal(3 * coords.shape[0])
+    z = rng.uniform(0.05, 1.0, cells.shape[0])
+    O = oracle_lib.Oracle(cells, coords, E=E, nu=nu, p=p, pmin=pmin, layout=1)
+    vf = prob.vector_function()
+    assert rel_inf(vf.value(u, z), O.residual(u, z, faces, flux)) <= 1e-10
+    f, gu, gz = O.energy(u, z)
+    sf = prob.scalar_function()
+    assert abs(sf.value(u, z) - f) <= 1e-10 * abs(f)
+    assert rel_inf(sf.gradient_u(u, z), gu) <= 1e-10
+    assert rel_inf(sf.gradient_z(u, z), gz) <= 1e-10
+
+
+@pytest.mark.parametrize("layout,lengths", [("cell", (8.0, 5.0, 4.0)), ("nodal", (4.0, 7.5, 2.0))])
+def test_box_assembled_gradient_u(pa, oracle_lib, layout, lengths):
+    """VectorFunction::gradient_u on a box mesh: the per-block lattice
+    assembly (no atomics) equals the oracle's block CRS matrix and, to
+    rounding, the per-cell atomic assembly (box kernels switched off);
+    reordered columns (pa_mesh_set_graph) fall back to the per-cell one."""
+    dims = (8, 5, 4)
+    mesh = pa.Mesh.box(*dims, *lengths)
+    assert mesh.box_kernels
+    cells, coords = mesh.arrays()
+    rng = np.random.default_rng(23)
+    E, nu, p, pmin = 2.0, 0.3, 3.0, 1e-6
+    z = rng.uniform(0.05, 1.0, cells.shape[0] if layout == "cell" else coords.shape[0])
+    u = rng.standard_normal(3 * coords.shape[0])
+    prob = pa.Problem(mesh, E, nu, p, pmin, control_layout=layout)
+    K = prob.vector_function().gradient_u(u, z)
+    O = oracle_lib.Oracle(cells, coords, E=E, nu=nu, p=p, pmin=pmin, layout=1 if layout == "cell" else 0)
+    assert rel_inf(K, O.jacobian(u, z, mesh.graph())) <= 1e-12
+    mesh.set_box_kernels(False)
+    K_atomic = prob.vector_function().gradient_u(u, z)
+    assert rel_inf(K, K_atomic) <= 1e-13
+    mesh.set_box_kernels(True)
+    # a graph with every row's columns reversed: the lattice path steps aside
+    rowmap, cols = mesh.graph()
+    rev = cols.copy()
+    for v in range(coords.shape[0]):
+        rev[rowmap[v]:rowmap[v + 1]] = cols[rowmap[v]:rowmap[v + 1]][::-1]
+    mesh.set_graph(rowmap, rev)
+    K_rev = prob.vector_function().gradient_u(u, z)
+    assert rel_inf(K_rev, O.jacobian(u, z, mesh.graph())) <= 1e-12
