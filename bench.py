@@ -40,7 +40,8 @@ FALLBACK_HBM_GBS = 6650.0
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default: 100 for the multigrid cantilever solve, 20 otherwise)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--dims", default="160x80x80")
@@ -69,7 +70,10 @@ def parse():
                          "per-cell entry point timed against its roofline")
     ap.add_argument("--simp-iterations", type=int, default=30)
     ap.add_argument("--train-steps", type=int, default=400)
-    return ap.parse_args()
+    args = ap.parse_args()
+    if args.steps is None:  # a timed region of about a second for the multigrid solve
+        args.steps = 100 if args.workload == "cantilever" and args.method == "mg" and args.impl == "ours" else 20
+    return args
 
 
 def dims_of(s):
@@ -115,7 +119,7 @@ class ClockSampler:
         os.close(fd)
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
