@@ -220,7 +220,10 @@ __device__ __forceinline__ void box_hex(const T (&u)[8][3], const T (&lw)[6], co
 // Grid: (ceil(px / 31), ceil(py / 7), ceil(pz / kz)) CTAs of 256 threads.
 template <typename T, int WM, bool CUBE, class In, class Out>
 __global__ void __launch_bounds__(kBoxThreads) k_box(BoxDims d, BoxGeo<T> g, BoxW<T, WM> bw, int kz, In in,
-                                                     Out out, BoxRed red) {
+                                                     Out out, BoxRed red, const double* skip) {
+  // skip (may be null): two flags; the launch is a no-op when either is set
+  // (a solve that converged or broke down inside a batch of captured iterations)
+  if (skip && (skip[0] != 0.0 || skip[1] != 0.0)) return;
   __shared__ BoxV4<T> xs[4][kBoxPlane];
   __shared__ BoxV4<T> yb[2][8][32];
   __shared__ double s_red[32];

@@ -52,7 +52,9 @@ constexpr int kVT = 256;
 int vec_blocks(int64_t n) { return int(std::min<int64_t>((n + kVT - 1) / kVT, 148 * 8)); }
 
 // device scalars of the outer CG
-enum : int { kRz = 0, kPq, kAlpha, kBeta, kRr, kBreak, kFirst, kScalars };
+// outer CG scalars on the device; kBreak and kDone adjacent (the skip flags of
+// the captured iteration's launches), kRr .. kIters read by the host together
+enum : int { kRz = 0, kPq, kAlpha, kBeta, kRr, kBreak, kDone, kIters, kFirst, kTol, kScalars };
 
 // Axis paths of the six tets (pa_box.cuh): (y,x,z) (y,z,x) (z,y,x) (z,x,y)
 // (x,z,y) (x,y,z), two bits per axis, tet t at bits 6t.
@@ -427,12 +429,14 @@ __device__ __forceinline__ void grid_reduce_finish(double v, double* partials, u
   }
 }
 
-// x += alpha p; r -= alpha q; r . r
-__global__ void __launch_bounds__(kVT) k_bcg_update(int64_t n, const double* __restrict__ sc_in,
-                                                    const double* __restrict__ p, const double* __restrict__ q,
-                                                    double* __restrict__ x, double* __restrict__ r,
-                                                    double* partials, unsigned int* counter, double* rr_out) {
-  const double a = sc_in[kAlpha];
+// x += alpha p; r -= alpha q; r . r into sc[kRr]; the last CTA counts the
+// iteration and sets kDone when r . r <= sc[kTol].  A no-op once kBreak or
+// kDone is set.
+__global__ void __launch_bounds__(kVT) k_bcg_update(int64_t n, double* sc, const double* __restrict__ p,
+                                                    const double* __restrict__ q, double* __restrict__ x,
+                                                    double* __restrict__ r, double* partials, unsigned int* counter) {
+  if (sc[kBreak] != 0.0 || sc[kDone] != 0.0) return;
+  const double a = sc[kAlpha];
   double s = 0.0;
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
     x[i] += a * p[i];
@@ -440,7 +444,27 @@ __global__ void __launch_bounds__(kVT) k_bcg_update(int64_t n, const double* __r
     r[i] = ri;
     s += ri * ri;
   }
-  grid_reduce_finish(s, partials, counter, rr_out);
+  __shared__ double s_red[32];
+  __shared__ bool s_last;
+  const double b = block_sum_box(s, s_red);
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = b;
+    __threadfence();
+    s_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (s_last) {
+    __threadfence();
+    double t = 0.0;
+    for (unsigned k = threadIdx.x; k < gridDim.x; k += blockDim.x) t += __ldcg(&partials[k]);
+    t = block_sum_box(t, s_red);
+    if (threadIdx.x == 0) {
+      *counter = 0u;
+      sc[kRr] = t;
+      sc[kIters] += 1.0;
+      if (t <= sc[kTol]) sc[kDone] = 1.0;
+    }
+  }
 }
 
 // out = mask ? 0 : a - b (b may be null), and out . out (one thread per node,
@@ -462,13 +486,18 @@ __global__ void __launch_bounds__(kVT) k_bres64(int N, const double* __restrict_
   grid_reduce_finish(s, partials, counter, nrm_out);
 }
 
-__global__ void k_bcg_reset(double* sc) {
+// (re)start of the outer CG: scalars cleared, convergence threshold tol2 on
+// r . r; the executed-iteration count only at the start of a solve (full)
+__global__ void k_bcg_reset(double* sc, double tol2, int full) {
   sc[kRz] = 0.0;
   sc[kPq] = 0.0;
   sc[kAlpha] = 0.0;
   sc[kBeta] = 0.0;
   sc[kBreak] = 0.0;
+  sc[kDone] = 0.0;
   sc[kFirst] = 1.0;
+  sc[kTol] = tol2;
+  if (full) sc[kIters] = 0.0;
 }
 
 // x_soa[d N + lattice(v)] = scale * value for each Dirichlet dof (dof = 3 v + d)
@@ -490,7 +519,9 @@ __global__ void k_bset_bc(int64_t nbc, const int32_t* __restrict__ dofs, const d
 
 // Restriction (R = P^T of trilinear interpolation), coarse masked dofs zero.
 __global__ void k_brestrict(int cnx, int cny, int cnz, const float* __restrict__ f, int Nf,
-                            const uint8_t* __restrict__ cmask, float* __restrict__ c, int Nc) {
+                            const uint8_t* __restrict__ cmask, float* __restrict__ c, int Nc,
+                            const double* skip = nullptr) {
+  if (skip && (skip[0] != 0.0 || skip[1] != 0.0)) return;
   const int v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= Nc) return;
   const int cpx = cnx + 1, cpy = cny + 1;
@@ -523,7 +554,9 @@ __global__ void k_brestrict(int cnx, int cny, int cnz, const float* __restrict__
 // x_fine += P e (trilinear interpolation of the coarse correction), fine
 // masked dofs untouched (they stay zero).
 __global__ void k_bprolong_add(int cnx, int cny, const float* __restrict__ e, int Nc,
-                               const uint8_t* __restrict__ fmask, float* __restrict__ x, int Nf) {
+                               const uint8_t* __restrict__ fmask, float* __restrict__ x, int Nf,
+                               const double* skip = nullptr) {
+  if (skip && (skip[0] != 0.0 || skip[1] != 0.0)) return;
   const int v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= Nf) return;
   const int fpx = 2 * cnx + 1, fpy = 2 * cny + 1;
@@ -671,29 +704,55 @@ __global__ void k_bcoarse_w(BoxDims c, BoxDims f, const double* __restrict__ wf,
 
 // dinv = masked ? 0 : 1 / diag(K), diag from the tets around each node:
 // K_vv,dd = s [lam g_d^2 + mu g_d^2 + mu |g|^2], g the vertex's barycentric gradient.
-__global__ void k_bdinv(BoxDims d, double hx, double hy, double hz, double lam, double mu, const double* __restrict__ w,
-                        int wm, const uint8_t* __restrict__ mask, float* __restrict__ dinv) {
-  const int64_t v = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  if (v >= d.N) return;
-  const int i = int(v % d.px), j = int((v / d.px) % d.py), k = int(v / (int64_t(d.px) * d.py));
+// Diagonal of the unweighted tet stiffness, per hex corner: the tets whose
+// path passes through corner q and vol ((lam + mu) g_c^2 + mu |g|^2) of the
+// corner's gradient g in each (corners 0 and 7 lie on all six paths, the
+// others on two).  Built on the host per level.
+struct DinvTab {
+  int cnt[8];
+  int t[8][6];
+  double coef[8][6][3];
+};
+
+DinvTab make_dinv_tab(double hx, double hy, double hz, double lam, double mu) {
+  DinvTab T{};
   const double ih[3] = {1.0 / hx, 1.0 / hy, 1.0 / hz};
   const double vol = hx * hy * hz / 6.0;
-  double dg[3] = {0.0, 0.0, 0.0};
-  for (int q = 0; q < 8; ++q) {  // this node is corner q of hex (i, j, k) - offset(q)
-    const int hi = i - (q & 1), hj = j - ((q >> 1) & 1), hk = k - (q >> 2);
-    if (hi < 0 || hi >= d.nx || hj < 0 || hj >= d.ny || hk < 0 || hk >= d.nz) continue;
-    const int64_t h = hi + int64_t(d.nx) * (hj + int64_t(d.ny) * hk);
+  for (int q = 0; q < 8; ++q) {
+    T.cnt[q] = 0;
     for (int t = 0; t < 6; ++t)
       for (int m = 0; m < 4; ++m) {
         if (path_vertex(t, m) != q) continue;
         double g[3] = {0.0, 0.0, 0.0};
         if (m >= 1) g[path_axis(t, m - 1)] += ih[path_axis(t, m - 1)];
         if (m <= 2) g[path_axis(t, m)] -= ih[path_axis(t, m)];
-        const double s = vol * (wm ? w[t * d.H + h] : w[h]);
         const double gg = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) dg[c] += s * ((lam + mu) * g[c] * g[c] + mu * gg);
+        const int e = T.cnt[q]++;
+        T.t[q][e] = t;
+        for (int c = 0; c < 3; ++c) T.coef[q][e][c] = vol * ((lam + mu) * g[c] * g[c] + mu * gg);
       }
+  }
+  return T;
+}
+
+// dinv = 1 / diag K per node and component (0 on masked dofs), from the
+// weights (per hex or per tet) and the corner table
+__global__ void k_bdinv(BoxDims d, DinvTab T, const double* __restrict__ w, int wm, const uint8_t* __restrict__ mask,
+                        float* __restrict__ dinv) {
+  const int64_t v = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (v >= d.N) return;
+  const int i = int(v % d.px), j = int((v / d.px) % d.py), k = int(v / (int64_t(d.px) * d.py));
+  double dg[3] = {0.0, 0.0, 0.0};
+  for (int q = 0; q < 8; ++q) {  // this node is corner q of hex (i, j, k) - offset(q)
+    const int hi = i - (q & 1), hj = j - ((q >> 1) & 1), hk = k - (q >> 2);
+    if (hi < 0 || hi >= d.nx || hj < 0 || hj >= d.ny || hk < 0 || hk >= d.nz) continue;
+    const int64_t h = hi + int64_t(d.nx) * (hj + int64_t(d.ny) * hk);
+    const double wh = wm ? 0.0 : w[h];
+    for (int e = 0; e < T.cnt[q]; ++e) {
+      const double s = wm ? w[T.t[q][e] * d.H + h] : wh;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) dg[c] = fma(s, T.coef[q][e][c], dg[c]);
+    }
   }
   const uint8_t mk = mask[v];
 #pragma unroll
@@ -860,7 +919,7 @@ void set_dims(BoxLevel& L, int nx, int ny, int nz, double lx, double ly, double 
 
 template <typename T, int WM, bool CUBE, class In, class Out>
 void launch_box_t(const BoxLevel& L, const BoxGeo<T>& g, const T* w, const In& in, const Out& out, BoxRed red,
-                  cudaStream_t s, double p = 0.0, double pmin = 0.0) {
+                  cudaStream_t s, double p = 0.0, double pmin = 0.0, const double* skip = nullptr) {
   static int occupancy = 0;  // resident CTAs per SM of this instance
   if (occupancy == 0) {
     int o = 0;
@@ -869,7 +928,8 @@ void launch_box_t(const BoxLevel& L, const BoxGeo<T>& g, const T* w, const In& i
   }
   int kz = 2;
   const dim3 grid = box_grid(L.d, occupancy * num_sms(), &kz);
-  k_box<T, WM, CUBE, In, Out><<<grid, kBoxThreads, 0, s>>>(L.d, g, BoxW<T, WM>{w, L.d.H, p, pmin}, kz, in, out, red);
+  k_box<T, WM, CUBE, In, Out><<<grid, kBoxThreads, 0, s>>>(L.d, g, BoxW<T, WM>{w, L.d.H, p, pmin}, kz, in, out, red,
+                                                          skip);
   PA_LAUNCHED();
   g_box_launches += 1;
 }
@@ -877,17 +937,17 @@ void launch_box_t(const BoxLevel& L, const BoxGeo<T>& g, const T* w, const In& i
 // dispatch on the level's weight layout and hex shape
 template <typename T, class In, class Out>
 void launch_box(const BoxLevel& L, const BoxGeo<T>& g, const T* w, const In& in, const Out& out, BoxRed red,
-                cudaStream_t s) {
+                cudaStream_t s, const double* skip = nullptr) {
   if (L.wm) {
     if (L.cube)
-      launch_box_t<T, 1, true>(L, g, w, in, out, red, s);
+      launch_box_t<T, 1, true>(L, g, w, in, out, red, s, 0.0, 0.0, skip);
     else
-      launch_box_t<T, 1, false>(L, g, w, in, out, red, s);
+      launch_box_t<T, 1, false>(L, g, w, in, out, red, s, 0.0, 0.0, skip);
   } else {
     if (L.cube)
-      launch_box_t<T, 0, true>(L, g, w, in, out, red, s);
+      launch_box_t<T, 0, true>(L, g, w, in, out, red, s, 0.0, 0.0, skip);
     else
-      launch_box_t<T, 0, false>(L, g, w, in, out, red, s);
+      launch_box_t<T, 0, false>(L, g, w, in, out, red, s, 0.0, 0.0, skip);
   }
 }
 
@@ -1081,8 +1141,8 @@ bool boxmg_setup(Problem& P, const double* z) {
   for (size_t l = 0; l < H.L.size(); ++l) {
     BoxLevel& L = *H.L[l];
     const double* lw = l == 0 ? fw64 : L.w64.get();
-    k_bdinv<<<int((L.d.N + kVT - 1) / kVT), kVT, 0, s>>>(L.d, L.h[0], L.h[1], L.h[2], iso.lam, iso.mu, lw,
-                                                         l == 0 ? F.wm : 0, L.mask, L.dinv.get());
+    const DinvTab tab = make_dinv_tab(L.h[0], L.h[1], L.h[2], iso.lam, iso.mu);
+    k_bdinv<<<int((L.d.N + kVT - 1) / kVT), kVT, 0, s>>>(L.d, tab, lw, l == 0 ? F.wm : 0, L.mask, L.dinv.get());
     PA_LAUNCHED();
     g_box_launches += 1;
   }
@@ -1182,26 +1242,28 @@ const double* level_w64(const BoxHierarchy& H, size_t l) {
 }
 
 // the part of the V-cycle on level l and below that reads b (B) and writes x_out (O)
+// skip: the outer CG's kBreak / kDone flags (the launches become no-ops once set)
 template <typename B, typename O, bool RZ>
 void vcycle_level(const Problem& P, BoxHierarchy& H, size_t l, const B* b, O* xo, const double* rvec, double* sc,
-                  cudaStream_t s);
+                  cudaStream_t s, const double* skip);
 
-void vcycle(const Problem& P, BoxHierarchy& H, size_t l, cudaStream_t s) {
+void vcycle(const Problem& P, BoxHierarchy& H, size_t l, cudaStream_t s, const double* skip) {
   // levels >= 1: b and x in the level's FP32 buffers
   BoxLevel& L = *H.L[l];
   if (l + 1 == H.L.size()) {
     const int64_t n3 = 3 * L.d.N;
-    k_mg_dense_solve<<<int((32 * n3 + kVT - 1) / kVT), kVT, 0, s>>>(n3, L.nd, L.dense.get(), L.b.get(), L.x.get());
+    k_mg_dense_solve<<<int((32 * n3 + kVT - 1) / kVT), kVT, 0, s>>>(n3, L.nd, L.dense.get(), L.b.get(), L.x.get(),
+                                                                    skip);
     PA_LAUNCHED();
     g_box_launches += 1;
     return;
   }
-  vcycle_level<float, float, false>(P, H, l, L.b.get(), L.x.get(), nullptr, nullptr, s);
+  vcycle_level<float, float, false>(P, H, l, L.b.get(), L.x.get(), nullptr, nullptr, s, skip);
 }
 
 template <typename B, typename O, bool RZ>
 void vcycle_level(const Problem& P, BoxHierarchy& H, size_t l, const B* b, O* xo, const double* rvec, double* sc,
-                  cudaStream_t s) {
+                  cudaStream_t s, const double* skip) {
   BoxLevel& L = *H.L[l];
   BoxLevel& C = *H.L[l + 1];
   const float* ch = H.cheb.get() + 3 * l;
@@ -1211,24 +1273,24 @@ void vcycle_level(const Problem& P, BoxHierarchy& H, size_t l, const B* b, O* xo
   const int64_t N = L.d.N;
   // pre-smoothing from x = 0
   launch_box<float>(L, g, w, InDinvB<B>{b, L.dinv.get(), ch, N},
-                    OutPre<B>{L.x.get(), b, L.dinv.get(), ch, N}, red, s);
+                    OutPre<B>{L.x.get(), b, L.dinv.get(), ch, N}, red, s, skip);
   // residual, restricted to the coarse right-hand side
   launch_box<float>(L, g, w, InVec<float, float>{L.x.get(), nullptr, N}, OutRes<B>{L.r.get(), b, L.mask, N}, red,
-                    s);
+                    s, skip);
   k_brestrict<<<int((C.d.N + kVT - 1) / kVT), kVT, 0, s>>>(C.d.nx, C.d.ny, C.d.nz, L.r.get(), int(N), C.mask, C.b.get(),
-                                                           C.d.N);
+                                                           C.d.N, skip);
   PA_LAUNCHED();
   g_box_launches += 1;
-  vcycle(P, H, l + 1, s);
+  vcycle(P, H, l + 1, s, skip);
   // post-smoothing from x + P e
   k_bprolong_add<<<int((N + kVT - 1) / kVT), kVT, 0, s>>>(C.d.nx, C.d.ny, C.x.get(), int(C.d.N), L.mask, L.x.get(),
-                                                          int(N));
+                                                          int(N), skip);
   PA_LAUNCHED();
   g_box_launches += 1;
   launch_box<float>(L, g, w, InVec<float, float>{L.x.get(), nullptr, N}, OutPost1<B>{L.r.get(), b, L.dinv.get(), N},
-                    red, s);
+                    red, s, skip);
   launch_box<float>(L, g, w, InScaled{L.r.get(), ch, N},
-                    OutPost2<O, RZ>{xo, L.x.get(), L.r.get(), L.dinv.get(), ch, N, rvec, sc}, red, s);
+                    OutPost2<O, RZ>{xo, L.x.get(), L.r.get(), L.dinv.get(), ch, N, rvec, sc}, red, s, skip);
 }
 
 // y = K x (FP64, box kernel) with optional masks on input and output
@@ -1293,7 +1355,7 @@ bool solve_boxmg(Problem& P, const double* z, const double* b, double* x_out, co
   PA_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, s));
   PA_CUDA(cudaMemcpyAsync(r, bp, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
   PA_CUDA(cudaMemsetAsync(H.p0.get(), 0, sizeof(double) * n, s));
-  k_bcg_reset<<<1, 1, 0, s>>>(sc);
+  k_bcg_reset<<<1, 1, 0, s>>>(sc, tol2, 1);
   PA_LAUNCHED();
   // this solve's Chebyshev coefficients, read by the captured iteration
   {
@@ -1324,11 +1386,10 @@ bool solve_boxmg(Problem& P, const double* z, const double* b, double* x_out, co
       double* pnew = k == 0 ? H.p1.get() : H.p0.get();
       const int64_t before = g_box_launches;
       PA_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-      vcycle_level<double, double, true>(P, H, 0, r, zv, r, sc, s);
+      vcycle_level<double, double, true>(P, H, 0, r, zv, r, sc, s, sc + kBreak);
       launch_box<double>(F, box_geo<double>(F, P.ep), w64, InCgP{zv, pold, pnew, sc, N},
-                         OutCgQ{H.q.get(), zv, pold, mask, sc, N}, red, s);
-      k_bcg_update<<<vec_blocks(n), kVT, 0, s>>>(n, sc, pnew, H.q.get(), x, r, H.partials.get(), H.counter.get(),
-                                                 sc + kRr);
+                         OutCgQ{H.q.get(), zv, pold, mask, sc, N}, red, s, sc + kBreak);
+      k_bcg_update<<<vec_blocks(n), kVT, 0, s>>>(n, sc, pnew, H.q.get(), x, r, H.partials.get(), H.counter.get());
       g_box_launches += 1;
       cudaGraph_t graph = nullptr;
       const cudaError_t ce = cudaStreamEndCapture(s, &graph);
@@ -1348,21 +1409,35 @@ bool solve_boxmg(Problem& P, const double* z, const double* b, double* x_out, co
   int iters = 0, restarts = 0;
   double rr_true = bb;
   bool converged = false, breakdown = false;
-  double h2[2];
+  // Iterations run in batches of captured graphs with one host read per
+  // batch: the device counts the iterations it executes, marks convergence
+  // (r . r <= tol2) and breakdown, and every launch after either is a no-op.
+  // The batch after the first is the number of iterations the mean reduction
+  // so far predicts to convergence (at most 16).
+  constexpr int kFirstBatch = 4, kMaxBatch = 16;
+  double h4[4];  // r . r, breakdown, done, executed iterations
   while (!converged && iters < max_iters && !breakdown) {
-    double rr = bb;
-    while (iters < max_iters) {
-      PA_CUDA(cudaGraphLaunch(H.gexec[iters & 1], s));
-      g_box_launches += per_iter;
-      ++iters;
-      PA_CUDA(cudaMemcpyAsync(h2, sc + kRr, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    const int cycle_start = iters;
+    const double rr_start = iters == 0 ? bb : rr_true;
+    int batch = std::min(kFirstBatch, max_iters - iters);
+    while (true) {
+      for (int b = 0; b < batch; ++b) {
+        PA_CUDA(cudaGraphLaunch(H.gexec[(iters + b) & 1], s));
+        g_box_launches += per_iter;
+      }
+      PA_CUDA(cudaMemcpyAsync(h4, sc + kRr, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
       PA_CUDA(cudaStreamSynchronize(s));
-      rr = h2[0];
-      if (h2[1] != 0.0) {
+      iters = int(h4[3]);
+      if (h4[1] != 0.0) {
         breakdown = true;
         break;
       }
-      if (rr <= tol2) break;
+      if (h4[2] != 0.0 || iters >= max_iters) break;
+      const int done_in_cycle = iters - cycle_start;
+      const double rate = done_in_cycle > 0 && rr_start > 0.0 ? std::pow(h4[0] / rr_start, 1.0 / done_in_cycle) : 0.0;
+      int m = kFirstBatch;
+      if (rate > 0.0 && rate < 1.0 && h4[0] > tol2) m = int(std::ceil(std::log(tol2 / h4[0]) / std::log(rate)));
+      batch = std::max(1, std::min({m, kMaxBatch, max_iters - iters}));
     }
     if (breakdown) break;
     // confirm on the true residual r = b' - K x (p and the scalars restart)
@@ -1375,7 +1450,7 @@ bool solve_boxmg(Problem& P, const double* z, const double* b, double* x_out, co
     converged = rr_true <= tol2;
     if (!converged && iters < max_iters) {
       ++restarts;
-      k_bcg_reset<<<1, 1, 0, s>>>(sc);
+      k_bcg_reset<<<1, 1, 0, s>>>(sc, tol2, 0);
       PA_LAUNCHED();
     }
   }

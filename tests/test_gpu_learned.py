@@ -159,3 +159,29 @@ def test_untrained_network_flexible_cg_is_jacobi_pcg(pa):
     # flexible CG stalls into the fallback instead)
     assert abs(sl["iterations"] - sj["iterations"]) <= 0.25 * sj["iterations"] + 32, (sl, sj)
     assert np.abs(ul - uj).max() <= 1e-6 * np.abs(uj).max()
+
+
+def test_network_forward_exact_when_every_sum_is_exact(pa):
+    """Weights, biases and inputs that are small integers (sparse weights in
+    {-1, 0, 1}) make every layer's FP32 sum an exact integer whatever the
+    accumulation order, and the BF16 roundings of equal values agree: the
+    tensor-core forward must then equal the oracle bit for bit, so any error
+    in the MMA operand layouts or the halo gather shows at full size."""
+    grid = (11, 19, 3)
+    rng = np.random.default_rng(31)
+    p = np.zeros(np_net.num_params(), np.float32)
+    o = 0
+    for ci, co in zip(np_net.CIN, np_net.COUT):
+        n = co * ci * 27
+        p[o:o + n] = rng.choice([-1.0, 0.0, 1.0], size=n, p=[0.04, 0.92, 0.04])
+        o += n
+        p[o:o + co] = rng.integers(-1, 2, co)
+        o += co
+    pc = pa.LearnedPreconditioner(grid, seed=1)
+    pc.set_params(p)
+    f = rng.integers(-1, 3, size=(np.prod(grid), 5)).astype(np.float32)
+    got = pc.forward(f).reshape(-1, 3)
+    ref, acts = np_net.forward(p, f, grid)
+    assert max(np.abs(a).max() for a in acts[1:]) > 4  # the layers are not trivially zero
+    assert np.abs(ref).max() > 4
+    assert np.array_equal(got, ref.astype(np.float32)), np.abs(got - ref).max()
