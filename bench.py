@@ -605,7 +605,7 @@ def run_ours(args):
         "config": {"workload": f"SIMP cantilever {dims[0]}x{dims[1]}x{dims[2]} hex x 6 tets, "
                                f"Problem::solution to relres {args.rel_tol:g}",
                    "cells": C, "nodes": N, "dofs": ndof, "method": args.method, "mg_coarse": args.mg_coarse, "parallelism": f"replicas x{world}",
-                   "preconditioner": ("geometric multigrid V-cycle: box hierarchy to the coarsest even level, "
+                   "preconditioner": ("geometric multigrid V-cycle: box hierarchy of ceil(n/2) hexes per axis per level, "
                                       "Chebyshev(2) smoothing in D^-1 K before and after the coarse correction, "
                                       "trilinear transfers, dense FP64 inverse on the coarsest level")
                    if args.method == "mg" else "Jacobi",

@@ -267,7 +267,8 @@ pa_status pa_apply_block_constraints(pa_problem* problem, double* entries, doubl
 #define PA_SOLVER_PCG_FP64 0  /* matrix-free Jacobi-PCG, FP64 throughout */
 #define PA_SOLVER_PCG_MIXED 1 /* FP32 apply/vectors, FP64 dots, FP64 true-residual updates */
 #define PA_SOLVER_PCG_MG 3    /* FP64 CG preconditioned by a geometric multigrid V-cycle (FP32 Chebyshev
-                                 smoothing); box meshes from pa_mesh_create_box with even hex counts */
+                                 smoothing); meshes that are a structured box under some node, cell and
+                                 vertex numbering (pa_mesh_create_box or arrays), any hex counts */
 #define PA_SOLVER_FCG_LEARNED 2 /* flexible CG preconditioned by the problem's learned network
                                    (pa_problem_set_preconditioner), precision as PA_SOLVER_PCG_MIXED;
                                    continues as PA_SOLVER_PCG_MIXED when the residual stalls or the

@@ -470,7 +470,10 @@ pa_status pa_vf_gradient_z(pa_problem* problem, const double* u, const double* z
     const double* dz = st.in(z, P.nz(), "z");
     const int64_t n = P.ep.layout == PA_CONTROL_CELL ? 12 * P.C() : 3 * P.mesh->B;
     double* de = st.out(entries, n, "entries");
-    pa::launch_gradient_z(P, du, dz, de, P.stream);
+    if (pa::box_entry_eligible(P))
+      pa::box_entry_gradient_z(P, dz, du, de);
+    else
+      pa::launch_gradient_z(P, du, dz, de, P.stream);
     st.finish();
   });
 }

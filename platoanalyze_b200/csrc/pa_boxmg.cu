@@ -31,10 +31,18 @@
 //    the lattice (no cell permutation, no atomics), and a fine level whose six
 //    tets of every hex share one weight (per-hex densities) reads one weight
 //    per hex.
+//  * a level with an odd hex count along an axis is coarsened to ceil(n / 2)
+//    hexes: the coarse level spans one more fine hex layer, which holds no
+//    fine node and counts as weight zero in the coarse weights, so every box
+//    size has a hierarchy down to a few hundred dofs;
+//  * the kernels of an iteration are programmatic dependent launches: each
+//    may be scheduled while its predecessor finishes, and waits for it before
+//    touching memory.
 // Requirements: a box lattice (mesh_make_box, or arrays recognised by
-// detect_lattice: the solver permutes b and x at its boundary) with even hex
-// counts, an elastic operator (J2 tangent solves keep pa_mg.cu), one part.
+// detect_lattice: the solver permutes b and x at its boundary), an elastic
+// operator (J2 tangent solves keep pa_mg.cu), one part.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <memory>
 #include <vector>
@@ -435,6 +443,8 @@ __device__ __forceinline__ void grid_reduce_finish(double v, double* partials, u
 __global__ void __launch_bounds__(kVT) k_bcg_update(int64_t n, double* sc, const double* __restrict__ p,
                                                     const double* __restrict__ q, double* __restrict__ x,
                                                     double* __restrict__ r, double* partials, unsigned int* counter) {
+  pdl_trigger();
+  pdl_wait();
   if (sc[kBreak] != 0.0 || sc[kDone] != 0.0) return;
   const double a = sc[kAlpha];
   double s = 0.0;
@@ -518,58 +528,62 @@ __global__ void k_bset_bc(int64_t nbc, const int32_t* __restrict__ dofs, const d
 }
 
 // Restriction (R = P^T of trilinear interpolation), coarse masked dofs zero.
-__global__ void k_brestrict(int cnx, int cny, int cnz, const float* __restrict__ f, int Nf,
-                            const uint8_t* __restrict__ cmask, float* __restrict__ c, int Nc,
-                            const double* skip = nullptr) {
+// The coarse level spans 2 c.nx fine hexes along x (and so on), at least the
+// fine level's f.nx: a fine level with an odd count is padded by one hex
+// layer that holds no fine node.
+__global__ void k_brestrict(BoxDims c, BoxDims f, const float* __restrict__ fv_in, const uint8_t* __restrict__ cmask,
+                            float* __restrict__ cv_out, const double* skip) {
+  pdl_trigger();
+  pdl_wait();
   if (skip && (skip[0] != 0.0 || skip[1] != 0.0)) return;
   const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  const int Nc = int(c.N), Nf = int(f.N);
   if (v >= Nc) return;
-  const int cpx = cnx + 1, cpy = cny + 1;
-  const int I = v % cpx, J = (v / cpx) % cpy, K = v / (cpx * cpy);
-  const int fpx = 2 * cnx + 1, fpy = 2 * cny + 1, fpz = 2 * cnz + 1;
+  const int I = v % c.px, J = (v / c.px) % c.py, K = v / (c.px * c.py);
   float s[3] = {0.f, 0.f, 0.f};
   for (int dc = -1; dc <= 1; ++dc) {
     const int k = 2 * K + dc;
-    if (k < 0 || k >= fpz) continue;
+    if (k < 0 || k >= f.pz) continue;
     const float wc = dc ? 0.5f : 1.0f;
     for (int db = -1; db <= 1; ++db) {
       const int j = 2 * J + db;
-      if (j < 0 || j >= fpy) continue;
+      if (j < 0 || j >= f.py) continue;
       const float wb = wc * (db ? 0.5f : 1.0f);
       for (int da = -1; da <= 1; ++da) {
         const int i = 2 * I + da;
-        if (i < 0 || i >= fpx) continue;
+        if (i < 0 || i >= f.px) continue;
         const float w = wb * (da ? 0.5f : 1.0f);
-        const int fv = i + fpx * (j + fpy * k);
+        const int fv = i + f.px * (j + f.py * k);
 #pragma unroll
-        for (int d = 0; d < 3; ++d) s[d] += w * f[d * Nf + fv];
+        for (int d = 0; d < 3; ++d) s[d] += w * fv_in[d * Nf + fv];
       }
     }
   }
   const uint8_t mk = cmask[v];
 #pragma unroll
-  for (int d = 0; d < 3; ++d) c[d * Nc + v] = ((mk >> d) & 1) ? 0.f : s[d];
+  for (int d = 0; d < 3; ++d) cv_out[d * Nc + v] = ((mk >> d) & 1) ? 0.f : s[d];
 }
 
 // x_fine += P e (trilinear interpolation of the coarse correction), fine
-// masked dofs untouched (they stay zero).
-__global__ void k_bprolong_add(int cnx, int cny, const float* __restrict__ e, int Nc,
-                               const uint8_t* __restrict__ fmask, float* __restrict__ x, int Nf,
-                               const double* skip = nullptr) {
+// masked dofs untouched (they stay zero).  Fine node i lies at coarse
+// position i / 2; every coarse node it reads exists (2 c.nx >= f.nx).
+__global__ void k_bprolong_add(BoxDims c, BoxDims f, const float* __restrict__ e, const uint8_t* __restrict__ fmask,
+                               float* __restrict__ x, const double* skip) {
+  pdl_trigger();
+  pdl_wait();
   if (skip && (skip[0] != 0.0 || skip[1] != 0.0)) return;
   const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  const int Nc = int(c.N), Nf = int(f.N);
   if (v >= Nf) return;
-  const int fpx = 2 * cnx + 1, fpy = 2 * cny + 1;
-  const int i = v % fpx, j = (v / fpx) % fpy, k = v / (fpx * fpy);
-  const int cpx = cnx + 1, cpy = cny + 1;
+  const int i = v % f.px, j = (v / f.px) % f.py, k = v / (f.px * f.py);
   const int ia = i >> 1, ja = j >> 1, ka = k >> 1;
   const int ni = (i & 1) + 1, nj = (j & 1) + 1, nk = (k & 1) + 1;
   const float w = (ni == 1 ? 1.f : 0.5f) * (nj == 1 ? 1.f : 0.5f) * (nk == 1 ? 1.f : 0.5f);
   float s[3] = {0.f, 0.f, 0.f};
-  for (int c = 0; c < nk; ++c)
+  for (int cc = 0; cc < nk; ++cc)
     for (int b = 0; b < nj; ++b)
       for (int a = 0; a < ni; ++a) {
-        const int cv = (ia + a) + cpx * ((ja + b) + cpy * (ka + c));
+        const int cv = (ia + a) + c.px * ((ja + b) + c.py * (ka + cc));
 #pragma unroll
         for (int d = 0; d < 3; ++d) s[d] += e[d * Nc + cv];
       }
@@ -681,7 +695,9 @@ __global__ void k_bweights(BoxDims d, const double* __restrict__ z, int layout, 
   if (!same) atomicOr(differ, 1u);
 }
 
-// Coarse hex weight = mean of the 48 child tets (per-hex or tet-major fine weights).
+// Coarse hex weight = mean of the 48 child tets (per-hex or tet-major fine
+// weights); the children in a padding layer (2 I + a >= f.nx, ...) count as
+// weight zero, so a coarse hex half outside the fine box has half the weight.
 __global__ void k_bcoarse_w(BoxDims c, BoxDims f, const double* __restrict__ wf, int wm, double* __restrict__ w64,
                             float* __restrict__ w32) {
   const int64_t h = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
@@ -691,6 +707,7 @@ __global__ void k_bcoarse_w(BoxDims c, BoxDims f, const double* __restrict__ wf,
   for (int cc = 0; cc < 2; ++cc)
     for (int b = 0; b < 2; ++b)
       for (int a = 0; a < 2; ++a) {
+        if (2 * I + a >= f.nx || 2 * J + b >= f.ny || 2 * K + cc >= f.nz) continue;
         const int64_t fh = (2 * I + a) + int64_t(f.nx) * ((2 * J + b) + int64_t(f.ny) * (2 * K + cc));
         if (wm)
           for (int t = 0; t < 6; ++t) s += wf[t * f.H + fh];
@@ -928,9 +945,8 @@ void launch_box_t(const BoxLevel& L, const BoxGeo<T>& g, const T* w, const In& i
   }
   int kz = 2;
   const dim3 grid = box_grid(L.d, occupancy * num_sms(), &kz);
-  k_box<T, WM, CUBE, In, Out><<<grid, kBoxThreads, 0, s>>>(L.d, g, BoxW<T, WM>{w, L.d.H, p, pmin}, kz, in, out, red,
-                                                          skip);
-  PA_LAUNCHED();
+  launch_pdl(k_box<T, WM, CUBE, In, Out>, grid, dim3(kBoxThreads), 0, s, L.d, g, BoxW<T, WM>{w, L.d.H, p, pmin}, kz,
+             in, out, red, skip);
   g_box_launches += 1;
 }
 
@@ -961,28 +977,49 @@ int64_t max_grid_blocks(const BoxHierarchy& H) {
   return m;
 }
 
-// coarse masks by injection (fine node (2I, 2J, 2K))
+// coarse masks by injection (fine node (2I, 2J, 2K)); a coarse node beyond a
+// padded fine level (2 I > f.nx) takes the mask of the last fine node plane
 void coarse_mask(const BoxLevel& f, BoxLevel& c, const std::vector<uint8_t>& fmask, std::vector<uint8_t>& cmask) {
   cmask.assign(size_t(c.d.N), 0);
   for (int64_t K = 0; K < c.d.pz; ++K)
     for (int64_t J = 0; J < c.d.py; ++J)
-      for (int64_t I = 0; I < c.d.px; ++I)
-        cmask[size_t(I + c.d.px * (J + c.d.py * K))] = fmask[size_t(2 * I + f.d.px * (2 * J + f.d.py * 2 * K))];
+      for (int64_t I = 0; I < c.d.px; ++I) {
+        const int64_t i = std::min<int64_t>(2 * I, f.d.nx), j = std::min<int64_t>(2 * J, f.d.ny),
+                      k = std::min<int64_t>(2 * K, f.d.nz);
+        cmask[size_t(I + c.d.px * (J + c.d.py * K))] = fmask[size_t(i + f.d.px * (j + f.d.py * k))];
+      }
+}
+
+// Hex counts of the multigrid levels of an nx x ny x nz box: the next level
+// has ceil(n / 2) hexes per axis (an odd level is padded by one hex layer of
+// weight zero), while every axis has at least 4 hexes, or at least 2 while
+// the level still has more than kDenseMax dofs; the last level is the
+// coarsest, solved by a dense inverse.
+constexpr int64_t kDenseMax = 2048;
+std::vector<std::array<int, 3>> box_level_counts(const int* n0) {
+  std::vector<std::array<int, 3>> out;
+  std::array<int, 3> n = {n0[0], n0[1], n0[2]};
+  while (true) {
+    out.push_back(n);
+    const int mn = std::min(std::min(n[0], n[1]), n[2]);
+    const int64_t dofs = 3LL * (n[0] + 1) * (n[1] + 1) * (n[2] + 1);
+    if (!(mn >= 4 || (mn >= 2 && dofs > kDenseMax))) break;
+    for (int a = 0; a < 3; ++a) n[a] = (n[a] + 1) / 2;
+  }
+  return out;
 }
 
 }  // namespace
 
 // True when the box kernels can run this problem's multigrid solve: a box
-// of mesh_make_box with even hex counts, one part, and a coarsest level (the
-// box halved while every axis stays even with at least 4 hexes) of at most
-// 2048 dofs for the dense inverse.
+// lattice (any hex counts), one part, at least one coarse level, and a
+// coarsest level of at most 2048 dofs for the dense inverse.
 bool boxmg_eligible(const Problem& P) {
   const Mesh& m = *P.mesh;
-  if (!box_apply_eligible(P) || m.lat_n[0] % 2 || m.lat_n[1] % 2 || m.lat_n[2] % 2) return false;
-  int n[3] = {m.lat_n[0], m.lat_n[1], m.lat_n[2]};
-  while (!(n[0] % 2 || n[1] % 2 || n[2] % 2 || std::min(std::min(n[0], n[1]), n[2]) < 4))
-    for (int a = 0; a < 3; ++a) n[a] /= 2;
-  return 3LL * (n[0] + 1) * (n[1] + 1) * (n[2] + 1) <= 2048;
+  if (!box_apply_eligible(P)) return false;
+  const auto lv = box_level_counts(m.lat_n);
+  const auto& c = lv.back();
+  return lv.size() >= 2 && 3LL * (c[0] + 1) * (c[1] + 1) * (c[2] + 1) <= kDenseMax;
 }
 
 // True when the box kernel can apply this problem's operator (pa_apply).
@@ -1004,14 +1041,18 @@ void boxmg_setup_levels(Problem& P) {
   cudaStream_t s = P.stream;
   boxmg_release(P);
   std::unique_ptr<BoxHierarchy> H(new BoxHierarchy());
-  int n[3] = {m.lat_n[0], m.lat_n[1], m.lat_n[2]};
   for (int a = 0; a < 3; ++a) {
-    H->fine_n[a] = n[a];
+    H->fine_n[a] = m.lat_n[a];
     H->fine_l[a] = m.lat_l[a];
   }
-  for (int l = 0;; ++l) {
+  const auto counts = box_level_counts(m.lat_n);
+  double len[3] = {m.lat_l[0], m.lat_l[1], m.lat_l[2]};
+  for (size_t l = 0; l < counts.size(); ++l) {
+    const auto& n = counts[l];
+    if (l > 0)  // hexes twice the size of the level above (a padded level spans more)
+      for (int a = 0; a < 3; ++a) len[a] = 2.0 * H->L[l - 1]->h[a] * n[a];
     std::unique_ptr<BoxLevel> L(new BoxLevel());
-    set_dims(*L, n[0], n[1], n[2], m.lat_l[0], m.lat_l[1], m.lat_l[2]);
+    set_dims(*L, n[0], n[1], n[2], len[0], len[1], len[2]);
     const int64_t n3 = 3 * L->d.N;
     L->dinv.resize(n3);
     L->x.resize(n3);
@@ -1024,8 +1065,6 @@ void boxmg_setup_levels(Problem& P) {
       L->mask = L->own_mask.get();
     }
     H->L.push_back(std::move(L));
-    if (n[0] % 2 || n[1] % 2 || n[2] % 2 || std::min(std::min(n[0], n[1]), n[2]) < 4) break;
-    for (int a = 0; a < 3; ++a) n[a] /= 2;
   }
   const BoxLevel& F = *H->L[0];
   H->w64t.resize(6 * F.d.H);
@@ -1252,9 +1291,8 @@ void vcycle(const Problem& P, BoxHierarchy& H, size_t l, cudaStream_t s, const d
   BoxLevel& L = *H.L[l];
   if (l + 1 == H.L.size()) {
     const int64_t n3 = 3 * L.d.N;
-    k_mg_dense_solve<<<int((32 * n3 + kVT - 1) / kVT), kVT, 0, s>>>(n3, L.nd, L.dense.get(), L.b.get(), L.x.get(),
-                                                                    skip);
-    PA_LAUNCHED();
+    launch_pdl(k_mg_dense_solve, dim3(unsigned((32 * n3 + kVT - 1) / kVT)), dim3(kVT), 0, s, n3, L.nd,
+               L.dense.get(), L.b.get(), L.x.get(), skip);
     g_box_launches += 1;
     return;
   }
@@ -1277,15 +1315,13 @@ void vcycle_level(const Problem& P, BoxHierarchy& H, size_t l, const B* b, O* xo
   // residual, restricted to the coarse right-hand side
   launch_box<float>(L, g, w, InVec<float, float>{L.x.get(), nullptr, N}, OutRes<B>{L.r.get(), b, L.mask, N}, red,
                     s, skip);
-  k_brestrict<<<int((C.d.N + kVT - 1) / kVT), kVT, 0, s>>>(C.d.nx, C.d.ny, C.d.nz, L.r.get(), int(N), C.mask, C.b.get(),
-                                                           C.d.N, skip);
-  PA_LAUNCHED();
+  launch_pdl(k_brestrict, dim3(unsigned((C.d.N + kVT - 1) / kVT)), dim3(kVT), 0, s, C.d, L.d, L.r.get(), C.mask,
+             C.b.get(), skip);
   g_box_launches += 1;
   vcycle(P, H, l + 1, s, skip);
   // post-smoothing from x + P e
-  k_bprolong_add<<<int((N + kVT - 1) / kVT), kVT, 0, s>>>(C.d.nx, C.d.ny, C.x.get(), int(C.d.N), L.mask, L.x.get(),
-                                                          int(N), skip);
-  PA_LAUNCHED();
+  launch_pdl(k_bprolong_add, dim3(unsigned((N + kVT - 1) / kVT)), dim3(kVT), 0, s, C.d, L.d, C.x.get(), L.mask,
+             L.x.get(), skip);
   g_box_launches += 1;
   launch_box<float>(L, g, w, InVec<float, float>{L.x.get(), nullptr, N}, OutPost1<B>{L.r.get(), b, L.dinv.get(), N},
                     red, s, skip);
@@ -1389,7 +1425,8 @@ bool solve_boxmg(Problem& P, const double* z, const double* b, double* x_out, co
       vcycle_level<double, double, true>(P, H, 0, r, zv, r, sc, s, sc + kBreak);
       launch_box<double>(F, box_geo<double>(F, P.ep), w64, InCgP{zv, pold, pnew, sc, N},
                          OutCgQ{H.q.get(), zv, pold, mask, sc, N}, red, s, sc + kBreak);
-      k_bcg_update<<<vec_blocks(n), kVT, 0, s>>>(n, sc, pnew, H.q.get(), x, r, H.partials.get(), H.counter.get());
+      launch_pdl(k_bcg_update, dim3(unsigned(vec_blocks(n))), dim3(kVT), 0, s, n, sc, pnew, H.q.get(), x, r,
+                 H.partials.get(), H.counter.get());
       g_box_launches += 1;
       cudaGraph_t graph = nullptr;
       const cudaError_t ce = cudaStreamEndCapture(s, &graph);
@@ -1652,6 +1689,100 @@ __global__ void __launch_bounds__(256) k_benergy(BoxDims d, double ih0, double i
   if (threadIdx.x == 0) partials[blockIdx.x] = b;
 }
 
+// VectorFunction::gradient_z with per-cell controls: dR/dz of every cell, 12
+// values in the cell's own vertex order (vals[12 c + 3 n + d]): one thread per
+// tet.  Cell c = 6 h + t is path tet t of hex h, whose barycentric gradients
+// are g_0 = -e_a0, g_m = e_a(m-1) - e_am, g_3 = e_a2 (axes a_m of the path,
+// over the hex side), so the nodal force of path vertex m is the difference
+// of two stress columns.  The cell's node ids give each vertex slot's corner
+// (any vertex order of a template tet).  A warp stages its 32 cells' 384
+// values in shared memory and writes them as contiguous 256-byte rows.
+__global__ void __launch_bounds__(256) k_bgradient_z(BoxDims d, double ih0, double ih1, double ih2, double vol,
+                                                     Iso<double> iso, double p, double pmin,
+                                                     const int4* __restrict__ cells, const double* __restrict__ u,
+                                                     const double* __restrict__ z, double* __restrict__ vals) {
+  constexpr int kRow = 13;  // staging stride per cell (odd: two-way bank conflicts at most)
+  __shared__ double stage[8][32 * kRow];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t C = 6 * d.H;
+  const int64_t c0 = blockIdx.x * int64_t(blockDim.x) + 32 * w;
+  const int64_t c = c0 + lane;
+  double* st = stage[w] + kRow * lane;
+  if (c < C) {
+    const int64_t h = c / 6;
+    const int t = int(c - 6 * h);
+    const int i = int(h % d.nx), j = int((h / d.nx) % d.ny), k = int(h / (int64_t(d.nx) * d.ny));
+    const int plane = d.px * d.py;
+    const int b0 = i + d.px * (j + d.py * k);
+    const double ih[3] = {ih0, ih1, ih2};
+    int ax[3], off[4];
+    double uv[4][3];
+    int q = 0;
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      if (m > 0) {
+        ax[m - 1] = path_axis(t, m - 1);
+        q |= 1 << ax[m - 1];
+      }
+      off[m] = (q & 1) + d.px * ((q >> 1) & 1) + plane * (q >> 2);
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) uv[m][cc] = u[3 * int64_t(b0 + off[m]) + cc];
+    }
+    double du[3][3];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      const int a = ax[m];
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) du[cc][a] = (uv[m + 1][cc] - uv[m][cc]) * ih[a];
+    }
+    const double e[6] = {du[0][0], du[1][1], du[2][2], du[1][2] + du[2][1], du[0][2] + du[2][0],
+                         du[0][1] + du[1][0]};
+    double sg[6];
+    tet_stress(iso, vol * simp_deriv(z[c], p, pmin), e, sg);
+    // stress column a (Voigt: 0 xx, 1 yy, 2 zz, 3 yz, 4 xz, 5 xy) times ih[a]
+    auto col = [&](int a, double (&o)[3]) {
+      const double s = ih[a];
+      o[0] = s * (a == 0 ? sg[0] : a == 1 ? sg[5] : sg[4]);
+      o[1] = s * (a == 0 ? sg[5] : a == 1 ? sg[1] : sg[3]);
+      o[2] = s * (a == 0 ? sg[4] : a == 1 ? sg[3] : sg[2]);
+    };
+    double f[4][3];
+    {
+      double s0[3], s1[3], s2[3];
+      col(ax[0], s0);
+      col(ax[1], s1);
+      col(ax[2], s2);
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) {
+        f[0][cc] = -s0[cc];
+        f[1][cc] = s0[cc] - s1[cc];
+        f[2][cc] = s1[cc] - s2[cc];
+        f[3][cc] = s2[cc];
+      }
+    }
+    const int4 cv = cells[c];
+    const int vs[4] = {cv.x - b0, cv.y - b0, cv.z - b0, cv.w - b0};
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+      double r[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+      for (int m = 0; m < 4; ++m)
+        if (vs[n] == off[m])
+#pragma unroll
+          for (int cc = 0; cc < 3; ++cc) r[cc] = f[m][cc];
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) st[3 * n + cc] = r[cc];
+    }
+  }
+  __syncwarp();
+  const int64_t base = 12 * c0, end = 12 * C;
+#pragma unroll
+  for (int r = 0; r < 12; ++r) {
+    const int e = 32 * r + lane;
+    if (base + e < end) vals[base + e] = stage[w][kRow * (e / 12) + e % 12];
+  }
+}
+
 __global__ void k_bsum_partials(int n, const double* __restrict__ partials, double* __restrict__ out) {
   __shared__ double red[32];
   double v = 0.0;
@@ -1677,6 +1808,17 @@ void box_entry_apply(Problem& P, const double* z, const double* u, double* y) {
     launch_box_t<double, 2, true>(F, g, z, InAoS64{u}, OutAoS64{y}, red, P.stream, P.ep.p, P.ep.pmin);
   else
     launch_box_t<double, 2, false>(F, g, z, InAoS64{u}, OutAoS64{y}, red, P.stream, P.ep.p, P.ep.pmin);
+}
+
+void box_entry_gradient_z(Problem& P, const double* z, const double* u, double* vals) {
+  boxmg_ensure(P);
+  const BoxLevel& F = *P.boxmg->L[0];
+  const double vol = F.h[0] * F.h[1] * F.h[2] / 6.0;
+  const int64_t C = 6 * F.d.H;
+  k_bgradient_z<<<int((C + 255) / 256), 256, 0, P.stream>>>(
+      F.d, 1.0 / F.h[0], 1.0 / F.h[1], 1.0 / F.h[2], vol, P.ep.iso(), P.ep.p, P.ep.pmin,
+      reinterpret_cast<const int4*>(P.mesh->d_cells.get()), u, z, vals);
+  PA_LAUNCHED();
 }
 
 void box_entry_energy(Problem& P, const double* z, const double* u, double* value, double* grad_z) {

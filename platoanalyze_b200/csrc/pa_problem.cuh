@@ -88,14 +88,16 @@ void mg_release(Problem& P);
 // Structured boxes (pa_boxmg.cu): the box kernel of pa_box.cuh applies the
 // operator; multigrid CG with every level on it.
 // Per-cell entry points on a box mesh in its own numbering with per-cell
-// controls: y = K(z) u (interleaved) and the internal energy (value, one
-// device double; may be null) with dF/dz per cell (may be null).
+// controls: y = K(z) u (interleaved), the internal energy (value, one
+// device double; may be null) with dF/dz per cell (may be null), and dR/dz
+// per cell (12 values in each cell's vertex order).
 bool box_entry_eligible(const Problem& P);
 // The assembled K(z) (block CRS entries) on a box mesh in its own numbering
 // with sorted columns; false (nothing launched) on any other mesh.
 bool box_gradient_u(Problem& P, const double* z, double* entries);
 void box_entry_apply(Problem& P, const double* z, const double* u, double* y);
 void box_entry_energy(Problem& P, const double* z, const double* u, double* value, double* grad_z);
+void box_entry_gradient_z(Problem& P, const double* z, const double* u, double* vals);
 bool box_apply_eligible(const Problem& P);
 bool boxmg_eligible(const Problem& P);
 // false (nothing written) when the coarsest operator is singular

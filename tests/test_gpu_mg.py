@@ -43,10 +43,11 @@ def test_mg_matches_the_oracle_and_fp64_pcg(pa, oracle_lib, dims):
 
 @pytest.mark.parametrize("dims", [(16, 8, 8), (40, 20, 20)])
 def test_mg_coarse_direct_matches_chebyshev(pa, dims):
-    """The dense Gauss-Jordan inverse on the coarsest level (4x2x2 hexes:
-    135 dofs, 3 elimination blocks; 10x5x5 as for 160x80x80: 1188 dofs, 19
-    blocks) against the degree-40 Chebyshev coarse solve: the same solution,
-    no more outer iterations (an exact coarse solve), far fewer launches."""
+    """The box multigrid with its dense Gauss-Jordan inverse on the coarsest
+    level (4x2x2 hexes: 135 dofs; 5x3x3 as for 160x80x80: 288 dofs, 5
+    elimination blocks) against the tile-kernel multigrid with the degree-40
+    Chebyshev coarse solve: the same solution, no more outer iterations, far
+    fewer launches."""
     mesh, prob, faces, dofs, z = _cantilever(pa, dims, 7)
     u_d, st_d = prob.solution(z, options=pa.SolveOptions("mg", rel_tol=1e-10))
     u_c, st_c = prob.solution(z, options=pa.SolveOptions("mg", rel_tol=1e-10, mg_coarse="chebyshev"))
@@ -73,8 +74,8 @@ def test_mg_inhomogeneous_dirichlet_and_reuse(pa):
 
 def test_mg_accepts_array_boxes_and_refuses_unsupported_meshes(pa):
     """A box given as arrays is recognised as a lattice (the box kernels solve
-    it); with the box kernels switched off, and with an odd hex count, the
-    multigrid method refuses."""
+    it); with the box kernels switched off the multigrid method refuses it,
+    and an odd hex count, which the box multigrid solves."""
     from oracle import np_ref
     from platoanalyze_b200._abi import PaError
     cells, coords = np_ref.box_mesh(8, 4, 4, 8.0, 4.0, 4.0)
@@ -89,10 +90,12 @@ def test_mg_accepts_array_boxes_and_refuses_unsupported_meshes(pa):
     m.set_box_kernels(False)
     with pytest.raises(PaError):
         prob.solution(np.ones(m.num_cells), options=pa.SolveOptions("mg"))
-    m2 = pa.Mesh.box(7, 4, 4, 7.0, 4.0, 4.0)  # odd hex count
-    prob2 = pa.Problem(m2, 1.0, 0.3, 3.0, 1e-9, control_layout="cell")
+    m2, prob2, _, _, z2 = _cantilever(pa, (7, 4, 4), 3)  # odd hex count
+    u3, st3 = prob2.solution(z2, options=pa.SolveOptions("mg"))
+    assert st3["converged"], st3
+    m2.set_box_kernels(False)
     with pytest.raises(PaError):
-        prob2.solution(np.ones(m2.num_cells), options=pa.SolveOptions("mg"))
+        prob2.solution(z2, options=pa.SolveOptions("mg"))
 
 
 def test_mg_above_six_hundred_thousand_nodes(pa):
@@ -107,3 +110,26 @@ def test_mg_above_six_hundred_thousand_nodes(pa):
     f64 = prob.scalar_function().value(u64, z)
     assert abs(f - f64) <= 1e-7 * abs(f64)
     assert rel_inf(u, u64) <= 1e-5
+
+
+@pytest.mark.parametrize("dims", [(7, 4, 4), (17, 9, 11), (33, 17, 15), (25, 5, 3)])
+def test_mg_odd_boxes_against_the_oracle(pa, oracle_lib, dims):
+    """Boxes with odd hex counts: each coarse level has ceil(n / 2) hexes per
+    axis and a padding layer of weight zero.  The solution solves the oracle's
+    constrained system to the requested tolerance and equals the FP64
+    Jacobi-PCG solution; the iteration count stays that of a multigrid."""
+    from oracle import np_ref
+    mesh, prob, faces, dofs, z = _cantilever(pa, dims, 11)
+    u, st = prob.solution(z, options=pa.SolveOptions("mg", rel_tol=1e-10))
+    assert st["converged"] and st["rel_residual"] <= 1e-10, st
+    assert st["iterations"] <= 60, st
+    u64, s64 = prob.solution(z, options=pa.SolveOptions("fp64", rel_tol=1e-11))
+    assert rel_inf(u, u64) <= 1e-7
+    nx, ny, nz = dims
+    cells, coords = np_ref.box_mesh(nx, ny, nz, float(nx), float(ny), float(nz))
+    O = oracle_lib.Oracle(cells, coords, E=1.0, nu=0.3, p=3.0, pmin=1e-9, layout=1)
+    flux = np.array([0.0, 0.0, -1.0 / (ny * nz)])
+    F = -O.residual(np.zeros_like(u), z, faces, flux)
+    res = F - O.apply(u, z)
+    res[dofs] = 0.0
+    assert np.linalg.norm(res) <= 1.01e-10 * np.linalg.norm(F)
