@@ -51,7 +51,10 @@ def test_cpu_cantilever_matches_gpu_workload_definition(oracle_lib):
     assert np.all(cc.F[0::3] == 0.0) and np.all(cc.F[1::3] == 0.0)
     cc.assemble()
     x, info = cc.solve(1e-10, report_tol=1e-8)
-    assert 0 < info["report_iterations"] <= info["iterations"] and info["rel_residual"] < 1.01e-10
+    # the stop is on the recursive residual; the reported (true) one may sit a
+    # little above the tolerance, by an amount that depends on the host's
+    # floating-point contraction and thread count
+    assert 0 < info["report_iterations"] <= info["iterations"] and info["rel_residual"] < 2e-10
     res = cc.F - cc.O.apply(x, cc.z)
     res[cc.dofs] = 0.0
     assert np.linalg.norm(res) / np.linalg.norm(cc.F) < 2e-10
