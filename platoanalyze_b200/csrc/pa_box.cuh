@@ -221,11 +221,6 @@ __device__ __forceinline__ void box_hex(const T (&u)[8][3], const T (&lw)[6], co
 template <typename T, int WM, bool CUBE, class In, class Out>
 __global__ void __launch_bounds__(kBoxThreads) k_box(BoxDims d, BoxGeo<T> g, BoxW<T, WM> bw, int kz, In in,
                                                      Out out, BoxRed red, const double* skip) {
-  // launched as a programmatic dependent: the next kernel may be scheduled at
-  // once (its CTAs take SM slots as this grid's CTAs exit); nothing global is
-  // read before the kernels this one depends on have completed
-  pdl_trigger();
-  pdl_wait();
   // skip (may be null): two flags; the launch is a no-op when either is set
   // (a solve that converged or broke down inside a batch of captured iterations)
   if (skip && (skip[0] != 0.0 || skip[1] != 0.0)) return;

@@ -34,10 +34,7 @@
 //  * a level with an odd hex count along an axis is coarsened to ceil(n / 2)
 //    hexes: the coarse level spans one more fine hex layer, which holds no
 //    fine node and counts as weight zero in the coarse weights, so every box
-//    size has a hierarchy down to a few hundred dofs;
-//  * the kernels of an iteration are programmatic dependent launches: each
-//    may be scheduled while its predecessor finishes, and waits for it before
-//    touching memory.
+//    size has a hierarchy down to a few hundred dofs.
 // Requirements: a box lattice (mesh_make_box, or arrays recognised by
 // detect_lattice: the solver permutes b and x at its boundary), an elastic
 // operator (J2 tangent solves keep pa_mg.cu), one part.
@@ -443,8 +440,6 @@ __device__ __forceinline__ void grid_reduce_finish(double v, double* partials, u
 __global__ void __launch_bounds__(kVT) k_bcg_update(int64_t n, double* sc, const double* __restrict__ p,
                                                     const double* __restrict__ q, double* __restrict__ x,
                                                     double* __restrict__ r, double* partials, unsigned int* counter) {
-  pdl_trigger();
-  pdl_wait();
   if (sc[kBreak] != 0.0 || sc[kDone] != 0.0) return;
   const double a = sc[kAlpha];
   double s = 0.0;
@@ -533,8 +528,6 @@ __global__ void k_bset_bc(int64_t nbc, const int32_t* __restrict__ dofs, const d
 // layer that holds no fine node.
 __global__ void k_brestrict(BoxDims c, BoxDims f, const float* __restrict__ fv_in, const uint8_t* __restrict__ cmask,
                             float* __restrict__ cv_out, const double* skip) {
-  pdl_trigger();
-  pdl_wait();
   if (skip && (skip[0] != 0.0 || skip[1] != 0.0)) return;
   const int v = blockIdx.x * blockDim.x + threadIdx.x;
   const int Nc = int(c.N), Nf = int(f.N);
@@ -569,8 +562,6 @@ __global__ void k_brestrict(BoxDims c, BoxDims f, const float* __restrict__ fv_i
 // position i / 2; every coarse node it reads exists (2 c.nx >= f.nx).
 __global__ void k_bprolong_add(BoxDims c, BoxDims f, const float* __restrict__ e, const uint8_t* __restrict__ fmask,
                                float* __restrict__ x, const double* skip) {
-  pdl_trigger();
-  pdl_wait();
   if (skip && (skip[0] != 0.0 || skip[1] != 0.0)) return;
   const int v = blockIdx.x * blockDim.x + threadIdx.x;
   const int Nc = int(c.N), Nf = int(f.N);
@@ -945,8 +936,9 @@ void launch_box_t(const BoxLevel& L, const BoxGeo<T>& g, const T* w, const In& i
   }
   int kz = 2;
   const dim3 grid = box_grid(L.d, occupancy * num_sms(), &kz);
-  launch_pdl(k_box<T, WM, CUBE, In, Out>, grid, dim3(kBoxThreads), 0, s, L.d, g, BoxW<T, WM>{w, L.d.H, p, pmin}, kz,
-             in, out, red, skip);
+  k_box<T, WM, CUBE, In, Out><<<grid, kBoxThreads, 0, s>>>(L.d, g, BoxW<T, WM>{w, L.d.H, p, pmin}, kz, in, out, red,
+                                                          skip);
+  PA_LAUNCHED();
   g_box_launches += 1;
 }
 
@@ -993,9 +985,9 @@ void coarse_mask(const BoxLevel& f, BoxLevel& c, const std::vector<uint8_t>& fma
 // Hex counts of the multigrid levels of an nx x ny x nz box: the next level
 // has ceil(n / 2) hexes per axis (an odd level is padded by one hex layer of
 // weight zero), while every axis has at least 4 hexes, or at least 2 while
-// the level still has more than kDenseMax dofs; the last level is the
-// coarsest, solved by a dense inverse.
-constexpr int64_t kDenseMax = 2048;
+// the level still has more than kCoarseDofs dofs; the last level is the
+// coarsest, solved by a dense inverse of at most kDenseMax dofs.
+constexpr int64_t kDenseMax = 2048, kCoarseDofs = 512;
 std::vector<std::array<int, 3>> box_level_counts(const int* n0) {
   std::vector<std::array<int, 3>> out;
   std::array<int, 3> n = {n0[0], n0[1], n0[2]};
@@ -1003,7 +995,7 @@ std::vector<std::array<int, 3>> box_level_counts(const int* n0) {
     out.push_back(n);
     const int mn = std::min(std::min(n[0], n[1]), n[2]);
     const int64_t dofs = 3LL * (n[0] + 1) * (n[1] + 1) * (n[2] + 1);
-    if (!(mn >= 4 || (mn >= 2 && dofs > kDenseMax))) break;
+    if (!(mn >= 4 || (mn >= 2 && dofs > kCoarseDofs))) break;
     for (int a = 0; a < 3; ++a) n[a] = (n[a] + 1) / 2;
   }
   return out;
@@ -1291,8 +1283,9 @@ void vcycle(const Problem& P, BoxHierarchy& H, size_t l, cudaStream_t s, const d
   BoxLevel& L = *H.L[l];
   if (l + 1 == H.L.size()) {
     const int64_t n3 = 3 * L.d.N;
-    launch_pdl(k_mg_dense_solve, dim3(unsigned((32 * n3 + kVT - 1) / kVT)), dim3(kVT), 0, s, n3, L.nd,
-               L.dense.get(), L.b.get(), L.x.get(), skip);
+    k_mg_dense_solve<<<int((32 * n3 + kVT - 1) / kVT), kVT, 0, s>>>(n3, L.nd, L.dense.get(), L.b.get(), L.x.get(),
+                                                                    skip);
+    PA_LAUNCHED();
     g_box_launches += 1;
     return;
   }
@@ -1315,13 +1308,13 @@ void vcycle_level(const Problem& P, BoxHierarchy& H, size_t l, const B* b, O* xo
   // residual, restricted to the coarse right-hand side
   launch_box<float>(L, g, w, InVec<float, float>{L.x.get(), nullptr, N}, OutRes<B>{L.r.get(), b, L.mask, N}, red,
                     s, skip);
-  launch_pdl(k_brestrict, dim3(unsigned((C.d.N + kVT - 1) / kVT)), dim3(kVT), 0, s, C.d, L.d, L.r.get(), C.mask,
-             C.b.get(), skip);
+  k_brestrict<<<int((C.d.N + kVT - 1) / kVT), kVT, 0, s>>>(C.d, L.d, L.r.get(), C.mask, C.b.get(), skip);
+  PA_LAUNCHED();
   g_box_launches += 1;
   vcycle(P, H, l + 1, s, skip);
   // post-smoothing from x + P e
-  launch_pdl(k_bprolong_add, dim3(unsigned((N + kVT - 1) / kVT)), dim3(kVT), 0, s, C.d, L.d, C.x.get(), L.mask,
-             L.x.get(), skip);
+  k_bprolong_add<<<int((N + kVT - 1) / kVT), kVT, 0, s>>>(C.d, L.d, C.x.get(), L.mask, L.x.get(), skip);
+  PA_LAUNCHED();
   g_box_launches += 1;
   launch_box<float>(L, g, w, InVec<float, float>{L.x.get(), nullptr, N}, OutPost1<B>{L.r.get(), b, L.dinv.get(), N},
                     red, s, skip);
@@ -1425,8 +1418,7 @@ bool solve_boxmg(Problem& P, const double* z, const double* b, double* x_out, co
       vcycle_level<double, double, true>(P, H, 0, r, zv, r, sc, s, sc + kBreak);
       launch_box<double>(F, box_geo<double>(F, P.ep), w64, InCgP{zv, pold, pnew, sc, N},
                          OutCgQ{H.q.get(), zv, pold, mask, sc, N}, red, s, sc + kBreak);
-      launch_pdl(k_bcg_update, dim3(unsigned(vec_blocks(n))), dim3(kVT), 0, s, n, sc, pnew, H.q.get(), x, r,
-                 H.partials.get(), H.counter.get());
+      k_bcg_update<<<vec_blocks(n), kVT, 0, s>>>(n, sc, pnew, H.q.get(), x, r, H.partials.get(), H.counter.get());
       g_box_launches += 1;
       cudaGraph_t graph = nullptr;
       const cudaError_t ce = cudaStreamEndCapture(s, &graph);
@@ -1704,14 +1696,16 @@ __global__ void __launch_bounds__(256) k_bgradient_z(BoxDims d, double ih0, doub
   constexpr int kRow = 13;  // staging stride per cell (odd: two-way bank conflicts at most)
   __shared__ double stage[8][32 * kRow];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int64_t C = 6 * d.H;
-  const int64_t c0 = blockIdx.x * int64_t(blockDim.x) + 32 * w;
-  const int64_t c = c0 + lane;
+  // 32-bit indices: the box path has 3 N < 2^31, so 6 H < 2^31
+  const int C = int(6 * d.H);
+  const int c0 = blockIdx.x * blockDim.x + 32 * w;
+  const int c = c0 + lane;
   double* st = stage[w] + kRow * lane;
   if (c < C) {
-    const int64_t h = c / 6;
-    const int t = int(c - 6 * h);
-    const int i = int(h % d.nx), j = int((h / d.nx) % d.ny), k = int(h / (int64_t(d.nx) * d.ny));
+    const int h = c / 6;
+    const int t = c - 6 * h;
+    const int hy = h / d.nx, k = hy / d.ny;
+    const int i = h - hy * d.nx, j = hy - k * d.ny;
     const int plane = d.px * d.py;
     const int b0 = i + d.px * (j + d.py * k);
     const double ih[3] = {ih0, ih1, ih2};
@@ -1775,7 +1769,7 @@ __global__ void __launch_bounds__(256) k_bgradient_z(BoxDims d, double ih0, doub
     }
   }
   __syncwarp();
-  const int64_t base = 12 * c0, end = 12 * C;
+  const int64_t base = 12 * int64_t(c0), end = 12 * int64_t(C);
 #pragma unroll
   for (int r = 0; r < 12; ++r) {
     const int e = 32 * r + lane;

@@ -223,8 +223,6 @@ __global__ void __launch_bounds__(256) k_gj_invert(int nd, double* A, const doub
 // skip (may be null): two flags; the launch is a no-op when either is set.
 __global__ void k_mg_dense_solve(int64_t n3, int64_t nd, const double* __restrict__ Ainv, const float* __restrict__ b,
                                  float* __restrict__ x, const double* skip = nullptr) {
-  pdl_trigger();
-  pdl_wait();
   if (skip && (skip[0] != 0.0 || skip[1] != 0.0)) return;
   const int64_t r = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;

@@ -7,7 +7,6 @@
 #include <string>
 #include <vector>
 #include <stdexcept>
-#include <utility>
 
 #include "pa_b200.h"  // include/ is on the compiler include path
 
@@ -36,33 +35,6 @@ void set_last_error(const std::string& msg);
 
 // Launch-error check after a kernel launch.
 #define PA_LAUNCHED() PA_CUDA(cudaGetLastError())
-
-// -------------------------------------------- programmatic dependent launch --
-// A kernel launched by launch_pdl may be scheduled while the kernel before it
-// on the stream is still running, so that its launch latency overlaps that
-// kernel's tail.  Such a kernel calls pdl_wait() before its first access to
-// global memory: the wait returns once every kernel it depends on has
-// completed and its writes are visible (immediately when there is none).
-// pdl_trigger() lets the next kernel be scheduled; a kernel that never calls
-// it triggers when it exits.
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
-__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
-
-template <typename... KArgs, typename... Args>
-inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
-                       Args&&... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = grid;
-  cfg.blockDim = block;
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = s;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = at;
-  cfg.numAttrs = 1;
-  PA_CUDA(cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(std::forward<Args>(args))...));
-}
 
 // ----------------------------------------------------------- device buffer --
 template <typename T>
