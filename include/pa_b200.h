@@ -540,6 +540,33 @@ pa_status pa_pc_train(pa_problem* problem, pa_pc* pc, int32_t num_densities, con
  * mesh must be the network's grid.  The problem does not own the network. */
 pa_status pa_problem_set_preconditioner(pa_problem* problem, pa_pc* pc);
 
+/* ------------------------------------ learned coarse-level multigrid weights --
+ * No counterpart in the reference (it solves with AmgX / Belos).  The box
+ * multigrid of PA_SOLVER_PCG_MG gives each level-1 hex the mean weight of its
+ * children; a network (pa_pc on the level-1 hex grid: gx, gy, gz = its hex
+ * counts) may multiply it by exp(delta), delta its first output channel, fed
+ * with 5 features per level-1 hex (logarithms of the mean, geometric mean,
+ * minimum and maximum child weight, and the fraction of children inside the
+ * box).  A network whose last layer is zero (a new one) leaves the method
+ * unchanged.  Arrays may be device or host pointers. */
+/* Level-1 hex counts of the problem's box multigrid; PA_ERR_INVALID_ARG when
+ * the mesh has none. */
+pa_status pa_boxmg_coarse_grid(pa_problem* problem, int32_t dims[3]);
+/* The network's input features for control z: 5 per level-1 hex, channel-last. */
+pa_status pa_boxmg_coarse_features(pa_problem* problem, const double* z, float* features);
+/* Training loss and gradient for an explicit correction delta (one per
+ * level-1 hex): the mean over the residual/error pairs (residuals: num x 3N,
+ * interleaved, K e_s = r_s at control z, energies[s] = e_s . r_s) of
+ * ||e_s - V r_s||_K^2 / ||e_s||_K^2, V the V-cycle, and its gradient in delta
+ * (exact for a two-level hierarchy; deeper levels and level 1's smoother are
+ * held fixed otherwise). */
+pa_status pa_boxmg_coarse_sensitivity(pa_problem* problem, const double* z, const float* delta,
+                                      int32_t num_residuals, const double* residuals, const double* energies,
+                                      double* loss, float* grad_delta);
+/* Attach (or detach with NULL) the network that corrects the level-1 weights
+ * of every later PA_SOLVER_PCG_MG solve; the problem does not own it. */
+pa_status pa_problem_set_coarse_network(pa_problem* problem, pa_pc* pc);
+
 #ifdef __cplusplus
 }
 #endif

@@ -117,6 +117,10 @@ SIGNATURES = [
     ("pa_pc_apply", I32, [P, P, P, P, P]),
     ("pa_pc_train", I32, [P, P, I32, P, I32, P, P, P, ct.POINTER(PcTrainOptions), ct.POINTER(PcTrainStats)]),
     ("pa_problem_set_preconditioner", I32, [P, P]),
+    ("pa_boxmg_coarse_grid", I32, [P, P]),
+    ("pa_boxmg_coarse_features", I32, [P, P, P]),
+    ("pa_boxmg_coarse_sensitivity", I32, [P, P, P, I32, P, P, ct.POINTER(F64), P]),
+    ("pa_problem_set_coarse_network", I32, [P, P]),
     ("pa_exodus_open", I32, [ct.c_char_p, ct.POINTER(P)]),
     ("pa_exodus_sizes", I32, [P, ct.POINTER(I64), ct.POINTER(I64), ct.POINTER(I32)]),
     ("pa_exodus_mesh", I32, [P, P, P]),

@@ -317,6 +317,46 @@ class Problem:
         self.mesh.num_tiles = T.value
         return k.value, dict(zip((64, 128, 256), ms.tolist()))
 
+    def coarse_grid(self):
+        """Level-1 hex counts of the box multigrid (the coarse-weight network's grid)."""
+        d = np.zeros(3, np.int32)
+        _abi.check(self._lib.pa_boxmg_coarse_grid(self._h, _ptr(d, np.int32, 3)))
+        return tuple(int(v) for v in d)
+
+    def coarse_features(self, z, out=None):
+        """The coarse-weight network's input features for control z (5 per level-1 hex)."""
+        z = _as(z, np.float64)
+        g = self.coarse_grid()
+        n = 5 * g[0] * g[1] * g[2]
+        out = _empty(z, n, np.float32) if out is None else out
+        _abi.check(self._lib.pa_boxmg_coarse_features(self._h, _ptr(z, np.float64, self.nz, "z"),
+                                                      _ptr(out, np.float32, n, "features")))
+        return out
+
+    def coarse_sensitivity(self, z, delta, residuals, energies, grad=None):
+        """(loss, dloss/ddelta) of the V-cycle with level-1 weights mean * exp(delta)
+        on residual/error pairs (residuals: k x 3N, energies: k)."""
+        z = _as(z, np.float64)
+        delta = _as(delta, np.float32)
+        residuals = _as(residuals, np.float64)
+        en = np.ascontiguousarray(np.asarray(energies, np.float64).ravel())
+        k = en.size
+        g = self.coarse_grid()
+        H1 = g[0] * g[1] * g[2]
+        grad = _empty(delta, H1, np.float32) if grad is None else grad
+        loss = ct.c_double()
+        _abi.check(self._lib.pa_boxmg_coarse_sensitivity(
+            self._h, _ptr(z, np.float64, self.nz, "z"), _ptr(delta, np.float32, H1, "delta"), int(k),
+            _ptr(residuals, np.float64, k * self.ndof, "residuals"), _ptr(en, np.float64, k), ct.byref(loss),
+            _ptr(grad, np.float32, H1, "grad")))
+        return loss.value, grad
+
+    def set_coarse_network(self, net):
+        """Network that corrects the box multigrid's level-1 weights (None detaches)."""
+        h = net._h if net is not None else None
+        _abi.check(self._lib.pa_problem_set_coarse_network(self._h, h))
+        self._coarse_net = net
+
     def set_preconditioner(self, pc):
         """Network SolveOptions("learned") uses (None detaches); the mesh must be its grid."""
         _abi.check(self._lib.pa_problem_set_preconditioner(self._h, pc._h if pc is not None else None))
@@ -688,3 +728,74 @@ class LearnedPreconditioner:
             self.close()
         except Exception:
             pass
+
+
+class LearnedCoarsening:
+    """Learned level-1 weights of the box multigrid (PA_SOLVER_PCG_MG): a
+    convolutional network on the level-1 hex grid (the same four-layer BF16
+    network as LearnedPreconditioner, tcgen05 forward, the library's backward
+    kernels) maps 5 features per coarse hex to delta, and the coarse hex gets
+    mean(child weights) * exp(delta).  A new network (last layer zero) is the
+    plain multigrid.  Trained on residual/error pairs (K e = r) of SIMP designs
+    by Adam on the mean of ||e - V r||_K^2 / ||e||_K^2 (V the V-cycle), with
+    dloss/ddelta from pa_boxmg_coarse_sensitivity.  No counterpart in the
+    reference."""
+
+    def __init__(self, problem, seed=0):
+        self.grid = problem.coarse_grid()
+        self.net = LearnedPreconditioner(self.grid, seed)
+        self.num_points = self.net.num_points
+
+    def delta(self, problem, z):
+        """The correction delta (one per level-1 hex) the network gives for control z."""
+        return self.net.forward(problem.coarse_features(z))[0::3]
+
+    def attach(self, problem):
+        problem.set_coarse_network(self.net)
+
+    def train(self, problem, designs, residuals, energies, sample_design, steps=100, batch=4, learning_rate=3e-3,
+              seed=0, log=None):
+        """designs: D x nz controls; residuals[s] (3N, zero on constrained dofs)
+        with K(designs[sample_design[s]]) e_s = residuals[s], energies[s] = e_s . r_s.
+        Each step takes one design and `batch` of its samples.  Returns the
+        loss history (per step, before the update)."""
+        import torch
+        dev = residuals.device
+        sd = np.asarray(sample_design, np.int64)
+        en = np.asarray(energies, np.float64)
+        rng = np.random.default_rng(seed)
+        params = torch.tensor(self.net.get_params(), device=dev)
+        m = torch.zeros_like(params)
+        v = torch.zeros_like(params)
+        b1, b2, eps = 0.9, 0.999, 1e-8
+        feats = {}
+        hist = []
+        for step in range(steps):
+            d = int(sd[rng.integers(0, sd.size)])
+            idx = np.flatnonzero(sd == d)
+            pick = rng.choice(idx, size=min(batch, idx.size), replace=False)
+            z = designs[d]
+            if d not in feats:
+                feats[d] = problem.coarse_features(z)
+            f = feats[d]
+            out = self.net.forward(f)
+            delta = out[0::3].contiguous()
+            loss, gd = problem.coarse_sensitivity(z, delta, residuals[torch.as_tensor(pick, device=dev)].contiguous(),
+                                                  en[pick])
+            gout = torch.zeros(3 * self.num_points, dtype=torch.float32, device=dev)
+            gout[0::3] = gd
+            g = self.net.backward(f, gout)
+            hist.append(loss)
+            if log:
+                log(step, loss)
+            m.mul_(b1).add_(g, alpha=1 - b1)
+            v.mul_(b2).addcmul_(g, g, value=1 - b2)
+            mh = m / (1 - b1 ** (step + 1))
+            vh = v / (1 - b2 ** (step + 1))
+            params.sub_(learning_rate * mh / (vh.sqrt() + eps))
+            _abi.check(self.net._lib.pa_pc_set_params(self.net._h, _ptr(params, np.float32, self.net.num_params,
+                                                                         "params")))
+        return hist
+
+    def close(self):
+        self.net.close()

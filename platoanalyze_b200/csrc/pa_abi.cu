@@ -160,6 +160,7 @@ struct pa_problem {
   pa::Problem P;
   pa_mesh* mesh = nullptr;  // the problem keeps its mesh alive until it is destroyed
   pa_pc* pc = nullptr;      // and its attached network
+  pa_pc* cpc = nullptr;     // and its coarse-weight network
 };
 struct pa_pc {
   pa::LearnedPC* pc = nullptr;
@@ -369,6 +370,7 @@ pa_status pa_problem_destroy(pa_problem* problem) {
     if (P.ev1) cudaEventDestroy(P.ev1);
     cudaStream_t s = P.own_stream ? P.stream : nullptr;
     pa_pc* pc = problem->pc;
+    pa_pc* cpc = problem->cpc;
     pa::mg_release(P);
     pa::boxmg_release(P);
     delete problem;
@@ -376,6 +378,7 @@ pa_status pa_problem_destroy(pa_problem* problem) {
     mh->m.live_problems -= 1;
     if (mh->m.live_problems == 0 && mh->destroy_requested) delete mh;
     if (pc && --pc->attached == 0 && pc->destroy_requested) delete pc;
+    if (cpc && --cpc->attached == 0 && cpc->destroy_requested) delete cpc;
   });
 }
 
@@ -1065,6 +1068,82 @@ pa_status pa_problem_set_preconditioner(pa_problem* problem, pa_pc* pc) {
     problem->pc = pc;
     pc->attached += 1;
     P.pc = &L;
+  });
+}
+
+pa_status pa_problem_set_coarse_network(pa_problem* problem, pa_pc* pc) {
+  return guard([&] {
+    Problem& P = prob(problem);
+    auto detach = [&]() {
+      pa_pc* old = problem->cpc;
+      problem->cpc = nullptr;
+      P.coarse_pc = nullptr;
+      if (old && --old->attached == 0 && old->destroy_requested) delete old;
+    };
+    if (!pc) {
+      detach();
+      return;
+    }
+    PA_CHECK(!pc->destroy_requested, "network already destroyed");
+    pa::LearnedPC& L = pcref(pc);
+    PA_CHECK(pa::pc_device(L) == P.mesh->device, "network and problem live on different devices");
+    int dims[3];
+    PA_CHECK(pa::boxmg_coarse_grid(P, dims), "the problem's mesh has no box multigrid");
+    PA_CHECK(pa::pc_grid_points(L) == int64_t(dims[0]) * dims[1] * dims[2],
+             "the network's grid is not the level-1 hex grid (pa_boxmg_coarse_grid)");
+    if (problem->cpc == pc) return;
+    detach();
+    problem->cpc = pc;
+    pc->attached += 1;
+    P.coarse_pc = &L;
+  });
+}
+
+pa_status pa_boxmg_coarse_grid(pa_problem* problem, int32_t dims[3]) {
+  return guard([&] {
+    Problem& P = prob(problem);
+    PA_CHECK(dims, "null argument");
+    int d[3];
+    PA_CHECK(pa::boxmg_coarse_grid(P, d), "the problem's mesh has no box multigrid");
+    for (int a = 0; a < 3; ++a) dims[a] = d[a];
+  });
+}
+
+pa_status pa_boxmg_coarse_features(pa_problem* problem, const double* z, float* features) {
+  return guard([&] {
+    Problem& P = prob(problem);
+    int d[3];
+    PA_CHECK(pa::boxmg_coarse_grid(P, d), "the problem's mesh has no box multigrid");
+    const int64_t H1 = int64_t(d[0]) * d[1] * d[2];
+    pa::Stage st(P);
+    const double* dz = st.in(z, P.nz(), "z");
+    float* df = st.out(features, 5 * H1, "features");
+    pa::boxmg_coarse_features(P, dz, df);
+    st.finish();
+  });
+}
+
+pa_status pa_boxmg_coarse_sensitivity(pa_problem* problem, const double* z, const float* delta,
+                                      int32_t num_residuals, const double* residuals, const double* energies,
+                                      double* loss, float* grad_delta) {
+  return guard([&] {
+    Problem& P = prob(problem);
+    PA_CHECK(loss && energies && num_residuals > 0, "null argument or no residuals");
+    int d[3];
+    PA_CHECK(pa::boxmg_coarse_grid(P, d), "the problem's mesh has no box multigrid");
+    const int64_t H1 = int64_t(d[0]) * d[1] * d[2];
+    std::vector<double> en(static_cast<size_t>(num_residuals));
+    if (pa::is_device_pointer(energies))
+      PA_CUDA(cudaMemcpy(en.data(), energies, sizeof(double) * en.size(), cudaMemcpyDeviceToHost));
+    else
+      std::copy(energies, energies + num_residuals, en.begin());
+    pa::Stage st(P);
+    const double* dz = st.in(z, P.nz(), "z");
+    const float* dd = st.in(delta, H1, "delta");
+    const double* dr = st.in(residuals, int64_t(num_residuals) * P.ndof(), "residuals");
+    float* dg = st.out(grad_delta, H1, "grad_delta");
+    pa::boxmg_coarse_sensitivity(P, dz, dd, num_residuals, dr, en.data(), loss, dg);
+    st.finish();
   });
 }
 

@@ -47,6 +47,7 @@
 #include "pa_box.cuh"
 #include "pa_cell.cuh"
 #include "pa_dense.cuh"
+#include "pa_learned.cuh"
 #include "pa_problem.cuh"
 
 namespace pa {
@@ -689,8 +690,10 @@ __global__ void k_bweights(BoxDims d, const double* __restrict__ z, int layout, 
 // Coarse hex weight = mean of the 48 child tets (per-hex or tet-major fine
 // weights); the children in a padding layer (2 I + a >= f.nx, ...) count as
 // weight zero, so a coarse hex half outside the fine box has half the weight.
+// delta (may be null): a learned correction, w = mean exp(delta[h dstride])
+// with delta clamped to [-8, 8].
 __global__ void k_bcoarse_w(BoxDims c, BoxDims f, const double* __restrict__ wf, int wm, double* __restrict__ w64,
-                            float* __restrict__ w32) {
+                            float* __restrict__ w32, const float* __restrict__ delta, int dstride) {
   const int64_t h = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (h >= c.H) return;
   const int I = int(h % c.nx), J = int((h / c.nx) % c.ny), K = int(h / (int64_t(c.nx) * c.ny));
@@ -705,9 +708,141 @@ __global__ void k_bcoarse_w(BoxDims c, BoxDims f, const double* __restrict__ wf,
         else
           s += 6.0 * wf[fh];
       }
-  const double w = s / 48.0;
+  double w = s / 48.0;
+  if (delta) w *= exp(fmin(fmax(double(delta[h * dstride]), -8.0), 8.0));
   w64[h] = w;
   w32[h] = float(w);
+}
+
+// Input features of the learned coarse-weight correction, per coarse hex
+// (channel-last, 5 per hex) from the per-hex weights of its existing
+// children (the mean of the six tets when the fine weights are per tet):
+// with L(w) = 1 + log10(w) / 9 (0 at the SIMP minimum 1e-9, 1 at full
+// material), L of the mean over all eight children (padding as zero, the
+// weight the coarse level is given), of their geometric mean, minimum and
+// maximum, and the fraction of the eight children inside the fine box.
+__global__ void k_bcoarse_feat(BoxDims c, BoxDims f, const double* __restrict__ wf, int wm, float* __restrict__ feat) {
+  const int64_t h = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (h >= c.H) return;
+  const int I = int(h % c.nx), J = int((h / c.nx) % c.ny), K = int(h / (int64_t(c.nx) * c.ny));
+  double sum = 0.0, lsum = 0.0, mn = 1e300, mx = 0.0;
+  int cnt = 0;
+  for (int cc = 0; cc < 2; ++cc)
+    for (int b = 0; b < 2; ++b)
+      for (int a = 0; a < 2; ++a) {
+        if (2 * I + a >= f.nx || 2 * J + b >= f.ny || 2 * K + cc >= f.nz) continue;
+        const int64_t fh = (2 * I + a) + int64_t(f.nx) * ((2 * J + b) + int64_t(f.ny) * (2 * K + cc));
+        double w = 0.0;
+        if (wm)
+          for (int t = 0; t < 6; ++t) w += wf[t * f.H + fh] / 6.0;
+        else
+          w = wf[fh];
+        w = fmax(w, 1e-30);
+        sum += w;
+        lsum += log(w);
+        mn = fmin(mn, w);
+        mx = fmax(mx, w);
+        ++cnt;
+      }
+  auto L = [](double w) { return float(1.0 + log10(fmax(w, 1e-30)) / 9.0); };
+  float* o = feat + 5 * h;
+  o[0] = L(sum / 8.0);
+  o[1] = L(exp(lsum / cnt));
+  o[2] = L(mn);
+  o[3] = L(mx);
+  o[4] = float(cnt) / 8.f;
+}
+
+// gw[h] += scale a^T A_h b for every hex of a level: A_h the unweighted
+// stiffness of the hex's six tets, a and b FP32 component-major vectors of
+// the level; a^T A_t b = vol sigma(eps(a)) . eps(b) (engineering shears).
+__global__ void __launch_bounds__(256) k_bbilinear(BoxDims d, double ih0, double ih1, double ih2, double vol,
+                                                   Iso<double> iso, const float* __restrict__ a,
+                                                   const float* __restrict__ b, double scale, double* __restrict__ gw) {
+  const int64_t h = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (h >= d.H) return;
+  const int i = int(h % d.nx), j = int((h / d.nx) % d.ny), k = int(h / (int64_t(d.nx) * d.ny));
+  const double ih[3] = {ih0, ih1, ih2};
+  const int N = int(d.N);
+  double ua[8][3], ub[8][3];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const int v = (i + (q & 1)) + d.px * ((j + ((q >> 1) & 1)) + d.py * (k + (q >> 2)));
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      ua[q][c] = a[c * N + v];
+      ub[q][c] = b[c * N + v];
+    }
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int t = 0; t < 6; ++t) {
+    double ga[3][3], gb[3][3];
+    int prev = 0;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      const int ax = path_axis(t, m), nxt = prev | (1 << ax);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        ga[c][ax] = (ua[nxt][c] - ua[prev][c]) * ih[ax];
+        gb[c][ax] = (ub[nxt][c] - ub[prev][c]) * ih[ax];
+      }
+      prev = nxt;
+    }
+    const double ea[6] = {ga[0][0], ga[1][1], ga[2][2], ga[1][2] + ga[2][1], ga[0][2] + ga[2][0], ga[0][1] + ga[1][0]};
+    const double eb[6] = {gb[0][0], gb[1][1], gb[2][2], gb[1][2] + gb[2][1], gb[0][2] + gb[2][0], gb[0][1] + gb[1][0]};
+    double sg[6];
+    tet_stress(iso, vol, ea, sg);
+    s += voigt_dot(sg, eb);
+  }
+  gw[h] += scale * s;
+}
+
+// x = 0 on the masked dofs (component-major FP32)
+__global__ void k_bmask_f(int N, const uint8_t* __restrict__ mask, float* __restrict__ x) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= N) return;
+  const uint8_t mk = mask[v];
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+    if ((mk >> c) & 1) x[c * N + v] = 0.f;
+}
+
+// acc += 1 - (r . z + z . rho) / E: the relative energy-norm error
+// ||e - z||_K^2 / E of z = M r for K e = r, E = e . r (rho = r - K z)
+__global__ void __launch_bounds__(kVT) k_bcoarse_loss(int64_t n, const float* __restrict__ r,
+                                                      const float* __restrict__ z, const float* __restrict__ rho,
+                                                      double inv_e, double* partials, unsigned int* counter,
+                                                      double* acc) {
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    s += double(z[i]) * (double(r[i]) + double(rho[i]));
+  __shared__ double s_red[32];
+  __shared__ bool s_last;
+  const double b = block_sum_box(s, s_red);
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = b;
+    __threadfence();
+    s_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (s_last) {
+    __threadfence();
+    double t = 0.0;
+    for (unsigned k = threadIdx.x; k < gridDim.x; k += blockDim.x) t += __ldcg(&partials[k]);
+    t = block_sum_box(t, s_red);
+    if (threadIdx.x == 0) {
+      *counter = 0u;
+      *acc += 1.0 - t * inv_e;
+    }
+  }
+}
+
+// dL/ddelta = w dL/dw / n (w = mean exp(delta), the weight the level holds)
+__global__ void k_bgrad_delta(int64_t H, const double* __restrict__ gw, const double* __restrict__ w, double inv_n,
+                              float* __restrict__ grad) {
+  const int64_t h = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (h < H) grad[h] = float(w[h] * gw[h] * inv_n);
 }
 
 // dinv = masked ? 0 : 1 / diag(K), diag from the tets around each node:
@@ -848,6 +983,10 @@ struct BoxHierarchy {
   bool masks_valid = false;
   DevBuf<float> cheb;  // per smoothed level: 1 / theta, ca, c2 (read by the captured iteration)
   DevBuf<double> e_partials, e_value;  // the per-cell entry points' energy reduction
+  // learned coarse-weight correction: features and network output of level 1,
+  // and an explicit correction (stride 1) that overrides the network while set
+  DevBuf<float> cfeat, cout3;
+  const float* delta_arg = nullptr;
   DevBuf<double> gu_k0;                // assembled K on the box: unpenalized blocks per table entry
   double gu_key[5] = {0, 0, 0, 0, 0};  // the hex sides and Lame constants they were made for
   // the captured outer iteration (two variants alternate the p buffers),
@@ -1136,13 +1275,30 @@ bool boxmg_setup(Problem& P, const double* z) {
   F.wm = differ ? 1 : 0;
   const double* fw64 = F.wm ? H.w64t.get() : H.w64h.get();
   g_box_launches += 1;
+  // learned correction of the level-1 weights: the explicit one of a
+  // sensitivity evaluation, else the problem's coarse-weight network
+  const float* delta = H.delta_arg;
+  int dstride = 1;
+  if (!delta && P.coarse_pc) {
+    const BoxLevel& L1 = *H.L[1];
+    PA_CHECK(pc_grid_points(*P.coarse_pc) == L1.d.H, "coarse-weight network: grid is not the level-1 hex grid");
+    H.cfeat.resize(size_t(5 * L1.d.H));
+    H.cout3.resize(size_t(3 * L1.d.H));
+    k_bcoarse_feat<<<int((L1.d.H + kVT - 1) / kVT), kVT, 0, s>>>(L1.d, F.d, fw64, F.wm, H.cfeat.get());
+    PA_LAUNCHED();
+    pc_forward_features(*P.coarse_pc, H.cfeat.get(), H.cout3.get(), s);
+    g_box_launches += 7;
+    delta = H.cout3.get();
+    dstride = 3;
+  }
   // coarse weights of every level
   const Iso<double> iso = P.ep.iso();
   for (size_t l = 1; l < H.L.size(); ++l) {
     BoxLevel& L = *H.L[l];
     const BoxLevel& Fl = *H.L[l - 1];
     k_bcoarse_w<<<int((L.d.H + kVT - 1) / kVT), kVT, 0, s>>>(L.d, Fl.d, l == 1 ? fw64 : Fl.w64.get(),
-                                                             l == 1 ? F.wm : 0, L.w64.get(), L.w32.get());
+                                                             l == 1 ? F.wm : 0, L.w64.get(), L.w32.get(),
+                                                             l == 1 ? delta : nullptr, dstride);
     PA_LAUNCHED();
     g_box_launches += 1;
   }
@@ -1322,6 +1478,21 @@ void vcycle_level(const Problem& P, BoxHierarchy& H, size_t l, const B* b, O* xo
                     OutPost2<O, RZ>{xo, L.x.get(), L.r.get(), L.dinv.get(), ch, N, rvec, sc}, red, s, skip);
 }
 
+// The Chebyshev coefficients of every smoothed level (from its lmax) into
+// H.cheb, which the V-cycle's launches read.
+void upload_cheb(BoxHierarchy& H, cudaStream_t s) {
+  const size_t NS = H.L.size() - 1;
+  std::vector<float> ch(3 * NS);
+  for (size_t l = 0; l < NS; ++l) {
+    const ChebStep c = cheb2(H.L[l]->lmax);
+    ch[3 * l] = c.inv_theta;
+    ch[3 * l + 1] = c.ca;
+    ch[3 * l + 2] = c.c2;
+  }
+  if (H.cheb.n != ch.size()) H.cheb.resize(ch.size());
+  PA_CUDA(cudaMemcpyAsync(H.cheb.get(), ch.data(), sizeof(float) * ch.size(), cudaMemcpyHostToDevice, s));
+}
+
 // y = K x (FP64, box kernel) with optional masks on input and output
 void box_apply64(const BoxLevel& L, const ElasticParams& ep, const double* w, const double* x, double* y,
                  const uint8_t* mask, BoxRed red, cudaStream_t s) {
@@ -1387,18 +1558,7 @@ bool solve_boxmg(Problem& P, const double* z, const double* b, double* x_out, co
   k_bcg_reset<<<1, 1, 0, s>>>(sc, tol2, 1);
   PA_LAUNCHED();
   // this solve's Chebyshev coefficients, read by the captured iteration
-  {
-    const size_t NS = H.L.size() - 1;
-    std::vector<float> ch(3 * NS);
-    for (size_t l = 0; l < NS; ++l) {
-      const ChebStep c = cheb2(H.L[l]->lmax);
-      ch[3 * l] = c.inv_theta;
-      ch[3 * l + 1] = c.ca;
-      ch[3 * l + 2] = c.c2;
-    }
-    if (H.cheb.n != ch.size()) H.cheb.resize(ch.size());
-    PA_CUDA(cudaMemcpyAsync(H.cheb.get(), ch.data(), sizeof(float) * ch.size(), cudaMemcpyHostToDevice, s));
-  }
+  upload_cheb(H, s);
   // one outer iteration as a graph; two variants alternate the p buffers.
   // Captured once and relaunched by later solves while the buffers, the
   // weight layout and the material are the same.
@@ -1802,6 +1962,116 @@ void box_entry_apply(Problem& P, const double* z, const double* u, double* y) {
     launch_box_t<double, 2, true>(F, g, z, InAoS64{u}, OutAoS64{y}, red, P.stream, P.ep.p, P.ep.pmin);
   else
     launch_box_t<double, 2, false>(F, g, z, InAoS64{u}, OutAoS64{y}, red, P.stream, P.ep.p, P.ep.pmin);
+}
+
+// ------------------------------------------- learned coarse-level weights --
+// The level-1 weights of the box multigrid may carry a learned correction
+// w1 = mean exp(delta) (k_bcoarse_w), delta from a convolutional network on the
+// level-1 hex grid (pa_learned.cu) fed with k_bcoarse_feat.  Training needs
+// dL/ddelta of the V-cycle's energy-norm error on residual/error pairs
+// (K e = r, E = e . r): with z = V r, L = ||e - z||_K^2 / E = 1 - (r.z + z.rho) / E
+// (rho = r - K z), and for the two-grid cycle with exact coarse solve
+// x_c = A^-1 R (r - K S r) (A the level-1 operator, R = P^T, S the symmetric
+// Chebyshev smoother),
+//   dL/dw_h = 2 a^T A_h x_c / E,  a = A^-1 R (I - K S) rho,
+// A_h the unweighted stiffness of coarse hex h.  A^-1 is applied by the
+// level-1 V-cycle (exact when level 1 is the coarsest), and the dependence
+// of deeper levels and of level 1's smoother on w1 is not followed.
+
+bool boxmg_coarse_grid(const Problem& P, int dims[3]) {
+  if (!boxmg_eligible(P)) return false;
+  const auto lv = box_level_counts(P.mesh->lat_n);
+  for (int a = 0; a < 3; ++a) dims[a] = lv[1][a];
+  return true;
+}
+
+void boxmg_coarse_features(Problem& P, const double* z, float* feat) {
+  PA_CHECK(boxmg_eligible(P), "the problem's mesh has no box multigrid");
+  const LearnedPC* keep = P.coarse_pc;
+  P.coarse_pc = nullptr;  // the set-up below only needs the fine weights
+  bool ok = false;
+  try {
+    ok = boxmg_setup(P, z);
+  } catch (...) {
+    P.coarse_pc = const_cast<LearnedPC*>(keep);
+    throw;
+  }
+  P.coarse_pc = const_cast<LearnedPC*>(keep);
+  PA_CHECK(ok, "singular coarsest operator");
+  BoxHierarchy& H = *P.boxmg;
+  const BoxLevel& F = *H.L[0];
+  const BoxLevel& L1 = *H.L[1];
+  const double* fw64 = F.wm ? H.w64t.get() : H.w64h.get();
+  k_bcoarse_feat<<<int((L1.d.H + kVT - 1) / kVT), kVT, 0, P.stream>>>(L1.d, F.d, fw64, F.wm, feat);
+  PA_LAUNCHED();
+}
+
+void boxmg_coarse_sensitivity(Problem& P, const double* z, const float* delta, int nres, const double* res,
+                              const double* energies, double* loss, float* grad) {
+  PA_CHECK(boxmg_eligible(P), "the problem's mesh has no box multigrid");
+  PA_CHECK(nres > 0, "no residuals");
+  boxmg_ensure(P);
+  BoxHierarchy& H = *P.boxmg;
+  H.delta_arg = delta;
+  bool ok = false;
+  try {
+    ok = boxmg_setup(P, z);
+  } catch (...) {
+    H.delta_arg = nullptr;
+    throw;
+  }
+  H.delta_arg = nullptr;
+  PA_CHECK(ok, "singular coarsest operator");
+  cudaStream_t s = P.stream;
+  upload_cheb(H, s);
+  BoxLevel& F = *H.L[0];
+  BoxLevel& C = *H.L[1];
+  const int64_t N = F.d.N, n = 3 * N, N1 = C.d.N;
+  const Mesh& m = *P.mesh;
+  const int32_t* node_of = m.lat_permuted ? m.d_lat_node.get() : nullptr;
+  DevBuf<float> r32(n), z32(n), rho(n), sr(n), zeta(n), xc(3 * N1);
+  DevBuf<double> gw(size_t(C.d.H)), acc(1);
+  PA_CUDA(cudaMemsetAsync(gw.get(), 0, sizeof(double) * C.d.H, s));
+  PA_CUDA(cudaMemsetAsync(acc.get(), 0, sizeof(double), s));
+  const BoxGeo<float> g = box_geo<float>(F, P.ep);
+  const float* w0 = level_w32(H, 0);
+  const float* ch0 = H.cheb.get();
+  const BoxRed red{H.partials.get(), H.counter.get()};
+  const double vol1 = C.h[0] * C.h[1] * C.h[2] / 6.0;
+  for (int k = 0; k < nres; ++k) {
+    const double E = energies[k];
+    PA_CHECK(E > 0.0, "residual energies must be positive");
+    k_bperm_in<double, float><<<vec_blocks(N), kVT, 0, s>>>(int(N), node_of, m.lat_flip, res + int64_t(k) * n,
+                                                            r32.get());
+    k_bmask_f<<<int((N + kVT - 1) / kVT), kVT, 0, s>>>(int(N), F.mask, r32.get());
+    PA_LAUNCHED();
+    // z = V r; x_c = the level-1 correction of this cycle
+    vcycle_level<float, float, false>(P, H, 0, r32.get(), z32.get(), nullptr, nullptr, s, nullptr);
+    PA_CUDA(cudaMemcpyAsync(xc.get(), C.x.get(), sizeof(float) * 3 * N1, cudaMemcpyDeviceToDevice, s));
+    // rho = r - K z; the loss
+    launch_box<float>(F, g, w0, InVec<float, float>{z32.get(), nullptr, N}, OutRes<float>{rho.get(), r32.get(), F.mask, N},
+                      red, s);
+    k_bcoarse_loss<<<vec_blocks(n), kVT, 0, s>>>(n, r32.get(), z32.get(), rho.get(), 1.0 / E, H.partials.get(),
+                                                 H.counter.get(), acc.get());
+    PA_LAUNCHED();
+    // zeta = (I - K S) rho, a = A^-1 R zeta
+    launch_box<float>(F, g, w0, InDinvB<float>{rho.get(), F.dinv.get(), ch0, N},
+                      OutPre<float>{sr.get(), rho.get(), F.dinv.get(), ch0, N}, red, s);
+    launch_box<float>(F, g, w0, InVec<float, float>{sr.get(), nullptr, N},
+                      OutRes<float>{zeta.get(), rho.get(), F.mask, N}, red, s);
+    k_brestrict<<<int((N1 + kVT - 1) / kVT), kVT, 0, s>>>(C.d, F.d, zeta.get(), C.mask, C.b.get(), nullptr);
+    PA_LAUNCHED();
+    vcycle(P, H, 1, s, nullptr);
+    k_bbilinear<<<int((C.d.H + 255) / 256), 256, 0, s>>>(C.d, 1.0 / C.h[0], 1.0 / C.h[1], 1.0 / C.h[2], vol1,
+                                                        P.ep.iso(), C.x.get(), xc.get(), 2.0 / E, gw.get());
+    PA_LAUNCHED();
+  }
+  k_bgrad_delta<<<int((C.d.H + kVT - 1) / kVT), kVT, 0, s>>>(C.d.H, gw.get(), C.w64.get(), 1.0 / nres, grad);
+  PA_LAUNCHED();
+  double a = 0.0;
+  PA_CUDA(cudaMemcpyAsync(&a, acc.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
+  PA_CUDA(cudaStreamSynchronize(s));
+  *loss = a / nres;
 }
 
 void box_entry_gradient_z(Problem& P, const double* z, const double* u, double* vals) {

@@ -43,6 +43,7 @@ struct BoxHierarchy;
 struct Problem {
   Mesh* mesh = nullptr;
   LearnedPC* pc = nullptr;  // network of PA_SOLVER_FCG_LEARNED (not owned)
+  LearnedPC* coarse_pc = nullptr;  // learned level-1 weight correction of the box multigrid (not owned)
   MgHierarchy* mg = nullptr;  // coarse levels of PA_SOLVER_PCG_MG (owned; mg_release)
   BoxHierarchy* boxmg = nullptr;  // the same on box kernels (owned; boxmg_release)
   ElasticParams ep{};
@@ -98,6 +99,15 @@ bool box_gradient_u(Problem& P, const double* z, double* entries);
 void box_entry_apply(Problem& P, const double* z, const double* u, double* y);
 void box_entry_energy(Problem& P, const double* z, const double* u, double* value, double* grad_z);
 void box_entry_gradient_z(Problem& P, const double* z, const double* u, double* vals);
+// Learned level-1 weights of the box multigrid (pa_boxmg.cu): the level-1 hex
+// grid (false: no box multigrid), the network's input features for control z
+// (5 per level-1 hex, device), and the loss and dL/ddelta of the V-cycle on
+// residual/error pairs for an explicit correction delta (device arrays;
+// energies and loss on the host).
+bool boxmg_coarse_grid(const Problem& P, int dims[3]);
+void boxmg_coarse_features(Problem& P, const double* z, float* feat);
+void boxmg_coarse_sensitivity(Problem& P, const double* z, const float* delta, int nres, const double* res,
+                              const double* energies, double* loss, float* grad);
 bool box_apply_eligible(const Problem& P);
 bool boxmg_eligible(const Problem& P);
 // false (nothing written) when the coarsest operator is singular
