@@ -544,7 +544,7 @@ pa_status pa_problem_set_preconditioner(pa_problem* problem, pa_pc* pc);
  * No counterpart in the reference (it solves with AmgX / Belos).  The box
  * multigrid of PA_SOLVER_PCG_MG gives each level-1 hex the mean weight of its
  * children; a network (pa_pc on the level-1 hex grid: gx, gy, gz = its hex
- * counts) may multiply it by exp(delta), delta its first output channel, fed
+ * counts) may multiply it by exp(0.5 tanh(delta)), delta its first output channel, fed
  * with 5 features per level-1 hex (logarithms of the mean, geometric mean,
  * minimum and maximum child weight, and the fraction of children inside the
  * box).  A network whose last layer is zero (a new one) leaves the method
@@ -559,7 +559,8 @@ pa_status pa_boxmg_coarse_features(pa_problem* problem, const double* z, float* 
  * interleaved, K e_s = r_s at control z, energies[s] = e_s . r_s) of
  * ||e_s - V r_s||_K^2 / ||e_s||_K^2, V the V-cycle, and its gradient in delta
  * (exact for a two-level hierarchy; deeper levels and level 1's smoother are
- * held fixed otherwise). */
+ * held fixed otherwise).  The fine smoother's spectral estimate is made from
+ * its cold start in every call, so equal inputs give equal results. */
 pa_status pa_boxmg_coarse_sensitivity(pa_problem* problem, const double* z, const float* delta,
                                       int32_t num_residuals, const double* residuals, const double* energies,
                                       double* loss, float* grad_delta);

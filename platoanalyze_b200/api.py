@@ -735,11 +735,14 @@ class LearnedCoarsening:
     convolutional network on the level-1 hex grid (the same four-layer BF16
     network as LearnedPreconditioner, tcgen05 forward, the library's backward
     kernels) maps 5 features per coarse hex to delta, and the coarse hex gets
-    mean(child weights) * exp(delta).  A new network (last layer zero) is the
-    plain multigrid.  Trained on residual/error pairs (K e = r) of SIMP designs
-    by Adam on the mean of ||e - V r||_K^2 / ||e||_K^2 (V the V-cycle), with
-    dloss/ddelta from pa_boxmg_coarse_sensitivity.  No counterpart in the
-    reference."""
+    mean(child weights) * exp(0.5 tanh(delta)).  A new network (last layer
+    zero) is the plain multigrid.  Trained on residual/error pairs (K e = r) of
+    SIMP designs by Adam on the mean of ||e - V r||_K^2 / ||e||_K^2 (V the
+    V-cycle), with dloss/ddelta from pa_boxmg_coarse_sensitivity; the plain
+    multigrid judges: every `check_every` steps the CG iterations on a
+    validation control are counted, and training keeps the parameters with
+    the fewest (the untrained ones unless some beat them).  No counterpart in
+    the reference."""
 
     def __init__(self, problem, seed=0):
         self.grid = problem.coarse_grid()
@@ -753,12 +756,24 @@ class LearnedCoarsening:
     def attach(self, problem):
         problem.set_coarse_network(self.net)
 
+    def iterations(self, problem, z, rel_tol=1e-8):
+        """CG iterations of the multigrid solve of control z with this network attached."""
+        self.attach(problem)
+        try:
+            _, st = problem.solution(z, options=SolveOptions("mg", rel_tol=rel_tol), allow_not_converged=True)
+        finally:
+            problem.set_coarse_network(None)
+        return st["iterations"]
+
     def train(self, problem, designs, residuals, energies, sample_design, steps=100, batch=4, learning_rate=3e-3,
-              seed=0, log=None):
+              seed=0, log=None, validation=None, check_every=20):
         """designs: D x nz controls; residuals[s] (3N, zero on constrained dofs)
         with K(designs[sample_design[s]]) e_s = residuals[s], energies[s] = e_s . r_s.
-        Each step takes one design and `batch` of its samples.  Returns the
-        loss history (per step, before the update)."""
+        Each step takes one design and `batch` of its samples.  validation: a
+        control whose multigrid CG iterations select the parameters kept
+        (None: the last ones).  Returns {"loss": per-step loss before the
+        update, "iterations": [(step, iterations)], "kept_step": step of the
+        kept parameters (0: untrained)}."""
         import torch
         dev = residuals.device
         sd = np.asarray(sample_design, np.int64)
@@ -770,6 +785,11 @@ class LearnedCoarsening:
         b1, b2, eps = 0.9, 0.999, 1e-8
         feats = {}
         hist = []
+        checks = []
+        best = None
+        if validation is not None:
+            best = (self.iterations(problem, validation), 0, params.clone())
+            checks.append((0, best[0]))
         for step in range(steps):
             d = int(sd[rng.integers(0, sd.size)])
             idx = np.flatnonzero(sd == d)
@@ -793,9 +813,21 @@ class LearnedCoarsening:
             mh = m / (1 - b1 ** (step + 1))
             vh = v / (1 - b2 ** (step + 1))
             params.sub_(learning_rate * mh / (vh.sqrt() + eps))
-            _abi.check(self.net._lib.pa_pc_set_params(self.net._h, _ptr(params, np.float32, self.net.num_params,
-                                                                         "params")))
-        return hist
+            self._upload(params)
+            if validation is not None and ((step + 1) % check_every == 0 or step + 1 == steps):
+                it = self.iterations(problem, validation)
+                checks.append((step + 1, it))
+                if it < best[0]:
+                    best = (it, step + 1, params.clone())
+        kept = steps
+        if best is not None:
+            self._upload(best[2])
+            kept = best[1]
+        return {"loss": hist, "iterations": checks, "kept_step": kept}
+
+    def _upload(self, params):
+        _abi.check(self.net._lib.pa_pc_set_params(self.net._h, _ptr(params, np.float32, self.net.num_params,
+                                                                     "params")))
 
     def close(self):
         self.net.close()

@@ -687,11 +687,13 @@ __global__ void k_bweights(BoxDims d, const double* __restrict__ z, int layout, 
   if (!same) atomicOr(differ, 1u);
 }
 
+constexpr double kDeltaScale = 0.5;
+
 // Coarse hex weight = mean of the 48 child tets (per-hex or tet-major fine
 // weights); the children in a padding layer (2 I + a >= f.nx, ...) count as
 // weight zero, so a coarse hex half outside the fine box has half the weight.
-// delta (may be null): a learned correction, w = mean exp(delta[h dstride])
-// with delta clamped to [-8, 8].
+// delta (may be null): a learned correction, w = mean exp(kDeltaScale
+// tanh(delta[h dstride])), within exp(+-0.5) of the mean.
 __global__ void k_bcoarse_w(BoxDims c, BoxDims f, const double* __restrict__ wf, int wm, double* __restrict__ w64,
                             float* __restrict__ w32, const float* __restrict__ delta, int dstride) {
   const int64_t h = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
@@ -709,7 +711,7 @@ __global__ void k_bcoarse_w(BoxDims c, BoxDims f, const double* __restrict__ wf,
           s += 6.0 * wf[fh];
       }
   double w = s / 48.0;
-  if (delta) w *= exp(fmin(fmax(double(delta[h * dstride]), -8.0), 8.0));
+  if (delta) w *= exp(kDeltaScale * tanh(double(delta[h * dstride])));
   w64[h] = w;
   w32[h] = float(w);
 }
@@ -838,11 +840,14 @@ __global__ void __launch_bounds__(kVT) k_bcoarse_loss(int64_t n, const float* __
   }
 }
 
-// dL/ddelta = w dL/dw / n (w = mean exp(delta), the weight the level holds)
-__global__ void k_bgrad_delta(int64_t H, const double* __restrict__ gw, const double* __restrict__ w, double inv_n,
-                              float* __restrict__ grad) {
+// dL/ddelta = w dL/dw kDeltaScale (1 - tanh^2 delta) / n (w the weight the
+// level holds)
+__global__ void k_bgrad_delta(int64_t H, const double* __restrict__ gw, const double* __restrict__ w,
+                              const float* __restrict__ delta, double inv_n, float* __restrict__ grad) {
   const int64_t h = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  if (h < H) grad[h] = float(w[h] * gw[h] * inv_n);
+  if (h >= H) return;
+  const double t = tanh(double(delta[h]));
+  grad[h] = float(w[h] * gw[h] * kDeltaScale * (1.0 - t * t) * inv_n);
 }
 
 // dinv = masked ? 0 : 1 / diag(K), diag from the tets around each node:
@@ -987,6 +992,10 @@ struct BoxHierarchy {
   // and an explicit correction (stride 1) that overrides the network while set
   DevBuf<float> cfeat, cout3;
   const float* delta_arg = nullptr;
+  // spectral estimates from the deterministic cold start (20 power steps)
+  // instead of the previous solve's vector: loss evaluations then depend on
+  // the control and the correction only
+  bool cold_spectrum = false;
   DevBuf<double> gu_k0;                // assembled K on the box: unpenalized blocks per table entry
   double gu_key[5] = {0, 0, 0, 0, 0};  // the hex sides and Lame constants they were made for
   // the captured outer iteration (two variants alternate the p buffers),
@@ -1350,7 +1359,7 @@ bool boxmg_setup(Problem& P, const double* z) {
       L.pw1.resize(n3);
       L.pw_valid = false;
     }
-    const bool warm = L.pw_valid;
+    const bool warm = L.pw_valid && !H.cold_spectrum;
     if (!warm)
       k_bseed<<<vec_blocks(L.d.N), kVT, 0, s>>>(int(L.d.N), L.mask, L.pw0.get(), H.partials.get(), H.counter.get(), nl);
     else
@@ -1380,7 +1389,7 @@ bool boxmg_setup(Problem& P, const double* z) {
   if (flag != 0.0) return false;
   for (size_t l = 0; l < NS; ++l) {
     BoxLevel& L = *H.L[l];
-    const bool warm = L.pw_valid;
+    const bool warm = L.pw_valid && !H.cold_spectrum;
     const int steps = warm ? kPowerWarm : kPower;
     PA_CHECK(h[l * (kPower + 1)] > 0.0, "multigrid level without free dofs");
     double lam = 0.0;
@@ -1966,7 +1975,7 @@ void box_entry_apply(Problem& P, const double* z, const double* u, double* y) {
 
 // ------------------------------------------- learned coarse-level weights --
 // The level-1 weights of the box multigrid may carry a learned correction
-// w1 = mean exp(delta) (k_bcoarse_w), delta from a convolutional network on the
+// w1 = mean exp(0.5 tanh(delta)) (k_bcoarse_w), delta from a network on the
 // level-1 hex grid (pa_learned.cu) fed with k_bcoarse_feat.  Training needs
 // dL/ddelta of the V-cycle's energy-norm error on residual/error pairs
 // (K e = r, E = e . r): with z = V r, L = ||e - z||_K^2 / E = 1 - (r.z + z.rho) / E
@@ -2013,14 +2022,17 @@ void boxmg_coarse_sensitivity(Problem& P, const double* z, const float* delta, i
   boxmg_ensure(P);
   BoxHierarchy& H = *P.boxmg;
   H.delta_arg = delta;
+  H.cold_spectrum = true;
   bool ok = false;
   try {
     ok = boxmg_setup(P, z);
   } catch (...) {
     H.delta_arg = nullptr;
+    H.cold_spectrum = false;
     throw;
   }
   H.delta_arg = nullptr;
+  H.cold_spectrum = false;
   PA_CHECK(ok, "singular coarsest operator");
   cudaStream_t s = P.stream;
   upload_cheb(H, s);
@@ -2066,7 +2078,7 @@ void boxmg_coarse_sensitivity(Problem& P, const double* z, const float* delta, i
                                                         P.ep.iso(), C.x.get(), xc.get(), 2.0 / E, gw.get());
     PA_LAUNCHED();
   }
-  k_bgrad_delta<<<int((C.d.H + kVT - 1) / kVT), kVT, 0, s>>>(C.d.H, gw.get(), C.w64.get(), 1.0 / nres, grad);
+  k_bgrad_delta<<<int((C.d.H + kVT - 1) / kVT), kVT, 0, s>>>(C.d.H, gw.get(), C.w64.get(), delta, 1.0 / nres, grad);
   PA_LAUNCHED();
   double a = 0.0;
   PA_CUDA(cudaMemcpyAsync(&a, acc.get(), sizeof(double), cudaMemcpyDeviceToHost, s));

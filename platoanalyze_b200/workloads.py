@@ -84,11 +84,12 @@ def oc_update(rho, dc, volfrac, move=0.2, eta=0.5, rho_min=1e-3):
 
 
 def simp_training_pairs(prob, dims, iterations=30, snapshots=(8, 32, 128, 512), volfrac=0.4, move=0.2,
-                        check_every=64, device="cuda", log=None):
+                        check_every=64, device="cuda", log=None, solver="mixed", first=0):
     """Run `iterations` SIMP/OC design iterations on the cantilever; at each,
-    the plain (Jacobi-PCG) solve to 1e-10 gives u*, and the iterates x_k of
-    plain solves stopped after k in `snapshots` iterations give the pairs
-    e = u* - x_k, r = K e (constrained operator), E = e . r.
+    the plain solve (solver "mixed": Jacobi-PCG; "mg": the box multigrid CG)
+    to 1e-10 gives u*, and the iterates x_k of plain solves stopped after k in
+    `snapshots` iterations give the pairs e = u* - x_k, r = K e (constrained
+    operator), E = e . r; pairs are taken from design iteration `first` on.
 
     Returns (densities [n_it x C], sample_density, residuals [n_s x 3N],
     energies, final_density, history) with the big arrays as torch tensors on
@@ -100,7 +101,7 @@ def simp_training_pairs(prob, dims, iterations=30, snapshots=(8, 32, 128, 512), 
     H = nx * ny * nz
     rho = np.full(H, volfrac)
     dens, sd, res, en, hist = [], [], [], [], []
-    plain = SolveOptions("mixed", rel_tol=1e-10, check_every=check_every)
+    plain = SolveOptions(solver, rel_tol=1e-10, check_every=check_every)
     for it in range(iterations):
         zc = torch.tensor(np.repeat(rho, 6), device=device)
         u, st = prob.solution(zc, options=plain)
@@ -108,8 +109,8 @@ def simp_training_pairs(prob, dims, iterations=30, snapshots=(8, 32, 128, 512), 
         g = prob.criterion_gradient(zc, u)  # compliance sensitivity at equilibrium (<= 0), per cell
         dc = g.view(-1, 6).sum(1).cpu().numpy()
         dens.append(zc)
-        for k in snapshots:
-            xk, _ = prob.solution(zc, options=SolveOptions("mixed", rel_tol=1e-14, max_iters=k,
+        for k in (snapshots if it >= first else ()):
+            xk, _ = prob.solution(zc, options=SolveOptions(solver, rel_tol=1e-14, max_iters=k,
                                                            check_every=check_every), allow_not_converged=True)
             e = u - xk
             r = prob.apply(zc, e, constrained=True)
