@@ -894,6 +894,26 @@ def run_learned(args):
     ms_m, st_m, f_m = timed("mixed", max(1, args.steps // 2), 1)
     ms_d, st_d, f_d = timed("fp64", max(1, args.steps // 2), 1)
     ms_g, st_g, f_g = timed("mg", max(1, args.steps // 2), 1)
+    # learned level-1 weights of the box multigrid: pairs from multigrid
+    # solves of the same design iterations, training judged by the CG
+    # iterations on the last training design; the held-out final design
+    # solved with the parameters kept
+    from platoanalyze_b200.api import LearnedCoarsening
+    t0 = time.perf_counter()
+    dens_c, sd_c, res_c, en_c, _, _ = simp_training_pairs(prob, dims, iterations=args.simp_iterations,
+                                                          snapshots=(2, 4, 8, 16), solver="mg", first=8)
+    lc = LearnedCoarsening(prob, seed=0)
+    tr_c = lc.train(prob, dens_c, res_c, en_c, sd_c, steps=args.train_steps // 2, batch=4, learning_rate=3e-3, seed=1,
+                    validation=dens_c[-1], check_every=20)
+    t_c = time.perf_counter() - t0
+    lc.attach(prob)
+    ms_c, st_c, f_c = timed("mg", max(1, args.steps // 2), 1)
+    prob.set_coarse_network(None)
+    coarse = {"solve_s": ms_c * 1e-3, **st_c, "compliance_rel_err_vs_fp64": abs(f_c - f_d) / abs(f_d),
+              "validation_cg_iterations_by_step": tr_c["iterations"], "kept_step": tr_c["kept_step"],
+              "loss_first_20": float(np.mean(tr_c["loss"][:20])), "loss_last_20": float(np.mean(tr_c["loss"][-20:])),
+              "pairs": int(len(sd_c)), "pairs_and_training_s": t_c}
+    lc.close()
     line = {
         "metric": METRIC, "value": C / (ms_l * 1e-3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_l, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -907,6 +927,7 @@ def run_learned(args):
         "jacobi_mixed": {"solve_s": ms_m * 1e-3, **st_m, "compliance_rel_err_vs_fp64": abs(f_m - f_d) / abs(f_d)},
         "jacobi_fp64": {"solve_s": ms_d * 1e-3, **st_d},
         "multigrid": {"solve_s": ms_g * 1e-3, **st_g, "compliance_rel_err_vs_fp64": abs(f_g - f_d) / abs(f_d)},
+        "multigrid_learned_coarse_weights": coarse,
         "speedup_learned_vs_fp64": ms_d / ms_l, "speedup_mixed_vs_fp64": ms_d / ms_m,
         "speedup_multigrid_vs_fp64": ms_d / ms_g,
         "training": tr, "pair_generation_s": t_pairs,
