@@ -1856,30 +1856,48 @@ __global__ void __launch_bounds__(256) k_benergy(BoxDims d, double ih0, double i
 // are g_0 = -e_a0, g_m = e_a(m-1) - e_am, g_3 = e_a2 (axes a_m of the path,
 // over the hex side), so the nodal force of path vertex m is the difference
 // of two stress columns.  The cell's node ids give each vertex slot's corner
-// (any vertex order of a template tet).  A warp stages its 32 cells' 384
-// values in shared memory and writes them as contiguous 256-byte rows.
+// (any vertex order of a template tet).  A warp's 32 cells lie in at most 7
+// hexes: the warp first loads those hexes' 8 corner displacements into shared
+// memory (168 values, instead of 12 gathers per cell), and at the end stages
+// its 384 outputs there and writes them as contiguous 256-byte rows.
 __global__ void __launch_bounds__(256) k_bgradient_z(BoxDims d, double ih0, double ih1, double ih2, double vol,
                                                      Iso<double> iso, double p, double pmin,
                                                      const int4* __restrict__ cells, const double* __restrict__ u,
                                                      const double* __restrict__ z, double* __restrict__ vals) {
   constexpr int kRow = 13;  // staging stride per cell (odd: two-way bank conflicts at most)
+  constexpr int kHex = 7;   // hexes of a warp's 32 cells at most
   __shared__ double stage[8][32 * kRow];
+  __shared__ double ucor[8][kHex * 24];  // [hex][corner][component]
+  __shared__ int sb0[8][kHex];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   // 32-bit indices: the box path has 3 N < 2^31, so 6 H < 2^31
   const int C = int(6 * d.H);
   const int c0 = blockIdx.x * blockDim.x + 32 * w;
+  if (c0 >= C) return;  // whole warp past the end (warp-uniform)
   const int c = c0 + lane;
+  const int plane = d.px * d.py;
+  const int hA = c0 / 6, hB = min(c0 + 31, C - 1) / 6, nh = hB - hA + 1;
+  if (lane < nh) {
+    const int h = hA + lane;
+    const int hy = h / d.nx, k = hy / d.ny;
+    sb0[w][lane] = (h - hy * d.nx) + d.px * ((hy - k * d.ny) + d.py * k);
+  }
+  __syncwarp();
+  for (int e = lane; e < nh * 24; e += 32) {
+    const int q = e / 24, r = e - 24 * q, cr = r / 3, cc = r - 3 * cr;
+    const int node = sb0[w][q] + (cr & 1) + d.px * ((cr >> 1) & 1) + plane * (cr >> 2);
+    ucor[w][e] = u[3 * int64_t(node) + cc];
+  }
+  __syncwarp();
   double* st = stage[w] + kRow * lane;
   if (c < C) {
     const int h = c / 6;
     const int t = c - 6 * h;
-    const int hy = h / d.nx, k = hy / d.ny;
-    const int i = h - hy * d.nx, j = hy - k * d.ny;
-    const int plane = d.px * d.py;
-    const int b0 = i + d.px * (j + d.py * k);
-    const double ih[3] = {ih0, ih1, ih2};
-    int ax[3], off[4];
-    double uv[4][3];
+    const int b0 = sb0[w][h - hA];
+    const double* uc = ucor[w] + 24 * (h - hA);
+    // the path's axes and corners (selects, not indexed arrays: t varies per thread)
+    auto ihs = [&](int a) { return a == 0 ? ih0 : a == 1 ? ih1 : ih2; };
+    int ax[3], off[4], cor[4];
     int q = 0;
 #pragma unroll
     for (int m = 0; m < 4; ++m) {
@@ -1887,24 +1905,30 @@ __global__ void __launch_bounds__(256) k_bgradient_z(BoxDims d, double ih0, doub
         ax[m - 1] = path_axis(t, m - 1);
         q |= 1 << ax[m - 1];
       }
+      cor[m] = q;
       off[m] = (q & 1) + d.px * ((q >> 1) & 1) + plane * (q >> 2);
-#pragma unroll
-      for (int cc = 0; cc < 3; ++cc) uv[m][cc] = u[3 * int64_t(b0 + off[m]) + cc];
     }
-    double du[3][3];
+    // edge differences g[m] = (u(v_m+1) - u(v_m)) / h along axis ax[m]; column a of
+    // grad u is the g[m] with ax[m] == a
+    double g[3][3];
 #pragma unroll
     for (int m = 0; m < 3; ++m) {
-      const int a = ax[m];
+      const double s = ihs(ax[m]);
 #pragma unroll
-      for (int cc = 0; cc < 3; ++cc) du[cc][a] = (uv[m + 1][cc] - uv[m][cc]) * ih[a];
+      for (int cc = 0; cc < 3; ++cc) g[m][cc] = (uc[3 * cor[m + 1] + cc] - uc[3 * cor[m] + cc]) * s;
     }
+    double du[3][3];  // du[cc][a]
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) du[cc][a] = ax[0] == a ? g[0][cc] : ax[1] == a ? g[1][cc] : g[2][cc];
     const double e[6] = {du[0][0], du[1][1], du[2][2], du[1][2] + du[2][1], du[0][2] + du[2][0],
                          du[0][1] + du[1][0]};
     double sg[6];
     tet_stress(iso, vol * simp_deriv(z[c], p, pmin), e, sg);
-    // stress column a (Voigt: 0 xx, 1 yy, 2 zz, 3 yz, 4 xz, 5 xy) times ih[a]
+    // stress column a (Voigt: 0 xx, 1 yy, 2 zz, 3 yz, 4 xz, 5 xy) times 1 / h_a
     auto col = [&](int a, double (&o)[3]) {
-      const double s = ih[a];
+      const double s = ihs(a);
       o[0] = s * (a == 0 ? sg[0] : a == 1 ? sg[5] : sg[4]);
       o[1] = s * (a == 0 ? sg[5] : a == 1 ? sg[1] : sg[3]);
       o[2] = s * (a == 0 ? sg[4] : a == 1 ? sg[3] : sg[2]);
