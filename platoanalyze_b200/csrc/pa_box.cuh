@@ -218,8 +218,12 @@ __device__ __forceinline__ void box_hex(const T (&u)[8][3], const T (&lw)[6], co
 // Node indices are 32-bit (3 N < 2^31).  Node plane p is formed three hex
 // layers ahead into buffer (p - k0 + 1) % 4.
 // Grid: (ceil(px / 31), ceil(py / 7), ceil(pz / kz)) CTAs of 256 threads.
+// The FP64 instances with per-cell controls (the per-cell entry points) are
+// held to 128 registers for two CTAs per SM: measured on 160x80x80, the
+// residual 105 -> 87 us with the few spills this costs; the FP64 CG apply
+// (about 200 registers) spills heavily at that bound and keeps one CTA per SM.
 template <typename T, int WM, bool CUBE, class In, class Out>
-__global__ void __launch_bounds__(kBoxThreads) k_box(BoxDims d, BoxGeo<T> g, BoxW<T, WM> bw, int kz, In in,
+__global__ void __launch_bounds__(kBoxThreads, (sizeof(T) == 8 && WM == 2) ? 2 : 1) k_box(BoxDims d, BoxGeo<T> g, BoxW<T, WM> bw, int kz, In in,
                                                      Out out, BoxRed red, const double* skip) {
   // skip (may be null): two flags; the launch is a no-op when either is set
   // (a solve that converged or broke down inside a batch of captured iterations)

@@ -1947,18 +1947,15 @@ __global__ void __launch_bounds__(256) k_bgradient_z(BoxDims d, double ih0, doub
         f[3][cc] = s2[cc];
       }
     }
+    // path vertex m goes to the cell's vertex slot n whose node is at offset
+    // off[m] from the hex's base node (the four slots are the four corners)
     const int4 cv = cells[c];
-    const int vs[4] = {cv.x - b0, cv.y - b0, cv.z - b0, cv.w - b0};
+    const int vs0 = cv.x - b0, vs1 = cv.y - b0, vs2 = cv.z - b0;
 #pragma unroll
-    for (int n = 0; n < 4; ++n) {
-      double r[3] = {0.0, 0.0, 0.0};
+    for (int m = 0; m < 4; ++m) {
+      const int n = vs0 == off[m] ? 0 : vs1 == off[m] ? 1 : vs2 == off[m] ? 2 : 3;
 #pragma unroll
-      for (int m = 0; m < 4; ++m)
-        if (vs[n] == off[m])
-#pragma unroll
-          for (int cc = 0; cc < 3; ++cc) r[cc] = f[m][cc];
-#pragma unroll
-      for (int cc = 0; cc < 3; ++cc) st[3 * n + cc] = r[cc];
+      for (int cc = 0; cc < 3; ++cc) st[3 * n + cc] = f[m][cc];
     }
   }
   __syncwarp();
