@@ -1070,8 +1070,10 @@ def run_batched(args):
             mg_ms.append(e0.elapsed_time(e1))
             mg_its = its_k
         # the same problems from 8 host threads, each box on its own stream
-        # (the library releases no lock it holds across calls; ctypes drops the
-        # GIL), largest boxes first, time from the host clock around the batch
+        # (ctypes drops the GIL), largest boxes first, time from the host clock
+        # around the batch.  Each problem's first solve (hierarchy and graph
+        # capture) runs in this thread: concurrent first solves from several
+        # threads failed inside a capture in one run
         import threading
         streams = [torch.cuda.Stream() for _ in probs]
         probs_t = []
@@ -1099,8 +1101,11 @@ def run_batched(args):
             except Exception as ex:  # reported after the join
                 errors.append(ex)
 
+        for k in order:
+            _, p2, zi, ui = probs_t[k]
+            p2.solution(zi, ui, options=mg_opts)
         thr_ms = []
-        for rep in range(1 + max(1, args.steps)):  # the first pass builds hierarchies and graphs
+        for rep in range(1 + max(1, args.steps)):  # the first pass is a warm-up
             flush.fill_(1)
             torch.cuda.synchronize()
             t0 = time.perf_counter()

@@ -1585,14 +1585,28 @@ bool solve_boxmg(Problem& P, const double* z, const double* b, double* x_out, co
       double* pnew = k == 0 ? H.p1.get() : H.p0.get();
       const int64_t before = g_box_launches;
       PA_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-      vcycle_level<double, double, true>(P, H, 0, r, zv, r, sc, s, sc + kBreak);
-      launch_box<double>(F, box_geo<double>(F, P.ep), w64, InCgP{zv, pold, pnew, sc, N},
-                         OutCgQ{H.q.get(), zv, pold, mask, sc, N}, red, s, sc + kBreak);
-      k_bcg_update<<<vec_blocks(n), kVT, 0, s>>>(n, sc, pnew, H.q.get(), x, r, H.partials.get(), H.counter.get());
+      try {
+        vcycle_level<double, double, true>(P, H, 0, r, zv, r, sc, s, sc + kBreak);
+        launch_box<double>(F, box_geo<double>(F, P.ep), w64, InCgP{zv, pold, pnew, sc, N},
+                           OutCgQ{H.q.get(), zv, pold, mask, sc, N}, red, s, sc + kBreak);
+        k_bcg_update<<<vec_blocks(n), kVT, 0, s>>>(n, sc, pnew, H.q.get(), x, r, H.partials.get(), H.counter.get());
+      } catch (...) {
+        // end the capture so that the stream is usable again, then report
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(s, &g);
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        H.drop_graphs();
+        throw;
+      }
       g_box_launches += 1;
       cudaGraph_t graph = nullptr;
       const cudaError_t ce = cudaStreamEndCapture(s, &graph);
-      if (ce != cudaSuccess) throw Error(PA_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+      if (ce != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        H.drop_graphs();
+        throw Error(PA_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+      }
       const cudaError_t ie = cudaGraphInstantiate(&H.gexec[k], graph, 0);
       cudaGraphDestroy(graph);
       if (ie != cudaSuccess) {
@@ -1807,79 +1821,48 @@ struct OutAoS64 {  // y = K x, interleaved
 // Internal energy of every tet (1/2 V sigma(eps) . eps, unpenalized), summed
 // with the SIMP weights of the per-cell controls (box slot order 6 h + t) into
 // one partial per CTA, and dF/dz = dw/dz e0 per cell (grad_z may be null).
-// One thread per tet (cell c = 6 h + t, path tet t of hex h), warps striding
-// over chunks of 32 cells: a chunk lies in at most 7 hexes, whose 8 corner
-// displacements the warp loads into shared memory once; column axis(t, m) of grad u is the difference of u
-// along path edge m over h[axis] (selects, not indexed arrays: t varies per
-// thread).
+// Path tet t runs 0 -> +axis(t,0) -> +axis(t,1) -> 7, so column axis(t,m) of
+// grad u is the difference of u along edge m over h[axis].
 __global__ void __launch_bounds__(256) k_benergy(BoxDims d, double ih0, double ih1, double ih2, double vol,
                                                  Iso<double> iso, double p, double pmin, const double* __restrict__ u,
                                                  const double* __restrict__ z, double* __restrict__ partials,
                                                  double* __restrict__ grad_z) {
-  constexpr int kHex = 7;
   __shared__ double red[32];
-  __shared__ double ucor[8][kHex * 24];
-  __shared__ int sb0[8][kHex];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int C = int(6 * d.H);  // 3 N < 2^31 on the box path
-  const int plane = d.px * d.py;
+  const int64_t h = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   double f = 0.0;
-  // grid-stride over warp chunks of 32 cells (the grid is at most a few waves)
-  for (int c0 = (blockIdx.x * 8 + w) * 32; c0 < C; c0 += gridDim.x * 256) {
-    const int c = c0 + lane;
-    const int hA = c0 / 6, hB = min(c0 + 31, C - 1) / 6, nh = hB - hA + 1;
-    __syncwarp();  // the previous chunk's reads of ucor are done
-    if (lane < nh) {
-      const int h = hA + lane;
-      const int hy = h / d.nx, k = hy / d.ny;
-      sb0[w][lane] = (h - hy * d.nx) + d.px * ((hy - k * d.ny) + d.py * k);
-    }
-    __syncwarp();
-    for (int e = lane; e < nh * 24; e += 32) {
-      const int q = e / 24, r = e - 24 * q, cr = r / 3, cc = r - 3 * cr;
-      const int node = sb0[w][q] + (cr & 1) + d.px * ((cr >> 1) & 1) + plane * (cr >> 2);
-      ucor[w][e] = u[3 * int64_t(node) + cc];
-    }
-    __syncwarp();
-    if (c < C) {
-      const int h = c / 6;
-      const int t = c - 6 * h;
-      const double* uc = ucor[w] + 24 * (h - hA);
-      auto ihs = [&](int a) { return a == 0 ? ih0 : a == 1 ? ih1 : ih2; };
-      int ax[3], cor[4];
-      int q = 0;
+  if (h < d.H) {
+    const int i = int(h % d.nx), j = int((h / d.nx) % d.ny), k = int(h / (int64_t(d.nx) * d.ny));
+    const double ih[3] = {ih0, ih1, ih2};
+    double uc[8][3];
 #pragma unroll
-      for (int m = 0; m < 4; ++m) {
-        if (m > 0) {
-          ax[m - 1] = path_axis(t, m - 1);
-          q |= 1 << ax[m - 1];
-        }
-        cor[m] = q;
-      }
-      double g[3][3];
+    for (int q = 0; q < 8; ++q) {
+      const int64_t v = (i + (q & 1)) + int64_t(d.px) * ((j + ((q >> 1) & 1)) + int64_t(d.py) * (k + (q >> 2)));
+#pragma unroll
+      for (int c = 0; c < 3; ++c) uc[q][c] = u[3 * v + c];
+    }
+#pragma unroll
+    for (int t = 0; t < 6; ++t) {
+      double du[3][3];
+      int prev = 0;
 #pragma unroll
       for (int m = 0; m < 3; ++m) {
-        const double sc = ihs(ax[m]);
+        const int a = path_axis(t, m), nxt = prev | (1 << a);
 #pragma unroll
-        for (int cc = 0; cc < 3; ++cc) g[m][cc] = (uc[3 * cor[m + 1] + cc] - uc[3 * cor[m] + cc]) * sc;
+        for (int c = 0; c < 3; ++c) du[c][a] = (uc[nxt][c] - uc[prev][c]) * ih[a];
+        prev = nxt;
       }
-      double du[3][3];  // du[cc][a]
-#pragma unroll
-      for (int a = 0; a < 3; ++a)
-#pragma unroll
-        for (int cc = 0; cc < 3; ++cc) du[cc][a] = ax[0] == a ? g[0][cc] : ax[1] == a ? g[1][cc] : g[2][cc];
       const double e[6] = {du[0][0], du[1][1], du[2][2], du[1][2] + du[2][1], du[0][2] + du[2][0],
                            du[0][1] + du[1][0]};
       double sig[6];
       tet_stress(iso, vol, e, sig);
       const double e0 = 0.5 * voigt_dot(sig, e);
-      const double zt = z[c];
+      const double zt = z[6 * h + t];
       f += simp(zt, p, pmin) * e0;
-      if (grad_z) grad_z[c] = simp_deriv(zt, p, pmin) * e0;
+      if (grad_z) grad_z[6 * h + t] = simp_deriv(zt, p, pmin) * e0;
     }
   }
-  const double bs = block_sum_box(f, red);
-  if (threadIdx.x == 0) partials[blockIdx.x] = bs;
+  const double b = block_sum_box(f, red);
+  if (threadIdx.x == 0) partials[blockIdx.x] = b;
 }
 
 // VectorFunction::gradient_z with per-cell controls: dR/dz of every cell, 12
@@ -2154,7 +2137,7 @@ void box_entry_energy(Problem& P, const double* z, const double* u, double* valu
   boxmg_ensure(P);
   BoxHierarchy& H = *P.boxmg;
   const BoxLevel& F = *H.L[0];
-  const int blocks = int(std::min<int64_t>((6 * F.d.H + 255) / 256, 8 * num_sms()));
+  const int blocks = int((F.d.H + 255) / 256);
   if (H.e_partials.n < size_t(blocks)) H.e_partials.resize(blocks);
   const double vol = F.h[0] * F.h[1] * F.h[2] / 6.0;
   k_benergy<<<blocks, 256, 0, P.stream>>>(F.d, 1.0 / F.h[0], 1.0 / F.h[1], 1.0 / F.h[2], vol, P.ep.iso(), P.ep.p,
