@@ -202,6 +202,89 @@ __device__ __forceinline__ void box_hex(const T (&u)[8][3], const T (&lw)[6], co
   }
 }
 
+// The same with the six tet weights and the Lame parameters passed apart, each
+// tet forming its own products: fewer live registers, used by the FP64
+// per-cell-control instances held to 128 registers (the FP32 instances keep
+// the form above, which stays within their 128).
+template <bool CUBE, typename T>
+__device__ __forceinline__ void box_hex_w(const T (&u)[8][3], const T (&w)[6], T lam, T mu, const T (&ih)[3],
+                                          T (&f)[8][3]) {
+  T X00[3], X10[3], X01[3], X11[3], Y00[3], Y10[3], Y01[3], Y11[3], Z00[3], Z10[3], Z01[3], Z11[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    X00[c] = u[1][c] - u[0][c];
+    X10[c] = u[3][c] - u[2][c];
+    X01[c] = u[5][c] - u[4][c];
+    X11[c] = u[7][c] - u[6][c];
+    Y00[c] = u[2][c] - u[0][c];
+    Y10[c] = u[3][c] - u[1][c];
+    Y01[c] = u[6][c] - u[4][c];
+    Y11[c] = u[7][c] - u[5][c];
+    Z00[c] = u[4][c] - u[0][c];
+    Z10[c] = u[5][c] - u[1][c];
+    Z01[c] = u[6][c] - u[2][c];
+    Z11[c] = u[7][c] - u[3][c];
+    if constexpr (!CUBE) {
+      X00[c] *= ih[0]; X10[c] *= ih[0]; X01[c] *= ih[0]; X11[c] *= ih[0];
+      Y00[c] *= ih[1]; Y10[c] *= ih[1]; Y01[c] *= ih[1]; Y11[c] *= ih[1];
+      Z00[c] *= ih[2]; Z10[c] *= ih[2]; Z01[c] *= ih[2]; Z11[c] *= ih[2];
+    }
+  }
+  // stress columns (edge fluxes) of a tet with gradient columns gx, gy, gz
+  auto tet = [&](const T (&gx)[3], const T (&gy)[3], const T (&gz)[3], T l, T m, T (&sx)[3], T (&sy)[3],
+                 T (&sz)[3]) {
+    const T lt = l * (gx[0] + gy[1] + gz[2]);
+    const T m2 = m + m;
+    const T sxy = m * (gy[0] + gx[1]), sxz = m * (gz[0] + gx[2]), syz = m * (gz[1] + gy[2]);
+    sx[0] = fma(m2, gx[0], lt);
+    sy[1] = fma(m2, gy[1], lt);
+    sz[2] = fma(m2, gz[2], lt);
+    sx[1] = sy[0] = sxy;
+    sx[2] = sz[0] = sxz;
+    sy[2] = sz[1] = syz;
+    if constexpr (!CUBE) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        sx[c] *= ih[0];
+        sy[c] *= ih[1];
+        sz[c] *= ih[2];
+      }
+    }
+  };
+  T qX00[3], qX10[3], qX01[3], qX11[3], qY00[3], qY10[3], qY01[3], qY11[3], qZ00[3], qZ10[3], qZ01[3], qZ11[3];
+  T a[3], b[3], c3[3];
+  tet(X10, Y00, Z11, w[0] * lam, w[0] * mu, qX10, qY00, qZ11);  // t0
+  tet(X11, Y00, Z01, w[1] * lam, w[1] * mu, qX11, a, qZ01);      // t1
+#pragma unroll
+  for (int c = 0; c < 3; ++c) qY00[c] += a[c];
+  tet(X11, Y01, Z00, w[2] * lam, w[2] * mu, a, qY01, qZ00);      // t2
+#pragma unroll
+  for (int c = 0; c < 3; ++c) qX11[c] += a[c];
+  tet(X01, Y11, Z00, w[3] * lam, w[3] * mu, qX01, qY11, a);      // t3
+#pragma unroll
+  for (int c = 0; c < 3; ++c) qZ00[c] += a[c];
+  tet(X00, Y11, Z10, w[4] * lam, w[4] * mu, qX00, a, qZ10);      // t4
+#pragma unroll
+  for (int c = 0; c < 3; ++c) qY11[c] += a[c];
+  tet(X00, Y10, Z11, w[5] * lam, w[5] * mu, b, qY10, c3);        // t5
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    qX00[c] += b[c];
+    qZ11[c] += c3[c];
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    f[0][c] = -(qX00[c] + qY00[c]) - qZ00[c];
+    f[1][c] = qX00[c] - qY10[c] - qZ10[c];
+    f[2][c] = qY00[c] - qX10[c] - qZ01[c];
+    f[3][c] = qX10[c] + qY10[c] - qZ11[c];
+    f[4][c] = qZ00[c] - qX01[c] - qY01[c];
+    f[5][c] = qX01[c] + qZ10[c] - qY11[c];
+    f[6][c] = qY01[c] + qZ01[c] - qX11[c];
+    f[7][c] = qX11[c] + qY11[c] + qZ11[c];
+  }
+}
+
 // y = K x on the box with a fused input former and epilogue.  Both are split
 // into a load part (global loads into registers, issued a hex layer before
 // the values are needed) and a compute part:
@@ -218,12 +301,14 @@ __device__ __forceinline__ void box_hex(const T (&u)[8][3], const T (&lw)[6], co
 // Node indices are 32-bit (3 N < 2^31).  Node plane p is formed three hex
 // layers ahead into buffer (p - k0 + 1) % 4.
 // Grid: (ceil(px / 31), ceil(py / 7), ceil(pz / kz)) CTAs of 256 threads.
-// The FP64 instances with per-cell controls (the per-cell entry points) are
-// held to 128 registers for two CTAs per SM: measured on 160x80x80, the
-// residual 105 -> 87 us with the few spills this costs; the FP64 CG apply
-// (about 200 registers) spills heavily at that bound and keeps one CTA per SM.
+// Two CTAs of 256 threads per SM (at most 128 registers) for every FP32
+// instance and for the FP64 instances with per-cell controls (the per-cell
+// entry points): measured on 160x80x80, the FP64 residual 105 -> 87 us with
+// the few spills this costs (fewer still with box_hex_w and the late weight
+// loads).  The FP64 CG apply (about 210 registers) spills heavily at that
+// bound and did not speed up the solve, so those instances keep one CTA per SM.
 template <typename T, int WM, bool CUBE, class In, class Out>
-__global__ void __launch_bounds__(kBoxThreads, (sizeof(T) == 8 && WM == 2) ? 2 : 1) k_box(BoxDims d, BoxGeo<T> g, BoxW<T, WM> bw, int kz, In in,
+__global__ void __launch_bounds__(kBoxThreads, (sizeof(T) == 4 || WM == 2) ? 2 : 1) k_box(BoxDims d, BoxGeo<T> g, BoxW<T, WM> bw, int kz, In in,
                                                      Out out, BoxRed red, const double* skip) {
   // skip (may be null): two flags; the launch is a no-op when either is set
   // (a solve that converged or broke down inside a batch of captured iterations)
@@ -307,8 +392,14 @@ __global__ void __launch_bounds__(kBoxThreads, (sizeof(T) == 8 && WM == 2) ? 2 :
     const int v = v0 + k * plane;
     typename Out::Pre pre;
     if (own) pre = out.load(v);
-    T lw[6], mw[6];
-    {
+    // FP64 per-cell-control instances (two CTAs per SM at 128 registers): the
+    // raw weights go into the hex work and the next layer's load follows it
+    constexpr bool kLateW = WM == 2 && sizeof(T) == 8;
+    T lw[6], mw[6], w6[6];
+    if constexpr (kLateW) {
+#pragma unroll
+      for (int t = 0; t < 6; ++t) w6[t] = wn[t];
+    } else {
       T w[WM ? 6 : 1];
 #pragma unroll
       for (int t = 0; t < (WM ? 6 : 1); ++t) w[t] = wn[t];
@@ -317,8 +408,8 @@ __global__ void __launch_bounds__(kBoxThreads, (sizeof(T) == 8 && WM == 2) ? 2 :
         lw[t] = w[WM ? t : 0] * g.lam;
         mw[t] = w[WM ? t : 0] * g.mu;
       }
+      load_w(k + 1);
     }
-    load_w(k + 1);
     T f[8][3];
     if (hex_ij && k >= 0 && k < d.nz) {
       T u[8][3];
@@ -334,11 +425,15 @@ __global__ void __launch_bounds__(kBoxThreads, (sizeof(T) == 8 && WM == 2) ? 2 :
         u[q + 4][1] = hi.y;
         u[q + 4][2] = hi.z;
       }
-      box_hex<CUBE>(u, lw, mw, g.ih, f);
+      if constexpr (kLateW)
+        box_hex_w<CUBE>(u, w6, g.lam, g.mu, g.ih, f);
+      else
+        box_hex<CUBE>(u, lw, mw, g.ih, f);
     } else {
 #pragma unroll
       for (int c = 0; c < 8; ++c) f[c][0] = f[c][1] = f[c][2] = T(0);
     }
+    if constexpr (kLateW) load_w(k + 1);
     // plane-k forces of the four corners: carried top of the layer below + bottom
     T P[4][3];
 #pragma unroll
