@@ -115,3 +115,63 @@ def test_batched_parts_match_the_oracle(pa, oracle_lib):
         res[dofs] = 0.0
         assert np.linalg.norm(res) <= 2e-8 * np.linalg.norm(F), p
         c0 += C
+
+
+def test_box_multigrid_solves_from_host_threads(pa):
+    """Independent box problems (odd and even sizes), one stream each: after
+    each problem's first solve in this thread, second solves from four host
+    threads give the same bits as second solves in sequence on twin problems,
+    and solve the oracle-checked system to the tolerance."""
+    import threading
+    import torch
+    from platoanalyze_b200.workloads import _box, cell_density
+    specs = [(17, 9, 9), (16, 8, 8), (21, 11, 7), (12, 12, 12), (9, 5, 5), (24, 8, 10), (15, 7, 9), (10, 10, 6)]
+    opts = pa.SolveOptions("mg", rel_tol=1e-9)
+
+    def make(i, dims):
+        nx, ny, nz = dims
+        cells, coords, faces, clamp = _box(nx, ny, nz)
+        mesh = pa.Mesh.from_arrays(cells, coords)
+        s = torch.cuda.Stream()
+        prob = pa.Problem(mesh, 1.0, 0.3, 3.0, 1e-9, control_layout="cell", stream=s.cuda_stream)
+        prob.add_traction(faces, np.array([0.0, 0.3, -1.0]) / (ny * nz))
+        prob.set_dirichlet(np.sort(np.concatenate([3 * clamp, 3 * clamp + 1, 3 * clamp + 2])).astype(np.int32))
+        z = torch.tensor(cell_density(dims, 40 + i, kind="smoothed", sigma=1.5, lo=0.01, hi=1.0), device="cuda")
+        u = torch.empty(3 * mesh.num_nodes, dtype=torch.float64, device="cuda")
+        return mesh, prob, z, u, s
+
+    seq = [make(i, d) for i, d in enumerate(specs)]
+    thr = [make(i, d) for i, d in enumerate(specs)]
+    for group in (seq, thr):
+        for mesh, prob, z, u, s in group:
+            _, st = prob.solution(z, u, options=opts)
+            assert st["converged"], st
+    ref = []
+    for mesh, prob, z, u, s in seq:
+        _, st = prob.solution(z, u, options=opts)
+        torch.cuda.synchronize()
+        ref.append((u.clone(), st["iterations"]))
+    errors = []
+
+    def worker(idx):
+        try:
+            for k in idx:
+                mesh, prob, z, u, s = thr[k]
+                _, st = prob.solution(z, u, options=opts)
+                assert st["converged"] and st["iterations"] == ref[k][1], (k, st)
+        except Exception as ex:
+            errors.append(ex)
+
+    threads = [threading.Thread(target=worker, args=(list(range(t, len(specs), 4)),)) for t in range(4)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    torch.cuda.synchronize()
+    assert not errors, errors
+    for k in range(len(specs)):
+        assert torch.equal(thr[k][3], ref[k][0]), k
+    for group in (seq, thr):
+        for mesh, prob, z, u, s in group:
+            prob.close()
+            mesh.close()
