@@ -988,6 +988,8 @@ struct BoxHierarchy {
   bool masks_valid = false;
   DevBuf<float> cheb;  // per smoothed level: 1 / theta, ca, c2 (read by the captured iteration)
   DevBuf<double> e_partials, e_value;  // the per-cell entry points' energy reduction
+  DevBuf<double> gu_k0;                // assembled K on the box: unpenalized blocks per table entry
+  double gu_key[5] = {0, 0, 0, 0, 0};  // the hex sides and Lame constants they were made for
   // learned coarse-weight correction: features and network output of level 1,
   // and an explicit correction (stride 1) that overrides the network while set
   DevBuf<float> cfeat, cout3;
@@ -2202,14 +2204,9 @@ BoxEdges make_box_edges() {
 
 constexpr int kGuNodes = 16;  // nodes per CTA of k_bgradient_u (15 slots each)
 
-// The block of an edge (v, w) is sum over its tets of w_t vol K0(t), K0 =
-// lam g_v g_w^T + mu g_w g_v^T + mu (g_v . g_w) I with g the vertices'
-// gradients; the thread accumulates A = sum w_t a a'^T of the integer edge
-// patterns a, a' (entries -1, 0, 1; g = a / h per axis) and forms
-// K = lam A + mu A^T + mu tr(A) I once, scaled by 1 / (h_i h_j).
 __global__ void __launch_bounds__(15 * kGuNodes) k_bgradient_u(BoxDims d, double vol, double p, double pmin,
-                                                             int layout, BoxEdges E, Iso<double> iso, double ih0,
-                                                             double ih1, double ih2, const double* __restrict__ z,
+                                                             int layout, BoxEdges E, const double* __restrict__ k0,
+                                                             const double* __restrict__ z,
                                                              const int32_t* __restrict__ rowmap,
                                                              double* __restrict__ vals) {
   // thread (slot, node) = (tid / 16, tid % 16): a warp holds two slots of 16
@@ -2227,9 +2224,14 @@ __global__ void __launch_bounds__(15 * kGuNodes) k_bgradient_u(BoxDims d, double
       return i >= 0 && i <= d.nx && j >= 0 && j <= d.ny && k >= 0 && k <= d.nz;
     };
     if (inside(vi + E.off[sl][0], vj + E.off[sl][1], vk + E.off[sl][2])) {
-      int rank = 0;
-      for (int q = 0; q < sl; ++q) rank += inside(vi + E.off[q][0], vj + E.off[q][1], vk + E.off[q][2]) ? 1 : 0;
-      double A[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      // the block's position in the row: its slot for an interior node (every
+      // neighbour exists), else the count of existing neighbours before it
+      int rank = sl;
+      if (vi == 0 || vj == 0 || vk == 0 || vi == d.nx || vj == d.ny || vk == d.nz) {
+        rank = 0;
+        for (int q = 0; q < sl; ++q) rank += inside(vi + E.off[q][0], vj + E.off[q][1], vk + E.off[q][2]) ? 1 : 0;
+      }
+      double K[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
       for (int o = 0; o < 8; ++o) {
         const int n = E.count[sl][o];
         if (n == 0) continue;
@@ -2249,28 +2251,15 @@ __global__ void __launch_bounds__(15 * kGuNodes) k_bgradient_u(BoxDims d, double
                               int64_t(d.px) * ((oj + ((c >> 1) & 1)) + int64_t(d.py) * (ok + (c >> 2)))];
             }
           }
-          const double w = simp(rho, p, pmin);
-          const int code = E.tet[sl][o][e], mv = (code >> 3) & 3, mw = code >> 5;
-          const int8_t* ga = E.grad[t][mv];
-          const int8_t* gb = E.grad[t][mw];
+          const double w = vol * simp(rho, p, pmin);
+          const double* kb = k0 + 9 * ((sl * 8 + o) * 6 + e);
 #pragma unroll
-          for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int j = 0; j < 3; ++j)
-              if (ga[i] * gb[j] != 0) A[3 * i + j] = fma(w, double(ga[i] * gb[j]), A[3 * i + j]);
+          for (int q = 0; q < 9; ++q) K[q] = fma(w, __ldg(kb + q), K[q]);
         }
       }
-      const double ih[3] = {ih0, ih1, ih2};
-#pragma unroll
-      for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j) A[3 * i + j] *= vol * ih[i] * ih[j];
-      const double tr = iso.mu * (A[0] + A[4] + A[8]);
       double* dst = stage + 9 * (int64_t(rowmap[v]) - base + rank);
 #pragma unroll
-      for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j) dst[3 * i + j] = iso.lam * A[3 * i + j] + iso.mu * A[3 * j + i] + (i == j ? tr : 0.0);
+      for (int q = 0; q < 9; ++q) dst[q] = K[q];
     }
   }
   __syncthreads();
@@ -2288,10 +2277,33 @@ bool box_gradient_u(Problem& P, const double* z, double* entries) {
   boxmg_ensure(P);
   BoxHierarchy& H = *P.boxmg;
   const BoxLevel& F = *H.L[0];
+  // the unpenalized 3 x 3 block of every (slot, hex corner, tet) entry: on a
+  // uniform box it depends only on the hex sides and the Lame constants
   const Iso<double> iso = P.ep.iso();
+  const double key[5] = {F.h[0], F.h[1], F.h[2], iso.lam, iso.mu};
+  if (!H.gu_k0.n || !std::equal(key, key + 5, H.gu_key)) {
+    std::vector<double> k0(size_t(15 * 8 * 6 * 9), 0.0);
+    const double ih[3] = {1.0 / F.h[0], 1.0 / F.h[1], 1.0 / F.h[2]};
+    for (int sl = 0; sl < 15; ++sl)
+      for (int o = 0; o < 8; ++o)
+        for (int e = 0; e < edges.count[sl][o]; ++e) {
+          const int code = edges.tet[sl][o][e], t = code & 7, mv = (code >> 3) & 3, mw = code >> 5;
+          double ga[3], gb[3];
+          for (int c = 0; c < 3; ++c) {
+            ga[c] = ih[c] * edges.grad[t][mv][c];
+            gb[c] = ih[c] * edges.grad[t][mw][c];
+          }
+          const double dd = iso.mu * (ga[0] * gb[0] + ga[1] * gb[1] + ga[2] * gb[2]);
+          double* kb = &k0[size_t(9 * ((sl * 8 + o) * 6 + e))];
+          for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) kb[3 * i + j] = iso.lam * ga[i] * gb[j] + iso.mu * ga[j] * gb[i] + (i == j ? dd : 0.0);
+        }
+    H.gu_k0.upload(k0.data(), k0.size(), P.stream);
+    std::copy(key, key + 5, H.gu_key);
+  }
   k_bgradient_u<<<int((F.d.N + kGuNodes - 1) / kGuNodes), 15 * kGuNodes, 0, P.stream>>>(
-      F.d, F.h[0] * F.h[1] * F.h[2] / 6.0, P.ep.p, P.ep.pmin, P.ep.layout, edges, iso, 1.0 / F.h[0], 1.0 / F.h[1],
-      1.0 / F.h[2], z, m.d_rowmap.get(), entries);
+      F.d, F.h[0] * F.h[1] * F.h[2] / 6.0, P.ep.p, P.ep.pmin, P.ep.layout, edges, H.gu_k0.get(), z,
+      m.d_rowmap.get(), entries);
   PA_LAUNCHED();
   return true;
 }
