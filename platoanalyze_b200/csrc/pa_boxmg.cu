@@ -526,33 +526,46 @@ __global__ void k_bset_bc(int64_t nbc, const int32_t* __restrict__ dofs, const d
 // Restriction (R = P^T of trilinear interpolation), coarse masked dofs zero.
 // The coarse level spans 2 c.nx fine hexes along x (and so on), at least the
 // fine level's f.nx: a fine level with an odd count is padded by one hex
-// layer that holds no fine node.
+// layer that holds no fine node.  The 27 fine neighbours' loads are unrolled
+// and predicated (a missing neighbour reads as zero), so that they are all in
+// flight at once: on the small levels these launches are a few CTAs whose
+// time was the chain of dependent loads.  The sum runs in the same order.
 __global__ void k_brestrict(BoxDims c, BoxDims f, const float* __restrict__ fv_in, const uint8_t* __restrict__ cmask,
-                            float* __restrict__ cv_out, const double* skip) {
+                            float* __restrict__ cv_out, const double* skip = nullptr) {
   if (skip && (skip[0] != 0.0 || skip[1] != 0.0)) return;
   const int v = blockIdx.x * blockDim.x + threadIdx.x;
   const int Nc = int(c.N), Nf = int(f.N);
   if (v >= Nc) return;
   const int I = v % c.px, J = (v / c.px) % c.py, K = v / (c.px * c.py);
-  float s[3] = {0.f, 0.f, 0.f};
-  for (int dc = -1; dc <= 1; ++dc) {
-    const int k = 2 * K + dc;
-    if (k < 0 || k >= f.pz) continue;
-    const float wc = dc ? 0.5f : 1.0f;
-    for (int db = -1; db <= 1; ++db) {
-      const int j = 2 * J + db;
-      if (j < 0 || j >= f.py) continue;
-      const float wb = wc * (db ? 0.5f : 1.0f);
-      for (int da = -1; da <= 1; ++da) {
-        const int i = 2 * I + da;
-        if (i < 0 || i >= f.px) continue;
-        const float w = wb * (da ? 0.5f : 1.0f);
-        const int fv = i + f.px * (j + f.py * k);
+  float val[27][3];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) s[d] += w * fv_in[d * Nf + fv];
+  for (int dc = 0; dc < 3; ++dc)
+#pragma unroll
+    for (int db = 0; db < 3; ++db)
+#pragma unroll
+      for (int da = 0; da < 3; ++da) {
+        const int i = 2 * I + da - 1, j = 2 * J + db - 1, k = 2 * K + dc - 1;
+        const bool in = i >= 0 && i < f.px && j >= 0 && j < f.py && k >= 0 && k < f.pz;
+        const int fv = in ? i + f.px * (j + f.py * k) : 0;
+        const int e = da + 3 * (db + 3 * dc);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) val[e][d] = in ? __ldg(&fv_in[d * Nf + fv]) : 0.f;
       }
-    }
-  }
+  float s[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+  for (int dc = 0; dc < 3; ++dc)
+#pragma unroll
+    for (int db = 0; db < 3; ++db)
+#pragma unroll
+      for (int da = 0; da < 3; ++da) {
+        const float w = (dc != 1 ? 0.5f : 1.0f) * (db != 1 ? 0.5f : 1.0f) * (da != 1 ? 0.5f : 1.0f);
+        const int i = 2 * I + da - 1, j = 2 * J + db - 1, k = 2 * K + dc - 1;
+        const bool in = i >= 0 && i < f.px && j >= 0 && j < f.py && k >= 0 && k < f.pz;
+        const int e = da + 3 * (db + 3 * dc);
+        if (in)
+#pragma unroll
+          for (int d = 0; d < 3; ++d) s[d] += w * val[e][d];
+      }
   const uint8_t mk = cmask[v];
 #pragma unroll
   for (int d = 0; d < 3; ++d) cv_out[d * Nc + v] = ((mk >> d) & 1) ? 0.f : s[d];
@@ -560,9 +573,10 @@ __global__ void k_brestrict(BoxDims c, BoxDims f, const float* __restrict__ fv_i
 
 // x_fine += P e (trilinear interpolation of the coarse correction), fine
 // masked dofs untouched (they stay zero).  Fine node i lies at coarse
-// position i / 2; every coarse node it reads exists (2 c.nx >= f.nx).
+// position i / 2; every coarse node it reads exists (2 c.nx >= f.nx).  The
+// (up to) eight coarse loads are unrolled and predicated, summed in order.
 __global__ void k_bprolong_add(BoxDims c, BoxDims f, const float* __restrict__ e, const uint8_t* __restrict__ fmask,
-                               float* __restrict__ x, const double* skip) {
+                               float* __restrict__ x, const double* skip = nullptr) {
   if (skip && (skip[0] != 0.0 || skip[1] != 0.0)) return;
   const int v = blockIdx.x * blockDim.x + threadIdx.x;
   const int Nc = int(c.N), Nf = int(f.N);
@@ -571,14 +585,28 @@ __global__ void k_bprolong_add(BoxDims c, BoxDims f, const float* __restrict__ e
   const int ia = i >> 1, ja = j >> 1, ka = k >> 1;
   const int ni = (i & 1) + 1, nj = (j & 1) + 1, nk = (k & 1) + 1;
   const float w = (ni == 1 ? 1.f : 0.5f) * (nj == 1 ? 1.f : 0.5f) * (nk == 1 ? 1.f : 0.5f);
-  float s[3] = {0.f, 0.f, 0.f};
-  for (int cc = 0; cc < nk; ++cc)
-    for (int b = 0; b < nj; ++b)
-      for (int a = 0; a < ni; ++a) {
-        const int cv = (ia + a) + c.px * ((ja + b) + c.py * (ka + cc));
+  float val[8][3];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) s[d] += e[d * Nc + cv];
+  for (int cc = 0; cc < 2; ++cc)
+#pragma unroll
+    for (int b = 0; b < 2; ++b)
+#pragma unroll
+      for (int a = 0; a < 2; ++a) {
+        const bool in = a < ni && b < nj && cc < nk;
+        const int cv = in ? (ia + a) + c.px * ((ja + b) + c.py * (ka + cc)) : 0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) val[a + 2 * (b + 2 * cc)][d] = in ? __ldg(&e[d * Nc + cv]) : 0.f;
       }
+  float s[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+  for (int cc = 0; cc < 2; ++cc)
+#pragma unroll
+    for (int b = 0; b < 2; ++b)
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+        if (a < ni && b < nj && cc < nk)
+#pragma unroll
+          for (int d = 0; d < 3; ++d) s[d] += val[a + 2 * (b + 2 * cc)][d];
   const uint8_t mk = fmask[v];
 #pragma unroll
   for (int d = 0; d < 3; ++d)
