@@ -343,20 +343,31 @@ __global__ void __launch_bounds__(kBoxThreads, (sizeof(T) == 4 || WM == 2) ? 2 :
     for (int q = 0; q < kSlots; ++q)
       if (fin[q] && p >= 0 && p < d.pz) raw[q] = in.load(fv[q] + p * plane, fown[q] && p >= k0 && p < k1);
   };
-  auto form_store = [&](int p, int b) {
+  auto form_store_from = [&](const typename In::Raw (&rr)[kSlots], int p, int b) {
 #pragma unroll
     for (int q = 0; q < kSlots; ++q) {
       const int e = threadIdx.x + q * kBoxThreads;
       if (e >= kBoxPlane) continue;
       T v[3] = {T(0), T(0), T(0)};
-      if (fin[q] && p >= 0 && p < d.pz) in.make(raw[q], fv[q] + p * plane, fown[q] && p >= k0 && p < k1, v);
+      if (fin[q] && p >= 0 && p < d.pz) in.make(rr[q], fv[q] + p * plane, fown[q] && p >= k0 && p < k1, v);
       xs[b][e] = BoxV4<T>(v[0], v[1], v[2]);
     }
   };
+  auto form_store = [&](int p, int b) { form_store_from(raw, p, b); };
 
-  for (int p = 0; p < 3; ++p) {
-    form_load(k0 - 1 + p);
-    form_store(k0 - 1 + p, p);
+  // the first three planes: every load issued before any is used (a CTA with
+  // a one-plane chunk forms nothing else, so these loads are its latency)
+  {
+    typename In::Raw raw3[3][kSlots];
+#pragma unroll
+    for (int pl = 0; pl < 3; ++pl) {
+      const int p = k0 - 1 + pl;
+#pragma unroll
+      for (int q = 0; q < kSlots; ++q)
+        if (fin[q] && p >= 0 && p < d.pz) raw3[pl][q] = in.load(fv[q] + p * plane, fown[q] && p >= k0 && p < k1);
+    }
+#pragma unroll
+    for (int pl = 0; pl < 3; ++pl) form_store_from(raw3[pl], k0 - 1 + pl, pl);
   }
   __syncthreads();
 
