@@ -355,22 +355,6 @@ __global__ void __launch_bounds__(kBoxThreads, (sizeof(T) == 4 || WM == 2) ? 2 :
   };
   auto form_store = [&](int p, int b) { form_store_from(raw, p, b); };
 
-  // the first three planes: every load issued before any is used (a CTA with
-  // a one-plane chunk forms nothing else, so these loads are its latency)
-  {
-    typename In::Raw raw3[3][kSlots];
-#pragma unroll
-    for (int pl = 0; pl < 3; ++pl) {
-      const int p = k0 - 1 + pl;
-#pragma unroll
-      for (int q = 0; q < kSlots; ++q)
-        if (fin[q] && p >= 0 && p < d.pz) raw3[pl][q] = in.load(fv[q] + p * plane, fown[q] && p >= k0 && p < k1);
-    }
-#pragma unroll
-    for (int pl = 0; pl < 3; ++pl) form_store_from(raw3[pl], k0 - 1 + pl, pl);
-  }
-  __syncthreads();
-
   // hex weights, loaded one layer ahead; hex (i, j, k) = h0 + k * layer
   const int layer = d.nx * d.ny, h0 = hex_ij ? i + d.nx * j : 0;
   T wn[WM ? 6 : 1];
@@ -388,7 +372,24 @@ __global__ void __launch_bounds__(kBoxThreads, (sizeof(T) == 4 || WM == 2) ? 2 :
       }
     }
   };
-  load_w(k0 - 1);
+  load_w(k0 - 1);  // the first layer's weights, in flight with the planes below
+
+  // the first three planes: every load issued before any is used (a CTA with
+  // a one-plane chunk forms nothing else, so these loads are its latency)
+  {
+    typename In::Raw raw3[3][kSlots];
+#pragma unroll
+    for (int pl = 0; pl < 3; ++pl) {
+      const int p = k0 - 1 + pl;
+#pragma unroll
+      for (int q = 0; q < kSlots; ++q)
+        if (fin[q] && p >= 0 && p < d.pz) raw3[pl][q] = in.load(fv[q] + p * plane, fown[q] && p >= k0 && p < k1);
+    }
+#pragma unroll
+    for (int pl = 0; pl < 3; ++pl) form_store_from(raw3[pl], k0 - 1 + pl, pl);
+  }
+  __syncthreads();
+
   const int v0 = i + d.px * j;
   T carry[4][3];
 #pragma unroll
