@@ -253,10 +253,15 @@ inline void gj_invert(cudaStream_t s, int64_t nd, double* A, const double* diag0
     PA_CHECK(occ > 0, "k_gj_invert does not fit on a multiprocessor");
     grid = sms * std::min(occ, 2);
   }
+  // no more CTAs than the largest phase has tiles (fewer CTAs also make the
+  // grid barriers cheaper): phase 2 updates (nb - 1) nb tiles, one CTA more
+  // inverts the next pivot tile
+  const int nb = int(nd / kGJ);
+  const int g = std::max(1, std::min(grid, std::max(2 * nb, (nb - 1) * nb + 1)));
   PA_CUDA(cudaMemsetAsync(sync, 0, sizeof(unsigned), s));
   int ndi = int(nd);
   void* args[] = {&ndi, &A, &diag0, &piv, &cp, &sync, &flag};
-  PA_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_gj_invert), dim3(unsigned(grid)), dim3(256),
+  PA_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_gj_invert), dim3(unsigned(g)), dim3(256),
                                       args, 0, s));
 }
 
