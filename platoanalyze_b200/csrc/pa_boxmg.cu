@@ -1040,22 +1040,10 @@ struct BoxHierarchy {
   } key;
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   int64_t per_iter = 0;
-  // side stream of the set-up: the coarsest inverse runs there beside the
-  // diagonals and spectral estimates of the other levels
-  cudaStream_t side = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   BoxHierarchy() = default;
   BoxHierarchy(const BoxHierarchy&) = delete;
   BoxHierarchy& operator=(const BoxHierarchy&) = delete;
-  ~BoxHierarchy() {
-    drop_graphs();
-    if (side) {
-      cudaStreamSynchronize(side);
-      cudaStreamDestroy(side);
-    }
-    if (ev_fork) cudaEventDestroy(ev_fork);
-    if (ev_join) cudaEventDestroy(ev_join);
-  }
+  ~BoxHierarchy() { drop_graphs(); }
   void drop_graphs() {
     for (auto& e : gexec) {
       if (e) cudaGraphExecDestroy(e);
@@ -1371,16 +1359,10 @@ bool boxmg_setup(Problem& P, const double* z) {
                                                                         Lc.w64.get(), Lc.mask, nd, Lc.dense.get());
     k_bdense_ident<<<int((nd + kVT - 1) / kVT), kVT, 0, s>>>(Lc.d.N, nd, Lc.mask, Lc.dense.get(), Lc.diag0.get());
     PA_LAUNCHED();
-    if (!H.side) {
-      PA_CUDA(cudaStreamCreateWithFlags(&H.side, cudaStreamNonBlocking));
-      PA_CUDA(cudaEventCreateWithFlags(&H.ev_fork, cudaEventDisableTiming));
-      PA_CUDA(cudaEventCreateWithFlags(&H.ev_join, cudaEventDisableTiming));
-    }
-    PA_CUDA(cudaEventRecord(H.ev_fork, s));
-    PA_CUDA(cudaStreamWaitEvent(H.side, H.ev_fork, 0));
-    gj_invert(H.side, nd, Lc.dense.get(), Lc.diag0.get(), Lc.gj_c.get(), Lc.gj_p.get(), Lc.gj_sync.get(),
-              Lc.flag.get());
-    PA_CUDA(cudaEventRecord(H.ev_join, H.side));
+    // (on a side stream beside the other levels' set-up the median solve was
+    // slower: 7.97 against 7.91 ms on 160x80x80, the cooperative launch at
+    // times waiting for the power iterations' CTAs)
+    gj_invert(s, nd, Lc.dense.get(), Lc.diag0.get(), Lc.gj_c.get(), Lc.gj_p.get(), Lc.gj_sync.get(), Lc.flag.get());
     g_box_launches += 3;
   }
   // every level's inverse diagonal
@@ -1432,7 +1414,6 @@ bool boxmg_setup(Problem& P, const double* z) {
   }
   std::vector<double> h(NL * (kPower + 1));
   PA_CUDA(cudaMemcpyAsync(h.data(), H.norms.get(), sizeof(double) * h.size(), cudaMemcpyDeviceToHost, s));
-  PA_CUDA(cudaStreamWaitEvent(s, H.ev_join, 0));  // the coarsest inverse
   double flag = 0.0;
   PA_CUDA(cudaMemcpyAsync(&flag, Lc.flag.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
   PA_CUDA(cudaStreamSynchronize(s));
