@@ -895,7 +895,7 @@ def run_learned(args):
     ms_d, st_d, f_d = timed("fp64", max(1, args.steps // 2), 1)
     ms_g, st_g, f_g = timed("mg", max(1, args.steps // 2), 1)
     # learned level-1 weights of the box multigrid: pairs from multigrid
-    # solves of the same design iterations, training judged by the CG
+    # solves of the same design iterations, parameters selected by the CG
     # iterations on the last training design; the held-out final design
     # solved with the parameters kept
     from platoanalyze_b200.api import LearnedCoarsening

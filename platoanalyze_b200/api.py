@@ -739,7 +739,7 @@ class LearnedCoarsening:
     zero) is the plain multigrid.  Trained on residual/error pairs (K e = r) of
     SIMP designs by Adam on the mean of ||e - V r||_K^2 / ||e||_K^2 (V the
     V-cycle), with dloss/ddelta from pa_boxmg_coarse_sensitivity; the plain
-    multigrid judges: every `check_every` steps the CG iterations on a
+    multigrid decides: every `check_every` steps the CG iterations on a
     validation control are counted, and training keeps the parameters with
     the fewest (the untrained ones unless some beat them).  No counterpart in
     the reference."""

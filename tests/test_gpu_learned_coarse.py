@@ -78,7 +78,7 @@ def test_new_coarse_network_is_the_plain_multigrid(pa):
     lc.close()
 
 
-def test_trained_coarse_network_judged_by_the_plain_multigrid(pa):
+def test_trained_coarse_network_selected_by_cg_iterations(pa):
     """32^3 SIMP cantilever: residual/error pairs from multigrid solves of
     design iterations 8-29, Adam on the V-cycle's energy-norm loss, the CG
     iterations on the last training design counted every 20 steps.  The loss
