@@ -473,6 +473,45 @@ __global__ void __launch_bounds__(kVT) k_bcg_update(int64_t n, double* sc, const
   }
 }
 
+// Jacobi preconditioner of the outer CG: z = dinv r (dinv zero on the masked
+// dofs), r . z reduced in a fixed order, and the CG scalars updated as the
+// V-cycle's last kernel does (beta, r . z, breakdown).  A no-op once kBreak or
+// kDone is set.
+__global__ void __launch_bounds__(kVT) k_bjacobi_z(int64_t n, const float* __restrict__ dinv,
+                                                   const double* __restrict__ r, double* __restrict__ z, double* sc,
+                                                   double* partials, unsigned int* counter) {
+  if (sc[kBreak] != 0.0 || sc[kDone] != 0.0) return;
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    const double zi = double(dinv[i]) * r[i];
+    z[i] = zi;
+    s += zi * r[i];
+  }
+  __shared__ double s_red[32];
+  __shared__ bool s_last;
+  const double b = block_sum_box(s, s_red);
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = b;
+    __threadfence();
+    s_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (s_last) {
+    __threadfence();
+    double t = 0.0;
+    for (unsigned k = threadIdx.x; k < gridDim.x; k += blockDim.x) t += __ldcg(&partials[k]);
+    t = block_sum_box(t, s_red);
+    if (threadIdx.x == 0) {
+      *counter = 0u;
+      const double old = sc[kRz];
+      sc[kBeta] = sc[kFirst] != 0.0 ? 0.0 : t / old;
+      sc[kFirst] = 0.0;
+      sc[kRz] = t;
+      if (!(t > 0.0) || !isfinite(t)) sc[kBreak] = 1.0;
+    }
+  }
+}
+
 // out = mask ? 0 : a - b (b may be null), and out . out (one thread per node,
 // 32-bit node ids: 3 N < 2^31 on the box path)
 __global__ void __launch_bounds__(kVT) k_bres64(int N, const double* __restrict__ a, const double* __restrict__ b,
@@ -1032,10 +1071,11 @@ struct BoxHierarchy {
     const void* ptr[6] = {};
     int wm = -1;
     double lam = 0.0, mu = 0.0;
+    bool jacobi = false;
     bool operator==(const GraphKey& o) const {
       for (int k = 0; k < 6; ++k)
         if (ptr[k] != o.ptr[k]) return false;
-      return wm == o.wm && lam == o.lam && mu == o.mu;
+      return wm == o.wm && lam == o.lam && mu == o.mu && jacobi == o.jacobi;
     }
   } key;
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
@@ -1555,7 +1595,7 @@ void boxmg_ensure(Problem& P) {
 // Solve K x = b with the box multigrid-preconditioned CG for control z.
 // Returns false (nothing written) when the coarsest operator is singular.
 bool solve_boxmg(Problem& P, const double* z, const double* b, double* x_out, const pa_solve_options& o,
-                 pa_solve_stats* st, pa_status* status) {
+                 pa_solve_stats* st, pa_status* status, bool jacobi) {
   cudaStream_t s = P.stream;
   PA_CHECK(o.rel_tol > 0.0, "rel_tol must be positive");
   g_box_launches = 0;
@@ -1596,7 +1636,9 @@ bool solve_boxmg(Problem& P, const double* z, const double* b, double* x_out, co
   PA_CUDA(cudaStreamSynchronize(s));
   if (!(bb > 0.0)) bb = 1.0;
   const double tol2 = o.rel_tol * o.rel_tol * bb;
-  const int max_iters = o.max_iters > 0 ? o.max_iters : 1000;
+  const int max_iters = o.max_iters > 0 ? o.max_iters
+                        : jacobi   ? int(20.0 * std::sqrt(double(n)) + 1000.0)  // as pa_solve's default
+                                   : 1000;
   PA_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, s));
   PA_CUDA(cudaMemcpyAsync(r, bp, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
   PA_CUDA(cudaMemsetAsync(H.p0.get(), 0, sizeof(double) * n, s));
@@ -1613,6 +1655,7 @@ bool solve_boxmg(Problem& P, const double* z, const double* b, double* x_out, co
   key.wm = F.wm;
   key.lam = P.ep.iso().lam;
   key.mu = P.ep.iso().mu;
+  key.jacobi = jacobi;
   if (!(H.gexec[0] && H.key == key)) {
     H.drop_graphs();
     for (int k = 0; k < 2; ++k) {
@@ -1621,7 +1664,12 @@ bool solve_boxmg(Problem& P, const double* z, const double* b, double* x_out, co
       const int64_t before = g_box_launches;
       PA_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
       try {
-        vcycle_level<double, double, true>(P, H, 0, r, zv, r, sc, s, sc + kBreak);
+        if (jacobi) {
+          k_bjacobi_z<<<vec_blocks(n), kVT, 0, s>>>(n, F.dinv.get(), r, zv, sc, H.partials.get(), H.counter.get());
+          g_box_launches += 1;
+        } else {
+          vcycle_level<double, double, true>(P, H, 0, r, zv, r, sc, s, sc + kBreak);
+        }
         launch_box<double>(F, box_geo<double>(F, P.ep), w64, InCgP{zv, pold, pnew, sc, N},
                            OutCgQ{H.q.get(), zv, pold, mask, sc, N}, red, s, sc + kBreak);
         k_bcg_update<<<vec_blocks(n), kVT, 0, s>>>(n, sc, pnew, H.q.get(), x, r, H.partials.get(), H.counter.get());
@@ -1662,7 +1710,8 @@ bool solve_boxmg(Problem& P, const double* z, const double* b, double* x_out, co
   // (r . r <= tol2) and breakdown, and every launch after either is a no-op.
   // The batch after the first is the number of iterations the mean reduction
   // so far predicts to convergence (at most 16).
-  constexpr int kFirstBatch = 4, kMaxBatch = 16;
+  constexpr int kFirstBatch = 4;
+  const int kMaxBatch = jacobi ? 128 : 16;  // Jacobi iterations are many and short
   double h4[4];  // r . r, breakdown, done, executed iterations
   while (!converged && iters < max_iters && !breakdown) {
     const int cycle_start = iters;

@@ -110,9 +110,12 @@ void boxmg_coarse_sensitivity(Problem& P, const double* z, const float* delta, i
                               const double* energies, double* loss, float* grad);
 bool box_apply_eligible(const Problem& P);
 bool boxmg_eligible(const Problem& P);
-// false (nothing written) when the coarsest operator is singular
+// false (nothing written) when the coarsest operator is singular.  jacobi:
+// the same FP64 outer CG on the box kernel preconditioned by the fine level's
+// inverse diagonal instead of the V-cycle (PA_SOLVER_PCG_FP64 on box meshes:
+// deterministic, no atomics)
 bool solve_boxmg(Problem& P, const double* z, const double* b, double* x_out, const pa_solve_options& o,
-                 pa_solve_stats* st, pa_status* status);
+                 pa_solve_stats* st, pa_status* status, bool jacobi = false);
 // interleaved x, y in the caller's order; xs, ys: 3N scratch
 template <typename T>
 void box_apply(Problem& P, const double* z, const T* x, T* y, bool constrained, T* xs, T* ys);

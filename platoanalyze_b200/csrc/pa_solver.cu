@@ -1011,19 +1011,21 @@ pa_status solve_device(Problem& P, const double* z, const double* b, double* x_o
   }
   const bool mixed = o.method == PA_SOLVER_PCG_MIXED;
   const bool mg = o.method == PA_SOLVER_PCG_MG;
+  const bool box_jacobi = o.method == PA_SOLVER_PCG_FP64 && !o.use_initial_guess && boxmg_eligible(P);
   const int64_t n = P.ndof();
   const int grid_need = std::max(std::max(fused_apply_grid<double>(*P.mesh), fused_apply_grid<float>(*P.mesh)),
                                 vec_grid(n));
-  P.ws.ensure(n, P.C(), grid_need, mixed || mg);
+  P.ws.ensure(n, P.C(), grid_need, mixed || mg || box_jacobi);
   SolverWorkspace& ws = P.ws;
   if (!P.ev0) { PA_CUDA(cudaEventCreate(&P.ev0)); PA_CUDA(cudaEventCreate(&P.ev1)); }
-  if (mg && o.mg_coarse_solver == PA_MG_COARSE_AUTO && boxmg_eligible(P)) {
-    // structured box: every level on the box kernel
+  if ((mg && o.mg_coarse_solver == PA_MG_COARSE_AUTO && boxmg_eligible(P)) || box_jacobi) {
+    // structured box: every level (or, for FP64 Jacobi-PCG, the fine level) on
+    // the box kernel, deterministic
     cudaEvent_t t0;
     PA_CUDA(cudaEventCreate(&t0));
     PA_CUDA(cudaEventRecord(t0, P.stream));
     pa_status status = PA_OK;
-    const bool done = solve_boxmg(P, z, b, x_out, o, st, &status);
+    const bool done = solve_boxmg(P, z, b, x_out, o, st, &status, box_jacobi);
     if (done) {
       float ms = 0.f;
       PA_CUDA(cudaEventElapsedTime(&ms, t0, P.ev1));

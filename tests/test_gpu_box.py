@@ -336,3 +336,32 @@ def test_box_assembled_gradient_u(pa, oracle_lib, layout, lengths):
     mesh.set_graph(rowmap, rev)
     K_rev = prob.vector_function().gradient_u(u, z)
     assert rel_inf(K_rev, O.jacobian(u, z, mesh.graph())) <= 1e-12
+
+
+@pytest.mark.parametrize("dims", [(24, 12, 12), (17, 9, 7)])
+def test_box_fp64_jacobi_pcg_deterministic(pa, oracle_lib, dims):
+    """PA_SOLVER_PCG_FP64 on a box runs the outer CG on the box kernel with
+    the inverse diagonal (no atomics): two fresh problems give the same bits,
+    the solution solves the oracle's constrained system, and it equals the
+    tile kernel's FP64 Jacobi-PCG (box kernels off) to the tolerance."""
+    from oracle import np_ref
+    opts = pa.SolveOptions("fp64", rel_tol=1e-10)
+    mesh, prob, faces, dofs, z = _cantilever(dims, 9)
+    u, st = prob.solution(z, options=opts)
+    assert st["converged"] and st["rel_residual"] <= 1e-10, st
+    _, prob2, _, _, _ = _cantilever(dims, 9)
+    u2, st2 = prob2.solution(z, options=opts)
+    assert st2["iterations"] == st["iterations"] and np.array_equal(u2, u)
+    nx, ny, nz = dims
+    cells, coords = np_ref.box_mesh(nx, ny, nz, float(nx), float(ny), float(nz))
+    O = oracle_lib.Oracle(cells, coords, E=1.0, nu=0.3, p=3.0, pmin=1e-9, layout=1)
+    flux = np.array([0.0, 0.0, -1.0 / (ny * nz)])
+    F = -O.residual(np.zeros_like(u), z, faces, flux)
+    res = F - O.apply(u, z)
+    res[dofs] = 0.0
+    assert np.linalg.norm(res) <= 1.01e-10 * np.linalg.norm(F)
+    mesh.set_box_kernels(False)
+    ut, stt = prob.solution(z, options=opts)
+    assert stt["converged"], stt
+    assert rel_inf(ut, u) <= 1e-8
+    assert abs(stt["iterations"] - st["iterations"]) <= 0.05 * st["iterations"] + 2, (st, stt)
