@@ -17,7 +17,7 @@ void launch_dRdz_transpose_times(const Problem& P, const double* u, const double
                                  double* g, cudaStream_t s);
 void launch_block_constraints(const Problem& P, double* entries, double* rhs, double scale, cudaStream_t s);
 void launch_scale(double* v, int64_t n, double a, cudaStream_t s);
-void launch_gradient_x(const Problem& P, const double* u, const double* z, double* entries, cudaStream_t s);
+void launch_gradient_x(Problem& P, const double* u, const double* z, double* entries, cudaStream_t s);
 void launch_energy_grad_x(const Problem& P, const double* u, const double* z, double* gx, cudaStream_t s);
 double time_cg_apply(Problem& P, const double* z, bool fp32, int reps);
 double time_apply(Problem& P, const double* z, bool fp32, int reps);

@@ -2353,6 +2353,119 @@ __global__ void __launch_bounds__(15 * kGuNodes) k_bgradient_u(BoxDims d, double
   for (int64_t e = threadIdx.x; e < count; e += blockDim.x) vals[9 * base + e] = stage[e];
 }
 
+// VectorFunction::gradient_x on a box mesh in its own numbering with sorted
+// columns, by the same (slot, node) threads as k_bgradient_u: the block at row
+// v, column w holds d R_w / d x_v ([k][j] = d R_w,j / d x_v,k), summed over the
+// tets of the edge.  For a linear tet with barycentric gradients g, volume V,
+// displacement gradient H = sum_m u_m g_m^T and stress S = w sigma(sym H), the
+// nodal force is R_a = V S g_a, and moving vertex b along e_k gives
+// dV = V g_b,k, dg_a = -g_a,k g_b, dH = -H e_k g_b^T (= D), dS = w sigma(sym D):
+//   d R_a / d x_b,k = V (g_b,k S g_a + dS g_a - g_a,k S g_b),
+// with tr D = -(H^T g_b)_k and dS g_a = w (lam tr D g_a - mu (g_b . g_a) H e_k
+// - mu (H^T g_a)_k g_b).  u is read at the tet's four lattice corners.
+__global__ void __launch_bounds__(15 * kGuNodes) k_bgradient_x(BoxDims d, double vol, double p, double pmin,
+                                                             int layout, BoxEdges E, Iso<double> iso, double ih0,
+                                                             double ih1, double ih2, const double* __restrict__ u,
+                                                             const double* __restrict__ z,
+                                                             const int32_t* __restrict__ rowmap,
+                                                             double* __restrict__ vals) {
+  __shared__ double stage[15 * kGuNodes * 9];
+  const int64_t v0 = int64_t(blockIdx.x) * kGuNodes;
+  const int64_t v1 = v0 + kGuNodes < d.N ? v0 + kGuNodes : d.N;
+  const int sl = int(threadIdx.x) / kGuNodes;
+  const int64_t v = v0 + int(threadIdx.x) % kGuNodes;
+  const int64_t base = rowmap[v0];
+  const double ih[3] = {ih0, ih1, ih2};
+  if (v < v1) {
+    const int vi = int(v % d.px), vj = int((v / d.px) % d.py), vk = int(v / (int64_t(d.px) * d.py));
+    auto inside = [&](int i, int j, int k) {
+      return i >= 0 && i <= d.nx && j >= 0 && j <= d.ny && k >= 0 && k <= d.nz;
+    };
+    if (inside(vi + E.off[sl][0], vj + E.off[sl][1], vk + E.off[sl][2])) {
+      int rank = sl;
+      if (vi == 0 || vj == 0 || vk == 0 || vi == d.nx || vj == d.ny || vk == d.nz) {
+        rank = 0;
+        for (int q = 0; q < sl; ++q) rank += inside(vi + E.off[q][0], vj + E.off[q][1], vk + E.off[q][2]) ? 1 : 0;
+      }
+      double K[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      for (int o = 0; o < 8; ++o) {
+        const int n = E.count[sl][o];
+        if (n == 0) continue;
+        const int oi = vi - (o & 1), oj = vj - ((o >> 1) & 1), ok = vk - (o >> 2);
+        if (oi < 0 || oj < 0 || ok < 0 || oi >= d.nx || oj >= d.ny || ok >= d.nz) continue;
+        const int64_t h = oi + int64_t(d.nx) * (oj + int64_t(d.ny) * ok);
+        for (int e = 0; e < n; ++e) {
+          const int code = E.tet[sl][o][e], t = code & 7, mv = (code >> 3) & 3, mw = code >> 5;
+          double rho;
+          if (layout == PA_CONTROL_CELL) {
+            rho = z[6 * h + t];
+          } else {
+            rho = 0.0;
+            for (int m = 0; m < 4; ++m) {
+              const int c = path_vertex(t, m);
+              rho += 0.25 * z[(oi + (c & 1)) +
+                              int64_t(d.px) * ((oj + ((c >> 1) & 1)) + int64_t(d.py) * (ok + (c >> 2)))];
+            }
+          }
+          const double w = simp(rho, p, pmin);
+          // H = sum_m u_m g_m^T over the tet's path vertices
+          double H[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+          for (int m = 0; m < 4; ++m) {
+            const int c = path_vertex(t, m);
+            const int64_t node = (oi + (c & 1)) + int64_t(d.px) * ((oj + ((c >> 1) & 1)) + int64_t(d.py) * (ok + (c >> 2)));
+            double gm[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) gm[a] = E.grad[t][m][a] * ih[a];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+              const double ui = u[3 * node + i];
+#pragma unroll
+              for (int a = 0; a < 3; ++a) H[i][a] = fma(ui, gm[a], H[i][a]);
+            }
+          }
+          const double tr = H[0][0] + H[1][1] + H[2][2];
+          double S[3][3];
+#pragma unroll
+          for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+              S[i][j] = w * ((i == j ? iso.lam * tr : 0.0) + iso.mu * (H[i][j] + H[j][i]));
+          double gv[3], gw[3];
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            gv[a] = E.grad[t][mv][a] * ih[a];
+            gw[a] = E.grad[t][mw][a] * ih[a];
+          }
+          double Sgw[3], Sgv[3], Htv[3], Htw[3];
+#pragma unroll
+          for (int i = 0; i < 3; ++i) {
+            Sgw[i] = S[i][0] * gw[0] + S[i][1] * gw[1] + S[i][2] * gw[2];
+            Sgv[i] = S[i][0] * gv[0] + S[i][1] * gv[1] + S[i][2] * gv[2];
+            Htv[i] = H[0][i] * gv[0] + H[1][i] * gv[1] + H[2][i] * gv[2];
+            Htw[i] = H[0][i] * gw[0] + H[1][i] * gw[1] + H[2][i] * gw[2];
+          }
+          const double gvgw = gv[0] * gw[0] + gv[1] * gw[1] + gv[2] * gw[2];
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            const double trD = -Htv[k];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+              const double dSgw = w * (iso.lam * trD * gw[j] - iso.mu * (H[j][k] * gvgw + gv[j] * Htw[k]));
+              K[3 * k + j] += vol * (gv[k] * Sgw[j] + dSgw - gw[k] * Sgv[j]);
+            }
+          }
+        }
+      }
+      double* dst = stage + 9 * (int64_t(rowmap[v]) - base + rank);
+#pragma unroll
+      for (int q = 0; q < 9; ++q) dst[q] = K[q];
+    }
+  }
+  __syncthreads();
+  const int64_t count = 9 * (int64_t(rowmap[v1]) - base);
+  for (int64_t e = threadIdx.x; e < count; e += blockDim.x) vals[9 * base + e] = stage[e];
+}
+
 }  // namespace
 
 bool box_gradient_u(Problem& P, const double* z, double* entries) {
@@ -2390,6 +2503,22 @@ bool box_gradient_u(Problem& P, const double* z, double* entries) {
   k_bgradient_u<<<int((F.d.N + kGuNodes - 1) / kGuNodes), 15 * kGuNodes, 0, P.stream>>>(
       F.d, F.h[0] * F.h[1] * F.h[2] / 6.0, P.ep.p, P.ep.pmin, P.ep.layout, edges, H.gu_k0.get(), z,
       m.d_rowmap.get(), entries);
+  PA_LAUNCHED();
+  return true;
+}
+
+// VectorFunction::gradient_x on a box mesh (the volume term; the caller adds
+// the surface loads): false (nothing launched) on any other mesh.
+bool box_gradient_x(Problem& P, const double* u, const double* z, double* entries) {
+  const Mesh& m = *P.mesh;
+  if (!(m.box_kernels && m.lat_n[0] > 0 && !m.lat_permuted && m.lat_flip == 0 && m.cols_sorted && m.d_rowmap.n))
+    return false;
+  static const BoxEdges edges = make_box_edges();
+  boxmg_ensure(P);
+  const BoxLevel& F = *P.boxmg->L[0];
+  k_bgradient_x<<<int((F.d.N + kGuNodes - 1) / kGuNodes), 15 * kGuNodes, 0, P.stream>>>(
+      F.d, F.h[0] * F.h[1] * F.h[2] / 6.0, P.ep.p, P.ep.pmin, P.ep.layout, edges, P.ep.iso(), 1.0 / F.h[0],
+      1.0 / F.h[1], 1.0 / F.h[2], u, z, m.d_rowmap.get(), entries);
   PA_LAUNCHED();
   return true;
 }

@@ -466,10 +466,12 @@ void launch_block_constraints(const Problem& P, double* entries, double* rhs, do
   PA_LAUNCHED();
 }
 
-void launch_gradient_x(const Problem& P, const double* u, const double* z, double* entries, cudaStream_t s) {
-  PA_CUDA(cudaMemsetAsync(entries, 0, sizeof(double) * 9 * P.mesh->B, s));
-  k_gradient_x<<<grid_for(P.C(), 128), 128, 0, s>>>(cell_in(P), mat64(P), u, z, P.mesh->d_cell_entry.get(), entries);
-  PA_LAUNCHED();
+void launch_gradient_x(Problem& P, const double* u, const double* z, double* entries, cudaStream_t s) {
+  if (!box_gradient_x(P, u, z, entries)) {  // box meshes: every block written once, no atomics
+    PA_CUDA(cudaMemsetAsync(entries, 0, sizeof(double) * 9 * P.mesh->B, s));
+    k_gradient_x<<<grid_for(P.C(), 128), 128, 0, s>>>(cell_in(P), mat64(P), u, z, P.mesh->d_cell_entry.get(), entries);
+    PA_LAUNCHED();
+  }
   const int64_t nf = int64_t(P.faces.size() / 3);
   if (nf) {
     k_traction_x<<<grid_for(nf), kThreads, 0, s>>>(P.d_faces.get(), P.d_face_flux.get(), nf, P.mesh->d_coords.get(),

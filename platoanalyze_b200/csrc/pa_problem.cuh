@@ -96,6 +96,8 @@ bool box_entry_eligible(const Problem& P);
 // The assembled K(z) (block CRS entries) on a box mesh in its own numbering
 // with sorted columns; false (nothing launched) on any other mesh.
 bool box_gradient_u(Problem& P, const double* z, double* entries);
+// dR/dx (the volume term) likewise; the caller adds the surface loads
+bool box_gradient_x(Problem& P, const double* u, const double* z, double* entries);
 void box_entry_apply(Problem& P, const double* z, const double* u, double* y);
 void box_entry_energy(Problem& P, const double* z, const double* u, double* value, double* grad_z);
 void box_entry_gradient_z(Problem& P, const double* z, const double* u, double* vals);
