@@ -2362,119 +2362,20 @@ __global__ void __launch_bounds__(15 * kGuNodes) k_bgradient_u(BoxDims d, double
 // dV = V g_b,k, dg_a = -g_a,k g_b, dH = -H e_k g_b^T (= D), dS = w sigma(sym D):
 //   d R_a / d x_b,k = V (g_b,k S g_a + dS g_a - g_a,k S g_b),
 // with tr D = -(H^T g_b)_k and dS g_a = w (lam tr D g_a - mu (g_b . g_a) H e_k
-// - mu (H^T g_a)_k g_b).  A CTA whose 16 nodes lie in one node row first forms
-// H and S of the 6 tets of each of the 17 x 2 x 2 hexes around them in shared
-// memory (each tet once, instead of once per block it touches); a CTA that
-// spans two rows forms them per block.
-constexpr int kGxHex = 17 * 2 * 2;             // hexes around one row of 16 nodes
-constexpr int kGxRec = 16;                     // H (9), S (6, symmetric) and the SIMP weight per tet
-constexpr int kGxStage = 15 * kGuNodes * 9;    // doubles of the row staging
-constexpr size_t kGxSmem = sizeof(double) * (kGxStage + size_t(kGxHex) * 6 * kGxRec);
-
-// H and S of tet t of the hex with origin (oi, oj, ok)
-__device__ __forceinline__ void gx_tet_hs(const BoxDims& d, const BoxEdges& E, const Iso<double>& iso,
-                                          const double (&ih)[3], double p, double pmin, int layout,
-                                          const double* __restrict__ u, const double* __restrict__ z, int oi, int oj,
-                                          int ok, int t, double (&H)[3][3], double (&S6)[6], double& w_out) {
-  const int64_t h = oi + int64_t(d.nx) * (oj + int64_t(d.ny) * ok);
-  double rho;
-  if (layout == PA_CONTROL_CELL) {
-    rho = z[6 * h + t];
-  } else {
-    rho = 0.0;
-    for (int m = 0; m < 4; ++m) {
-      const int c = path_vertex(t, m);
-      rho += 0.25 * z[(oi + (c & 1)) + int64_t(d.px) * ((oj + ((c >> 1) & 1)) + int64_t(d.py) * (ok + (c >> 2)))];
-    }
-  }
-  const double w = simp(rho, p, pmin);
-  w_out = w;
-#pragma unroll
-  for (int i = 0; i < 3; ++i) H[i][0] = H[i][1] = H[i][2] = 0.0;
-  for (int m = 0; m < 4; ++m) {
-    const int c = path_vertex(t, m);
-    const int64_t node = (oi + (c & 1)) + int64_t(d.px) * ((oj + ((c >> 1) & 1)) + int64_t(d.py) * (ok + (c >> 2)));
-    double gm[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) gm[a] = E.grad[t][m][a] * ih[a];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      const double ui = u[3 * node + i];
-#pragma unroll
-      for (int a = 0; a < 3; ++a) H[i][a] = fma(ui, gm[a], H[i][a]);
-    }
-  }
-  const double tr = H[0][0] + H[1][1] + H[2][2];
-  // S in Voigt order xx, yy, zz, yz, xz, xy
-  S6[0] = w * (iso.lam * tr + 2.0 * iso.mu * H[0][0]);
-  S6[1] = w * (iso.lam * tr + 2.0 * iso.mu * H[1][1]);
-  S6[2] = w * (iso.lam * tr + 2.0 * iso.mu * H[2][2]);
-  S6[3] = w * iso.mu * (H[1][2] + H[2][1]);
-  S6[4] = w * iso.mu * (H[0][2] + H[2][0]);
-  S6[5] = w * iso.mu * (H[0][1] + H[1][0]);
-}
-
-// K += V (g_v,k S g_w + dS g_w - g_w,k S g_v) for one tet
-__device__ __forceinline__ void gx_block(const double (&H)[3][3], const double (&S6)[6], const double (&gv)[3],
-                                         const double (&gw)[3], double w_lam, double w_mu, double vol,
-                                         double (&K)[9]) {
-  const double S[3][3] = {{S6[0], S6[5], S6[4]}, {S6[5], S6[1], S6[3]}, {S6[4], S6[3], S6[2]}};
-  double Sgw[3], Sgv[3], Htv[3], Htw[3];
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    Sgw[i] = S[i][0] * gw[0] + S[i][1] * gw[1] + S[i][2] * gw[2];
-    Sgv[i] = S[i][0] * gv[0] + S[i][1] * gv[1] + S[i][2] * gv[2];
-    Htv[i] = H[0][i] * gv[0] + H[1][i] * gv[1] + H[2][i] * gv[2];
-    Htw[i] = H[0][i] * gw[0] + H[1][i] * gw[1] + H[2][i] * gw[2];
-  }
-  const double gvgw = gv[0] * gw[0] + gv[1] * gw[1] + gv[2] * gw[2];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    const double trD = -Htv[k];
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      const double dSgw = w_lam * trD * gw[j] - w_mu * (H[j][k] * gvgw + gv[j] * Htw[k]);
-      K[3 * k + j] += vol * (gv[k] * Sgw[j] + dSgw - gw[k] * Sgv[j]);
-    }
-  }
-}
-
+// - mu (H^T g_a)_k g_b).  u is read at the tet's four lattice corners.
 __global__ void __launch_bounds__(15 * kGuNodes) k_bgradient_x(BoxDims d, double vol, double p, double pmin,
                                                              int layout, BoxEdges E, Iso<double> iso, double ih0,
                                                              double ih1, double ih2, const double* __restrict__ u,
                                                              const double* __restrict__ z,
                                                              const int32_t* __restrict__ rowmap,
                                                              double* __restrict__ vals) {
-  extern __shared__ double gx_smem[];
-  double* stage = gx_smem;
-  double* rec = gx_smem + kGxStage;  // [hex][tet][15]: H row-major, then S (Voigt)
+  __shared__ double stage[15 * kGuNodes * 9];
   const int64_t v0 = int64_t(blockIdx.x) * kGuNodes;
   const int64_t v1 = v0 + kGuNodes < d.N ? v0 + kGuNodes : d.N;
   const int sl = int(threadIdx.x) / kGuNodes;
   const int64_t v = v0 + int(threadIdx.x) % kGuNodes;
   const int64_t base = rowmap[v0];
   const double ih[3] = {ih0, ih1, ih2};
-  // the CTA's first node: its row (j0, k0) and the hexes around the row
-  const int i0 = int(v0 % d.px), j0 = int((v0 / d.px) % d.py), k0 = int(v0 / (int64_t(d.px) * d.py));
-  const bool one_row = i0 + int(v1 - v0) - 1 < d.px;  // uniform over the CTA
-  if (one_row) {
-    for (int r = threadIdx.x; r < kGxHex * 6; r += blockDim.x) {
-      const int lh = r / 6, t = r - 6 * lh;
-      const int oi = i0 - 1 + lh % 17, oj = j0 - 1 + (lh / 17) % 2, ok = k0 - 1 + lh / 34;
-      if (oi < 0 || oj < 0 || ok < 0 || oi >= d.nx || oj >= d.ny || ok >= d.nz) continue;
-      double H[3][3], S6[6], w;
-      gx_tet_hs(d, E, iso, ih, p, pmin, layout, u, z, oi, oj, ok, t, H, S6, w);
-      double* q = rec + kGxRec * r;
-#pragma unroll
-      for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int a = 0; a < 3; ++a) q[3 * i + a] = H[i][a];
-#pragma unroll
-      for (int c = 0; c < 6; ++c) q[9 + c] = S6[c];
-      q[15] = w;
-    }
-    __syncthreads();
-  }
   if (v < v1) {
     const int vi = int(v % d.px), vj = int((v / d.px) % d.py), vk = int(v / (int64_t(d.px) * d.py));
     auto inside = [&](int i, int j, int k) {
@@ -2492,29 +2393,67 @@ __global__ void __launch_bounds__(15 * kGuNodes) k_bgradient_x(BoxDims d, double
         if (n == 0) continue;
         const int oi = vi - (o & 1), oj = vj - ((o >> 1) & 1), ok = vk - (o >> 2);
         if (oi < 0 || oj < 0 || ok < 0 || oi >= d.nx || oj >= d.ny || ok >= d.nz) continue;
+        const int64_t h = oi + int64_t(d.nx) * (oj + int64_t(d.ny) * ok);
         for (int e = 0; e < n; ++e) {
           const int code = E.tet[sl][o][e], t = code & 7, mv = (code >> 3) & 3, mw = code >> 5;
-          double H[3][3], S6[6], w;
-          if (one_row) {
-            const int lh = (oi - i0 + 1) + 17 * ((oj - j0 + 1) + 2 * (ok - k0 + 1));
-            const double* q = rec + kGxRec * (6 * lh + t);
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-              for (int a = 0; a < 3; ++a) H[i][a] = q[3 * i + a];
-#pragma unroll
-            for (int c = 0; c < 6; ++c) S6[c] = q[9 + c];
-            w = q[15];
+          double rho;
+          if (layout == PA_CONTROL_CELL) {
+            rho = z[6 * h + t];
           } else {
-            gx_tet_hs(d, E, iso, ih, p, pmin, layout, u, z, oi, oj, ok, t, H, S6, w);
+            rho = 0.0;
+            for (int m = 0; m < 4; ++m) {
+              const int c = path_vertex(t, m);
+              rho += 0.25 * z[(oi + (c & 1)) +
+                              int64_t(d.px) * ((oj + ((c >> 1) & 1)) + int64_t(d.py) * (ok + (c >> 2)))];
+            }
           }
+          const double w = simp(rho, p, pmin);
+          // H = sum_m u_m g_m^T over the tet's path vertices
+          double H[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+          for (int m = 0; m < 4; ++m) {
+            const int c = path_vertex(t, m);
+            const int64_t node = (oi + (c & 1)) + int64_t(d.px) * ((oj + ((c >> 1) & 1)) + int64_t(d.py) * (ok + (c >> 2)));
+            double gm[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) gm[a] = E.grad[t][m][a] * ih[a];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+              const double ui = u[3 * node + i];
+#pragma unroll
+              for (int a = 0; a < 3; ++a) H[i][a] = fma(ui, gm[a], H[i][a]);
+            }
+          }
+          const double tr = H[0][0] + H[1][1] + H[2][2];
+          double S[3][3];
+#pragma unroll
+          for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+              S[i][j] = w * ((i == j ? iso.lam * tr : 0.0) + iso.mu * (H[i][j] + H[j][i]));
           double gv[3], gw[3];
 #pragma unroll
           for (int a = 0; a < 3; ++a) {
             gv[a] = E.grad[t][mv][a] * ih[a];
             gw[a] = E.grad[t][mw][a] * ih[a];
           }
-          gx_block(H, S6, gv, gw, w * iso.lam, w * iso.mu, vol, K);
+          double Sgw[3], Sgv[3], Htv[3], Htw[3];
+#pragma unroll
+          for (int i = 0; i < 3; ++i) {
+            Sgw[i] = S[i][0] * gw[0] + S[i][1] * gw[1] + S[i][2] * gw[2];
+            Sgv[i] = S[i][0] * gv[0] + S[i][1] * gv[1] + S[i][2] * gv[2];
+            Htv[i] = H[0][i] * gv[0] + H[1][i] * gv[1] + H[2][i] * gv[2];
+            Htw[i] = H[0][i] * gw[0] + H[1][i] * gw[1] + H[2][i] * gw[2];
+          }
+          const double gvgw = gv[0] * gw[0] + gv[1] * gw[1] + gv[2] * gw[2];
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            const double trD = -Htv[k];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+              const double dSgw = w * (iso.lam * trD * gw[j] - iso.mu * (H[j][k] * gvgw + gv[j] * Htw[k]));
+              K[3 * k + j] += vol * (gv[k] * Sgw[j] + dSgw - gw[k] * Sgv[j]);
+            }
+          }
         }
       }
       double* dst = stage + 9 * (int64_t(rowmap[v]) - base + rank);
@@ -2577,12 +2516,7 @@ bool box_gradient_x(Problem& P, const double* u, const double* z, double* entrie
   static const BoxEdges edges = make_box_edges();
   boxmg_ensure(P);
   const BoxLevel& F = *P.boxmg->L[0];
-  static bool attr = false;
-  if (!attr) {
-    PA_CUDA(cudaFuncSetAttribute(k_bgradient_x, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kGxSmem)));
-    attr = true;
-  }
-  k_bgradient_x<<<int((F.d.N + kGuNodes - 1) / kGuNodes), 15 * kGuNodes, kGxSmem, P.stream>>>(
+  k_bgradient_x<<<int((F.d.N + kGuNodes - 1) / kGuNodes), 15 * kGuNodes, 0, P.stream>>>(
       F.d, F.h[0] * F.h[1] * F.h[2] / 6.0, P.ep.p, P.ep.pmin, P.ep.layout, edges, P.ep.iso(), 1.0 / F.h[0],
       1.0 / F.h[1], 1.0 / F.h[2], u, z, m.d_rowmap.get(), entries);
   PA_LAUNCHED();

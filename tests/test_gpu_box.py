@@ -367,15 +367,13 @@ def test_box_fp64_jacobi_pcg_deterministic(pa, oracle_lib, dims):
     assert abs(stt["iterations"] - st["iterations"]) <= 0.05 * st["iterations"] + 2, (st, stt)
 
 
-@pytest.mark.parametrize("layout,lengths", [("cell", (24.0, 5.0, 4.0)), ("nodal", (12.0, 7.5, 2.0))])
+@pytest.mark.parametrize("layout,lengths", [("cell", (8.0, 5.0, 4.0)), ("nodal", (4.0, 7.5, 2.0))])
 def test_box_assembled_gradient_x(pa, oracle_lib, layout, lengths):
     """VectorFunction::gradient_x on a box mesh: the per-block lattice
     assembly of the volume term (closed-form shape derivatives, no atomics)
     plus the surface loads equals the oracle's dR/dx and, to rounding, the
-    per-cell dual-number kernel with atomics (box kernels switched off).  With
-    25 nodes per row, CTAs of 16 nodes both lie in one row (tets staged in
-    shared memory) and span two (tets formed per block)."""
-    dims = (24, 5, 4)
+    per-cell dual-number kernel with atomics (box kernels switched off)."""
+    dims = (8, 5, 4)
     mesh = pa.Mesh.box(*dims, *lengths)
     assert mesh.box_kernels
     cells, coords = mesh.arrays()
