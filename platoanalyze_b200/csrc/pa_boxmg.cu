@@ -2244,10 +2244,10 @@ void box_entry_energy(Problem& P, const double* z, const double* u, double* valu
 // monotone path 0 -> e_a -> e_a + e_b -> (1,1,1) through its hex, so the
 // neighbours of node v are v +- e_S for the seven non-empty axis sets S, and
 // in node-id order they are the fifteen slots of BoxEdges (px, py >= 2).
-// A CTA takes 16 consecutive nodes with one thread per (slot, node), so that a
-// warp shares its slot (the loops over the hexes and tets of an edge are
-// uniform and their table entries, kernel parameters, broadcast), and writes
-// its rows from shared memory as one contiguous range.
+// A CTA takes 32 consecutive nodes with one warp per slot, so the loops over
+// the hexes and tets of an edge are uniform in a warp and their table entries,
+// kernel parameters, broadcast, and writes its rows from shared memory as one
+// contiguous range.
 namespace {
 
 struct BoxEdges {
@@ -2288,14 +2288,14 @@ BoxEdges make_box_edges() {
   return E;
 }
 
-constexpr int kGuNodes = 16;  // nodes per CTA of k_bgradient_u (15 slots each)
+constexpr int kGuNodes = 32;  // nodes per CTA of k_bgradient_u and k_bgradient_x (15 slots each)
 
 __global__ void __launch_bounds__(15 * kGuNodes) k_bgradient_u(BoxDims d, double vol, double p, double pmin,
                                                              int layout, BoxEdges E, const double* __restrict__ k0,
                                                              const double* __restrict__ z,
                                                              const int32_t* __restrict__ rowmap,
                                                              double* __restrict__ vals) {
-  // thread (slot, node) = (tid / 16, tid % 16): a warp holds two slots of 16
+  // thread (slot, node) = (tid / 32, tid % 32): a warp holds one slot of 32
   // consecutive nodes; the CTA's blocks are staged in shared memory and its
   // rows written as one contiguous range
   __shared__ double stage[15 * kGuNodes * 9];
