@@ -2244,9 +2244,12 @@ void box_entry_energy(Problem& P, const double* z, const double* u, double* valu
 // monotone path 0 -> e_a -> e_a + e_b -> (1,1,1) through its hex, so the
 // neighbours of node v are v +- e_S for the seven non-empty axis sets S, and
 // in node-id order they are the fifteen slots of BoxEdges (px, py >= 2).
-// A CTA takes 32 consecutive nodes with one warp per slot, so the loops over
-// the hexes and tets of an edge are uniform in a warp and their table entries,
-// kernel parameters, broadcast, and writes its rows from shared memory as one
+// A CTA takes 32 consecutive nodes, one node per lane, and its four warps
+// split the fifteen slots into groups of equal tet counts (the node itself has
+// 24 tets, every neighbour 4 or 6: 96 in all), so the loops over the hexes and
+// tets of an edge are uniform in a warp, their table entries (kernel
+// parameters) broadcast, and the warps reach the barrier before the rows'
+// write-back together; the CTA writes its rows from shared memory as one
 // contiguous range.
 namespace {
 
@@ -2255,6 +2258,8 @@ struct BoxEdges {
   uint8_t count[15][8];   // tets of the edge in the hex at origin v - corner(o)
   uint8_t tet[15][8][6];  // t | m_v << 3 | m_w << 5
   int8_t grad[6][4][3];   // gradient of vertex m of tet t on a unit hex (-1, 0, 1 per axis)
+  uint8_t group[4][6];    // slots of each warp of a CTA, 24 tets per warp
+  uint8_t group_n[4];
 };
 
 BoxEdges make_box_edges() {
@@ -2285,67 +2290,84 @@ BoxEdges make_box_edges() {
       }
     }
   }
+  // warp groups: the node itself (24 tets), four six-tet slots, four
+  // six-tet slots, six four-tet slots
+  static const int kGroup[4][6] = {{7}, {0, 3, 5, 6}, {8, 9, 11, 14}, {1, 2, 4, 10, 12, 13}};
+  static const int kGroupN[4] = {1, 4, 4, 6};
+  for (int g = 0; g < 4; ++g) {
+    E.group_n[g] = uint8_t(kGroupN[g]);
+    int tets = 0;
+    for (int q = 0; q < kGroupN[g]; ++q) {
+      E.group[g][q] = uint8_t(kGroup[g][q]);
+      for (int o = 0; o < 8; ++o) tets += E.count[kGroup[g][q]][o];
+    }
+    PA_CHECK(tets == 24, "unbalanced slot groups");
+  }
   return E;
 }
 
 constexpr int kGuNodes = 32;  // nodes per CTA of k_bgradient_u and k_bgradient_x (15 slots each)
+constexpr int kGuWarps = 4;   // warps per CTA, one slot group each
 
-__global__ void __launch_bounds__(15 * kGuNodes) k_bgradient_u(BoxDims d, double vol, double p, double pmin,
+__global__ void __launch_bounds__(32 * kGuWarps) k_bgradient_u(BoxDims d, double vol, double p, double pmin,
                                                              int layout, BoxEdges E, const double* __restrict__ k0,
                                                              const double* __restrict__ z,
                                                              const int32_t* __restrict__ rowmap,
                                                              double* __restrict__ vals) {
-  // thread (slot, node) = (tid / 32, tid % 32): a warp holds one slot of 32
+  // thread (group, node) = (warp, lane): a warp takes its group's slots of 32
   // consecutive nodes; the CTA's blocks are staged in shared memory and its
   // rows written as one contiguous range
   __shared__ double stage[15 * kGuNodes * 9];
   const int64_t v0 = int64_t(blockIdx.x) * kGuNodes;
   const int64_t v1 = v0 + kGuNodes < d.N ? v0 + kGuNodes : d.N;
-  const int sl = int(threadIdx.x) / kGuNodes;
-  const int64_t v = v0 + int(threadIdx.x) % kGuNodes;
+  const int grp = int(threadIdx.x) / 32;
+  const int64_t v = v0 + int(threadIdx.x) % 32;
   const int64_t base = rowmap[v0];
   if (v < v1) {
     const int vi = int(v % d.px), vj = int((v / d.px) % d.py), vk = int(v / (int64_t(d.px) * d.py));
     auto inside = [&](int i, int j, int k) {
       return i >= 0 && i <= d.nx && j >= 0 && j <= d.ny && k >= 0 && k <= d.nz;
     };
-    if (inside(vi + E.off[sl][0], vj + E.off[sl][1], vk + E.off[sl][2])) {
-      // the block's position in the row: its slot for an interior node (every
-      // neighbour exists), else the count of existing neighbours before it
-      int rank = sl;
-      if (vi == 0 || vj == 0 || vk == 0 || vi == d.nx || vj == d.ny || vk == d.nz) {
-        rank = 0;
-        for (int q = 0; q < sl; ++q) rank += inside(vi + E.off[q][0], vj + E.off[q][1], vk + E.off[q][2]) ? 1 : 0;
-      }
-      double K[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-      for (int o = 0; o < 8; ++o) {
-        const int n = E.count[sl][o];
-        if (n == 0) continue;
-        const int oi = vi - (o & 1), oj = vj - ((o >> 1) & 1), ok = vk - (o >> 2);
-        if (oi < 0 || oj < 0 || ok < 0 || oi >= d.nx || oj >= d.ny || ok >= d.nz) continue;
-        const int64_t h = oi + int64_t(d.nx) * (oj + int64_t(d.ny) * ok);
-        for (int e = 0; e < n; ++e) {
-          const int t = E.tet[sl][o][e] & 7;
-          double rho;
-          if (layout == PA_CONTROL_CELL) {
-            rho = z[6 * h + t];
-          } else {
-            rho = 0.0;
-            for (int m = 0; m < 4; ++m) {
-              const int c = path_vertex(t, m);
-              rho += 0.25 * z[(oi + (c & 1)) +
-                              int64_t(d.px) * ((oj + ((c >> 1) & 1)) + int64_t(d.py) * (ok + (c >> 2)))];
-            }
-          }
-          const double w = vol * simp(rho, p, pmin);
-          const double* kb = k0 + 9 * ((sl * 8 + o) * 6 + e);
-#pragma unroll
-          for (int q = 0; q < 9; ++q) K[q] = fma(w, __ldg(kb + q), K[q]);
+    for (int gq = 0; gq < E.group_n[grp]; ++gq) {
+      const int sl = E.group[grp][gq];
+      if (inside(vi + E.off[sl][0], vj + E.off[sl][1], vk + E.off[sl][2])) {
+        // the block's position in the row: its slot for an interior node (every
+        // neighbour exists), else the count of existing neighbours before it
+        int rank = sl;
+        if (vi == 0 || vj == 0 || vk == 0 || vi == d.nx || vj == d.ny || vk == d.nz) {
+          rank = 0;
+          for (int q = 0; q < sl; ++q) rank += inside(vi + E.off[q][0], vj + E.off[q][1], vk + E.off[q][2]) ? 1 : 0;
         }
-      }
-      double* dst = stage + 9 * (int64_t(rowmap[v]) - base + rank);
+        double K[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int o = 0; o < 8; ++o) {
+          const int n = E.count[sl][o];
+          if (n == 0) continue;
+          const int oi = vi - (o & 1), oj = vj - ((o >> 1) & 1), ok = vk - (o >> 2);
+          if (oi < 0 || oj < 0 || ok < 0 || oi >= d.nx || oj >= d.ny || ok >= d.nz) continue;
+          const int64_t h = oi + int64_t(d.nx) * (oj + int64_t(d.ny) * ok);
+          for (int e = 0; e < n; ++e) {
+            const int t = E.tet[sl][o][e] & 7;
+            double rho;
+            if (layout == PA_CONTROL_CELL) {
+              rho = z[6 * h + t];
+            } else {
+              rho = 0.0;
+              for (int m = 0; m < 4; ++m) {
+                const int c = path_vertex(t, m);
+                rho += 0.25 * z[(oi + (c & 1)) +
+                                int64_t(d.px) * ((oj + ((c >> 1) & 1)) + int64_t(d.py) * (ok + (c >> 2)))];
+              }
+            }
+            const double w = vol * simp(rho, p, pmin);
+            const double* kb = k0 + 9 * ((sl * 8 + o) * 6 + e);
 #pragma unroll
-      for (int q = 0; q < 9; ++q) dst[q] = K[q];
+            for (int q = 0; q < 9; ++q) K[q] = fma(w, __ldg(kb + q), K[q]);
+          }
+        }
+        double* dst = stage + 9 * (int64_t(rowmap[v]) - base + rank);
+#pragma unroll
+        for (int q = 0; q < 9; ++q) dst[q] = K[q];
+      }
     }
   }
   __syncthreads();
@@ -2354,7 +2376,7 @@ __global__ void __launch_bounds__(15 * kGuNodes) k_bgradient_u(BoxDims d, double
 }
 
 // VectorFunction::gradient_x on a box mesh in its own numbering with sorted
-// columns, by the same (slot, node) threads as k_bgradient_u: the block at row
+// columns, by the same (slot group, node) threads as k_bgradient_u: the block at row
 // v, column w holds d R_w / d x_v ([k][j] = d R_w,j / d x_v,k), summed over the
 // tets of the edge.  For a linear tet with barycentric gradients g, volume V,
 // displacement gradient H = sum_m u_m g_m^T and stress S = w sigma(sym H), the
@@ -2363,7 +2385,7 @@ __global__ void __launch_bounds__(15 * kGuNodes) k_bgradient_u(BoxDims d, double
 //   d R_a / d x_b,k = V (g_b,k S g_a + dS g_a - g_a,k S g_b),
 // with tr D = -(H^T g_b)_k and dS g_a = w (lam tr D g_a - mu (g_b . g_a) H e_k
 // - mu (H^T g_a)_k g_b).  u is read at the tet's four lattice corners.
-__global__ void __launch_bounds__(15 * kGuNodes) k_bgradient_x(BoxDims d, double vol, double p, double pmin,
+__global__ void __launch_bounds__(32 * kGuWarps) k_bgradient_x(BoxDims d, double vol, double p, double pmin,
                                                              int layout, BoxEdges E, Iso<double> iso, double ih0,
                                                              double ih1, double ih2, const double* __restrict__ u,
                                                              const double* __restrict__ z,
@@ -2372,8 +2394,8 @@ __global__ void __launch_bounds__(15 * kGuNodes) k_bgradient_x(BoxDims d, double
   __shared__ double stage[15 * kGuNodes * 9];
   const int64_t v0 = int64_t(blockIdx.x) * kGuNodes;
   const int64_t v1 = v0 + kGuNodes < d.N ? v0 + kGuNodes : d.N;
-  const int sl = int(threadIdx.x) / kGuNodes;
-  const int64_t v = v0 + int(threadIdx.x) % kGuNodes;
+  const int grp = int(threadIdx.x) / 32;
+  const int64_t v = v0 + int(threadIdx.x) % 32;
   const int64_t base = rowmap[v0];
   const double ih[3] = {ih0, ih1, ih2};
   if (v < v1) {
@@ -2381,84 +2403,87 @@ __global__ void __launch_bounds__(15 * kGuNodes) k_bgradient_x(BoxDims d, double
     auto inside = [&](int i, int j, int k) {
       return i >= 0 && i <= d.nx && j >= 0 && j <= d.ny && k >= 0 && k <= d.nz;
     };
-    if (inside(vi + E.off[sl][0], vj + E.off[sl][1], vk + E.off[sl][2])) {
-      int rank = sl;
-      if (vi == 0 || vj == 0 || vk == 0 || vi == d.nx || vj == d.ny || vk == d.nz) {
-        rank = 0;
-        for (int q = 0; q < sl; ++q) rank += inside(vi + E.off[q][0], vj + E.off[q][1], vk + E.off[q][2]) ? 1 : 0;
-      }
-      double K[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-      for (int o = 0; o < 8; ++o) {
-        const int n = E.count[sl][o];
-        if (n == 0) continue;
-        const int oi = vi - (o & 1), oj = vj - ((o >> 1) & 1), ok = vk - (o >> 2);
-        if (oi < 0 || oj < 0 || ok < 0 || oi >= d.nx || oj >= d.ny || ok >= d.nz) continue;
-        const int64_t h = oi + int64_t(d.nx) * (oj + int64_t(d.ny) * ok);
-        for (int e = 0; e < n; ++e) {
-          const int code = E.tet[sl][o][e], t = code & 7, mv = (code >> 3) & 3, mw = code >> 5;
-          double rho;
-          if (layout == PA_CONTROL_CELL) {
-            rho = z[6 * h + t];
-          } else {
-            rho = 0.0;
+    for (int gq = 0; gq < E.group_n[grp]; ++gq) {
+      const int sl = E.group[grp][gq];
+      if (inside(vi + E.off[sl][0], vj + E.off[sl][1], vk + E.off[sl][2])) {
+        int rank = sl;
+        if (vi == 0 || vj == 0 || vk == 0 || vi == d.nx || vj == d.ny || vk == d.nz) {
+          rank = 0;
+          for (int q = 0; q < sl; ++q) rank += inside(vi + E.off[q][0], vj + E.off[q][1], vk + E.off[q][2]) ? 1 : 0;
+        }
+        double K[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int o = 0; o < 8; ++o) {
+          const int n = E.count[sl][o];
+          if (n == 0) continue;
+          const int oi = vi - (o & 1), oj = vj - ((o >> 1) & 1), ok = vk - (o >> 2);
+          if (oi < 0 || oj < 0 || ok < 0 || oi >= d.nx || oj >= d.ny || ok >= d.nz) continue;
+          const int64_t h = oi + int64_t(d.nx) * (oj + int64_t(d.ny) * ok);
+          for (int e = 0; e < n; ++e) {
+            const int code = E.tet[sl][o][e], t = code & 7, mv = (code >> 3) & 3, mw = code >> 5;
+            double rho;
+            if (layout == PA_CONTROL_CELL) {
+              rho = z[6 * h + t];
+            } else {
+              rho = 0.0;
+              for (int m = 0; m < 4; ++m) {
+                const int c = path_vertex(t, m);
+                rho += 0.25 * z[(oi + (c & 1)) +
+                                int64_t(d.px) * ((oj + ((c >> 1) & 1)) + int64_t(d.py) * (ok + (c >> 2)))];
+              }
+            }
+            const double w = simp(rho, p, pmin);
+            // H = sum_m u_m g_m^T over the tet's path vertices
+            double H[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
             for (int m = 0; m < 4; ++m) {
               const int c = path_vertex(t, m);
-              rho += 0.25 * z[(oi + (c & 1)) +
-                              int64_t(d.px) * ((oj + ((c >> 1) & 1)) + int64_t(d.py) * (ok + (c >> 2)))];
-            }
-          }
-          const double w = simp(rho, p, pmin);
-          // H = sum_m u_m g_m^T over the tet's path vertices
-          double H[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-          for (int m = 0; m < 4; ++m) {
-            const int c = path_vertex(t, m);
-            const int64_t node = (oi + (c & 1)) + int64_t(d.px) * ((oj + ((c >> 1) & 1)) + int64_t(d.py) * (ok + (c >> 2)));
-            double gm[3];
+              const int64_t node = (oi + (c & 1)) + int64_t(d.px) * ((oj + ((c >> 1) & 1)) + int64_t(d.py) * (ok + (c >> 2)));
+              double gm[3];
 #pragma unroll
-            for (int a = 0; a < 3; ++a) gm[a] = E.grad[t][m][a] * ih[a];
+              for (int a = 0; a < 3; ++a) gm[a] = E.grad[t][m][a] * ih[a];
+#pragma unroll
+              for (int i = 0; i < 3; ++i) {
+                const double ui = u[3 * node + i];
+#pragma unroll
+                for (int a = 0; a < 3; ++a) H[i][a] = fma(ui, gm[a], H[i][a]);
+              }
+            }
+            const double tr = H[0][0] + H[1][1] + H[2][2];
+            double S[3][3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+              for (int j = 0; j < 3; ++j)
+                S[i][j] = w * ((i == j ? iso.lam * tr : 0.0) + iso.mu * (H[i][j] + H[j][i]));
+            double gv[3], gw[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+              gv[a] = E.grad[t][mv][a] * ih[a];
+              gw[a] = E.grad[t][mw][a] * ih[a];
+            }
+            double Sgw[3], Sgv[3], Htv[3], Htw[3];
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
-              const double ui = u[3 * node + i];
-#pragma unroll
-              for (int a = 0; a < 3; ++a) H[i][a] = fma(ui, gm[a], H[i][a]);
+              Sgw[i] = S[i][0] * gw[0] + S[i][1] * gw[1] + S[i][2] * gw[2];
+              Sgv[i] = S[i][0] * gv[0] + S[i][1] * gv[1] + S[i][2] * gv[2];
+              Htv[i] = H[0][i] * gv[0] + H[1][i] * gv[1] + H[2][i] * gv[2];
+              Htw[i] = H[0][i] * gw[0] + H[1][i] * gw[1] + H[2][i] * gw[2];
             }
-          }
-          const double tr = H[0][0] + H[1][1] + H[2][2];
-          double S[3][3];
+            const double gvgw = gv[0] * gw[0] + gv[1] * gw[1] + gv[2] * gw[2];
 #pragma unroll
-          for (int i = 0; i < 3; ++i)
+            for (int k = 0; k < 3; ++k) {
+              const double trD = -Htv[k];
 #pragma unroll
-            for (int j = 0; j < 3; ++j)
-              S[i][j] = w * ((i == j ? iso.lam * tr : 0.0) + iso.mu * (H[i][j] + H[j][i]));
-          double gv[3], gw[3];
-#pragma unroll
-          for (int a = 0; a < 3; ++a) {
-            gv[a] = E.grad[t][mv][a] * ih[a];
-            gw[a] = E.grad[t][mw][a] * ih[a];
-          }
-          double Sgw[3], Sgv[3], Htv[3], Htw[3];
-#pragma unroll
-          for (int i = 0; i < 3; ++i) {
-            Sgw[i] = S[i][0] * gw[0] + S[i][1] * gw[1] + S[i][2] * gw[2];
-            Sgv[i] = S[i][0] * gv[0] + S[i][1] * gv[1] + S[i][2] * gv[2];
-            Htv[i] = H[0][i] * gv[0] + H[1][i] * gv[1] + H[2][i] * gv[2];
-            Htw[i] = H[0][i] * gw[0] + H[1][i] * gw[1] + H[2][i] * gw[2];
-          }
-          const double gvgw = gv[0] * gw[0] + gv[1] * gw[1] + gv[2] * gw[2];
-#pragma unroll
-          for (int k = 0; k < 3; ++k) {
-            const double trD = -Htv[k];
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-              const double dSgw = w * (iso.lam * trD * gw[j] - iso.mu * (H[j][k] * gvgw + gv[j] * Htw[k]));
-              K[3 * k + j] += vol * (gv[k] * Sgw[j] + dSgw - gw[k] * Sgv[j]);
+              for (int j = 0; j < 3; ++j) {
+                const double dSgw = w * (iso.lam * trD * gw[j] - iso.mu * (H[j][k] * gvgw + gv[j] * Htw[k]));
+                K[3 * k + j] += vol * (gv[k] * Sgw[j] + dSgw - gw[k] * Sgv[j]);
+              }
             }
           }
         }
-      }
-      double* dst = stage + 9 * (int64_t(rowmap[v]) - base + rank);
+        double* dst = stage + 9 * (int64_t(rowmap[v]) - base + rank);
 #pragma unroll
-      for (int q = 0; q < 9; ++q) dst[q] = K[q];
+        for (int q = 0; q < 9; ++q) dst[q] = K[q];
+      }
     }
   }
   __syncthreads();
@@ -2500,7 +2525,7 @@ bool box_gradient_u(Problem& P, const double* z, double* entries) {
     H.gu_k0.upload(k0.data(), k0.size(), P.stream);
     std::copy(key, key + 5, H.gu_key);
   }
-  k_bgradient_u<<<int((F.d.N + kGuNodes - 1) / kGuNodes), 15 * kGuNodes, 0, P.stream>>>(
+  k_bgradient_u<<<int((F.d.N + kGuNodes - 1) / kGuNodes), 32 * kGuWarps, 0, P.stream>>>(
       F.d, F.h[0] * F.h[1] * F.h[2] / 6.0, P.ep.p, P.ep.pmin, P.ep.layout, edges, H.gu_k0.get(), z,
       m.d_rowmap.get(), entries);
   PA_LAUNCHED();
@@ -2516,7 +2541,7 @@ bool box_gradient_x(Problem& P, const double* u, const double* z, double* entrie
   static const BoxEdges edges = make_box_edges();
   boxmg_ensure(P);
   const BoxLevel& F = *P.boxmg->L[0];
-  k_bgradient_x<<<int((F.d.N + kGuNodes - 1) / kGuNodes), 15 * kGuNodes, 0, P.stream>>>(
+  k_bgradient_x<<<int((F.d.N + kGuNodes - 1) / kGuNodes), 32 * kGuWarps, 0, P.stream>>>(
       F.d, F.h[0] * F.h[1] * F.h[2] / 6.0, P.ep.p, P.ep.pmin, P.ep.layout, edges, P.ep.iso(), 1.0 / F.h[0],
       1.0 / F.h[1], 1.0 / F.h[2], u, z, m.d_rowmap.get(), entries);
   PA_LAUNCHED();
