@@ -2375,6 +2375,12 @@ __global__ void __launch_bounds__(32 * kGuWarps) k_bgradient_u(BoxDims d, double
   for (int64_t e = threadIdx.x; e < count; e += blockDim.x) vals[9 * base + e] = stage[e];
 }
 
+// barycentric gradients of the six path tets' vertices on the box's hexes
+// (the BoxEdges unit-hex pattern scaled by 1 / h per axis)
+struct TetGrads {
+  double g[6][4][3];
+};
+
 // VectorFunction::gradient_x on a box mesh in its own numbering with sorted
 // columns, by the same (slot group, node) threads as k_bgradient_u: the block at row
 // v, column w holds d R_w / d x_v ([k][j] = d R_w,j / d x_v,k), summed over the
@@ -2386,8 +2392,8 @@ __global__ void __launch_bounds__(32 * kGuWarps) k_bgradient_u(BoxDims d, double
 // with tr D = -(H^T g_b)_k and dS g_a = w (lam tr D g_a - mu (g_b . g_a) H e_k
 // - mu (H^T g_a)_k g_b).  u is read at the tet's four lattice corners.
 __global__ void __launch_bounds__(32 * kGuWarps) k_bgradient_x(BoxDims d, double vol, double p, double pmin,
-                                                             int layout, BoxEdges E, Iso<double> iso, double ih0,
-                                                             double ih1, double ih2, const double* __restrict__ u,
+                                                             int layout, BoxEdges E, Iso<double> iso, TetGrads G,
+                                                             const double* __restrict__ u,
                                                              const double* __restrict__ z,
                                                              const int32_t* __restrict__ rowmap,
                                                              double* __restrict__ vals) {
@@ -2397,7 +2403,6 @@ __global__ void __launch_bounds__(32 * kGuWarps) k_bgradient_x(BoxDims d, double
   const int grp = int(threadIdx.x) / 32;
   const int64_t v = v0 + int(threadIdx.x) % 32;
   const int64_t base = rowmap[v0];
-  const double ih[3] = {ih0, ih1, ih2};
   if (v < v1) {
     const int vi = int(v % d.px), vj = int((v / d.px) % d.py), vk = int(v / (int64_t(d.px) * d.py));
     auto inside = [&](int i, int j, int k) {
@@ -2439,7 +2444,7 @@ __global__ void __launch_bounds__(32 * kGuWarps) k_bgradient_x(BoxDims d, double
               const int64_t node = (oi + (c & 1)) + int64_t(d.px) * ((oj + ((c >> 1) & 1)) + int64_t(d.py) * (ok + (c >> 2)));
               double gm[3];
 #pragma unroll
-              for (int a = 0; a < 3; ++a) gm[a] = E.grad[t][m][a] * ih[a];
+              for (int a = 0; a < 3; ++a) gm[a] = G.g[t][m][a];
 #pragma unroll
               for (int i = 0; i < 3; ++i) {
                 const double ui = u[3 * node + i];
@@ -2457,8 +2462,8 @@ __global__ void __launch_bounds__(32 * kGuWarps) k_bgradient_x(BoxDims d, double
             double gv[3], gw[3];
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
-              gv[a] = E.grad[t][mv][a] * ih[a];
-              gw[a] = E.grad[t][mw][a] * ih[a];
+              gv[a] = G.g[t][mv][a];
+              gw[a] = G.g[t][mw][a];
             }
             double Sgw[3], Sgv[3], Htv[3], Htw[3];
 #pragma unroll
@@ -2541,9 +2546,13 @@ bool box_gradient_x(Problem& P, const double* u, const double* z, double* entrie
   static const BoxEdges edges = make_box_edges();
   boxmg_ensure(P);
   const BoxLevel& F = *P.boxmg->L[0];
+  TetGrads G;
+  for (int t = 0; t < 6; ++t)
+    for (int mm = 0; mm < 4; ++mm)
+      for (int a = 0; a < 3; ++a) G.g[t][mm][a] = edges.grad[t][mm][a] / F.h[a];
   k_bgradient_x<<<int((F.d.N + kGuNodes - 1) / kGuNodes), 32 * kGuWarps, 0, P.stream>>>(
-      F.d, F.h[0] * F.h[1] * F.h[2] / 6.0, P.ep.p, P.ep.pmin, P.ep.layout, edges, P.ep.iso(), 1.0 / F.h[0],
-      1.0 / F.h[1], 1.0 / F.h[2], u, z, m.d_rowmap.get(), entries);
+      F.d, F.h[0] * F.h[1] * F.h[2] / 6.0, P.ep.p, P.ep.pmin, P.ep.layout, edges, P.ep.iso(), G, u, z,
+      m.d_rowmap.get(), entries);
   PA_LAUNCHED();
   return true;
 }
