@@ -306,13 +306,15 @@ def test_box_gradient_z_any_vertex_order(pa, oracle_lib):
     assert rel_inf(g, g_cell) <= 1e-12
 
 
+@pytest.mark.parametrize("dims", [(8, 5, 4), (37, 2, 3)])
 @pytest.mark.parametrize("layout,lengths", [("cell", (8.0, 5.0, 4.0)), ("nodal", (4.0, 7.5, 2.0))])
-def test_box_assembled_gradient_u(pa, oracle_lib, layout, lengths):
+def test_box_assembled_gradient_u(pa, oracle_lib, layout, lengths, dims):
     """VectorFunction::gradient_u on a box mesh: the per-block lattice
     assembly (no atomics) equals the oracle's block CRS matrix and, to
     rounding, the per-cell atomic assembly (box kernels switched off);
-    reordered columns (pa_mesh_set_graph) fall back to the per-cell one."""
-    dims = (8, 5, 4)
+    reordered columns (pa_mesh_set_graph) fall back to the per-cell one.
+    37x2x3: rows longer than a CTA's 32 nodes, CTAs across rows, and nearly
+    every node on the boundary."""
     mesh = pa.Mesh.box(*dims, *lengths)
     assert mesh.box_kernels
     cells, coords = mesh.arrays()
@@ -367,13 +369,13 @@ def test_box_fp64_jacobi_pcg_deterministic(pa, oracle_lib, dims):
     assert abs(stt["iterations"] - st["iterations"]) <= 0.05 * st["iterations"] + 2, (st, stt)
 
 
+@pytest.mark.parametrize("dims", [(8, 5, 4), (37, 2, 3)])
 @pytest.mark.parametrize("layout,lengths", [("cell", (8.0, 5.0, 4.0)), ("nodal", (4.0, 7.5, 2.0))])
-def test_box_assembled_gradient_x(pa, oracle_lib, layout, lengths):
+def test_box_assembled_gradient_x(pa, oracle_lib, layout, lengths, dims):
     """VectorFunction::gradient_x on a box mesh: the per-block lattice
     assembly of the volume term (closed-form shape derivatives, no atomics)
     plus the surface loads equals the oracle's dR/dx and, to rounding, the
     per-cell dual-number kernel with atomics (box kernels switched off)."""
-    dims = (8, 5, 4)
     mesh = pa.Mesh.box(*dims, *lengths)
     assert mesh.box_kernels
     cells, coords = mesh.arrays()
